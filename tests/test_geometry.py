@@ -1,0 +1,58 @@
+"""The project's geometry builder against fixtures produced by the reference's own
+init code (geom_init.py, make_pupil.py).  Integer maps must match bit for bit."""
+
+import numpy as np
+import pytest
+
+from aob200 import geometry as G
+
+SH = {
+    "sh16": G.ShParams(nxsub=16, npix=8, pixsize=0.3, wavelength_um=0.7, fracsub=0.5, gsmag=8.0),
+    "sh40": G.ShParams(nxsub=40, npix=6, pixsize=0.36, wavelength_um=0.7, fracsub=0.5, gsmag=8.0),
+    "sh8": G.ShParams(nxsub=8, npix=2, pixsize=0.3, wavelength_um=0.7, fracsub=0.5, gsmag=8.0),
+}
+SH_PUP = {"sh16": 128, "sh40": 240, "sh8": 48}
+
+
+@pytest.mark.parametrize("name", sorted(SH))
+def test_sh_geometry_matches_reference(name, golden):
+    ref = golden("geom_" + name)
+    g = G.sh_geometry(SH[name], SH_PUP[name], diam=8.0, cobs=0.14, ittime=0.001)
+    for k in ("pdiam", "nfft", "ntot", "nrebin", "nvalid"):
+        assert getattr(g, k) == int(ref[k]), k
+    assert g.tel.n == int(ref["n"])
+    for k in ("spupil", "mpupil", "ipupil"):
+        np.testing.assert_array_equal(getattr(g.tel, k), ref[k])
+    for k in ("isvalid", "validsubsx", "validsubsy", "validpuppixx", "validpuppixy",
+              "phasemap", "binmap", "hrmap"):
+        a = getattr(g, k)
+        assert a.dtype == ref[k].dtype, k
+        np.testing.assert_array_equal(a, ref[k], err_msg=k)
+    for k in ("fluxPerSub", "fluxPerSub_grid", "halfxy"):
+        np.testing.assert_array_equal(getattr(g, k), ref[k], err_msg=k)
+    # tip/tilt projection (not on the image-formation path): float rounding only
+    np.testing.assert_allclose(g.ttprojmat, ref["ttprojmat"], rtol=1e-6, atol=1e-7)
+    # the reference keeps these two through float32 parameter setters
+    assert np.float32(g.pixsize) == np.float32(ref["pixsize"])
+    assert np.float32(g.qpixsize) == np.float32(ref["qpixsize"])
+    assert g.nphotons == pytest.approx(float(ref["nphotons"]), rel=1e-6)
+
+
+PYR = {
+    "pyr16": (G.PyrParams(nxsub=16, wavelength_um=0.7, ampl=3.0, npts=8, pup_sep=12, fssize=3.2), 64),
+    "pyr50": (G.PyrParams(nxsub=50, wavelength_um=1.075, ampl=3.0, npts=24, pup_sep=32, fssize=3.2), 100),
+}
+
+
+@pytest.mark.parametrize("name", sorted(PYR))
+def test_pyr_geometry_matches_reference(name, golden):
+    ref = golden("geom_" + name)
+    p, pup = PYR[name]
+    g = G.pyr_geometry(p, pup, diam=8.0, cobs=0.14, ittime=0.001)
+    for k in ("pdiam", "nfft", "ntot", "nrebin", "nvalid"):
+        assert getattr(g, k) == int(ref[k]), k
+    np.testing.assert_array_equal(g.tel.mpupil, ref["mpupil"])
+    for k in ("validsubsx", "validsubsy", "isvalid", "phasemap"):
+        np.testing.assert_array_equal(getattr(g, k), ref[k], err_msg=k)
+    for k in ("halfxy", "pyr_cx", "pyr_cy", "sincar", "submask", "fluxPerSub"):
+        np.testing.assert_array_equal(getattr(g, k), ref[k], err_msg=k)
