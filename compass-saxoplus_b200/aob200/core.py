@@ -1,0 +1,339 @@
+"""Python objects over the C ABI: SH sensor, centroider, LS controller.
+
+These are the host-side mirror of the reference's SutraWfsSH /
+SutraCentroider* / SutraControllerLs (see include/aob200.h for the file:line
+of each replaced interface).  Host arrays follow the reference's convention:
+numpy arrays indexed [x, y] with x the fastest device index (Fortran order).
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import addr, call, d2h, h2d, host_array
+
+CENTRO_TYPES = {"cog": 0, "tcog": 1, "wcog": 2, "pyr": 3, "pyrhr": 3}
+PRECISIONS = {"f32": 0, "fp32": 0, "float32": 0, "bf16": 1, "bfloat16": 1, "fp8": 2, "e4m3": 2}
+
+
+class DeviceArray:
+    """View of a device buffer owned by the library (the carma object role).
+
+    ``np.array(obj)`` / ``obj.host()`` copy it to the host, reshaped to
+    ``shape`` in Fortran order like the reference's carma arrays.
+    """
+
+    def __init__(self, ptr: int, n: int, dtype, shape=None, owner=None):
+        self.ptr = int(ptr or 0)
+        self.n = int(n)
+        self.dtype = np.dtype(dtype)
+        self.shape = tuple(shape) if shape is not None else (self.n,)
+        self._owner = owner
+
+    def host(self) -> np.ndarray:
+        if self.ptr == 0 or self.n == 0:
+            return np.zeros(self.shape, dtype=self.dtype)
+        return d2h(self.ptr, self.n, self.dtype).reshape(self.shape, order="F")
+
+    def __array__(self, dtype=None, copy=None):
+        a = self.host()
+        return a.astype(dtype) if dtype is not None else a
+
+    def set(self, a) -> None:
+        a = host_array(a, self.dtype)
+        if a.size != self.n:
+            raise ValueError(f"size mismatch: {a.size} != {self.n}")
+        h2d(self.ptr, a)
+
+    def get_dims(self):
+        return self.shape
+
+    def __len__(self):
+        return self.shape[0]
+
+
+def _buffer(fn: str, handle, which: str, dtype, shape=None, owner=None) -> DeviceArray:
+    p = ctypes.c_void_p()
+    n = ctypes.c_int64()
+    call(fn, handle, which.encode(), ctypes.addressof(p), ctypes.addressof(n))
+    if shape is not None and int(np.prod(shape)) != n.value:
+        shape = None
+    return DeviceArray(p.value or 0, n.value, dtype, shape, owner)
+
+
+class ShWfs:
+    """Shack-Hartmann sensor on one GPU (SutraWfsSH)."""
+
+    def __init__(self, nxsub, nvalid, npix, nphase, nrebin, nfft, ntot, npup, pdiam, nphot,
+                 nphot4imat=0.0, device=0, lambda_um=0.5):
+        self.h = ctypes.c_void_p()
+        call("aob_sh_create", ctypes.addressof(self.h), int(device), int(nxsub), int(nvalid), int(npix),
+             int(nphase), int(nrebin), int(nfft), int(ntot), int(npup), float(pdiam), float(nphot),
+             float(nphot4imat))
+        self.nxsub, self.nvalid, self.npix, self.nphase = int(nxsub), int(nvalid), int(npix), int(nphase)
+        self.nrebin, self.nfft, self.ntot, self.npup = int(nrebin), int(nfft), int(ntot), int(npup)
+        self.pdiam, self.nphot, self.nphot4imat = float(pdiam), float(nphot), float(nphot4imat)
+        self.device = int(device)
+        self.noise = -1.0
+        self.lambda_um = float(lambda_um)
+        call("aob_sh_set_lambda", self.h, float(lambda_um))
+
+    @classmethod
+    def from_geometry(cls, g, device=0, noise=-1.0, seed=1234):
+        w = cls(g.nxsub, g.nvalid, g.npix, g.pdiam, g.nrebin, g.nfft, g.ntot, g.tel.n, g.subapd,
+                g.nphotons, device=device, lambda_um=g.wavelength_um)
+        w.load_arrays(g.phasemap, g.hrmap, g.binmap, g.halfxy, g.fluxPerSub, g.validsubsx, g.validsubsy,
+                      g.validpuppixx, g.validpuppixy)
+        w.set_pupil(g.tel.mpupil)
+        w.set_noise(noise, seed)
+        return w
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value and _lib._lib is not None:
+            _lib.lib().aob_sh_destroy(h)
+            self.h = None
+
+    def load_arrays(self, phasemap, hrmap, binmap, offsets, fluxPerSub, validsubsx, validsubsy,
+                    istart, jstart, ttprojmat=None, kernel=None):
+        i32, f32 = np.int32, np.float32
+        keep = [host_array(binmap, i32), host_array(offsets, f32), host_array(fluxPerSub, f32),
+                host_array(validsubsx, i32), host_array(validsubsy, i32), host_array(istart, i32),
+                host_array(jstart, i32)]
+        call("aob_sh_load_arrays", self.h, None, None, *[k.ctypes.data for k in keep], None, None)
+
+    def set_pupil(self, pupil):
+        a = host_array(pupil, np.float32)
+        if a.size != self.npup * self.npup:
+            raise ValueError("pupil must be npup x npup")
+        call("aob_sh_set_pupil", self.h, a.ctypes.data)
+
+    def set_noise(self, noise, seed=1234):
+        self.noise = float(noise)
+        call("aob_sh_set_noise", self.h, float(noise), int(seed))
+
+    def set_lambda(self, lam):
+        self.lambda_um = float(lam)
+        call("aob_sh_set_lambda", self.h, float(lam))
+
+    def set_nphot(self, nphot):
+        self.nphot = float(nphot)
+        call("aob_sh_set_nphot", self.h, float(nphot))
+
+    @property
+    def frame(self) -> int:
+        f = ctypes.c_uint64()
+        call("aob_sh_get_frame", self.h, ctypes.addressof(f))
+        return f.value
+
+    @frame.setter
+    def frame(self, v):
+        call("aob_sh_set_frame", self.h, int(v))
+
+    def buffer(self, which, dtype=np.float32, shape=None) -> DeviceArray:
+        return _buffer("aob_sh_buffer", self.h, which, dtype, shape, self)
+
+    @property
+    def d_phase(self):
+        return self.buffer("phase", shape=(self.npup, self.npup))
+
+    @property
+    def d_bincube(self):
+        return self.buffer("bincube", shape=(self.npix, self.npix, self.nvalid))
+
+    @property
+    def d_binimg(self):
+        n = self.npix * self.nxsub
+        return self.buffer("binimg", shape=(n, n))
+
+    @property
+    def d_intensities(self):
+        return self.buffer("intensities")
+
+    def set_phase(self, phase):
+        self.d_phase.set(phase)
+
+    def comp_image(self, noise=True, stream=None):
+        call("aob_sh_comp_image", self.h, 1 if noise else 0, stream)
+
+    def fill_binimage(self, stream=None):
+        call("aob_sh_fill_binimage", self.h, stream)
+
+
+class Centroider:
+    """CoG / tCoG / wCoG centroider (SutraCentroider*)."""
+
+    def __init__(self, nvalid, offset, scale, typec="cog", device=0, wfs: ShWfs | None = None):
+        self.h = ctypes.c_void_p()
+        self.type = typec
+        call("aob_centro_create", ctypes.addressof(self.h), int(device), CENTRO_TYPES[typec], int(nvalid),
+             float(offset), float(scale))
+        self.nvalid = int(nvalid)
+        self.wfs = None
+        if wfs is not None:
+            self.attach(wfs)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value and _lib._lib is not None:
+            _lib.lib().aob_centro_destroy(h)
+            self.h = None
+
+    def attach(self, wfs):
+        self.wfs = wfs
+        call("aob_centro_attach_wfs", self.h, wfs.h if wfs is not None else None)
+
+    def set_npix(self, npix):
+        call("aob_centro_set_npix", self.h, int(npix))
+
+    def set_scale(self, v):
+        call("aob_centro_set_scale", self.h, float(v))
+
+    def set_offset(self, v):
+        call("aob_centro_set_offset", self.h, float(v))
+
+    def set_threshold(self, v):
+        call("aob_centro_set_threshold", self.h, float(v))
+
+    def set_slope_order(self, order):
+        call("aob_centro_set_slope_order", self.h, int(order))
+
+    def load_validpos(self, vx, vy, n=None):
+        a, b = host_array(vx, np.int32), host_array(vy, np.int32)
+        call("aob_centro_load_validpos", self.h, a.ctypes.data, b.ctypes.data, int(a.size))
+
+    def set_centroids_ref(self, ref):
+        a = host_array(ref, np.float32)
+        call("aob_centro_set_centroids_ref", self.h, a.ctypes.data)
+
+    def load_weights(self, w, ndim=None):
+        a = host_array(w, np.float32)
+        call("aob_centro_load_weights", self.h, a.ctypes.data, int(a.size))
+
+    def load_img(self, img, m=None, n=None):
+        img = np.asarray(img, dtype=np.float32)
+        a = host_array(img, np.float32)
+        call("aob_centro_load_img", self.h, a.ctypes.data, int(img.shape[0]), int(img.shape[1]))
+
+    def set_dark(self, d, n=None):
+        a = host_array(d, np.float32)
+        call("aob_centro_set_dark", self.h, a.ctypes.data, int(np.sqrt(a.size)))
+
+    def set_flat(self, f, n=None):
+        a = host_array(f, np.float32)
+        call("aob_centro_set_flat", self.h, a.ctypes.data, int(np.sqrt(a.size)))
+
+    def calibrate_img(self, stream=None):
+        call("aob_centro_calibrate_img", self.h, stream)
+
+    def get_cog(self, dev_slopes: int, stream=None):
+        call("aob_centro_get_cog", self.h, dev_slopes, stream)
+
+    def buffer(self, which, dtype=np.float32, shape=None):
+        return _buffer("aob_centro_buffer", self.h, which, dtype, shape, self)
+
+    def params(self):
+        t, nv, npx = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        o, s, th = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        call("aob_centro_get_params", self.h, *[ctypes.addressof(x) for x in (t, nv, npx, o, s, th)])
+        return dict(type=t.value, nvalid=nv.value, npix=npx.value, offset=o.value, scale=s.value,
+                    threshold=th.value)
+
+
+class LsController:
+    """Least-squares controller (SutraControllerLs + SutraController)."""
+
+    def __init__(self, nslope, nactu, delay=0.0, device=0):
+        self.h = ctypes.c_void_p()
+        call("aob_ls_create", ctypes.addressof(self.h), int(device), int(nslope), int(nactu), float(delay))
+        self.nslope, self.nactu = int(nslope), int(nactu)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value and _lib._lib is not None:
+            _lib.lib().aob_ls_destroy(h)
+            self.h = None
+
+    def _vec(self, fn, a, dtype=np.float32, *extra):
+        a = host_array(a, dtype)
+        call(fn, self.h, a.ctypes.data, *extra)
+        return a
+
+    def set_cmat(self, cmat):
+        cmat = np.asarray(cmat)
+        if cmat.shape != (self.nactu, self.nslope):
+            raise ValueError(f"cmat must be ({self.nactu}, {self.nslope})")
+        self._vec("aob_ls_set_cmat", cmat)
+
+    def set_imat(self, imat):
+        imat = np.asarray(imat)
+        if imat.shape != (self.nslope, self.nactu):
+            raise ValueError(f"imat must be ({self.nslope}, {self.nactu})")
+        self._vec("aob_ls_set_imat", imat)
+
+    def set_modal_gains(self, g):
+        self._vec("aob_ls_set_modal_gains", g)
+
+    def set_gain(self, g):
+        call("aob_ls_set_gain", self.h, float(g))
+
+    def set_delay(self, d):
+        call("aob_ls_set_delay", self.h, float(d))
+
+    def set_open_loop(self, ol, reset=True):
+        call("aob_ls_set_open_loop", self.h, int(ol), 1 if reset else 0)
+
+    def set_com_range(self, lo, hi):
+        call("aob_ls_set_com_range", self.h, float(lo), float(hi))
+
+    def set_com(self, com, n=None):
+        a = host_array(com, np.float32)
+        call("aob_ls_set_com", self.h, a.ctypes.data, int(a.size))
+
+    def set_centroids(self, s):
+        a = host_array(s, np.float32)
+        call("aob_ls_set_centroids", self.h, a.ctypes.data, int(a.size))
+
+    def set_precision(self, prec):
+        call("aob_ls_set_precision", self.h, PRECISIONS[prec] if isinstance(prec, str) else int(prec))
+
+    def comp_com(self, stream=None):
+        call("aob_ls_comp_com", self.h, stream)
+
+    def clip(self, stream=None):
+        call("aob_ls_clip", self.h, stream)
+
+    def comp_voltage(self, stream=None):
+        call("aob_ls_comp_voltage", self.h, stream)
+
+    def add_perturb(self, name, pert, n):
+        a = host_array(np.asarray(pert, dtype=np.float32).reshape(int(n), self.nactu, order="F"), np.float32)
+        call("aob_ls_add_perturb", self.h, name.encode(), a.ctypes.data, int(n))
+
+    def remove_perturb(self, name):
+        call("aob_ls_remove_perturb", self.h, name.encode())
+
+    def enable_perturb(self, name, on=True):
+        call("aob_ls_enable_perturb", self.h, name.encode(), 1 if on else 0)
+
+    def reset_perturb(self):
+        call("aob_ls_reset_perturb", self.h)
+
+    def svdec_imat(self):
+        call("aob_ls_svdec_imat", self.h)
+
+    def build_cmat(self, nfilt):
+        call("aob_ls_build_cmat", self.h, int(nfilt))
+
+    def buffer(self, which, dtype=np.float32, shape=None):
+        return _buffer("aob_ls_buffer", self.h, which, dtype, shape, self)
+
+    def params(self):
+        ns, na, ol, pr = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        de, ga, lo, hi = ctypes.c_float(), ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        call("aob_ls_get_params", self.h, *[ctypes.addressof(x) for x in (ns, na, de, ga, ol, lo, hi, pr)])
+        return dict(nslope=ns.value, nactu=na.value, delay=de.value, gain=ga.value, open_loop=ol.value,
+                    volt_min=lo.value, volt_max=hi.value, prec=pr.value)

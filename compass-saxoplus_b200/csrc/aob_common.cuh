@@ -1,0 +1,166 @@
+// Shared device helpers: error plumbing, Philox4x32-10, noise samplers,
+// warp reductions.  sm_100a only.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <stdexcept>
+#include <string>
+
+namespace aob {
+
+// ---------------------------------------------------------------------------
+// host-side error plumbing: every C entry point catches aob::Error and turns
+// it into AOB_ERR plus a thread-local message.
+struct Error : std::runtime_error {
+  explicit Error(const std::string &m) : std::runtime_error(m) {}
+};
+
+void set_last_error(const std::string &msg);
+
+inline void cuda_check(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) throw Error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define AOB_CUDA(call) ::aob::cuda_check((call), #call)
+#define AOB_LAUNCH_CHECK(name) ::aob::cuda_check(cudaGetLastError(), name)
+#define AOB_REQUIRE(cond, msg)                 \
+  do {                                         \
+    if (!(cond)) throw ::aob::Error(msg);      \
+  } while (0)
+
+// RAII device buffer
+template <typename T>
+struct DevBuf {
+  T *p = nullptr;
+  int64_t n = 0;
+  DevBuf() = default;
+  explicit DevBuf(int64_t count) { alloc(count); }
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf &operator=(DevBuf &&o) noexcept {
+    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void alloc(int64_t count) {
+    release();
+    n = count;
+    if (count > 0) {
+      AOB_CUDA(cudaMalloc(&p, sizeof(T) * (size_t)count));
+      AOB_CUDA(cudaMemset(p, 0, sizeof(T) * (size_t)count));
+    }
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void upload(const T *host, int64_t count) {
+    AOB_REQUIRE(count <= n, "upload larger than buffer");
+    if (count > 0) AOB_CUDA(cudaMemcpy(p, host, sizeof(T) * (size_t)count, cudaMemcpyHostToDevice));
+  }
+  size_t bytes() const { return sizeof(T) * (size_t)n; }
+};
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon et al., SC'11).  Counter layout used by the sensors:
+// c0 = pixel index, c1 = frame, c2 = stream tag, c3 = draw number.
+struct U4 {
+  uint32_t x, y, z, w;
+};
+
+__host__ __device__ __forceinline__ void mulhilo32(uint32_t a, uint32_t b, uint32_t &hi, uint32_t &lo) {
+#ifdef __CUDA_ARCH__
+  hi = __umulhi(a, b);
+  lo = a * b;
+#else
+  uint64_t p = (uint64_t)a * (uint64_t)b;
+  hi = (uint32_t)(p >> 32);
+  lo = (uint32_t)p;
+#endif
+}
+
+__host__ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    uint32_t hi0, lo0, hi1, lo1;
+    mulhilo32(0xD2511F53u, c.x, hi0, lo0);
+    mulhilo32(0xCD9E8D57u, c.z, hi1, lo1);
+    U4 n;
+    n.x = hi1 ^ c.y ^ k0;
+    n.y = lo1;
+    n.z = hi0 ^ c.w ^ k1;
+    n.w = lo0;
+    c = n;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+
+enum : uint32_t { TAG_POISSON = 0, TAG_GAUSS = 1 };
+
+__device__ __forceinline__ double u01(uint32_t x) {
+  return __dmul_rn(__dadd_rn((double)x, 0.5), 2.3283064365386963e-10);  // (x + 0.5) / 2^32
+}
+
+// Poisson deviate: inversion for small means, PTRS (Hoermann 1993) otherwise.
+// float64 arithmetic with explicit rounding intrinsics so that no multiply-add
+// is contracted -- the CPU oracle performs the same operation sequence.
+static __device__ __noinline__ double poisson_sample(double lam, uint32_t idx, uint32_t frame, uint32_t k0,
+                                              uint32_t k1) {
+  if (!(lam > 0.0)) return 0.0;
+  U4 w = philox4x32_10(U4{idx, frame, TAG_POISSON, 0u}, k0, k1);
+  if (lam < 10.0) {
+    double u = u01(w.x);
+    double p = exp(-lam);
+    double f = p;
+    int k = 0;
+    while (u > f && k < 1000) {
+      k += 1;
+      p = __dmul_rn(p, __ddiv_rn(lam, (double)k));
+      f = __dadd_rn(f, p);
+    }
+    return (double)k;
+  }
+  const double slam = sqrt(lam);
+  const double loglam = log(lam);
+  const double b = __dadd_rn(0.931, __dmul_rn(2.53, slam));
+  const double a = __dadd_rn(-0.059, __dmul_rn(0.02483, b));
+  const double invalpha = __dadd_rn(1.1239, __ddiv_rn(1.1328, __dadd_rn(b, -3.4)));
+  const double vr = __dadd_rn(0.9277, -__ddiv_rn(3.6224, __dadd_rn(b, -2.0)));
+  for (uint32_t d = 0; d < 64u; ++d) {
+    if (d > 0) w = philox4x32_10(U4{idx, frame, TAG_POISSON, d}, k0, k1);
+    double u = __dadd_rn(u01(w.x), -0.5);
+    double v = u01(w.y);
+    double us = __dadd_rn(0.5, -fabs(u));
+    double t = __dadd_rn(__dadd_rn(__dmul_rn(__dadd_rn(__ddiv_rn(__dmul_rn(2.0, a), us), b), u), lam),
+                         0.43);
+    double k = floor(t);
+    if (us >= 0.07 && v <= vr) return k;
+    if (k < 0.0 || (us < 0.013 && v > us)) continue;
+    double lhs = __dadd_rn(__dadd_rn(log(v), log(invalpha)),
+                           -log(__dadd_rn(__ddiv_rn(a, __dmul_rn(us, us)), b)));
+    double rhs = __dadd_rn(__dadd_rn(-lam, __dmul_rn(k, loglam)), -lgamma(__dadd_rn(k, 1.0)));
+    if (lhs <= rhs) return k;
+  }
+  return floor(lam + 0.5);
+}
+
+__device__ __forceinline__ double gauss_sample(uint32_t idx, uint32_t frame, uint32_t k0, uint32_t k1) {
+  U4 w = philox4x32_10(U4{idx, frame, TAG_GAUSS, 0u}, k0, k1);
+  double u1 = u01(w.x);
+  double u2 = u01(w.z);
+  return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+}
+
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace aob

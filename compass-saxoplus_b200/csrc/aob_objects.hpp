@@ -1,0 +1,130 @@
+// Host-side objects behind the C ABI.  Each owns its device buffers; the C
+// entry points in capi.cu are thin wrappers that translate exceptions into
+// status codes.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <deque>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "aob200.h"
+#include "aob_common.cuh"
+
+struct aob_centro;
+
+// ---------------------------------------------------------------------------
+// Shack-Hartmann sensor (replaces SutraWfsSH, libsutra/src.cpp/sutra_wfs_sh.cpp)
+struct aob_sh {
+  int device = 0;
+  int nxsub = 0, nvalid = 0, npix = 0, nphase = 0, nrebin = 0, nfft = 0, ntot = 0, npup = 0;
+  float pdiam = 0.f, nphot = 0.f, nphot4imat = 0.f;
+  float lambda_um = 0.5f;
+  float noise = -1.f;
+  int64_t seed = 1234;
+  uint64_t frame = 0;
+  bool loaded = false;
+
+  // geometry (device)
+  aob::DevBuf<float> phase;        // npup x npup guide-star phase [um]
+  aob::DevBuf<float> pupil;        // npup x npup amplitude
+  aob::DevBuf<int32_t> istart, jstart, validsubsx, validsubsy, binmap;
+  aob::DevBuf<float> offsets, fluxPerSub;
+  // pruned-DFT tables derived from binmap at load time
+  int nu = 0, nv = 0;
+  aob::DevBuf<int32_t> ulist, vlist, cbin;
+  // outputs
+  aob::DevBuf<float> bincube, binimg, intensities, slopes;
+  // centroider whose slopes are fused into comp_image (may be null)
+  aob_centro *fused = nullptr;
+  uint64_t image_gen = 0;  // bumped whenever binimg changes
+
+  aob_sh(int device, int nxsub, int nvalid, int npix, int nphase, int nrebin, int nfft, int ntot,
+         int npup, float pdiam, float nphot, float nphot4imat);
+  void load_arrays(const int32_t *binmap, const float *offsets, const float *fluxPerSub,
+                   const int32_t *validsubsx, const int32_t *validsubsy, const int32_t *istart,
+                   const int32_t *jstart);
+  void comp_image(bool noise, cudaStream_t s);
+  void fill_binimage(cudaStream_t s);
+  size_t smem_bytes() const;
+};
+
+// ---------------------------------------------------------------------------
+// centroiders (replaces SutraCentroiderCog / Tcog / Wcog)
+struct aob_centro {
+  int device = 0;
+  int type = 0;
+  int nvalid = 0;
+  int npix = 0;
+  float offset = 0.f, scale = 1.f, threshold = 0.f;
+  int order = 0;
+  aob_sh *wfs = nullptr;
+  aob::DevBuf<int32_t> validx, validy;
+  aob::DevBuf<float> ref, weights, intensities;
+  int weights_per_sub = 0;  // 0: one npix^2 map, 1: npix^2*nvalid
+  // image path when not attached to a sensor (load_img + calibrate_img)
+  int img_m = 0, img_n = 0;
+  aob::DevBuf<float> img_raw, img, dark, flat;
+  // fused slopes staged by the sensor kernel
+  aob::DevBuf<float> fused_slopes;
+  uint64_t fused_gen = ~0ull;     // sensor image generation they belong to
+  uint64_t params_gen = 0;        // bumped on every parameter change
+  uint64_t fused_params_gen = ~0ull;
+
+  aob_centro(int device, int type, int nvalid, float offset, float scale);
+  void touch() { ++params_gen; }
+  bool fused_ready() const;
+  void get_cog(float *dev_slopes, cudaStream_t s);
+  void calibrate(cudaStream_t s);
+};
+
+// ---------------------------------------------------------------------------
+// least-squares controller (replaces SutraControllerLs + SutraController)
+struct aob_ls {
+  int device = 0;
+  int nslope = 0, nactu = 0;
+  float delay = 0.f, a = 0.f, b = 1.f, gain = 0.f;
+  int open_loop = 0;
+  float volt_min = -1.0e6f, volt_max = 1.0e6f;
+  int prec = 0;
+  int nblocks = 0;  // MVM grid size (chosen by the autotuner, 0 = default)
+
+  aob::DevBuf<float> centroids, err, com_clipped, gains, cmat, imat, eigenvals_f;
+  std::deque<aob::DevBuf<float>> ring;  // command history, back() = current command
+  // packed row-major copies of cmat for the MVM
+  int ld = 0;  // elements per packed row
+  aob::DevBuf<float> cm_f32;
+  aob::DevBuf<uint16_t> cm_bf16;
+  aob::DevBuf<uint8_t> cm_fp8;
+  aob::DevBuf<float> row_scale;
+  bool packed_valid[3] = {false, false, false};
+  std::vector<float> h_cmat;  // column-major host copy used for (re)packing
+  // FP64 eigen decomposition state (svdec_imat)
+  aob::DevBuf<double> U, eig;
+
+  struct Perturb {
+    aob::DevBuf<float> buf;
+    int n = 0;
+    int cpt = 0;
+    bool on = true;
+  };
+  std::map<std::string, Perturb> perturb;
+
+  aob_ls(int device, int nslope, int nactu, float delay);
+  float *com() { return ring.back().p; }
+  void set_delay(float d);
+  void ensure_packed(int p);
+  void comp_com(cudaStream_t s);
+  void comp_voltage(cudaStream_t s);
+  void clip(cudaStream_t s);
+  void svdec_imat();
+  void build_cmat(int nfilt);
+};
+
+namespace aob {
+int num_sms(int device);
+}

@@ -1,0 +1,170 @@
+// Centre-of-gravity centroiders on a sensor image (CoG, thresholded CoG,
+// weighted CoG) and the raw-image calibration.
+//
+// Reference kernels: centroids<> in libsutra/src.cu/sutra_centroider_cog.cu:28-81,
+// sutra_centroider_tcog.cu:27-81 (writes the thresholded pixels back into the
+// image, :63), sutra_centroider_wcog.cu:58-113; calib_krnl in
+// sutra_centroider.cu:89-96.  The reference launches one CTA of npix^2
+// threads per sub-aperture and reduces with three CUB BlockReduce passes; here
+// one warp handles a sub-aperture and reduces with shuffles.  When the
+// centroider is attached to a SH sensor the same sums are produced inside the
+// sensor kernel (sh_wfs.cu) and this kernel only runs if the image changed
+// after that or a parameter was modified.
+
+#include <algorithm>
+
+#include "aob_objects.hpp"
+
+namespace aob {
+
+struct CogArgs {
+  const float *img;
+  float *img_out;  // tCoG write-back target (may alias img); null = none
+  int size;        // image is size x size
+  const int32_t *validx;
+  const int32_t *validy;
+  int nvalid, npix, kind, order;
+  float scale, offset, thresh;
+  const float *ref;
+  const float *weights;
+  int wper;
+  float *slopes;
+  float *intens;
+};
+
+__global__ void cog_kernel(CogArgs A) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int npix2 = A.npix * A.npix;
+  const int64_t lim = (int64_t)A.size * A.size;
+  for (int k = warp; k < A.nvalid; k += nwarps) {
+    const int vx = A.validx[k], vy = A.validy[k];
+    float cs = 0.f, cx = 0.f, cy = 0.f;
+    for (int p = lane; p < npix2; p += 32) {
+      const int x = p % A.npix, y = p / A.npix;
+      const int64_t idim = (int64_t)(x + vx) + (int64_t)(y + vy) * A.size;
+      if (idim < 0 || idim >= lim) continue;
+      float d = A.img[idim];
+      if (A.kind == 1 || A.kind == 2) d = (d > A.thresh) ? d - A.thresh : 1.e-6f;
+      if (A.kind == 1 && A.img_out) A.img_out[idim] = d;
+      if (A.kind == 2) d *= A.weights[p + (A.wper ? k * npix2 : 0)];
+      cs += d;
+      cx = fmaf(d, (float)x, cx);
+      cy = fmaf(d, (float)y, cy);
+    }
+    cs = warp_sum(cs);
+    cx = warp_sum(cx);
+    cy = warp_sum(cy);
+    if (lane == 0) {
+      const int ix = A.order ? 2 * k : k;
+      const int iy = A.order ? 2 * k + 1 : k + A.nvalid;
+      A.slopes[ix] = (cx / (cs + 1.e-6f) - A.offset) * A.scale - A.ref[ix];
+      A.slopes[iy] = (cy / (cs + 1.e-6f) - A.offset) * A.scale - A.ref[iy];
+      A.intens[k] = cs;
+    }
+  }
+}
+
+// tCoG side effect for slopes that were produced inside the sensor kernel:
+// store the thresholded pixels of every valid sub-aperture into the image.
+__global__ void tcog_writeback_kernel(float *img, int size, const int32_t *validx, const int32_t *validy,
+                                      int nvalid, int npix, float thresh) {
+  const int npix2 = npix * npix;
+  const int64_t lim = (int64_t)size * size;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npix2 * nvalid; t += gridDim.x * blockDim.x) {
+    const int k = t / npix2, p = t - k * npix2;
+    const int64_t idim = (int64_t)(p % npix + validx[k]) + (int64_t)(p / npix + validy[k]) * size;
+    if (idim < 0 || idim >= lim) continue;
+    const float d = img[idim];
+    img[idim] = (d > thresh) ? d - thresh : 1.e-6f;
+  }
+}
+
+__global__ void calib_kernel(const float *raw, float *cal, const float *dark, const float *flat, int64_t n) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    cal[t] = (raw[t] - dark[t]) * flat[t];
+}
+
+}  // namespace aob
+
+using namespace aob;
+
+aob_centro::aob_centro(int device_, int type_, int nvalid_, float offset_, float scale_)
+    : device(device_), type(type_), nvalid(nvalid_), offset(offset_), scale(scale_) {
+  AOB_REQUIRE(nvalid > 0, "centroider: nvalid must be > 0");
+  AOB_REQUIRE(type >= 0 && type <= 3, "centroider: unknown type");
+  AOB_CUDA(cudaSetDevice(device));
+  ref.alloc(2 * (int64_t)nvalid);
+  intensities.alloc(nvalid);
+  fused_slopes.alloc(2 * (int64_t)nvalid);
+}
+
+bool aob_centro::fused_ready() const {
+  return wfs != nullptr && wfs->fused == this && fused_gen == wfs->image_gen &&
+         fused_params_gen == params_gen;
+}
+
+void aob_centro::calibrate(cudaStream_t s) {
+  AOB_REQUIRE(img_raw.p != nullptr, "calibrate_img: image not loaded");
+  AOB_CUDA(cudaSetDevice(device));
+  const int64_t n = (int64_t)img_m * img_n;
+  if (!img.p || img.n != n) img.alloc(n);
+  if (!dark.p || dark.n != n) dark.alloc(n);
+  if (!flat.p || flat.n != n) {
+    flat.alloc(n);
+    std::vector<float> one(n, 1.f);
+    flat.upload(one.data(), n);
+  }
+  calib_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, s>>>(img_raw.p, img.p, dark.p, flat.p, n);
+  AOB_LAUNCH_CHECK("calib_kernel");
+}
+
+void aob_centro::get_cog(float *dev_slopes, cudaStream_t s) {
+  AOB_REQUIRE(type <= 2, "get_cog: not a CoG-family centroider");
+  AOB_REQUIRE(npix > 0, "get_cog: npix not set");
+  AOB_REQUIRE(validx.p != nullptr && validx.n >= nvalid, "get_cog: valid positions not loaded");
+  if (type == 2) AOB_REQUIRE(weights.p != nullptr, "wcog: weights not loaded");
+  AOB_CUDA(cudaSetDevice(device));
+  if (fused_ready()) {
+    AOB_CUDA(cudaMemcpyAsync(dev_slopes, fused_slopes.p, sizeof(float) * 2 * nvalid,
+                             cudaMemcpyDeviceToDevice, s));
+    if (type == 1) {
+      const int n = npix * npix * nvalid;
+      tcog_writeback_kernel<<<std::min((n + 255) / 256, 4096), 256, 0, s>>>(
+          wfs->binimg.p, wfs->npix * wfs->nxsub, validx.p, validy.p, nvalid, npix, threshold);
+      AOB_LAUNCH_CHECK("tcog_writeback_kernel");
+      ++wfs->image_gen;  // a second get_cog thresholds again, as the reference does
+    }
+    return;
+  }
+  CogArgs A{};
+  if (wfs) {
+    A.img = wfs->binimg.p;
+    A.size = wfs->npix * wfs->nxsub;
+  } else {
+    AOB_REQUIRE(img.p != nullptr, "get_cog: no image (load_img + calibrate_img first)");
+    A.img = img.p;
+    A.size = img_m;
+  }
+  A.img_out = (type == 1) ? const_cast<float *>(A.img) : nullptr;
+  A.validx = validx.p;
+  A.validy = validy.p;
+  A.nvalid = nvalid;
+  A.npix = npix;
+  A.kind = type;
+  A.order = order;
+  A.scale = scale;
+  A.offset = offset;
+  A.thresh = threshold;
+  A.ref = ref.p;
+  A.weights = weights.p;
+  A.wper = weights_per_sub;
+  A.slopes = dev_slopes;
+  A.intens = intensities.p;
+  const int warps_per_block = 8;
+  const int grid = std::max(1, std::min((nvalid + warps_per_block - 1) / warps_per_block, num_sms(device) * 8));
+  cog_kernel<<<grid, warps_per_block * 32, 0, s>>>(A);
+  AOB_LAUNCH_CHECK("cog_kernel");
+  if (wfs && type == 1) ++wfs->image_gen;
+}

@@ -1,0 +1,425 @@
+// Least-squares controller: command-matrix MVM fused with the integrator,
+// command delay / latency interpolation / perturbation / clip, and the
+// float64 pseudo-inverse of the interaction matrix.
+//
+// Reference: SutraControllerLs::comp_com (libsutra/src.cpp/sutra_controller_ls.cpp:
+// 251-285) runs cuBLAS Sgemv on the column-major cmat, then mult_int_krnl
+// (libsutra/src.cu/sutra_utils.cu:631-639).  comp_voltage
+// (sutra_controller.cpp:245-263) is a chain of axpy / copy / clip launches.
+//
+// Layout in HBM: besides the caller-visible column-major float32 cmat, the MVM
+// reads a row-major (actuator-major) packed copy -- float32, bfloat16, or FP8
+// E4M3 with one float32 scale per actuator row -- with rows padded to 16 bytes.
+// Each CTA owns a contiguous block of actuator rows, stages the slope vector in
+// shared memory, and each warp streams whole rows with 16-byte loads (8 loads
+// in flight per lane), accumulates in float32 and applies the integrator in
+// the epilogue.  No cross-CTA reduction is needed, so the result is
+// deterministic.
+
+#include <cublas_v2.h>
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "aob_objects.hpp"
+
+namespace aob {
+
+struct MvmArgs {
+  const void *mat;        // packed rows
+  const float *rscale;    // per-row scale (FP8) or null
+  int ld;                 // elements per packed row
+  int nrow, ncol;
+  const float *s;         // slopes (device)
+  float *err;             // -cmat.s
+  float *com;             // integrator state
+  const float *mgain;     // modal gains
+  float gain;
+  int integrate;
+};
+
+// Dot product of one 16-byte packed chunk with its slopes.  The slopes are
+// staged in shared memory in a lane-swizzled order: the V/4 float4 groups of
+// chunk c = lane + 32*j live at float4 index (j*(V/4) + q)*32 + lane, so a warp
+// reads them with conflict-free 128-bit loads for every precision.
+template <typename T>
+struct Pack;
+template <>
+struct Pack<float> {
+  static constexpr int N = 4;
+  __device__ static float dot(const uint4 &q, const float4 *sv) {
+    const float *f = reinterpret_cast<const float *>(&q);
+    const float4 s = sv[0];
+    float a = f[0] * s.x;
+    a = fmaf(f[1], s.y, a);
+    a = fmaf(f[2], s.z, a);
+    return fmaf(f[3], s.w, a);
+  }
+};
+template <>
+struct Pack<__nv_bfloat16> {
+  static constexpr int N = 8;
+  __device__ static float dot(const uint4 &q, const float4 *sv) {
+    const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
+    float a = 0.f;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const float4 s = sv[32 * i];
+      const float2 f0 = __bfloat1622float2(h[2 * i]);
+      const float2 f1 = __bfloat1622float2(h[2 * i + 1]);
+      a = fmaf(f0.x, s.x, a);
+      a = fmaf(f0.y, s.y, a);
+      a = fmaf(f1.x, s.z, a);
+      a = fmaf(f1.y, s.w, a);
+    }
+    return a;
+  }
+};
+template <>
+struct Pack<__nv_fp8_e4m3> {
+  static constexpr int N = 16;
+  __device__ static float dot(const uint4 &q, const float4 *sv) {
+    const __nv_fp8x2_e4m3 *h = reinterpret_cast<const __nv_fp8x2_e4m3 *>(&q);
+    float a = 0.f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float4 s = sv[32 * i];
+      const float2 f0 = static_cast<float2>(h[2 * i]);
+      const float2 f1 = static_cast<float2>(h[2 * i + 1]);
+      a = fmaf(f0.x, s.x, a);
+      a = fmaf(f0.y, s.y, a);
+      a = fmaf(f1.x, s.z, a);
+      a = fmaf(f1.y, s.w, a);
+    }
+    return a;
+  }
+};
+
+constexpr int MVM_THREADS = 512;
+constexpr int MVM_UNROLL = 8;
+
+// shared floats needed for the swizzled slope vector (whole 32-chunk rounds)
+__host__ __device__ inline int mvm_smem_floats(int ld, int v) { return ((ld / v + 31) / 32) * 32 * v; }
+
+template <typename T>
+__global__ void __launch_bounds__(MVM_THREADS) ls_mvm_kernel(MvmArgs A) {
+  extern __shared__ __align__(16) float s_sh[];
+  constexpr int V = Pack<T>::N;
+  constexpr int Q = V / 4;
+  const int nchunk = A.ld / V;  // 16-byte chunks per row
+  const int nsh = mvm_smem_floats(A.ld, V);
+  for (int i = threadIdx.x; i < nsh; i += blockDim.x) {
+    // inverse of the swizzle: float i sits in group g = i/4, element e = i%4
+    const int g = i >> 2, e = i & 3;
+    const int l = g & 31, jq = g >> 5;
+    const int j = jq / Q, q = jq - j * Q;
+    const int src = (l + 32 * j) * V + 4 * q + e;
+    s_sh[i] = (src < A.ncol) ? A.s[src] : 0.f;
+  }
+  __syncthreads();
+  const float4 *sv = reinterpret_cast<const float4 *>(s_sh);
+  const int r0 = (int)(((int64_t)blockIdx.x * A.nrow) / gridDim.x);
+  const int r1 = (int)(((int64_t)(blockIdx.x + 1) * A.nrow) / gridDim.x);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nw = blockDim.x >> 5;
+  const float4 *svl = sv + lane;
+  for (int r = r0 + warp; r < r1; r += nw) {
+    const uint4 *row = reinterpret_cast<const uint4 *>(static_cast<const T *>(A.mat) + (size_t)r * A.ld) + lane;
+    float acc[MVM_UNROLL];
+#pragma unroll
+    for (int u = 0; u < MVM_UNROLL; ++u) acc[u] = 0.f;
+    int j = 0;
+    for (; 32 * (j + MVM_UNROLL - 1) + lane < nchunk; j += MVM_UNROLL) {
+      uint4 q[MVM_UNROLL];
+#pragma unroll
+      for (int u = 0; u < MVM_UNROLL; ++u) q[u] = __ldcs(row + 32 * (j + u));
+#pragma unroll
+      for (int u = 0; u < MVM_UNROLL; ++u) acc[u] += Pack<T>::dot(q[u], svl + 32 * Q * (j + u));
+    }
+    for (; 32 * j + lane < nchunk; ++j) acc[0] += Pack<T>::dot(__ldcs(row + 32 * j), svl + 32 * Q * j);
+    float tot = 0.f;
+#pragma unroll
+    for (int u = 0; u < MVM_UNROLL; ++u) tot += acc[u];
+    tot = warp_sum(tot);
+    if (lane == 0) {
+      if (A.rscale) tot *= A.rscale[r];
+      const float e = -tot;
+      A.err[r] = e;
+      if (A.integrate) A.com[r] = A.gain * (e * A.mgain[r]) + A.com[r];
+    }
+  }
+}
+
+struct VoltArgs {
+  const float *com;
+  float *oldest;       // ring[0]: read for latency, then overwritten with com
+  const float *second; // ring[1]
+  float a, b;
+  int delayed;
+  const float *pert[8];
+  int pn[8];
+  int pcpt[8];
+  int npert;
+  float vmin, vmax;
+  int do_clip;
+  float *out;
+  int n;
+};
+
+__global__ void voltage_kernel(VoltArgs A) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+    float v;
+    if (A.delayed) {
+      v = A.a * A.oldest[i] + A.b * A.second[i];
+      A.oldest[i] = A.com[i];
+    } else {
+      v = A.com[i];
+    }
+    for (int j = 0; j < A.npert; ++j) v += A.pert[j][A.pcpt[j] + (int64_t)i * A.pn[j]];
+    if (A.do_clip) v = fminf(fmaxf(v, A.vmin), A.vmax);
+    A.out[i] = v;
+  }
+}
+
+__global__ void clip_kernel(float *x, int n, float lo, float hi) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = fminf(fmaxf(x[i], lo), hi);
+}
+
+__global__ void d2f_kernel(const double *a, float *b, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+__global__ void f2d_kernel(const float *a, double *b, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (double)a[i];
+}
+__global__ void scale_cols_kernel(const double *U, const double *w, double *out, int n) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < (int64_t)n * n; t += (int64_t)gridDim.x * blockDim.x)
+    out[t] = U[t] * w[t / n];
+}
+
+}  // namespace aob
+
+using namespace aob;
+
+aob_ls::aob_ls(int device_, int nslope_, int nactu_, float delay_)
+    : device(device_), nslope(nslope_), nactu(nactu_) {
+  AOB_REQUIRE(nslope > 0 && nactu > 0, "ls: nslope and nactu must be > 0");
+  AOB_CUDA(cudaSetDevice(device));
+  set_delay(delay_);
+  centroids.alloc(nslope);
+  err.alloc(nactu);
+  com_clipped.alloc(nactu);
+  gains.alloc(nactu);
+  std::vector<float> one(nactu, 1.f);
+  gains.upload(one.data(), nactu);
+  cmat.alloc((int64_t)nactu * nslope);
+  h_cmat.assign((size_t)nactu * nslope, 0.f);
+  const int nring = delay > 0 ? (int)delay + 2 : 1;
+  for (int i = 0; i < nring; ++i) ring.emplace_back(nactu);
+}
+
+void aob_ls::set_delay(float d) {
+  delay = d;
+  const int fl = (int)d;
+  a = d - (float)fl;
+  b = 1.f - a;
+}
+
+void aob_ls::ensure_packed(int p) {
+  if (packed_valid[p]) return;
+  AOB_CUDA(cudaSetDevice(device));
+  if (p == AOB_PREC_F32) {
+    ld = (nslope + 3) / 4 * 4;
+    std::vector<float> rows((size_t)nactu * ld, 0.f);
+    for (int s = 0; s < nslope; ++s)
+      for (int r = 0; r < nactu; ++r) rows[(size_t)r * ld + s] = h_cmat[(size_t)s * nactu + r];
+    cm_f32.alloc((int64_t)nactu * ld);
+    cm_f32.upload(rows.data(), (int64_t)nactu * ld);
+  } else if (p == AOB_PREC_BF16) {
+    const int l = (nslope + 7) / 8 * 8;
+    std::vector<__nv_bfloat16> rows((size_t)nactu * l, __float2bfloat16(0.f));
+    for (int s = 0; s < nslope; ++s)
+      for (int r = 0; r < nactu; ++r) rows[(size_t)r * l + s] = __float2bfloat16(h_cmat[(size_t)s * nactu + r]);
+    cm_bf16.alloc((int64_t)nactu * l);
+    cm_bf16.upload(reinterpret_cast<const uint16_t *>(rows.data()), (int64_t)nactu * l);
+  } else {
+    const int l = (nslope + 15) / 16 * 16;
+    std::vector<__nv_fp8_e4m3> rows((size_t)nactu * l, __nv_fp8_e4m3(0.f));
+    std::vector<float> sc(nactu, 1.f);
+    for (int r = 0; r < nactu; ++r) {
+      float m = 0.f;
+      for (int s = 0; s < nslope; ++s) m = std::max(m, std::fabs(h_cmat[(size_t)s * nactu + r]));
+      sc[r] = m > 0.f ? m / 448.f : 1.f;  // 448 = largest finite E4M3 value
+      const float inv = 1.f / sc[r];
+      for (int s = 0; s < nslope; ++s) rows[(size_t)r * l + s] = __nv_fp8_e4m3(h_cmat[(size_t)s * nactu + r] * inv);
+    }
+    cm_fp8.alloc((int64_t)nactu * l);
+    cm_fp8.upload(reinterpret_cast<const uint8_t *>(rows.data()), (int64_t)nactu * l);
+    row_scale.alloc(nactu);
+    row_scale.upload(sc.data(), nactu);
+  }
+  packed_valid[p] = true;
+}
+
+void aob_ls::comp_com(cudaStream_t s) {
+  if (open_loop) return;
+  AOB_CUDA(cudaSetDevice(device));
+  ensure_packed(prec);
+  MvmArgs A{};
+  A.nrow = nactu;
+  A.ncol = nslope;
+  A.s = centroids.p;
+  A.err = err.p;
+  A.com = com();
+  A.mgain = gains.p;
+  A.gain = gain;
+  A.integrate = 1;
+  const int grid = nblocks > 0 ? std::min(nblocks, nactu) : std::min(nactu, num_sms(device));
+  if (prec == AOB_PREC_F32) {
+    A.mat = cm_f32.p;
+    A.ld = (nslope + 3) / 4 * 4;
+    const size_t sm = sizeof(float) * mvm_smem_floats(A.ld, 4);
+    AOB_CUDA(cudaFuncSetAttribute(ls_mvm_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    ls_mvm_kernel<float><<<grid, MVM_THREADS, sm, s>>>(A);
+  } else if (prec == AOB_PREC_BF16) {
+    A.mat = cm_bf16.p;
+    A.ld = (nslope + 7) / 8 * 8;
+    const size_t sm = sizeof(float) * mvm_smem_floats(A.ld, 8);
+    AOB_CUDA(cudaFuncSetAttribute(ls_mvm_kernel<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    ls_mvm_kernel<__nv_bfloat16><<<grid, MVM_THREADS, sm, s>>>(A);
+  } else {
+    A.mat = cm_fp8.p;
+    A.rscale = row_scale.p;
+    A.ld = (nslope + 15) / 16 * 16;
+    const size_t sm = sizeof(float) * mvm_smem_floats(A.ld, 16);
+    AOB_CUDA(cudaFuncSetAttribute(ls_mvm_kernel<__nv_fp8_e4m3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    ls_mvm_kernel<__nv_fp8_e4m3><<<grid, MVM_THREADS, sm, s>>>(A);
+  }
+  AOB_LAUNCH_CHECK("ls_mvm_kernel");
+}
+
+void aob_ls::comp_voltage(cudaStream_t s) {
+  AOB_CUDA(cudaSetDevice(device));
+  VoltArgs A{};
+  A.com = com();
+  A.delayed = delay > 0 ? 1 : 0;
+  if (A.delayed) {
+    A.oldest = ring[0].p;
+    A.second = ring[1].p;
+  }
+  A.a = a;
+  A.b = b;
+  for (auto &kv : perturb) {
+    Perturb &p = kv.second;
+    if (!p.on) continue;
+    AOB_REQUIRE(A.npert < 8, "comp_voltage: at most 8 enabled perturbation buffers");
+    A.pert[A.npert] = p.buf.p;
+    A.pn[A.npert] = p.n;
+    A.pcpt[A.npert] = p.cpt;
+    ++A.npert;
+    p.cpt = (p.cpt < p.n - 1) ? p.cpt + 1 : 0;
+  }
+  A.vmin = volt_min;
+  A.vmax = volt_max;
+  A.do_clip = volt_min < volt_max ? 1 : 0;
+  A.out = com_clipped.p;
+  A.n = nactu;
+  voltage_kernel<<<std::max(1, std::min((nactu + 255) / 256, 1024)), 256, 0, s>>>(A);
+  AOB_LAUNCH_CHECK("voltage_kernel");
+  if (A.delayed) {
+    // the oldest buffer now holds a copy of the current command and becomes it
+    aob::DevBuf<float> t = std::move(ring.front());
+    ring.pop_front();
+    ring.push_back(std::move(t));
+  }
+}
+
+void aob_ls::clip(cudaStream_t s) {
+  if (!(volt_min < volt_max)) return;
+  AOB_CUDA(cudaSetDevice(device));
+  clip_kernel<<<std::max(1, std::min((nactu + 255) / 256, 1024)), 256, 0, s>>>(com_clipped.p, nactu, volt_min, volt_max);
+  AOB_LAUNCH_CHECK("clip_kernel");
+}
+
+namespace {
+void cublas_check(cublasStatus_t st, const char *w) {
+  if (st != CUBLAS_STATUS_SUCCESS) throw aob::Error(std::string(w) + ": cublas status " + std::to_string((int)st));
+}
+void cusolver_check(cusolverStatus_t st, const char *w) {
+  if (st != CUSOLVER_STATUS_SUCCESS) throw aob::Error(std::string(w) + ": cusolver status " + std::to_string((int)st));
+}
+}  // namespace
+
+// svdec_imat: U = imat^T imat (float64), eigen-decomposed in place with
+// cuSOLVER Dsyevd; eigenvalues ascending (sutra_controller_ls.cpp:116-150).
+void aob_ls::svdec_imat() {
+  AOB_REQUIRE(imat.p != nullptr, "svdec_imat: imat not set");
+  AOB_CUDA(cudaSetDevice(device));
+  DevBuf<double> D((int64_t)nslope * nactu);
+  f2d_kernel<<<1024, 256>>>(imat.p, D.p, D.n);
+  AOB_LAUNCH_CHECK("f2d_kernel");
+  U.alloc((int64_t)nactu * nactu);
+  eig.alloc(nactu);
+  cublasHandle_t hb;
+  cublas_check(cublasCreate(&hb), "cublasCreate");
+  const double one = 1.0, zero = 0.0;
+  cublasStatus_t st = cublasDgemm(hb, CUBLAS_OP_T, CUBLAS_OP_N, nactu, nactu, nslope, &one, D.p, nslope, D.p,
+                                  nslope, &zero, U.p, nactu);
+  cublasDestroy(hb);
+  cublas_check(st, "cublasDgemm");
+  cusolverDnHandle_t hs;
+  cusolver_check(cusolverDnCreate(&hs), "cusolverDnCreate");
+  int lwork = 0;
+  cusolverStatus_t ss = cusolverDnDsyevd_bufferSize(hs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nactu,
+                                                    U.p, nactu, eig.p, &lwork);
+  if (ss != CUSOLVER_STATUS_SUCCESS) { cusolverDnDestroy(hs); cusolver_check(ss, "Dsyevd_bufferSize"); }
+  DevBuf<double> work(std::max(lwork, 1));
+  DevBuf<int> info(1);
+  ss = cusolverDnDsyevd(hs, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nactu, U.p, nactu, eig.p, work.p,
+                        lwork, info.p);
+  cusolverDnDestroy(hs);
+  cusolver_check(ss, "cusolverDnDsyevd");
+  int h_info = 0;
+  AOB_CUDA(cudaMemcpy(&h_info, info.p, sizeof(int), cudaMemcpyDeviceToHost));
+  AOB_REQUIRE(h_info == 0, "svdec_imat: eigen decomposition did not converge");
+  eigenvals_f.alloc(nactu);
+  d2f_kernel<<<64, 256>>>(eig.p, eigenvals_f.p, nactu);
+  AOB_LAUNCH_CHECK("d2f_kernel");
+  AOB_CUDA(cudaDeviceSynchronize());
+}
+
+// build_cmat: cmat = U diag(1/ev, first nfilt modes and |ev| <= 1e-9 dropped) U^T imat^T
+// (sutra_controller_ls.cpp:174-217), in float64, stored as float32.
+void aob_ls::build_cmat(int nfilt) {
+  AOB_REQUIRE(U.p != nullptr, "build_cmat: call svdec_imat first");
+  AOB_CUDA(cudaSetDevice(device));
+  std::vector<double> ev(nactu), inv(nactu, 0.0);
+  AOB_CUDA(cudaMemcpy(ev.data(), eig.p, sizeof(double) * nactu, cudaMemcpyDeviceToHost));
+  for (int i = std::max(nfilt, 0); i < nactu; ++i) inv[i] = std::fabs(ev[i]) > 1.e-9 ? 1.0 / ev[i] : 0.0;
+  DevBuf<double> w(nactu), T1((int64_t)nactu * nactu), T2((int64_t)nactu * nactu), D((int64_t)nslope * nactu),
+      C((int64_t)nactu * nslope);
+  w.upload(inv.data(), nactu);
+  scale_cols_kernel<<<1024, 256>>>(U.p, w.p, T1.p, nactu);
+  f2d_kernel<<<1024, 256>>>(imat.p, D.p, D.n);
+  AOB_LAUNCH_CHECK("build_cmat prep");
+  cublasHandle_t hb;
+  cublas_check(cublasCreate(&hb), "cublasCreate");
+  const double one = 1.0, zero = 0.0;
+  cublasStatus_t st = cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, nactu, nactu, nactu, &one, T1.p, nactu, U.p, nactu,
+                                  &zero, T2.p, nactu);
+  if (st == CUBLAS_STATUS_SUCCESS)
+    st = cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, nactu, nslope, nactu, &one, T2.p, nactu, D.p, nslope, &zero, C.p,
+                     nactu);
+  cublasDestroy(hb);
+  cublas_check(st, "cublasDgemm");
+  d2f_kernel<<<1024, 256>>>(C.p, cmat.p, C.n);
+  AOB_LAUNCH_CHECK("d2f_kernel");
+  AOB_CUDA(cudaMemcpy(h_cmat.data(), cmat.p, sizeof(float) * h_cmat.size(), cudaMemcpyDeviceToHost));
+  packed_valid[0] = packed_valid[1] = packed_valid[2] = false;
+}

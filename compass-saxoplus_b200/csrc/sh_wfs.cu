@@ -1,0 +1,392 @@
+// Shack-Hartmann image formation: one fused kernel per sensor image.
+//
+// The reference runs eight launches and two memsets per image
+// (SutraWfsSH::comp_generic, libsutra/src.cpp/sutra_wfs_sh.cpp:337-589):
+// fill the padded Nfft x Nfft field cube (camplipup_krnl, sutra_wfs.cu:27-53),
+// batched cuFFT, |E|^2 (abs2c_krnl, sutra_utils.cu:144-168), binning through
+// binmap (fillbincube_krnl, sutra_wfs.cu:369-414), per-sub-aperture sum
+// (reduce2, sutra_wfs.cu:556-590), normalisation (subapnorm_krnl,
+// sutra_utils.cu:170-193), cuRAND Poisson + Gaussian noise, then the image
+// scatter (bimg_krnl, sutra_wfs.cu:183-229).  The padded cube (2.5 MB at 40x40)
+// is written and re-read several times.
+//
+// Here one warp owns one sub-aperture from phase to pixels:
+//  * the pdiam x pdiam field is built in shared memory (the Nfft^2 - pdiam^2
+//    zero padding is never materialised);
+//  * the 2-D DFT is evaluated only at the spatial frequencies that binmap
+//    reads (an nu x nv subset of the Nfft x Nfft grid, found on the host from
+//    binmap), as two separable passes of exact twiddle-table products -- the
+//    same transform as the reference's forward cuFFT, pruned on both input
+//    and output;
+//  * binning, normalisation, Philox-keyed Poisson/readout noise, the bincube
+//    and image writes, and (optionally) the CoG/tCoG/wCoG centroid of the
+//    sub-aperture happen in registers before the warp moves on.
+// HBM traffic per image is the phase and pupil samples read once, the cube,
+// image and slopes written once.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "aob_objects.hpp"
+
+namespace aob {
+
+constexpr int SH_WARPS = 4;      // sub-apertures per CTA
+constexpr int SH_MAX_PPL = 8;    // binned pixels per lane -> npix^2 <= 256
+
+struct ShKernelArgs {
+  const float *phase;
+  const float *pupil;
+  int npup;
+  const int32_t *puppixx;
+  const int32_t *puppixy;
+  const float *offsets;
+  float scale;
+  int pdiam, nvalid, npix, nrebin2;
+  int nu, nv;
+  const int32_t *ulist;
+  const int32_t *vlist;
+  const int32_t *cbin;  // [nrebin2, npix^2] indexes into the nu x nv intensity tile
+  const float *flux;
+  float nphot;
+  float *bincube;
+  float *binimg;
+  int img_size;
+  const int32_t *validsubsx;
+  const int32_t *validsubsy;
+  float *intensities;
+  int noise_mode;  // 0 none, 1 photon, 2 photon + readout
+  float noise;
+  uint32_t frame, k0, k1;
+  // fused centroider (kind < 0: none)
+  int ckind;
+  float c_scale, c_offset, c_thresh;
+  const float *c_ref;
+  const float *c_weights;
+  int c_wper;
+  int c_order;
+  float *c_slopes;
+  float *c_intens;
+};
+
+template <int NFFT>
+__global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2 *tw = reinterpret_cast<float2 *>(smem);
+  int32_t *ul = reinterpret_cast<int32_t *>(tw + NFFT);
+  int32_t *vl = ul + NFFT;
+  int32_t *cb = vl + NFFT;
+  const int ncb = P.nrebin2 * P.npix * P.npix;
+  const int pd2 = P.pdiam * P.pdiam;
+  const size_t hdr = ((sizeof(float2) * NFFT + sizeof(int32_t) * (2 * NFFT + ncb)) + 15) & ~size_t(15);
+  const size_t per_warp = ((size_t)(pd2 + P.nu * P.pdiam) * sizeof(float2) + (size_t)P.nu * P.nv * sizeof(float) + 15) & ~size_t(15);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < NFFT; i += blockDim.x) {
+    double s, c;
+    sincospi(2.0 * (double)i / (double)NFFT, &s, &c);
+    tw[i] = make_float2((float)c, (float)-s);  // exp(-2 pi i m / N): forward transform
+  }
+  for (int i = threadIdx.x; i < P.nu; i += blockDim.x) ul[i] = P.ulist[i];
+  for (int i = threadIdx.x; i < P.nv; i += blockDim.x) vl[i] = P.vlist[i];
+  for (int i = threadIdx.x; i < ncb; i += blockDim.x) cb[i] = P.cbin[i];
+  __syncthreads();
+
+  float2 *E = reinterpret_cast<float2 *>(smem + hdr + per_warp * warp);
+  float2 *Gt = E + pd2;
+  float *I = reinterpret_cast<float *>(Gt + P.nu * P.pdiam);
+  const int npix2 = P.npix * P.npix;
+
+  for (int k = blockIdx.x * SH_WARPS + warp; k < P.nvalid; k += gridDim.x * SH_WARPS) {
+    // 1. complex field of the sub-aperture: pupil * exp(i (phase*2pi/lambda - offset))
+    const int px = P.puppixx[k], py = P.puppixy[k];
+    for (int i = lane; i < pd2; i += 32) {
+      const int x = i % P.pdiam, y = i / P.pdiam;
+      const int id = (x + px) + (y + py) * P.npup;
+      const float ph = P.phase[id] * P.scale - P.offsets[i];
+      float s, c;
+      sincosf(ph, &s, &c);
+      const float a = P.pupil[id];
+      E[i] = make_float2(c * a, s * a);
+    }
+    __syncwarp();
+    // 2. DFT along x at the needed kx: G[a, y] = sum_x E[x, y] W^(u_a x)
+    for (int i = lane; i < P.nu * P.pdiam; i += 32) {
+      const int a = i % P.nu, y = i / P.nu;
+      const int ua = ul[a];
+      const float2 *e = E + y * P.pdiam;
+      float re = 0.f, im = 0.f;
+      int m = 0;
+      for (int x = 0; x < P.pdiam; ++x) {
+        const float2 w = tw[m], v = e[x];
+        re = fmaf(v.x, w.x, fmaf(-v.y, w.y, re));
+        im = fmaf(v.x, w.y, fmaf(v.y, w.x, im));
+        m = (m + ua) & (NFFT - 1);
+      }
+      Gt[i] = make_float2(re, im);
+    }
+    __syncwarp();
+    // 3. DFT along y at the needed ky and |.|^2: I[a, b]
+    for (int i = lane; i < P.nu * P.nv; i += 32) {
+      const int a = i % P.nu, b = i / P.nu;
+      const int vb = vl[b];
+      float re = 0.f, im = 0.f;
+      int m = 0;
+      for (int y = 0; y < P.pdiam; ++y) {
+        const float2 w = tw[m], v = Gt[a + y * P.nu];
+        re = fmaf(v.x, w.x, fmaf(-v.y, w.y, re));
+        im = fmaf(v.x, w.y, fmaf(v.y, w.x, im));
+        m = (m + vb) & (NFFT - 1);
+      }
+      I[i] = fmaf(re, re, im * im);
+    }
+    __syncwarp();
+    // 4. binning and per-sub-aperture flux
+    float bv[SH_MAX_PPL];
+    float part = 0.f;
+#pragma unroll
+    for (int j = 0; j < SH_MAX_PPL; ++j) {
+      const int p = lane + 32 * j;
+      float v = 0.f;
+      if (p < npix2) {
+        const int32_t *c = cb + p * P.nrebin2;
+        for (int r = 0; r < P.nrebin2; ++r) v += I[c[r]];
+      }
+      bv[j] = v;
+      part += v;
+    }
+    const float tot = warp_sum(part);
+    if (lane == 0) P.intensities[k] = tot;
+    const float fk = P.flux[k];
+    // 5. normalise, noise, write cube + image, centroid partial sums
+    const int vx = P.validsubsx[k], vy = P.validsubsy[k];
+    float cs = 0.f, cx = 0.f, cy = 0.f;
+#pragma unroll
+    for (int j = 0; j < SH_MAX_PPL; ++j) {
+      const int p = lane + 32 * j;
+      if (p < npix2) {
+        float v = bv[j];
+        if (tot != 0.f) v = v * fk / tot * P.nphot;
+        const uint32_t pix = (uint32_t)(p + k * npix2);
+        if (P.noise_mode >= 1) v = (float)poisson_sample((double)v, pix, P.frame, P.k0, P.k1);
+        if (P.noise_mode >= 2) v = v + P.noise * (float)gauss_sample(pix, P.frame, P.k0, P.k1);
+        P.bincube[pix] = v;
+        const int x = p % P.npix, y = p / P.npix;
+        const int idim = (x + vx) + (y + vy) * P.img_size;
+        float d = v;
+        if (P.ckind == 1 || P.ckind == 2) d = (v > P.c_thresh) ? v - P.c_thresh : 1.e-6f;
+        // raw pixels here; the tCoG write-back of thresholded pixels happens when
+        // the slopes are collected (aob_centro::get_cog), as in the reference
+        P.binimg[idim] = v;
+        if (P.ckind == 2) d *= P.c_weights[p + (P.c_wper ? k * npix2 : 0)];
+        cs += d;
+        cx = fmaf(d, (float)x, cx);
+        cy = fmaf(d, (float)y, cy);
+      }
+    }
+    if (P.ckind >= 0) {
+      cs = warp_sum(cs);
+      cx = warp_sum(cx);
+      cy = warp_sum(cy);
+      if (lane == 0) {
+        const int ix = P.c_order ? 2 * k : k;
+        const int iy = P.c_order ? 2 * k + 1 : k + P.nvalid;
+        P.c_slopes[ix] = (cx / (cs + 1.e-6f) - P.c_offset) * P.c_scale - P.c_ref[ix];
+        P.c_slopes[iy] = (cy / (cs + 1.e-6f) - P.c_offset) * P.c_scale - P.c_ref[iy];
+        P.c_intens[k] = cs;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+__global__ void sh_fill_image_kernel(float *img, const float *cube, const int32_t *vx,
+                                     const int32_t *vy, int npix, int nvalid, int size) {
+  const int npix2 = npix * npix;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npix2 * nvalid; t += gridDim.x * blockDim.x) {
+    const int k = t / npix2, p = t - k * npix2;
+    img[(p % npix + vx[k]) + (p / npix + vy[k]) * size] = cube[t];
+  }
+}
+
+}  // namespace aob
+
+using namespace aob;
+
+aob_sh::aob_sh(int device_, int nxsub_, int nvalid_, int npix_, int nphase_, int nrebin_, int nfft_,
+               int ntot_, int npup_, float pdiam_, float nphot_, float nphot4imat_)
+    : device(device_), nxsub(nxsub_), nvalid(nvalid_), npix(npix_), nphase(nphase_), nrebin(nrebin_),
+      nfft(nfft_), ntot(ntot_), npup(npup_), pdiam(pdiam_), nphot(nphot_), nphot4imat(nphot4imat_) {
+  AOB_REQUIRE(nvalid > 0 && npix > 0 && nphase > 0 && nrebin > 0 && npup > 0, "sh: sizes must be > 0");
+  AOB_REQUIRE(nfft == 16 || nfft == 32 || nfft == 64, "sh: nfft must be 16, 32 or 64");
+  AOB_REQUIRE(ntot == nfft, "sh: extended field of view (ntot != nfft) is not supported");
+  AOB_REQUIRE(nphase <= nfft && nphase <= 32, "sh: nphase must be <= min(nfft, 32)");
+  AOB_REQUIRE(npix * npix <= 32 * SH_MAX_PPL, "sh: npix^2 must be <= 256");
+  AOB_REQUIRE((int64_t)nxsub * npix < (1 << 15), "sh: image too large");
+  AOB_CUDA(cudaSetDevice(device));
+  phase.alloc((int64_t)npup * npup);
+  pupil.alloc((int64_t)npup * npup);
+  istart.alloc(nvalid);
+  jstart.alloc(nvalid);
+  validsubsx.alloc(nvalid);
+  validsubsy.alloc(nvalid);
+  binmap.alloc((int64_t)nrebin * nrebin * npix * npix);
+  offsets.alloc((int64_t)nphase * nphase);
+  fluxPerSub.alloc(nvalid);
+  bincube.alloc((int64_t)npix * npix * nvalid);
+  binimg.alloc((int64_t)npix * nxsub * npix * nxsub);
+  intensities.alloc(nvalid);
+  slopes.alloc(2 * (int64_t)nvalid);
+}
+
+void aob_sh::load_arrays(const int32_t *h_binmap, const float *h_offsets, const float *h_flux,
+                         const int32_t *h_vx, const int32_t *h_vy, const int32_t *h_istart,
+                         const int32_t *h_jstart) {
+  AOB_REQUIRE(h_binmap && h_offsets && h_flux && h_vx && h_vy && h_istart && h_jstart,
+              "sh.load_arrays: a required array is NULL");
+  AOB_CUDA(cudaSetDevice(device));
+  const int nr2 = nrebin * nrebin, np2 = npix * npix;
+  const int n2 = nfft * nfft;
+  const int img = npix * nxsub;
+  for (int i = 0; i < nvalid; ++i) {
+    AOB_REQUIRE(h_istart[i] >= 0 && h_jstart[i] >= 0 && h_istart[i] + nphase <= npup &&
+                    h_jstart[i] + nphase <= npup,
+                "sh.load_arrays: sub-aperture phase window outside the screen");
+    AOB_REQUIRE(h_vx[i] >= 0 && h_vy[i] >= 0 && h_vx[i] + npix <= img && h_vy[i] + npix <= img,
+                "sh.load_arrays: sub-aperture outside the sensor image");
+  }
+  // frequencies that binmap reads: kx = m % nfft, ky = m / nfft
+  std::vector<int> usex(nfft, -1), usey(nfft, -1);
+  for (int i = 0; i < nr2 * np2; ++i) {
+    const int m = h_binmap[i];
+    AOB_REQUIRE(m >= 0 && m < n2, "sh.load_arrays: binmap entry out of range");
+    usex[m % nfft] = 1;
+    usey[m / nfft] = 1;
+  }
+  std::vector<int32_t> U, V;
+  for (int i = 0; i < nfft; ++i) {
+    if (usex[i] > 0) { usex[i] = (int)U.size(); U.push_back(i); }
+    if (usey[i] > 0) { usey[i] = (int)V.size(); V.push_back(i); }
+  }
+  nu = (int)U.size();
+  nv = (int)V.size();
+  std::vector<int32_t> C(nr2 * np2);
+  for (int i = 0; i < nr2 * np2; ++i) {
+    const int m = h_binmap[i];
+    C[i] = usex[m % nfft] + usey[m / nfft] * nu;
+  }
+  ulist.alloc(nu);
+  vlist.alloc(nv);
+  cbin.alloc((int64_t)nr2 * np2);
+  ulist.upload(U.data(), nu);
+  vlist.upload(V.data(), nv);
+  cbin.upload(C.data(), (int64_t)nr2 * np2);
+  binmap.upload(h_binmap, (int64_t)nr2 * np2);
+  offsets.upload(h_offsets, (int64_t)nphase * nphase);
+  fluxPerSub.upload(h_flux, nvalid);
+  validsubsx.upload(h_vx, nvalid);
+  validsubsy.upload(h_vy, nvalid);
+  istart.upload(h_istart, nvalid);
+  jstart.upload(h_jstart, nvalid);
+  AOB_REQUIRE(smem_bytes() <= 200 * 1024, "sh: shared-memory footprint too large for this geometry");
+  loaded = true;
+}
+
+size_t aob_sh::smem_bytes() const {
+  const int ncb = nrebin * nrebin * npix * npix;
+  const size_t hdr = ((sizeof(float2) * nfft + sizeof(int32_t) * (2 * nfft + ncb)) + 15) & ~size_t(15);
+  const size_t per_warp =
+      ((size_t)(nphase * nphase + nu * nphase) * sizeof(float2) + (size_t)nu * nv * sizeof(float) + 15) &
+      ~size_t(15);
+  return hdr + SH_WARPS * per_warp;
+}
+
+void aob_sh::comp_image(bool with_noise, cudaStream_t s) {
+  AOB_REQUIRE(loaded, "sh.comp_image: load_arrays has not been called");
+  AOB_CUDA(cudaSetDevice(device));
+  ShKernelArgs P{};
+  P.phase = phase.p;
+  P.pupil = pupil.p;
+  P.npup = npup;
+  P.puppixx = istart.p;
+  P.puppixy = jstart.p;
+  P.offsets = offsets.p;
+  P.scale = (float)(2.0 * M_PI / (double)lambda_um);
+  P.pdiam = nphase;
+  P.nvalid = nvalid;
+  P.npix = npix;
+  P.nrebin2 = nrebin * nrebin;
+  P.nu = nu;
+  P.nv = nv;
+  P.ulist = ulist.p;
+  P.vlist = vlist.p;
+  P.cbin = cbin.p;
+  P.flux = fluxPerSub.p;
+  P.nphot = nphot;
+  P.bincube = bincube.p;
+  P.binimg = binimg.p;
+  P.img_size = npix * nxsub;
+  P.validsubsx = validsubsx.p;
+  P.validsubsy = validsubsy.p;
+  P.intensities = intensities.p;
+  const float nz = with_noise ? noise : -1.f;
+  P.noise_mode = nz > 0 ? 2 : (nz > -1 ? 1 : 0);
+  P.noise = nz;
+  P.frame = (uint32_t)frame;
+  P.k0 = (uint32_t)((uint64_t)seed & 0xffffffffu);
+  P.k1 = (uint32_t)((uint64_t)seed >> 32);
+  P.ckind = -1;
+  aob_centro *c = fused;
+  if (c && c->npix == npix && c->nvalid == nvalid && c->type <= 2 && c->validx.n == nvalid) {
+    P.ckind = c->type;
+    P.c_scale = c->scale;
+    P.c_offset = c->offset;
+    P.c_thresh = c->threshold;
+    P.c_ref = c->ref.p;
+    P.c_weights = c->weights.p;
+    P.c_wper = c->weights_per_sub;
+    P.c_order = c->order;
+    P.c_slopes = c->fused_slopes.p;
+    P.c_intens = c->intensities.p;
+    if (c->type == 2) AOB_REQUIRE(c->weights.p != nullptr, "wcog: weights not loaded");
+  } else {
+    c = nullptr;
+  }
+  const int nsm = num_sms(device);
+  int grid = (nvalid + SH_WARPS - 1) / SH_WARPS;
+  grid = std::max(1, std::min(grid, nsm * 16));
+  const size_t sm = smem_bytes();
+  switch (nfft) {
+    case 16:
+      AOB_CUDA(cudaFuncSetAttribute(sh_image_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      sh_image_kernel<16><<<grid, SH_WARPS * 32, sm, s>>>(P);
+      break;
+    case 32:
+      AOB_CUDA(cudaFuncSetAttribute(sh_image_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      sh_image_kernel<32><<<grid, SH_WARPS * 32, sm, s>>>(P);
+      break;
+    default:
+      AOB_CUDA(cudaFuncSetAttribute(sh_image_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      sh_image_kernel<64><<<grid, SH_WARPS * 32, sm, s>>>(P);
+      break;
+  }
+  AOB_LAUNCH_CHECK("sh_image_kernel");
+  if (P.noise_mode) ++frame;
+  ++image_gen;
+  if (c) {
+    c->fused_gen = image_gen;
+    c->fused_params_gen = c->params_gen;
+  }
+}
+
+void aob_sh::fill_binimage(cudaStream_t s) {
+  AOB_CUDA(cudaSetDevice(device));
+  const int n = npix * npix * nvalid;
+  sh_fill_image_kernel<<<std::min((n + 255) / 256, 4096), 256, 0, s>>>(
+      binimg.p, bincube.p, validsubsx.p, validsubsy.p, npix, nvalid, npix * nxsub);
+  AOB_LAUNCH_CHECK("sh_fill_image_kernel");
+  ++image_gen;
+}

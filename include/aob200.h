@@ -1,0 +1,201 @@
+/*
+ * aob200.h -- C ABI of the B200-native adaptive-optics hot path.
+ *
+ * One shared library (libaob200.so) exports these entry points.  They take
+ * plain pointers and sizes, return an int status (AOB_OK = 0, AOB_ERR = 1)
+ * and never throw; the message of the last failure on the calling thread is
+ * available from aob_last_error().  Streams are passed as void* (a
+ * cudaStream_t; NULL = the legacy default stream).  Host arrays are in the
+ * reference's Fortran (column-major) order: element (x, y) of an n x n map
+ * is at x + y*n.
+ *
+ * Each entry point names the reference interface it replaces (paths within
+ * the reference project).  The drop-in Python modules `sutra` / `carma` shipped
+ * with this library bind exactly these symbols with ctypes.
+ */
+#ifndef AOB200_H
+#define AOB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define AOB_OK 0
+#define AOB_ERR 1
+
+/* ---- library --------------------------------------------------------- */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *aob_last_error(void);
+/* Library version string. */
+const char *aob_version(void);
+/* Number of CUDA devices visible (0 when none); never fails. */
+int aob_device_count(void);
+/* Copies between host and a device buffer owned by this library or the
+ * caller (the carma array buffer protocol, python_module/carma/src/obj.hpp:32-76). */
+int aob_memcpy_d2h(void *dst_host, const void *src_dev, size_t bytes, void *stream);
+int aob_memcpy_h2d(void *dst_dev, const void *src_host, size_t bytes, void *stream);
+int aob_memcpy_d2d(void *dst_dev, const void *src_dev, size_t bytes, void *stream);
+int aob_malloc(void **dev_ptr, size_t bytes, int device);
+int aob_free(void *dev_ptr);
+int aob_stream_sync(void *stream);
+/* Fill a device float buffer with a value (CarmaObj::memset / reset). */
+int aob_fill_f32(float *dev, size_t n, float value, void *stream);
+
+/* ---- Shack-Hartmann sensor ------------------------------------------ *
+ * Replaces SutraWfsSH (libsutra/src.cpp/sutra_wfs_sh.cpp) as created by
+ * SutraSensors (sutra_sensors.cpp:25-135) and bound by
+ * python_module/sutra/src/wfs_sh.cpp:41-148.                             */
+typedef struct aob_sh aob_sh;
+
+/* Constructor arguments of SutraWfsSH (sutra_wfs_sh.cpp:27-75). npup is the
+ * side of the guide-star phase screen the sensor reads (p_geom._n). */
+int aob_sh_create(aob_sh **out, int device, int nxsub, int nvalid, int npix, int nphase,
+                  int nrebin, int nfft, int ntot, int npup, float pdiam, float nphot,
+                  float nphot4imat);
+int aob_sh_destroy(aob_sh *h);
+/* SutraWfsSH::load_arrays (sutra_wfs_sh.cpp:308-331); phasemap, hrmap,
+ * ttprojmat and kernel are accepted for interface parity and may be NULL.
+ * binmap is [nrebin^2, npix^2], offsets [nphase^2]; fluxPerSub, validsubsx,
+ * validsubsy, istart and jstart have nvalid entries. */
+int aob_sh_load_arrays(aob_sh *h, const int32_t *phasemap, const int32_t *hrmap,
+                       const int32_t *binmap, const float *offsets, const float *fluxPerSub,
+                       const int32_t *validsubsx, const int32_t *validsubsy,
+                       const int32_t *istart, const int32_t *jstart, const float *ttprojmat,
+                       const float *kernel_c64);
+/* SutraWfs::set_pupil (sutra_wfs.cpp) -- npup x npup amplitude. */
+int aob_sh_set_pupil(aob_sh *h, const float *pupil_host);
+/* SutraWfs::set_noise (sutra_wfs.cpp:123-141); the generator is the
+ * project's Philox4x32-10 keyed by seed (not cuRAND). */
+int aob_sh_set_noise(aob_sh *h, float noise, int64_t seed);
+/* Guide-star wavelength in micron: phase scale 2*pi/lambda (sutra_source.cpp:97). */
+int aob_sh_set_lambda(aob_sh *h, float lambda_um);
+int aob_sh_set_nphot(aob_sh *h, float nphot);
+/* Frame counter used as the noise-stream counter (advances on each noisy image). */
+int aob_sh_set_frame(aob_sh *h, uint64_t frame);
+int aob_sh_get_frame(aob_sh *h, uint64_t *frame);
+/* Device pointers of the sensor's buffers (the Wfs d_* properties,
+ * python_module/sutra/src/wfs.cpp:54-225). which: "phase", "pupil",
+ * "bincube", "binimg", "intensities", "validsubsx", "validsubsy",
+ * "fluxPerSub", "binmap", "offsets", "istart", "jstart", "slopes". */
+int aob_sh_buffer(aob_sh *h, const char *which, void **dev_ptr, int64_t *nelem);
+/* SutraWfsSH::comp_image(noise) (sutra_wfs_sh.cpp:623-643): fused field fill,
+ * pruned 2-D DFT, |E|^2, binning, flux normalisation, photon/readout noise
+ * and image scatter in one kernel.  If a centroider is attached with
+ * aob_centro_attach_wfs, its slopes are computed in the same pass and kept
+ * for the next aob_centro_get_cog on that centroider. */
+int aob_sh_comp_image(aob_sh *h, int noise, void *stream);
+/* SutraWfsSH::fill_binimage (sutra_wfs_sh.cpp:599-621): re-scatter bincube. */
+int aob_sh_fill_binimage(aob_sh *h, void *stream);
+/* set_bincube / set_binimg: overwrite from host. */
+int aob_sh_set_bincube(aob_sh *h, const float *host, int64_t n);
+int aob_sh_set_binimg(aob_sh *h, const float *host, int64_t n);
+
+/* ---- centroiders ------------------------------------------------------ *
+ * Replaces SutraCentroiderCog / Tcog / Wcog (libsutra/src.cpp/
+ * sutra_centroider_{cog,tcog,wcog}.cpp, kernels sutra_centroider_*.cu) as
+ * bound by python_module/sutra/src/centroider*.cpp.                      */
+typedef struct aob_centro aob_centro;
+#define AOB_CENTRO_COG 0
+#define AOB_CENTRO_TCOG 1
+#define AOB_CENTRO_WCOG 2
+#define AOB_CENTRO_PYR 3
+#define AOB_SLOPES_UNTIED 0
+#define AOB_SLOPES_INTERLEAVED 1
+
+/* SutraRtc::add_centroider (libsutra/src.cpp/sutra_rtc.cpp:64-111). */
+int aob_centro_create(aob_centro **out, int device, int type, int nvalid, float offset,
+                      float scale);
+int aob_centro_destroy(aob_centro *c);
+/* Bind to a SH sensor: the centroider reads its binimg (SutraCentroider
+ * ctor, sutra_centroider.cpp:42-46) and its slopes are fused into
+ * aob_sh_comp_image. */
+int aob_centro_attach_wfs(aob_centro *c, aob_sh *h);
+int aob_centro_set_npix(aob_centro *c, int npix);
+int aob_centro_set_scale(aob_centro *c, float scale);
+int aob_centro_set_offset(aob_centro *c, float offset);
+int aob_centro_set_threshold(aob_centro *c, float threshold);
+int aob_centro_set_slope_order(aob_centro *c, int order);
+/* load_validpos (sutra_centroider.cpp:287-298). */
+int aob_centro_load_validpos(aob_centro *c, const int32_t *validx, const int32_t *validy, int n);
+/* set_centroids_ref (sutra_centroider.cpp:300-304). */
+int aob_centro_set_centroids_ref(aob_centro *c, const float *ref);
+/* wCoG weights: n == npix*npix (one map for all sub-apertures) or
+ * npix*npix*nvalid (sutra_centroider_wcog.cpp:47-75). */
+int aob_centro_load_weights(aob_centro *c, const float *weights, int64_t n);
+/* load_img / set_dark / set_flat / calibrate_img (sutra_centroider.cpp:
+ * 233-285,120-140,200-230): image of m x n pixels from host. */
+int aob_centro_load_img(aob_centro *c, const float *img, int m, int n);
+int aob_centro_set_dark(aob_centro *c, const float *dark, int n);
+int aob_centro_set_flat(aob_centro *c, const float *flat, int n);
+int aob_centro_calibrate_img(aob_centro *c, void *stream);
+/* get_cog (sutra_centroider_cog.cpp:51-98): slopes into dev_slopes (2*nvalid
+ * floats, device) and intensities into the centroider's buffer. */
+int aob_centro_get_cog(aob_centro *c, float *dev_slopes, void *stream);
+int aob_centro_buffer(aob_centro *c, const char *which, void **dev_ptr, int64_t *nelem);
+int aob_centro_get_params(aob_centro *c, int *type, int *nvalid, int *npix, float *offset,
+                          float *scale, float *threshold);
+
+/* ---- least-squares controller ------------------------------------------ *
+ * Replaces SutraControllerLs + SutraController (libsutra/src.cpp/
+ * sutra_controller_ls.cpp, sutra_controller.cpp) as bound by
+ * python_module/sutra/src/controller_ls.cpp:69-245 and controller.cpp.    */
+typedef struct aob_ls aob_ls;
+#define AOB_PREC_F32 0
+#define AOB_PREC_BF16 1
+#define AOB_PREC_FP8 2
+
+int aob_ls_create(aob_ls **out, int device, int nslope, int nactu, float delay);
+int aob_ls_destroy(aob_ls *c);
+/* set_cmat (sutra_controller_ls.cpp:152-157): column-major [nactu, nslope]. */
+int aob_ls_set_cmat(aob_ls *c, const float *cmat);
+int aob_ls_set_imat(aob_ls *c, const float *imat);
+/* set_modal_gains (sutra_controller_ls.cpp:166-171). */
+int aob_ls_set_modal_gains(aob_ls *c, const float *gains);
+int aob_ls_set_gain(aob_ls *c, float gain);
+int aob_ls_set_delay(aob_ls *c, float delay);
+int aob_ls_set_open_loop(aob_ls *c, int open_loop, int reset);
+int aob_ls_set_com_range(aob_ls *c, float volt_min, float volt_max);
+int aob_ls_set_com(aob_ls *c, const float *com, int n);
+int aob_ls_set_centroids(aob_ls *c, const float *s, int n);
+/* Precision of the command-matrix MVM: F32 (reference), BF16, or FP8 E4M3
+ * with one float32 scale per actuator row; accumulation is always float32. */
+int aob_ls_set_precision(aob_ls *c, int prec);
+/* comp_com (sutra_controller_ls.cpp:251-285): err = -cmat.s,
+ * com += gain * err * modal_gains, one kernel. */
+int aob_ls_comp_com(aob_ls *c, void *stream);
+/* clip_commands (sutra_controller.cpp:221-229). */
+int aob_ls_clip(aob_ls *c, void *stream);
+/* comp_voltage (sutra_controller.cpp:245-263): latency interpolation,
+ * command delay ring, perturbation voltages, clip. */
+int aob_ls_comp_voltage(aob_ls *c, void *stream);
+/* Perturbation voltages (sutra_controller.cpp:98-195): perturb is
+ * [N, nactu] column-major. */
+int aob_ls_add_perturb(aob_ls *c, const char *name, const float *perturb, int n);
+int aob_ls_remove_perturb(aob_ls *c, const char *name);
+int aob_ls_enable_perturb(aob_ls *c, const char *name, int enable);
+int aob_ls_reset_perturb(aob_ls *c);
+/* One SVD-style eigen decomposition of imat^T imat in float64 on the GPU
+ * (svdec_imat, sutra_controller_ls.cpp:116-150) and the filtered
+ * pseudo-inverse (build_cmat, :174-217). */
+int aob_ls_svdec_imat(aob_ls *c);
+int aob_ls_build_cmat(aob_ls *c, int nfilt);
+/* which: "centroids", "com", "com_clipped", "voltage", "err", "cmat",
+ * "imat", "eigenvals", "gain", "com0", "com1". */
+int aob_ls_buffer(aob_ls *c, const char *which, void **dev_ptr, int64_t *nelem);
+int aob_ls_get_params(aob_ls *c, int *nslope, int *nactu, float *delay, float *gain,
+                      int *open_loop, float *volt_min, float *volt_max, int *prec);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif /* AOB200_H */

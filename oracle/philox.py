@@ -1,0 +1,140 @@
+"""Philox4x32-10 counter-based generator and the noise samplers built on it.
+
+Philox is the published generator of Salmon, Moraes, Dror and Shaw,
+"Parallel random numbers: as easy as 1, 2, 3" (SC'11): ten rounds of a
+multiply-xor bijection over a 128-bit counter, keyed by a 64-bit key bumped
+by the golden-ratio Weyl constants each round.  The GPU kernels use the same
+stream, so the raw 32-bit words are bit-identical between this module and the
+device.  This replaces the reference's cuRAND XORWOW states
+(libcarma/src.cu/carma_rng.cu:35-141), whose streams cannot be reproduced.
+
+Counter layout used by the sensors (one 128-bit block per pixel and draw):
+  c0 = pixel index, c1 = frame number, c2 = stream tag, c3 = draw number
+  key = (seed & 0xffffffff, seed >> 32)
+Stream tags: 0 = photon (Poisson) noise, 1 = readout (Gaussian) noise.
+
+Poisson sampling (replaces curand_poisson, carma_rng.cu:135-141):
+  lambda < 10: sequential-search inversion (Devroye 1986, ch. X.3) on one
+               uniform, in float64 with no fused multiply-add;
+  lambda >= 10: PTRS transformed rejection (Hoermann 1993, "The transformed
+               rejection method for generating Poisson random variables").
+Gaussian: Box-Muller on one block (u1 from words 0-1, u2 from words 2-3).
+"""
+
+import math
+
+import numpy as np
+
+M0 = 0xD2511F53
+M1 = 0xCD9E8D57
+W0 = 0x9E3779B9
+W1 = 0xBB67AE85
+MASK = 0xFFFFFFFF
+
+TAG_POISSON = 0
+TAG_GAUSS = 1
+POISSON_SMALL = 10.0
+POISSON_MAX_DRAWS = 64
+
+
+def philox4x32(c0, c1, c2, c3, k0, k1):
+    """Ten Philox rounds on uint32 numpy arrays (broadcasting); returns 4 uint32 arrays."""
+    c0 = np.asarray(c0, dtype=np.uint64) & MASK
+    c1 = np.asarray(c1, dtype=np.uint64) & MASK
+    c2 = np.asarray(c2, dtype=np.uint64) & MASK
+    c3 = np.asarray(c3, dtype=np.uint64) & MASK
+    k0 = np.asarray(k0, dtype=np.uint64) & MASK
+    k1 = np.asarray(k1, dtype=np.uint64) & MASK
+    for r in range(10):
+        p0 = c0 * np.uint64(M0)
+        p1 = c2 * np.uint64(M1)
+        hi0, lo0 = p0 >> np.uint64(32), p0 & np.uint64(MASK)
+        hi1, lo1 = p1 >> np.uint64(32), p1 & np.uint64(MASK)
+        c0, c1, c2, c3 = (hi1 ^ c1 ^ k0) & np.uint64(MASK), lo1, (hi0 ^ c3 ^ k1) & np.uint64(MASK), lo0
+        if r < 9:
+            k0 = (k0 + np.uint64(W0)) & np.uint64(MASK)
+            k1 = (k1 + np.uint64(W1)) & np.uint64(MASK)
+    return (c0.astype(np.uint32), c1.astype(np.uint32), c2.astype(np.uint32), c3.astype(np.uint32))
+
+
+def key_of(seed):
+    seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    return seed & MASK, seed >> 32
+
+
+def u01(x):
+    """Open-interval uniform from one 32-bit word, exact in float64."""
+    return (np.asarray(x, dtype=np.float64) + 0.5) * (1.0 / 4294967296.0)
+
+
+def _ptrs(lam, words_of_draw):
+    slam = math.sqrt(lam)
+    loglam = math.log(lam)
+    b = 0.931 + 2.53 * slam
+    a = -0.059 + 0.02483 * b
+    invalpha = 1.1239 + 1.1328 / (b - 3.4)
+    vr = 0.9277 - 3.6224 / (b - 2.0)
+    for d in range(POISSON_MAX_DRAWS):
+        w = words_of_draw(d)
+        u = float(u01(w[0])) - 0.5
+        v = float(u01(w[1]))
+        us = 0.5 - abs(u)
+        k = math.floor((2.0 * a / us + b) * u + lam + 0.43)
+        if us >= 0.07 and v <= vr:
+            return k
+        if k < 0 or (us < 0.013 and v > us):
+            continue
+        if (math.log(v) + math.log(invalpha) - math.log(a / (us * us) + b)
+                <= -lam + k * loglam - math.lgamma(k + 1.0)):
+            return k
+    return math.floor(lam + 0.5)
+
+
+def _inversion(lam, u):
+    p = math.exp(-lam)
+    f = p
+    k = 0
+    while u > f and k < 1000:
+        k += 1
+        p = p * (lam / k)
+        f = f + p
+    return k
+
+
+def poisson(lam, index, frame, seed):
+    """Poisson deviates for an array of means ``lam`` at pixel ``index``; float64 out."""
+    lam = np.asarray(lam, dtype=np.float64)
+    index = np.asarray(index, dtype=np.uint64)
+    k0, k1 = key_of(seed)
+    out = np.zeros(lam.shape, dtype=np.float64)
+    flat_l = lam.ravel()
+    flat_i = np.broadcast_to(index, lam.shape).ravel()
+    w0 = philox4x32(flat_i, frame, TAG_POISSON, 0, k0, k1)
+    res = out.ravel()
+    for j in range(flat_l.size):
+        m = float(flat_l[j])
+        if not (m > 0.0):
+            res[j] = 0.0
+        elif m < POISSON_SMALL:
+            res[j] = _inversion(m, float(u01(w0[0][j])))
+        else:
+            ij = int(flat_i[j])
+
+            def words(d, ij=ij, j=j):
+                if d == 0:
+                    return (w0[0][j], w0[1][j])
+                w = philox4x32(ij, frame, TAG_POISSON, d, k0, k1)
+                return (w[0], w[1])
+
+            res[j] = _ptrs(m, words)
+    return res.reshape(lam.shape)
+
+
+def gaussian(index, frame, seed):
+    """Standard normal deviates (float64) for pixel indices ``index``."""
+    index = np.asarray(index, dtype=np.uint64)
+    k0, k1 = key_of(seed)
+    w = philox4x32(index, frame, TAG_GAUSS, 0, k0, k1)
+    u1 = u01(w[0])
+    u2 = u01(w[2])
+    return np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2)

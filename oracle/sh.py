@@ -1,0 +1,95 @@
+"""Shack-Hartmann image formation in float64 (oracle).
+
+Follows the reference's SutraWfsSH::comp_generic / fill_binimage
+(libsutra/src.cpp/sutra_wfs_sh.cpp:337-621) and its kernels:
+  camplipup_krnl   libsutra/src.cu/sutra_wfs.cu:27-53   field in each sub-aperture
+  cuFFT forward    sutra_wfs_sh.cpp:393 (carma_fft.cpp:175-179, dir=1 -> CUFFT_FORWARD)
+  abs2c_krnl       libsutra/src.cu/sutra_utils.cu:144-168
+  fillbincube_krnl sutra_wfs.cu:369-414   binning through ``binmap``
+  reduce2          sutra_wfs.cu:556-590   per-sub-aperture sum
+  subapnorm_krnl   sutra_utils.cu:170-193 flux normalisation (skipped when the sum is 0)
+  prng('P'), prng('N', noise, 1)  sutra_wfs_sh.cpp:580-587 photon + readout noise
+  bimg_krnl        sutra_wfs.cu:183-229   scatter to the 2-D image
+Only the Ntot == Nfft (no field-of-view extension), natural-guide-star path
+is restated.
+
+Array convention: every 2-D numpy array ``a`` here is indexed ``a[x, y]`` with
+``x`` the fastest-varying device index (the reference passes F-ordered arrays).
+"""
+
+import numpy as np
+
+from . import philox
+
+
+def spot_field(phase, pupil, puppixx, puppixy, offsets, scale, pdiam, nfft):
+    """Complex field cube [nfft, nfft, nvalid], non-zero in the top-left pdiam x pdiam."""
+    nvalid = len(puppixx)
+    x = np.arange(pdiam)
+    ix = puppixx[None, None, :] + x[:, None, None]
+    iy = puppixy[None, None, :] + x[None, :, None]
+    ph = phase[ix, iy].astype(np.float64) * scale - offsets.astype(np.float64)[:, :, None]
+    amp = pupil[ix, iy].astype(np.float64)
+    cube = np.zeros((nfft, nfft, nvalid), dtype=np.complex128)
+    cube[:pdiam, :pdiam, :] = amp * np.exp(1j * ph)
+    return cube
+
+
+def hr_images(field):
+    """|FFT|^2 of every sub-aperture (forward transform, unnormalised)."""
+    return np.abs(np.fft.fft2(field, axes=(0, 1))) ** 2
+
+
+def bin_cube(hr, binmap):
+    """bincube[p, k] = sum_r hr_flat[binmap[r, p], k] with hr_flat[x + y*nfft]."""
+    nfft = hr.shape[0]
+    flat = hr.reshape(nfft * nfft, -1, order="F")
+    return flat[binmap, :].sum(axis=0)
+
+
+def normalise(bincube, flux_per_sub, nphot):
+    """Scale each sub-aperture to flux_per_sub * nphot photons; returns (cube, raw sums)."""
+    sums = bincube.sum(axis=0)
+    out = bincube.copy()
+    nz = sums != 0
+    out[:, nz] = bincube[:, nz] * flux_per_sub[nz] / sums[nz] * nphot
+    return out, sums
+
+
+def add_noise(bincube, noise, seed, frame):
+    """Photon noise when noise > -1, then readout noise of rms ``noise`` when noise > 0."""
+    out = bincube.astype(np.float64)
+    idx = np.arange(out.size, dtype=np.uint64).reshape(out.shape, order="F")
+    if noise > -1:
+        # the device samples the float32 mean, as the reference's curand_poisson does
+        out = philox.poisson(out.astype(np.float32).astype(np.float64), idx, frame, seed)
+    if noise > 0:
+        out = out.astype(np.float32).astype(np.float64) + np.float32(noise) * philox.gaussian(idx, frame, seed)
+    return out
+
+
+def bin_image(bincube, validsubsx, validsubsy, npix, nxsub):
+    """Scatter sub-aperture cubes into the npix*nxsub square sensor image."""
+    size = npix * nxsub
+    img = np.zeros((size, size), dtype=bincube.dtype)
+    p = np.arange(npix * npix)
+    px, py = p % npix, p // npix
+    for k in range(bincube.shape[1]):
+        img[validsubsx[k] + px, validsubsy[k] + py] = bincube[:, k]
+    return img
+
+
+def comp_image(phase, pupil, g, scale, nphot, noise=-1.0, seed=1234, frame=0):
+    """Full SH image: returns (bincube, binimg, intensities) in float64.
+
+    ``g`` is an object/dict with the SH geometry fields (validpuppixx/y,
+    halfxy, binmap, fluxPerSub, validsubsx/y, pdiam, nfft, npix, nxsub).
+    """
+    get = (lambda k: g[k]) if isinstance(g, dict) else (lambda k: getattr(g, k))
+    field = spot_field(phase, pupil, get("validpuppixx"), get("validpuppixy"), get("halfxy"),
+                       scale, int(get("pdiam")), int(get("nfft")))
+    cube = bin_cube(hr_images(field), get("binmap"))
+    cube, sums = normalise(cube, get("fluxPerSub").astype(np.float64), nphot)
+    cube = add_noise(cube, noise, seed, frame)
+    img = bin_image(cube, get("validsubsx"), get("validsubsy"), int(get("npix")), int(get("nxsub")))
+    return cube, img, sums

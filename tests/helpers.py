@@ -1,0 +1,36 @@
+"""Shared test inputs: seeded phase screens and geometry builders."""
+
+import numpy as np
+
+from aob200 import geometry as G
+
+SH_CASES = {
+    "sh8": (G.ShParams(nxsub=8, npix=2, pixsize=0.3, wavelength_um=0.7, fracsub=0.5, gsmag=8.0), 48),
+    "sh16": (G.ShParams(nxsub=16, npix=8, pixsize=0.3, wavelength_um=0.7, fracsub=0.5, gsmag=8.0), 128),
+    "sh40": (G.ShParams(nxsub=40, npix=6, pixsize=0.36, wavelength_um=0.7, fracsub=0.5, gsmag=8.0), 240),
+}
+
+
+def sh_geometry(name):
+    p, pup = SH_CASES[name]
+    return G.sh_geometry(p, pup, diam=8.0, cobs=0.14, ittime=0.001)
+
+
+def kolmogorov_screen(n, r0_pixels, seed, lam_um=0.5):
+    """FFT-filtered Kolmogorov phase screen in micron (test input only)."""
+    rng = np.random.default_rng(seed)
+    f = np.fft.fftfreq(n)
+    fx, fy = np.meshgrid(f, f, indexing="ij")
+    k = np.hypot(fx, fy)
+    k[0, 0] = 1.0
+    psd = 0.023 * r0_pixels ** (-5.0 / 3.0) * k ** (-11.0 / 3.0)
+    psd[0, 0] = 0.0
+    noise = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    ph = np.fft.ifft2(noise * np.sqrt(psd)).real * n  # radians at 0.5 um
+    return (ph * lam_um / (2 * np.pi)).astype(np.float32)
+
+
+def rel_rms(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.sqrt(np.mean((a - b) ** 2)) / max(np.sqrt(np.mean(b**2)), 1e-300))

@@ -1,0 +1,191 @@
+"""GPU parity of the SH sensor, centroiders and LS controller against the CPU oracle.
+
+Tolerances (stated by the project's accuracy contract):
+  * slopes: relative rms error <= 1e-4 against the float64 oracle;
+  * spot images / intensities: relative rms error <= 1e-5;
+  * Poisson photon noise: bit-exact given the same float32 means;
+  * readout noise (Box-Muller in float64, stored float32): |diff| <= 1e-5 * noise;
+  * MVM float32: relative rms <= 1e-6; bf16 / fp8 within the stated quantisation bounds.
+"""
+
+import numpy as np
+import pytest
+
+from helpers import kolmogorov_screen, rel_rms, sh_geometry
+from oracle import philox, rtc as ortc, sh as osh
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def core():
+    from aob200 import core as C
+    from aob200 import _lib
+
+    if _lib.device_count() < 1:
+        pytest.fail("no CUDA device visible to libaob200")
+    return C
+
+
+def _setup(core, name, noise=-1.0, seed=7):
+    g = sh_geometry(name)
+    w = core.ShWfs.from_geometry(g, noise=noise, seed=seed)
+    phase = kolmogorov_screen(g.tel.n, r0_pixels=0.16 / (8.0 / g.tel.pupdiam), seed=seed)
+    w.set_phase(phase)
+    return g, w, phase
+
+
+@pytest.mark.parametrize("name", ["sh8", "sh16", "sh40"])
+def test_sh_image_matches_oracle(core, name):
+    g, w, phase = _setup(core, name)
+    w.comp_image(noise=False)
+    cube = np.array(w.d_bincube).reshape(g.npix * g.npix, g.nvalid, order="F")
+    img = np.array(w.d_binimg)
+    inten = np.array(w.d_intensities)
+    scale = 2 * np.pi / g.wavelength_um
+    ocube, oimg, osums = osh.comp_image(phase, g.tel.mpupil, g, scale, g.nphotons, noise=-1)
+    assert rel_rms(cube, ocube) < 1e-5
+    assert rel_rms(img, oimg) < 1e-5
+    assert rel_rms(inten, osums) < 1e-5
+
+
+@pytest.mark.parametrize("kind", ["cog", "tcog", "wcog"])
+@pytest.mark.parametrize("name", ["sh16", "sh40"])
+def test_fused_and_standalone_centroids_match_oracle(core, name, kind):
+    g, w, phase = _setup(core, name)
+    offset, scale = g.npix / 2 - 0.5, g.pixsize
+    c = core.Centroider(g.nvalid, offset, scale, kind)
+    c.set_npix(g.npix)
+    c.load_validpos(g.validsubsx, g.validsubsy)
+    thr = 0.05 * g.nphotons / (g.npix * g.npix)
+    c.set_threshold(thr)
+    wts = None
+    if kind == "wcog":
+        x = np.arange(g.npix) - (g.npix - 1) / 2
+        wts = np.exp(-(x[:, None] ** 2 + x[None, :] ** 2) / (2 * (g.npix / 2.0) ** 2)).astype(np.float32)
+        c.load_weights(wts)
+    ref = np.random.default_rng(3).standard_normal(2 * g.nvalid).astype(np.float32) * 0.01
+    c.set_centroids_ref(ref)
+    c.attach(w)
+    ls = core.LsController(2 * g.nvalid, 4)
+    dslopes = ls.buffer("centroids")
+
+    w.comp_image(noise=False)
+    img0 = np.array(w.d_binimg)
+    c.get_cog(dslopes.ptr)  # fused path
+    fused = np.array(dslopes)
+    img_after = np.array(w.d_binimg)
+
+    wflat = None if wts is None else np.tile(wts.ravel(order="F"), g.nvalid)
+    os_, oint, oimg = ortc.centroids(img0, g.validsubsx, g.validsubsy, g.npix, scale, offset, ref=ref,
+                                     kind=kind, threshold=thr, weights=wflat)
+    assert rel_rms(fused, os_) < 1e-4
+    assert rel_rms(np.array(c.buffer("intensities")), oint) < 1e-5
+    # tCoG leaves its thresholded pixels in the image, like the reference
+    assert rel_rms(img_after, oimg) < 1e-6
+
+    # standalone kernel on a fresh image gives the same slopes
+    c.attach(None)
+    w.comp_image(noise=False)
+    c2 = core.Centroider(g.nvalid, offset, scale, kind, wfs=None)
+    c2.set_npix(g.npix)
+    c2.load_validpos(g.validsubsx, g.validsubsy)
+    c2.set_threshold(thr)
+    c2.set_centroids_ref(ref)
+    if wts is not None:
+        c2.load_weights(wts)
+    c2.load_img(np.array(w.d_binimg))
+    c2.calibrate_img()
+    c2.get_cog(dslopes.ptr)
+    assert rel_rms(np.array(dslopes), os_) < 1e-4
+
+
+def test_photon_noise_bit_exact_and_readout_noise(core):
+    g, w, phase = _setup(core, "sh16", noise=0.5, seed=11)
+    w.comp_image(noise=False)
+    lam = np.array(w.d_bincube).reshape(-1, order="F").astype(np.float32)
+    frame = w.frame
+    w.comp_image(noise=True)
+    noisy = np.array(w.d_bincube).reshape(-1, order="F")
+    idx = np.arange(lam.size, dtype=np.uint64)
+    pois = philox.poisson(lam.astype(np.float64), idx, frame, 11)
+    gaus = philox.gaussian(idx, frame, 11)
+    expected = pois.astype(np.float32) + np.float32(0.5) * gaus.astype(np.float32)
+    # float32 rounding of (photons + noise * N): allow two ulps of the result
+    assert np.all(np.abs(noisy - expected) <= 2 * np.spacing(np.abs(expected)) + 1e-5)
+    # photon part alone: exact
+    w.set_noise(0.0, 11)
+    w.frame = frame
+    w.comp_image(noise=True)
+    p_gpu = np.array(w.d_bincube).reshape(-1, order="F")
+    np.testing.assert_array_equal(p_gpu, pois.astype(np.float32))
+    assert w.frame == frame + 1
+
+
+def test_ls_mvm_integrator_precisions(core):
+    rng = np.random.default_rng(5)
+    nslope, nactu = 2496, 1377
+    cmat = (rng.standard_normal((nactu, nslope)) * 0.01).astype(np.float32)
+    s = rng.standard_normal(nslope).astype(np.float32)
+    gains = rng.uniform(0.5, 1.5, nactu).astype(np.float32)
+    ref = -(cmat.astype(np.float64) @ s.astype(np.float64))
+    for prec, tol in (("f32", 1e-6), ("bf16", 8e-3), ("fp8", 6e-2)):
+        c = core.LsController(nslope, nactu)
+        c.set_precision(prec)
+        c.set_cmat(cmat)
+        c.set_gain(0.4)
+        c.set_modal_gains(gains)
+        c.set_centroids(s)
+        c.comp_com()
+        err = np.array(c.buffer("err"))
+        com = np.array(c.buffer("com"))
+        assert rel_rms(err, ref) < tol, prec
+        assert rel_rms(com, 0.4 * ref * gains) < tol, prec
+        c.comp_com()
+        assert rel_rms(np.array(c.buffer("com")), 0.8 * ref * gains) < tol, prec
+
+
+def test_ls_voltage_delay_perturb_clip_matches_oracle(core):
+    rng = np.random.default_rng(9)
+    nslope, nactu = 200, 60
+    for delay in (0.0, 1.0, 1.3, 2.7):
+        c = core.LsController(nslope, nactu, delay=delay)
+        o = ortc.LsController(nslope, nactu, delay=delay, gain=0.3)
+        cm = rng.standard_normal((nactu, nslope)).astype(np.float32) * 0.05
+        c.set_cmat(cm)
+        o.cmat = cm.astype(np.float64)
+        c.set_gain(0.3)
+        c.set_com_range(-0.8, 0.8)
+        o.volt_min, o.volt_max = -0.8, 0.8
+        pert = rng.standard_normal((3, nactu)).astype(np.float32) * 0.1
+        c.add_perturb("p", pert, 3)
+        o.perturb["p"] = [pert.astype(np.float64), 0, True]
+        for it in range(6):
+            s = rng.standard_normal(nslope).astype(np.float32)
+            c.set_centroids(s)
+            o.centroids = s.astype(np.float64)
+            c.comp_com()
+            o.comp_com()
+            c.comp_voltage()
+            v = o.comp_voltage()
+            assert rel_rms(np.array(c.buffer("voltage")), v) < 1e-5, (delay, it)
+            assert rel_rms(np.array(c.buffer("com")), o.com) < 1e-5, (delay, it)
+
+
+def test_svd_cmat_matches_numpy(core):
+    rng = np.random.default_rng(4)
+    nslope, nactu = 300, 120
+    imat = rng.standard_normal((nslope, nactu)).astype(np.float32)
+    c = core.LsController(nslope, nactu)
+    c.set_imat(imat)
+    c.svdec_imat()
+    ev = np.array(c.buffer("eigenvals"))
+    D = imat.astype(np.float64)
+    w, U = np.linalg.eigh(D.T @ D)
+    np.testing.assert_allclose(ev, w, rtol=1e-5)
+    nfilt = 5
+    c.build_cmat(nfilt)
+    inv = np.zeros_like(w)
+    inv[nfilt:] = 1.0 / w[nfilt:]
+    cm = (U * inv) @ U.T @ D.T
+    assert rel_rms(np.array(c.buffer("cmat", shape=(nactu, nslope))), cm) < 1e-5

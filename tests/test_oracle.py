@@ -1,0 +1,159 @@
+"""Pins the CPU oracle before it is trusted as the checker.
+
+* Philox4x32-10 against the published known-answer vectors (Random123 KAT).
+* Centroiders / control law / clip / latency against the same NumPy expressions
+  the reference's own test-suite uses (shesha/tests/pytest/rtc/test_rtcFFF.py:
+  154-163 CoG via scipy center_of_mass, 166-171 control law, 174-187 clip,
+  229-247 comp_voltage, 255-285 tCoG, 324-363 wCoG), at its tolerance 1e-2
+  (max error relative to the max) -- and far tighter here.
+* SH spot formation by analytic properties (the reference has no golden data
+  for it): a flat wavefront gives a centred spot, a tilt moves it by the
+  predicted number of pixels, total flux is normalised.
+"""
+
+import numpy as np
+import pytest
+from scipy.ndimage import center_of_mass
+
+from aob200 import geometry as G
+from oracle import philox, rtc, sh
+
+
+def test_philox_known_answers():
+    kat = [
+        ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+        ((0xFFFFFFFF,) * 4, (0xFFFFFFFF, 0xFFFFFFFF), (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+        ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+         (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+    ]
+    for ctr, key, want in kat:
+        got = philox.philox4x32(*ctr, *key)
+        assert tuple(int(x) for x in got) == want
+
+
+def test_poisson_statistics():
+    for lam in (0.3, 4.0, 9.9, 10.0, 57.0, 3000.0):
+        idx = np.arange(20000, dtype=np.uint64)
+        x = philox.poisson(np.full(idx.shape, lam), idx, frame=3, seed=99)
+        assert np.all(x == np.floor(x)) and np.all(x >= 0)
+        assert abs(x.mean() - lam) < 5 * np.sqrt(lam / x.size) + 1e-9
+        assert abs(x.var() / lam - 1) < 0.06
+
+
+def test_gaussian_statistics():
+    z = philox.gaussian(np.arange(200000, dtype=np.uint64), frame=1, seed=5)
+    assert abs(z.mean()) < 0.01 and abs(z.std() - 1) < 0.01
+
+
+def _image_from_cube(cube, g):
+    return sh.bin_image(cube, g.validsubsx, g.validsubsy, g.npix, g.nxsub)
+
+
+@pytest.fixture(scope="module")
+def geom16():
+    return G.sh_geometry(G.ShParams(nxsub=16, npix=8, pixsize=0.3, wavelength_um=0.7), 128)
+
+
+def _cube_as_xyk(cube, npix):
+    return cube.reshape(npix, npix, -1, order="F")
+
+
+def test_cog_matches_center_of_mass(geom16):
+    g = geom16
+    rng = np.random.default_rng(0)
+    cube = rng.random((g.npix * g.npix, g.nvalid))
+    img = _image_from_cube(cube, g)
+    offset, scale = g.npix / 2 - 0.5, g.pixsize
+    s, inten, _ = rtc.centroids(img, g.validsubsx, g.validsubsy, g.npix, scale, offset)
+    ref = np.zeros(2 * g.nvalid)
+    c3 = _cube_as_xyk(cube, g.npix)
+    for k in range(g.nvalid):
+        cm = center_of_mass(c3[:, :, k])
+        ref[k] = (cm[0] - offset) * scale
+        ref[k + g.nvalid] = (cm[1] - offset) * scale
+    assert np.abs(s - ref).max() / np.abs(ref).max() < 1e-6
+    np.testing.assert_allclose(inten, cube.sum(axis=0), rtol=1e-12)
+
+
+def test_tcog_and_wcog_match_reference_expressions(geom16):
+    g = geom16
+    rng = np.random.default_rng(1)
+    cube = rng.random((g.npix * g.npix, g.nvalid))
+    img = _image_from_cube(cube, g)
+    offset, scale, thr = g.npix / 2 - 0.5, g.pixsize, 0.1
+    s, _, img2 = rtc.centroids(img, g.validsubsx, g.validsubsy, g.npix, scale, offset,
+                               kind="tcog", threshold=thr)
+    c3 = _cube_as_xyk(cube, g.npix) - thr
+    c3[c3 < 0] = 0
+    ref = np.zeros(2 * g.nvalid)
+    for k in range(g.nvalid):
+        cm = center_of_mass(c3[:, :, k])
+        ref[k], ref[k + g.nvalid] = (cm[0] - offset) * scale, (cm[1] - offset) * scale
+    assert np.abs(s - ref).max() / np.abs(ref).max() < 1e-4
+    # the thresholded pixels are written back into the image
+    k0 = 0
+    blk = img2[g.validsubsx[k0]:g.validsubsx[k0] + g.npix, g.validsubsy[k0]:g.validsubsy[k0] + g.npix]
+    exp = _cube_as_xyk(cube, g.npix)[:, :, k0] - thr
+    np.testing.assert_allclose(blk, np.where(exp > 0, exp, 1e-6))
+
+    w = rng.random(g.npix * g.npix)
+    wfull = np.tile(w, g.nvalid)
+    s, _, _ = rtc.centroids(img, g.validsubsx, g.validsubsy, g.npix, scale, offset,
+                            kind="wcog", threshold=thr, weights=wfull)
+    c3 = _cube_as_xyk(cube, g.npix) - thr
+    c3[c3 < 0] = 1e-6
+    w2 = w.reshape(g.npix, g.npix, order="F")
+    for k in range(g.nvalid):
+        cm = center_of_mass(c3[:, :, k] * w2)
+        ref[k], ref[k + g.nvalid] = (cm[0] - offset) * scale, (cm[1] - offset) * scale
+    assert np.abs(s - ref).max() / np.abs(ref).max() < 1e-4
+
+
+def test_control_law_clip_and_latency():
+    rng = np.random.default_rng(2)
+    nslope, nactu = 60, 25
+    c = rtc.LsController(nslope, nactu, delay=1.3, gain=0.4)
+    c.cmat = rng.standard_normal((nactu, nslope))
+    c.centroids = rng.standard_normal(nslope)
+    c.comp_com()
+    np.testing.assert_allclose(c.com, -0.4 * c.cmat @ c.centroids)
+    # latency: a*ring[0] + b*ring[1] then perturbation then clip
+    com0, com1 = c.ring[0].copy(), c.ring[1].copy()
+    pert = rng.random(nactu)
+    c.perturb["test"] = [pert[None, :], 0, True]
+    c.volt_min, c.volt_max = -1, 1
+    v = c.comp_voltage()
+    exp = np.clip(0.3 * com0 + 0.7 * com1 + pert, -1, 1)
+    np.testing.assert_allclose(v, exp)
+
+
+def test_flat_wavefront_gives_centred_spot(geom16):
+    g = geom16
+    pupil = g.tel.mpupil
+    phase = np.zeros_like(pupil)
+    scale = 2 * np.pi / g.wavelength_um
+    cube, img, sums = sh.comp_image(phase, pupil, g, scale, g.nphotons, noise=-1)
+    # flux normalisation
+    np.testing.assert_allclose(cube.sum(axis=0), g.fluxPerSub.astype(np.float64) * g.nphotons, rtol=1e-12)
+    s, _, _ = rtc.centroids(img, g.validsubsx, g.validsubsy, g.npix, g.pixsize, g.npix / 2 - 0.5)
+    full = g.fluxPerSub > 0.999
+    assert np.abs(s[:g.nvalid][full]).max() < 1e-9
+    assert np.abs(s[g.nvalid:][full]).max() < 1e-9
+
+
+def test_tilt_moves_spot_by_prediction(geom16):
+    g = geom16
+    pupil = g.tel.mpupil
+    n = pupil.shape[0]
+    # tilt of 0.1 arcsec along x: phase [um] = theta[rad] * x[m] * 1e6
+    theta = 0.1 / G.RAD2ARCSEC
+    dx = 8.0 / g.tel.pupdiam
+    x = (np.arange(n) - n / 2) * dx
+    phase = (theta * x * 1e6)[:, None] * np.ones((1, n))
+    scale = 2 * np.pi / g.wavelength_um
+    _, img, _ = sh.comp_image(phase, pupil, g, scale, g.nphotons, noise=-1)
+    s, _, _ = rtc.centroids(img, g.validsubsx, g.validsubsy, g.npix, g.pixsize, g.npix / 2 - 0.5)
+    full = g.fluxPerSub > 0.999
+    # spot moves by +/- 0.1 arcsec (sign follows the forward FFT convention)
+    assert np.allclose(np.abs(s[:g.nvalid][full]), 0.1, atol=0.02)
+    assert np.abs(s[g.nvalid:][full]).max() < 1e-6
