@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Benchmark: AO loop iterations/s at the SAXO-scale 40x40 Shack-Hartmann loop.
+
+One step = one RTC iteration of the ``saxo40`` workload on one GPU: SH image
+formation from a resident phase screen (photon + 0.5 e- readout noise),
+weighted CoG with threshold fused into the sensor kernel, the 1377 x 2496
+command-matrix MVM with the integrator, and the voltage stage (delay ring,
+clip).  The L2 cache (126 MB) is flushed before every timed step by writing a
+256 MB buffer, so the 13.7 MB float32 command matrix is read from HBM each
+iteration.  Each step is bracketed by CUDA events on the launching stream; the
+value is steps / (sum of step times).
+
+Other keys of the JSON line:
+  e2e       the same step through the C ABI call a caller makes
+            (aob_loop_step) with the phase screen copied in from pinned host
+            memory and the voltages copied back every step;
+  roofline  the dominant kernel's algorithmic bytes / measured duration against
+            the measured HBM copy bandwidth in MEASURED_PEAKS.json;
+  cpu_baseline  the float64 NumPy/SciPy restatement timed on the host cores.
+
+--impl reference runs the reference-algorithm CPU restatement (the reference
+has no CPU implementation of this path; its GPU code needs its own CMake build)
+as the baseline arm.  Multi-GPU (torchrun): the path does not shard -- every
+rank runs an independent replica; value = total steps / max-over-ranks time.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "compass-saxoplus_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "AO loop iters/s at 40x40 SH (learned vs LS recon, same Strehl); % HBM peak"
+UNIT = "iters/s"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _profile_traffic(name):
+    """DRAM bytes per launch recorded from an ncu capture (profiles/<name>.txt)."""
+    p = os.path.join(ROOT, "profiles", name + ".txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    smax = float(f[2])
+                except ValueError:
+                    continue
+                for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                                    "sw_power_cap"), f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(name)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_baseline(setup, budget_s=12.0, max_iters=400):
+    """Time the float64 CPU restatement on a bounded number of iterations."""
+    from oracle.loop_cpu import CpuShLoop
+    from aob200.workloads import von_karman_screens
+
+    g = setup.geom
+    screens = von_karman_screens(g.tel.n, 8.0 / g.tel.pupdiam, 0.14, 25.0, 4, seed=1)
+    loop = CpuShLoop(g, setup.cmat, setup.centroider, setup.threshold, setup.weights, setup.noise)
+    loop.step(screens[0])
+    n = 0
+    t0 = time.perf_counter()
+    while n < max_iters and (time.perf_counter() - t0) < budget_s:
+        loop.step(screens[n % len(screens)])
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": UNIT, "cores": loop.workers, "kind": "port",
+            "sample": f"{n} iterations of the saxo40 RTC step (float64 NumPy/SciPy, {loop.workers} threads)"}
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    from aob200.workloads import sh_loop_setup
+
+    setup = sh_loop_setup("saxo40")
+    from oracle.loop_cpu import CpuShLoop
+    from aob200.workloads import von_karman_screens
+
+    g = setup.geom
+    screens = von_karman_screens(g.tel.n, 8.0 / g.tel.pupdiam, 0.14, 25.0, 4, seed=1)
+    loop = CpuShLoop(g, setup.cmat, setup.centroider, setup.threshold, setup.weights, setup.noise)
+    per_step = 3  # RTC iterations per benchmark step (bounded CPU sample)
+    for i in range(args.warmup):
+        loop.step(screens[i % 4])
+    t0 = time.perf_counter()
+    for i in range(args.steps * per_step):
+        loop.step(screens[i % 4])
+    dt = time.perf_counter() - t0
+    v = args.steps * per_step / dt
+    res = [{"cores": loop.workers,
+            "sample": f"{args.steps * per_step} iterations of the saxo40 RTC step "
+                      f"(float64 NumPy/SciPy, {loop.workers} threads)"}]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "saxo40: 40x40 SH, 1248 valid, 6x6 px, Nfft 32, wCoG+thr, photon+0.5e- noise, "
+                               "1377x2496 LS MVM", "device": "cpu"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": res[0]["cores"], "kind": "port",
+                         "sample": res[0]["sample"]},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "bf16", "fp8"])
+    ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    ws, rank, local = _dist()
+    import torch
+
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    device = local if ws > 1 else 0
+    torch.cuda.set_device(device)
+
+    from aob200 import _lib
+    from aob200.workloads import build_sh_loop, sh_loop_setup, von_karman_screens
+
+    setup = sh_loop_setup("saxo40")
+    g = setup.geom
+    wfs, centro, ls, loop = build_sh_loop(setup, precision=args.precision, device=device,
+                                          graph=not args.no_graph, seed=1234 + rank)
+    n = g.tel.n
+    nscreen = 8
+    screens = von_karman_screens(n, 8.0 / g.tel.pupdiam, 0.14, 25.0, nscreen, seed=rank)
+    d_screens = torch.from_numpy(np.ascontiguousarray(np.stack([s.ravel(order="F") for s in screens]))).cuda()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    phase_ptr = wfs.d_phase.ptr
+    nbytes_phase = n * n * 4
+
+    def load_phase(i):
+        _lib.call("aob_memcpy_d2d", phase_ptr, d_screens[i % nscreen].data_ptr(), nbytes_phase, sptr)
+
+    # ---- value: device-resident inputs, L2 flushed before each step --------
+    for i in range(args.warmup):
+        load_phase(i)
+        flush.zero_()
+        loop.step(None, None, noise=True, stream=sptr)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(device) as clk:
+        for i in range(args.steps):
+            load_phase(i)
+            flush.zero_()
+            starts[i].record(stream)
+            loop.step(None, None, noise=True, stream=sptr)
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    if dist:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    clocks = clk.summary()
+    ms_per_step = total_ms / args.steps
+    value = ws * args.steps / (total_ms / 1000.0)
+    launches = loop.kernels_per_step() * args.steps
+
+    # ---- per-kernel durations (dominant kernel roofline) -------------------
+    def time_kernel(fn, reps):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        for _ in range(3):
+            flush.zero_()
+            fn()
+        for a, b in evs:
+            flush.zero_()
+            a.record(stream)
+            fn()
+            b.record(stream)
+        torch.cuda.synchronize()
+        return statistics.mean(a.elapsed_time(b) for a, b in evs) / 1000.0
+
+    reps = max(20, min(args.steps, 200))
+    t_mvm = time_kernel(lambda: ls.comp_com(stream=sptr), reps)
+    t_wfs = time_kernel(lambda: wfs.comp_image(noise=True, stream=sptr), reps)
+    esize = {"f32": 4, "bf16": 2, "fp8": 1}[args.precision]
+    ld = {"f32": 4, "bf16": 8, "fp8": 16}[args.precision]
+    ncol_pad = (setup.nslope + ld - 1) // ld * ld
+    mvm_bytes = setup.nactu * ncol_pad * esize + setup.nslope * 4 + setup.nactu * 4 * 4 + \
+        (setup.nactu * 4 if args.precision == "fp8" else 0)
+    npix2 = g.npix * g.npix
+    wfs_bytes = 2 * g.nvalid * g.pdiam * g.pdiam * 4 + g.nvalid * npix2 * 4 * 2 + g.nvalid * (8 + 4 + 4 + 16) + \
+        2 * g.nvalid * 4
+    peak, peak_kind = _peaks()
+    if t_mvm >= t_wfs:
+        dom, dbytes, dt, prof = "ls_mvm_kernel<float>" if args.precision == "f32" else "ls_mvm_kernel", mvm_bytes, \
+            t_mvm, f"ls_mvm_saxo40_{args.precision}"
+    else:
+        dom, dbytes, dt, prof = "sh_image_kernel<32>", wfs_bytes, t_wfs, "sh_image_saxo40"
+    achieved = dbytes / dt / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": _profile_traffic(prof), "kernel": dom, "algorithmic_bytes": dbytes,
+                "duration_us": dt * 1e6, "peak_source": peak_kind,
+                "kernels_us": {"sh_image": t_wfs * 1e6, "ls_mvm": t_mvm * 1e6}}
+
+    # ---- e2e: through aob_loop_step with pinned host buffers ---------------
+    h_phase = torch.from_numpy(np.ascontiguousarray(np.stack([s.ravel(order="F") for s in screens]))).pin_memory()
+    h_volt = torch.zeros(setup.nactu, dtype=torch.float32).pin_memory()
+    e2e_steps = max(10, args.steps)
+    for i in range(3):
+        loop.step(h_phase[i % nscreen].data_ptr(), h_volt.data_ptr(), noise=True, stream=sptr)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(e2e_steps)]
+    wall = 0.0
+    for i, (a, b) in enumerate(ev):
+        flush.zero_()
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        a.record(stream)
+        loop.step(h_phase[i % nscreen].data_ptr(), h_volt.data_ptr(), noise=True, stream=sptr)
+        b.record(stream)
+        wall += time.perf_counter() - w0
+    torch.cuda.synchronize()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in ev)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": ws * e2e_steps / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": nbytes_phase,
+           "d2h_bytes_per_step": setup.nactu * 4, "wall_clock_value": e2e_steps / wall,
+           "call": "aob_loop_step(host phase -> host voltages)"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(setup)
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": args.precision, "data": "synthetic",
+        "config": {"workload": "saxo40: 40x40 SH (1248 valid, 2496 slopes), 6x6 px, Nfft 32, nrebin 3, "
+                               "wCoG+threshold, photon + 0.5 e- readout noise, LS 1377x2496 MVM + integrator + "
+                               "voltage; one RTC iteration per step",
+                   "l2": "flushed before every timed step (256 MB write)",
+                   "parallelism": f"replicas x{ws}", "cuda_graph": not args.no_graph,
+                   "mvm_precision": args.precision},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": launches,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

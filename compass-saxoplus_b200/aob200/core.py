@@ -337,3 +337,32 @@ class LsController:
         call("aob_ls_get_params", self.h, *[ctypes.addressof(x) for x in (ns, na, de, ga, ol, lo, hi, pr)])
         return dict(nslope=ns.value, nactu=na.value, delay=de.value, gain=ga.value, open_loop=ol.value,
                     volt_min=lo.value, volt_max=hi.value, prec=pr.value)
+
+
+class Loop:
+    """One RTC iteration bound to a sensor, a centroider and an LS controller."""
+
+    def __init__(self, wfs: ShWfs, centro: Centroider, ls: LsController, graph=True):
+        self.h = ctypes.c_void_p()
+        call("aob_loop_create", ctypes.addressof(self.h), wfs.h, centro.h, ls.h)
+        self.wfs, self.centro, self.ls = wfs, centro, ls
+        centro.wfs = wfs
+        self.use_graph(graph)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value and _lib._lib is not None:
+            _lib.lib().aob_loop_destroy(h)
+            self.h = None
+
+    def use_graph(self, on=True):
+        call("aob_loop_use_graph", self.h, 1 if on else 0)
+
+    def kernels_per_step(self) -> int:
+        n = ctypes.c_int()
+        call("aob_loop_kernels_per_step", self.h, ctypes.addressof(n))
+        return n.value
+
+    def step(self, host_phase=None, host_voltage=None, noise=True, stream=None):
+        """host_phase / host_voltage: numpy float32 arrays (pinned for speed) or None."""
+        call("aob_loop_step", self.h, addr(host_phase), addr(host_voltage), 1 if noise else 0, stream)

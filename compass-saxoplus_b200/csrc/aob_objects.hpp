@@ -49,6 +49,9 @@ struct aob_sh {
                    const int32_t *validsubsx, const int32_t *validsubsy, const int32_t *istart,
                    const int32_t *jstart);
   void comp_image(bool noise, cudaStream_t s);
+  // slopes_dst: write the fused centroider's slopes there instead of its staging
+  // buffer; frame_ptr: read the noise frame number from device memory
+  void comp_image_to(bool noise, cudaStream_t s, float *slopes_dst, const uint32_t *frame_ptr);
   void fill_binimage(cudaStream_t s);
   size_t smem_bytes() const;
 };
@@ -118,11 +121,32 @@ struct aob_ls {
   float *com() { return ring.back().p; }
   void set_delay(float d);
   void ensure_packed(int p);
-  void comp_com(cudaStream_t s);
+  void comp_com(cudaStream_t s, uint32_t *bump = nullptr);
   void comp_voltage(cudaStream_t s);
   void clip(cudaStream_t s);
   void svdec_imat();
   void build_cmat(int nfilt);
+};
+
+// ---------------------------------------------------------------------------
+// one RTC iteration bound to a sensor, a centroider and a controller
+struct aob_loop {
+  aob_sh *wfs;
+  aob_centro *centro;
+  aob_ls *ls;
+  aob::DevBuf<uint32_t> d_frame;
+  bool use_graph = false;
+  std::vector<cudaGraphExec_t> graphs;   // one per command-ring rotation
+  std::vector<uint64_t> graph_key;       // parameter snapshot each graph was built for
+  std::vector<const void *> graph_front; // ring front buffer each graph was built for
+  uint64_t frame_mirror = ~0ull;         // value held by d_frame
+  uint32_t frame_host = 0;
+  aob_loop(aob_sh *w, aob_centro *c, aob_ls *l);
+  ~aob_loop();
+  void device_step(bool noise, cudaStream_t s, bool frame_on_device);
+  void step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s);
+  uint64_t key(bool noise) const;
+  void drop_graphs();
 };
 
 namespace aob {

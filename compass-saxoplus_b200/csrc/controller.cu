@@ -40,6 +40,7 @@ struct MvmArgs {
   const float *mgain;     // modal gains
   float gain;
   int integrate;
+  uint32_t *bump;         // incremented once per launch when set (noise frame counter)
 };
 
 // Dot product of one 16-byte packed chunk with its slopes.  The slopes are
@@ -120,6 +121,7 @@ __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_kernel(MvmArgs A) {
     const int src = (l + 32 * j) * V + 4 * q + e;
     s_sh[i] = (src < A.ncol) ? A.s[src] : 0.f;
   }
+  if (A.bump && blockIdx.x == 0 && threadIdx.x == 0) *A.bump += 1u;
   __syncthreads();
   const float4 *sv = reinterpret_cast<const float4 *>(s_sh);
   const int r0 = (int)(((int64_t)blockIdx.x * A.nrow) / gridDim.x);
@@ -267,7 +269,7 @@ void aob_ls::ensure_packed(int p) {
   packed_valid[p] = true;
 }
 
-void aob_ls::comp_com(cudaStream_t s) {
+void aob_ls::comp_com(cudaStream_t s, uint32_t *bump) {
   if (open_loop) return;
   AOB_CUDA(cudaSetDevice(device));
   ensure_packed(prec);
@@ -280,6 +282,7 @@ void aob_ls::comp_com(cudaStream_t s) {
   A.mgain = gains.p;
   A.gain = gain;
   A.integrate = 1;
+  A.bump = bump;
   const int grid = nblocks > 0 ? std::min(nblocks, nactu) : std::min(nactu, num_sms(device));
   if (prec == AOB_PREC_F32) {
     A.mat = cm_f32.p;

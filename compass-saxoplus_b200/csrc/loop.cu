@@ -1,0 +1,213 @@
+// One RTC iteration (sensor image + fused centroids -> MVM + integrator ->
+// voltages) bound into one object, optionally replayed from CUDA graphs.
+//
+// The reference drives these stages as separate Python -> C++ calls, each a
+// handful of launches on the default stream with host synchronisation in
+// between (CompassSupervisor.next, shesha/shesha/supervisor/
+// compassSupervisor.py:175-289).  Here the device part is three kernels on one
+// stream: the sensor kernel writes the slopes directly into the controller's
+// input vector, the MVM kernel bumps the noise frame counter held in device
+// memory (so a captured graph stays valid from one iteration to the next),
+// and the voltage kernel applies delay / perturbation / clip.  Because the
+// command-history ring rotates every iteration, one graph is captured per
+// rotation phase; a graph is rebuilt when a parameter it baked in changes.
+
+#include <cstring>
+
+#include "aob_objects.hpp"
+
+using namespace aob;
+
+aob_loop::aob_loop(aob_sh *w, aob_centro *c, aob_ls *l) : wfs(w), centro(c), ls(l) {
+  AOB_REQUIRE(w && c && l, "loop: sensor, centroider and controller are required");
+  AOB_REQUIRE(w->device == c->device && w->device == l->device, "loop: objects on different devices");
+  AOB_REQUIRE(c->type <= 2, "loop: SH loops need a CoG-family centroider");
+  AOB_REQUIRE(2 * w->nvalid == l->nslope, "loop: controller nslope must be 2*nvalid of the sensor");
+  AOB_REQUIRE(c->nvalid == w->nvalid, "loop: centroider nvalid differs from the sensor's");
+  AOB_CUDA(cudaSetDevice(w->device));
+  d_frame.alloc(1);
+  if (c->wfs && c->wfs->fused == c && c->wfs != w) c->wfs->fused = nullptr;
+  c->wfs = w;
+  w->fused = c;
+}
+
+aob_loop::~aob_loop() { drop_graphs(); }
+
+void aob_loop::drop_graphs() {
+  for (auto &g : graphs)
+    if (g) cudaGraphExecDestroy(g);
+  graphs.clear();
+  graph_key.clear();
+  graph_front.clear();
+}
+
+// Everything a captured graph bakes into its kernel parameters.
+uint64_t aob_loop::key(bool noise) const {
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&h](const void *p, size_t n) {
+    const unsigned char *b = (const unsigned char *)p;
+    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+  };
+  mix(&noise, sizeof noise);
+  mix(&wfs->noise, sizeof wfs->noise);
+  mix(&wfs->seed, sizeof wfs->seed);
+  mix(&wfs->lambda_um, sizeof wfs->lambda_um);
+  mix(&wfs->nphot, sizeof wfs->nphot);
+  mix(&centro->params_gen, sizeof centro->params_gen);
+  mix(&ls->gain, sizeof ls->gain);
+  mix(&ls->a, sizeof ls->a);
+  mix(&ls->volt_min, sizeof ls->volt_min);
+  mix(&ls->volt_max, sizeof ls->volt_max);
+  mix(&ls->prec, sizeof ls->prec);
+  mix(&ls->nblocks, sizeof ls->nblocks);
+  const void *pm[4] = {ls->cm_f32.p, ls->cm_bf16.p, ls->cm_fp8.p, centro->weights.p};
+  mix(pm, sizeof pm);
+  return h;
+}
+
+void aob_loop::device_step(bool noise, cudaStream_t s, bool frame_on_device) {
+  const bool noisy = noise && wfs->noise > -1.f;
+  wfs->comp_image_to(noise, s, ls->centroids.p, frame_on_device ? d_frame.p : nullptr);
+  ls->comp_com(s, (frame_on_device && noisy) ? d_frame.p : nullptr);
+  ls->comp_voltage(s);
+}
+
+void aob_loop::step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s) {
+  AOB_CUDA(cudaSetDevice(wfs->device));
+  if (host_phase)
+    AOB_CUDA(cudaMemcpyAsync(wfs->phase.p, host_phase, wfs->phase.bytes(), cudaMemcpyHostToDevice, s));
+  bool perturbed = false;
+  for (auto &kv : ls->perturb) perturbed |= kv.second.on;
+  const bool graphable = use_graph && !perturbed && !ls->open_loop;
+  if (!graphable) {
+    device_step(noise, s, false);
+  } else {
+    // the ring of command buffers rotates every iteration: the graph for the
+    // current rotation is the one captured with the same front buffer
+    const void *front = ls->ring.front().p;
+    int slot = -1;
+    for (size_t i = 0; i < graphs.size(); ++i)
+      if (graph_front[i] == front) slot = (int)i;
+    if (slot < 0) {
+      graphs.push_back(nullptr);
+      graph_key.push_back(0);
+      graph_front.push_back(front);
+      slot = (int)graphs.size() - 1;
+    }
+    const uint64_t k = key(noise);
+    ls->ensure_packed(ls->prec);  // no synchronous copies may happen inside a capture
+    // the device frame counter must equal the host one at the start of the step
+    if (frame_mirror != wfs->frame) {
+      frame_host = (uint32_t)wfs->frame;
+      AOB_CUDA(cudaMemcpyAsync(d_frame.p, &frame_host, sizeof frame_host, cudaMemcpyHostToDevice, s));
+      frame_mirror = wfs->frame;
+    }
+    if (!graphs[slot] || graph_key[slot] != k) {
+      if (graphs[slot]) cudaGraphExecDestroy(graphs[slot]);
+      graphs[slot] = nullptr;
+      // capture on a private stream so that the caller's stream may be the legacy default one
+      cudaStream_t cs;
+      AOB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+      cudaGraph_t g = nullptr;
+      const uint64_t frame0 = wfs->frame;
+      cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        try {
+          device_step(noise, cs, true);
+        } catch (...) {
+          cudaStreamEndCapture(cs, &g);
+          if (g) cudaGraphDestroy(g);
+          cudaStreamDestroy(cs);
+          throw;
+        }
+        e = cudaStreamEndCapture(cs, &g);
+      }
+      cudaStreamDestroy(cs);
+      AOB_CUDA(e);
+      // the capture advanced the host-side state (ring rotation, frame); undo it,
+      // the replay below performs the step
+      wfs->frame = frame0;
+      if (ls->delay > 0) {
+        aob::DevBuf<float> t = std::move(ls->ring.back());
+        ls->ring.pop_back();
+        ls->ring.push_front(std::move(t));
+      }
+      cudaGraphExec_t ge = nullptr;
+      e = cudaGraphInstantiate(&ge, g, 0);
+      cudaGraphDestroy(g);
+      AOB_CUDA(e);
+      graphs[slot] = ge;
+      graph_key[slot] = k;
+    }
+    AOB_CUDA(cudaGraphLaunch(graphs[slot], s));
+    // host-side state the graph's kernels correspond to
+    if (noise && wfs->noise > -1.f) {
+      ++wfs->frame;
+      ++frame_mirror;
+    }
+    if (ls->delay > 0) {
+      aob::DevBuf<float> t = std::move(ls->ring.front());
+      ls->ring.pop_front();
+      ls->ring.push_back(std::move(t));
+    }
+    ++wfs->image_gen;
+  }
+  if (host_voltage) {
+    AOB_CUDA(cudaMemcpyAsync(host_voltage, ls->com_clipped.p, ls->com_clipped.bytes(), cudaMemcpyDeviceToHost, s));
+    AOB_CUDA(cudaStreamSynchronize(s));
+  }
+}
+
+extern "C" {
+
+int aob_loop_create(aob_loop **out, aob_sh *wfs, aob_centro *centro, aob_ls *ls) {
+  try {
+    if (!out) throw Error("aob_loop_create: null out pointer");
+    *out = nullptr;
+    *out = new aob_loop(wfs, centro, ls);
+    return AOB_OK;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return AOB_ERR;
+  }
+}
+
+int aob_loop_destroy(aob_loop *l) {
+  if (l) {
+    cudaSetDevice(l->wfs->device);
+    delete l;
+  }
+  return AOB_OK;
+}
+
+int aob_loop_step(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream) {
+  try {
+    if (!l) throw Error("aob_loop_step: null handle");
+    l->step(host_phase, host_voltage, noise != 0, reinterpret_cast<cudaStream_t>(stream));
+    return AOB_OK;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return AOB_ERR;
+  }
+}
+
+int aob_loop_use_graph(aob_loop *l, int enable) {
+  if (!l) {
+    set_last_error("aob_loop_use_graph: null handle");
+    return AOB_ERR;
+  }
+  l->use_graph = enable != 0;
+  if (!l->use_graph) l->drop_graphs();
+  return AOB_OK;
+}
+
+int aob_loop_kernels_per_step(aob_loop *l, int *n) {
+  if (!l || !n) {
+    set_last_error("aob_loop_kernels_per_step: null pointer");
+    return AOB_ERR;
+  }
+  *n = 3;
+  return AOB_OK;
+}
+
+}  // extern "C"

@@ -61,6 +61,7 @@ struct ShKernelArgs {
   int noise_mode;  // 0 none, 1 photon, 2 photon + readout
   float noise;
   uint32_t frame, k0, k1;
+  const uint32_t *frame_ptr;  // when set, the frame number is read from device memory
   // fused centroider (kind < 0: none)
   int ckind;
   float c_scale, c_offset, c_thresh;
@@ -161,6 +162,7 @@ __global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P)
     const float tot = warp_sum(part);
     if (lane == 0) P.intensities[k] = tot;
     const float fk = P.flux[k];
+    const uint32_t frame = P.frame_ptr ? *P.frame_ptr : P.frame;
     // 5. normalise, noise, write cube + image, centroid partial sums
     const int vx = P.validsubsx[k], vy = P.validsubsy[k];
     float cs = 0.f, cx = 0.f, cy = 0.f;
@@ -171,8 +173,8 @@ __global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P)
         float v = bv[j];
         if (tot != 0.f) v = v * fk / tot * P.nphot;
         const uint32_t pix = (uint32_t)(p + k * npix2);
-        if (P.noise_mode >= 1) v = (float)poisson_sample((double)v, pix, P.frame, P.k0, P.k1);
-        if (P.noise_mode >= 2) v = v + P.noise * (float)gauss_sample(pix, P.frame, P.k0, P.k1);
+        if (P.noise_mode >= 1) v = (float)poisson_sample((double)v, pix, frame, P.k0, P.k1);
+        if (P.noise_mode >= 2) v = v + P.noise * (float)gauss_sample(pix, frame, P.k0, P.k1);
         P.bincube[pix] = v;
         const int x = p % P.npix, y = p / P.npix;
         const int idim = (x + vx) + (y + vy) * P.img_size;
@@ -304,7 +306,9 @@ size_t aob_sh::smem_bytes() const {
   return hdr + SH_WARPS * per_warp;
 }
 
-void aob_sh::comp_image(bool with_noise, cudaStream_t s) {
+void aob_sh::comp_image(bool with_noise, cudaStream_t s) { comp_image_to(with_noise, s, nullptr, nullptr); }
+
+void aob_sh::comp_image_to(bool with_noise, cudaStream_t s, float *slopes_dst, const uint32_t *frame_ptr) {
   AOB_REQUIRE(loaded, "sh.comp_image: load_arrays has not been called");
   AOB_CUDA(cudaSetDevice(device));
   ShKernelArgs P{};
@@ -338,6 +342,7 @@ void aob_sh::comp_image(bool with_noise, cudaStream_t s) {
   P.frame = (uint32_t)frame;
   P.k0 = (uint32_t)((uint64_t)seed & 0xffffffffu);
   P.k1 = (uint32_t)((uint64_t)seed >> 32);
+  P.frame_ptr = frame_ptr;
   P.ckind = -1;
   aob_centro *c = fused;
   if (c && c->npix == npix && c->nvalid == nvalid && c->type <= 2 && c->validx.n == nvalid) {
@@ -349,7 +354,7 @@ void aob_sh::comp_image(bool with_noise, cudaStream_t s) {
     P.c_weights = c->weights.p;
     P.c_wper = c->weights_per_sub;
     P.c_order = c->order;
-    P.c_slopes = c->fused_slopes.p;
+    P.c_slopes = slopes_dst ? slopes_dst : c->fused_slopes.p;
     P.c_intens = c->intensities.p;
     if (c->type == 2) AOB_REQUIRE(c->weights.p != nullptr, "wcog: weights not loaded");
   } else {
@@ -376,7 +381,7 @@ void aob_sh::comp_image(bool with_noise, cudaStream_t s) {
   AOB_LAUNCH_CHECK("sh_image_kernel");
   if (P.noise_mode) ++frame;
   ++image_gen;
-  if (c) {
+  if (c && !slopes_dst) {
     c->fused_gen = image_gen;
     c->fused_params_gen = c->params_gen;
   }

@@ -192,6 +192,27 @@ int aob_ls_buffer(aob_ls *c, const char *which, void **dev_ptr, int64_t *nelem);
 int aob_ls_get_params(aob_ls *c, int *nslope, int *nactu, float *delay, float *gain,
                       int *open_loop, float *volt_min, float *volt_max, int *prec);
 
+
+/* ---- one closed-loop RTC iteration ------------------------------------ *
+ * The per-iteration RTC sequence that CompassSupervisor.next() drives
+ * through separate calls (shesha/shesha/supervisor/compassSupervisor.py:
+ * 175-289: compute_wfs_image -> do_centroids -> do_control -> apply_control
+ * with comp_voltage), bound into one object so that it runs as three kernels
+ * (SH image + fused centroids, MVM + integrator, voltage) with the slopes
+ * written straight into the controller's input. */
+typedef struct aob_loop aob_loop;
+int aob_loop_create(aob_loop **out, aob_sh *wfs, aob_centro *centro, aob_ls *ls);
+int aob_loop_destroy(aob_loop *l);
+/* One iteration.  host_phase (npup*npup floats, may be NULL = use the
+ * sensor's current device phase) is copied in first; host_voltage (nactu
+ * floats, may be NULL) receives the voltages, and the call then waits for
+ * the stream.  noise != 0 adds photon/readout noise. */
+int aob_loop_step(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream);
+/* Replay the device part of a step from a CUDA graph (enable != 0). */
+int aob_loop_use_graph(aob_loop *l, int enable);
+/* Kernels launched by the device part of one step. */
+int aob_loop_kernels_per_step(aob_loop *l, int *n);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -189,3 +189,44 @@ def test_svd_cmat_matches_numpy(core):
     inv[nfilt:] = 1.0 / w[nfilt:]
     cm = (U * inv) @ U.T @ D.T
     assert rel_rms(np.array(c.buffer("cmat", shape=(nactu, nslope))), cm) < 1e-5
+
+
+@pytest.mark.parametrize("graph", [False, True])
+@pytest.mark.parametrize("delay", [0.0, 1.0])
+def test_loop_matches_separate_calls(core, graph, delay):
+    """The bound loop (with or without CUDA-graph replay) equals the separate calls."""
+    rng = np.random.default_rng(21)
+    g = sh_geometry("sh16")
+    nact = 97
+
+    def build():
+        w = core.ShWfs.from_geometry(g, noise=0.5, seed=5)
+        c = core.Centroider(g.nvalid, g.npix / 2 - 0.5, g.pixsize, "wcog")
+        c.set_npix(g.npix)
+        c.load_validpos(g.validsubsx, g.validsubsy)
+        c.set_threshold(1.0)
+        c.load_weights(np.ones((g.npix, g.npix), np.float32))
+        ls = core.LsController(2 * g.nvalid, nact, delay=delay)
+        ls.set_cmat(cm)
+        ls.set_gain(0.3)
+        ls.set_com_range(-0.5, 0.5)
+        return w, c, ls
+
+    cm = (rng.standard_normal((nact, 2 * g.nvalid)) * 0.01).astype(np.float32)
+    screens = [kolmogorov_screen(g.tel.n, 20.0, seed=s) for s in range(5)]
+    w1, c1, l1 = build()
+    c1.attach(w1)
+    w2, c2, l2 = build()
+    loop = core.Loop(w2, c2, l2, graph=graph)
+    v2 = np.zeros(nact, np.float32)
+    for it, ph in enumerate(screens):
+        w1.set_phase(ph)
+        w1.comp_image(noise=True)
+        c1.get_cog(l1.buffer("centroids").ptr)
+        l1.comp_com()
+        l1.comp_voltage()
+        loop.step(np.ascontiguousarray(ph.ravel(order="F")), v2, noise=True)
+        v1 = np.array(l1.buffer("voltage"))
+        np.testing.assert_array_equal(np.array(l2.buffer("centroids")), np.array(l1.buffer("centroids")))
+        np.testing.assert_array_equal(v2, v1)
+    assert w1.frame == w2.frame == len(screens)

@@ -157,3 +157,20 @@ def test_tilt_moves_spot_by_prediction(geom16):
     # spot moves by +/- 0.1 arcsec (sign follows the forward FFT convention)
     assert np.allclose(np.abs(s[:g.nvalid][full]), 0.1, atol=0.02)
     assert np.abs(s[g.nvalid:][full]).max() < 1e-6
+
+
+def test_cpu_baseline_loop_matches_oracle(geom16):
+    """The vectorised CPU-baseline step equals the scalar oracle (noise off)."""
+    from oracle.loop_cpu import CpuShLoop
+
+    g = geom16
+    rng = np.random.default_rng(3)
+    nact = 50
+    cmat = rng.standard_normal((nact, 2 * g.nvalid)) * 0.01
+    n = g.tel.n
+    phase = (0.1 * rng.standard_normal((n, n))).astype(np.float32)
+    loop = CpuShLoop(g, cmat, "cog", gain=0.5, workers=2)
+    com = loop.step(phase)
+    _, img, _ = sh.comp_image(phase, g.tel.mpupil, g, 2 * np.pi / g.wavelength_um, g.nphotons)
+    s, _, _ = rtc.centroids(img, g.validsubsx, g.validsubsy, g.npix, g.pixsize, g.npix / 2 - 0.5)
+    np.testing.assert_allclose(com, -0.5 * cmat @ s, rtol=1e-9, atol=1e-12)
