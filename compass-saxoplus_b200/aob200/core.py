@@ -162,6 +162,9 @@ class ShWfs:
     def fill_binimage(self, stream=None):
         call("aob_sh_fill_binimage", self.h, stream)
 
+    def set_tuning(self, warps_per_subap=0):
+        call("aob_sh_set_tuning", self.h, int(warps_per_subap))
+
 
 class Centroider:
     """CoG / tCoG / wCoG centroider (SutraCentroider*)."""
@@ -302,6 +305,14 @@ class LsController:
 
     def comp_com(self, stream=None):
         call("aob_ls_comp_com", self.h, stream)
+
+    def set_tuning(self, kind=0, nblocks=0):
+        call("aob_ls_set_tuning", self.h, int(kind), int(nblocks))
+
+    def status(self, reset=False) -> int:
+        st = ctypes.c_uint32()
+        call("aob_ls_status", self.h, ctypes.addressof(st), 1 if reset else 0)
+        return st.value
 
     def clip(self, stream=None):
         call("aob_ls_clip", self.h, stream)

@@ -16,6 +16,9 @@
 #include "aob_common.cuh"
 
 struct aob_centro;
+namespace aob {
+struct MvmArgs;
+}
 
 // ---------------------------------------------------------------------------
 // Shack-Hartmann sensor (replaces SutraWfsSH, libsutra/src.cpp/sutra_wfs_sh.cpp)
@@ -53,7 +56,9 @@ struct aob_sh {
   // buffer; frame_ptr: read the noise frame number from device memory
   void comp_image_to(bool noise, cudaStream_t s, float *slopes_dst, const uint32_t *frame_ptr);
   void fill_binimage(cudaStream_t s);
-  size_t smem_bytes() const;
+  int wps_override = 0;  // warps per sub-aperture chosen by the autotuner (0 = heuristic)
+  size_t smem_bytes(int wps) const;
+  int pick_wps() const;
 };
 
 // ---------------------------------------------------------------------------
@@ -94,7 +99,9 @@ struct aob_ls {
   int open_loop = 0;
   float volt_min = -1.0e6f, volt_max = 1.0e6f;
   int prec = 0;
-  int nblocks = 0;  // MVM grid size (chosen by the autotuner, 0 = default)
+  int nblocks = 0;   // MVM grid size (chosen by the autotuner, 0 = one CTA per SM)
+  int mvm_kind = 0;  // 0 auto (bulk copy when it fits), 1 bulk copy, 2 register streaming
+  aob::DevBuf<uint32_t> status;  // error word of the MVM kernels
 
   aob::DevBuf<float> centroids, err, com_clipped, gains, cmat, imat, eigenvals_f;
   std::deque<aob::DevBuf<float>> ring;  // command history, back() = current command
@@ -122,6 +129,7 @@ struct aob_ls {
   void set_delay(float d);
   void ensure_packed(int p);
   void comp_com(cudaStream_t s, uint32_t *bump = nullptr);
+  void launch_mvm(struct aob::MvmArgs &A, cudaStream_t s);
   void comp_voltage(cudaStream_t s);
   void clip(cudaStream_t s);
   void svdec_imat();

@@ -208,6 +208,13 @@ int aob_sh_fill_binimage(aob_sh *h, void *stream) {
   h->fill_binimage(S(stream));
   AOB_API_END
 }
+int aob_sh_set_tuning(aob_sh *h, int wps) {
+  AOB_API_BEGIN
+  NEED(h);
+  if (wps != 0 && wps != 1 && wps != 2 && wps != 4) throw Error("sh.set_tuning: warps per sub-aperture must be 0, 1, 2 or 4");
+  h->wps_override = wps;
+  AOB_API_END
+}
 int aob_sh_set_bincube(aob_sh *h, const float *host, int64_t n) {
   AOB_API_BEGIN
   NEED(h); NEED(host);
@@ -488,6 +495,22 @@ int aob_ls_set_precision(aob_ls *c, int prec) {
   if (prec < 0 || prec > 2) throw Error("ls.set_precision: 0=F32, 1=BF16, 2=FP8");
   c->prec = prec;
   c->ensure_packed(prec);
+  AOB_API_END
+}
+int aob_ls_set_tuning(aob_ls *c, int kind, int nblocks) {
+  AOB_API_BEGIN
+  NEED(c);
+  if (kind < 0 || kind > 2 || nblocks < 0) throw Error("ls.set_tuning: kind 0..2, nblocks >= 0");
+  c->mvm_kind = kind;
+  c->nblocks = nblocks;
+  AOB_API_END
+}
+int aob_ls_status(aob_ls *c, uint32_t *st, int reset) {
+  AOB_API_BEGIN
+  NEED(c); NEED(st);
+  AOB_CUDA(cudaSetDevice(c->device));
+  AOB_CUDA(cudaMemcpy(st, c->status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (reset) AOB_CUDA(cudaMemset(c->status.p, 0, sizeof(uint32_t)));
   AOB_API_END
 }
 int aob_ls_comp_com(aob_ls *c, void *stream) {

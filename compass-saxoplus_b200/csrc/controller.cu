@@ -41,6 +41,8 @@ struct MvmArgs {
   float gain;
   int integrate;
   uint32_t *bump;         // incremented once per launch when set (noise frame counter)
+  uint32_t *status;       // error word (bounded waits that expired)
+  int rows_per_cta;       // bulk kernel: rows staged per CTA (host-checked to fit)
 };
 
 // Dot product of one 16-byte packed chunk with its slopes.  The slopes are
@@ -156,6 +158,80 @@ __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_kernel(MvmArgs A) {
   }
 }
 
+// Bulk-copy MVM.  Each CTA owns rows [r0, r1) of the packed matrix; one
+// thread issues one TMA bulk copy per row into shared memory (each completing
+// on its own mbarrier) before anything else happens, so the whole matrix is in
+// flight from the first microsecond.  Warps then take rows as they land and
+// reduce them against the lane-swizzled slope vector.  Waits are bounded: an
+// expired wait sets ERR_MBAR_TIMEOUT in *status and the row is skipped.
+constexpr uint32_t MBAR_MAX_POLLS = 1u << 22;
+
+template <typename T>
+__global__ void __launch_bounds__(MVM_THREADS) ls_mvm_bulk_kernel(MvmArgs A) {
+  extern __shared__ __align__(128) unsigned char sm[];
+  constexpr int V = Pack<T>::N;
+  constexpr int Q = V / 4;
+  const int nchunk = A.ld / V;
+  const int nsh = mvm_smem_floats(A.ld, V);
+  const uint32_t row_bytes = (uint32_t)(A.ld * sizeof(T));
+  const int r0 = (int)(((int64_t)blockIdx.x * A.nrow) / gridDim.x);
+  const int r1 = (int)(((int64_t)(blockIdx.x + 1) * A.nrow) / gridDim.x);
+  const int R = r1 - r0;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sm);
+  float *s_sh = reinterpret_cast<float *>(sm + 128 * ((A.rows_per_cta * 8 + 127) / 128));
+  unsigned char *rows = reinterpret_cast<unsigned char *>(s_sh + nsh);
+  if (threadIdx.x == 0) {
+    for (int r = 0; r < R; ++r) mbar_init(&bars[r], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned char *src = static_cast<const unsigned char *>(A.mat) + (size_t)r0 * row_bytes;
+    for (int r = 0; r < R; ++r) {
+      mbar_expect_tx(&bars[r], row_bytes);
+      bulk_g2s(rows + (size_t)r * row_bytes, src + (size_t)r * row_bytes, row_bytes, &bars[r]);
+    }
+  }
+  if (A.bump && blockIdx.x == 0 && threadIdx.x == 0) *A.bump += 1u;
+  for (int i = threadIdx.x; i < nsh; i += blockDim.x) {
+    const int g = i >> 2, e = i & 3;
+    const int l = g & 31, jq = g >> 5;
+    const int j = jq / Q, q = jq - j * Q;
+    const int src = (l + 32 * j) * V + 4 * q + e;
+    s_sh[i] = (src < A.ncol) ? A.s[src] : 0.f;
+  }
+  __syncthreads();
+  const float4 *svl = reinterpret_cast<const float4 *>(s_sh) + (threadIdx.x & 31);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nw = blockDim.x >> 5;
+  for (int r = warp; r < R; r += nw) {
+    if (!mbar_wait(&bars[r], 0, MBAR_MAX_POLLS)) {
+      if (lane == 0 && A.status) atomicOr(A.status, (uint32_t)ERR_MBAR_TIMEOUT);
+      continue;
+    }
+    const uint4 *row = reinterpret_cast<const uint4 *>(rows + (size_t)r * row_bytes) + lane;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    int j = 0;
+    for (; 32 * (j + 3) + lane < nchunk; j += 4) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) acc[u] += Pack<T>::dot(row[32 * (j + u)], svl + 32 * Q * (j + u));
+    }
+    for (; 32 * j + lane < nchunk; ++j) acc[0] += Pack<T>::dot(row[32 * j], svl + 32 * Q * j);
+    float tot = warp_sum((acc[0] + acc[1]) + (acc[2] + acc[3]));
+    if (lane == 0) {
+      const int gr = r0 + r;
+      if (A.rscale) tot *= A.rscale[gr];
+      const float e = -tot;
+      A.err[gr] = e;
+      if (A.integrate) A.com[gr] = A.gain * (e * A.mgain[gr]) + A.com[gr];
+    }
+  }
+  // no CTA may exit with a copy still landing in its shared memory
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int r = 0; r < R; ++r) mbar_wait(&bars[r], 0, MBAR_MAX_POLLS);
+}
+
 struct VoltArgs {
   const float *com;
   float *oldest;       // ring[0]: read for latency, then overwritten with com
@@ -215,6 +291,7 @@ aob_ls::aob_ls(int device_, int nslope_, int nactu_, float delay_)
   AOB_CUDA(cudaSetDevice(device));
   set_delay(delay_);
   centroids.alloc(nslope);
+  status.alloc(1);
   err.alloc(nactu);
   com_clipped.alloc(nactu);
   gains.alloc(nactu);
@@ -283,28 +360,62 @@ void aob_ls::comp_com(cudaStream_t s, uint32_t *bump) {
   A.gain = gain;
   A.integrate = 1;
   A.bump = bump;
-  const int grid = nblocks > 0 ? std::min(nblocks, nactu) : std::min(nactu, num_sms(device));
+  A.status = status.p;
   if (prec == AOB_PREC_F32) {
     A.mat = cm_f32.p;
     A.ld = (nslope + 3) / 4 * 4;
-    const size_t sm = sizeof(float) * mvm_smem_floats(A.ld, 4);
-    AOB_CUDA(cudaFuncSetAttribute(ls_mvm_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    ls_mvm_kernel<float><<<grid, MVM_THREADS, sm, s>>>(A);
   } else if (prec == AOB_PREC_BF16) {
     A.mat = cm_bf16.p;
     A.ld = (nslope + 7) / 8 * 8;
-    const size_t sm = sizeof(float) * mvm_smem_floats(A.ld, 8);
-    AOB_CUDA(cudaFuncSetAttribute(ls_mvm_kernel<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    ls_mvm_kernel<__nv_bfloat16><<<grid, MVM_THREADS, sm, s>>>(A);
   } else {
     A.mat = cm_fp8.p;
     A.rscale = row_scale.p;
     A.ld = (nslope + 15) / 16 * 16;
-    const size_t sm = sizeof(float) * mvm_smem_floats(A.ld, 16);
-    AOB_CUDA(cudaFuncSetAttribute(ls_mvm_kernel<__nv_fp8_e4m3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    ls_mvm_kernel<__nv_fp8_e4m3><<<grid, MVM_THREADS, sm, s>>>(A);
   }
-  AOB_LAUNCH_CHECK("ls_mvm_kernel");
+  launch_mvm(A, s);
+}
+
+namespace {
+template <typename T>
+void launch_mvm_t(const MvmArgs &A0, int grid, bool bulk, cudaStream_t s) {
+  MvmArgs A = A0;
+  constexpr int V = Pack<T>::N;
+  const size_t slope_bytes = sizeof(float) * mvm_smem_floats(A.ld, V);
+  if (bulk) {
+    A.rows_per_cta = (A.nrow + grid - 1) / grid;
+    const size_t sm = 128 * ((A.rows_per_cta * 8 + 127) / 128) + slope_bytes + (size_t)A.rows_per_cta * A.ld * sizeof(T);
+    AOB_CUDA(cudaFuncSetAttribute(ls_mvm_bulk_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    ls_mvm_bulk_kernel<T><<<grid, MVM_THREADS, sm, s>>>(A);
+    AOB_LAUNCH_CHECK("ls_mvm_bulk_kernel");
+  } else {
+    AOB_CUDA(cudaFuncSetAttribute(ls_mvm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slope_bytes));
+    ls_mvm_kernel<T><<<grid, MVM_THREADS, slope_bytes, s>>>(A);
+    AOB_LAUNCH_CHECK("ls_mvm_kernel");
+  }
+}
+}  // namespace
+
+// Largest shared-memory budget a CTA may request on sm_100 (227 KB).
+constexpr size_t MVM_SMEM_MAX = 227 * 1024;
+
+// Kernel and grid for this matrix: the bulk-copy kernel when a CTA's rows fit in
+// shared memory with one CTA per SM, the register-streaming kernel otherwise
+// (or when the caller forces it).  ``nblocks`` > 0 overrides the grid size.
+void aob_ls::launch_mvm(MvmArgs &A, cudaStream_t s) {
+  const int nsm = num_sms(device);
+  int esize = prec == AOB_PREC_F32 ? 4 : (prec == AOB_PREC_BF16 ? 2 : 1);
+  int V = 16 / esize;
+  int grid = nblocks > 0 ? std::min(nblocks, nactu) : std::min(nactu, nsm);
+  const size_t slope_bytes = sizeof(float) * mvm_smem_floats(A.ld, V);
+  const int rpc = (nactu + grid - 1) / grid;
+  const size_t need = 128 * ((rpc * 8 + 127) / 128) + slope_bytes + (size_t)rpc * A.ld * esize;
+  const bool bulk = (mvm_kind == 0 || mvm_kind == 1) && need <= MVM_SMEM_MAX && mvm_kind != 2;
+  if (prec == AOB_PREC_F32)
+    launch_mvm_t<float>(A, grid, bulk, s);
+  else if (prec == AOB_PREC_BF16)
+    launch_mvm_t<__nv_bfloat16>(A, grid, bulk, s);
+  else
+    launch_mvm_t<__nv_fp8_e4m3>(A, grid, bulk, s);
 }
 
 void aob_ls::comp_voltage(cudaStream_t s) {

@@ -60,6 +60,8 @@ uint64_t aob_loop::key(bool noise) const {
   mix(&ls->volt_max, sizeof ls->volt_max);
   mix(&ls->prec, sizeof ls->prec);
   mix(&ls->nblocks, sizeof ls->nblocks);
+  mix(&ls->mvm_kind, sizeof ls->mvm_kind);
+  mix(&wfs->wps_override, sizeof wfs->wps_override);
   const void *pm[4] = {ls->cm_f32.p, ls->cm_bf16.p, ls->cm_fp8.p, centro->weights.p};
   mix(pm, sizeof pm);
   return h;

@@ -73,8 +73,38 @@ struct ShKernelArgs {
   float *c_intens;
 };
 
-template <int NFFT>
+// i / d for 0 <= i < 4096 and 0 < d < 256 with magic = ceil(2^20 / d)
+__device__ __forceinline__ int fdiv(int i, uint32_t magic) { return (int)(((uint32_t)i * magic) >> 20); }
+
+// Group of WPS warps working on one sub-aperture: named barrier per group
+// (barrier 0 is __syncthreads).
+template <int WPS>
+__device__ __forceinline__ void group_sync(int group) {
+  if (WPS == 1)
+    __syncwarp();
+  else
+    asm volatile("bar.sync %0, %1;" ::"r"(group + 1), "r"(WPS * 32) : "memory");
+}
+
+// Sum over the group; every thread of the group gets the result.
+template <int WPS>
+__device__ __forceinline__ float group_sum(float v, float *red, int gw, int lane, int group) {
+  v = warp_sum(v);
+  if (WPS == 1) return v;
+  if (lane == 0) red[gw] = v;
+  group_sync<WPS>(group);
+  float t = 0.f;
+#pragma unroll
+  for (int i = 0; i < WPS; ++i) t += red[i];
+  group_sync<WPS>(group);
+  return t;
+}
+
+template <int NFFT, int WPS>
 __global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P) {
+  constexpr int GT = WPS * 32;                // threads per sub-aperture
+  constexpr int GROUPS = SH_WARPS / WPS;      // sub-apertures per CTA
+  constexpr int PPT = (32 * SH_MAX_PPL) / GT; // binned pixels per thread
   extern __shared__ __align__(16) unsigned char smem[];
   float2 *tw = reinterpret_cast<float2 *>(smem);
   int32_t *ul = reinterpret_cast<int32_t *>(tw + NFFT);
@@ -83,40 +113,47 @@ __global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P)
   const int ncb = P.nrebin2 * P.npix * P.npix;
   const int pd2 = P.pdiam * P.pdiam;
   const size_t hdr = ((sizeof(float2) * NFFT + sizeof(int32_t) * (2 * NFFT + ncb)) + 15) & ~size_t(15);
-  const size_t per_warp = ((size_t)(pd2 + P.nu * P.pdiam) * sizeof(float2) + (size_t)P.nu * P.nv * sizeof(float) + 15) & ~size_t(15);
+  const size_t per_grp = ((size_t)(pd2 + P.nu * P.pdiam) * sizeof(float2) + (size_t)P.nu * P.nv * sizeof(float) +
+                          4 * WPS * sizeof(float) + 15) & ~size_t(15);
 
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int group = threadIdx.x / GT;
+  const int gt = threadIdx.x - group * GT;
+  const int lane = threadIdx.x & 31;
+  const int gw = gt >> 5;  // warp index inside the group
   for (int i = threadIdx.x; i < NFFT; i += blockDim.x) {
-    double s, c;
-    sincospi(2.0 * (double)i / (double)NFFT, &s, &c);
-    tw[i] = make_float2((float)c, (float)-s);  // exp(-2 pi i m / N): forward transform
+    double sn, cs;
+    sincospi(2.0 * (double)i / (double)NFFT, &sn, &cs);
+    tw[i] = make_float2((float)cs, (float)-sn);  // exp(-2 pi i m / N): forward transform
   }
   for (int i = threadIdx.x; i < P.nu; i += blockDim.x) ul[i] = P.ulist[i];
   for (int i = threadIdx.x; i < P.nv; i += blockDim.x) vl[i] = P.vlist[i];
   for (int i = threadIdx.x; i < ncb; i += blockDim.x) cb[i] = P.cbin[i];
   __syncthreads();
 
-  float2 *E = reinterpret_cast<float2 *>(smem + hdr + per_warp * warp);
+  float2 *E = reinterpret_cast<float2 *>(smem + hdr + per_grp * group);
   float2 *Gt = E + pd2;
   float *I = reinterpret_cast<float *>(Gt + P.nu * P.pdiam);
+  float *red = I + P.nu * P.nv;
   const int npix2 = P.npix * P.npix;
+  const uint32_t mg_pd = (1u << 20) / P.pdiam + 1, mg_nu = (1u << 20) / P.nu + 1,
+                 mg_np = (1u << 20) / P.npix + 1;
 
-  for (int k = blockIdx.x * SH_WARPS + warp; k < P.nvalid; k += gridDim.x * SH_WARPS) {
+  for (int k = blockIdx.x * GROUPS + group; k < P.nvalid; k += gridDim.x * GROUPS) {
     // 1. complex field of the sub-aperture: pupil * exp(i (phase*2pi/lambda - offset))
     const int px = P.puppixx[k], py = P.puppixy[k];
-    for (int i = lane; i < pd2; i += 32) {
-      const int x = i % P.pdiam, y = i / P.pdiam;
+    for (int i = gt; i < pd2; i += GT) {
+      const int y = fdiv(i, mg_pd), x = i - y * P.pdiam;
       const int id = (x + px) + (y + py) * P.npup;
       const float ph = P.phase[id] * P.scale - P.offsets[i];
-      float s, c;
-      sincosf(ph, &s, &c);
+      float sn, cs;
+      sincosf(ph, &sn, &cs);
       const float a = P.pupil[id];
-      E[i] = make_float2(c * a, s * a);
+      E[i] = make_float2(cs * a, sn * a);
     }
-    __syncwarp();
+    group_sync<WPS>(group);
     // 2. DFT along x at the needed kx: G[a, y] = sum_x E[x, y] W^(u_a x)
-    for (int i = lane; i < P.nu * P.pdiam; i += 32) {
-      const int a = i % P.nu, y = i / P.nu;
+    for (int i = gt; i < P.nu * P.pdiam; i += GT) {
+      const int y = fdiv(i, mg_nu), a = i - y * P.nu;
       const int ua = ul[a];
       const float2 *e = E + y * P.pdiam;
       float re = 0.f, im = 0.f;
@@ -129,10 +166,10 @@ __global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P)
       }
       Gt[i] = make_float2(re, im);
     }
-    __syncwarp();
+    group_sync<WPS>(group);
     // 3. DFT along y at the needed ky and |.|^2: I[a, b]
-    for (int i = lane; i < P.nu * P.nv; i += 32) {
-      const int a = i % P.nu, b = i / P.nu;
+    for (int i = gt; i < P.nu * P.nv; i += GT) {
+      const int b = fdiv(i, mg_nu), a = i - b * P.nu;
       const int vb = vl[b];
       float re = 0.f, im = 0.f;
       int m = 0;
@@ -144,13 +181,13 @@ __global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P)
       }
       I[i] = fmaf(re, re, im * im);
     }
-    __syncwarp();
+    group_sync<WPS>(group);
     // 4. binning and per-sub-aperture flux
-    float bv[SH_MAX_PPL];
+    float bv[PPT];
     float part = 0.f;
 #pragma unroll
-    for (int j = 0; j < SH_MAX_PPL; ++j) {
-      const int p = lane + 32 * j;
+    for (int j = 0; j < PPT; ++j) {
+      const int p = gt + GT * j;
       float v = 0.f;
       if (p < npix2) {
         const int32_t *c = cb + p * P.nrebin2;
@@ -159,16 +196,16 @@ __global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P)
       bv[j] = v;
       part += v;
     }
-    const float tot = warp_sum(part);
-    if (lane == 0) P.intensities[k] = tot;
+    const float tot = group_sum<WPS>(part, red, gw, lane, group);
+    if (gt == 0) P.intensities[k] = tot;
     const float fk = P.flux[k];
     const uint32_t frame = P.frame_ptr ? *P.frame_ptr : P.frame;
     // 5. normalise, noise, write cube + image, centroid partial sums
     const int vx = P.validsubsx[k], vy = P.validsubsy[k];
     float cs = 0.f, cx = 0.f, cy = 0.f;
 #pragma unroll
-    for (int j = 0; j < SH_MAX_PPL; ++j) {
-      const int p = lane + 32 * j;
+    for (int j = 0; j < PPT; ++j) {
+      const int p = gt + GT * j;
       if (p < npix2) {
         float v = bv[j];
         if (tot != 0.f) v = v * fk / tot * P.nphot;
@@ -176,7 +213,7 @@ __global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P)
         if (P.noise_mode >= 1) v = (float)poisson_sample((double)v, pix, frame, P.k0, P.k1);
         if (P.noise_mode >= 2) v = v + P.noise * (float)gauss_sample(pix, frame, P.k0, P.k1);
         P.bincube[pix] = v;
-        const int x = p % P.npix, y = p / P.npix;
+        const int y = fdiv(p, mg_np), x = p - y * P.npix;
         const int idim = (x + vx) + (y + vy) * P.img_size;
         float d = v;
         if (P.ckind == 1 || P.ckind == 2) d = (v > P.c_thresh) ? v - P.c_thresh : 1.e-6f;
@@ -190,10 +227,10 @@ __global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P)
       }
     }
     if (P.ckind >= 0) {
-      cs = warp_sum(cs);
-      cx = warp_sum(cx);
-      cy = warp_sum(cy);
-      if (lane == 0) {
+      cs = group_sum<WPS>(cs, red + WPS, gw, lane, group);
+      cx = group_sum<WPS>(cx, red + 2 * WPS, gw, lane, group);
+      cy = group_sum<WPS>(cy, red + 3 * WPS, gw, lane, group);
+      if (gt == 0) {
         const int ix = P.c_order ? 2 * k : k;
         const int iy = P.c_order ? 2 * k + 1 : k + P.nvalid;
         P.c_slopes[ix] = (cx / (cs + 1.e-6f) - P.c_offset) * P.c_scale - P.c_ref[ix];
@@ -201,7 +238,7 @@ __global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P)
         P.c_intens[k] = cs;
       }
     }
-    __syncwarp();
+    group_sync<WPS>(group);
   }
 }
 
@@ -227,6 +264,7 @@ aob_sh::aob_sh(int device_, int nxsub_, int nvalid_, int npix_, int nphase_, int
   AOB_REQUIRE(ntot == nfft, "sh: extended field of view (ntot != nfft) is not supported");
   AOB_REQUIRE(nphase <= nfft && nphase <= 32, "sh: nphase must be <= min(nfft, 32)");
   AOB_REQUIRE(npix * npix <= 32 * SH_MAX_PPL, "sh: npix^2 must be <= 256");
+  AOB_REQUIRE(nphase * nphase < 4096 && nfft * nfft <= 4096, "sh: sizes beyond the index arithmetic range");
   AOB_REQUIRE((int64_t)nxsub * npix < (1 << 15), "sh: image too large");
   AOB_CUDA(cudaSetDevice(device));
   phase.alloc((int64_t)npup * npup);
@@ -293,17 +331,45 @@ void aob_sh::load_arrays(const int32_t *h_binmap, const float *h_offsets, const 
   validsubsy.upload(h_vy, nvalid);
   istart.upload(h_istart, nvalid);
   jstart.upload(h_jstart, nvalid);
-  AOB_REQUIRE(smem_bytes() <= 200 * 1024, "sh: shared-memory footprint too large for this geometry");
+  AOB_REQUIRE(smem_bytes(1) <= 200 * 1024, "sh: shared-memory footprint too large for this geometry");
   loaded = true;
 }
 
-size_t aob_sh::smem_bytes() const {
+size_t aob_sh::smem_bytes(int wps) const {
   const int ncb = nrebin * nrebin * npix * npix;
   const size_t hdr = ((sizeof(float2) * nfft + sizeof(int32_t) * (2 * nfft + ncb)) + 15) & ~size_t(15);
-  const size_t per_warp =
-      ((size_t)(nphase * nphase + nu * nphase) * sizeof(float2) + (size_t)nu * nv * sizeof(float) + 15) &
-      ~size_t(15);
-  return hdr + SH_WARPS * per_warp;
+  const size_t per_grp = ((size_t)(nphase * nphase + nu * nphase) * sizeof(float2) + (size_t)nu * nv * sizeof(float) +
+                          4 * wps * sizeof(float) + 15) & ~size_t(15);
+  return hdr + (SH_WARPS / wps) * per_grp;
+}
+
+// Warps per sub-aperture: the autotuner's choice if set, otherwise enough to
+// give every SM at least ~24 resident warps.
+int aob_sh::pick_wps() const {
+  if (wps_override == 1 || wps_override == 2 || wps_override == 4) return wps_override;
+  const int nsm = num_sms(device);
+  if (nvalid >= 24 * nsm) return 1;
+  if (nvalid >= 12 * nsm) return 2;
+  return 4;
+}
+
+template <int NFFT, int WPS>
+static void launch_sh(const ShKernelArgs &P, int nvalid, size_t sm, int nsm, cudaStream_t s) {
+  constexpr int GROUPS = SH_WARPS / WPS;
+  int grid = (nvalid + GROUPS - 1) / GROUPS;
+  grid = std::max(1, std::min(grid, nsm * 32));
+  AOB_CUDA(cudaFuncSetAttribute(sh_image_kernel<NFFT, WPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  sh_image_kernel<NFFT, WPS><<<grid, SH_WARPS * 32, sm, s>>>(P);
+}
+
+template <int NFFT>
+static void launch_sh_n(int wps, const ShKernelArgs &P, int nvalid, size_t sm, int nsm, cudaStream_t s) {
+  if (wps == 1)
+    launch_sh<NFFT, 1>(P, nvalid, sm, nsm, s);
+  else if (wps == 2)
+    launch_sh<NFFT, 2>(P, nvalid, sm, nsm, s);
+  else
+    launch_sh<NFFT, 4>(P, nvalid, sm, nsm, s);
 }
 
 void aob_sh::comp_image(bool with_noise, cudaStream_t s) { comp_image_to(with_noise, s, nullptr, nullptr); }
@@ -361,23 +427,14 @@ void aob_sh::comp_image_to(bool with_noise, cudaStream_t s, float *slopes_dst, c
     c = nullptr;
   }
   const int nsm = num_sms(device);
-  int grid = (nvalid + SH_WARPS - 1) / SH_WARPS;
-  grid = std::max(1, std::min(grid, nsm * 16));
-  const size_t sm = smem_bytes();
-  switch (nfft) {
-    case 16:
-      AOB_CUDA(cudaFuncSetAttribute(sh_image_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      sh_image_kernel<16><<<grid, SH_WARPS * 32, sm, s>>>(P);
-      break;
-    case 32:
-      AOB_CUDA(cudaFuncSetAttribute(sh_image_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      sh_image_kernel<32><<<grid, SH_WARPS * 32, sm, s>>>(P);
-      break;
-    default:
-      AOB_CUDA(cudaFuncSetAttribute(sh_image_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      sh_image_kernel<64><<<grid, SH_WARPS * 32, sm, s>>>(P);
-      break;
-  }
+  const int wps = pick_wps();
+  const size_t sm = smem_bytes(wps);
+  if (nfft == 16)
+    launch_sh_n<16>(wps, P, nvalid, sm, nsm, s);
+  else if (nfft == 32)
+    launch_sh_n<32>(wps, P, nvalid, sm, nsm, s);
+  else
+    launch_sh_n<64>(wps, P, nvalid, sm, nsm, s);
   AOB_LAUNCH_CHECK("sh_image_kernel");
   if (P.noise_mode) ++frame;
   ++image_gen;

@@ -93,6 +93,9 @@ int aob_sh_buffer(aob_sh *h, const char *which, void **dev_ptr, int64_t *nelem);
 int aob_sh_comp_image(aob_sh *h, int noise, void *stream);
 /* SutraWfsSH::fill_binimage (sutra_wfs_sh.cpp:599-621): re-scatter bincube. */
 int aob_sh_fill_binimage(aob_sh *h, void *stream);
+/* Launch shape of the sensor kernel: warps per sub-aperture (1, 2 or 4;
+ * 0 = heuristic).  Set by the project's autotuner; results are unchanged. */
+int aob_sh_set_tuning(aob_sh *h, int warps_per_subap);
 /* set_bincube / set_binimg: overwrite from host. */
 int aob_sh_set_bincube(aob_sh *h, const float *host, int64_t n);
 int aob_sh_set_binimg(aob_sh *h, const float *host, int64_t n);
@@ -167,6 +170,12 @@ int aob_ls_set_centroids(aob_ls *c, const float *s, int n);
 /* Precision of the command-matrix MVM: F32 (reference), BF16, or FP8 E4M3
  * with one float32 scale per actuator row; accumulation is always float32. */
 int aob_ls_set_precision(aob_ls *c, int prec);
+/* MVM kernel choice: kind 0 = auto, 1 = bulk-copy (TMA) staging of the
+ * CTA's rows in shared memory, 2 = register streaming; nblocks = grid size
+ * (0 = one CTA per SM).  Set by the autotuner; results are unchanged. */
+int aob_ls_set_tuning(aob_ls *c, int kind, int nblocks);
+/* Error word of the MVM kernels (bit 0: a bounded wait expired); reset = clear it. */
+int aob_ls_status(aob_ls *c, uint32_t *status, int reset);
 /* comp_com (sutra_controller_ls.cpp:251-285): err = -cmat.s,
  * com += gain * err * modal_gains, one kernel. */
 int aob_ls_comp_com(aob_ls *c, void *stream);

@@ -230,3 +230,36 @@ def test_loop_matches_separate_calls(core, graph, delay):
         np.testing.assert_array_equal(np.array(l2.buffer("centroids")), np.array(l1.buffer("centroids")))
         np.testing.assert_array_equal(v2, v1)
     assert w1.frame == w2.frame == len(screens)
+
+
+@pytest.mark.parametrize("wps", [1, 2, 4])
+def test_sh_launch_shapes_agree(core, wps):
+    """Every autotuner launch shape of the sensor kernel gives the oracle's image."""
+    g, w, phase = _setup(core, "sh40")
+    w.set_tuning(wps)
+    w.comp_image(noise=False)
+    cube = np.array(w.d_bincube).reshape(g.npix * g.npix, g.nvalid, order="F")
+    ocube, _, _ = osh.comp_image(phase, g.tel.mpupil, g, 2 * np.pi / g.wavelength_um, g.nphotons)
+    assert rel_rms(cube, ocube) < 1e-5
+
+
+@pytest.mark.parametrize("prec", ["f32", "bf16", "fp8"])
+def test_mvm_kernels_agree_and_status_clean(core, prec):
+    rng = np.random.default_rng(8)
+    nslope, nactu = 4016, 1600
+    cmat = (rng.standard_normal((nactu, nslope)) * 0.01).astype(np.float32)
+    s = rng.standard_normal(nslope).astype(np.float32)
+    out = {}
+    for kind, nb in ((1, 0), (2, 0), (1, 300), (2, 37)):
+        c = core.LsController(nslope, nactu)
+        c.set_precision(prec)
+        c.set_cmat(cmat)
+        c.set_gain(1.0)
+        c.set_centroids(s)
+        c.set_tuning(kind, nb)
+        c.comp_com()
+        out[(kind, nb)] = np.array(c.buffer("err"))
+        assert c.status() == 0
+    base = out[(2, 0)]
+    for k, v in out.items():
+        assert rel_rms(v, base) < 1e-6, k
