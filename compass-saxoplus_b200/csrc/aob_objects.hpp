@@ -42,6 +42,7 @@ struct aob_sh {
   aob::DevBuf<int32_t> ulist, vlist, cbin;
   // outputs
   aob::DevBuf<float> bincube, binimg, intensities, slopes;
+  aob::DevBuf<double> logfact, rk;  // noise-sampler tables
   // centroider whose slopes are fused into comp_image (may be null)
   aob_centro *fused = nullptr;
   uint64_t image_gen = 0;  // bumped whenever binimg changes

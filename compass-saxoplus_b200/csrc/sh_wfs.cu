@@ -62,6 +62,7 @@ struct ShKernelArgs {
   float noise;
   uint32_t frame, k0, k1;
   const uint32_t *frame_ptr;  // when set, the frame number is read from device memory
+  NoiseTables tables;
   // fused centroider (kind < 0: none)
   int ckind;
   float c_scale, c_offset, c_thresh;
@@ -100,8 +101,10 @@ __device__ __forceinline__ float group_sum(float v, float *red, int gw, int lane
   return t;
 }
 
-template <int NFFT, int WPS>
-__global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P) {
+// PD > 0: phase-grid side known at compile time (the DFT loops unroll and all
+// their shared-memory loads issue back to back); PD == 0: runtime side.
+template <int NFFT, int WPS, int PD>
+__global__ void __launch_bounds__(SH_WARPS * 32, 6) sh_image_kernel(ShKernelArgs P) {
   constexpr int GT = WPS * 32;                // threads per sub-aperture
   constexpr int GROUPS = SH_WARPS / WPS;      // sub-apertures per CTA
   constexpr int PPT = (32 * SH_MAX_PPL) / GT; // binned pixels per thread
@@ -111,9 +114,10 @@ __global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P)
   int32_t *vl = ul + NFFT;
   int32_t *cb = vl + NFFT;
   const int ncb = P.nrebin2 * P.npix * P.npix;
-  const int pd2 = P.pdiam * P.pdiam;
+  const int pd = PD > 0 ? PD : P.pdiam;
+  const int pd2 = pd * pd;
   const size_t hdr = ((sizeof(float2) * NFFT + sizeof(int32_t) * (2 * NFFT + ncb)) + 15) & ~size_t(15);
-  const size_t per_grp = ((size_t)(pd2 + P.nu * P.pdiam) * sizeof(float2) + (size_t)P.nu * P.nv * sizeof(float) +
+  const size_t per_grp = ((size_t)(pd2 + P.nu * pd) * sizeof(float2) + (size_t)P.nu * P.nv * sizeof(float) +
                           4 * WPS * sizeof(float) + 15) & ~size_t(15);
 
   const int group = threadIdx.x / GT;
@@ -132,17 +136,17 @@ __global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P)
 
   float2 *E = reinterpret_cast<float2 *>(smem + hdr + per_grp * group);
   float2 *Gt = E + pd2;
-  float *I = reinterpret_cast<float *>(Gt + P.nu * P.pdiam);
+  float *I = reinterpret_cast<float *>(Gt + P.nu * pd);
   float *red = I + P.nu * P.nv;
   const int npix2 = P.npix * P.npix;
-  const uint32_t mg_pd = (1u << 20) / P.pdiam + 1, mg_nu = (1u << 20) / P.nu + 1,
+  const uint32_t mg_pd = (1u << 20) / pd + 1, mg_nu = (1u << 20) / P.nu + 1,
                  mg_np = (1u << 20) / P.npix + 1;
 
   for (int k = blockIdx.x * GROUPS + group; k < P.nvalid; k += gridDim.x * GROUPS) {
     // 1. complex field of the sub-aperture: pupil * exp(i (phase*2pi/lambda - offset))
     const int px = P.puppixx[k], py = P.puppixy[k];
     for (int i = gt; i < pd2; i += GT) {
-      const int y = fdiv(i, mg_pd), x = i - y * P.pdiam;
+      const int y = fdiv(i, mg_pd), x = i - y * pd;
       const int id = (x + px) + (y + py) * P.npup;
       const float ph = P.phase[id] * P.scale - P.offsets[i];
       float sn, cs;
@@ -152,17 +156,17 @@ __global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P)
     }
     group_sync<WPS>(group);
     // 2. DFT along x at the needed kx: G[a, y] = sum_x E[x, y] W^(u_a x)
-    for (int i = gt; i < P.nu * P.pdiam; i += GT) {
+    for (int i = gt; i < P.nu * pd; i += GT) {
       const int y = fdiv(i, mg_nu), a = i - y * P.nu;
       const int ua = ul[a];
-      const float2 *e = E + y * P.pdiam;
+      const float2 *e = E + y * pd;
       float re = 0.f, im = 0.f;
-      int m = 0;
-      for (int x = 0; x < P.pdiam; ++x) {
-        const float2 w = tw[m], v = e[x];
+#pragma unroll
+      for (int x = 0; x < (PD > 0 ? PD : 32); ++x) {
+        if (PD == 0 && x >= pd) break;
+        const float2 w = tw[(ua * x) & (NFFT - 1)], v = e[x];
         re = fmaf(v.x, w.x, fmaf(-v.y, w.y, re));
         im = fmaf(v.x, w.y, fmaf(v.y, w.x, im));
-        m = (m + ua) & (NFFT - 1);
       }
       Gt[i] = make_float2(re, im);
     }
@@ -172,12 +176,12 @@ __global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P)
       const int b = fdiv(i, mg_nu), a = i - b * P.nu;
       const int vb = vl[b];
       float re = 0.f, im = 0.f;
-      int m = 0;
-      for (int y = 0; y < P.pdiam; ++y) {
-        const float2 w = tw[m], v = Gt[a + y * P.nu];
+#pragma unroll
+      for (int y = 0; y < (PD > 0 ? PD : 32); ++y) {
+        if (PD == 0 && y >= pd) break;
+        const float2 w = tw[(vb * y) & (NFFT - 1)], v = Gt[a + y * P.nu];
         re = fmaf(v.x, w.x, fmaf(-v.y, w.y, re));
         im = fmaf(v.x, w.y, fmaf(v.y, w.x, im));
-        m = (m + vb) & (NFFT - 1);
       }
       I[i] = fmaf(re, re, im * im);
     }
@@ -210,8 +214,8 @@ __global__ void __launch_bounds__(SH_WARPS * 32) sh_image_kernel(ShKernelArgs P)
         float v = bv[j];
         if (tot != 0.f) v = v * fk / tot * P.nphot;
         const uint32_t pix = (uint32_t)(p + k * npix2);
-        if (P.noise_mode >= 1) v = (float)poisson_sample((double)v, pix, frame, P.k0, P.k1);
-        if (P.noise_mode >= 2) v = v + P.noise * (float)gauss_sample(pix, frame, P.k0, P.k1);
+        if (P.noise_mode >= 1) v = (float)poisson_sample((double)v, pix, frame, P.k0, P.k1, P.tables);
+        if (P.noise_mode >= 2) v = v + P.noise * gauss_sample(pix, frame, P.k0, P.k1);
         P.bincube[pix] = v;
         const int y = fdiv(p, mg_np), x = p - y * P.npix;
         const int idim = (x + vx) + (y + vy) * P.img_size;
@@ -280,6 +284,14 @@ aob_sh::aob_sh(int device_, int nxsub_, int nvalid_, int npix_, int nphase_, int
   binimg.alloc((int64_t)npix * nxsub * npix * nxsub);
   intensities.alloc(nvalid);
   slopes.alloc(2 * (int64_t)nvalid);
+  // noise tables: log(k!) as cumulative sums of log(i), and 1/k (same as the CPU oracle)
+  std::vector<double> lf(AOB_LOGFACT_N, 0.0), rkh(AOB_RK_N, 0.0);
+  for (int k = 1; k < AOB_LOGFACT_N; ++k) lf[k] = lf[k - 1] + std::log((double)k);
+  for (int k = 1; k < AOB_RK_N; ++k) rkh[k] = 1.0 / (double)k;
+  logfact.alloc(AOB_LOGFACT_N);
+  logfact.upload(lf.data(), AOB_LOGFACT_N);
+  rk.alloc(AOB_RK_N);
+  rk.upload(rkh.data(), AOB_RK_N);
 }
 
 void aob_sh::load_arrays(const int32_t *h_binmap, const float *h_offsets, const float *h_flux,
@@ -353,23 +365,39 @@ int aob_sh::pick_wps() const {
   return 4;
 }
 
-template <int NFFT, int WPS>
+template <int NFFT, int WPS, int PD>
 static void launch_sh(const ShKernelArgs &P, int nvalid, size_t sm, int nsm, cudaStream_t s) {
   constexpr int GROUPS = SH_WARPS / WPS;
   int grid = (nvalid + GROUPS - 1) / GROUPS;
   grid = std::max(1, std::min(grid, nsm * 32));
-  AOB_CUDA(cudaFuncSetAttribute(sh_image_kernel<NFFT, WPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  sh_image_kernel<NFFT, WPS><<<grid, SH_WARPS * 32, sm, s>>>(P);
+  // the attribute is set once per instantiation (a driver call per launch costs microseconds)
+  static size_t configured = 0;
+  if (sm > configured) {
+    AOB_CUDA(cudaFuncSetAttribute(sh_image_kernel<NFFT, WPS, PD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)std::max<size_t>(sm, 48 * 1024)));
+    configured = std::max<size_t>(sm, 48 * 1024);
+  }
+  sh_image_kernel<NFFT, WPS, PD><<<grid, SH_WARPS * 32, sm, s>>>(P);
+}
+
+template <int NFFT, int WPS>
+static void launch_sh_pd(int pd, const ShKernelArgs &P, int nvalid, size_t sm, int nsm, cudaStream_t s) {
+  switch (pd) {
+    case 4: launch_sh<NFFT, WPS, 4>(P, nvalid, sm, nsm, s); break;
+    case 6: launch_sh<NFFT, WPS, 6>(P, nvalid, sm, nsm, s); break;
+    case 8: launch_sh<NFFT, WPS, 8>(P, nvalid, sm, nsm, s); break;
+    default: launch_sh<NFFT, WPS, 0>(P, nvalid, sm, nsm, s); break;
+  }
 }
 
 template <int NFFT>
 static void launch_sh_n(int wps, const ShKernelArgs &P, int nvalid, size_t sm, int nsm, cudaStream_t s) {
   if (wps == 1)
-    launch_sh<NFFT, 1>(P, nvalid, sm, nsm, s);
+    launch_sh_pd<NFFT, 1>(P.pdiam, P, nvalid, sm, nsm, s);
   else if (wps == 2)
-    launch_sh<NFFT, 2>(P, nvalid, sm, nsm, s);
+    launch_sh_pd<NFFT, 2>(P.pdiam, P, nvalid, sm, nsm, s);
   else
-    launch_sh<NFFT, 4>(P, nvalid, sm, nsm, s);
+    launch_sh_pd<NFFT, 4>(P.pdiam, P, nvalid, sm, nsm, s);
 }
 
 void aob_sh::comp_image(bool with_noise, cudaStream_t s) { comp_image_to(with_noise, s, nullptr, nullptr); }
@@ -409,6 +437,7 @@ void aob_sh::comp_image_to(bool with_noise, cudaStream_t s, float *slopes_dst, c
   P.k0 = (uint32_t)((uint64_t)seed & 0xffffffffu);
   P.k1 = (uint32_t)((uint64_t)seed >> 32);
   P.frame_ptr = frame_ptr;
+  P.tables = NoiseTables{logfact.p, rk.p};
   P.ckind = -1;
   aob_centro *c = fused;
   if (c && c->npix == npix && c->nvalid == nvalid && c->type <= 2 && c->validx.n == nvalid) {

@@ -15,10 +15,12 @@ Stream tags: 0 = photon (Poisson) noise, 1 = readout (Gaussian) noise.
 
 Poisson sampling (replaces curand_poisson, carma_rng.cu:135-141):
   lambda < 10: sequential-search inversion (Devroye 1986, ch. X.3) on one
-               uniform, in float64 with no fused multiply-add;
+               uniform, in float64 with no fused multiply-add (1/k from a table);
   lambda >= 10: PTRS transformed rejection (Hoermann 1993, "The transformed
-               rejection method for generating Poisson random variables").
-Gaussian: Box-Muller on one block (u1 from words 0-1, u2 from words 2-3).
+               rejection method for generating Poisson random variables") with
+               its acceptance test in product form and log(k!) from a table of
+               cumulative log sums (two-term Stirling series beyond 4095).
+Gaussian: Box-Muller in float32 on one block (u1 from word 0, u2 from word 2).
 """
 
 import math
@@ -67,25 +69,55 @@ def u01(x):
     return (np.asarray(x, dtype=np.float64) + 0.5) * (1.0 / 4294967296.0)
 
 
+LOGFACT_N = 4096
+RK_N = 1024
+
+
+def _tables():
+    """log(k!) by cumulative sums of log(i) and 1/k -- the same tables the device uses."""
+    lf = [0.0] * LOGFACT_N
+    for k in range(1, LOGFACT_N):
+        lf[k] = lf[k - 1] + math.log(k)
+    rk = [0.0] + [1.0 / k for k in range(1, RK_N)]
+    return lf, rk
+
+
+LOGFACT, RK = _tables()
+
+
+def log_factorial(k):
+    if k < LOGFACT_N:
+        return LOGFACT[int(k)]
+    x = k + 1.0
+    ix = 1.0 / x
+    r = (x + -0.5) * math.log(x)
+    r = (r + -x) + 0.91893853320467274178
+    c = 0.08333333333333333 * ix + -((0.002777777777777778 * ix) * (ix * ix))
+    return r + c
+
+
 def _ptrs(lam, words_of_draw):
+    """PTRS transformed rejection with the acceptance test in product form."""
     slam = math.sqrt(lam)
     loglam = math.log(lam)
     b = 0.931 + 2.53 * slam
     a = -0.059 + 0.02483 * b
-    invalpha = 1.1239 + 1.1328 / (b - 3.4)
-    vr = 0.9277 - 3.6224 / (b - 2.0)
+    invalpha = 1.1239 + 1.1328 / (b + -3.4)
+    vr = 0.9277 + -(3.6224 / (b + -2.0))
+    a2 = 2.0 * a
     for d in range(POISSON_MAX_DRAWS):
         w = words_of_draw(d)
-        u = float(u01(w[0])) - 0.5
+        u = float(u01(w[0])) + -0.5
         v = float(u01(w[1]))
-        us = 0.5 - abs(u)
-        k = math.floor((2.0 * a / us + b) * u + lam + 0.43)
+        us = 0.5 + -abs(u)
+        k = math.floor((((a2 / us) + b) * u + lam) + 0.43)
         if us >= 0.07 and v <= vr:
             return k
         if k < 0 or (us < 0.013 and v > us):
             continue
-        if (math.log(v) + math.log(invalpha) - math.log(a / (us * us) + b)
-                <= -lam + k * loglam - math.lgamma(k + 1.0)):
+        lhs = (v * invalpha) / ((a / (us * us)) + b)
+        rhs = math.exp(((k * loglam) + -lam) + -log_factorial(k))
+        if lhs <= rhs:
             return k
     return math.floor(lam + 0.5)
 
@@ -94,9 +126,9 @@ def _inversion(lam, u):
     p = math.exp(-lam)
     f = p
     k = 0
-    while u > f and k < 1000:
+    while u > f and k < RK_N - 1:
         k += 1
-        p = p * (lam / k)
+        p = p * (lam * RK[k])
         f = f + p
     return k
 
@@ -131,10 +163,10 @@ def poisson(lam, index, frame, seed):
 
 
 def gaussian(index, frame, seed):
-    """Standard normal deviates (float64) for pixel indices ``index``."""
+    """Standard normal deviates (float32 Box-Muller, 24-bit uniforms) for pixel indices."""
     index = np.asarray(index, dtype=np.uint64)
     k0, k1 = key_of(seed)
     w = philox4x32(index, frame, TAG_GAUSS, 0, k0, k1)
-    u1 = u01(w[0])
-    u2 = u01(w[2])
-    return np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2)
+    u1 = ((w[0] >> np.uint32(8)).astype(np.float32) + np.float32(0.5)) * np.float32(5.9604644775390625e-08)
+    u2 = ((w[2] >> np.uint32(8)).astype(np.float32) + np.float32(0.5)) * np.float32(5.9604644775390625e-08)
+    return np.sqrt(np.float32(-2.0) * np.log(u1)) * np.cos(np.float32(2.0 * np.pi) * u2.astype(np.float64)).astype(np.float32)
