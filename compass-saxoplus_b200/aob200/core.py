@@ -369,6 +369,10 @@ class Loop:
     def use_graph(self, on=True):
         call("aob_loop_use_graph", self.h, 1 if on else 0)
 
+    def set_mode(self, mode=0, fused_wps=1):
+        """0: fused cooperative kernel when it fits, 1: three kernels, 2: fused only."""
+        call("aob_loop_set_mode", self.h, int(mode), int(fused_wps))
+
     def kernels_per_step(self) -> int:
         n = ctypes.c_int()
         call("aob_loop_kernels_per_step", self.h, ctypes.addressof(n))

@@ -18,6 +18,7 @@
 struct aob_centro;
 namespace aob {
 struct MvmArgs;
+struct ShKernelArgs;
 }
 
 // ---------------------------------------------------------------------------
@@ -43,6 +44,7 @@ struct aob_sh {
   // outputs
   aob::DevBuf<float> bincube, binimg, intensities, slopes;
   aob::DevBuf<double> logfact, rk;  // noise-sampler tables
+  aob::DevBuf<float> twiddle;       // exp(-2 pi i m / nfft) as (re, im) pairs
   // centroider whose slopes are fused into comp_image (may be null)
   aob_centro *fused = nullptr;
   uint64_t image_gen = 0;  // bumped whenever binimg changes
@@ -57,6 +59,9 @@ struct aob_sh {
   // buffer; frame_ptr: read the noise frame number from device memory
   void comp_image_to(bool noise, cudaStream_t s, float *slopes_dst, const uint32_t *frame_ptr);
   void fill_binimage(cudaStream_t s);
+  // kernel arguments for one image; returns the fused centroider (or null)
+  aob_centro *make_args(bool noise, float *slopes_dst, const uint32_t *frame_ptr, aob::ShKernelArgs &P);
+  void after_image(const aob::ShKernelArgs &P, aob_centro *c, bool staged);
   int wps_override = 0;  // warps per sub-aperture chosen by the autotuner (0 = heuristic)
   size_t smem_bytes(int wps) const;
   int pick_wps() const;
@@ -149,10 +154,15 @@ struct aob_loop {
   std::vector<uint64_t> graph_key;       // parameter snapshot each graph was built for
   std::vector<const void *> graph_front; // ring front buffer each graph was built for
   uint64_t frame_mirror = ~0ull;         // value held by d_frame
+  aob::DevBuf<uint32_t> gbar;            // grid barrier state of the fused kernel
+  int mode = 0;                          // 0 auto (fused when it fits), 1 three kernels, 2 fused only
+  int fused_wps = 1;                     // warps per sub-aperture in the fused kernel
+  int last_kernels = 3;                  // kernels launched by the last device step
   uint32_t frame_host = 0;
   aob_loop(aob_sh *w, aob_centro *c, aob_ls *l);
   ~aob_loop();
   void device_step(bool noise, cudaStream_t s, bool frame_on_device);
+  bool launch_fused(bool noise, cudaStream_t s, bool frame_on_device, bool dry);
   void step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s);
   uint64_t key(bool noise) const;
   void drop_graphs();

@@ -26,6 +26,7 @@ aob_loop::aob_loop(aob_sh *w, aob_centro *c, aob_ls *l) : wfs(w), centro(c), ls(
   AOB_REQUIRE(c->nvalid == w->nvalid, "loop: centroider nvalid differs from the sensor's");
   AOB_CUDA(cudaSetDevice(w->device));
   d_frame.alloc(1);
+  gbar.alloc(2);
   if (c->wfs && c->wfs->fused == c && c->wfs != w) c->wfs->fused = nullptr;
   c->wfs = w;
   w->fused = c;
@@ -62,12 +63,27 @@ uint64_t aob_loop::key(bool noise) const {
   mix(&ls->nblocks, sizeof ls->nblocks);
   mix(&ls->mvm_kind, sizeof ls->mvm_kind);
   mix(&wfs->wps_override, sizeof wfs->wps_override);
+  mix(&mode, sizeof mode);
+  mix(&fused_wps, sizeof fused_wps);
   const void *pm[4] = {ls->cm_f32.p, ls->cm_bf16.p, ls->cm_fp8.p, centro->weights.p};
   mix(pm, sizeof pm);
   return h;
 }
 
 void aob_loop::device_step(bool noise, cudaStream_t s, bool frame_on_device) {
+  if (mode != 1) {
+    // barrier state is re-armed before every fused launch (a timed-out launch
+    // can leave the arrival count non-zero)
+    if (launch_fused(noise, s, frame_on_device, true)) {
+      AOB_CUDA(cudaMemsetAsync(gbar.p, 0, 2 * sizeof(uint32_t), s));
+      if (launch_fused(noise, s, frame_on_device, false)) {
+        last_kernels = 1;
+        return;
+      }
+    }
+    AOB_REQUIRE(mode != 2, "loop: the fused kernel does not fit this configuration");
+  }
+  last_kernels = 3;
   const bool noisy = noise && wfs->noise > -1.f;
   wfs->comp_image_to(noise, s, ls->centroids.p, frame_on_device ? d_frame.p : nullptr);
   ls->comp_com(s, (frame_on_device && noisy) ? d_frame.p : nullptr);
@@ -208,7 +224,17 @@ int aob_loop_kernels_per_step(aob_loop *l, int *n) {
     set_last_error("aob_loop_kernels_per_step: null pointer");
     return AOB_ERR;
   }
-  *n = 3;
+  *n = l->last_kernels;
+  return AOB_OK;
+}
+
+int aob_loop_set_mode(aob_loop *l, int mode, int fused_wps) {
+  if (!l || mode < 0 || mode > 2 || (fused_wps != 0 && fused_wps != 1 && fused_wps != 2 && fused_wps != 4)) {
+    set_last_error("aob_loop_set_mode: mode 0..2, fused_wps 0/1/2/4");
+    return AOB_ERR;
+  }
+  l->mode = mode;
+  l->fused_wps = fused_wps > 0 ? fused_wps : 1;
   return AOB_OK;
 }
 

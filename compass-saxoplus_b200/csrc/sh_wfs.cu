@@ -31,219 +31,28 @@
 #include <vector>
 
 #include "aob_objects.hpp"
+#include "sh_core.cuh"
 
 namespace aob {
 
-constexpr int SH_WARPS = 4;      // sub-apertures per CTA
-constexpr int SH_MAX_PPL = 8;    // binned pixels per lane -> npix^2 <= 256
-
-struct ShKernelArgs {
-  const float *phase;
-  const float *pupil;
-  int npup;
-  const int32_t *puppixx;
-  const int32_t *puppixy;
-  const float *offsets;
-  float scale;
-  int pdiam, nvalid, npix, nrebin2;
-  int nu, nv;
-  const int32_t *ulist;
-  const int32_t *vlist;
-  const int32_t *cbin;  // [nrebin2, npix^2] indexes into the nu x nv intensity tile
-  const float *flux;
-  float nphot;
-  float *bincube;
-  float *binimg;
-  int img_size;
-  const int32_t *validsubsx;
-  const int32_t *validsubsy;
-  float *intensities;
-  int noise_mode;  // 0 none, 1 photon, 2 photon + readout
-  float noise;
-  uint32_t frame, k0, k1;
-  const uint32_t *frame_ptr;  // when set, the frame number is read from device memory
-  NoiseTables tables;
-  // fused centroider (kind < 0: none)
-  int ckind;
-  float c_scale, c_offset, c_thresh;
-  const float *c_ref;
-  const float *c_weights;
-  int c_wper;
-  int c_order;
-  float *c_slopes;
-  float *c_intens;
-};
-
-// i / d for 0 <= i < 4096 and 0 < d < 256 with magic = ceil(2^20 / d)
-__device__ __forceinline__ int fdiv(int i, uint32_t magic) { return (int)(((uint32_t)i * magic) >> 20); }
-
-// Group of WPS warps working on one sub-aperture: named barrier per group
-// (barrier 0 is __syncthreads).
-template <int WPS>
-__device__ __forceinline__ void group_sync(int group) {
-  if (WPS == 1)
-    __syncwarp();
-  else
-    asm volatile("bar.sync %0, %1;" ::"r"(group + 1), "r"(WPS * 32) : "memory");
-}
-
-// Sum over the group; every thread of the group gets the result.
-template <int WPS>
-__device__ __forceinline__ float group_sum(float v, float *red, int gw, int lane, int group) {
-  v = warp_sum(v);
-  if (WPS == 1) return v;
-  if (lane == 0) red[gw] = v;
-  group_sync<WPS>(group);
-  float t = 0.f;
-#pragma unroll
-  for (int i = 0; i < WPS; ++i) t += red[i];
-  group_sync<WPS>(group);
-  return t;
-}
+constexpr int SH_WARPS = 4;  // warps per CTA of the standalone sensor kernel
 
 // PD > 0: phase-grid side known at compile time (the DFT loops unroll and all
 // their shared-memory loads issue back to back); PD == 0: runtime side.
 template <int NFFT, int WPS, int PD>
 __global__ void __launch_bounds__(SH_WARPS * 32, 6) sh_image_kernel(ShKernelArgs P) {
-  constexpr int GT = WPS * 32;                // threads per sub-aperture
-  constexpr int GROUPS = SH_WARPS / WPS;      // sub-apertures per CTA
-  constexpr int PPT = (32 * SH_MAX_PPL) / GT; // binned pixels per thread
+  constexpr int GT = WPS * 32;
+  constexpr int GROUPS = SH_WARPS / WPS;
   extern __shared__ __align__(16) unsigned char smem[];
-  float2 *tw = reinterpret_cast<float2 *>(smem);
-  int32_t *ul = reinterpret_cast<int32_t *>(tw + NFFT);
-  int32_t *vl = ul + NFFT;
-  int32_t *cb = vl + NFFT;
-  const int ncb = P.nrebin2 * P.npix * P.npix;
   const int pd = PD > 0 ? PD : P.pdiam;
-  const int pd2 = pd * pd;
-  const size_t hdr = ((sizeof(float2) * NFFT + sizeof(int32_t) * (2 * NFFT + ncb)) + 15) & ~size_t(15);
-  const size_t per_grp = ((size_t)(pd2 + P.nu * pd) * sizeof(float2) + (size_t)P.nu * P.nv * sizeof(float) +
-                          4 * WPS * sizeof(float) + 15) & ~size_t(15);
-
+  const ShSmem L(NFFT, P.nu, P.nv, pd, P.nrebin2 * P.npix * P.npix, P.npix * P.npix, WPS);
+  sh_load_tables<NFFT>(P, smem, threadIdx.x, blockDim.x);
+  __syncthreads();
   const int group = threadIdx.x / GT;
   const int gt = threadIdx.x - group * GT;
-  const int lane = threadIdx.x & 31;
-  const int gw = gt >> 5;  // warp index inside the group
-  for (int i = threadIdx.x; i < NFFT; i += blockDim.x) {
-    double sn, cs;
-    sincospi(2.0 * (double)i / (double)NFFT, &sn, &cs);
-    tw[i] = make_float2((float)cs, (float)-sn);  // exp(-2 pi i m / N): forward transform
-  }
-  for (int i = threadIdx.x; i < P.nu; i += blockDim.x) ul[i] = P.ulist[i];
-  for (int i = threadIdx.x; i < P.nv; i += blockDim.x) vl[i] = P.vlist[i];
-  for (int i = threadIdx.x; i < ncb; i += blockDim.x) cb[i] = P.cbin[i];
-  __syncthreads();
-
-  float2 *E = reinterpret_cast<float2 *>(smem + hdr + per_grp * group);
-  float2 *Gt = E + pd2;
-  float *I = reinterpret_cast<float *>(Gt + P.nu * pd);
-  float *red = I + P.nu * P.nv;
-  const int npix2 = P.npix * P.npix;
-  const uint32_t mg_pd = (1u << 20) / pd + 1, mg_nu = (1u << 20) / P.nu + 1,
-                 mg_np = (1u << 20) / P.npix + 1;
-
-  for (int k = blockIdx.x * GROUPS + group; k < P.nvalid; k += gridDim.x * GROUPS) {
-    // 1. complex field of the sub-aperture: pupil * exp(i (phase*2pi/lambda - offset))
-    const int px = P.puppixx[k], py = P.puppixy[k];
-    for (int i = gt; i < pd2; i += GT) {
-      const int y = fdiv(i, mg_pd), x = i - y * pd;
-      const int id = (x + px) + (y + py) * P.npup;
-      const float ph = P.phase[id] * P.scale - P.offsets[i];
-      float sn, cs;
-      sincosf(ph, &sn, &cs);
-      const float a = P.pupil[id];
-      E[i] = make_float2(cs * a, sn * a);
-    }
-    group_sync<WPS>(group);
-    // 2. DFT along x at the needed kx: G[a, y] = sum_x E[x, y] W^(u_a x)
-    for (int i = gt; i < P.nu * pd; i += GT) {
-      const int y = fdiv(i, mg_nu), a = i - y * P.nu;
-      const int ua = ul[a];
-      const float2 *e = E + y * pd;
-      float re = 0.f, im = 0.f;
-#pragma unroll
-      for (int x = 0; x < (PD > 0 ? PD : 32); ++x) {
-        if (PD == 0 && x >= pd) break;
-        const float2 w = tw[(ua * x) & (NFFT - 1)], v = e[x];
-        re = fmaf(v.x, w.x, fmaf(-v.y, w.y, re));
-        im = fmaf(v.x, w.y, fmaf(v.y, w.x, im));
-      }
-      Gt[i] = make_float2(re, im);
-    }
-    group_sync<WPS>(group);
-    // 3. DFT along y at the needed ky and |.|^2: I[a, b]
-    for (int i = gt; i < P.nu * P.nv; i += GT) {
-      const int b = fdiv(i, mg_nu), a = i - b * P.nu;
-      const int vb = vl[b];
-      float re = 0.f, im = 0.f;
-#pragma unroll
-      for (int y = 0; y < (PD > 0 ? PD : 32); ++y) {
-        if (PD == 0 && y >= pd) break;
-        const float2 w = tw[(vb * y) & (NFFT - 1)], v = Gt[a + y * P.nu];
-        re = fmaf(v.x, w.x, fmaf(-v.y, w.y, re));
-        im = fmaf(v.x, w.y, fmaf(v.y, w.x, im));
-      }
-      I[i] = fmaf(re, re, im * im);
-    }
-    group_sync<WPS>(group);
-    // 4. binning and per-sub-aperture flux
-    float bv[PPT];
-    float part = 0.f;
-#pragma unroll
-    for (int j = 0; j < PPT; ++j) {
-      const int p = gt + GT * j;
-      float v = 0.f;
-      if (p < npix2) {
-        const int32_t *c = cb + p * P.nrebin2;
-        for (int r = 0; r < P.nrebin2; ++r) v += I[c[r]];
-      }
-      bv[j] = v;
-      part += v;
-    }
-    const float tot = group_sum<WPS>(part, red, gw, lane, group);
-    if (gt == 0) P.intensities[k] = tot;
-    const float fk = P.flux[k];
-    const uint32_t frame = P.frame_ptr ? *P.frame_ptr : P.frame;
-    // 5. normalise, noise, write cube + image, centroid partial sums
-    const int vx = P.validsubsx[k], vy = P.validsubsy[k];
-    float cs = 0.f, cx = 0.f, cy = 0.f;
-#pragma unroll
-    for (int j = 0; j < PPT; ++j) {
-      const int p = gt + GT * j;
-      if (p < npix2) {
-        float v = bv[j];
-        if (tot != 0.f) v = v * fk / tot * P.nphot;
-        const uint32_t pix = (uint32_t)(p + k * npix2);
-        if (P.noise_mode >= 1) v = (float)poisson_sample((double)v, pix, frame, P.k0, P.k1, P.tables);
-        if (P.noise_mode >= 2) v = v + P.noise * gauss_sample(pix, frame, P.k0, P.k1);
-        P.bincube[pix] = v;
-        const int y = fdiv(p, mg_np), x = p - y * P.npix;
-        const int idim = (x + vx) + (y + vy) * P.img_size;
-        float d = v;
-        if (P.ckind == 1 || P.ckind == 2) d = (v > P.c_thresh) ? v - P.c_thresh : 1.e-6f;
-        // raw pixels here; the tCoG write-back of thresholded pixels happens when
-        // the slopes are collected (aob_centro::get_cog), as in the reference
-        P.binimg[idim] = v;
-        if (P.ckind == 2) d *= P.c_weights[p + (P.c_wper ? k * npix2 : 0)];
-        cs += d;
-        cx = fmaf(d, (float)x, cx);
-        cy = fmaf(d, (float)y, cy);
-      }
-    }
-    if (P.ckind >= 0) {
-      cs = group_sum<WPS>(cs, red + WPS, gw, lane, group);
-      cx = group_sum<WPS>(cx, red + 2 * WPS, gw, lane, group);
-      cy = group_sum<WPS>(cy, red + 3 * WPS, gw, lane, group);
-      if (gt == 0) {
-        const int ix = P.c_order ? 2 * k : k;
-        const int iy = P.c_order ? 2 * k + 1 : k + P.nvalid;
-        P.c_slopes[ix] = (cx / (cs + 1.e-6f) - P.c_offset) * P.c_scale - P.c_ref[ix];
-        P.c_slopes[iy] = (cy / (cs + 1.e-6f) - P.c_offset) * P.c_scale - P.c_ref[iy];
-        P.c_intens[k] = cs;
-      }
-    }
-    group_sync<WPS>(group);
-  }
+  unsigned char *scratch = smem + L.hdr + L.per_grp * group;
+  for (int k = blockIdx.x * GROUPS + group; k < P.nvalid; k += gridDim.x * GROUPS)
+    sh_subap<NFFT, WPS, PD>(P, k, smem, scratch, group, gt);
 }
 
 __global__ void sh_fill_image_kernel(float *img, const float *cube, const int32_t *vx,
@@ -288,6 +97,14 @@ aob_sh::aob_sh(int device_, int nxsub_, int nvalid_, int npix_, int nphase_, int
   std::vector<double> lf(AOB_LOGFACT_N, 0.0), rkh(AOB_RK_N, 0.0);
   for (int k = 1; k < AOB_LOGFACT_N; ++k) lf[k] = lf[k - 1] + std::log((double)k);
   for (int k = 1; k < AOB_RK_N; ++k) rkh[k] = 1.0 / (double)k;
+  std::vector<float> tw(2 * nfft);
+  for (int m = 0; m < nfft; ++m) {
+    const double ang = 2.0 * M_PI * (double)m / (double)nfft;
+    tw[2 * m] = (float)std::cos(ang);
+    tw[2 * m + 1] = (float)-std::sin(ang);  // forward transform: exp(-2 pi i m / nfft)
+  }
+  twiddle.alloc(2 * nfft);
+  twiddle.upload(tw.data(), 2 * nfft);
   logfact.alloc(AOB_LOGFACT_N);
   logfact.upload(lf.data(), AOB_LOGFACT_N);
   rk.alloc(AOB_RK_N);
@@ -343,16 +160,13 @@ void aob_sh::load_arrays(const int32_t *h_binmap, const float *h_offsets, const 
   validsubsy.upload(h_vy, nvalid);
   istart.upload(h_istart, nvalid);
   jstart.upload(h_jstart, nvalid);
-  AOB_REQUIRE(smem_bytes(1) <= 200 * 1024, "sh: shared-memory footprint too large for this geometry");
+  AOB_REQUIRE(smem_bytes(4) <= 200 * 1024, "sh: shared-memory footprint too large for this geometry");
   loaded = true;
 }
 
 size_t aob_sh::smem_bytes(int wps) const {
-  const int ncb = nrebin * nrebin * npix * npix;
-  const size_t hdr = ((sizeof(float2) * nfft + sizeof(int32_t) * (2 * nfft + ncb)) + 15) & ~size_t(15);
-  const size_t per_grp = ((size_t)(nphase * nphase + nu * nphase) * sizeof(float2) + (size_t)nu * nv * sizeof(float) +
-                          4 * wps * sizeof(float) + 15) & ~size_t(15);
-  return hdr + (SH_WARPS / wps) * per_grp;
+  const ShSmem L(nfft, nu, nv, nphase, nrebin * nrebin * npix * npix, npix * npix, wps);
+  return L.bytes(SH_WARPS / wps);
 }
 
 // Warps per sub-aperture: the autotuner's choice if set, otherwise enough to
@@ -402,10 +216,9 @@ static void launch_sh_n(int wps, const ShKernelArgs &P, int nvalid, size_t sm, i
 
 void aob_sh::comp_image(bool with_noise, cudaStream_t s) { comp_image_to(with_noise, s, nullptr, nullptr); }
 
-void aob_sh::comp_image_to(bool with_noise, cudaStream_t s, float *slopes_dst, const uint32_t *frame_ptr) {
+aob_centro *aob_sh::make_args(bool with_noise, float *slopes_dst, const uint32_t *frame_ptr, ShKernelArgs &P) {
   AOB_REQUIRE(loaded, "sh.comp_image: load_arrays has not been called");
-  AOB_CUDA(cudaSetDevice(device));
-  ShKernelArgs P{};
+  P = ShKernelArgs{};
   P.phase = phase.p;
   P.pupil = pupil.p;
   P.npup = npup;
@@ -419,6 +232,7 @@ void aob_sh::comp_image_to(bool with_noise, cudaStream_t s, float *slopes_dst, c
   P.nrebin2 = nrebin * nrebin;
   P.nu = nu;
   P.nv = nv;
+  P.twiddle = reinterpret_cast<const float2 *>(twiddle.p);
   P.ulist = ulist.p;
   P.vlist = vlist.p;
   P.cbin = cbin.p;
@@ -452,9 +266,25 @@ void aob_sh::comp_image_to(bool with_noise, cudaStream_t s, float *slopes_dst, c
     P.c_slopes = slopes_dst ? slopes_dst : c->fused_slopes.p;
     P.c_intens = c->intensities.p;
     if (c->type == 2) AOB_REQUIRE(c->weights.p != nullptr, "wcog: weights not loaded");
-  } else {
-    c = nullptr;
+    return c;
   }
+  return nullptr;
+}
+
+// Host-side bookkeeping after an image was launched with make_args' arguments.
+void aob_sh::after_image(const ShKernelArgs &P, aob_centro *c, bool staged) {
+  if (P.noise_mode) ++frame;
+  ++image_gen;
+  if (c && staged) {
+    c->fused_gen = image_gen;
+    c->fused_params_gen = c->params_gen;
+  }
+}
+
+void aob_sh::comp_image_to(bool with_noise, cudaStream_t s, float *slopes_dst, const uint32_t *frame_ptr) {
+  AOB_CUDA(cudaSetDevice(device));
+  ShKernelArgs P;
+  aob_centro *c = make_args(with_noise, slopes_dst, frame_ptr, P);
   const int nsm = num_sms(device);
   const int wps = pick_wps();
   const size_t sm = smem_bytes(wps);
@@ -465,12 +295,7 @@ void aob_sh::comp_image_to(bool with_noise, cudaStream_t s, float *slopes_dst, c
   else
     launch_sh_n<64>(wps, P, nvalid, sm, nsm, s);
   AOB_LAUNCH_CHECK("sh_image_kernel");
-  if (P.noise_mode) ++frame;
-  ++image_gen;
-  if (c && !slopes_dst) {
-    c->fused_gen = image_gen;
-    c->fused_params_gen = c->params_gen;
-  }
+  after_image(P, c, slopes_dst == nullptr);
 }
 
 void aob_sh::fill_binimage(cudaStream_t s) {

@@ -219,8 +219,12 @@ int aob_loop_destroy(aob_loop *l);
 int aob_loop_step(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream);
 /* Replay the device part of a step from a CUDA graph (enable != 0). */
 int aob_loop_use_graph(aob_loop *l, int enable);
-/* Kernels launched by the device part of one step. */
+/* Kernels launched by the device part of the last step. */
 int aob_loop_kernels_per_step(aob_loop *l, int *n);
+/* mode 0 = fused single cooperative kernel when the configuration fits
+ * (otherwise three kernels), 1 = always three kernels, 2 = fused only (error
+ * if it does not fit); fused_wps = warps per sub-aperture in the fused kernel. */
+int aob_loop_set_mode(aob_loop *l, int mode, int fused_wps);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -191,10 +191,12 @@ def test_svd_cmat_matches_numpy(core):
     assert rel_rms(np.array(c.buffer("cmat", shape=(nactu, nslope))), cm) < 1e-5
 
 
+@pytest.mark.parametrize("mode", [1, 2])
 @pytest.mark.parametrize("graph", [False, True])
-@pytest.mark.parametrize("delay", [0.0, 1.0])
-def test_loop_matches_separate_calls(core, graph, delay):
-    """The bound loop (with or without CUDA-graph replay) equals the separate calls."""
+@pytest.mark.parametrize("delay", [0.0, 1.0, 1.4])
+def test_loop_matches_separate_calls(core, graph, delay, mode):
+    """The bound loop -- three kernels (mode 1) or the fused cooperative kernel
+    (mode 2), with or without CUDA-graph replay -- equals the separate calls."""
     rng = np.random.default_rng(21)
     g = sh_geometry("sh16")
     nact = 97
@@ -218,6 +220,7 @@ def test_loop_matches_separate_calls(core, graph, delay):
     c1.attach(w1)
     w2, c2, l2 = build()
     loop = core.Loop(w2, c2, l2, graph=graph)
+    loop.set_mode(mode)
     v2 = np.zeros(nact, np.float32)
     for it, ph in enumerate(screens):
         w1.set_phase(ph)
@@ -228,8 +231,11 @@ def test_loop_matches_separate_calls(core, graph, delay):
         loop.step(np.ascontiguousarray(ph.ravel(order="F")), v2, noise=True)
         v1 = np.array(l1.buffer("voltage"))
         np.testing.assert_array_equal(np.array(l2.buffer("centroids")), np.array(l1.buffer("centroids")))
-        np.testing.assert_array_equal(v2, v1)
+        assert rel_rms(v2, v1) < 1e-6
+        assert rel_rms(np.array(l2.buffer("com")), np.array(l1.buffer("com"))) < 1e-6
     assert w1.frame == w2.frame == len(screens)
+    assert l2.status() == 0
+    assert loop.kernels_per_step() == (1 if mode == 2 else 3)
 
 
 @pytest.mark.parametrize("wps", [1, 2, 4])
