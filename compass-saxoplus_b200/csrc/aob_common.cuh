@@ -132,7 +132,7 @@ __device__ __forceinline__ double log_factorial(double k, const NoiseTables &T) 
   return __dadd_rn(r, c);
 }
 
-static __device__ __noinline__ double poisson_sample(double lam, uint32_t idx, uint32_t frame, uint32_t k0,
+static __device__ __forceinline__ double poisson_sample(double lam, uint32_t idx, uint32_t frame, uint32_t k0,
                                                      uint32_t k1, NoiseTables T) {
   if (!(lam > 0.0)) return 0.0;
   U4 w = philox4x32_10(U4{idx, frame, TAG_POISSON, 0u}, k0, k1);
@@ -149,12 +149,13 @@ static __device__ __noinline__ double poisson_sample(double lam, uint32_t idx, u
     return (double)k;
   }
   const double slam = sqrt(lam);
-  const double loglam = log(lam);
   const double b = __dadd_rn(0.931, __dmul_rn(2.53, slam));
   const double a = __dadd_rn(-0.059, __dmul_rn(0.02483, b));
-  const double invalpha = __dadd_rn(1.1239, __ddiv_rn(1.1328, __dadd_rn(b, -3.4)));
   const double vr = __dadd_rn(0.9277, -__ddiv_rn(3.6224, __dadd_rn(b, -2.0)));
   const double a2 = __dmul_rn(2.0, a);
+  // constants of the exact acceptance test, computed only when a draw needs it
+  double loglam = 0.0, invalpha = 0.0;
+  bool slow_ready = false;
   for (uint32_t d = 0; d < 64u; ++d) {
     if (d > 0) w = philox4x32_10(U4{idx, frame, TAG_POISSON, d}, k0, k1);
     const double u = __dadd_rn(u01(w.x), -0.5);
@@ -163,6 +164,11 @@ static __device__ __noinline__ double poisson_sample(double lam, uint32_t idx, u
     const double k = floor(__dadd_rn(__dadd_rn(__dmul_rn(__dadd_rn(__ddiv_rn(a2, us), b), u), lam), 0.43));
     if (us >= 0.07 && v <= vr) return k;
     if (k < 0.0 || (us < 0.013 && v > us)) continue;
+    if (!slow_ready) {
+      loglam = log(lam);
+      invalpha = __dadd_rn(1.1239, __ddiv_rn(1.1328, __dadd_rn(b, -3.4)));
+      slow_ready = true;
+    }
     const double lhs = __ddiv_rn(__dmul_rn(v, invalpha), __dadd_rn(__ddiv_rn(a, __dmul_rn(us, us)), b));
     const double rhs = exp(__dadd_rn(__dadd_rn(__dmul_rn(k, loglam), -lam), -log_factorial(k, T)));
     if (lhs <= rhs) return k;

@@ -166,7 +166,8 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
     const int group = threadIdx.x / GT;
     const int gt = threadIdx.x - group * GT;
     unsigned char *scratch = shm + L.hdr + L.per_grp * group;
-    for (int k = blockIdx.x * GROUPS + group; k < A.sh.nvalid; k += gridDim.x * GROUPS)
+    // round-robin over CTAs first so that every SM gets nvalid / nsm sub-apertures
+    for (int k = group * gridDim.x + blockIdx.x; k < A.sh.nvalid; k += gridDim.x * GROUPS)
       sh_subap<NFFT, WPS, PD>(A.sh, k, shm, scratch, group, gt);
   }
   // ---- all slopes published ----

@@ -40,7 +40,7 @@ constexpr int SH_WARPS = 4;  // warps per CTA of the standalone sensor kernel
 // PD > 0: phase-grid side known at compile time (the DFT loops unroll and all
 // their shared-memory loads issue back to back); PD == 0: runtime side.
 template <int NFFT, int WPS, int PD>
-__global__ void __launch_bounds__(SH_WARPS * 32, 6) sh_image_kernel(ShKernelArgs P) {
+__global__ void __launch_bounds__(SH_WARPS * 32, 4) sh_image_kernel(ShKernelArgs P) {
   constexpr int GT = WPS * 32;
   constexpr int GROUPS = SH_WARPS / WPS;
   extern __shared__ __align__(16) unsigned char smem[];

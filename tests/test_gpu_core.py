@@ -217,6 +217,7 @@ def test_loop_matches_separate_calls(core, graph, delay, mode):
     cm = (rng.standard_normal((nact, 2 * g.nvalid)) * 0.01).astype(np.float32)
     screens = [kolmogorov_screen(g.tel.n, 20.0, seed=s) for s in range(5)]
     w1, c1, l1 = build()
+    w1.set_tuning(1)  # same launch shape (one warp per sub-aperture) as the fused kernel
     c1.attach(w1)
     w2, c2, l2 = build()
     loop = core.Loop(w2, c2, l2, graph=graph)
@@ -231,6 +232,7 @@ def test_loop_matches_separate_calls(core, graph, delay, mode):
         loop.step(np.ascontiguousarray(ph.ravel(order="F")), v2, noise=True)
         v1 = np.array(l1.buffer("voltage"))
         np.testing.assert_array_equal(np.array(l2.buffer("centroids")), np.array(l1.buffer("centroids")))
+        np.testing.assert_array_equal(np.array(w2.d_binimg), np.array(w1.d_binimg))
         assert rel_rms(v2, v1) < 1e-6
         assert rel_rms(np.array(l2.buffer("com")), np.array(l1.buffer("com"))) < 1e-6
     assert w1.frame == w2.frame == len(screens)
