@@ -264,42 +264,70 @@ def main():
     value = ws * args.steps / (total_ms / 1000.0)
     launches = loop.kernels_per_step() * args.steps
 
-    # ---- per-kernel durations (dominant kernel roofline) -------------------
-    def time_kernel(fn, reps):
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
-        for _ in range(3):
-            flush.zero_()
-            fn()
-        for a, b in evs:
-            flush.zero_()
-            a.record(stream)
-            fn()
-            b.record(stream)
+    # ---- per-kernel device durations (graph replay, no host gaps) ----------
+    def graph_time(fn, n=20, with_flush=True):
+        """Mean device time of fn() per launch: n x [flush, fn] minus n x [flush], replayed as one graph."""
+        gs = torch.cuda.Stream()
         torch.cuda.synchronize()
-        return statistics.mean(a.elapsed_time(b) for a, b in evs) / 1000.0
+        with torch.cuda.stream(gs):
+            for _ in range(2):
+                fn(gs.cuda_stream)
+        torch.cuda.synchronize()
 
-    reps = max(20, min(args.steps, 200))
-    t_mvm = time_kernel(lambda: ls.comp_com(stream=sptr), reps)
-    t_wfs = time_kernel(lambda: wfs.comp_image(noise=True, stream=sptr), reps)
+        def capture(body):
+            gr = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(gr, stream=gs):
+                for _ in range(n):
+                    if with_flush:
+                        flush.zero_()
+                    body()
+            return gr
+
+        g1 = capture(lambda: fn(gs.cuda_stream))
+        g0 = capture(lambda: None)
+        out = []
+        for gr in (g1, g0):
+            for _ in range(2):
+                gr.replay()
+            torch.cuda.synchronize()
+            best = float("inf")
+            for _ in range(5):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                gr.replay()
+                b.record()
+                torch.cuda.synchronize()
+                best = min(best, a.elapsed_time(b) / 1000.0)
+            out.append(best)
+        return (out[0] - out[1]) / n
+
+    loop.use_graph(False)
+    t_step = graph_time(lambda sp: loop.step(None, None, True, sp))
+    fused = loop.kernels_per_step() == 1
+    t_wfs = graph_time(lambda sp: wfs.comp_image(True, sp))
+    t_mvm = graph_time(lambda sp: ls.comp_com(sp))
+    loop.use_graph(not args.no_graph)
     esize = {"f32": 4, "bf16": 2, "fp8": 1}[args.precision]
     ld = {"f32": 4, "bf16": 8, "fp8": 16}[args.precision]
     ncol_pad = (setup.nslope + ld - 1) // ld * ld
-    mvm_bytes = setup.nactu * ncol_pad * esize + setup.nslope * 4 + setup.nactu * 4 * 4 + \
-        (setup.nactu * 4 if args.precision == "fp8" else 0)
     npix2 = g.npix * g.npix
-    wfs_bytes = 2 * g.nvalid * g.pdiam * g.pdiam * 4 + g.nvalid * npix2 * 4 * 2 + g.nvalid * (8 + 4 + 4 + 16) + \
+    # algorithmic bytes: every input read once, every output written once
+    mvm_bytes = setup.nactu * ncol_pad * esize + setup.nslope * 4 + setup.nactu * 4 * 5 + \
+        (setup.nactu * 4 if args.precision == "fp8" else 0)
+    wfs_bytes = 2 * g.nvalid * g.pdiam * g.pdiam * 4 + 2 * g.nvalid * npix2 * 4 + g.nvalid * 4 * 6 + \
         2 * g.nvalid * 4
     peak, peak_kind = _peaks()
-    if t_mvm >= t_wfs:
-        dom, dbytes, dt, prof = "ls_mvm_kernel<float>" if args.precision == "f32" else "ls_mvm_kernel", mvm_bytes, \
-            t_mvm, f"ls_mvm_saxo40_{args.precision}"
+    if fused:
+        dom, dbytes, dt, prof = "rtc_fused_kernel", mvm_bytes + wfs_bytes, t_step, f"rtc_fused_saxo40_{args.precision}"
+    elif t_mvm >= t_wfs:
+        dom, dbytes, dt, prof = "ls_mvm_bulk_kernel", mvm_bytes, t_mvm, f"ls_mvm_saxo40_{args.precision}"
     else:
-        dom, dbytes, dt, prof = "sh_image_kernel<32>", wfs_bytes, t_wfs, "sh_image_saxo40"
+        dom, dbytes, dt, prof = "sh_image_kernel", wfs_bytes, t_wfs, "sh_image_saxo40"
     achieved = dbytes / dt / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": _profile_traffic(prof), "kernel": dom, "algorithmic_bytes": dbytes,
-                "duration_us": dt * 1e6, "peak_source": peak_kind,
-                "kernels_us": {"sh_image": t_wfs * 1e6, "ls_mvm": t_mvm * 1e6}}
+                "traffic": _profile_traffic(prof), "kernel": dom, "algorithmic_bytes_per_launch": dbytes,
+                "duration_us": dt * 1e6, "peak_source": peak_kind, "timing": "graph replay, L2 flushed per launch",
+                "kernels_us": {"rtc_step": t_step * 1e6, "sh_image": t_wfs * 1e6, "ls_mvm": t_mvm * 1e6}}
 
     # ---- e2e: through aob_loop_step with pinned host buffers ---------------
     h_phase = torch.from_numpy(np.ascontiguousarray(np.stack([s.ravel(order="F") for s in screens]))).pin_memory()

@@ -220,8 +220,9 @@ def test_loop_matches_separate_calls(core, graph, delay, mode):
     w1.set_tuning(1)  # same launch shape (one warp per sub-aperture) as the fused kernel
     c1.attach(w1)
     w2, c2, l2 = build()
+    w2.set_tuning(1)
     loop = core.Loop(w2, c2, l2, graph=graph)
-    loop.set_mode(mode)
+    loop.set_mode(mode, 1)
     v2 = np.zeros(nact, np.float32)
     for it, ph in enumerate(screens):
         w1.set_phase(ph)
