@@ -202,6 +202,74 @@ int aob_ls_get_params(aob_ls *c, int *nslope, int *nactu, float *delay, float *g
                       int *open_loop, float *volt_min, float *volt_max, int *prec);
 
 
+/* ---- batched 2-D FFT ---------------------------------------------------- *
+ * In-place complex64 n x n transforms of `batch` contiguous images, n a power
+ * of two in [8, 2048]; cuFFT sign convention (forward = exp(-i...)),
+ * unnormalised.  Replaces the CarmaFFT calls of the target and pyramid paths
+ * (libcarma/src.cpp/carma_fft.cpp:165-179). */
+int aob_fft2d_c64(void *dev_data, int n, int batch, int inverse, int device, void *stream);
+
+/* ---- turbulent layers ----------------------------------------------------- *
+ * Replaces SutraAtmos / SutraTurbuScreen (libsutra/src.cpp/sutra_atmos.cpp,
+ * sutra_tscreen.cpp) as bound by python_module/sutra/src/atmos.cpp. */
+typedef struct aob_atmos aob_atmos;
+int aob_atmos_create(aob_atmos **out, int device);
+int aob_atmos_destroy(aob_atmos *a);
+/* add_screen + init_screen (sutra_atmos.cpp:52-81): A is dim x nstencil and B
+ * dim x dim, column-major; istx/isty index the flattened screen; r0 in pixels. */
+int aob_atmos_add_screen(aob_atmos *a, int dim, int nstencil, float r0_pix, float altitude, float deltax,
+                         float deltay, const float *A, const float *B, const uint32_t *istx,
+                         const uint32_t *isty, int64_t seed, int *index);
+/* refresh_screen (sutra_tscreen.cpp:113-127): zero, then 2*dim extrusions. */
+int aob_atmos_refresh_screen(aob_atmos *a, int idx, void *stream);
+/* move_atmos (sutra_atmos.cpp:82-100). */
+int aob_atmos_move(aob_atmos *a, void *stream);
+/* Current screen of layer idx (device pointer changes after each extrusion). */
+int aob_atmos_screen(aob_atmos *a, int idx, void **dev_screen, int *dim, float *accumx, float *accumy);
+int aob_atmos_nscreens(aob_atmos *a, int *n);
+/* Float64 factorisation of the extrusion operators on the GPU (iterkolmo.AB,
+ * shesha/shesha/util/iterkolmo.py:225-251) from the host covariances zz
+ * (nst x nst), xz (n x nst), xx (n x n), column-major; outputs A (n x nst) and
+ * B (n x n) column-major float32. */
+int aob_kolmo_factor_ab(int device, int n, int nst, const double *zz, const double *xz, const double *xx,
+                        float *A, float *B);
+
+/* ---- deformable mirror ---------------------------------------------------- *
+ * Replaces SutraDm (pzt) as loaded by pzt_loadarrays
+ * (libsutra/src.cpp/sutra_dm.cpp) and shaped by comp_shape (sutra_dm.cu:43-133). */
+typedef struct aob_dm aob_dm;
+/* influ: influsize x influsize x nact (Fortran order); i1/j1: lower-left pixel of
+ * each influence patch in the dim x dim DM screen. */
+int aob_dm_create(aob_dm **out, int device, int dim, int nact, int influsize, const float *influ,
+                  const int32_t *i1, const int32_t *j1);
+int aob_dm_destroy(aob_dm *d);
+/* dev_com: nact commands on the device (NULL = the DM's own command buffer). */
+int aob_dm_comp_shape(aob_dm *d, const float *dev_com, void *stream);
+/* which: "shape", "com". */
+int aob_dm_buffer(aob_dm *d, const char *which, void **dev_ptr, int64_t *nelem);
+
+/* ---- raytracing ------------------------------------------------------------ *
+ * SutraSource::raytrace (libsutra/src.cpp/sutra_source.cpp:222-320) with the
+ * bilinear generic_raytrace (sutra_target.cu:25-70): out (nx x ny) = (reset ? 0 :
+ * out) + sum over nsrc screens of screen_k sampled at (x + xoff_k, y + yoff_k).
+ * nsrc <= 8. */
+int aob_raytrace(float *dev_out, int nx, int ny, int nsrc, const float *const *dev_screens, const int *dims,
+                 const float *xoff, const float *yoff, int reset, void *stream);
+
+/* ---- science target -------------------------------------------------------- *
+ * SutraSource::comp_image / comp_strehl (sutra_source.cpp:397-515) without the
+ * sinc fit: short- and long-exposure PSF normalised so that the peak is the
+ * Strehl ratio. */
+typedef struct aob_target aob_target;
+int aob_target_create(aob_target **out, int device, int npup, int nfft, const float *pupil, float lambda_um);
+int aob_target_destroy(aob_target *t);
+/* dev_phase: npup x npup phase in micron (NULL = the target's own buffer). */
+int aob_target_comp_image(aob_target *t, const float *dev_phase, int comp_le, void *stream);
+int aob_target_strehl(aob_target *t, float *se, float *le, void *stream);
+int aob_target_reset_le(aob_target *t, void *stream);
+/* which: "phase", "image_se", "image_le", "amplipup". */
+int aob_target_buffer(aob_target *t, const char *which, void **dev_ptr, int64_t *nelem);
+
 /* ---- one closed-loop RTC iteration ------------------------------------ *
  * The per-iteration RTC sequence that CompassSupervisor.next() drives
  * through separate calls (shesha/shesha/supervisor/compassSupervisor.py:

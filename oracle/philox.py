@@ -170,3 +170,12 @@ def gaussian(index, frame, seed):
     u1 = ((w[0] >> np.uint32(8)).astype(np.float32) + np.float32(0.5)) * np.float32(5.9604644775390625e-08)
     u2 = ((w[2] >> np.uint32(8)).astype(np.float32) + np.float32(0.5)) * np.float32(5.9604644775390625e-08)
     return np.sqrt(np.float32(-2.0) * np.log(u1)) * np.cos(np.float32(2.0 * np.pi) * u2.astype(np.float64)).astype(np.float32)
+
+
+def normal_f32(c0, c1, c2, c3, seed):
+    """float32 Box-Muller deviate from the Philox block (c0, c1, c2, c3) (words 0 and 2)."""
+    k0, k1 = key_of(seed)
+    w = philox4x32(c0, c1, c2, c3, k0, k1)
+    u1 = ((w[0] >> np.uint32(8)).astype(np.float32) + np.float32(0.5)) * np.float32(5.9604644775390625e-08)
+    u2 = ((w[2] >> np.uint32(8)).astype(np.float32) + np.float32(0.5)) * np.float32(5.9604644775390625e-08)
+    return np.sqrt(np.float32(-2.0) * np.log(u1)) * np.cos(np.float32(2.0 * np.pi) * u2.astype(np.float64)).astype(np.float32)

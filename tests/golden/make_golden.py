@@ -156,47 +156,72 @@ def make_pyr(conf, gi, c):
     )
 
 
-def make_kolmo(itk, n, L0, seed):
-    zref = 0
+def make_kolmo(itk, n, L0, deltax, deltay):
     with contextlib.redirect_stdout(io.StringIO()):
-        A, B, istx, isty = itk.AB(n, L0)
-    return dict(A=A, B=B, istencilx=istx, istencily=isty)
+        A, B, istx, isty = itk.AB(n, L0, deltax, deltay, 0)
+    r2 = np.concatenate([np.linspace(0.0, 4.0, 41), np.linspace(4.0, 3.0 * n * n, 200)])
+    return dict(A=A, B=B, istencilx=istx, istencily=isty, stencil_size=itk.stencil_size(n),
+                struct_r2=r2, struct_L0=np.float64(L0), struct_val=itk.phase_struct(r2, L0))
 
 
-def make_dm(conf, gi, dmi, sh, nact, thresh, coupling, cobs=0.14, pupdiam=240):
+class _FakeDms:
+    """Records what the reference's dm_init hands to the GPU object."""
+
+    def __init__(self):
+        self.added = []
+        self.d_dms = []
+
+    def add_dm(self, *args):
+        self.added.append(args)
+        rec = types.SimpleNamespace()
+
+        def pzt_loadarrays(influ, influpos, ninflu, influstart, i1, j1):
+            rec.arrays = dict(influ=influ, influpos=influpos, ninflu=ninflu, influstart=influstart,
+                              i1=i1, j1=j1)
+
+        rec.pzt_loadarrays = pzt_loadarrays
+        self.d_dms.append(rec)
+
+
+def make_dm(conf, gi, dmi, c):
     p_geom = conf.ParamGeom()
-    p_geom.set_pupdiam(pupdiam)
+    p_geom.set_pupdiam(c["pupdiam"])
     p_geom.set_zenithangle(0.0)
     p_tel = conf.ParamTel()
     p_tel.set_diam(8.0)
-    p_tel.set_cobs(cobs)
+    p_tel.set_cobs(c["cobs"])
     with contextlib.redirect_stdout(io.StringIO()):
         gi.geom_init(p_geom, p_tel)
     p_dm = conf.ParamDm()
     p_dm.set_type("pzt")
-    p_dm.set_nact(nact)
+    p_dm.set_nact(c["nact"])
     p_dm.set_alt(0.0)
-    p_dm.set_thresh(thresh)
-    p_dm.set_coupling(coupling)
+    p_dm.set_coupling(c["coupling"])
     p_dm.set_unitpervolt(1.0)
     p_dm.set_push4imat(1.0)
     p_dm.set_influ_type("gaussian")
+    if c.get("margin_out") is not None:
+        p_dm.set_margin_out(c["margin_out"])
+    fake = _FakeDms()
     with contextlib.redirect_stdout(io.StringIO()):
-        dmi.dim_dm_init(p_tel, p_dm, p_geom, "pzt") if hasattr(dmi, "dim_dm_init") else None
-        if p_dm._n1 is None or p_dm._n1 == 0:
-            # same padding the reference applies in dm_init for an altitude-0 pzt DM
-            extent = p_geom.pupdiam + 2 * np.ceil(1.0 * p_geom.pupdiam / (nact - 1))
-            dim = int(max(p_geom._n, extent))
-            p_dm._n1 = int(np.floor(p_geom.cent - dim / 2.0))
-            p_dm._n2 = p_dm._n1 + dim - 1
-        dmi.make_pzt_dm(p_dm, p_geom, cobs)
+        dmi._dm_init(types.SimpleNamespace(active_device=0), fake, p_dm, [0.0], [0.0], p_geom, 8.0, c["cobs"],
+                     0.0, 0)
+    a = fake.d_dms[-1].arrays
+    args = fake.added[-1]
     return dict(
-        xpos=p_dm._xpos, ypos=p_dm._ypos, i1=p_dm._i1, j1=p_dm._j1,
-        influ=p_dm._influ, ntotact=p_dm._ntotact, influsize=p_dm._influsize,
-        pitch=p_dm._pitch, n1=p_dm._n1, n2=p_dm._n2, ninflu=p_dm._ninflu,
-        influstart=p_dm._influstart, influpos=p_dm._influpos,
-        dim_screen=p_dm._n2 - p_dm._n1 + 1,
+        xpos=p_dm._xpos, ypos=p_dm._ypos, i1=a["i1"], j1=a["j1"], influ=a["influ"],
+        ntotact=p_dm._ntotact, influsize=p_dm._influsize, pitch=np.float64(p_dm._pitch),
+        n1=p_dm._n1, n2=p_dm._n2, dim=args[3], n_mpupil=p_geom._n, cent=np.float64(p_geom.cent),
     )
+
+
+DM_CASES = {
+    "dm17": dict(pupdiam=128, nact=17, coupling=0.3, cobs=0.14),
+    "dm41": dict(pupdiam=240, nact=41, coupling=0.3, cobs=0.14, margin_out=1.0),
+}
+
+KOLMO_CASES = {"kolmo32": dict(n=32, L0=25.0 * 32 / 8.0, deltax=0.5, deltay=0.3),
+               "kolmo64neg": dict(n=64, L0=25.0 * 64 / 8.0, deltax=-0.7, deltay=-0.2)}
 
 
 def main():
@@ -215,6 +240,22 @@ def main():
         out = make_pyr(conf, gi, c)
         np.savez_compressed(os.path.join(HERE, f"geom_{name}.npz"), **out)
         print(name, "nvalid", out["nvalid"], "nfft", out["nfft"], "nrebin", out["nrebin"])
+    import shesha.init.dm_init as dmi
+    import shesha.util.iterkolmo as itk
+
+    only = os.environ.get("AO_GOLDEN_ONLY")
+    for name, c in DM_CASES.items():
+        if only and only != name:
+            continue
+        out = make_dm(conf, gi, dmi, c)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        print(name, "ntotact", out["ntotact"], "influsize", out["influsize"], "dim", out["dim"])
+    for name, c in KOLMO_CASES.items():
+        if only and only != name:
+            continue
+        out = make_kolmo(itk, c["n"], c["L0"], c["deltax"], c["deltay"])
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        print(name, "A", out["A"].shape, "B", out["B"].shape)
 
 
 if __name__ == "__main__":

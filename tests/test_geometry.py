@@ -56,3 +56,18 @@ def test_pyr_geometry_matches_reference(name, golden):
         np.testing.assert_array_equal(getattr(g, k), ref[k], err_msg=k)
     for k in ("halfxy", "pyr_cx", "pyr_cy", "sincar", "submask", "fluxPerSub"):
         np.testing.assert_array_equal(getattr(g, k), ref[k], err_msg=k)
+
+
+@pytest.mark.parametrize("name,nact,pup,margin", [("dm17", 17, 128, None), ("dm41", 41, 240, 1.0)])
+def test_dm_geometry_matches_reference(name, nact, pup, margin, golden):
+    from aob200 import dm_geometry as D
+
+    ref = golden(name)
+    tel = G.telescope_geometry(pup, 8.0, 0.14)
+    g = D.pzt_dm_geometry(nact, tel.pupdiam, tel.cent, tel.ssize, tel.n, 0.14, coupling=0.3, margin_out=margin)
+    assert g.ntotact == int(ref["ntotact"])
+    assert (g.n1, g.n2, g.dim, g.influsize) == (int(ref["n1"]), int(ref["n2"]), int(ref["dim"]), int(ref["influsize"]))
+    np.testing.assert_array_equal(g.i1, ref["i1"])
+    np.testing.assert_array_equal(g.j1, ref["j1"])
+    np.testing.assert_array_equal(g.xpos, ref["xpos"])
+    np.testing.assert_allclose(g.influ, ref["influ"], rtol=1e-6, atol=1e-7)
