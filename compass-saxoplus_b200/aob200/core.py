@@ -93,9 +93,12 @@ class ShWfs:
 
     def __del__(self):
         h = getattr(self, "h", None)
-        if h is not None and h.value and _lib._lib is not None:
-            _lib.lib().aob_sh_destroy(h)
-            self.h = None
+        try:
+            if h is not None and h.value and _lib._lib is not None:
+                _lib.lib().aob_sh_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown: module globals already cleared
+            pass
+        self.h = None
 
     def load_arrays(self, phasemap, hrmap, binmap, offsets, fluxPerSub, validsubsx, validsubsy,
                     istart, jstart, ttprojmat=None, kernel=None):
@@ -181,9 +184,12 @@ class Centroider:
 
     def __del__(self):
         h = getattr(self, "h", None)
-        if h is not None and h.value and _lib._lib is not None:
-            _lib.lib().aob_centro_destroy(h)
-            self.h = None
+        try:
+            if h is not None and h.value and _lib._lib is not None:
+                _lib.lib().aob_centro_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown: module globals already cleared
+            pass
+        self.h = None
 
     def attach(self, wfs):
         self.wfs = wfs
@@ -256,9 +262,12 @@ class LsController:
 
     def __del__(self):
         h = getattr(self, "h", None)
-        if h is not None and h.value and _lib._lib is not None:
-            _lib.lib().aob_ls_destroy(h)
-            self.h = None
+        try:
+            if h is not None and h.value and _lib._lib is not None:
+                _lib.lib().aob_ls_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown: module globals already cleared
+            pass
+        self.h = None
 
     def _vec(self, fn, a, dtype=np.float32, *extra):
         a = host_array(a, dtype)
@@ -362,9 +371,12 @@ class Loop:
 
     def __del__(self):
         h = getattr(self, "h", None)
-        if h is not None and h.value and _lib._lib is not None:
-            _lib.lib().aob_loop_destroy(h)
-            self.h = None
+        try:
+            if h is not None and h.value and _lib._lib is not None:
+                _lib.lib().aob_loop_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown: module globals already cleared
+            pass
+        self.h = None
 
     def use_graph(self, on=True):
         call("aob_loop_use_graph", self.h, 1 if on else 0)

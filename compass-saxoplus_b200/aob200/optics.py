@@ -30,9 +30,12 @@ class Dm:
 
     def __del__(self):
         h = getattr(self, "h", None)
-        if h is not None and h.value and _lib._lib is not None:
-            _lib.lib().aob_dm_destroy(h)
-            self.h = None
+        try:
+            if h is not None and h.value and _lib._lib is not None:
+                _lib.lib().aob_dm_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown: module globals already cleared
+            pass
+        self.h = None
 
     def buffer(self, which, shape=None) -> DeviceArray:
         return _buffer("aob_dm_buffer", self.h, which, np.float32, shape, self)
@@ -72,9 +75,12 @@ class Target:
 
     def __del__(self):
         h = getattr(self, "h", None)
-        if h is not None and h.value and _lib._lib is not None:
-            _lib.lib().aob_target_destroy(h)
-            self.h = None
+        try:
+            if h is not None and h.value and _lib._lib is not None:
+                _lib.lib().aob_target_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown: module globals already cleared
+            pass
+        self.h = None
 
     def buffer(self, which, shape=None) -> DeviceArray:
         return _buffer("aob_target_buffer", self.h, which, np.float32, shape, self)

@@ -101,8 +101,9 @@ def extrusion_operators(n, L0, deltax=1.0, deltay=1.0, device=0):
     nst = ist.size
     A = np.zeros((n, nst), dtype=np.float32, order="F")
     B = np.zeros((n, n), dtype=np.float32, order="F")
-    call("aob_kolmo_factor_ab", int(device), int(n), int(nst), host_array(zz, np.float64).ctypes.data,
-         host_array(xz, np.float64).ctypes.data, host_array(xxm, np.float64).ctypes.data,
+    # keep the host copies alive for the duration of the call
+    zzf, xzf, xxf = host_array(zz, np.float64), host_array(xz, np.float64), host_array(xxm, np.float64)
+    call("aob_kolmo_factor_ab", int(device), int(n), int(nst), zzf.ctypes.data, xzf.ctypes.data, xxf.ctypes.data,
          A.ctypes.data, B.ctypes.data)
     test = np.zeros(n * n, np.float32)
     test[ist] = np.arange(nst) + 1
@@ -171,9 +172,12 @@ class Atmosphere:
 
     def __del__(self):
         h = getattr(self, "h", None)
-        if h is not None and h.value and _lib._lib is not None:
-            _lib.lib().aob_atmos_destroy(h)
-            self.h = None
+        try:
+            if h is not None and h.value and _lib._lib is not None:
+                _lib.lib().aob_atmos_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown: module globals already cleared
+            pass
+        self.h = None
 
     def refresh(self, idx, stream=None):
         call("aob_atmos_refresh_screen", self.h, int(idx), stream)
