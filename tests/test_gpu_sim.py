@@ -71,12 +71,13 @@ def test_atmosphere_extrusion_matches_oracle(lib, dx, dy):
         scr = OT.extrude(scr, A, B, istx, isty, float(amp), xi, d)
         counter += 1
     assert rel_rms(atm.screen_host(0), scr) < 1e-4
-    # a few moves: accumulate shifts, extrude along x then y
-    ax = ay = 0.0
+    # a few moves: accumulate shifts in float32 like the reference's float accumx/accumy
+    # (sutra_atmos.cpp:100-119), extrude along x then y
+    ax = ay = np.float32(0.0)
     for _ in range(5):
         atm.move()
-        ax += dx
-        ay += dy
+        ax = np.float32(ax + np.float32(dx))
+        ay = np.float32(ay + np.float32(dy))
         for axis, acc in ((1, ax), (2, ay)):
             k = int(acc)
             c = 1 if k > 0 else -1
@@ -85,12 +86,12 @@ def test_atmosphere_extrusion_matches_oracle(lib, dx, dy):
                 scr = OT.extrude(scr, A, B, istx, isty, float(amp), xi, axis * c)
                 counter += 1
             if axis == 1:
-                ax -= k
+                ax = np.float32(ax - np.float32(k))
             else:
-                ay -= k
+                ay = np.float32(ay - np.float32(k))
     assert rel_rms(atm.screen_host(0), scr) < 1e-4
     _, _, gax, gay = atm.screen(0)
-    assert abs(gax - ax) < 1e-5 and abs(gay - ay) < 1e-5
+    assert gax == ax and gay == ay
 
 
 def test_raytrace_and_dm_shape_match_oracle(lib, golden):
