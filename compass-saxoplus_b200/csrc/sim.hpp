@@ -17,6 +17,13 @@ struct RaySources {
 };
 
 void raytrace(float *out, int nx, int ny, const RaySources &S, bool reset, cudaStream_t s);
+
+// One extrusion step (sim.cu): the new column/row y = A z + amp B xi + ref from the
+// stencil of `screen`, then the shift of the screen by one sample with y inserted.
+__global__ void extrude_gemv_kernel(const float *screen, int n, int nst, const float *Arm, const float *Brm,
+                                    const uint32_t *ist, int x0ref, float amp, uint32_t k0, uint32_t k1,
+                                    uint32_t counter, uint32_t layer, float *y);
+__global__ void extrude_shift_kernel(float *dst, const float *src, const float *y, int n, int dir);
 void kolmo_factor_ab(int device, int n, int nst, const double *zz, const double *xz, const double *xx, float *A,
                      float *B);
 

@@ -234,6 +234,28 @@ int aob_atmos_nscreens(aob_atmos *a, int *n);
 int aob_kolmo_factor_ab(int device, int n, int nst, const double *zz, const double *xz, const double *xx,
                         float *A, float *B);
 
+/* Allocation-free extrusion: no counterpart in the reference.  For callers that
+ * may not allocate device memory while they run -- a real-time controller with
+ * all memory reserved at start-up (cudaMalloc / cudaFree synchronise the device
+ * and take an unbounded time) or a plugin inside a host that owns the device
+ * memory.  Extrudes the caller's n x n screen (x fastest, updated in place) by
+ * one column (direction +-1) or row (+-2), exactly like one step of
+ * aob_atmos_move: A is n x nstencil and B n x n stored ROW-major (row i
+ * contiguous, the transpose of the column-major arrays aob_atmos_add_screen
+ * takes), dev_stencil holds nstencil indexes < n*n, amplitude is
+ * r0_pix^(-5/6) * 0.5 / (2 pi), and (seed, counter, layer_index) select the
+ * noise exactly as the layer's extrusion counter and index do there.
+ * Limit: n <= AOB_NOALLOC_EXTRUDE_MAX_N; larger n is rejected with AOB_ERR.
+ * The scratch is one fixed device array (about 1 MB, held by every GPU that
+ * loads the library until exit) shared by all calls: calls that overlap on the
+ * GPU (other streams, other host threads) race on it -- order them.  The first
+ * call on a device looks the array's address up (cudaGetSymbolAddress); make
+ * that first call before any stream capture. */
+#define AOB_NOALLOC_EXTRUDE_MAX_N 512
+int aob_extrude_noalloc(float *dev_screen, int n, int nstencil, const float *dev_A_rows,
+                        const float *dev_B_rows, const uint32_t *dev_stencil, int direction, float amplitude,
+                        int64_t seed, uint32_t counter, int layer_index, int device, void *stream);
+
 /* ---- deformable mirror ---------------------------------------------------- *
  * Replaces SutraDm (pzt) as loaded by pzt_loadarrays
  * (libsutra/src.cpp/sutra_dm.cpp) and shaped by comp_shape (sutra_dm.cu:43-133). */
