@@ -165,8 +165,9 @@ class ShWfs:
     def fill_binimage(self, stream=None):
         call("aob_sh_fill_binimage", self.h, stream)
 
-    def set_tuning(self, warps_per_subap=0):
-        call("aob_sh_set_tuning", self.h, int(warps_per_subap))
+    def set_tuning(self, subaps_per_cta=0):
+        """Sub-apertures per CTA batch of the sensor kernel (0 = heuristic); results are unchanged."""
+        call("aob_sh_set_tuning", self.h, int(subaps_per_cta))
 
 
 class Centroider:
@@ -381,9 +382,12 @@ class Loop:
     def use_graph(self, on=True):
         call("aob_loop_use_graph", self.h, 1 if on else 0)
 
-    def set_mode(self, mode=0, fused_wps=1):
-        """0: fused cooperative kernel when it fits, 1: three kernels, 2: fused only."""
-        call("aob_loop_set_mode", self.h, int(mode), int(fused_wps))
+    def set_mode(self, mode=0, fused_batch=0):
+        """0: fused cooperative kernel when it fits, 1: three kernels, 2: fused only.
+
+        fused_batch: at most this many sub-apertures per CTA and round in the fused
+        kernel (0 = a CTA's whole share at once); results are unchanged."""
+        call("aob_loop_set_mode", self.h, int(mode), int(fused_batch))
 
     def kernels_per_step(self) -> int:
         n = ctypes.c_int()

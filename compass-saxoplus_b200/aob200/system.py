@@ -171,7 +171,7 @@ class ShAoSystem:
     # ------------------------------------------------------------------ loop
     def close(self, graph=False, mode=0):
         self.loop = core.Loop(self.wfs, self.centro, self.ls, graph=graph)
-        self.loop.set_mode(mode, 1)
+        self.loop.set_mode(mode)
         return self.loop
 
     def next(self, stream=None, compute_psf=True, noise=True):

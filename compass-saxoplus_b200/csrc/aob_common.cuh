@@ -100,28 +100,39 @@ __host__ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t
   return c;
 }
 
-enum : uint32_t { TAG_POISSON = 0, TAG_GAUSS = 1 };
+enum : uint32_t { TAG_POISSON = 0 };
 
 __device__ __forceinline__ double u01(uint32_t x) {
   return __dmul_rn(__dadd_rn((double)x, 0.5), 2.3283064365386963e-10);  // (x + 0.5) / 2^32
 }
+// 24-bit uniform in (0, 1), exact in float32: ((x >> 8) + 0.5) / 2^24
+__device__ __forceinline__ float u01f(uint32_t x) { return ((float)(x >> 8) + 0.5f) * 5.9604644775390625e-08f; }
 
-// Poisson deviate: inversion for small means, PTRS (Hoermann 1993,
-// "The transformed rejection method for generating Poisson random variables")
-// otherwise, with the acceptance test in product form (one exp instead of three
-// logs and an lgamma).  log(k!) comes from a table (k < AOB_LOGFACT_N) built on the
-// host by cumulative sums of log(i), 1/k from a table of IEEE quotients; beyond
-// the table a two-term Stirling series is used.  float64 throughout with explicit
-// rounding intrinsics so that no multiply-add is contracted: the CPU oracle
-// performs the same operation sequence.
+// Photon and readout noise of one pixel.  One Philox block per (pixel, frame,
+// draw): draw 0 gives the first Poisson draw (words x, y) and the readout
+// noise (words z, w); rejected Poisson draws continue with draws 1, 2, ...
+//
+// Poisson deviate: inversion for small means (Devroye 1986, X.3), PTRS
+// (Hoermann 1993, "The transformed rejection method for generating Poisson
+// random variables") otherwise.  Every value that decides the outcome is
+// computed with correctly rounded IEEE operations only (explicit _rn
+// intrinsics, no contracted multiply-add), so the CPU oracle reproduces it:
+//  * inversion: float64, u from word x (32-bit uniform), p0 = exp(-lambda),
+//    1/k as the correctly rounded reciprocal;
+//  * PTRS fast path (acceptance ~86 % of draws): float32 sqrt / div / mul /
+//    add on 24-bit uniforms;
+//  * PTRS exact acceptance test: float64 in product form, log(k!) from the
+//    table of cumulative log sums (first AOB_LOGFACT_SMEM entries from shared
+//    memory), two-term Stirling series beyond the table.
 #define AOB_LOGFACT_N 4096
+#define AOB_LOGFACT_SMEM 1024
 #define AOB_RK_N 1024
 struct NoiseTables {
-  const double *logfact;  // log(k!) for k < AOB_LOGFACT_N
-  const double *rk;       // 1/k for 1 <= k < AOB_RK_N (rk[0] unused)
+  const double *logfact;  // log(k!) for k < AOB_LOGFACT_N (device memory)
 };
 
-__device__ __forceinline__ double log_factorial(double k, const NoiseTables &T) {
+__device__ __forceinline__ double log_factorial(double k, const double *lf_smem, const NoiseTables &T) {
+  if (k < (double)AOB_LOGFACT_SMEM) return lf_smem[(int)k];
   if (k < (double)AOB_LOGFACT_N) return __ldg(T.logfact + (int)k);
   const double x = __dadd_rn(k, 1.0);
   const double ix = __ddiv_rn(1.0, x);
@@ -132,57 +143,62 @@ __device__ __forceinline__ double log_factorial(double k, const NoiseTables &T) 
   return __dadd_rn(r, c);
 }
 
-static __device__ __forceinline__ double poisson_sample(double lam, uint32_t idx, uint32_t frame, uint32_t k0,
-                                                     uint32_t k1, NoiseTables T) {
-  if (!(lam > 0.0)) return 0.0;
-  U4 w = philox4x32_10(U4{idx, frame, TAG_POISSON, 0u}, k0, k1);
-  if (lam < 10.0) {
-    const double u = u01(w.x);
+// lam: the float32 mean; w0: Philox block of draw 0.
+static __device__ __forceinline__ float poisson_sample(float lamf, const U4 &w0, uint32_t idx, uint32_t frame,
+                                                    uint32_t k0, uint32_t k1, const double *lf_smem,
+                                                    NoiseTables T) {
+  if (!(lamf > 0.f)) return 0.f;
+  if (lamf < 10.f) {
+    const double lam = (double)lamf;
+    const double u = u01(w0.x);
     double p = exp(-lam);
     double f = p;
     int k = 0;
     while (u > f && k < AOB_RK_N - 1) {
       k += 1;
-      p = __dmul_rn(p, __dmul_rn(lam, __ldg(T.rk + k)));
+      p = __dmul_rn(p, __dmul_rn(lam, __drcp_rn((double)k)));
       f = __dadd_rn(f, p);
     }
-    return (double)k;
+    return (float)k;
   }
-  const double slam = sqrt(lam);
-  const double b = __dadd_rn(0.931, __dmul_rn(2.53, slam));
-  const double a = __dadd_rn(-0.059, __dmul_rn(0.02483, b));
-  const double vr = __dadd_rn(0.9277, -__ddiv_rn(3.6224, __dadd_rn(b, -2.0)));
-  const double a2 = __dmul_rn(2.0, a);
+  const float slam = __fsqrt_rn(lamf);
+  const float b = __fadd_rn(0.931f, __fmul_rn(2.53f, slam));
+  const float a = __fadd_rn(-0.059f, __fmul_rn(0.02483f, b));
+  const float vr = __fadd_rn(0.9277f, -__fdiv_rn(3.6224f, __fadd_rn(b, -2.0f)));
+  const float a2 = __fmul_rn(2.0f, a);
   // constants of the exact acceptance test, computed only when a draw needs it
   double loglam = 0.0, invalpha = 0.0;
   bool slow_ready = false;
+  U4 w = w0;
   for (uint32_t d = 0; d < 64u; ++d) {
     if (d > 0) w = philox4x32_10(U4{idx, frame, TAG_POISSON, d}, k0, k1);
-    const double u = __dadd_rn(u01(w.x), -0.5);
-    const double v = u01(w.y);
-    const double us = __dadd_rn(0.5, -fabs(u));
-    const double k = floor(__dadd_rn(__dadd_rn(__dmul_rn(__dadd_rn(__ddiv_rn(a2, us), b), u), lam), 0.43));
-    if (us >= 0.07 && v <= vr) return k;
-    if (k < 0.0 || (us < 0.013 && v > us)) continue;
+    const float u = __fadd_rn(u01f(w.x), -0.5f);
+    const float v = u01f(w.y);
+    const float us = __fadd_rn(0.5f, -fabsf(u));
+    const float k = floorf(__fadd_rn(__fadd_rn(__fmul_rn(__fadd_rn(__fdiv_rn(a2, us), b), u), lamf), 0.43f));
+    if (us >= 0.07f && v <= vr) return k;
+    if (k < 0.f || (us < 0.013f && v > us)) continue;
     if (!slow_ready) {
-      loglam = log(lam);
-      invalpha = __dadd_rn(1.1239, __ddiv_rn(1.1328, __dadd_rn(b, -3.4)));
+      loglam = log((double)lamf);
+      invalpha = __dadd_rn(1.1239, __ddiv_rn(1.1328, __dadd_rn((double)b, -3.4)));
       slow_ready = true;
     }
-    const double lhs = __ddiv_rn(__dmul_rn(v, invalpha), __dadd_rn(__ddiv_rn(a, __dmul_rn(us, us)), b));
-    const double rhs = exp(__dadd_rn(__dadd_rn(__dmul_rn(k, loglam), -lam), -log_factorial(k, T)));
+    const double usd = (double)us;
+    const double lhs =
+        __ddiv_rn(__dmul_rn((double)v, invalpha), __dadd_rn(__ddiv_rn((double)a, __dmul_rn(usd, usd)), (double)b));
+    const double rhs = exp(__dadd_rn(__dadd_rn(__dmul_rn((double)k, loglam), -(double)lamf),
+                                     -log_factorial((double)k, lf_smem, T)));
     if (lhs <= rhs) return k;
   }
-  return floor(lam + 0.5);
+  return floorf(__fadd_rn(lamf, 0.5f));
 }
 
-// Standard normal deviate by Box-Muller in float32 (u1 from word 0, u2 from
-// word 2, 24-bit uniforms).  The readout-noise value is compared with the CPU
-// oracle within a tolerance, not bit for bit.
-__device__ __forceinline__ float gauss_sample(uint32_t idx, uint32_t frame, uint32_t k0, uint32_t k1) {
-  const U4 w = philox4x32_10(U4{idx, frame, TAG_GAUSS, 0u}, k0, k1);
-  const float u1 = ((float)(w.x >> 8) + 0.5f) * 5.9604644775390625e-08f;
-  const float u2 = ((float)(w.z >> 8) + 0.5f) * 5.9604644775390625e-08f;
+// Standard normal deviate by Box-Muller in float32 from words z (u1) and w (u2)
+// of the pixel's draw-0 block.  Compared with the CPU oracle within a
+// tolerance, not bit for bit.
+__device__ __forceinline__ float gauss_sample(const U4 &w0) {
+  const float u1 = u01f(w0.z);
+  const float u2 = u01f(w0.w);
   return sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
 }
 

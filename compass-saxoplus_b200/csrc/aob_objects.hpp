@@ -43,8 +43,9 @@ struct aob_sh {
   aob::DevBuf<int32_t> ulist, vlist, cbin;
   // outputs
   aob::DevBuf<float> bincube, binimg, intensities, slopes;
-  aob::DevBuf<double> logfact, rk;  // noise-sampler tables
+  aob::DevBuf<double> logfact;      // noise-sampler table log(k!)
   aob::DevBuf<float> twiddle;       // exp(-2 pi i m / nfft) as (re, im) pairs
+  aob::DevBuf<float> wxy;           // the same values gathered per (frequency, sample)
   // centroider whose slopes are fused into comp_image (may be null)
   aob_centro *fused = nullptr;
   uint64_t image_gen = 0;  // bumped whenever binimg changes
@@ -62,9 +63,9 @@ struct aob_sh {
   // kernel arguments for one image; returns the fused centroider (or null)
   aob_centro *make_args(bool noise, float *slopes_dst, const uint32_t *frame_ptr, aob::ShKernelArgs &P);
   void after_image(const aob::ShKernelArgs &P, aob_centro *c, bool staged);
-  int wps_override = 0;  // warps per sub-aperture chosen by the autotuner (0 = heuristic)
-  size_t smem_bytes(int wps) const;
-  int pick_wps() const;
+  int batch_override = 0;  // sub-apertures per CTA chosen by the autotuner (0 = heuristic)
+  size_t smem_bytes(int batch) const;
+  int pick_batch() const;
 };
 
 // ---------------------------------------------------------------------------
@@ -154,9 +155,9 @@ struct aob_loop {
   std::vector<uint64_t> graph_key;       // parameter snapshot each graph was built for
   std::vector<const void *> graph_front; // ring front buffer each graph was built for
   uint64_t frame_mirror = ~0ull;         // value held by d_frame
-  aob::DevBuf<uint32_t> gbar;            // grid barrier state of the fused kernel
+  aob::DevBuf<unsigned long long> gbar;  // grid-barrier arrival counter of the fused kernel
   int mode = 0;                          // 0 auto (fused when it fits), 1 three kernels, 2 fused only
-  int fused_wps = 1;                     // warps per sub-aperture in the fused kernel
+  int fused_batch = 0;                   // max sub-apertures per CTA and round in the fused kernel (0 = all)
   int last_kernels = 3;                  // kernels launched by the last device step
   uint32_t frame_host = 0;
   aob_loop(aob_sh *w, aob_centro *c, aob_ls *l);

@@ -208,11 +208,11 @@ int aob_sh_fill_binimage(aob_sh *h, void *stream) {
   h->fill_binimage(S(stream));
   AOB_API_END
 }
-int aob_sh_set_tuning(aob_sh *h, int wps) {
+int aob_sh_set_tuning(aob_sh *h, int subaps_per_cta) {
   AOB_API_BEGIN
   NEED(h);
-  if (wps != 0 && wps != 1 && wps != 2 && wps != 4) throw Error("sh.set_tuning: warps per sub-aperture must be 0, 1, 2 or 4");
-  h->wps_override = wps;
+  if (subaps_per_cta < 0 || subaps_per_cta > 32) throw Error("sh.set_tuning: sub-apertures per CTA must be in [0, 32]");
+  h->batch_override = subaps_per_cta;
   AOB_API_END
 }
 int aob_sh_set_bincube(aob_sh *h, const float *host, int64_t n) {

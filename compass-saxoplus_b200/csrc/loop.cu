@@ -26,7 +26,7 @@ aob_loop::aob_loop(aob_sh *w, aob_centro *c, aob_ls *l) : wfs(w), centro(c), ls(
   AOB_REQUIRE(c->nvalid == w->nvalid, "loop: centroider nvalid differs from the sensor's");
   AOB_CUDA(cudaSetDevice(w->device));
   d_frame.alloc(1);
-  gbar.alloc(2);
+  gbar.alloc(1);
   if (c->wfs && c->wfs->fused == c && c->wfs != w) c->wfs->fused = nullptr;
   c->wfs = w;
   w->fused = c;
@@ -62,9 +62,9 @@ uint64_t aob_loop::key(bool noise) const {
   mix(&ls->prec, sizeof ls->prec);
   mix(&ls->nblocks, sizeof ls->nblocks);
   mix(&ls->mvm_kind, sizeof ls->mvm_kind);
-  mix(&wfs->wps_override, sizeof wfs->wps_override);
+  mix(&wfs->batch_override, sizeof wfs->batch_override);
   mix(&mode, sizeof mode);
-  mix(&fused_wps, sizeof fused_wps);
+  mix(&fused_batch, sizeof fused_batch);
   const void *pm[4] = {ls->cm_f32.p, ls->cm_bf16.p, ls->cm_fp8.p, centro->weights.p};
   mix(pm, sizeof pm);
   return h;
@@ -72,10 +72,9 @@ uint64_t aob_loop::key(bool noise) const {
 
 void aob_loop::device_step(bool noise, cudaStream_t s, bool frame_on_device) {
   if (mode != 1) {
-    // barrier state is re-armed before every fused launch (a timed-out launch
-    // can leave the arrival count non-zero)
+    // the fused kernel's grid barrier is a 64-bit arrival counter that every
+    // launch raises by exactly its grid size, so it needs no re-arming
     if (launch_fused(noise, s, frame_on_device, true)) {
-      AOB_CUDA(cudaMemsetAsync(gbar.p, 0, 2 * sizeof(uint32_t), s));
       if (launch_fused(noise, s, frame_on_device, false)) {
         last_kernels = 1;
         return;
@@ -228,13 +227,13 @@ int aob_loop_kernels_per_step(aob_loop *l, int *n) {
   return AOB_OK;
 }
 
-int aob_loop_set_mode(aob_loop *l, int mode, int fused_wps) {
-  if (!l || mode < 0 || mode > 2 || (fused_wps != 0 && fused_wps != 1 && fused_wps != 2 && fused_wps != 4)) {
-    set_last_error("aob_loop_set_mode: mode 0..2, fused_wps 0/1/2/4");
+int aob_loop_set_mode(aob_loop *l, int mode, int fused_batch) {
+  if (!l || mode < 0 || mode > 2 || fused_batch < 0 || fused_batch > 64) {
+    set_last_error("aob_loop_set_mode: mode 0..2, fused_batch 0..64");
     return AOB_ERR;
   }
   l->mode = mode;
-  l->fused_wps = fused_wps > 0 ? fused_wps : 1;
+  l->fused_batch = fused_batch;
   return AOB_OK;
 }
 

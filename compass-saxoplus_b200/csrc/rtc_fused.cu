@@ -4,7 +4,8 @@
 // The MVM's HBM stream does not depend on the slopes, so it is started first:
 // at kernel entry one thread per CTA issues TMA bulk copies of that CTA's rows of
 // the packed command matrix into shared memory (one mbarrier per row).  While
-// those bytes are in flight the CTA's warps form sensor images (sh_core.cuh).
+// those bytes are in flight the CTA forms the sensor images of its share of the
+// sub-apertures (k = blockIdx.x + j * gridDim.x) in batches (sh_core.cuh).
 // A bounded grid barrier then publishes the slopes; every CTA stages them in
 // shared memory and reduces its rows, which by then have landed, applying the
 // integrator (sutra_controller_ls.cpp:251-285, sutra_utils.cu:631-639) and the
@@ -29,6 +30,8 @@ constexpr uint32_t GRID_MAX_POLLS = 1u << 24;
 constexpr uint32_t ROW_MAX_POLLS = 1u << 22;
 constexpr int FUSED_THREADS = 512;
 
+// Dot product of one 16-byte chunk of a packed command-matrix row with its
+// slopes sv[0 .. N/4) (contiguous float4s).
 template <typename T>
 struct FPack;
 template <>
@@ -48,7 +51,7 @@ struct FPack<__nv_bfloat16> {
     float a = 0.f;
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
-      const float4 s = sv[32 * i];
+      const float4 s = sv[i];
       const float2 f0 = __bfloat1622float2(h[2 * i]), f1 = __bfloat1622float2(h[2 * i + 1]);
       a = fmaf(f1.y, s.w, fmaf(f1.x, s.z, fmaf(f0.y, s.y, fmaf(f0.x, s.x, a))));
     }
@@ -63,7 +66,7 @@ struct FPack<__nv_fp8_e4m3> {
     float a = 0.f;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const float4 s = sv[32 * i];
+      const float4 s = sv[i];
       const float2 f0 = static_cast<float2>(h[2 * i]), f1 = static_cast<float2>(h[2 * i + 1]);
       a = fmaf(f1.y, s.w, fmaf(f1.x, s.z, fmaf(f0.y, s.y, fmaf(f0.x, s.x, a))));
     }
@@ -88,37 +91,40 @@ struct RtcFusedArgs {
   float *volt;
   uint32_t *bump;     // noise frame counter (incremented once)
   uint32_t *status;   // error word
-  uint32_t *gbar;     // grid barrier {arrived, generation}
+  unsigned long long *gbar;  // grid-barrier arrival counter (never reset)
   int rows_per_cta;
+  int batch;  // sub-apertures per CTA and round
 };
 
 __host__ __device__ inline int fused_slope_floats(int ld, int v) { return ((ld / v + 31) / 32) * 32 * v; }
+__host__ __device__ inline size_t fused_bars_bytes(int rows) { return 128 * (((size_t)rows * 8 + 127) / 128); }
+__host__ __device__ inline size_t fused_pre_bytes(int rows) { return 128 * (((size_t)rows * 20 + 127) / 128); }
 
-// Grid-wide barrier for a cooperative launch: {arrived, generation} in global
-// memory; the last CTA to arrive resets the count and advances the generation.
-// The wait is bounded; on expiry ERR_GRID_TIMEOUT is set and false returned.
-__device__ __forceinline__ bool grid_barrier(uint32_t *gbar, uint32_t nblocks, uint32_t *status) {
+// Grid-wide barrier for a cooperative launch.  ``ctr`` counts arrivals over the
+// whole life of the loop: launch n raises it from n * G to (n + 1) * G, so a
+// CTA's target is the next multiple of G above the value its own arrival saw
+// and nothing has to be reset between launches (every CTA arrives exactly
+// once per launch, also when a wait times out).  The wait is bounded; on
+// expiry ERR_GRID_TIMEOUT is set and false returned.
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ bool grid_barrier(unsigned long long *ctr, uint32_t nblocks, uint32_t *status) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    volatile uint32_t *vgen = gbar + 1;
-    const uint32_t gen = *vgen;
     __threadfence();
-    const uint32_t arrived = atomicAdd(gbar, 1u);
-    if (arrived == nblocks - 1) {
-      gbar[0] = 0u;
-      __threadfence();
-      atomicAdd(gbar + 1, 1u);
-    } else {
-      uint32_t i = 0;
-      while (*vgen == gen && i < GRID_MAX_POLLS) {
-        __nanosleep(32);
-        ++i;
-      }
-      if (*vgen == gen) {
+    const unsigned long long old = atomicAdd(ctr, 1ull);
+    const unsigned long long target = (old / nblocks + 1ull) * nblocks;
+    uint32_t i = 0;
+    while (ld_acquire_u64(ctr) < target) {
+      if (++i >= GRID_MAX_POLLS) {
         ok = 0;
         atomicOr(status, (uint32_t)ERR_GRID_TIMEOUT);
+        break;
       }
     }
     __threadfence();
@@ -128,24 +134,24 @@ __device__ __forceinline__ bool grid_barrier(uint32_t *gbar, uint32_t nblocks, u
   return s_ok != 0;
 }
 
-template <typename T, int NFFT, int WPS, int PD>
+template <typename T, int NFFT, int PD>
 __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArgs A) {
   extern __shared__ __align__(128) unsigned char sm[];
   constexpr int V = FPack<T>::N;
   constexpr int Q = V / 4;
-  constexpr int GT = WPS * 32;
-  constexpr int GROUPS = FUSED_THREADS / GT;
   const uint32_t row_bytes = (uint32_t)(A.ld * sizeof(T));
   const int r0 = (int)(((int64_t)blockIdx.x * A.nrow) / gridDim.x);
   const int r1 = (int)(((int64_t)(blockIdx.x + 1) * A.nrow) / gridDim.x);
   const int R = r1 - r0;
-  // shared memory: barriers | matrix rows | sensor tables + group scratch | slopes
+  // shared memory: barriers | per-row epilogue inputs | matrix rows |
+  //                sensor tables + batch work area | slopes
   uint64_t *bars = reinterpret_cast<uint64_t *>(sm);
-  unsigned char *rows = sm + 128 * ((A.rows_per_cta * 8 + 127) / 128);
+  float *pre = reinterpret_cast<float *>(sm + fused_bars_bytes(A.rows_per_cta));
+  unsigned char *rows = sm + fused_bars_bytes(A.rows_per_cta) + fused_pre_bytes(A.rows_per_cta);
   unsigned char *shm = rows + (size_t)A.rows_per_cta * row_bytes;
   const int pd = PD > 0 ? PD : A.sh.pdiam;
-  const ShSmem L(NFFT, A.sh.nu, A.sh.nv, pd, A.sh.nrebin2 * A.sh.npix * A.sh.npix, A.sh.npix * A.sh.npix, WPS);
-  float *s_sh = reinterpret_cast<float *>(shm + L.bytes(GROUPS));
+  const ShSmem L(NFFT, A.sh.nu, A.sh.nv, pd, A.sh.nrebin2 * A.sh.npix * A.sh.npix, A.sh.npix * A.sh.npix, A.batch);
+  float *s_sh = reinterpret_cast<float *>(shm + L.bytes());
 
   if (threadIdx.x == 0) {
     for (int r = 0; r < R; ++r) mbar_init(&bars[r], 1);
@@ -159,64 +165,108 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
       bulk_g2s(rows + (size_t)r * row_bytes, src + (size_t)r * row_bytes, row_bytes, &bars[r]);
     }
   }
-  // ---- sensor images and slopes ----
+  // epilogue inputs of this CTA's rows, fetched now so the epilogue makes no
+  // global round trip: [scale | modal gain | com | ring[0] | ring[1]]
+  const int RP = A.rows_per_cta;
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    const int gr = r0 + r;
+    pre[r] = A.rscale ? A.rscale[gr] : 1.f;
+    pre[RP + r] = A.mgain[gr];
+    pre[2 * RP + r] = A.com[gr];
+    if (A.delayed) {
+      pre[3 * RP + r] = A.oldest[gr];
+      pre[4 * RP + r] = A.second[gr];
+    }
+  }
+  // ---- sensor images and slopes: this CTA's sub-apertures, A.batch per round ----
   sh_load_tables<NFFT>(A.sh, shm, threadIdx.x, blockDim.x);
-  __syncthreads();
-  {
-    const int group = threadIdx.x / GT;
-    const int gt = threadIdx.x - group * GT;
-    unsigned char *scratch = shm + L.hdr + L.per_grp * group;
-    // round-robin over CTAs first so that every SM gets nvalid / nsm sub-apertures
-    for (int k = group * gridDim.x + blockIdx.x; k < A.sh.nvalid; k += gridDim.x * GROUPS)
-      sh_subap<NFFT, WPS, PD>(A.sh, k, shm, scratch, group, gt);
+  // (sh_batch synchronises before the tables are first read)
+  const int nvalid = A.sh.nvalid;
+  for (int base = blockIdx.x; base < nvalid; base += A.batch * gridDim.x) {
+    const int Sb = min(A.batch, (nvalid - base + (int)gridDim.x - 1) / (int)gridDim.x);
+    sh_batch<NFFT, PD>(A.sh, base, gridDim.x, Sb, shm, shm + L.hdr, L);
   }
   // ---- all slopes published ----
   const bool ok = grid_barrier(A.gbar, gridDim.x, A.status);
   if (ok) {
     if (A.bump && blockIdx.x == 0 && threadIdx.x == 0) *A.bump += 1u;
-    const int nsh = fused_slope_floats(A.ld, V);
-    for (int i = threadIdx.x; i < nsh; i += blockDim.x) {
-      const int g = i >> 2, e = i & 3;
+    // slopes into shared memory, 16 bytes per load (L2 only: they were written by
+    // other CTAs of this launch); group g of the layout holds slopes
+    // [(chunk) * V + 4 q, +4) for chunk = (g & 31) + 32 j, g >> 5 = j * Q + q
+    const int ngrp = fused_slope_floats(A.ld, V) / 4;
+    for (int g = threadIdx.x; g < ngrp; g += blockDim.x) {
       const int l = g & 31, jq = g >> 5;
       const int j = jq / Q, q = jq - j * Q;
-      const int src = (l + 32 * j) * V + 4 * q + e;
-      s_sh[i] = (src < A.ncol) ? __ldcg(A.sh.c_slopes + src) : 0.f;
+      const int src = (l + 32 * j) * V + 4 * q;
+      float4 v4;
+      if (src + 3 < A.ncol) {
+        v4 = __ldcg(reinterpret_cast<const float4 *>(A.sh.c_slopes + src));
+      } else {
+        v4.x = src < A.ncol ? __ldcg(A.sh.c_slopes + src) : 0.f;
+        v4.y = src + 1 < A.ncol ? __ldcg(A.sh.c_slopes + src + 1) : 0.f;
+        v4.z = src + 2 < A.ncol ? __ldcg(A.sh.c_slopes + src + 2) : 0.f;
+        v4.w = 0.f;
+      }
+      reinterpret_cast<float4 *>(s_sh)[g] = v4;
     }
     __syncthreads();
+    // Split-K over the CTA's rows: warp w, lane l take chunks c = l + 32 (w + NW i);
+    // each slope chunk is read once and applied to every row from registers,
+    // then the per-warp partial sums are added in warp order (deterministic).
+    constexpr int NW = FUSED_THREADS / 32;
+    constexpr int RB = 8;  // rows per register block
     const int nchunk = A.ld / V;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const float4 *svl = reinterpret_cast<const float4 *>(s_sh) + lane;
-    for (int r = warp; r < R; r += FUSED_THREADS / 32) {
-      if (!mbar_wait(&bars[r], 0, ROW_MAX_POLLS)) {
-        if (lane == 0) atomicOr(A.status, (uint32_t)ERR_MBAR_TIMEOUT);
-        continue;
-      }
-      const uint4 *row = reinterpret_cast<const uint4 *>(rows + (size_t)r * row_bytes) + lane;
-      float acc[4] = {0.f, 0.f, 0.f, 0.f};
-      int j = 0;
-      for (; 32 * (j + 3) + lane < nchunk; j += 4) {
+    bool rows_ok = true;
+    for (int r = 0; r < R; ++r) rows_ok &= mbar_wait(&bars[r], 0, ROW_MAX_POLLS);
+    if (!rows_ok && lane == 0) atomicOr(A.status, (uint32_t)ERR_MBAR_TIMEOUT);
+    float *part = reinterpret_cast<float *>(shm + L.hdr);  // [NW][rows_per_cta], sensor work area is free now
+    const float4 *sv4 = reinterpret_cast<const float4 *>(s_sh);
+    for (int rb = 0; rb < R; rb += RB) {
+      float acc[RB];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) acc[u] += FPack<T>::dot(row[32 * (j + u)], svl + 32 * Q * (j + u));
-      }
-      for (; 32 * j + lane < nchunk; ++j) acc[0] += FPack<T>::dot(row[32 * j], svl + 32 * Q * j);
-      float tot = warp_sum((acc[0] + acc[1]) + (acc[2] + acc[3]));
-      if (lane == 0) {
-        const int gr = r0 + r;
-        if (A.rscale) tot *= A.rscale[gr];
-        const float e = -tot;
-        A.err[gr] = e;
-        const float c = A.gain * (e * A.mgain[gr]) + A.com[gr];
-        A.com[gr] = c;
-        float v;
-        if (A.delayed) {
-          v = A.a * A.oldest[gr] + A.b * A.second[gr];
-          A.oldest[gr] = c;
-        } else {
-          v = c;
+      for (int u = 0; u < RB; ++u) acc[u] = 0.f;
+      if (rows_ok) {
+        for (int jj = warp; 32 * jj + lane < nchunk; jj += NW) {
+          const int c = lane + 32 * jj;
+          float4 sv[Q];
+#pragma unroll
+          for (int q = 0; q < Q; ++q) sv[q] = sv4[(jj * Q + q) * 32 + lane];
+#pragma unroll
+          for (int u = 0; u < RB; ++u)
+            if (rb + u < R) {
+              const uint4 q4 = reinterpret_cast<const uint4 *>(rows + (size_t)(rb + u) * row_bytes)[c];
+              acc[u] += FPack<T>::dot(q4, sv);
+            }
         }
-        if (A.do_clip) v = fminf(fmaxf(v, A.vmin), A.vmax);
-        A.volt[gr] = v;
       }
+#pragma unroll
+      for (int u = 0; u < RB; ++u) {
+        const float t = warp_sum(acc[u]);
+        if (lane == 0 && rb + u < R) part[warp * A.rows_per_cta + rb + u] = t;
+      }
+    }
+    __syncthreads();
+    // integrator and voltage per row, one thread per row
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+      float tot = 0.f;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) tot += part[w * A.rows_per_cta + r];
+      const int gr = r0 + r;
+      if (A.rscale) tot *= pre[r];
+      const float e = -tot;
+      A.err[gr] = e;
+      const float c = A.gain * (e * pre[RP + r]) + pre[2 * RP + r];
+      A.com[gr] = c;
+      float v;
+      if (A.delayed) {
+        v = A.a * pre[3 * RP + r] + A.b * pre[4 * RP + r];
+        A.oldest[gr] = c;
+      } else {
+        v = c;
+      }
+      if (A.do_clip) v = fminf(fmaxf(v, A.vmin), A.vmax);
+      A.volt[gr] = v;
     }
   }
   // no CTA may exit with a copy still landing in its shared memory
@@ -226,9 +276,9 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
 }
 
 // ---------------------------------------------------------------------------
-template <typename T, int NFFT, int WPS, int PD>
+template <typename T, int NFFT, int PD>
 static bool launch_fused_t(const RtcFusedArgs &A0, int grid, size_t sm, cudaStream_t s, bool dry) {
-  auto kern = rtc_fused_kernel<T, NFFT, WPS, PD>;
+  auto kern = rtc_fused_kernel<T, NFFT, PD>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) {
     cudaGetLastError();
     return false;
@@ -254,29 +304,21 @@ static bool launch_fused_t(const RtcFusedArgs &A0, int grid, size_t sm, cudaStre
   return true;
 }
 
-template <typename T, int NFFT, int WPS>
+template <typename T, int NFFT>
 static bool launch_fused_pd(int pd, const RtcFusedArgs &A, int grid, size_t sm, cudaStream_t s, bool dry) {
   switch (pd) {
-    case 4: return launch_fused_t<T, NFFT, WPS, 4>(A, grid, sm, s, dry);
-    case 6: return launch_fused_t<T, NFFT, WPS, 6>(A, grid, sm, s, dry);
-    case 8: return launch_fused_t<T, NFFT, WPS, 8>(A, grid, sm, s, dry);
-    default: return launch_fused_t<T, NFFT, WPS, 0>(A, grid, sm, s, dry);
+    case 4: return launch_fused_t<T, NFFT, 4>(A, grid, sm, s, dry);
+    case 6: return launch_fused_t<T, NFFT, 6>(A, grid, sm, s, dry);
+    case 8: return launch_fused_t<T, NFFT, 8>(A, grid, sm, s, dry);
+    default: return launch_fused_t<T, NFFT, 0>(A, grid, sm, s, dry);
   }
 }
 
-template <typename T, int NFFT>
-static bool launch_fused_w(int wps, int pd, const RtcFusedArgs &A, int grid, size_t sm, cudaStream_t s, bool dry) {
-  if (wps == 1) return launch_fused_pd<T, NFFT, 1>(pd, A, grid, sm, s, dry);
-  if (wps == 2) return launch_fused_pd<T, NFFT, 2>(pd, A, grid, sm, s, dry);
-  return launch_fused_pd<T, NFFT, 4>(pd, A, grid, sm, s, dry);
-}
-
 template <typename T>
-static bool launch_fused_n(int nfft, int wps, int pd, const RtcFusedArgs &A, int grid, size_t sm, cudaStream_t s,
-                           bool dry) {
-  if (nfft == 16) return launch_fused_w<T, 16>(wps, pd, A, grid, sm, s, dry);
-  if (nfft == 32) return launch_fused_w<T, 32>(wps, pd, A, grid, sm, s, dry);
-  return launch_fused_w<T, 64>(wps, pd, A, grid, sm, s, dry);
+static bool launch_fused_n(int nfft, int pd, const RtcFusedArgs &A, int grid, size_t sm, cudaStream_t s, bool dry) {
+  if (nfft == 16) return launch_fused_pd<T, 16>(pd, A, grid, sm, s, dry);
+  if (nfft == 32) return launch_fused_pd<T, 32>(pd, A, grid, sm, s, dry);
+  return launch_fused_pd<T, 64>(pd, A, grid, sm, s, dry);
 }
 
 }  // namespace aob
@@ -326,19 +368,28 @@ bool aob_loop::launch_fused(bool noise, cudaStream_t s, bool frame_on_device, bo
   const int nsm = num_sms(w->device);
   const int grid = std::min(nsm, c->nactu);
   A.rows_per_cta = (c->nactu + grid - 1) / grid;
-  const int wps = fused_wps > 0 ? fused_wps : 1;
-  const int groups = FUSED_THREADS / (32 * wps);
-  const ShSmem L(w->nfft, w->nu, w->nv, w->nphase, w->nrebin * w->nrebin * w->npix * w->npix, w->npix * w->npix, wps);
-  const size_t sm = 128 * ((A.rows_per_cta * 8 + 127) / 128) + (size_t)A.rows_per_cta * A.ld * esize +
-                    L.bytes(groups) + sizeof(float) * fused_slope_floats(A.ld, V);
+  // sub-apertures per CTA and round: the CTA's whole share if shared memory allows
+  const size_t fixed = fused_bars_bytes(A.rows_per_cta) + fused_pre_bytes(A.rows_per_cta) +
+                       (size_t)A.rows_per_cta * A.ld * esize + sizeof(float) * fused_slope_floats(A.ld, V);
+  const int npix2 = w->npix * w->npix;
+  const int share = (w->nvalid + grid - 1) / grid;
+  int batch = fused_batch > 0 ? std::min(fused_batch, share) : share;
+  auto smem_for = [&](int b) {
+    const ShSmem L(w->nfft, w->nu, w->nv, w->nphase, w->nrebin * w->nrebin * npix2, npix2, b);
+    // the sensor work area holds the MVM's per-warp partial sums afterwards
+    return fixed + std::max(L.bytes(), L.hdr + sizeof(float) * (FUSED_THREADS / 32) * A.rows_per_cta);
+  };
+  while (batch > 1 && smem_for(batch) > 227 * 1024) --batch;
+  A.batch = std::max(batch, 1);
+  const size_t sm = smem_for(A.batch);
   if (sm > 227 * 1024) return false;
   bool ok;
   if (c->prec == AOB_PREC_F32)
-    ok = launch_fused_n<float>(w->nfft, wps, w->nphase, A, grid, sm, s, dry);
+    ok = launch_fused_n<float>(w->nfft, w->nphase, A, grid, sm, s, dry);
   else if (c->prec == AOB_PREC_BF16)
-    ok = launch_fused_n<__nv_bfloat16>(w->nfft, wps, w->nphase, A, grid, sm, s, dry);
+    ok = launch_fused_n<__nv_bfloat16>(w->nfft, w->nphase, A, grid, sm, s, dry);
   else
-    ok = launch_fused_n<__nv_fp8_e4m3>(w->nfft, wps, w->nphase, A, grid, sm, s, dry);
+    ok = launch_fused_n<__nv_fp8_e4m3>(w->nfft, w->nphase, A, grid, sm, s, dry);
   if (!ok || dry) return ok;
   AOB_LAUNCH_CHECK("rtc_fused_kernel");
   w->after_image(A.sh, fc, false);

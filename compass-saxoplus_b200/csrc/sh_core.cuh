@@ -1,20 +1,25 @@
-// Per-sub-aperture Shack-Hartmann image formation, shared by the standalone
-// sensor kernel (sh_wfs.cu) and the fused RTC kernel (rtc_fused.cu).
+// Shack-Hartmann image formation for a batch of sub-apertures, shared by the
+// standalone sensor kernel (sh_wfs.cu) and the fused RTC kernel (rtc_fused.cu).
 //
-// A group of WPS warps owns one sub-aperture: field in shared memory, pruned
-// separable DFT at the frequencies binmap reads, |E|^2, binning, flux
-// normalisation, Philox-keyed photon/readout noise, cube/image writes and the
-// CoG-family centroid.  Every global load a sub-aperture needs is issued at
-// the top of the routine, before the first barrier, so that one memory round
-// trip (plus the index -> phase dependency) is paid per sub-aperture instead of
-// one per stage.
+// Every thread of the CTA works on the whole batch at once, stage by stage:
+//   0. per-sub-aperture metadata (phase window, flux, image position, refs)
+//   1. complex field  pupil * exp(i (phase * 2 pi / lambda - offset))
+//   2. DFT along x at the nu frequencies binmap reads
+//   3. DFT along y at the nv frequencies binmap reads, |.|^2
+//   4. binning through the compact binmap and the flux per sub-aperture
+//      (one warp per sub-aperture, fixed summation order)
+//   5. normalisation, Philox photon / readout noise, cube + image writes,
+//      centroid weights
+//   6. CoG-family centroid per sub-aperture (one warp each, fixed order)
+// so a CTA pays each stage's latency once for the batch instead of once per
+// sub-aperture.  The reductions run in an order that does not depend on the
+// batch size or the CTA size: the standalone and the fused kernels give
+// bit-identical images and slopes.
 #pragma once
 
 #include "aob_common.cuh"
 
 namespace aob {
-
-constexpr int SH_MAX_PPL = 8;  // binned pixels per warp lane -> npix^2 <= 256
 
 struct ShKernelArgs {
   const float *phase;
@@ -30,6 +35,7 @@ struct ShKernelArgs {
   const int32_t *ulist;
   const int32_t *vlist;
   const int32_t *cbin;  // [nrebin2, npix^2] indexes into the nu x nv intensity tile
+  const float2 *wxy;    // per-geometry twiddles: WX[a][x] (nu x pdiam) then WY[b][y] (nv x pdiam)
   const float *flux;
   float nphot;
   float *bincube;
@@ -43,6 +49,8 @@ struct ShKernelArgs {
   uint32_t frame, k0, k1;
   const uint32_t *frame_ptr;  // when set, the frame number is read from device memory
   NoiseTables tables;
+  // magic multipliers for the runtime divisions (see udiv)
+  uint32_t mg_pd, mg_pd2, mg_nu, mg_nupd, mg_nunv, mg_np, mg_np2;
   // fused centroider (kind < 0: none)
   int ckind;
   float c_scale, c_offset, c_thresh;
@@ -54,42 +62,37 @@ struct ShKernelArgs {
   float *c_intens;
 };
 
-// i / d for 0 <= i < 4096 and 0 < d < 256 with magic = floor(2^20 / d) + 1
-__device__ __forceinline__ int fdiv(int i, uint32_t magic) { return (int)(((uint32_t)i * magic) >> 20); }
-
-// Named barrier per group of WPS warps (barrier 0 is __syncthreads).
-template <int WPS>
-__device__ __forceinline__ void group_sync(int group) {
-  if (WPS == 1)
-    __syncwarp();
-  else
-    asm volatile("bar.sync %0, %1;" ::"r"(group + 1), "r"(WPS * 32) : "memory");
+// i / d for i * d < 2^32 with magic = floor(2^32 / d) + 1 (d >= 2).
+__host__ __device__ inline uint32_t udiv_magic(uint32_t d) {
+  return (uint32_t)((0x100000000ull / (uint64_t)d) + 1ull);
 }
+__device__ __forceinline__ int udiv(int i, uint32_t magic) { return (int)__umulhi((uint32_t)i, magic); }
 
-// Sum over the group; every thread of the group gets the result.
-template <int WPS>
-__device__ __forceinline__ float group_sum(float v, float *red, int gw, int lane, int group) {
-  v = warp_sum(v);
-  if (WPS == 1) return v;
-  if (lane == 0) red[gw] = v;
-  group_sync<WPS>(group);
-  float t = 0.f;
-#pragma unroll
-  for (int i = 0; i < WPS; ++i) t += red[i];
-  group_sync<WPS>(group);
-  return t;
-}
-
-// Shared-memory layout: CTA-wide tables, then one scratch area per group.
+// Shared-memory layout: CTA-wide tables, then the batch work area.
 struct ShSmem {
-  size_t hdr, per_grp;
+  size_t wxy, lf, hdr;                          // twiddle and log(k!) table offsets, header size
+  size_t meta, E, Gt, I, bins, dw, per_batch;   // offsets within the work area
   __host__ __device__ static size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
-  __host__ __device__ ShSmem(int nfft, int nu, int nv, int pd, int ncb, int npix2, int wps) {
-    hdr = align16(sizeof(float2) * nfft + sizeof(int32_t) * (2 * nfft + ncb) + sizeof(float) * npix2);
-    per_grp = align16((size_t)(pd * pd + nu * pd) * sizeof(float2) + (size_t)nu * nv * sizeof(float) +
-                      4 * wps * sizeof(float));
+  __host__ __device__ ShSmem(int nfft, int nu, int nv, int pd, int ncb, int npix2, int S) {
+    wxy = align16(sizeof(float2) * nfft + sizeof(int32_t) * (2 * nfft + ncb) + sizeof(float) * npix2);
+    lf = align16(wxy + sizeof(float2) * (size_t)(nu + nv) * pd);
+    hdr = align16(lf + sizeof(double) * AOB_LOGFACT_SMEM);
+    size_t o = 0;
+    meta = o;
+    o += align16(sizeof(int32_t) * 8 * (size_t)S);
+    E = o;
+    o += align16(sizeof(float2) * (size_t)S * pd * pd);
+    Gt = o;
+    o += align16(sizeof(float2) * (size_t)S * nu * pd);
+    I = o;
+    o += align16(sizeof(float) * (size_t)S * nu * nv);
+    bins = o;
+    o += align16(sizeof(float) * (size_t)S * npix2);
+    dw = o;
+    o += align16(sizeof(float) * (size_t)S * npix2);
+    per_batch = o;
   }
-  __host__ __device__ size_t bytes(int groups) const { return hdr + per_grp * groups; }
+  __host__ __device__ size_t bytes() const { return hdr + per_batch; }
 };
 
 // CTA-cooperative load of the tables (caller synchronises afterwards).
@@ -108,173 +111,270 @@ __device__ __forceinline__ void sh_load_tables(const ShKernelArgs &P, unsigned c
   for (int i = tid; i < ncb; i += nthreads) cb[i] = P.cbin[i];
   if (P.ckind == 2 && !P.c_wper)
     for (int i = tid; i < npix2; i += nthreads) wt[i] = P.c_weights[i];
+  const ShSmem L(NFFT, P.nu, P.nv, P.pdiam, ncb, npix2, 1);
+  float2 *wxy = reinterpret_cast<float2 *>(smem + L.wxy);
+  for (int i = tid; i < (P.nu + P.nv) * P.pdiam; i += nthreads) wxy[i] = P.wxy[i];
+  if (P.noise_mode >= 1) {
+    double *lf = reinterpret_cast<double *>(smem + L.lf);
+    for (int i = tid; i < AOB_LOGFACT_SMEM; i += nthreads) lf[i] = P.tables.logfact[i];
+  }
 }
 
-// One sub-aperture k processed by one group (gt = thread index in the group).
-template <int NFFT, int WPS, int PD>
-__device__ __forceinline__ void sh_subap(const ShKernelArgs &P, int k, const unsigned char *tables,
-                                         unsigned char *scratch, int group, int gt) {
-  constexpr int GT = WPS * 32;
-  constexpr int PPT = (32 * SH_MAX_PPL) / GT;  // binned pixels per thread
-  constexpr int FPT = PD > 0 ? (PD * PD + GT - 1) / GT : 1;
-  const int lane = gt & 31, gw = gt >> 5;
+// Sub-apertures k = base + s * stride for s < S, processed by the whole CTA.
+// Must be called by every thread of the CTA (it synchronises internally); the
+// caller guarantees base + (S - 1) * stride < nvalid.  On return the work area
+// may be reused.
+template <int NFFT, int PD>
+__device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int stride, int S,
+                                         const unsigned char *tables, unsigned char *work, const ShSmem &L) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   const float2 *tw = reinterpret_cast<const float2 *>(tables);
   const int32_t *ul = reinterpret_cast<const int32_t *>(tw + NFFT);
   const int32_t *vl = ul + NFFT;
   const int32_t *cb = vl + NFFT;
-  const int npix2 = P.npix * P.npix;
-  const float *wt = reinterpret_cast<const float *>(cb + P.nrebin2 * npix2);
+  const int npix = P.npix, npix2 = npix * npix, nr2 = P.nrebin2;
+  const float *wt = reinterpret_cast<const float *>(cb + nr2 * npix2);
+  const double *lf = reinterpret_cast<const double *>(tables + L.lf);
+  const int nu = P.nu, nv = P.nv;
   const int pd = PD > 0 ? PD : P.pdiam;
-  const int pd2 = pd * pd;
-  float2 *E = reinterpret_cast<float2 *>(scratch);
-  float2 *Gt = E + pd2;
-  float *I = reinterpret_cast<float *>(Gt + P.nu * pd);
-  float *red = I + P.nu * P.nv;
-  const uint32_t mg_pd = (1u << 20) / pd + 1, mg_nu = (1u << 20) / P.nu + 1, mg_np = (1u << 20) / P.npix + 1;
+  const int pd2 = pd * pd, nupd = nu * pd, nunv = nu * nv;
 
-  // ---- all per-sub-aperture global loads first ----
-  const int px = P.puppixx[k], py = P.puppixy[k];
-  const float fk = P.flux[k];
-  const int vx = P.validsubsx[k], vy = P.validsubsy[k];
-  const int ix = P.c_order ? 2 * k : k;
-  const int iy = P.c_order ? 2 * k + 1 : k + P.nvalid;
-  float refx = 0.f, refy = 0.f;
-  if (P.ckind >= 0 && gt == 0) {
-    refx = P.c_ref[ix];
-    refy = P.c_ref[iy];
-  }
-  const uint32_t frame = P.frame_ptr ? *P.frame_ptr : P.frame;
-  float wpix[PPT];
-  if (P.ckind == 2) {
-#pragma unroll
-    for (int j = 0; j < PPT; ++j) {
-      const int p = gt + GT * j;
-      wpix[j] = (p < npix2) ? (P.c_wper ? P.c_weights[p + k * npix2] : wt[p]) : 0.f;
+  int32_t *m_px = reinterpret_cast<int32_t *>(work + L.meta);
+  int32_t *m_py = m_px + S;
+  int32_t *m_vx = m_py + S;
+  int32_t *m_vy = m_vx + S;
+  float *m_fl = reinterpret_cast<float *>(m_vy + S);
+  float *m_tot = m_fl + S;
+  float *m_rx = m_tot + S;
+  float *m_ry = m_rx + S;
+  float2 *E = reinterpret_cast<float2 *>(work + L.E);
+  float2 *Gt = reinterpret_cast<float2 *>(work + L.Gt);
+  float *I = reinterpret_cast<float *>(work + L.I);
+  float *bins = reinterpret_cast<float *>(work + L.bins);
+  float *dw = reinterpret_cast<float *>(work + L.dw);
+
+  // ---- 0. metadata of the batch (one global round trip for all of it) ----
+  if (tid < S) {
+    const int k = base + tid * stride;
+    m_px[tid] = P.puppixx[k];
+    m_py[tid] = P.puppixy[k];
+    m_vx[tid] = P.validsubsx[k];
+    m_vy[tid] = P.validsubsy[k];
+    m_fl[tid] = P.flux[k];
+    if (P.ckind >= 0) {
+      m_rx[tid] = P.c_ref[P.c_order ? 2 * k : k];
+      m_ry[tid] = P.c_ref[P.c_order ? 2 * k + 1 : k + P.nvalid];
     }
   }
-  // 1. complex field: pupil * exp(i (phase*2pi/lambda - offset))
-  if (PD > 0) {
-    float ph[FPT], am[FPT], of[FPT];
+  const uint32_t frame = P.frame_ptr ? *P.frame_ptr : P.frame;
+  __syncthreads();
+
+  // ---- 1. complex field: loads of up to 4 elements issued before any use ----
+  const int nE = S * pd2;
+  for (int i0 = tid; i0 < nE; i0 += 4 * nt) {
+    float ph[4], am[4], of[4];
 #pragma unroll
-    for (int j = 0; j < FPT; ++j) {
-      const int i = gt + GT * j;
-      if (i < pd2) {
-        const int y = fdiv(i, mg_pd), x = i - y * pd;
-        const int id = (x + px) + (y + py) * P.npup;
+    for (int j = 0; j < 4; ++j) {
+      const int i = i0 + j * nt;
+      if (i < nE) {
+        const int s = PD > 0 ? i / (PD * PD) : udiv(i, P.mg_pd2);
+        const int l = i - s * pd2;
+        const int y = PD > 0 ? l / PD : udiv(l, P.mg_pd);
+        const int x = l - y * pd;
+        const int id = (x + m_px[s]) + (y + m_py[s]) * P.npup;
         ph[j] = P.phase[id];
         am[j] = P.pupil[id];
-        of[j] = P.offsets[i];
+        of[j] = P.offsets[l];
       }
     }
 #pragma unroll
-    for (int j = 0; j < FPT; ++j) {
-      const int i = gt + GT * j;
-      if (i < pd2) {
+    for (int j = 0; j < 4; ++j) {
+      const int i = i0 + j * nt;
+      if (i < nE) {
         float sn, cs;
         sincosf(ph[j] * P.scale - of[j], &sn, &cs);
         E[i] = make_float2(cs * am[j], sn * am[j]);
       }
     }
+  }
+  __syncthreads();
+
+  if constexpr (PD > 0) {
+    // Register-blocked DFTs: a thread keeps one input row (column) in registers
+    // and produces ACH (BCH) outputs from it, with the per-geometry twiddles
+    // WX / WY; lanes of a warp share the output chunk, so twiddle reads are
+    // broadcasts.  Each output accumulates over the input in the same order as
+    // the generic path below.
+    constexpr int ACH = 3, BCH = 6;
+    const float2 *WX = reinterpret_cast<const float2 *>(tables + L.wxy);
+    const float2 *WY = WX + nu * PD;
+    // ---- 2. DFT along x: Gt[y][s * nu + a] = sum_x E[s][y][x] WX[a][x] ----
+    const int R = S * PD, Q = S * nu;
+    const int nach = (nu + ACH - 1) / ACH;
+    const uint32_t mgR = udiv_magic((uint32_t)R);
+    for (int i = tid; i < R * nach; i += nt) {
+      const int c = udiv(i, mgR), row = i - c * R;
+      const int sl = row / PD, y = row - sl * PD;
+      float2 ev[PD];
+#pragma unroll
+      for (int x = 0; x < PD; ++x) ev[x] = E[row * PD + x];
+#pragma unroll
+      for (int j = 0; j < ACH; ++j) {
+        const int a = c * ACH + j;
+        if (a < nu) {
+          const float2 *w = WX + a * PD;
+          float re = 0.f, im = 0.f;
+#pragma unroll
+          for (int x = 0; x < PD; ++x) {
+            const float2 wv = w[x], v = ev[x];
+            re = fmaf(v.x, wv.x, fmaf(-v.y, wv.y, re));
+            im = fmaf(v.x, wv.y, fmaf(v.y, wv.x, im));
+          }
+          Gt[y * Q + sl * nu + a] = make_float2(re, im);
+        }
+      }
+    }
+    __syncthreads();
+    // ---- 3. DFT along y and |.|^2: I[s][b][a] ----
+    const int nbch = (nv + BCH - 1) / BCH;
+    const uint32_t mgQ = udiv_magic((uint32_t)Q);
+    for (int i = tid; i < Q * nbch; i += nt) {
+      const int c = udiv(i, mgQ), q = i - c * Q;
+      const int sl = udiv(q, P.mg_nu), a = q - sl * nu;
+      float2 gv[PD];
+#pragma unroll
+      for (int y = 0; y < PD; ++y) gv[y] = Gt[y * Q + q];
+#pragma unroll
+      for (int j = 0; j < BCH; ++j) {
+        const int b = c * BCH + j;
+        if (b < nv) {
+          const float2 *w = WY + b * PD;
+          float re = 0.f, im = 0.f;
+#pragma unroll
+          for (int y = 0; y < PD; ++y) {
+            const float2 wv = w[y], v = gv[y];
+            re = fmaf(v.x, wv.x, fmaf(-v.y, wv.y, re));
+            im = fmaf(v.x, wv.y, fmaf(v.y, wv.x, im));
+          }
+          I[sl * nunv + b * nu + a] = fmaf(re, re, im * im);
+        }
+      }
+    }
+    __syncthreads();
   } else {
-    for (int i = gt; i < pd2; i += GT) {
-      const int y = fdiv(i, mg_pd), x = i - y * pd;
-      const int id = (x + px) + (y + py) * P.npup;
-      float sn, cs;
-      sincosf(P.phase[id] * P.scale - P.offsets[i], &sn, &cs);
-      const float a = P.pupil[id];
-      E[i] = make_float2(cs * a, sn * a);
+    // ---- 2. DFT along x: Gt[s][y][a] = sum_x E[s][y][x] W^(u_a x) ----
+    for (int i = tid; i < S * nupd; i += nt) {
+      const int s = udiv(i, P.mg_nupd);
+      const int r = i - s * nupd;
+      const int y = udiv(r, P.mg_nu), a = r - y * nu;
+      const int ua = ul[a];
+      const float2 *e = E + s * pd2 + y * pd;
+      float re = 0.f, im = 0.f;
+      for (int x = 0; x < pd; ++x) {
+        const float2 w = tw[(ua * x) & (NFFT - 1)], v = e[x];
+        re = fmaf(v.x, w.x, fmaf(-v.y, w.y, re));
+        im = fmaf(v.x, w.y, fmaf(v.y, w.x, im));
+      }
+      Gt[i] = make_float2(re, im);
     }
-  }
-  group_sync<WPS>(group);
-  // 2. DFT along x at the needed kx: G[a, y] = sum_x E[x, y] W^(u_a x)
-  for (int i = gt; i < P.nu * pd; i += GT) {
-    const int y = fdiv(i, mg_nu), a = i - y * P.nu;
-    const int ua = ul[a];
-    const float2 *e = E + y * pd;
-    float re = 0.f, im = 0.f;
-#pragma unroll
-    for (int x = 0; x < (PD > 0 ? PD : 32); ++x) {
-      if (PD == 0 && x >= pd) break;
-      const float2 w = tw[(ua * x) & (NFFT - 1)], v = e[x];
-      re = fmaf(v.x, w.x, fmaf(-v.y, w.y, re));
-      im = fmaf(v.x, w.y, fmaf(v.y, w.x, im));
+    __syncthreads();
+    // ---- 3. DFT along y and |.|^2: I[s][b][a] ----
+    for (int i = tid; i < S * nunv; i += nt) {
+      const int s = udiv(i, P.mg_nunv);
+      const int r = i - s * nunv;
+      const int b = udiv(r, P.mg_nu), a = r - b * nu;
+      const int vb = vl[b];
+      const float2 *g = Gt + s * nupd + a;
+      float re = 0.f, im = 0.f;
+      for (int y = 0; y < pd; ++y) {
+        const float2 w = tw[(vb * y) & (NFFT - 1)], v = g[y * nu];
+        re = fmaf(v.x, w.x, fmaf(-v.y, w.y, re));
+        im = fmaf(v.x, w.y, fmaf(v.y, w.x, im));
+      }
+      I[i] = fmaf(re, re, im * im);
     }
-    Gt[i] = make_float2(re, im);
+    __syncthreads();
   }
-  group_sync<WPS>(group);
-  // 3. DFT along y at the needed ky and |.|^2: I[a, b]
-  for (int i = gt; i < P.nu * P.nv; i += GT) {
-    const int b = fdiv(i, mg_nu), a = i - b * P.nu;
-    const int vb = vl[b];
-    float re = 0.f, im = 0.f;
-#pragma unroll
-    for (int y = 0; y < (PD > 0 ? PD : 32); ++y) {
-      if (PD == 0 && y >= pd) break;
-      const float2 w = tw[(vb * y) & (NFFT - 1)], v = Gt[a + y * P.nu];
-      re = fmaf(v.x, w.x, fmaf(-v.y, w.y, re));
-      im = fmaf(v.x, w.y, fmaf(v.y, w.x, im));
-    }
-    I[i] = fmaf(re, re, im * im);
-  }
-  group_sync<WPS>(group);
-  // 4. binning and per-sub-aperture flux
-  float bv[PPT];
-  float part = 0.f;
-#pragma unroll
-  for (int j = 0; j < PPT; ++j) {
-    const int p = gt + GT * j;
-    float v = 0.f;
-    if (p < npix2) {
-      const int32_t *c = cb + p * P.nrebin2;
+
+  const int nP = S * npix2;
+  // ---- 4. binning and flux: one warp per sub-aperture; the flux is summed as
+  //      lane-strided partial sums, then a butterfly ----
+  for (int s = warp; s < S; s += nw) {
+    const float *Is = I + s * nunv;
+    float part = 0.f;
+    for (int p = lane; p < npix2; p += 32) {
+      const int32_t *c = cb + p * nr2;
       float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
       int r = 0;
-      for (; r + 3 < P.nrebin2; r += 4) {
-        v0 += I[c[r]];
-        v1 += I[c[r + 1]];
-        v2 += I[c[r + 2]];
-        v3 += I[c[r + 3]];
+      for (; r + 3 < nr2; r += 4) {
+        v0 += Is[c[r]];
+        v1 += Is[c[r + 1]];
+        v2 += Is[c[r + 2]];
+        v3 += Is[c[r + 3]];
       }
-      for (; r < P.nrebin2; ++r) v0 += I[c[r]];
-      v = (v0 + v1) + (v2 + v3);
+      for (; r < nr2; ++r) v0 += Is[c[r]];
+      const float v = (v0 + v1) + (v2 + v3);
+      bins[s * npix2 + p] = v;
+      part += v;
     }
-    bv[j] = v;
-    part += v;
-  }
-  const float tot = group_sum<WPS>(part, red, gw, lane, group);
-  if (gt == 0) P.intensities[k] = tot;
-  // 5. normalise, noise, write cube + image, centroid partial sums
-  float cs = 0.f, cx = 0.f, cy = 0.f;
-#pragma unroll
-  for (int j = 0; j < PPT; ++j) {
-    const int p = gt + GT * j;
-    if (p < npix2) {
-      float v = bv[j];
-      if (tot != 0.f) v = v * fk / tot * P.nphot;
-      const uint32_t pix = (uint32_t)(p + k * npix2);
-      if (P.noise_mode >= 1) v = (float)poisson_sample((double)v, pix, frame, P.k0, P.k1, P.tables);
-      if (P.noise_mode >= 2) v = v + P.noise * gauss_sample(pix, frame, P.k0, P.k1);
-      P.bincube[pix] = v;
-      const int y = fdiv(p, mg_np), x = p - y * P.npix;
-      P.binimg[(x + vx) + (y + vy) * P.img_size] = v;
-      float d = v;
-      if (P.ckind == 1 || P.ckind == 2) d = (v > P.c_thresh) ? v - P.c_thresh : 1.e-6f;
-      if (P.ckind == 2) d *= wpix[j];
-      cs += d;
-      cx = fmaf(d, (float)x, cx);
-      cy = fmaf(d, (float)y, cy);
+    part = warp_sum(part);
+    if (lane == 0) {
+      m_tot[s] = part;
+      P.intensities[base + s * stride] = part;
     }
   }
+  __syncthreads();
+
+  // ---- 5. normalise, noise, cube + image, centroid weights ----
+  for (int i = tid; i < nP; i += nt) {
+    const int s = udiv(i, P.mg_np2), p = i - s * npix2;
+    const int k = base + s * stride;
+    float wgt = 1.f;
+    if (P.ckind == 2) wgt = P.c_wper ? P.c_weights[p + k * npix2] : wt[p];
+    float v = bins[i];
+    const float tot = m_tot[s];
+    if (tot != 0.f) v = v * m_fl[s] / tot * P.nphot;
+    const uint32_t pix = (uint32_t)(p + k * npix2);
+    if (P.noise_mode >= 1) {
+      const U4 w0 = philox4x32_10(U4{pix, frame, TAG_POISSON, 0u}, P.k0, P.k1);
+      v = poisson_sample(v, w0, pix, frame, P.k0, P.k1, lf, P.tables);
+      if (P.noise_mode >= 2) v = v + P.noise * gauss_sample(w0);
+    }
+    P.bincube[pix] = v;
+    const int y = udiv(p, P.mg_np), x = p - y * npix;
+    P.binimg[(x + m_vx[s]) + (y + m_vy[s]) * P.img_size] = v;
+    float d = v;
+    if (P.ckind == 1 || P.ckind == 2) d = (v > P.c_thresh) ? v - P.c_thresh : 1.e-6f;
+    dw[i] = d * wgt;
+  }
+  __syncthreads();
+
+  // ---- 6. centroids ----
   if (P.ckind >= 0) {
-    cs = group_sum<WPS>(cs, red + WPS, gw, lane, group);
-    cx = group_sum<WPS>(cx, red + 2 * WPS, gw, lane, group);
-    cy = group_sum<WPS>(cy, red + 3 * WPS, gw, lane, group);
-    if (gt == 0) {
-      P.c_slopes[ix] = (cx / (cs + 1.e-6f) - P.c_offset) * P.c_scale - refx;
-      P.c_slopes[iy] = (cy / (cs + 1.e-6f) - P.c_offset) * P.c_scale - refy;
-      P.c_intens[k] = cs;
+    for (int s = warp; s < S; s += nw) {
+      float cs = 0.f, cx = 0.f, cy = 0.f;
+      for (int p = lane; p < npix2; p += 32) {
+        const float d = dw[s * npix2 + p];
+        const int y = udiv(p, P.mg_np), x = p - y * npix;
+        cs += d;
+        cx = fmaf(d, (float)x, cx);
+        cy = fmaf(d, (float)y, cy);
+      }
+      cs = warp_sum(cs);
+      cx = warp_sum(cx);
+      cy = warp_sum(cy);
+      if (lane == 0) {
+        const int k = base + s * stride;
+        const int ix = P.c_order ? 2 * k : k;
+        const int iy = P.c_order ? 2 * k + 1 : k + P.nvalid;
+        P.c_slopes[ix] = (cx / (cs + 1.e-6f) - P.c_offset) * P.c_scale - m_rx[s];
+        P.c_slopes[iy] = (cy / (cs + 1.e-6f) - P.c_offset) * P.c_scale - m_ry[s];
+        P.c_intens[k] = cs;
+      }
     }
   }
-  group_sync<WPS>(group);
+  __syncthreads();
 }
 
 }  // namespace aob

@@ -10,8 +10,9 @@
 // scatter (bimg_krnl, sutra_wfs.cu:183-229).  The padded cube (2.5 MB at 40x40)
 // is written and re-read several times.
 //
-// Here one warp owns one sub-aperture from phase to pixels:
-//  * the pdiam x pdiam field is built in shared memory (the Nfft^2 - pdiam^2
+// Here one kernel forms the whole image; each CTA takes a batch of
+// sub-apertures through the stages of sh_core.cuh with all its threads:
+//  * the pdiam x pdiam fields are built in shared memory (the Nfft^2 - pdiam^2
 //    zero padding is never materialised);
 //  * the 2-D DFT is evaluated only at the spatial frequencies that binmap
 //    reads (an nu x nv subset of the Nfft x Nfft grid, found on the host from
@@ -19,8 +20,8 @@
 //    same transform as the reference's forward cuFFT, pruned on both input
 //    and output;
 //  * binning, normalisation, Philox-keyed Poisson/readout noise, the bincube
-//    and image writes, and (optionally) the CoG/tCoG/wCoG centroid of the
-//    sub-aperture happen in registers before the warp moves on.
+//    and image writes, and (optionally) the CoG/tCoG/wCoG centroids follow in
+//    shared memory.
 // HBM traffic per image is the phase and pupil samples read once, the cube,
 // image and slopes written once.
 
@@ -35,24 +36,23 @@
 
 namespace aob {
 
-constexpr int SH_WARPS = 4;  // warps per CTA of the standalone sensor kernel
+constexpr int SH_THREADS = 256;  // threads per CTA of the standalone sensor kernel
+constexpr int SH_MAX_BATCH = 32;
 
 // PD > 0: phase-grid side known at compile time (the DFT loops unroll and all
 // their shared-memory loads issue back to back); PD == 0: runtime side.
-template <int NFFT, int WPS, int PD>
-__global__ void __launch_bounds__(SH_WARPS * 32, 4) sh_image_kernel(ShKernelArgs P) {
-  constexpr int GT = WPS * 32;
-  constexpr int GROUPS = SH_WARPS / WPS;
+// Sub-apertures k = blockIdx.x + (r * S + s) * gridDim.x, s < S, rounds r.
+template <int NFFT, int PD>
+__global__ void __launch_bounds__(SH_THREADS) sh_image_kernel(ShKernelArgs P, int S) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int pd = PD > 0 ? PD : P.pdiam;
-  const ShSmem L(NFFT, P.nu, P.nv, pd, P.nrebin2 * P.npix * P.npix, P.npix * P.npix, WPS);
+  const ShSmem L(NFFT, P.nu, P.nv, pd, P.nrebin2 * P.npix * P.npix, P.npix * P.npix, S);
   sh_load_tables<NFFT>(P, smem, threadIdx.x, blockDim.x);
-  __syncthreads();
-  const int group = threadIdx.x / GT;
-  const int gt = threadIdx.x - group * GT;
-  unsigned char *scratch = smem + L.hdr + L.per_grp * group;
-  for (int k = blockIdx.x * GROUPS + group; k < P.nvalid; k += gridDim.x * GROUPS)
-    sh_subap<NFFT, WPS, PD>(P, k, smem, scratch, group, gt);
+  // (sh_batch synchronises before the tables are first read)
+  for (int base = blockIdx.x; base < P.nvalid; base += S * gridDim.x) {
+    const int Sb = min(S, (P.nvalid - base + (int)gridDim.x - 1) / (int)gridDim.x);
+    sh_batch<NFFT, PD>(P, base, gridDim.x, Sb, smem, smem + L.hdr, L);
+  }
 }
 
 __global__ void sh_fill_image_kernel(float *img, const float *cube, const int32_t *vx,
@@ -76,7 +76,7 @@ aob_sh::aob_sh(int device_, int nxsub_, int nvalid_, int npix_, int nphase_, int
   AOB_REQUIRE(nfft == 16 || nfft == 32 || nfft == 64, "sh: nfft must be 16, 32 or 64");
   AOB_REQUIRE(ntot == nfft, "sh: extended field of view (ntot != nfft) is not supported");
   AOB_REQUIRE(nphase <= nfft && nphase <= 32, "sh: nphase must be <= min(nfft, 32)");
-  AOB_REQUIRE(npix * npix <= 32 * SH_MAX_PPL, "sh: npix^2 must be <= 256");
+  AOB_REQUIRE(npix >= 2 && nphase >= 2, "sh: npix and nphase must be >= 2");
   AOB_REQUIRE(nphase * nphase < 4096 && nfft * nfft <= 4096, "sh: sizes beyond the index arithmetic range");
   AOB_REQUIRE((int64_t)nxsub * npix < (1 << 15), "sh: image too large");
   AOB_CUDA(cudaSetDevice(device));
@@ -93,10 +93,9 @@ aob_sh::aob_sh(int device_, int nxsub_, int nvalid_, int npix_, int nphase_, int
   binimg.alloc((int64_t)npix * nxsub * npix * nxsub);
   intensities.alloc(nvalid);
   slopes.alloc(2 * (int64_t)nvalid);
-  // noise tables: log(k!) as cumulative sums of log(i), and 1/k (same as the CPU oracle)
-  std::vector<double> lf(AOB_LOGFACT_N, 0.0), rkh(AOB_RK_N, 0.0);
+  // noise table: log(k!) as cumulative sums of log(i) (same as the CPU oracle)
+  std::vector<double> lf(AOB_LOGFACT_N, 0.0);
   for (int k = 1; k < AOB_LOGFACT_N; ++k) lf[k] = lf[k - 1] + std::log((double)k);
-  for (int k = 1; k < AOB_RK_N; ++k) rkh[k] = 1.0 / (double)k;
   std::vector<float> tw(2 * nfft);
   for (int m = 0; m < nfft; ++m) {
     const double ang = 2.0 * M_PI * (double)m / (double)nfft;
@@ -107,8 +106,6 @@ aob_sh::aob_sh(int device_, int nxsub_, int nvalid_, int npix_, int nphase_, int
   twiddle.upload(tw.data(), 2 * nfft);
   logfact.alloc(AOB_LOGFACT_N);
   logfact.upload(lf.data(), AOB_LOGFACT_N);
-  rk.alloc(AOB_RK_N);
-  rk.upload(rkh.data(), AOB_RK_N);
 }
 
 void aob_sh::load_arrays(const int32_t *h_binmap, const float *h_offsets, const float *h_flux,
@@ -142,11 +139,26 @@ void aob_sh::load_arrays(const int32_t *h_binmap, const float *h_offsets, const 
   }
   nu = (int)U.size();
   nv = (int)V.size();
+  AOB_REQUIRE(nu >= 2 && nv >= 2, "sh.load_arrays: binmap reads fewer than 2 frequencies along an axis");
   std::vector<int32_t> C(nr2 * np2);
   for (int i = 0; i < nr2 * np2; ++i) {
     const int m = h_binmap[i];
     C[i] = usex[m % nfft] + usey[m / nfft] * nu;
   }
+  // per-geometry twiddles WX[a][x] = W^(U[a] x), WY[b][y] = W^(V[b] y): the same
+  // float values as the nfft-point table, gathered so the DFT loops need no index math
+  std::vector<float> W(2 * (size_t)(nu + nv) * nphase);
+  auto tw = [&](int m, float *out) {
+    const double ang = 2.0 * M_PI * (double)(m % nfft) / (double)nfft;
+    out[0] = (float)std::cos(ang);
+    out[1] = (float)-std::sin(ang);
+  };
+  for (int a = 0; a < nu; ++a)
+    for (int x = 0; x < nphase; ++x) tw(U[a] * x, &W[2 * ((size_t)a * nphase + x)]);
+  for (int b = 0; b < nv; ++b)
+    for (int y = 0; y < nphase; ++y) tw(V[b] * y, &W[2 * ((size_t)(nu + b) * nphase + y)]);
+  wxy.alloc((int64_t)W.size());
+  wxy.upload(W.data(), (int64_t)W.size());
   ulist.alloc(nu);
   vlist.alloc(nv);
   cbin.alloc((int64_t)nr2 * np2);
@@ -160,58 +172,45 @@ void aob_sh::load_arrays(const int32_t *h_binmap, const float *h_offsets, const 
   validsubsy.upload(h_vy, nvalid);
   istart.upload(h_istart, nvalid);
   jstart.upload(h_jstart, nvalid);
-  AOB_REQUIRE(smem_bytes(4) <= 200 * 1024, "sh: shared-memory footprint too large for this geometry");
+  AOB_REQUIRE(smem_bytes(1) <= 200 * 1024, "sh: shared-memory footprint too large for this geometry");
   loaded = true;
 }
 
-size_t aob_sh::smem_bytes(int wps) const {
-  const ShSmem L(nfft, nu, nv, nphase, nrebin * nrebin * npix * npix, npix * npix, wps);
-  return L.bytes(SH_WARPS / wps);
+size_t aob_sh::smem_bytes(int batch) const {
+  const ShSmem L(nfft, nu, nv, nphase, nrebin * nrebin * npix * npix, npix * npix, batch);
+  return L.bytes();
 }
 
-// Warps per sub-aperture: the autotuner's choice if set, otherwise enough to
-// give every SM at least ~24 resident warps.
-int aob_sh::pick_wps() const {
-  if (wps_override == 1 || wps_override == 2 || wps_override == 4) return wps_override;
-  const int nsm = num_sms(device);
-  if (nvalid >= 24 * nsm) return 1;
-  if (nvalid >= 12 * nsm) return 2;
-  return 4;
+// Sub-apertures per CTA: the autotuner's choice if set, otherwise enough for
+// about two CTAs per SM in a single wave.
+int aob_sh::pick_batch() const {
+  int b = batch_override > 0 ? batch_override : (nvalid + 2 * num_sms(device) - 1) / (2 * num_sms(device));
+  b = std::max(1, std::min(b, SH_MAX_BATCH));
+  while (b > 1 && smem_bytes(b) > 200 * 1024) --b;
+  return b;
 }
 
-template <int NFFT, int WPS, int PD>
-static void launch_sh(const ShKernelArgs &P, int nvalid, size_t sm, int nsm, cudaStream_t s) {
-  constexpr int GROUPS = SH_WARPS / WPS;
-  int grid = (nvalid + GROUPS - 1) / GROUPS;
-  grid = std::max(1, std::min(grid, nsm * 32));
+template <int NFFT, int PD>
+static void launch_sh(const ShKernelArgs &P, int nvalid, int S, size_t sm, cudaStream_t s) {
+  const int grid = std::max(1, (nvalid + S - 1) / S);
   // the attribute is set once per instantiation (a driver call per launch costs microseconds)
   static size_t configured = 0;
   if (sm > configured) {
-    AOB_CUDA(cudaFuncSetAttribute(sh_image_kernel<NFFT, WPS, PD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    AOB_CUDA(cudaFuncSetAttribute(sh_image_kernel<NFFT, PD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)std::max<size_t>(sm, 48 * 1024)));
     configured = std::max<size_t>(sm, 48 * 1024);
   }
-  sh_image_kernel<NFFT, WPS, PD><<<grid, SH_WARPS * 32, sm, s>>>(P);
-}
-
-template <int NFFT, int WPS>
-static void launch_sh_pd(int pd, const ShKernelArgs &P, int nvalid, size_t sm, int nsm, cudaStream_t s) {
-  switch (pd) {
-    case 4: launch_sh<NFFT, WPS, 4>(P, nvalid, sm, nsm, s); break;
-    case 6: launch_sh<NFFT, WPS, 6>(P, nvalid, sm, nsm, s); break;
-    case 8: launch_sh<NFFT, WPS, 8>(P, nvalid, sm, nsm, s); break;
-    default: launch_sh<NFFT, WPS, 0>(P, nvalid, sm, nsm, s); break;
-  }
+  sh_image_kernel<NFFT, PD><<<grid, SH_THREADS, sm, s>>>(P, S);
 }
 
 template <int NFFT>
-static void launch_sh_n(int wps, const ShKernelArgs &P, int nvalid, size_t sm, int nsm, cudaStream_t s) {
-  if (wps == 1)
-    launch_sh_pd<NFFT, 1>(P.pdiam, P, nvalid, sm, nsm, s);
-  else if (wps == 2)
-    launch_sh_pd<NFFT, 2>(P.pdiam, P, nvalid, sm, nsm, s);
-  else
-    launch_sh_pd<NFFT, 4>(P.pdiam, P, nvalid, sm, nsm, s);
+static void launch_sh_pd(const ShKernelArgs &P, int nvalid, int S, size_t sm, cudaStream_t s) {
+  switch (P.pdiam) {
+    case 4: launch_sh<NFFT, 4>(P, nvalid, S, sm, s); break;
+    case 6: launch_sh<NFFT, 6>(P, nvalid, S, sm, s); break;
+    case 8: launch_sh<NFFT, 8>(P, nvalid, S, sm, s); break;
+    default: launch_sh<NFFT, 0>(P, nvalid, S, sm, s); break;
+  }
 }
 
 void aob_sh::comp_image(bool with_noise, cudaStream_t s) { comp_image_to(with_noise, s, nullptr, nullptr); }
@@ -233,6 +232,7 @@ aob_centro *aob_sh::make_args(bool with_noise, float *slopes_dst, const uint32_t
   P.nu = nu;
   P.nv = nv;
   P.twiddle = reinterpret_cast<const float2 *>(twiddle.p);
+  P.wxy = reinterpret_cast<const float2 *>(wxy.p);
   P.ulist = ulist.p;
   P.vlist = vlist.p;
   P.cbin = cbin.p;
@@ -251,7 +251,14 @@ aob_centro *aob_sh::make_args(bool with_noise, float *slopes_dst, const uint32_t
   P.k0 = (uint32_t)((uint64_t)seed & 0xffffffffu);
   P.k1 = (uint32_t)((uint64_t)seed >> 32);
   P.frame_ptr = frame_ptr;
-  P.tables = NoiseTables{logfact.p, rk.p};
+  P.tables = NoiseTables{logfact.p};
+  P.mg_pd = udiv_magic((uint32_t)nphase);
+  P.mg_pd2 = udiv_magic((uint32_t)(nphase * nphase));
+  P.mg_nu = udiv_magic((uint32_t)nu);
+  P.mg_nupd = udiv_magic((uint32_t)(nu * nphase));
+  P.mg_nunv = udiv_magic((uint32_t)(nu * nv));
+  P.mg_np = udiv_magic((uint32_t)npix);
+  P.mg_np2 = udiv_magic((uint32_t)(npix * npix));
   P.ckind = -1;
   aob_centro *c = fused;
   if (c && c->npix == npix && c->nvalid == nvalid && c->type <= 2 && c->validx.n == nvalid) {
@@ -285,15 +292,14 @@ void aob_sh::comp_image_to(bool with_noise, cudaStream_t s, float *slopes_dst, c
   AOB_CUDA(cudaSetDevice(device));
   ShKernelArgs P;
   aob_centro *c = make_args(with_noise, slopes_dst, frame_ptr, P);
-  const int nsm = num_sms(device);
-  const int wps = pick_wps();
-  const size_t sm = smem_bytes(wps);
+  const int S = pick_batch();
+  const size_t sm = smem_bytes(S);
   if (nfft == 16)
-    launch_sh_n<16>(wps, P, nvalid, sm, nsm, s);
+    launch_sh_pd<16>(P, nvalid, S, sm, s);
   else if (nfft == 32)
-    launch_sh_n<32>(wps, P, nvalid, sm, nsm, s);
+    launch_sh_pd<32>(P, nvalid, S, sm, s);
   else
-    launch_sh_n<64>(wps, P, nvalid, sm, nsm, s);
+    launch_sh_pd<64>(P, nvalid, S, sm, s);
   AOB_LAUNCH_CHECK("sh_image_kernel");
   after_image(P, c, slopes_dst == nullptr);
 }

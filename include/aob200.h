@@ -93,9 +93,9 @@ int aob_sh_buffer(aob_sh *h, const char *which, void **dev_ptr, int64_t *nelem);
 int aob_sh_comp_image(aob_sh *h, int noise, void *stream);
 /* SutraWfsSH::fill_binimage (sutra_wfs_sh.cpp:599-621): re-scatter bincube. */
 int aob_sh_fill_binimage(aob_sh *h, void *stream);
-/* Launch shape of the sensor kernel: warps per sub-aperture (1, 2 or 4;
+/* Launch shape of the sensor kernel: sub-apertures per CTA batch (1..32;
  * 0 = heuristic).  Set by the project's autotuner; results are unchanged. */
-int aob_sh_set_tuning(aob_sh *h, int warps_per_subap);
+int aob_sh_set_tuning(aob_sh *h, int subaps_per_cta);
 /* set_bincube / set_binimg: overwrite from host. */
 int aob_sh_set_bincube(aob_sh *h, const float *host, int64_t n);
 int aob_sh_set_binimg(aob_sh *h, const float *host, int64_t n);
@@ -313,8 +313,9 @@ int aob_loop_use_graph(aob_loop *l, int enable);
 int aob_loop_kernels_per_step(aob_loop *l, int *n);
 /* mode 0 = fused single cooperative kernel when the configuration fits
  * (otherwise three kernels), 1 = always three kernels, 2 = fused only (error
- * if it does not fit); fused_wps = warps per sub-aperture in the fused kernel. */
-int aob_loop_set_mode(aob_loop *l, int mode, int fused_wps);
+ * if it does not fit); fused_batch = at most this many sub-apertures per CTA
+ * and round in the fused kernel (0 = a CTA's whole share in one round). */
+int aob_loop_set_mode(aob_loop *l, int mode, int fused_batch);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

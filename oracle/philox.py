@@ -9,18 +9,24 @@ device.  This replaces the reference's cuRAND XORWOW states
 (libcarma/src.cu/carma_rng.cu:35-141), whose streams cannot be reproduced.
 
 Counter layout used by the sensors (one 128-bit block per pixel and draw):
-  c0 = pixel index, c1 = frame number, c2 = stream tag, c3 = draw number
-  key = (seed & 0xffffffff, seed >> 32)
-Stream tags: 0 = photon (Poisson) noise, 1 = readout (Gaussian) noise.
+  c0 = pixel index, c1 = frame number, c2 = stream tag (0 = sensor noise),
+  c3 = draw number; key = (seed & 0xffffffff, seed >> 32).
+Draw 0 of a pixel gives the first Poisson draw (words 0, 1) and the readout
+noise (words 2, 3); rejected Poisson draws continue with draws 1, 2, ...
+(The turbulence extrusion uses tag 2, c3 = layer.)
 
-Poisson sampling (replaces curand_poisson, carma_rng.cu:135-141):
+Poisson sampling (replaces curand_poisson, carma_rng.cu:135-141), restating
+the device sampler operation for operation:
   lambda < 10: sequential-search inversion (Devroye 1986, ch. X.3) on one
-               uniform, in float64 with no fused multiply-add (1/k from a table);
+               32-bit uniform, in float64 with no fused multiply-add (1/k as
+               the IEEE quotient);
   lambda >= 10: PTRS transformed rejection (Hoermann 1993, "The transformed
-               rejection method for generating Poisson random variables") with
-               its acceptance test in product form and log(k!) from a table of
-               cumulative log sums (two-term Stirling series beyond 4095).
-Gaussian: Box-Muller in float32 on one block (u1 from word 0, u2 from word 2).
+               rejection method for generating Poisson random variables"):
+               the fast acceptance path in float32 on 24-bit uniforms, the
+               exact acceptance test in float64 in product form with log(k!)
+               from a table of cumulative log sums (two-term Stirling series
+               beyond 4095).
+Gaussian: Box-Muller in float32 on words 2 (u1) and 3 (u2) of draw 0.
 """
 
 import math
@@ -34,7 +40,6 @@ W1 = 0xBB67AE85
 MASK = 0xFFFFFFFF
 
 TAG_POISSON = 0
-TAG_GAUSS = 1
 POISSON_SMALL = 10.0
 POISSON_MAX_DRAWS = 64
 
@@ -74,7 +79,8 @@ RK_N = 1024
 
 
 def _tables():
-    """log(k!) by cumulative sums of log(i) and 1/k -- the same tables the device uses."""
+    """log(k!) by cumulative sums of log(i) (the device table) and 1/k (the device computes the
+    same correctly rounded value with __drcp_rn)."""
     lf = [0.0] * LOGFACT_N
     for k in range(1, LOGFACT_N):
         lf[k] = lf[k - 1] + math.log(k)
@@ -96,30 +102,43 @@ def log_factorial(k):
     return r + c
 
 
-def _ptrs(lam, words_of_draw):
-    """PTRS transformed rejection with the acceptance test in product form."""
-    slam = math.sqrt(lam)
-    loglam = math.log(lam)
-    b = 0.931 + 2.53 * slam
-    a = -0.059 + 0.02483 * b
-    invalpha = 1.1239 + 1.1328 / (b + -3.4)
-    vr = 0.9277 + -(3.6224 / (b + -2.0))
-    a2 = 2.0 * a
+F32 = np.float32
+
+
+def _u01f(x):
+    """24-bit uniform ((x >> 8) + 0.5) / 2^24, exact in float32."""
+    return (F32(int(x) >> 8) + F32(0.5)) * F32(5.9604644775390625e-08)
+
+
+def _ptrs(lamf, words_of_draw):
+    """PTRS transformed rejection: float32 fast path, float64 exact test in product form.
+
+    Every float32 operation is a single correctly rounded NumPy float32 scalar
+    operation, in the device's order.
+    """
+    slam = np.sqrt(lamf)
+    b = F32(0.931) + F32(2.53) * slam
+    a = F32(-0.059) + F32(0.02483) * b
+    vr = F32(0.9277) + -(F32(3.6224) / (b + F32(-2.0)))
+    a2 = F32(2.0) * a
+    loglam = math.log(float(lamf))
+    invalpha = 1.1239 + 1.1328 / (float(b) + -3.4)
     for d in range(POISSON_MAX_DRAWS):
         w = words_of_draw(d)
-        u = float(u01(w[0])) + -0.5
-        v = float(u01(w[1]))
-        us = 0.5 + -abs(u)
-        k = math.floor((((a2 / us) + b) * u + lam) + 0.43)
-        if us >= 0.07 and v <= vr:
-            return k
-        if k < 0 or (us < 0.013 and v > us):
+        u = _u01f(w[0]) + F32(-0.5)
+        v = _u01f(w[1])
+        us = F32(0.5) + -abs(u)
+        k = np.floor((((a2 / us) + b) * u + lamf) + F32(0.43))
+        if us >= F32(0.07) and v <= vr:
+            return float(k)
+        if k < 0 or (us < F32(0.013) and v > us):
             continue
-        lhs = (v * invalpha) / ((a / (us * us)) + b)
-        rhs = math.exp(((k * loglam) + -lam) + -log_factorial(k))
+        usd = float(us)
+        lhs = (float(v) * invalpha) / ((float(a) / (usd * usd)) + float(b))
+        rhs = math.exp(((float(k) * loglam) + -float(lamf)) + -log_factorial(float(k)))
         if lhs <= rhs:
-            return k
-    return math.floor(lam + 0.5)
+            return float(k)
+    return float(np.floor(lamf + F32(0.5)))
 
 
 def _inversion(lam, u):
@@ -134,8 +153,8 @@ def _inversion(lam, u):
 
 
 def poisson(lam, index, frame, seed):
-    """Poisson deviates for an array of means ``lam`` at pixel ``index``; float64 out."""
-    lam = np.asarray(lam, dtype=np.float64)
+    """Poisson deviates for an array of float32 means ``lam`` at pixel ``index``; float64 out."""
+    lam = np.asarray(lam, dtype=np.float32)
     index = np.asarray(index, dtype=np.uint64)
     k0, k1 = key_of(seed)
     out = np.zeros(lam.shape, dtype=np.float64)
@@ -144,11 +163,11 @@ def poisson(lam, index, frame, seed):
     w0 = philox4x32(flat_i, frame, TAG_POISSON, 0, k0, k1)
     res = out.ravel()
     for j in range(flat_l.size):
-        m = float(flat_l[j])
-        if not (m > 0.0):
+        m = flat_l[j]
+        if not (m > 0):
             res[j] = 0.0
         elif m < POISSON_SMALL:
-            res[j] = _inversion(m, float(u01(w0[0][j])))
+            res[j] = _inversion(float(m), float(u01(w0[0][j])))
         else:
             ij = int(flat_i[j])
 
@@ -163,12 +182,13 @@ def poisson(lam, index, frame, seed):
 
 
 def gaussian(index, frame, seed):
-    """Standard normal deviates (float32 Box-Muller, 24-bit uniforms) for pixel indices."""
+    """Readout-noise deviates: float32 Box-Muller on words 2 (u1) and 3 (u2) of each
+    pixel's draw-0 Poisson block (24-bit uniforms)."""
     index = np.asarray(index, dtype=np.uint64)
     k0, k1 = key_of(seed)
-    w = philox4x32(index, frame, TAG_GAUSS, 0, k0, k1)
-    u1 = ((w[0] >> np.uint32(8)).astype(np.float32) + np.float32(0.5)) * np.float32(5.9604644775390625e-08)
-    u2 = ((w[2] >> np.uint32(8)).astype(np.float32) + np.float32(0.5)) * np.float32(5.9604644775390625e-08)
+    w = philox4x32(index, frame, TAG_POISSON, 0, k0, k1)
+    u1 = ((w[2] >> np.uint32(8)).astype(np.float32) + np.float32(0.5)) * np.float32(5.9604644775390625e-08)
+    u2 = ((w[3] >> np.uint32(8)).astype(np.float32) + np.float32(0.5)) * np.float32(5.9604644775390625e-08)
     return np.sqrt(np.float32(-2.0) * np.log(u1)) * np.cos(np.float32(2.0 * np.pi) * u2.astype(np.float64)).astype(np.float32)
 
 

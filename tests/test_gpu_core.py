@@ -194,9 +194,12 @@ def test_svd_cmat_matches_numpy(core):
 @pytest.mark.parametrize("mode", [1, 2])
 @pytest.mark.parametrize("graph", [False, True])
 @pytest.mark.parametrize("delay", [0.0, 1.0, 1.4])
-def test_loop_matches_separate_calls(core, graph, delay, mode):
+@pytest.mark.parametrize("fused_batch", [0, 1])
+def test_loop_matches_separate_calls(core, graph, delay, mode, fused_batch):
     """The bound loop -- three kernels (mode 1) or the fused cooperative kernel
-    (mode 2), with or without CUDA-graph replay -- equals the separate calls."""
+    (mode 2, whole share per round or one sub-aperture per round), with or
+    without CUDA-graph replay -- equals the separate calls bit for bit in its
+    slopes and images (every launch shape reduces in the same order)."""
     rng = np.random.default_rng(21)
     g = sh_geometry("sh16")
     nact = 97
@@ -217,12 +220,10 @@ def test_loop_matches_separate_calls(core, graph, delay, mode):
     cm = (rng.standard_normal((nact, 2 * g.nvalid)) * 0.01).astype(np.float32)
     screens = [kolmogorov_screen(g.tel.n, 20.0, seed=s) for s in range(5)]
     w1, c1, l1 = build()
-    w1.set_tuning(1)  # same launch shape (one warp per sub-aperture) as the fused kernel
     c1.attach(w1)
     w2, c2, l2 = build()
-    w2.set_tuning(1)
     loop = core.Loop(w2, c2, l2, graph=graph)
-    loop.set_mode(mode, 1)
+    loop.set_mode(mode, fused_batch)
     v2 = np.zeros(nact, np.float32)
     for it, ph in enumerate(screens):
         w1.set_phase(ph)
@@ -241,15 +242,24 @@ def test_loop_matches_separate_calls(core, graph, delay, mode):
     assert loop.kernels_per_step() == (1 if mode == 2 else 3)
 
 
-@pytest.mark.parametrize("wps", [1, 2, 4])
-def test_sh_launch_shapes_agree(core, wps):
-    """Every autotuner launch shape of the sensor kernel gives the oracle's image."""
-    g, w, phase = _setup(core, "sh40")
-    w.set_tuning(wps)
-    w.comp_image(noise=False)
-    cube = np.array(w.d_bincube).reshape(g.npix * g.npix, g.nvalid, order="F")
+def test_sh_launch_shapes_agree(core):
+    """Every autotuner launch shape of the sensor kernel gives the oracle's image,
+    and all of them the same bits."""
+    g, w, phase = _setup(core, "sh40", noise=0.5, seed=3)
     ocube, _, _ = osh.comp_image(phase, g.tel.mpupil, g, 2 * np.pi / g.wavelength_um, g.nphotons)
-    assert rel_rms(cube, ocube) < 1e-5
+    first = None
+    for batch in (1, 3, 8, 32, 0):
+        w.set_tuning(batch)
+        w.comp_image(noise=False)
+        cube = np.array(w.d_bincube).reshape(g.npix * g.npix, g.nvalid, order="F")
+        assert rel_rms(cube, ocube) < 1e-5
+        w.frame = 4
+        w.comp_image(noise=True)
+        noisy = np.array(w.d_bincube)
+        if first is None:
+            first = (cube, noisy)
+        np.testing.assert_array_equal(cube, first[0])
+        np.testing.assert_array_equal(noisy, first[1])
 
 
 @pytest.mark.parametrize("prec", ["f32", "bf16", "fp8"])
