@@ -108,86 +108,149 @@ __device__ __forceinline__ double u01(uint32_t x) {
 // 24-bit uniform in (0, 1), exact in float32: ((x >> 8) + 0.5) / 2^24
 __device__ __forceinline__ float u01f(uint32_t x) { return ((float)(x >> 8) + 0.5f) * 5.9604644775390625e-08f; }
 
-// Photon and readout noise of one pixel.  One Philox block per (pixel, frame,
-// draw): draw 0 gives the first Poisson draw (words x, y) and the readout
-// noise (words z, w); rejected Poisson draws continue with draws 1, 2, ...
+// Photon and readout noise of one pixel.  Philox blocks (pixel, frame, tag 0,
+// block b): block 0 gives the first Poisson draw (words x, y) and the readout
+// noise (words z, w); rejected Poisson draws continue with block 1 (x, y then
+// z, w), block 2, ...
 //
-// Poisson deviate: inversion for small means (Devroye 1986, X.3), PTRS
-// (Hoermann 1993, "The transformed rejection method for generating Poisson
-// random variables") otherwise.  Every value that decides the outcome is
-// computed with correctly rounded IEEE operations only (explicit _rn
-// intrinsics, no contracted multiply-add), so the CPU oracle reproduces it:
-//  * inversion: float64, u from word x (32-bit uniform), p0 = exp(-lambda),
-//    1/k as the correctly rounded reciprocal;
-//  * PTRS fast path (acceptance ~86 % of draws): float32 sqrt / div / mul /
-//    add on 24-bit uniforms;
-//  * PTRS exact acceptance test: float64 in product form, log(k!) from the
-//    table of cumulative log sums (first AOB_LOGFACT_SMEM entries from shared
-//    memory), two-term Stirling series beyond the table.
-#define AOB_LOGFACT_N 4096
-#define AOB_LOGFACT_SMEM 1024
-#define AOB_RK_N 1024
-struct NoiseTables {
-  const double *logfact;  // log(k!) for k < AOB_LOGFACT_N (device memory)
-};
+// Poisson deviate: inversion for means below 40 (Devroye 1986, X.3; below 40
+// it is cheaper than PTRS, whose quick acceptance rate is low for small means),
+// PTRS (Hoermann 1993, "The transformed rejection method for generating
+// Poisson random variables") otherwise, all in float32.  Every value that decides the
+// outcome comes from correctly rounded IEEE operations only (explicit _rn
+// intrinsics, no contracted multiply-add) and the project's own exp / log
+// below, so the CPU oracle reproduces each sample bit for bit:
+//  * inversion: p0 = exp(-lambda), then p *= lambda / k, F += p until F >= u
+//    (at most 160 steps);
+//  * PTRS: the fast acceptance test as published; the exact test in the log
+//    domain with log(k!) in Stirling form, arranged as
+//      k log(lambda / (k+1)) - log(k+1) / 2 + (k + 1 - lambda) - log(2 pi) / 2
+//      - 1 / (12 (k+1)) + 1 / (360 (k+1)^3)
+//    so that no large terms cancel (a table of log(k!) for k < 10).
 
-__device__ __forceinline__ double log_factorial(double k, const double *lf_smem, const NoiseTables &T) {
-  if (k < (double)AOB_LOGFACT_SMEM) return lf_smem[(int)k];
-  if (k < (double)AOB_LOGFACT_N) return __ldg(T.logfact + (int)k);
-  const double x = __dadd_rn(k, 1.0);
-  const double ix = __ddiv_rn(1.0, x);
-  double r = __dmul_rn(__dadd_rn(x, -0.5), log(x));
-  r = __dadd_rn(__dadd_rn(r, -x), 0.91893853320467274178);
-  const double c = __dadd_rn(__dmul_rn(0.08333333333333333, ix), -__dmul_rn(__dmul_rn(0.002777777777777778, ix),
-                                                                            __dmul_rn(ix, ix)));
-  return __dadd_rn(r, c);
+// exp(x) for x in [-88, 0]: x = n ln2 + r (Cody-Waite split of ln2, n nearest
+// integer to x / ln2), |r| <= ln2 / 2, e^r by its degree-7 Taylor polynomial
+// (truncation below 1e-8 relative), times 2^n.
+__device__ __forceinline__ float aob_expf_neg(float x) {
+  const float n = rintf(__fmul_rn(x, 1.44269502f));
+  const float r = __fadd_rn(__fadd_rn(x, -__fmul_rn(n, 0.693145752f)), -__fmul_rn(n, 1.42860677e-06f));
+  float p = 1.98412701e-04f;
+  p = __fadd_rn(__fmul_rn(p, r), 1.38888892e-03f);
+  p = __fadd_rn(__fmul_rn(p, r), 8.33333377e-03f);
+  p = __fadd_rn(__fmul_rn(p, r), 4.16666679e-02f);
+  p = __fadd_rn(__fmul_rn(p, r), 1.66666672e-01f);
+  p = __fadd_rn(__fmul_rn(p, r), 0.5f);
+  p = __fadd_rn(__fmul_rn(p, r), 1.0f);
+  p = __fadd_rn(__fmul_rn(p, r), 1.0f);
+  return __fmul_rn(p, __int_as_float(((int)n + 127) << 23));
 }
 
-// lam: the float32 mean; w0: Philox block of draw 0.
-static __device__ __forceinline__ float poisson_sample(float lamf, const U4 &w0, uint32_t idx, uint32_t frame,
-                                                    uint32_t k0, uint32_t k1, const double *lf_smem,
-                                                    NoiseTables T) {
-  if (!(lamf > 0.f)) return 0.f;
-  if (lamf < 10.f) {
-    const double lam = (double)lamf;
-    const double u = u01(w0.x);
-    double p = exp(-lam);
-    double f = p;
-    int k = 0;
-    while (u > f && k < AOB_RK_N - 1) {
-      k += 1;
-      p = __dmul_rn(p, __dmul_rn(lam, __drcp_rn((double)k)));
-      f = __dadd_rn(f, p);
-    }
-    return (float)k;
+// log(m) for m in [sqrt(1/2), sqrt(2)] and log1p(d) for d in [-1/4, 1/2] through
+// atanh: log((1+s)/(1-s)) = 2 s + 2 s^3/3 + ... + 2 s^11/11 (|s| <= 0.2).
+__device__ __forceinline__ float aob_log_series(float s) {
+  const float s2 = __fmul_rn(s, s);
+  float t = 0.181818187f;                              // 2/11
+  t = __fadd_rn(__fmul_rn(t, s2), 0.222222224f);       // 2/9
+  t = __fadd_rn(__fmul_rn(t, s2), 0.285714298f);       // 2/7
+  t = __fadd_rn(__fmul_rn(t, s2), 0.400000006f);       // 2/5
+  t = __fadd_rn(__fmul_rn(t, s2), 0.666666687f);       // 2/3
+  return __fadd_rn(__fmul_rn(s, 2.0f), __fmul_rn(__fmul_rn(s, s2), t));
+}
+// log(x) for normal x > 0: x = m 2^e with m in [sqrt(1/2), sqrt(2)].
+__device__ __forceinline__ float aob_logf(float x) {
+  const int bits = __float_as_int(x);
+  int e = ((bits >> 23) & 0xff) - 127;
+  float m = __int_as_float((bits & 0x007fffff) | 0x3f800000);
+  if (m > 1.41421354f) {
+    m = __fmul_rn(m, 0.5f);
+    e += 1;
   }
+  const float s = __fdiv_rn(__fadd_rn(m, -1.0f), __fadd_rn(m, 1.0f));
+  const float fe = (float)e;
+  return __fadd_rn(__fmul_rn(fe, 0.693145752f), __fadd_rn(__fmul_rn(fe, 1.42860677e-06f), aob_log_series(s)));
+}
+// log(1 + d) for -1/4 <= d <= 1/2 (|s| <= 0.2)
+__device__ __forceinline__ float aob_log1pf(float d) { return aob_log_series(__fdiv_rn(d, __fadd_rn(2.0f, d))); }
+
+#define AOB_POISSON_INV_KMAX 160
+#define AOB_POISSON_INV_MAX_MEAN 40.f
+// log(k!) for k < 10, float32 of the exact values
+__device__ __forceinline__ float aob_logfact_small(int k) {
+  switch (k) {
+    case 0: case 1: return 0.f;
+    case 2: return 0.693147182f;
+    case 3: return 1.79175949f;
+    case 4: return 3.17805386f;
+    case 5: return 4.78749180f;
+    case 6: return 6.57925129f;
+    case 7: return 8.52516174f;
+    case 8: return 10.6046028f;
+    default: return 12.8018274f;
+  }
+}
+
+// Poisson deviate by inversion (lamf < AOB_POISSON_INV_MAX_MEAN): chop-down
+// search four steps per pass with the factors lambda / j from rk[j] (the
+// correctly rounded reciprocals of 1..AOB_POISSON_INV_KMAX); the products and
+// sums are formed in the sequential order, and since F only grows the first
+// step with F >= u is found from the pass's four comparisons.
+__device__ __forceinline__ float poisson_inversion(float lamf, const U4 &w0, const float *rk) {
+  if (!(lamf > 0.f)) return 0.f;
+  const float u = u01f(w0.x);
+  float p = aob_expf_neg(-lamf);
+  float f = p;
+  if (!(u > f)) return 0.f;
+  for (int k = 0; k < AOB_POISSON_INV_KMAX; k += 4) {
+    const float a1 = __fmul_rn(lamf, rk[k + 1]), a2 = __fmul_rn(lamf, rk[k + 2]);
+    const float a3 = __fmul_rn(lamf, rk[k + 3]), a4 = __fmul_rn(lamf, rk[k + 4]);
+    const float p1 = __fmul_rn(p, a1), p2 = __fmul_rn(p1, a2), p3 = __fmul_rn(p2, a3), p4 = __fmul_rn(p3, a4);
+    const float f1 = __fadd_rn(f, p1), f2 = __fadd_rn(f1, p2), f3 = __fadd_rn(f2, p3), f4 = __fadd_rn(f3, p4);
+    if (!(u > f4)) return (float)(k + 4 - (int)!(u > f3) - (int)!(u > f2) - (int)!(u > f1));
+    p = p4;
+    f = f4;
+  }
+  return (float)AOB_POISSON_INV_KMAX;
+}
+
+// Poisson deviate by PTRS (lamf >= AOB_POISSON_INV_MAX_MEAN); w0: Philox block 0.
+__device__ __forceinline__ float poisson_ptrs(float lamf, const U4 &w0, uint32_t idx, uint32_t frame, uint32_t k0,
+                                              uint32_t k1) {
   const float slam = __fsqrt_rn(lamf);
   const float b = __fadd_rn(0.931f, __fmul_rn(2.53f, slam));
   const float a = __fadd_rn(-0.059f, __fmul_rn(0.02483f, b));
   const float vr = __fadd_rn(0.9277f, -__fdiv_rn(3.6224f, __fadd_rn(b, -2.0f)));
   const float a2 = __fmul_rn(2.0f, a);
-  // constants of the exact acceptance test, computed only when a draw needs it
-  double loglam = 0.0, invalpha = 0.0;
-  bool slow_ready = false;
+  const float invalpha = __fadd_rn(1.1239f, __fdiv_rn(1.1328f, __fadd_rn(b, -3.4f)));
   U4 w = w0;
   for (uint32_t d = 0; d < 64u; ++d) {
-    if (d > 0) w = philox4x32_10(U4{idx, frame, TAG_POISSON, d}, k0, k1);
-    const float u = __fadd_rn(u01f(w.x), -0.5f);
-    const float v = u01f(w.y);
+    // draw 0: words x, y of block 0; draw d >= 1: block (d + 1) / 2, words x, y
+    // for odd d and z, w for even d
+    if (d & 1u) w = philox4x32_10(U4{idx, frame, TAG_POISSON, (d + 1u) >> 1}, k0, k1);
+    const uint32_t wu = (d == 0u || (d & 1u)) ? w.x : w.z;
+    const uint32_t wv = (d == 0u || (d & 1u)) ? w.y : w.w;
+    const float u = __fadd_rn(u01f(wu), -0.5f);
+    const float v = u01f(wv);
     const float us = __fadd_rn(0.5f, -fabsf(u));
     const float k = floorf(__fadd_rn(__fadd_rn(__fmul_rn(__fadd_rn(__fdiv_rn(a2, us), b), u), lamf), 0.43f));
     if (us >= 0.07f && v <= vr) return k;
     if (k < 0.f || (us < 0.013f && v > us)) continue;
-    if (!slow_ready) {
-      loglam = log((double)lamf);
-      invalpha = __dadd_rn(1.1239, __ddiv_rn(1.1328, __dadd_rn((double)b, -3.4)));
-      slow_ready = true;
+    // exact test: log(v * invalpha / (a / us^2 + b)) <= log(pmf(k) e^lambda / ...) in log domain
+    const float lhs =
+        aob_logf(__fdiv_rn(__fmul_rn(v, invalpha), __fadd_rn(__fdiv_rn(a, __fmul_rn(us, us)), b)));
+    float rhs;
+    if (k < 10.f) {
+      rhs = __fadd_rn(__fadd_rn(__fmul_rn(k, aob_logf(lamf)), -lamf), -aob_logfact_small((int)k));
+    } else {
+      const float x = __fadd_rn(k, 1.0f);
+      const float d = __fdiv_rn(__fadd_rn(lamf, -x), x);
+      const float lr = (d >= -0.25f && d <= 0.5f) ? aob_log1pf(d) : aob_logf(__fdiv_rn(lamf, x));
+      const float ix = __frcp_rn(x);
+      const float corr = __fadd_rn(__fmul_rn(0.0833333358f, ix),
+                                   -__fmul_rn(__fmul_rn(0.00277777785f, ix), __fmul_rn(ix, ix)));
+      rhs = __fadd_rn(__fmul_rn(k, lr), -__fmul_rn(0.5f, aob_logf(x)));
+      rhs = __fadd_rn(rhs, __fadd_rn(x, -lamf));
+      rhs = __fadd_rn(__fadd_rn(rhs, -0.918938518f), -corr);
     }
-    const double usd = (double)us;
-    const double lhs =
-        __ddiv_rn(__dmul_rn((double)v, invalpha), __dadd_rn(__ddiv_rn((double)a, __dmul_rn(usd, usd)), (double)b));
-    const double rhs = exp(__dadd_rn(__dadd_rn(__dmul_rn((double)k, loglam), -(double)lamf),
-                                     -log_factorial((double)k, lf_smem, T)));
     if (lhs <= rhs) return k;
   }
   return floorf(__fadd_rn(lamf, 0.5f));

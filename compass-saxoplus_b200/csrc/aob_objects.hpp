@@ -43,7 +43,6 @@ struct aob_sh {
   aob::DevBuf<int32_t> ulist, vlist, cbin;
   // outputs
   aob::DevBuf<float> bincube, binimg, intensities, slopes;
-  aob::DevBuf<double> logfact;      // noise-sampler table log(k!)
   aob::DevBuf<float> twiddle;       // exp(-2 pi i m / nfft) as (re, im) pairs
   aob::DevBuf<float> wxy;           // the same values gathered per (frequency, sample)
   // centroider whose slopes are fused into comp_image (may be null)

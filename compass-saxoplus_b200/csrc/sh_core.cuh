@@ -6,10 +6,9 @@
 //   1. complex field  pupil * exp(i (phase * 2 pi / lambda - offset))
 //   2. DFT along x at the nu frequencies binmap reads
 //   3. DFT along y at the nv frequencies binmap reads, |.|^2
-//   4. binning through the compact binmap and the flux per sub-aperture
-//      (one warp per sub-aperture, fixed summation order)
-//   5. normalisation, Philox photon / readout noise, cube + image writes,
-//      centroid weights
+//   4. binning through the compact binmap, the flux per sub-aperture (one
+//      warp per sub-aperture, fixed summation order) and normalisation
+//   5. Philox photon / readout noise, cube + image writes, centroid weights
 //   6. CoG-family centroid per sub-aperture (one warp each, fixed order)
 // so a CTA pays each stage's latency once for the batch instead of once per
 // sub-aperture.  The reductions run in an order that does not depend on the
@@ -48,7 +47,6 @@ struct ShKernelArgs {
   float noise;
   uint32_t frame, k0, k1;
   const uint32_t *frame_ptr;  // when set, the frame number is read from device memory
-  NoiseTables tables;
   // magic multipliers for the runtime divisions (see udiv)
   uint32_t mg_pd, mg_pd2, mg_nu, mg_nupd, mg_nunv, mg_np, mg_np2;
   // fused centroider (kind < 0: none)
@@ -70,13 +68,13 @@ __device__ __forceinline__ int udiv(int i, uint32_t magic) { return (int)__umulh
 
 // Shared-memory layout: CTA-wide tables, then the batch work area.
 struct ShSmem {
-  size_t wxy, lf, hdr;                          // twiddle and log(k!) table offsets, header size
-  size_t meta, E, Gt, I, bins, dw, per_batch;   // offsets within the work area
+  size_t wxy, rk, hdr;                          // twiddle and 1/k table offsets, header size
+  size_t meta, E, Gt, I, bins, dw, ord, per_batch;  // offsets within the work area
   __host__ __device__ static size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
   __host__ __device__ ShSmem(int nfft, int nu, int nv, int pd, int ncb, int npix2, int S) {
     wxy = align16(sizeof(float2) * nfft + sizeof(int32_t) * (2 * nfft + ncb) + sizeof(float) * npix2);
-    lf = align16(wxy + sizeof(float2) * (size_t)(nu + nv) * pd);
-    hdr = align16(lf + sizeof(double) * AOB_LOGFACT_SMEM);
+    rk = align16(wxy + sizeof(float2) * (size_t)(nu + nv) * pd);
+    hdr = align16(rk + sizeof(float) * (AOB_POISSON_INV_KMAX + 1));
     size_t o = 0;
     meta = o;
     o += align16(sizeof(int32_t) * 8 * (size_t)S);
@@ -90,6 +88,8 @@ struct ShSmem {
     o += align16(sizeof(float) * (size_t)S * npix2);
     dw = o;
     o += align16(sizeof(float) * (size_t)S * npix2);
+    ord = o;
+    o += align16(sizeof(int32_t) * (size_t)S * npix2);
     per_batch = o;
   }
   __host__ __device__ size_t bytes() const { return hdr + per_batch; }
@@ -115,8 +115,8 @@ __device__ __forceinline__ void sh_load_tables(const ShKernelArgs &P, unsigned c
   float2 *wxy = reinterpret_cast<float2 *>(smem + L.wxy);
   for (int i = tid; i < (P.nu + P.nv) * P.pdiam; i += nthreads) wxy[i] = P.wxy[i];
   if (P.noise_mode >= 1) {
-    double *lf = reinterpret_cast<double *>(smem + L.lf);
-    for (int i = tid; i < AOB_LOGFACT_SMEM; i += nthreads) lf[i] = P.tables.logfact[i];
+    float *rk = reinterpret_cast<float *>(smem + L.rk);
+    for (int i = tid; i <= AOB_POISSON_INV_KMAX; i += nthreads) rk[i] = i ? __frcp_rn((float)i) : 0.f;
   }
 }
 
@@ -135,7 +135,6 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
   const int32_t *cb = vl + NFFT;
   const int npix = P.npix, npix2 = npix * npix, nr2 = P.nrebin2;
   const float *wt = reinterpret_cast<const float *>(cb + nr2 * npix2);
-  const double *lf = reinterpret_cast<const double *>(tables + L.lf);
   const int nu = P.nu, nv = P.nv;
   const int pd = PD > 0 ? PD : P.pdiam;
   const int pd2 = pd * pd, nupd = nu * pd, nunv = nu * nv;
@@ -153,6 +152,8 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
   float *I = reinterpret_cast<float *>(work + L.I);
   float *bins = reinterpret_cast<float *>(work + L.bins);
   float *dw = reinterpret_cast<float *>(work + L.dw);
+  int *order = reinterpret_cast<int *>(work + L.ord);  // stage 4-5 pixel list
+  const float *rk = reinterpret_cast<const float *>(tables + L.rk);
 
   // ---- 0. metadata of the batch (one global round trip for all of it) ----
   if (tid < S) {
@@ -168,6 +169,8 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
     }
   }
   const uint32_t frame = P.frame_ptr ? *P.frame_ptr : P.frame;
+  __shared__ int n_listed[2];  // pixels listed for inversion / PTRS in stage 4
+  if (tid == 0) n_listed[0] = n_listed[1] = 0;
   __syncthreads();
 
   // ---- 1. complex field: loads of up to 4 elements issued before any use ----
@@ -323,22 +326,47 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
       m_tot[s] = part;
       P.intensities[base + s * stride] = part;
     }
+    // normalise in place; with photon noise list the pixels by sampler
+    // (inversion from the front of `order`, PTRS from the back) so that the
+    // warps of stage 5 each run one sampler
+    const float fl = m_fl[s];
+    for (int p0 = 0; p0 < npix2; p0 += 32) {
+      const int p = p0 + lane;
+      const bool valid = p < npix2;
+      float v = valid ? bins[s * npix2 + p] : 0.f;
+      if (valid && part != 0.f) v = v * fl / part * P.nphot;
+      if (valid) bins[s * npix2 + p] = v;
+      if (P.noise_mode >= 1) {
+        const bool inv = valid && v < AOB_POISSON_INV_MAX_MEAN;
+        const bool ptr = valid && !inv;
+        const unsigned mi = __ballot_sync(0xffffffffu, inv), mp = __ballot_sync(0xffffffffu, ptr);
+        int bi = 0, bp = 0;
+        if (lane == 0) {
+          bi = atomicAdd(&n_listed[0], __popc(mi));
+          bp = atomicAdd(&n_listed[1], __popc(mp));
+        }
+        bi = __shfl_sync(0xffffffffu, bi, 0);
+        bp = __shfl_sync(0xffffffffu, bp, 0);
+        const unsigned lt = (1u << lane) - 1u;
+        if (inv) order[bi + __popc(mi & lt)] = s * npix2 + p;
+        if (ptr) order[nP - 1 - (bp + __popc(mp & lt))] = s * npix2 + p;
+      }
+    }
   }
   __syncthreads();
 
-  // ---- 5. normalise, noise, cube + image, centroid weights ----
-  for (int i = tid; i < nP; i += nt) {
+  // ---- 5. noise, cube + image, centroid weights ----
+  for (int t = tid; t < nP; t += nt) {
+    const int i = P.noise_mode >= 1 ? order[t] : t;
     const int s = udiv(i, P.mg_np2), p = i - s * npix2;
     const int k = base + s * stride;
     float wgt = 1.f;
     if (P.ckind == 2) wgt = P.c_wper ? P.c_weights[p + k * npix2] : wt[p];
     float v = bins[i];
-    const float tot = m_tot[s];
-    if (tot != 0.f) v = v * m_fl[s] / tot * P.nphot;
     const uint32_t pix = (uint32_t)(p + k * npix2);
     if (P.noise_mode >= 1) {
       const U4 w0 = philox4x32_10(U4{pix, frame, TAG_POISSON, 0u}, P.k0, P.k1);
-      v = poisson_sample(v, w0, pix, frame, P.k0, P.k1, lf, P.tables);
+      v = v < AOB_POISSON_INV_MAX_MEAN ? poisson_inversion(v, w0, rk) : poisson_ptrs(v, w0, pix, frame, P.k0, P.k1);
       if (P.noise_mode >= 2) v = v + P.noise * gauss_sample(w0);
     }
     P.bincube[pix] = v;

@@ -93,9 +93,6 @@ aob_sh::aob_sh(int device_, int nxsub_, int nvalid_, int npix_, int nphase_, int
   binimg.alloc((int64_t)npix * nxsub * npix * nxsub);
   intensities.alloc(nvalid);
   slopes.alloc(2 * (int64_t)nvalid);
-  // noise table: log(k!) as cumulative sums of log(i) (same as the CPU oracle)
-  std::vector<double> lf(AOB_LOGFACT_N, 0.0);
-  for (int k = 1; k < AOB_LOGFACT_N; ++k) lf[k] = lf[k - 1] + std::log((double)k);
   std::vector<float> tw(2 * nfft);
   for (int m = 0; m < nfft; ++m) {
     const double ang = 2.0 * M_PI * (double)m / (double)nfft;
@@ -104,8 +101,6 @@ aob_sh::aob_sh(int device_, int nxsub_, int nvalid_, int npix_, int nphase_, int
   }
   twiddle.alloc(2 * nfft);
   twiddle.upload(tw.data(), 2 * nfft);
-  logfact.alloc(AOB_LOGFACT_N);
-  logfact.upload(lf.data(), AOB_LOGFACT_N);
 }
 
 void aob_sh::load_arrays(const int32_t *h_binmap, const float *h_offsets, const float *h_flux,
@@ -251,7 +246,6 @@ aob_centro *aob_sh::make_args(bool with_noise, float *slopes_dst, const uint32_t
   P.k0 = (uint32_t)((uint64_t)seed & 0xffffffffu);
   P.k1 = (uint32_t)((uint64_t)seed >> 32);
   P.frame_ptr = frame_ptr;
-  P.tables = NoiseTables{logfact.p};
   P.mg_pd = udiv_magic((uint32_t)nphase);
   P.mg_pd2 = udiv_magic((uint32_t)(nphase * nphase));
   P.mg_nu = udiv_magic((uint32_t)nu);

@@ -10,22 +10,23 @@ device.  This replaces the reference's cuRAND XORWOW states
 
 Counter layout used by the sensors (one 128-bit block per pixel and draw):
   c0 = pixel index, c1 = frame number, c2 = stream tag (0 = sensor noise),
-  c3 = draw number; key = (seed & 0xffffffff, seed >> 32).
-Draw 0 of a pixel gives the first Poisson draw (words 0, 1) and the readout
-noise (words 2, 3); rejected Poisson draws continue with draws 1, 2, ...
+  c3 = block number; key = (seed & 0xffffffff, seed >> 32).
+Block 0 of a pixel gives the first Poisson draw (words 0, 1) and the readout
+noise (words 2, 3); rejected Poisson draws continue with block 1 (words 0, 1,
+then 2, 3), block 2, ...
 (The turbulence extrusion uses tag 2, c3 = layer.)
 
 Poisson sampling (replaces curand_poisson, carma_rng.cu:135-141), restating
-the device sampler operation for operation:
-  lambda < 10: sequential-search inversion (Devroye 1986, ch. X.3) on one
-               32-bit uniform, in float64 with no fused multiply-add (1/k as
-               the IEEE quotient);
-  lambda >= 10: PTRS transformed rejection (Hoermann 1993, "The transformed
+the device sampler operation for operation, all in float32 on 24-bit uniforms:
+  lambda < 40: sequential-search inversion (Devroye 1986, ch. X.3, at most
+               160 steps) with
+               p0 = exp(-lambda) from the project's own exp (Cody-Waite
+               reduction, degree-7 Taylor polynomial);
+  lambda >= 40: PTRS transformed rejection (Hoermann 1993, "The transformed
                rejection method for generating Poisson random variables"):
-               the fast acceptance path in float32 on 24-bit uniforms, the
-               exact acceptance test in float64 in product form with log(k!)
-               from a table of cumulative log sums (two-term Stirling series
-               beyond 4095).
+               the published fast acceptance test, and the exact test in the
+               log domain with log(k!) in Stirling form arranged so that no
+               large terms cancel (own log / log1p by the atanh series).
 Gaussian: Box-Muller in float32 on words 2 (u1) and 3 (u2) of draw 0.
 """
 
@@ -40,7 +41,7 @@ W1 = 0xBB67AE85
 MASK = 0xFFFFFFFF
 
 TAG_POISSON = 0
-POISSON_SMALL = 10.0
+POISSON_SMALL = 40.0
 POISSON_MAX_DRAWS = 64
 
 
@@ -74,35 +75,8 @@ def u01(x):
     return (np.asarray(x, dtype=np.float64) + 0.5) * (1.0 / 4294967296.0)
 
 
-LOGFACT_N = 4096
-RK_N = 1024
-
-
-def _tables():
-    """log(k!) by cumulative sums of log(i) (the device table) and 1/k (the device computes the
-    same correctly rounded value with __drcp_rn)."""
-    lf = [0.0] * LOGFACT_N
-    for k in range(1, LOGFACT_N):
-        lf[k] = lf[k - 1] + math.log(k)
-    rk = [0.0] + [1.0 / k for k in range(1, RK_N)]
-    return lf, rk
-
-
-LOGFACT, RK = _tables()
-
-
-def log_factorial(k):
-    if k < LOGFACT_N:
-        return LOGFACT[int(k)]
-    x = k + 1.0
-    ix = 1.0 / x
-    r = (x + -0.5) * math.log(x)
-    r = (r + -x) + 0.91893853320467274178
-    c = 0.08333333333333333 * ix + -((0.002777777777777778 * ix) * (ix * ix))
-    return r + c
-
-
 F32 = np.float32
+INV_KMAX = 160
 
 
 def _u01f(x):
@@ -110,19 +84,55 @@ def _u01f(x):
     return (F32(int(x) >> 8) + F32(0.5)) * F32(5.9604644775390625e-08)
 
 
-def _ptrs(lamf, words_of_draw):
-    """PTRS transformed rejection: float32 fast path, float64 exact test in product form.
+# Every helper below uses single correctly rounded NumPy float32 scalar operations
+# in the device's order, so results equal the GPU's bit for bit.
+def _expf_neg(x):
+    """exp(x), x in [-88, 0]: Cody-Waite reduction by ln2, degree-7 Taylor polynomial."""
+    n = np.rint(x * F32(1.44269502))
+    r = (x + -(n * F32(0.693145752))) + -(n * F32(1.42860677e-06))
+    p = F32(1.98412701e-04)
+    for c in (1.38888892e-03, 8.33333377e-03, 4.16666679e-02, 1.66666672e-01, 0.5, 1.0, 1.0):
+        p = p * r + F32(c)
+    return p * np.ldexp(F32(1.0), int(n))
 
-    Every float32 operation is a single correctly rounded NumPy float32 scalar
-    operation, in the device's order.
-    """
+
+def _log_series(s):
+    """log((1+s)/(1-s)) = 2 s + 2 s^3/3 + ... + 2 s^11/11."""
+    s2 = s * s
+    t = F32(0.181818187)
+    for c in (0.222222224, 0.285714298, 0.400000006, 0.666666687):
+        t = t * s2 + F32(c)
+    return s * F32(2.0) + (s * s2) * t
+
+
+def _logf(x):
+    """log(x), normal x > 0, from x = m 2^e with m in [sqrt(1/2), sqrt(2)]."""
+    bits = int(np.asarray(F32(x)).view(np.int32))
+    e = ((bits >> 23) & 0xFF) - 127
+    m = np.asarray(np.int32((bits & 0x007FFFFF) | 0x3F800000)).view(np.float32)[()]
+    if m > F32(1.41421354):
+        m = m * F32(0.5)
+        e += 1
+    s = (m + F32(-1.0)) / (m + F32(1.0))
+    fe = F32(e)
+    return fe * F32(0.693145752) + (fe * F32(1.42860677e-06) + _log_series(s))
+
+
+def _log1pf(d):
+    return _log_series(d / (F32(2.0) + d))
+
+
+_LOGFACT_SMALL = [F32(math.lgamma(k + 1)) for k in range(10)]
+
+
+def _ptrs(lamf, words_of_draw):
+    """PTRS transformed rejection in float32; exact test in the log domain (Stirling form)."""
     slam = np.sqrt(lamf)
     b = F32(0.931) + F32(2.53) * slam
     a = F32(-0.059) + F32(0.02483) * b
     vr = F32(0.9277) + -(F32(3.6224) / (b + F32(-2.0)))
     a2 = F32(2.0) * a
-    loglam = math.log(float(lamf))
-    invalpha = 1.1239 + 1.1328 / (float(b) + -3.4)
+    invalpha = F32(1.1239) + F32(1.1328) / (b + F32(-3.4))
     for d in range(POISSON_MAX_DRAWS):
         w = words_of_draw(d)
         u = _u01f(w[0]) + F32(-0.5)
@@ -133,23 +143,32 @@ def _ptrs(lamf, words_of_draw):
             return float(k)
         if k < 0 or (us < F32(0.013) and v > us):
             continue
-        usd = float(us)
-        lhs = (float(v) * invalpha) / ((float(a) / (usd * usd)) + float(b))
-        rhs = math.exp(((float(k) * loglam) + -float(lamf)) + -log_factorial(float(k)))
+        lhs = _logf((v * invalpha) / ((a / (us * us)) + b))
+        if k < F32(10.0):
+            rhs = (k * _logf(lamf) + -lamf) + -_LOGFACT_SMALL[int(k)]
+        else:
+            x = k + F32(1.0)
+            dd = (lamf + -x) / x
+            lr = _log1pf(dd) if (F32(-0.25) <= dd <= F32(0.5)) else _logf(lamf / x)
+            ix = F32(1.0) / x
+            corr = F32(0.0833333358) * ix + -((F32(0.00277777785) * ix) * (ix * ix))
+            rhs = k * lr + -(F32(0.5) * _logf(x))
+            rhs = rhs + (x + -lamf)
+            rhs = (rhs + F32(-0.918938518)) + -corr
         if lhs <= rhs:
             return float(k)
     return float(np.floor(lamf + F32(0.5)))
 
 
-def _inversion(lam, u):
-    p = math.exp(-lam)
+def _inversion(lamf, u):
+    p = _expf_neg(-lamf)
     f = p
     k = 0
-    while u > f and k < RK_N - 1:
+    while u > f and k < INV_KMAX:
         k += 1
-        p = p * (lam * RK[k])
+        p = p * (lamf * (F32(1.0) / F32(k)))
         f = f + p
-    return k
+    return float(k)
 
 
 def poisson(lam, index, frame, seed):
@@ -167,15 +186,15 @@ def poisson(lam, index, frame, seed):
         if not (m > 0):
             res[j] = 0.0
         elif m < POISSON_SMALL:
-            res[j] = _inversion(float(m), float(u01(w0[0][j])))
+            res[j] = _inversion(m, _u01f(w0[0][j]))
         else:
             ij = int(flat_i[j])
 
             def words(d, ij=ij, j=j):
                 if d == 0:
                     return (w0[0][j], w0[1][j])
-                w = philox4x32(ij, frame, TAG_POISSON, d, k0, k1)
-                return (w[0], w[1])
+                w = philox4x32(ij, frame, TAG_POISSON, (d + 1) // 2, k0, k1)
+                return (w[0], w[1]) if d % 2 == 1 else (w[2], w[3])
 
             res[j] = _ptrs(m, words)
     return res.reshape(lam.shape)

@@ -32,7 +32,7 @@ def test_philox_known_answers():
 
 
 def test_poisson_statistics():
-    for lam in (0.3, 4.0, 9.9, 10.0, 57.0, 3000.0):
+    for lam in (0.3, 4.0, 9.9, 10.0, 39.9, 40.0, 57.0, 3000.0):
         idx = np.arange(20000, dtype=np.uint64)
         x = philox.poisson(np.full(idx.shape, lam), idx, frame=3, seed=99)
         assert np.all(x == np.floor(x)) and np.all(x >= 0)
@@ -174,3 +174,33 @@ def test_cpu_baseline_loop_matches_oracle(geom16):
     _, img, _ = sh.comp_image(phase, g.tel.mpupil, g, 2 * np.pi / g.wavelength_um, g.nphotons)
     s, _, _ = rtc.centroids(img, g.validsubsx, g.validsubsy, g.npix, g.pixsize, g.npix / 2 - 0.5)
     np.testing.assert_allclose(com, -0.5 * cmat @ s, rtol=1e-9, atol=1e-12)
+
+
+def test_float32_exp_log_accuracy():
+    """The sampler's own exp / log / log1p stay within a few float32 ulps."""
+    xs = np.linspace(-10.0, 0.0, 2001, dtype=np.float32)
+    e = np.array([philox._expf_neg(x) for x in xs], dtype=np.float64)
+    assert np.max(np.abs(e / np.exp(xs.astype(np.float64)) - 1)) < 5e-7
+    ys = np.geomspace(1e-6, 1e6, 2001).astype(np.float32)
+    lg = np.array([philox._logf(y) for y in ys], dtype=np.float64)
+    assert np.all(np.abs(lg - np.log(ys.astype(np.float64))) < 2e-6 * np.maximum(1, np.abs(np.log(ys))))
+    ds = np.linspace(-0.25, 0.5, 1001, dtype=np.float32)
+    l1 = np.array([philox._log1pf(d) for d in ds], dtype=np.float64)
+    assert np.max(np.abs(l1 - np.log1p(ds.astype(np.float64)))) < 3e-7
+
+
+@pytest.mark.parametrize("lam", [2.5, 9.75, 37.0, 39.9, 40.0, 61.0, 400.0, 5000.0])
+def test_poisson_sampler_matches_the_pmf(lam):
+    """Chi-square of 40k deviates against the exact Poisson pmf (both branches)."""
+    from scipy import stats
+
+    n = 40000
+    x = philox.poisson(np.full(n, lam, np.float32), np.arange(n, dtype=np.uint64), frame=17, seed=2024)
+    lo, hi = int(stats.poisson.ppf(1e-4, lam)), int(stats.poisson.ppf(1 - 1e-4, lam))
+    edges = np.unique(np.linspace(lo, hi + 1, 40).astype(int))
+    obs = np.histogram(x, bins=np.concatenate([[-1e9], edges[1:-1], [1e9]]))[0]
+    cdf = stats.poisson.cdf(edges[1:-1] - 1, lam)
+    exp_p = np.diff(np.concatenate([[0.0], cdf, [1.0]]))
+    chi2 = np.sum((obs - n * exp_p) ** 2 / (n * exp_p))
+    p = stats.chi2.sf(chi2, len(obs) - 1)
+    assert p > 1e-4, (lam, chi2, len(obs))
