@@ -45,15 +45,18 @@ struct MvmArgs {
   int rows_per_cta;       // bulk kernel: rows staged per CTA (host-checked to fit)
 };
 
-// Dot product of one 16-byte packed chunk with its slopes.  The slopes are
-// staged in shared memory in a lane-swizzled order: the V/4 float4 groups of
-// chunk c = lane + 32*j live at float4 index (j*(V/4) + q)*32 + lane, so a warp
-// reads them with conflict-free 128-bit loads for every precision.
+// Dot product of one 16-byte packed chunk with its slopes sv[STRIDE * q],
+// q < V/4.  The slopes are staged in shared memory in a lane-swizzled order:
+// the V/4 float4 groups of chunk c = lane + 32*j live at float4 index
+// (j*(V/4) + q)*32 + lane, so a warp reads them with conflict-free 128-bit
+// loads for every precision (STRIDE = 32 from the staged vector, 1 from a
+// register copy).
 template <typename T>
 struct Pack;
 template <>
 struct Pack<float> {
   static constexpr int N = 4;
+  template <int STRIDE = 32>
   __device__ static float dot(const uint4 &q, const float4 *sv) {
     const float *f = reinterpret_cast<const float *>(&q);
     const float4 s = sv[0];
@@ -66,12 +69,13 @@ struct Pack<float> {
 template <>
 struct Pack<__nv_bfloat16> {
   static constexpr int N = 8;
+  template <int STRIDE = 32>
   __device__ static float dot(const uint4 &q, const float4 *sv) {
     const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
     float a = 0.f;
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
-      const float4 s = sv[32 * i];
+      const float4 s = sv[STRIDE * i];
       const float2 f0 = __bfloat1622float2(h[2 * i]);
       const float2 f1 = __bfloat1622float2(h[2 * i + 1]);
       a = fmaf(f0.x, s.x, a);
@@ -85,12 +89,13 @@ struct Pack<__nv_bfloat16> {
 template <>
 struct Pack<__nv_fp8_e4m3> {
   static constexpr int N = 16;
+  template <int STRIDE = 32>
   __device__ static float dot(const uint4 &q, const float4 *sv) {
     const __nv_fp8x2_e4m3 *h = reinterpret_cast<const __nv_fp8x2_e4m3 *>(&q);
     float a = 0.f;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const float4 s = sv[32 * i];
+      const float4 s = sv[STRIDE * i];
       const float2 f0 = static_cast<float2>(h[2 * i]);
       const float2 f1 = static_cast<float2>(h[2 * i + 1]);
       a = fmaf(f0.x, s.x, a);
@@ -161,25 +166,34 @@ __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_kernel(MvmArgs A) {
 // Bulk-copy MVM.  Each CTA owns rows [r0, r1) of the packed matrix; one
 // thread issues one TMA bulk copy per row into shared memory (each completing
 // on its own mbarrier) before anything else happens, so the whole matrix is in
-// flight from the first microsecond.  Warps then take rows as they land and
-// reduce them against the lane-swizzled slope vector.  Waits are bounded: an
-// expired wait sets ERR_MBAR_TIMEOUT in *status and the row is skipped.
+// flight from the first microsecond.  The slopes are staged with 16-byte
+// loads; once the rows have landed the CTA reduces them split-K: warp w, lane
+// l take chunks c = l + 32 (w + NW i), read each slope chunk once and apply it
+// to every row from registers, and the per-warp partial sums are added in
+// warp order (deterministic).  Waits are bounded: an expired wait sets
+// ERR_MBAR_TIMEOUT in *status and the CTA's rows are skipped.
 constexpr uint32_t MBAR_MAX_POLLS = 1u << 22;
+
+__host__ __device__ inline size_t mvm_bars_bytes(int rows) { return 128 * (((size_t)rows * 8 + 127) / 128); }
 
 template <typename T>
 __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_bulk_kernel(MvmArgs A) {
   extern __shared__ __align__(128) unsigned char sm[];
   constexpr int V = Pack<T>::N;
   constexpr int Q = V / 4;
+  constexpr int NW = MVM_THREADS / 32;
+  constexpr int RB = 8;  // rows per register block
   const int nchunk = A.ld / V;
   const int nsh = mvm_smem_floats(A.ld, V);
   const uint32_t row_bytes = (uint32_t)(A.ld * sizeof(T));
   const int r0 = (int)(((int64_t)blockIdx.x * A.nrow) / gridDim.x);
   const int r1 = (int)(((int64_t)(blockIdx.x + 1) * A.nrow) / gridDim.x);
   const int R = r1 - r0;
+  // shared memory: barriers | slopes | rows | per-warp partial sums
   uint64_t *bars = reinterpret_cast<uint64_t *>(sm);
-  float *s_sh = reinterpret_cast<float *>(sm + 128 * ((A.rows_per_cta * 8 + 127) / 128));
+  float *s_sh = reinterpret_cast<float *>(sm + mvm_bars_bytes(A.rows_per_cta));
   unsigned char *rows = reinterpret_cast<unsigned char *>(s_sh + nsh);
+  float *part = reinterpret_cast<float *>(rows + (size_t)A.rows_per_cta * row_bytes);
   if (threadIdx.x == 0) {
     for (int r = 0; r < R; ++r) mbar_init(&bars[r], 1);
     fence_mbar_init();
@@ -193,32 +207,57 @@ __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_bulk_kernel(MvmArgs A) {
     }
   }
   if (A.bump && blockIdx.x == 0 && threadIdx.x == 0) *A.bump += 1u;
-  for (int i = threadIdx.x; i < nsh; i += blockDim.x) {
-    const int g = i >> 2, e = i & 3;
+  for (int g = threadIdx.x; g < nsh / 4; g += blockDim.x) {
     const int l = g & 31, jq = g >> 5;
     const int j = jq / Q, q = jq - j * Q;
-    const int src = (l + 32 * j) * V + 4 * q + e;
-    s_sh[i] = (src < A.ncol) ? A.s[src] : 0.f;
+    const int src = (l + 32 * j) * V + 4 * q;
+    float4 v4;
+    if (src + 3 < A.ncol) {
+      v4 = *reinterpret_cast<const float4 *>(A.s + src);
+    } else {
+      v4.x = src < A.ncol ? A.s[src] : 0.f;
+      v4.y = src + 1 < A.ncol ? A.s[src + 1] : 0.f;
+      v4.z = src + 2 < A.ncol ? A.s[src + 2] : 0.f;
+      v4.w = 0.f;
+    }
+    reinterpret_cast<float4 *>(s_sh)[g] = v4;
   }
   __syncthreads();
-  const float4 *svl = reinterpret_cast<const float4 *>(s_sh) + (threadIdx.x & 31);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nw = blockDim.x >> 5;
-  for (int r = warp; r < R; r += nw) {
-    if (!mbar_wait(&bars[r], 0, MBAR_MAX_POLLS)) {
-      if (lane == 0 && A.status) atomicOr(A.status, (uint32_t)ERR_MBAR_TIMEOUT);
-      continue;
-    }
-    const uint4 *row = reinterpret_cast<const uint4 *>(rows + (size_t)r * row_bytes) + lane;
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    int j = 0;
-    for (; 32 * (j + 3) + lane < nchunk; j += 4) {
+  bool rows_ok = true;
+  for (int r = 0; r < R; ++r) rows_ok &= mbar_wait(&bars[r], 0, MBAR_MAX_POLLS);
+  if (!rows_ok && threadIdx.x == 0 && A.status) atomicOr(A.status, (uint32_t)ERR_MBAR_TIMEOUT);
+  const float4 *sv4 = reinterpret_cast<const float4 *>(s_sh);
+  for (int rb = 0; rb < R; rb += RB) {
+    float acc[RB];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) acc[u] += Pack<T>::dot(row[32 * (j + u)], svl + 32 * Q * (j + u));
+    for (int u = 0; u < RB; ++u) acc[u] = 0.f;
+    if (rows_ok) {
+      for (int jj = warp; 32 * jj + lane < nchunk; jj += NW) {
+        const int c = lane + 32 * jj;
+        float4 sv[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) sv[q] = sv4[(jj * Q + q) * 32 + lane];
+#pragma unroll
+        for (int u = 0; u < RB; ++u)
+          if (rb + u < R) {
+            const uint4 q4 = reinterpret_cast<const uint4 *>(rows + (size_t)(rb + u) * row_bytes)[c];
+            acc[u] += Pack<T>::template dot<1>(q4, sv);
+          }
+      }
     }
-    for (; 32 * j + lane < nchunk; ++j) acc[0] += Pack<T>::dot(row[32 * j], svl + 32 * Q * j);
-    float tot = warp_sum((acc[0] + acc[1]) + (acc[2] + acc[3]));
-    if (lane == 0) {
+#pragma unroll
+    for (int u = 0; u < RB; ++u) {
+      const float t = warp_sum(acc[u]);
+      if (lane == 0 && rb + u < R) part[warp * A.rows_per_cta + rb + u] = t;
+    }
+  }
+  __syncthreads();
+  if (rows_ok) {
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+      float tot = 0.f;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) tot += part[w * A.rows_per_cta + r];
       const int gr = r0 + r;
       if (A.rscale) tot *= A.rscale[gr];
       const float e = -tot;
@@ -227,8 +266,7 @@ __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_bulk_kernel(MvmArgs A) {
     }
   }
   // no CTA may exit with a copy still landing in its shared memory
-  __syncthreads();
-  if (threadIdx.x == 0)
+  if (!rows_ok && threadIdx.x == 0)
     for (int r = 0; r < R; ++r) mbar_wait(&bars[r], 0, MBAR_MAX_POLLS);
 }
 
@@ -383,7 +421,8 @@ void launch_mvm_t(const MvmArgs &A0, int grid, bool bulk, cudaStream_t s) {
   const size_t slope_bytes = sizeof(float) * mvm_smem_floats(A.ld, V);
   if (bulk) {
     A.rows_per_cta = (A.nrow + grid - 1) / grid;
-    const size_t sm = 128 * ((A.rows_per_cta * 8 + 127) / 128) + slope_bytes + (size_t)A.rows_per_cta * A.ld * sizeof(T);
+    const size_t sm = mvm_bars_bytes(A.rows_per_cta) + slope_bytes + (size_t)A.rows_per_cta * A.ld * sizeof(T) +
+                      sizeof(float) * (MVM_THREADS / 32) * A.rows_per_cta;
     AOB_CUDA(cudaFuncSetAttribute(ls_mvm_bulk_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     ls_mvm_bulk_kernel<T><<<grid, MVM_THREADS, sm, s>>>(A);
     AOB_LAUNCH_CHECK("ls_mvm_bulk_kernel");
@@ -408,7 +447,8 @@ void aob_ls::launch_mvm(MvmArgs &A, cudaStream_t s) {
   int grid = nblocks > 0 ? std::min(nblocks, nactu) : std::min(nactu, nsm);
   const size_t slope_bytes = sizeof(float) * mvm_smem_floats(A.ld, V);
   const int rpc = (nactu + grid - 1) / grid;
-  const size_t need = 128 * ((rpc * 8 + 127) / 128) + slope_bytes + (size_t)rpc * A.ld * esize;
+  const size_t need = mvm_bars_bytes(rpc) + slope_bytes + (size_t)rpc * A.ld * esize +
+                      sizeof(float) * (MVM_THREADS / 32) * rpc;
   const bool bulk = (mvm_kind == 0 || mvm_kind == 1) && need <= MVM_SMEM_MAX && mvm_kind != 2;
   if (prec == AOB_PREC_F32)
     launch_mvm_t<float>(A, grid, bulk, s);
