@@ -1,4 +1,4 @@
-"""Python objects over the C ABI: SH sensor, centroider, LS controller.
+"""Python objects over the C ABI: SH and pyramid sensors, centroider, LS controller.
 
 These are the host-side mirror of the reference's SutraWfsSH /
 SutraCentroider* / SutraControllerLs (see include/aob200.h for the file:line
@@ -170,8 +170,116 @@ class ShWfs:
         call("aob_sh_set_tuning", self.h, int(subaps_per_cta))
 
 
+class PyrWfs:
+    """High-resolution modulated pyramid sensor on one GPU (SutraWfs_PyrHR)."""
+
+    def __init__(self, nxsub, nvalid, npix, nphase, nrebin, nfft, ntot, npts, pdiam, nphot,
+                 nphot4imat=0.0, device=0, lambda_um=0.5):
+        self.h = ctypes.c_void_p()
+        call("aob_pyr_create", ctypes.addressof(self.h), int(device), int(nxsub), int(nvalid), int(npix),
+             int(nphase), int(nrebin), int(nfft), int(ntot), int(npts), float(pdiam), float(nphot),
+             float(nphot4imat))
+        self.nxsub, self.nvalid, self.npix, self.nphase = int(nxsub), int(nvalid), int(npix), int(nphase)
+        self.nrebin, self.nfft, self.ntot, self.npts = int(nrebin), int(nfft), int(ntot), int(npts)
+        self.pdiam, self.nphot = float(pdiam), float(nphot)
+        self.device = int(device)
+        self.noise = -1.0
+        self.lambda_um = float(lambda_um)
+        call("aob_pyr_set_lambda", self.h, float(lambda_um))
+
+    @classmethod
+    def from_geometry(cls, g, device=0, noise=-1.0, seed=1234, weights=None):
+        w = cls(g.nxsub, g.nvalid, g.npix, g.pdiam, g.nrebin, g.nfft, g.ntot, g.pyr_cx.size, g.pdiam,
+                g.nphotons, device=device, lambda_um=g.wavelength_um)
+        w.load_arrays(g.halfxy, g.pyr_cx, g.pyr_cy, weights, g.sincar, g.submask, g.validsubsx, g.validsubsy,
+                      g.phasemap, g.fluxPerSub)
+        w.set_pupil(g.tel.mpupil)
+        w.set_noise(noise, seed)
+        return w
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        try:
+            if h is not None and h.value and _lib._lib is not None:
+                _lib.lib().aob_pyr_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown: module globals already cleared
+            pass
+        self.h = None
+
+    def load_arrays(self, halfxy, cx, cy, weights, sincar, submask, validsubsx, validsubsy, phasemap=None,
+                    fluxPerSub=None, ttprojmat=None):
+        """``halfxy``: the pyramid phase (float) as the geometry gives it; it is passed on as
+        exp(i halfxy), transposed, like the reference's wfs_init (wfs_init.py:203)."""
+        f32 = np.float32
+        ph = np.exp(1j * np.asarray(halfxy, np.float64)).astype(np.complex64).T
+        hx = np.asfortranarray(ph).ravel(order="F").view(np.float32).copy()
+        w = np.ones(np.asarray(cx).size, f32) if weights is None else weights
+        keep = [hx, host_array(cx, f32), host_array(cy, f32), host_array(w, f32), host_array(sincar, f32),
+                host_array(submask, f32), host_array(validsubsx, np.int32), host_array(validsubsy, np.int32)]
+        flux = host_array(fluxPerSub, f32) if fluxPerSub is not None else None
+        call("aob_pyr_load_arrays", self.h, *[k.ctypes.data for k in keep], None,
+             flux.ctypes.data if flux is not None else None, None)
+
+    def set_modulation(self, cx, cy, weights=None):
+        f32 = np.float32
+        a, b = host_array(cx, f32), host_array(cy, f32)
+        w = host_array(np.ones(a.size, f32) if weights is None else weights, f32)
+        call("aob_pyr_set_modulation", self.h, a.ctypes.data, b.ctypes.data, w.ctypes.data, int(a.size))
+        self.npts = int(a.size)
+
+    def set_pupil(self, pupil):
+        a = host_array(pupil, np.float32)
+        if a.size != self.ntot * self.ntot:
+            raise ValueError("pupil must be ntot x ntot")
+        call("aob_pyr_set_pupil", self.h, a.ctypes.data)
+
+    def set_noise(self, noise, seed=1234):
+        self.noise = float(noise)
+        call("aob_pyr_set_noise", self.h, float(noise), int(seed))
+
+    def set_lambda(self, lam):
+        self.lambda_um = float(lam)
+        call("aob_pyr_set_lambda", self.h, float(lam))
+
+    def set_nphot(self, nphot):
+        self.nphot = float(nphot)
+        call("aob_pyr_set_nphot", self.h, float(nphot))
+
+    @property
+    def frame(self) -> int:
+        f = ctypes.c_uint64()
+        call("aob_pyr_get_frame", self.h, ctypes.addressof(f))
+        return f.value
+
+    @frame.setter
+    def frame(self, v):
+        call("aob_pyr_set_frame", self.h, int(v))
+
+    def buffer(self, which, dtype=np.float32, shape=None) -> DeviceArray:
+        return _buffer("aob_pyr_buffer", self.h, which, dtype, shape, self)
+
+    @property
+    def d_phase(self):
+        return self.buffer("phase", shape=(self.ntot, self.ntot))
+
+    @property
+    def d_binimg(self):
+        n = self.nfft // self.nrebin
+        return self.buffer("binimg", shape=(n, n))
+
+    @property
+    def d_hrimg(self):
+        return self.buffer("hrimg", shape=(self.nfft, self.nfft))
+
+    def set_phase(self, phase):
+        self.d_phase.set(phase)
+
+    def comp_image(self, noise=True, stream=None):
+        call("aob_pyr_comp_image", self.h, 1 if noise else 0, stream)
+
+
 class Centroider:
-    """CoG / tCoG / wCoG centroider (SutraCentroider*)."""
+    """CoG / tCoG / wCoG / pyramid centroider (SutraCentroider*)."""
 
     def __init__(self, nvalid, offset, scale, typec="cog", device=0, wfs: ShWfs | None = None):
         self.h = ctypes.c_void_p()
@@ -194,7 +302,17 @@ class Centroider:
 
     def attach(self, wfs):
         self.wfs = wfs
-        call("aob_centro_attach_wfs", self.h, wfs.h if wfs is not None else None)
+        if isinstance(wfs, PyrWfs):
+            call("aob_centro_attach_pyr", self.h, wfs.h)
+        else:
+            call("aob_centro_attach_wfs", self.h, wfs.h if wfs is not None else None)
+
+    def set_pyr_method(self, method):
+        """0 nosin_global (default), 1 sin_global, 2 nosin_local, 3 sin_local."""
+        call("aob_centro_set_pyr_method", self.h, int(method))
+
+    def set_pyr_thresh(self, thresh):
+        call("aob_centro_set_pyr_thresh", self.h, float(thresh))
 
     def set_npix(self, npix):
         call("aob_centro_set_npix", self.h, int(npix))

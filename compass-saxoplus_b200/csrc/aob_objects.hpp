@@ -68,7 +68,41 @@ struct aob_sh {
 };
 
 // ---------------------------------------------------------------------------
-// centroiders (replaces SutraCentroiderCog / Tcog / Wcog)
+// high-resolution pyramid sensor (replaces SutraWfs_PyrHR)
+struct aob_pyr {
+  int device = 0;
+  int nxsub, nvalid, npix, nphase, nrebin, nfft, ntot, npts = 0;
+  int logn = 0;
+  float pdiam, nphot, nphot4imat;
+  float lambda_um = 0.5f;
+  float noise = -1.f;
+  int64_t seed = 1234;
+  uint64_t frame = 0;
+  bool loaded = false;
+  uint64_t image_gen = 0;
+  aob::DevBuf<float> phase, pupil;                 // ntot x ntot
+  aob::DevBuf<float> cx, cy, weights;              // modulation points
+  aob::DevBuf<float> submask, sincar;              // nfft x nfft (x fastest)
+  aob::DevBuf<float2> phalfxy;                     // exp(i pyramid phase), nfft x nfft
+  aob::DevBuf<float2> work;                        // npts x nfft x nfft focal / pupil planes
+  aob::DevBuf<float2> conv;                        // nfft x nfft, pixel-transfer convolution
+  aob::DevBuf<float> hrimg;                        // nfft x nfft high-resolution image
+  aob::DevBuf<float> binimg, partial;              // (nfft/nrebin)^2 image, per-row sums
+  aob::DevBuf<int32_t> validsubsx, validsubsy;     // 4 * nvalid pupil-image pixels
+  aob::DevBuf<float> fluxPerSub;
+
+  aob_pyr(int device, int nxsub, int nvalid, int npix, int nphase, int nrebin, int nfft, int ntot, int npts,
+          float pdiam, float nphot, float nphot4imat);
+  void load_arrays(const float2 *halfxy, const float *cx, const float *cy, const float *weights, const float *sincar,
+                   const float *submask, const int32_t *validsubsx, const int32_t *validsubsy,
+                   const float *fluxPerSub);
+  void set_modulation(const float *cx, const float *cy, const float *weights, int npts);
+  void comp_image(bool noise, cudaStream_t s);
+  int nbin() const { return nfft / nrebin; }
+};
+
+// ---------------------------------------------------------------------------
+// centroiders (replaces SutraCentroiderCog / Tcog / Wcog / Pyr)
 struct aob_centro {
   int device = 0;
   int type = 0;
@@ -77,6 +111,9 @@ struct aob_centro {
   float offset = 0.f, scale = 1.f, threshold = 0.f;
   int order = 0;
   aob_sh *wfs = nullptr;
+  aob_pyr *pyr = nullptr;       // pyramid centroider: the sensor whose image it reads
+  float valid_thresh = 1.e-4f;  // pyramid: flux below which slopes are 0
+  int pyr_method = 0;           // pyramid: bit 0 sine of the ratio, bit 1 per-sub-aperture flux
   aob::DevBuf<int32_t> validx, validy;
   aob::DevBuf<float> ref, weights, intensities;
   int weights_per_sub = 0;  // 0: one npix^2 map, 1: npix^2*nvalid

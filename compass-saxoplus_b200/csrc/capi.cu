@@ -262,6 +262,30 @@ int aob_centro_attach_wfs(aob_centro *c, aob_sh *h) {
   c->touch();
   AOB_API_END
 }
+int aob_centro_attach_pyr(aob_centro *c, aob_pyr *p) {
+  AOB_API_BEGIN
+  NEED(c);
+  if (c->type != AOB_CENTRO_PYR) throw Error("centro.attach_pyr: not a pyramid centroider");
+  if (p && p->nvalid != c->nvalid) throw Error("centro.attach_pyr: nvalid differs from the sensor's");
+  c->pyr = p;
+  c->touch();
+  AOB_API_END
+}
+int aob_centro_set_pyr_method(aob_centro *c, int method) {
+  AOB_API_BEGIN
+  NEED(c);
+  if (method < 0 || method > 3) throw Error("centro.set_pyr_method: method must be 0..3");
+  c->pyr_method = method;
+  c->touch();
+  AOB_API_END
+}
+int aob_centro_set_pyr_thresh(aob_centro *c, float thresh) {
+  AOB_API_BEGIN
+  NEED(c);
+  c->valid_thresh = thresh;
+  c->touch();
+  AOB_API_END
+}
 int aob_centro_set_npix(aob_centro *c, int npix) {
   AOB_API_BEGIN
   NEED(c);
@@ -302,9 +326,10 @@ int aob_centro_set_slope_order(aob_centro *c, int order) {
 int aob_centro_load_validpos(aob_centro *c, const int32_t *vx, const int32_t *vy, int n) {
   AOB_API_BEGIN
   NEED(c); NEED(vx); NEED(vy);
-  if (n != c->nvalid) throw Error("centro.load_validpos: n must equal nvalid");
+  const int want = c->type == AOB_CENTRO_PYR ? 4 * c->nvalid : c->nvalid;
+  if (n != want) throw Error("centro.load_validpos: n must equal nvalid (4 * nvalid for a pyramid centroider)");
   AOB_CUDA(cudaSetDevice(c->device));
-  if (!c->validx.p) {
+  if (!c->validx.p || c->validx.n != n) {
     c->validx.alloc(n);
     c->validy.alloc(n);
   }
@@ -617,6 +642,108 @@ int aob_ls_get_params(aob_ls *c, int *nslope, int *nactu, float *delay, float *g
   if (vmin) *vmin = c->volt_min;
   if (vmax) *vmax = c->volt_max;
   if (prec) *prec = c->prec;
+  AOB_API_END
+}
+
+// ---- pyramid sensor ---------------------------------------------------------
+int aob_pyr_create(aob_pyr **out, int device, int nxsub, int nvalid, int npix, int nphase, int nrebin, int nfft,
+                   int ntot, int npts, float pdiam, float nphot, float nphot4imat) {
+  AOB_API_BEGIN
+  NEED(out);
+  *out = nullptr;
+  AOB_CUDA(cudaSetDevice(device));
+  *out = new aob_pyr(device, nxsub, nvalid, npix, nphase, nrebin, nfft, ntot, npts, pdiam, nphot, nphot4imat);
+  AOB_API_END
+}
+int aob_pyr_destroy(aob_pyr *h) {
+  AOB_API_BEGIN
+  if (h) {
+    cudaSetDevice(h->device);
+    delete h;
+  }
+  AOB_API_END
+}
+int aob_pyr_load_arrays(aob_pyr *h, const float *halfxy_c64, const float *cx, const float *cy, const float *weights,
+                        const float *sincar, const float *submask, const int32_t *validsubsx,
+                        const int32_t *validsubsy, const int32_t *phasemap, const float *fluxPerSub,
+                        const float *ttprojmat) {
+  AOB_API_BEGIN
+  NEED(h);
+  (void)phasemap;
+  (void)ttprojmat;
+  AOB_CUDA(cudaSetDevice(h->device));
+  h->load_arrays(reinterpret_cast<const float2 *>(halfxy_c64), cx, cy, weights, sincar, submask, validsubsx,
+                 validsubsy, fluxPerSub);
+  AOB_API_END
+}
+int aob_pyr_set_modulation(aob_pyr *h, const float *cx, const float *cy, const float *weights, int npts) {
+  AOB_API_BEGIN
+  NEED(h);
+  AOB_CUDA(cudaSetDevice(h->device));
+  h->set_modulation(cx, cy, weights, npts);
+  AOB_API_END
+}
+int aob_pyr_set_pupil(aob_pyr *h, const float *pupil_host) {
+  AOB_API_BEGIN
+  NEED(h); NEED(pupil_host);
+  AOB_CUDA(cudaSetDevice(h->device));
+  h->pupil.upload(pupil_host, h->pupil.n);
+  AOB_API_END
+}
+int aob_pyr_set_noise(aob_pyr *h, float noise, int64_t seed) {
+  AOB_API_BEGIN
+  NEED(h);
+  h->noise = noise;
+  h->seed = seed;
+  AOB_API_END
+}
+int aob_pyr_set_lambda(aob_pyr *h, float lambda_um) {
+  AOB_API_BEGIN
+  NEED(h);
+  if (!(lambda_um > 0.f)) throw Error("pyr.set_lambda: lambda must be > 0");
+  h->lambda_um = lambda_um;
+  AOB_API_END
+}
+int aob_pyr_set_nphot(aob_pyr *h, float nphot) {
+  AOB_API_BEGIN
+  NEED(h);
+  h->nphot = nphot;
+  AOB_API_END
+}
+int aob_pyr_set_frame(aob_pyr *h, uint64_t frame) {
+  AOB_API_BEGIN
+  NEED(h);
+  h->frame = frame;
+  AOB_API_END
+}
+int aob_pyr_get_frame(aob_pyr *h, uint64_t *frame) {
+  AOB_API_BEGIN
+  NEED(h); NEED(frame);
+  *frame = h->frame;
+  AOB_API_END
+}
+int aob_pyr_buffer(aob_pyr *h, const char *which, void **dev_ptr, int64_t *nelem) {
+  AOB_API_BEGIN
+  NEED(h); NEED(which); NEED(dev_ptr);
+  const std::string w(which);
+  void *p = nullptr;
+  int64_t n = 0;
+  if (w == "phase") { p = h->phase.p; n = h->phase.n; }
+  else if (w == "pupil") { p = h->pupil.p; n = h->pupil.n; }
+  else if (w == "binimg") { p = h->binimg.p; n = h->binimg.n; }
+  else if (w == "hrimg") { p = h->hrimg.p; n = h->hrimg.n; }
+  else if (w == "validsubsx") { p = h->validsubsx.p; n = h->validsubsx.n; }
+  else if (w == "validsubsy") { p = h->validsubsy.p; n = h->validsubsy.n; }
+  else if (w == "fluxPerSub") { p = h->fluxPerSub.p; n = h->fluxPerSub.n; }
+  else throw Error("pyr.buffer: unknown buffer '" + w + "'");
+  *dev_ptr = p;
+  if (nelem) *nelem = n;
+  AOB_API_END
+}
+int aob_pyr_comp_image(aob_pyr *h, int noise, void *stream) {
+  AOB_API_BEGIN
+  NEED(h);
+  h->comp_image(noise != 0, S(stream));
   AOB_API_END
 }
 

@@ -81,6 +81,55 @@ __global__ void tcog_writeback_kernel(float *img, int size, const int32_t *valid
   }
 }
 
+// Pyramid slopes (pyr2slopes_krnl, libsutra/src.cu/sutra_centroider_pyr.cu:27-69,
+// flux as intensities_krnl, sutra_wfs.cu:2041-2054).  Quadrant k of valid
+// sub-aperture i is the binned-image pixel (validx[i + k nvalid], validy[...]).
+// With the global method (the reference default, nosin_global) every
+// sub-aperture is normalised by the mean flux (fillvalues, carma_obj.cu:194-201);
+// the sum runs in a fixed order (per-thread partial sums, then a tree), so
+// the slopes are deterministic.  One CTA.
+constexpr int PYR_SLOPE_THREADS = 1024;
+__global__ void __launch_bounds__(PYR_SLOPE_THREADS)
+    pyr_slopes_kernel(const float *img, int ns, const int32_t *vx, const int32_t *vy, int nvalid, float scale,
+                      float thresh, int method, const float *ref, int order, float *slopes, float *inten) {
+  __shared__ float red[PYR_SLOPE_THREADS];
+  const bool sinus = method & 1, local = method & 2;
+  float part = 0.f;
+  for (int i = threadIdx.x; i < nvalid; i += blockDim.x) {
+    const float q1 = img[vx[i] + vy[i] * ns], q2 = img[vx[i + nvalid] + vy[i + nvalid] * ns];
+    const float q3 = img[vx[i + 2 * nvalid] + vy[i + 2 * nvalid] * ns];
+    const float q4 = img[vx[i + 3 * nvalid] + vy[i + 3 * nvalid] * ns];
+    const float f = q1 + q2 + q3 + q4;
+    inten[i] = f;
+    part += f;
+  }
+  red[threadIdx.x] = part;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  const float mean = red[0] / (float)nvalid;
+  for (int i = threadIdx.x; i < nvalid; i += blockDim.x) {
+    const float q1 = img[vx[i] + vy[i] * ns], q2 = img[vx[i + nvalid] + vy[i + nvalid] * ns];
+    const float q3 = img[vx[i + 2 * nvalid] + vy[i + 2 * nvalid] * ns];
+    const float q4 = img[vx[i + 3 * nvalid] + vy[i + 3 * nvalid] * ns];
+    const float f = local ? inten[i] : mean;
+    const int ix = order ? 2 * i : i;
+    const int iy = order ? 2 * i + 1 : i + nvalid;
+    float sx = 0.f, sy = 0.f;
+    if (!(f < thresh)) {
+      const float tx = ((q1 + q4) - (q2 + q3)) / f;
+      const float ty = ((q1 + q3) - (q2 + q4)) / f;
+      sx = sinus ? scale * sinpif(tx / 2.f) : scale * tx;
+      sy = sinus ? scale * sinpif(ty / 2.f) : scale * ty;
+    }
+    slopes[ix] = sx - ref[ix];
+    slopes[iy] = sy - ref[iy];
+    if (!local) inten[i] = mean;
+  }
+}
+
 __global__ void calib_kernel(const float *raw, float *cal, const float *dark, const float *flat, int64_t n) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
     cal[t] = (raw[t] - dark[t]) * flat[t];
@@ -121,6 +170,24 @@ void aob_centro::calibrate(cudaStream_t s) {
 }
 
 void aob_centro::get_cog(float *dev_slopes, cudaStream_t s) {
+  if (type == 3) {
+    AOB_REQUIRE(validx.p != nullptr && validx.n >= 4 * (int64_t)nvalid, "get_pyr: 4 * nvalid valid positions not loaded");
+    const float *im;
+    int ns;
+    if (pyr) {
+      im = pyr->binimg.p;
+      ns = pyr->nbin();
+    } else {
+      AOB_REQUIRE(img.p != nullptr, "get_pyr: no image (attach a pyramid sensor or load_img + calibrate_img)");
+      im = img.p;
+      ns = img_m;
+    }
+    AOB_CUDA(cudaSetDevice(device));
+    pyr_slopes_kernel<<<1, PYR_SLOPE_THREADS, 0, s>>>(im, ns, validx.p, validy.p, nvalid, scale, valid_thresh, pyr_method,
+                                                      ref.p, order, dev_slopes, intensities.p);
+    AOB_LAUNCH_CHECK("pyr_slopes_kernel");
+    return;
+  }
   AOB_REQUIRE(type <= 2, "get_cog: not a CoG-family centroider");
   AOB_REQUIRE(npix > 0, "get_cog: npix not set");
   AOB_REQUIRE(validx.p != nullptr && validx.n >= nvalid, "get_cog: valid positions not loaded");

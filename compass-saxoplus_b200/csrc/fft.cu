@@ -44,33 +44,6 @@ const float2 *fft_twiddles(int device, int n) {
   return b->p;
 }
 
-__device__ __forceinline__ uint32_t bitrev(uint32_t x, int logn) { return __brev(x) >> (32 - logn); }
-
-// In-shared-memory radix-2 transform of ``cols`` interleaved sequences:
-// element m of sequence c lives at s[m * cols + c].
-__device__ __forceinline__ void smem_fft(float2 *s, int n, int logn, int cols, const float2 *tw, int inverse) {
-  const int nb = (n / 2) * cols;  // butterflies per stage
-  for (int st = 0; st < logn; ++st) {
-    const int half = 1 << st;
-    const int tstep = n >> (st + 1);
-    for (int t = threadIdx.x; t < nb; t += blockDim.x) {
-      const int c = t % cols;
-      const int b = t / cols;
-      const int grp = b >> st;
-      const int pos = b & (half - 1);
-      const int i = (grp * 2 * half + pos) * cols + c;
-      const int j = i + half * cols;
-      float2 w = __ldg(tw + pos * tstep);
-      if (inverse) w.y = -w.y;
-      const float2 u = s[i], v0 = s[j];
-      const float2 v = make_float2(v0.x * w.x - v0.y * w.y, v0.x * w.y + v0.y * w.x);
-      s[i] = make_float2(u.x + v.x, u.y + v.y);
-      s[j] = make_float2(u.x - v.x, u.y - v.y);
-    }
-    __syncthreads();
-  }
-}
-
 __global__ void fft_rows_kernel(float2 *data, int n, int logn, const float2 *tw, int inverse) {
   extern __shared__ float2 srow[];
   float2 *row = data + (size_t)blockIdx.x * n;  // blockIdx.x = row index over the whole batch

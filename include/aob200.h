@@ -100,6 +100,42 @@ int aob_sh_set_tuning(aob_sh *h, int subaps_per_cta);
 int aob_sh_set_bincube(aob_sh *h, const float *host, int64_t n);
 int aob_sh_set_binimg(aob_sh *h, const float *host, int64_t n);
 
+/* ---- pyramid sensor ------------------------------------------------- *
+ * Replaces SutraWfs_PyrHR (libsutra/src.cpp/sutra_wfs_pyr_pyrhr.cpp) as bound
+ * by python_module/sutra/src/wfs_pyrhr.cpp:131-163.  npts modulation points,
+ * nfft x nfft focal plane, ntot x ntot phase grid; binned image of
+ * (nfft / nrebin)^2 pixels.                                               */
+typedef struct aob_pyr aob_pyr;
+/* Constructor arguments of SutraWfs_PyrHR (sutra_wfs_pyr_pyrhr.cpp:28-120);
+ * npts is the reference's npup (number of modulation points). */
+int aob_pyr_create(aob_pyr **out, int device, int nxsub, int nvalid, int npix, int nphase, int nrebin,
+                   int nfft, int ntot, int npts, float pdiam, float nphot, float nphot4imat);
+int aob_pyr_destroy(aob_pyr *h);
+/* PYRWFS.load_arrays(halfxy, cx, cy, weights, sincar, submask, validsubsx,
+ * validsubsy, phasemap, fluxPerSub, ttprojmat) (sutra_wfs_pyr_pyrhr.cpp:313-350):
+ * halfxy = exp(i pyramid phase) as nfft^2 complex64 (float pairs), the
+ * reference's layout; cx, cy, weights: npts modulation tilts / weights
+ * (weights may be NULL = 1); sincar, submask: nfft^2; validsubsx / validsubsy:
+ * 4 * nvalid; phasemap and ttprojmat are accepted for interface parity. */
+int aob_pyr_load_arrays(aob_pyr *h, const float *halfxy_c64, const float *cx, const float *cy,
+                        const float *weights, const float *sincar, const float *submask,
+                        const int32_t *validsubsx, const int32_t *validsubsy, const int32_t *phasemap,
+                        const float *fluxPerSub, const float *ttprojmat);
+/* set_pyr_modulation_points (sutra_wfs_pyr_pyrhr.cpp:695-720). */
+int aob_pyr_set_modulation(aob_pyr *h, const float *cx, const float *cy, const float *weights, int npts);
+int aob_pyr_set_pupil(aob_pyr *h, const float *pupil_host);
+/* Photon (noise > -1) and readout (noise > 0) noise with the SH sensor's
+ * Philox streams keyed by seed. */
+int aob_pyr_set_noise(aob_pyr *h, float noise, int64_t seed);
+int aob_pyr_set_lambda(aob_pyr *h, float lambda_um);
+int aob_pyr_set_nphot(aob_pyr *h, float nphot);
+int aob_pyr_set_frame(aob_pyr *h, uint64_t frame);
+int aob_pyr_get_frame(aob_pyr *h, uint64_t *frame);
+/* which: "phase", "pupil", "binimg", "hrimg", "validsubsx", "validsubsy", "fluxPerSub". */
+int aob_pyr_buffer(aob_pyr *h, const char *which, void **dev_ptr, int64_t *nelem);
+/* SutraWfs_PyrHR::comp_image(noise) (sutra_wfs_pyr_pyrhr.cpp:379-627). */
+int aob_pyr_comp_image(aob_pyr *h, int noise, void *stream);
+
 /* ---- centroiders ------------------------------------------------------ *
  * Replaces SutraCentroiderCog / Tcog / Wcog (libsutra/src.cpp/
  * sutra_centroider_{cog,tcog,wcog}.cpp, kernels sutra_centroider_*.cu) as
@@ -125,7 +161,19 @@ int aob_centro_set_scale(aob_centro *c, float scale);
 int aob_centro_set_offset(aob_centro *c, float offset);
 int aob_centro_set_threshold(aob_centro *c, float threshold);
 int aob_centro_set_slope_order(aob_centro *c, int order);
-/* load_validpos (sutra_centroider.cpp:287-298). */
+/* Pyramid centroider (type AOB_CENTRO_PYR, SutraCentroiderPyr::get_pyr,
+ * libsutra/src.cpp/sutra_centroider_pyr.cpp:101-130): reads the binned image
+ * of the attached pyramid sensor; its valid positions are 4 * nvalid pixels
+ * (quadrant k of sub-aperture i at entry i + k nvalid).  method (set_pyr_method,
+ * python_module/sutra/src/centroider_pyr.cpp:35-64): bit 0 = sine of the
+ * normalised difference, bit 1 = per-sub-aperture flux (default 0 = the
+ * reference's nosin_global).  thresh: flux below which the slopes are 0
+ * (reference default 1e-4). */
+int aob_centro_attach_pyr(aob_centro *c, aob_pyr *p);
+int aob_centro_set_pyr_method(aob_centro *c, int method);
+int aob_centro_set_pyr_thresh(aob_centro *c, float thresh);
+/* load_validpos (sutra_centroider.cpp:287-298); n = nvalid (4 * nvalid for a
+ * pyramid centroider). */
 int aob_centro_load_validpos(aob_centro *c, const int32_t *validx, const int32_t *validy, int n);
 /* set_centroids_ref (sutra_centroider.cpp:300-304). */
 int aob_centro_set_centroids_ref(aob_centro *c, const float *ref);

@@ -1,0 +1,81 @@
+"""Modulated pyramid image formation and slopes in float64 (oracle).
+
+Follows the reference's SutraWfs_PyrHR::comp_generic / comp_modulation
+(libsutra/src.cpp/sutra_wfs_pyr_pyrhr.cpp:379-627) and kernels:
+  pyrgetpup_krnl  libsutra/src.cu/sutra_wfs.cu:1191-1233  padded field with the modulation tilt
+  CarmaFFT dir -1 (cuFFT inverse), libcarma/src.cpp/carma_fft.cpp:175-179
+  submask_krnl, submaskpyr_krnl   sutra_wfs.cu:1864-1958  field stop, pyramid phase
+  CarmaFFT dir +1 (cuFFT forward), abs2_krnl with factor   sutra_utils.cu:118-142
+  pixel transfer: inverse FFT, x sincar, forward FFT, real part
+  pyr_bimg_krnl   sutra_wfs.cu:1580-1630   nrebin x nrebin binning
+  pyr_fact        normalisation to nphot by the image sum
+and SutraCentroiderPyr::get_pyr (libsutra/src.cpp/sutra_centroider_pyr.cpp:101-130,
+pyr2slopes_krnl libsutra/src.cu/sutra_centroider_pyr.cu:27-69).
+
+Arrays are indexed [x, y] with x the fastest device index.  The pyramid
+phase mask is exp(i halfxy) transposed, as the reference's wfs_init passes it
+(shesha/shesha/init/wfs_init.py:203).
+"""
+
+import numpy as np
+
+from . import philox
+
+
+def hr_image(phase, pupil, g, lam_um, weights=None):
+    """High-resolution modulated image (before the pixel transfer function)."""
+    n_fft = g.nfft
+    n = phase.shape[0]
+    off = int((n_fft - n) / 2.0)
+    xx = np.arange(n) - n / 2.0
+    mask = g.submask.astype(np.float64) * np.exp(1j * g.halfxy.astype(np.float64)).T
+    w = np.ones(g.pyr_cx.size) if weights is None else np.asarray(weights, np.float64)
+    mic2rad = 2 * np.pi / lam_um
+    hr = np.zeros((n_fft, n_fft))
+    base = phase.astype(np.float64) * mic2rad
+    amp = pupil.astype(np.float64)
+    for p in range(g.pyr_cx.size):
+        phi = float(g.pyr_cx[p]) * xx[:, None] + float(g.pyr_cy[p]) * xx[None, :]
+        f = np.zeros((n_fft, n_fft), dtype=np.complex128)
+        f[off:off + n, off:off + n] = amp * np.exp(1j * (base + phi))
+        F = np.fft.ifft2(f) * (n_fft * n_fft)
+        G = np.fft.fft2(F * mask)
+        hr += w[p] * (G.real ** 2 + G.imag ** 2)
+    return hr
+
+
+def comp_image(phase, pupil, g, lam_um, nphot, weights=None, noise=-1.0, frame=0, seed=1234):
+    """Binned, normalised (and optionally noisy) pyramid image [nb, nb]."""
+    n_fft = g.nfft
+    hr = hr_image(phase, pupil, g, lam_um, weights)
+    T = np.fft.ifft2(hr) * (n_fft * n_fft)
+    hr2 = np.fft.fft2(T * g.sincar.astype(np.float64)).real
+    r = g.nrebin
+    nb = n_fft // r
+    b = hr2.reshape(nb, r, nb, r).sum(axis=(1, 3)) / (r * r)
+    b = b * (nphot / b.sum())
+    if noise > -1:
+        lam = b.astype(np.float32).ravel(order="F")
+        idx = np.arange(lam.size, dtype=np.uint64)
+        v = philox.poisson(lam, idx, frame, seed)
+        if noise > 0:
+            v = v + noise * philox.gaussian(idx, frame, seed).astype(np.float64)
+        b = v.reshape(nb, nb, order="F")
+    return b
+
+
+def slopes(img, validsubsx, validsubsy, nvalid, scale, ref=None, thresh=1e-4, method=0):
+    """Pyramid slopes (untied order) and the flux used for each sub-aperture."""
+    b = np.asarray(img, np.float64)
+    q = [b[validsubsx[k * nvalid:(k + 1) * nvalid], validsubsy[k * nvalid:(k + 1) * nvalid]] for k in range(4)]
+    flux = q[0] + q[1] + q[2] + q[3]
+    f = flux if (method & 2) else np.full(nvalid, flux.sum() / nvalid)
+    tx = ((q[0] + q[3]) - (q[1] + q[2])) / f
+    ty = ((q[0] + q[2]) - (q[1] + q[3])) / f
+    if method & 1:
+        tx, ty = np.sin(np.pi * tx / 2), np.sin(np.pi * ty / 2)
+    s = np.concatenate([scale * tx, scale * ty])
+    s[np.concatenate([f < thresh, f < thresh])] = 0.0
+    if ref is not None:
+        s = s - ref
+    return s, f

@@ -204,3 +204,43 @@ def test_poisson_sampler_matches_the_pmf(lam):
     chi2 = np.sum((obs - n * exp_p) ** 2 / (n * exp_p))
     p = stats.chi2.sf(chi2, len(obs) - 1)
     assert p > 1e-4, (lam, chi2, len(obs))
+
+
+@pytest.fixture(scope="module")
+def pyr16():
+    return G.pyr_geometry(G.PyrParams(nxsub=16, wavelength_um=0.7, ampl=3.0, npts=8, pup_sep=12, fssize=3.2), 64,
+                          diam=8.0, cobs=0.14)
+
+
+def test_pyramid_flat_wavefront_is_balanced(pyr16):
+    """Flat wavefront: the four pupil images carry equal flux and the mean slopes vanish."""
+    from oracle import pyr as opyr
+
+    g = pyr16
+    n = g.tel.n
+    img = opyr.comp_image(np.zeros((n, n)), g.tel.mpupil, g, g.wavelength_um, g.nphotons)
+    np.testing.assert_allclose(img.sum(), g.nphotons, rtol=1e-10)
+    s, flux = opyr.slopes(img, g.validsubsx, g.validsubsy, g.nvalid, 1.0)
+    q = [img[g.validsubsx[k * g.nvalid:(k + 1) * g.nvalid], g.validsubsy[k * g.nvalid:(k + 1) * g.nvalid]].sum()
+         for k in range(4)]
+    assert max(q) / min(q) - 1 < 1e-6
+    # per-sub-aperture slopes of a flat wavefront are not zero (edge diffraction,
+    # hence reference slopes) but they are antisymmetric: their means vanish
+    assert abs(s[:g.nvalid].mean()) < 1e-6 and abs(s[g.nvalid:].mean()) < 1e-6
+
+
+def test_pyramid_tilt_response_is_linear_and_signed(pyr16):
+    """A small tilt moves the x slopes, in proportion, and leaves the y slopes at zero on average."""
+    from oracle import pyr as opyr
+
+    g = pyr16
+    n = g.tel.n
+    x = (np.arange(n) - n / 2.0)[:, None] * np.ones((1, n))
+    out = []
+    for amp in (0.0005, 0.001):  # small-signal range of the modulated pyramid
+        img = opyr.comp_image(amp * x, g.tel.mpupil, g, g.wavelength_um, g.nphotons)
+        s, _ = opyr.slopes(img, g.validsubsx, g.validsubsy, g.nvalid, 1.0)
+        out.append((s[:g.nvalid].mean(), s[g.nvalid:].mean()))
+    (sx1, sy1), (sx2, sy2) = out
+    assert abs(sx1) > 1e-3 and abs(sx2 / sx1 - 2) < 0.1
+    assert abs(sy1) < 0.05 * abs(sx1) and abs(sy2) < 0.05 * abs(sx2)
