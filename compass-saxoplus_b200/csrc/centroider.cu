@@ -89,17 +89,38 @@ __global__ void tcog_writeback_kernel(float *img, int size, const int32_t *valid
 // the sum runs in a fixed order (per-thread partial sums, then a tree), so
 // the slopes are deterministic.  One CTA.
 constexpr int PYR_SLOPE_THREADS = 1024;
+constexpr int PYR_SLOPE_REG = 4;  // sub-apertures per thread kept in registers
 __global__ void __launch_bounds__(PYR_SLOPE_THREADS)
     pyr_slopes_kernel(const float *img, int ns, const int32_t *vx, const int32_t *vy, int nvalid, float scale,
                       float thresh, int method, const float *ref, int order, float *slopes, float *inten) {
   __shared__ float red[PYR_SLOPE_THREADS];
   const bool sinus = method & 1, local = method & 2;
+  auto quad = [&](int i, float *q) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) q[k] = img[vx[i + k * nvalid] + vy[i + k * nvalid] * ns];
+  };
+  // quadrant pixels of this thread's sub-apertures: gathered once (all loads
+  // issued before use) and kept in registers for the slope pass
+  float qr[PYR_SLOPE_REG][4];
+#pragma unroll
+  for (int it = 0; it < PYR_SLOPE_REG; ++it) {
+    const int i = threadIdx.x + it * blockDim.x;
+    if (i < nvalid) quad(i, qr[it]);
+  }
   float part = 0.f;
-  for (int i = threadIdx.x; i < nvalid; i += blockDim.x) {
-    const float q1 = img[vx[i] + vy[i] * ns], q2 = img[vx[i + nvalid] + vy[i + nvalid] * ns];
-    const float q3 = img[vx[i + 2 * nvalid] + vy[i + 2 * nvalid] * ns];
-    const float q4 = img[vx[i + 3 * nvalid] + vy[i + 3 * nvalid] * ns];
-    const float f = q1 + q2 + q3 + q4;
+#pragma unroll
+  for (int it = 0; it < PYR_SLOPE_REG; ++it) {
+    const int i = threadIdx.x + it * blockDim.x;
+    if (i < nvalid) {
+      const float f = qr[it][0] + qr[it][1] + qr[it][2] + qr[it][3];
+      inten[i] = f;
+      part += f;
+    }
+  }
+  for (int i = threadIdx.x + PYR_SLOPE_REG * blockDim.x; i < nvalid; i += blockDim.x) {
+    float q[4];
+    quad(i, q);
+    const float f = q[0] + q[1] + q[2] + q[3];
     inten[i] = f;
     part += f;
   }
@@ -110,23 +131,30 @@ __global__ void __launch_bounds__(PYR_SLOPE_THREADS)
     __syncthreads();
   }
   const float mean = red[0] / (float)nvalid;
-  for (int i = threadIdx.x; i < nvalid; i += blockDim.x) {
-    const float q1 = img[vx[i] + vy[i] * ns], q2 = img[vx[i + nvalid] + vy[i + nvalid] * ns];
-    const float q3 = img[vx[i + 2 * nvalid] + vy[i + 2 * nvalid] * ns];
-    const float q4 = img[vx[i + 3 * nvalid] + vy[i + 3 * nvalid] * ns];
+  auto emit = [&](int i, const float *q) {
     const float f = local ? inten[i] : mean;
     const int ix = order ? 2 * i : i;
     const int iy = order ? 2 * i + 1 : i + nvalid;
     float sx = 0.f, sy = 0.f;
     if (!(f < thresh)) {
-      const float tx = ((q1 + q4) - (q2 + q3)) / f;
-      const float ty = ((q1 + q3) - (q2 + q4)) / f;
+      const float tx = ((q[0] + q[3]) - (q[1] + q[2])) / f;
+      const float ty = ((q[0] + q[2]) - (q[1] + q[3])) / f;
       sx = sinus ? scale * sinpif(tx / 2.f) : scale * tx;
       sy = sinus ? scale * sinpif(ty / 2.f) : scale * ty;
     }
     slopes[ix] = sx - ref[ix];
     slopes[iy] = sy - ref[iy];
     if (!local) inten[i] = mean;
+  };
+#pragma unroll
+  for (int it = 0; it < PYR_SLOPE_REG; ++it) {
+    const int i = threadIdx.x + it * blockDim.x;
+    if (i < nvalid) emit(i, qr[it]);
+  }
+  for (int i = threadIdx.x + PYR_SLOPE_REG * blockDim.x; i < nvalid; i += blockDim.x) {
+    float q[4];
+    quad(i, q);
+    emit(i, q);
   }
 }
 

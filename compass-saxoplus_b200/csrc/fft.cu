@@ -1,10 +1,10 @@
 // Batched complex 2-D FFT for power-of-two sizes (16 .. 2048), single
 // precision, in place.  Used for the target PSF and the pyramid sensor.
 //
-// Row pass: one CTA per row, the row staged in shared memory in bit-reversed
-// order, log2(n) radix-2 butterfly stages, written back.  Column pass: one CTA
-// per group of 8 adjacent columns (64-byte row segments, coalesced), the same
-// transform per column in shared memory.  Twiddles come from a table computed
+// Row pass: one CTA per row, the row staged in shared memory, Stockham
+// radix-8 passes with the butterflies in registers (fft.cuh), written back.
+// Column pass: one CTA per group of 8 adjacent columns (64-byte row segments,
+// coalesced), the same transform per column in shared memory.  Twiddles come from a table computed
 // in double on the host.  Sign convention of cuFFT: forward = exp(-2 pi i k m / n),
 // inverse = exp(+2 pi i k m / n), both unnormalised.
 
@@ -47,9 +47,9 @@ const float2 *fft_twiddles(int device, int n) {
 __global__ void fft_rows_kernel(float2 *data, int n, int logn, const float2 *tw, int inverse) {
   extern __shared__ float2 srow[];
   float2 *row = data + (size_t)blockIdx.x * n;  // blockIdx.x = row index over the whole batch
-  for (int i = threadIdx.x; i < n; i += blockDim.x) srow[bitrev(i, logn)] = row[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) srow[i] = row[i];
   __syncthreads();
-  smem_fft(srow, n, logn, 1, tw, inverse);
+  smem_fft_stockham<1>(srow, n, 1, tw, inverse != 0);
   for (int i = threadIdx.x; i < n; i += blockDim.x) row[i] = srow[i];
 }
 
@@ -63,10 +63,10 @@ __global__ void fft_cols_kernel(float2 *data, int n, int logn, const float2 *tw,
   float2 *base = data + (size_t)img * n * n + c0;
   for (int t = threadIdx.x; t < n * FFT_COLS; t += blockDim.x) {
     const int m = t / FFT_COLS, c = t - m * FFT_COLS;
-    scol[bitrev(m, logn) * FFT_COLS + c] = base[(size_t)m * n + c];
+    scol[m * FFT_COLS + c] = base[(size_t)m * n + c];
   }
   __syncthreads();
-  smem_fft(scol, n, logn, FFT_COLS, tw, inverse);
+  smem_fft_stockham<4>(scol, n, FFT_COLS, tw, inverse != 0);
   for (int t = threadIdx.x; t < n * FFT_COLS; t += blockDim.x) {
     const int m = t / FFT_COLS, c = t - m * FFT_COLS;
     base[(size_t)m * n + c] = scol[m * FFT_COLS + c];

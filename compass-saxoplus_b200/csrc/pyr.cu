@@ -14,14 +14,17 @@
 // Here the npts modulation planes (npts x nfft^2 complex, 50 MB at 512^2 x 24:
 // resident in the 126 MB L2) go through three fused passes:
 //   rows   inverse transform along x of the ntot pupil rows only (the other
-//          rows of the padded field are zero), field and modulation tilt
-//          formed on the fly;
+//          rows of the padded field are zero), 8 rows per CTA, field and
+//          modulation tilt formed on the fly;
 //   cols   per 8 columns: inverse transform along y (zero rows skipped on
 //          load), field stop x pyramid mask, forward transform along y, all
 //          in shared memory;
-//   accum  per row: forward transform along x of every modulation plane at
-//          once (interleaved in shared memory) and the weighted |.|^2 summed
+//   accum  per row: forward transform along x of 8 modulation planes at a
+//          time (interleaved in shared memory) and the weighted |.|^2 summed
 //          over the points in registers, in point order.
+// The transforms are Stockham radix-8 passes with the butterflies in
+// registers (fft.cuh, fft_ct), compiled per nfft so that every index is a
+// constant expression, in natural order, so no permutation pass is needed.
 // The pixel-transfer convolution reuses the row / column pattern, the last
 // pass bins nrebin rows per CTA, and one kernel normalises and adds the
 // Philox photon / readout noise of the SH sensor (same sampler, same streams).
@@ -37,25 +40,24 @@
 
 namespace aob {
 
-constexpr int PYR_COLS = 8;
+constexpr int PYR_SEQ = 8;        // sequences (rows or columns) per CTA
 constexpr int PYR_THREADS = 512;
-constexpr int PYR_MAX_ACC = 4;  // nfft / PYR_THREADS <= 4 -> nfft <= 2048
 
 struct PyrArgs {
-  int n, logn, ntot, off, npts;
+  int ntot, off, npts;
   const float *phase, *pupil;
   float mic2rad;
   const float *cx, *cy, *w;
   const float *submask;
   const float2 *phalfxy;
   const float *sincar;
-  const float2 *tw;
-  float2 *work;   // npts x n x n
-  float2 *conv;   // n x n
-  float *hrimg;   // n x n
-  float *binimg;  // nb x nb
-  float *partial; // nb row sums
-  int nrebin, nb;
+  const float2 *tw;  // N/2 forward twiddles (global)
+  float2 *work;      // npts x N x N
+  float2 *conv;      // N x N
+  float *hrimg;      // N x N
+  float *binimg;     // nb x nb
+  float *partial;    // nb row sums
+  int nrebin, nb, rows_per_bin_cta;
 };
 
 // complex multiply
@@ -63,186 +65,201 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.y * b.x + a.x * b.y);
 }
 
-// 1. rows of the padded pupil field, inverse transform along x.
-//    CTA (p, yb): work[p][yb][:] for pupil row yb < ntot.
+// shared memory of every pyramid kernel: PYR_SEQ interleaved sequences of N
+// complex values, then the N/2 twiddles
+template <int N>
+__device__ __forceinline__ float2 *pyr_load_twiddles(float2 *sm, const float2 *tw) {
+  float2 *tws = sm + N * PYR_SEQ;
+  for (int i = threadIdx.x; i < N / 2; i += blockDim.x) tws[i] = tw[i];
+  return tws;
+}
+
+// 1. rows of the padded pupil field, inverse transform along x; a CTA takes
+//    PYR_SEQ pupil rows of one modulation point: work[p][yb][:].
+template <int N>
 __global__ void __launch_bounds__(PYR_THREADS) pyr_rows_kernel(PyrArgs A) {
-  extern __shared__ float2 srow[];
-  const int p = blockIdx.x / A.ntot, yb = blockIdx.x - p * A.ntot;
+  extern __shared__ float2 sm[];
+  float2 *tws = pyr_load_twiddles<N>(sm, A.tw);
+  const int groups = (A.ntot + PYR_SEQ - 1) / PYR_SEQ;
+  const int p = blockIdx.x / groups;
+  const int y0 = (blockIdx.x - p * groups) * PYR_SEQ;
   const float cxp = A.cx[p], cyp = A.cy[p];
-  const float yy = (float)yb - A.ntot / 2.0f;
-  for (int i = threadIdx.x; i < A.n; i += blockDim.x) {
-    const int x = i - A.off;
+  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+    const int c = t / N, i = t - c * N;
+    const int yb = y0 + c, x = i - A.off;
     float2 v = make_float2(0.f, 0.f);
-    if (x >= 0 && x < A.ntot) {
+    if (yb < A.ntot && x >= 0 && x < A.ntot) {
       const int id = x + yb * A.ntot;
-      const float xx = (float)x - A.ntot / 2.0f;
+      const float xx = (float)x - A.ntot / 2.0f, yy = (float)yb - A.ntot / 2.0f;
       float sn, cs;
       sincosf(A.phase[id] * A.mic2rad + (cxp * xx + cyp * yy), &sn, &cs);
       const float a = A.pupil[id];
       v = make_float2(cs * a, sn * a);
     }
-    srow[bitrev(i, A.logn)] = v;
+    sm[i * PYR_SEQ + c] = v;
   }
   __syncthreads();
-  smem_fft(srow, A.n, A.logn, 1, A.tw, 1);
-  float2 *out = A.work + ((size_t)p * A.n + yb) * A.n;
-  for (int i = threadIdx.x; i < A.n; i += blockDim.x) out[i] = srow[i];
+  fft_ct<N, PYR_SEQ, PYR_THREADS>(sm, tws, true);
+  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+    const int c = t / N, i = t - c * N;
+    if (y0 + c < A.ntot) A.work[((size_t)p * N + y0 + c) * N + i] = sm[i * PYR_SEQ + c];
+  }
 }
 
-// 2. per group of PYR_COLS columns of one modulation plane: inverse transform
+// 2. per group of PYR_SEQ columns of one modulation plane: inverse transform
 //    along y (rows outside the pupil are zero), x field stop, x pyramid
-//    phase mask, forward transform along y.  In place in work[p].
+//    phase mask (submask_krnl, submaskpyr_krnl), forward transform along y.
+//    In place in work[p].
+template <int N>
 __global__ void __launch_bounds__(PYR_THREADS) pyr_cols_kernel(PyrArgs A) {
-  extern __shared__ float2 scol[];
-  const int groups = A.n / PYR_COLS;
+  extern __shared__ float2 sm[];
+  float2 *tws = pyr_load_twiddles<N>(sm, A.tw);
+  constexpr int groups = N / PYR_SEQ;
   const int p = blockIdx.x / groups;
-  const int c0 = (blockIdx.x - p * groups) * PYR_COLS;
-  float2 *base = A.work + (size_t)p * A.n * A.n + c0;
-  const int nel = A.n * PYR_COLS;
-  for (int t = threadIdx.x; t < nel; t += blockDim.x) {
-    const int m = t / PYR_COLS, c = t - m * PYR_COLS;
+  const int c0 = (blockIdx.x - p * groups) * PYR_SEQ;
+  float2 *base = A.work + (size_t)p * N * N + c0;
+  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+    const int m = t / PYR_SEQ, c = t - m * PYR_SEQ;
     const int yb = m - A.off;
-    const float2 v = (yb >= 0 && yb < A.ntot) ? base[(size_t)yb * A.n + c] : make_float2(0.f, 0.f);
-    scol[bitrev(m, A.logn) * PYR_COLS + c] = v;
+    sm[t] = (yb >= 0 && yb < A.ntot) ? base[(size_t)yb * N + c] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  smem_fft(scol, A.n, A.logn, PYR_COLS, A.tw, 1);
-  // masks, and the bit-reversal permutation for the forward transform (each
-  // pair m < bitrev(m) is swapped by one thread)
-  for (int t = threadIdx.x; t < nel; t += blockDim.x) {
-    const int m = t / PYR_COLS, c = t - m * PYR_COLS;
-    const int r = (int)bitrev(m, A.logn);
-    if (m > r) continue;
-    const size_t gm = (size_t)(c0 + c) + (size_t)m * A.n, gr = (size_t)(c0 + c) + (size_t)r * A.n;
-    float2 a = scol[m * PYR_COLS + c];
-    const float sm = A.submask[gm];
-    a = cmul(make_float2(a.x * sm, a.y * sm), A.phalfxy[gm]);
-    if (m == r) {
-      scol[m * PYR_COLS + c] = a;
-    } else {
-      float2 b = scol[r * PYR_COLS + c];
-      const float sr = A.submask[gr];
-      b = cmul(make_float2(b.x * sr, b.y * sr), A.phalfxy[gr]);
-      scol[m * PYR_COLS + c] = b;
-      scol[r * PYR_COLS + c] = a;
-    }
+  fft_ct<N, PYR_SEQ, PYR_THREADS>(sm, tws, true);
+  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+    const int m = t / PYR_SEQ, c = t - m * PYR_SEQ;
+    const size_t g = (size_t)(c0 + c) + (size_t)m * N;
+    const float2 a = sm[t];
+    const float msk = A.submask[g];
+    sm[t] = cmul(make_float2(a.x * msk, a.y * msk), A.phalfxy[g]);
   }
   __syncthreads();
-  smem_fft(scol, A.n, A.logn, PYR_COLS, A.tw, 0);
-  for (int t = threadIdx.x; t < nel; t += blockDim.x) {
-    const int m = t / PYR_COLS, c = t - m * PYR_COLS;
-    base[(size_t)m * A.n + c] = scol[m * PYR_COLS + c];
+  fft_ct<N, PYR_SEQ, PYR_THREADS>(sm, tws, false);
+  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+    const int m = t / PYR_SEQ, c = t - m * PYR_SEQ;
+    base[(size_t)m * N + c] = sm[t];
   }
 }
 
-// 3. per row y: forward transform along x of ``pb`` modulation planes at a
-//    time (interleaved), hrimg[y][x] = sum_p w_p |.|^2 in point order.
-__global__ void __launch_bounds__(PYR_THREADS) pyr_accum_kernel(PyrArgs A, int pb_max) {
-  extern __shared__ float2 sacc[];
+// 3. per row y: forward transform along x of PYR_SEQ modulation planes at a
+//    time, hrimg[y][x] = sum_p w_p |.|^2 in point order (abs2_krnl with the
+//    modulation weight).
+template <int N>
+__global__ void __launch_bounds__(PYR_THREADS) pyr_accum_kernel(PyrArgs A) {
+  extern __shared__ float2 sm[];
+  float2 *tws = pyr_load_twiddles<N>(sm, A.tw);
+  constexpr int ACC = (N + PYR_THREADS - 1) / PYR_THREADS;
   const int y = blockIdx.x;
-  float acc[PYR_MAX_ACC];
+  float acc[ACC];
 #pragma unroll
-  for (int j = 0; j < PYR_MAX_ACC; ++j) acc[j] = 0.f;
-  for (int p0 = 0; p0 < A.npts; p0 += pb_max) {
-    const int pb = min(pb_max, A.npts - p0);
-    for (int t = threadIdx.x; t < A.n * pb; t += blockDim.x) {
-      const int q = t / A.n, m = t - q * A.n;
-      sacc[bitrev(m, A.logn) * pb + q] = A.work[((size_t)(p0 + q) * A.n + y) * A.n + m];
+  for (int j = 0; j < ACC; ++j) acc[j] = 0.f;
+  for (int p0 = 0; p0 < A.npts; p0 += PYR_SEQ) {
+    const int pb = min(PYR_SEQ, A.npts - p0);
+    for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+      const int q = t / N, m = t - q * N;
+      sm[m * PYR_SEQ + q] = q < pb ? A.work[((size_t)(p0 + q) * N + y) * N + m] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    smem_fft(sacc, A.n, A.logn, pb, A.tw, 0);
+    fft_ct<N, PYR_SEQ, PYR_THREADS>(sm, tws, false);
 #pragma unroll
-    for (int j = 0; j < PYR_MAX_ACC; ++j) {
-      const int m = threadIdx.x + j * blockDim.x;
-      if (m < A.n)
+    for (int j = 0; j < ACC; ++j) {
+      const int m = threadIdx.x + j * PYR_THREADS;
+      if (m < N)
         for (int q = 0; q < pb; ++q) {
-          const float2 v = sacc[m * pb + q];
+          const float2 v = sm[m * PYR_SEQ + q];
           acc[j] += A.w[p0 + q] * (v.x * v.x + v.y * v.y);
         }
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int j = 0; j < PYR_MAX_ACC; ++j) {
-    const int m = threadIdx.x + j * blockDim.x;
-    if (m < A.n) A.hrimg[(size_t)y * A.n + m] = acc[j];
+  for (int j = 0; j < ACC; ++j) {
+    const int m = threadIdx.x + j * PYR_THREADS;
+    if (m < N) A.hrimg[(size_t)y * N + m] = acc[j];
   }
 }
 
-// 4. pixel transfer function: rows of hrimg (real), inverse transform along x.
+// 4. pixel transfer function: PYR_SEQ rows of hrimg (real), inverse transform along x.
+template <int N>
 __global__ void __launch_bounds__(PYR_THREADS) pyr_conv_rows_kernel(PyrArgs A) {
-  extern __shared__ float2 srow[];
-  const int y = blockIdx.x;
-  for (int i = threadIdx.x; i < A.n; i += blockDim.x)
-    srow[bitrev(i, A.logn)] = make_float2(A.hrimg[(size_t)y * A.n + i], 0.f);
+  extern __shared__ float2 sm[];
+  float2 *tws = pyr_load_twiddles<N>(sm, A.tw);
+  const int y0 = blockIdx.x * PYR_SEQ;
+  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+    const int c = t / N, i = t - c * N;
+    sm[i * PYR_SEQ + c] = make_float2(A.hrimg[(size_t)(y0 + c) * N + i], 0.f);
+  }
   __syncthreads();
-  smem_fft(srow, A.n, A.logn, 1, A.tw, 1);
-  for (int i = threadIdx.x; i < A.n; i += blockDim.x) A.conv[(size_t)y * A.n + i] = srow[i];
+  fft_ct<N, PYR_SEQ, PYR_THREADS>(sm, tws, true);
+  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+    const int c = t / N, i = t - c * N;
+    A.conv[(size_t)(y0 + c) * N + i] = sm[i * PYR_SEQ + c];
+  }
 }
 
 // 5. columns: inverse transform along y, x sinc, forward transform along y.
+template <int N>
 __global__ void __launch_bounds__(PYR_THREADS) pyr_conv_cols_kernel(PyrArgs A) {
-  extern __shared__ float2 scol[];
-  const int c0 = blockIdx.x * PYR_COLS;
+  extern __shared__ float2 sm[];
+  float2 *tws = pyr_load_twiddles<N>(sm, A.tw);
+  const int c0 = blockIdx.x * PYR_SEQ;
   float2 *base = A.conv + c0;
-  const int nel = A.n * PYR_COLS;
-  for (int t = threadIdx.x; t < nel; t += blockDim.x) {
-    const int m = t / PYR_COLS, c = t - m * PYR_COLS;
-    scol[bitrev(m, A.logn) * PYR_COLS + c] = base[(size_t)m * A.n + c];
+  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+    const int m = t / PYR_SEQ, c = t - m * PYR_SEQ;
+    sm[t] = base[(size_t)m * N + c];
   }
   __syncthreads();
-  smem_fft(scol, A.n, A.logn, PYR_COLS, A.tw, 1);
-  for (int t = threadIdx.x; t < nel; t += blockDim.x) {
-    const int m = t / PYR_COLS, c = t - m * PYR_COLS;
-    const int r = (int)bitrev(m, A.logn);
-    if (m > r) continue;
-    float2 a = scol[m * PYR_COLS + c];
-    const float sm = A.sincar[(size_t)(c0 + c) + (size_t)m * A.n];
-    a = make_float2(a.x * sm, a.y * sm);
-    if (m == r) {
-      scol[m * PYR_COLS + c] = a;
-    } else {
-      float2 b = scol[r * PYR_COLS + c];
-      const float sr = A.sincar[(size_t)(c0 + c) + (size_t)r * A.n];
-      scol[m * PYR_COLS + c] = make_float2(b.x * sr, b.y * sr);
-      scol[r * PYR_COLS + c] = a;
-    }
+  fft_ct<N, PYR_SEQ, PYR_THREADS>(sm, tws, true);
+  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+    const int m = t / PYR_SEQ, c = t - m * PYR_SEQ;
+    const float msk = A.sincar[(size_t)(c0 + c) + (size_t)m * N];
+    const float2 a = sm[t];
+    sm[t] = make_float2(a.x * msk, a.y * msk);
   }
   __syncthreads();
-  smem_fft(scol, A.n, A.logn, PYR_COLS, A.tw, 0);
-  for (int t = threadIdx.x; t < nel; t += blockDim.x) {
-    const int m = t / PYR_COLS, c = t - m * PYR_COLS;
-    base[(size_t)m * A.n + c] = scol[m * PYR_COLS + c];
+  fft_ct<N, PYR_SEQ, PYR_THREADS>(sm, tws, false);
+  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+    const int m = t / PYR_SEQ, c = t - m * PYR_SEQ;
+    base[(size_t)m * N + c] = sm[t];
   }
 }
 
-// 6. nrebin rows per CTA: forward transform along x, real part, binning
-//    (pyr_bimg_krnl order: x offset outer, y offset inner, then / nrebin^2),
-//    and the row sum of the binned image for the normalisation.
+// 6. rows_per_bin_cta (a multiple of nrebin, <= PYR_SEQ) rows per CTA: forward
+//    transform along x, real part, binning (pyr_bimg_krnl order: x offset
+//    outer, y offset inner, then / nrebin^2) and the row sums of the binned
+//    image for the normalisation.
+template <int N>
 __global__ void __launch_bounds__(PYR_THREADS) pyr_bin_kernel(PyrArgs A) {
-  extern __shared__ float2 sbin[];
-  float *real = reinterpret_cast<float *>(sbin + A.n);  // nrebin x n
-  const int by = blockIdx.x;
-  for (int jj = 0; jj < A.nrebin; ++jj) {
-    const int y = by * A.nrebin + jj;
-    for (int i = threadIdx.x; i < A.n; i += blockDim.x) sbin[bitrev(i, A.logn)] = A.conv[(size_t)y * A.n + i];
-    __syncthreads();
-    smem_fft(sbin, A.n, A.logn, 1, A.tw, 0);
-    for (int i = threadIdx.x; i < A.n; i += blockDim.x) real[jj * A.n + i] = sbin[i].x;
-    __syncthreads();
-  }
-  const float inv = (float)(A.nrebin * A.nrebin);
-  for (int bx = threadIdx.x; bx < A.nb; bx += blockDim.x) {
-    float o = 0.f;
-    for (int ii = 0; ii < A.nrebin; ++ii)
-      for (int jj = 0; jj < A.nrebin; ++jj) o = o + real[jj * A.n + bx * A.nrebin + ii];
-    A.binimg[(size_t)by * A.nb + bx] = o / inv;
+  extern __shared__ float2 sm[];
+  float2 *tws = pyr_load_twiddles<N>(sm, A.tw);
+  float *real = reinterpret_cast<float *>(tws + N / 2);  // PYR_SEQ x N
+  const int rows = A.rows_per_bin_cta;
+  const int y0 = blockIdx.x * rows;
+  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+    const int c = t / N, i = t - c * N;
+    sm[i * PYR_SEQ + c] = c < rows ? A.conv[(size_t)(y0 + c) * N + i] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    float s = 0.f;
-    for (int bx = 0; bx < A.nb; ++bx) s += A.binimg[(size_t)by * A.nb + bx];
-    A.partial[by] = s;
+  fft_ct<N, PYR_SEQ, PYR_THREADS>(sm, tws, false);
+  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+    const int c = t / N, i = t - c * N;
+    real[c * N + i] = sm[i * PYR_SEQ + c].x;
+  }
+  __syncthreads();
+  const int nbr = rows / A.nrebin;
+  const float div = (float)(A.nrebin * A.nrebin);
+  for (int t = threadIdx.x; t < nbr * A.nb; t += PYR_THREADS) {
+    const int br = t / A.nb, bx = t - br * A.nb;
+    float o = 0.f;
+    for (int ii = 0; ii < A.nrebin; ++ii)
+      for (int jj = 0; jj < A.nrebin; ++jj) o = o + real[(br * A.nrebin + jj) * N + bx * A.nrebin + ii];
+    A.binimg[(size_t)(blockIdx.x * nbr + br) * A.nb + bx] = o / div;
+  }
+  __syncthreads();
+  if (threadIdx.x < nbr) {
+    const int by = blockIdx.x * nbr + threadIdx.x;
+    float sum = 0.f;
+    for (int bx = 0; bx < A.nb; ++bx) sum += A.binimg[(size_t)by * A.nb + bx];
+    A.partial[by] = sum;
   }
 }
 
@@ -272,6 +289,35 @@ __global__ void pyr_norm_noise_kernel(float *binimg, const float *partial, int n
   }
 }
 
+template <int N>
+static void pyr_launch(const PyrArgs &A, int npts, int ntot, int nbin_ctas, cudaStream_t s) {
+  const size_t sm = sizeof(float2) * (N * PYR_SEQ + N / 2);
+  const size_t bin_sm = sm + sizeof(float) * N * PYR_SEQ;
+  static bool configured = false;
+  if (!configured) {
+    const int lim = (int)std::max<size_t>(bin_sm, 48 * 1024);
+    AOB_CUDA(cudaFuncSetAttribute(pyr_rows_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    AOB_CUDA(cudaFuncSetAttribute(pyr_cols_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    AOB_CUDA(cudaFuncSetAttribute(pyr_accum_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    AOB_CUDA(cudaFuncSetAttribute(pyr_conv_rows_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    AOB_CUDA(cudaFuncSetAttribute(pyr_conv_cols_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    AOB_CUDA(cudaFuncSetAttribute(pyr_bin_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    configured = true;
+  }
+  pyr_rows_kernel<N><<<npts * ((ntot + PYR_SEQ - 1) / PYR_SEQ), PYR_THREADS, sm, s>>>(A);
+  AOB_LAUNCH_CHECK("pyr_rows_kernel");
+  pyr_cols_kernel<N><<<npts * (N / PYR_SEQ), PYR_THREADS, sm, s>>>(A);
+  AOB_LAUNCH_CHECK("pyr_cols_kernel");
+  pyr_accum_kernel<N><<<N, PYR_THREADS, sm, s>>>(A);
+  AOB_LAUNCH_CHECK("pyr_accum_kernel");
+  pyr_conv_rows_kernel<N><<<N / PYR_SEQ, PYR_THREADS, sm, s>>>(A);
+  AOB_LAUNCH_CHECK("pyr_conv_rows_kernel");
+  pyr_conv_cols_kernel<N><<<N / PYR_SEQ, PYR_THREADS, sm, s>>>(A);
+  AOB_LAUNCH_CHECK("pyr_conv_cols_kernel");
+  pyr_bin_kernel<N><<<nbin_ctas, PYR_THREADS, bin_sm, s>>>(A);
+  AOB_LAUNCH_CHECK("pyr_bin_kernel");
+}
+
 }  // namespace aob
 
 using namespace aob;
@@ -281,11 +327,12 @@ aob_pyr::aob_pyr(int device_, int nxsub_, int nvalid_, int npix_, int nphase_, i
     : device(device_), nxsub(nxsub_), nvalid(nvalid_), npix(npix_), nphase(nphase_), nrebin(nrebin_), nfft(nfft_),
       ntot(ntot_), npts(npts_), pdiam(pdiam_), nphot(nphot_), nphot4imat(nphot4imat_) {
   AOB_REQUIRE(nvalid > 0 && nrebin > 0 && ntot > 0 && npts > 0, "pyr: sizes must be > 0");
-  AOB_REQUIRE(nfft >= 64 && nfft <= PYR_THREADS * PYR_MAX_ACC && (nfft & (nfft - 1)) == 0,
+  AOB_REQUIRE(nfft >= 64 && nfft <= 2048 && (nfft & (nfft - 1)) == 0,
               "pyr: nfft must be a power of two in [64, 2048]");
+  AOB_REQUIRE(nrebin <= PYR_SEQ && nfft % ((PYR_SEQ / nrebin) * nrebin) == 0,
+              "pyr: nrebin must be <= 8 and the binning rows must tile nfft");
   AOB_REQUIRE(ntot <= nfft, "pyr: the phase grid (ntot) must fit in nfft");
   AOB_REQUIRE(nfft % nrebin == 0, "pyr: nfft must be a multiple of nrebin");
-  AOB_REQUIRE((size_t)nfft * PYR_COLS * sizeof(float2) <= 200 * 1024, "pyr: nfft too large for the column pass");
   while ((1 << logn) < nfft) ++logn;
   AOB_CUDA(cudaSetDevice(device));
   phase.alloc((int64_t)ntot * ntot);
@@ -340,8 +387,6 @@ void aob_pyr::comp_image(bool with_noise, cudaStream_t s) {
   AOB_REQUIRE(loaded, "pyr.comp_image: load_arrays has not been called");
   AOB_CUDA(cudaSetDevice(device));
   PyrArgs A{};
-  A.n = nfft;
-  A.logn = logn;
   A.ntot = ntot;
   A.off = (int)((nfft - ntot) / 2.0f);
   A.npts = npts;
@@ -362,34 +407,16 @@ void aob_pyr::comp_image(bool with_noise, cudaStream_t s) {
   A.partial = partial.p;
   A.nrebin = nrebin;
   A.nb = nbin();
-  const size_t row_sm = sizeof(float2) * nfft;
-  const size_t col_sm = sizeof(float2) * nfft * PYR_COLS;
-  const int pb = std::max(1, std::min(npts, (int)((200 * 1024) / row_sm)));
-  const size_t acc_sm = row_sm * pb;
-  const size_t bin_sm = row_sm + sizeof(float) * nfft * nrebin;
-  static size_t configured[3] = {0, 0, 0};
-  auto attr = [](const void *k, size_t sm, size_t &done) {
-    if (sm > done) {
-      AOB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(sm, 48 * 1024)));
-      done = std::max<size_t>(sm, 48 * 1024);
-    }
-  };
-  attr((const void *)pyr_cols_kernel, col_sm, configured[0]);
-  attr((const void *)pyr_accum_kernel, acc_sm, configured[1]);
-  attr((const void *)pyr_conv_cols_kernel, col_sm, configured[2]);
-  AOB_REQUIRE(bin_sm <= 48 * 1024, "pyr: nfft * nrebin too large for the binning pass");
-  pyr_rows_kernel<<<npts * ntot, PYR_THREADS, row_sm, s>>>(A);
-  AOB_LAUNCH_CHECK("pyr_rows_kernel");
-  pyr_cols_kernel<<<npts * (nfft / PYR_COLS), PYR_THREADS, col_sm, s>>>(A);
-  AOB_LAUNCH_CHECK("pyr_cols_kernel");
-  pyr_accum_kernel<<<nfft, PYR_THREADS, acc_sm, s>>>(A, pb);
-  AOB_LAUNCH_CHECK("pyr_accum_kernel");
-  pyr_conv_rows_kernel<<<nfft, PYR_THREADS, row_sm, s>>>(A);
-  AOB_LAUNCH_CHECK("pyr_conv_rows_kernel");
-  pyr_conv_cols_kernel<<<nfft / PYR_COLS, PYR_THREADS, col_sm, s>>>(A);
-  AOB_LAUNCH_CHECK("pyr_conv_cols_kernel");
-  pyr_bin_kernel<<<nbin(), PYR_THREADS, bin_sm, s>>>(A);
-  AOB_LAUNCH_CHECK("pyr_bin_kernel");
+  A.rows_per_bin_cta = (PYR_SEQ / nrebin) * nrebin;
+  const int nbin_ctas = nfft / A.rows_per_bin_cta;
+  switch (nfft) {
+    case 64: pyr_launch<64>(A, npts, ntot, nbin_ctas, s); break;
+    case 128: pyr_launch<128>(A, npts, ntot, nbin_ctas, s); break;
+    case 256: pyr_launch<256>(A, npts, ntot, nbin_ctas, s); break;
+    case 512: pyr_launch<512>(A, npts, ntot, nbin_ctas, s); break;
+    case 1024: pyr_launch<1024>(A, npts, ntot, nbin_ctas, s); break;
+    default: pyr_launch<2048>(A, npts, ntot, nbin_ctas, s); break;
+  }
   const float nz = with_noise ? noise : -1.f;
   const int noise_mode = nz > 0 ? 2 : (nz > -1 ? 1 : 0);
   const int nb2 = nbin() * nbin();
