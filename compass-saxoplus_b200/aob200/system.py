@@ -56,9 +56,11 @@ def saxo40() -> AoConfig:
 
 
 def plain16() -> AoConfig:
+    # maxcond 30 filters the weakly sensed edge-actuator modes (LE Strehl 0.83
+    # at 1.65 um instead of 0.33 with 1500 on this geometry)
     return AoConfig(nxsub=16, npix=8, pixsize=0.3, pupdiam=128, noise=-1.0, centroider="cog", nact=17,
                     dm_margin_out=None, r0=0.16, fracs=(1.0,), alts=(0.0,), winds=(10.0,), dirs=(0.0,),
-                    seeds=(1234,))
+                    seeds=(1234,), maxcond=30.0)
 
 
 class ShAoSystem:
@@ -174,13 +176,21 @@ class ShAoSystem:
         self.loop.set_mode(mode)
         return self.loop
 
-    def next(self, stream=None, compute_psf=True, noise=True):
-        """One closed-loop iteration (the supervisor's order)."""
+    def next(self, stream=None, compute_psf=True, noise=True, mlp=None, threshold=np.inf):
+        """One closed-loop iteration (the supervisor's order).  With ``mlp`` the
+        commands come from the learned reconstructor (aob_mlp_comp_com), with the
+        LS MVM as fallback when the predicted command norm exceeds ``threshold``."""
         self.atmos.move(stream)
         if compute_psf:
             self.trace_target(stream)
         self.trace_wfs(stream)
-        self.loop.step(None, None, noise, stream)
+        if mlp is None:
+            self.loop.step(None, None, noise, stream)
+        else:
+            self.wfs.comp_image(noise, stream)
+            self.centro.get_cog(self.ls.buffer("centroids").ptr, stream)
+            mlp.comp_com(self.ls, float(min(threshold, 3.0e38)), stream)
+            self.ls.comp_voltage(stream)
         self.dm.comp_shape(self.ls.buffer("voltage").ptr, stream)
         if compute_psf:
             self.target.comp_image(None, True, stream)

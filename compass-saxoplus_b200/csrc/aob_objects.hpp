@@ -171,7 +171,8 @@ struct aob_ls {
   float *com() { return ring.back().p; }
   void set_delay(float d);
   void ensure_packed(int p);
-  void comp_com(cudaStream_t s, uint32_t *bump = nullptr);
+  // use: device flag; when given and 0 the MVM is skipped (learned reconstructor path)
+  void comp_com(cudaStream_t s, uint32_t *bump = nullptr, const uint32_t *use = nullptr);
   void launch_mvm(struct aob::MvmArgs &A, cudaStream_t s);
   void comp_voltage(cudaStream_t s);
   void clip(cudaStream_t s);
@@ -203,6 +204,40 @@ struct aob_loop {
   void step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s);
   uint64_t key(bool noise) const;
   void drop_graphs();
+};
+
+// ---------------------------------------------------------------------------
+// learned reconstructor: MLP slopes -> DM commands with a linear skip path
+// (no counterpart in the reference)
+struct aob_mlp {
+  int device = 0;
+  int nin, nh1, nh2, nout;  // as given
+  int pin, ph1, ph2, pout;  // padded to multiples of 8
+  float in_scale = 1.f, out_scale = 1.f;
+  float beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f;
+  int64_t t = 0;  // Adam steps taken
+  // parameters: FP32 masters, BF16 copies, Adam moments, gradients
+  // layers 0..2: in -> h1 -> h2 -> out; layer 3: the linear skip in -> out (no bias)
+  aob::DevBuf<float> w[4], b[3], mw[4], vw[4], mb[3], vb[3], gw[4], gb[3];
+  aob::DevBuf<uint16_t> wb[4];
+  // batch workspace
+  int cap = 0;
+  aob::DevBuf<uint16_t> xb, h1b, h2b, dy, dz2, dz1;
+  aob::DevBuf<float> z1, z2, y, loss_part;
+  // batch-1 inference
+  aob::DevBuf<float> ix, ih1, ih2, iy;
+  aob::DevBuf<uint32_t> use_ls, fallbacks;
+
+  aob_mlp(int device, int nin, int nh1, int nh2, int nout);
+  int rows(int l) const { return l == 0 ? ph1 : (l == 1 ? ph2 : pout); }
+  int cols(int l) const { return l == 0 ? pin : (l == 1 ? ph1 : (l == 2 ? ph2 : pin)); }
+  void set_params(int layer, const float *w_host, const float *b_host);
+  void get_params(int layer, float *w_host, float *b_host);
+  void ensure_batch(int batch);
+  void forward(const float *x, int batch, float *y_out, cudaStream_t s);
+  void backward(const float *target, int batch, float *loss, cudaStream_t s);
+  void adam(float lr, cudaStream_t s);
+  void infer(const float *x, float *y_out, cudaStream_t s);
 };
 
 namespace aob {

@@ -43,6 +43,8 @@ struct MvmArgs {
   uint32_t *bump;         // incremented once per launch when set (noise frame counter)
   uint32_t *status;       // error word (bounded waits that expired)
   int rows_per_cta;       // bulk kernel: rows staged per CTA (host-checked to fit)
+  const uint32_t *use;    // when set and *use == 0 the launch does nothing (the learned
+                          // reconstructor's commands were used instead)
 };
 
 // Dot product of one 16-byte packed chunk with its slopes sv[STRIDE * q],
@@ -116,6 +118,7 @@ __host__ __device__ inline int mvm_smem_floats(int ld, int v) { return ((ld / v 
 template <typename T>
 __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_kernel(MvmArgs A) {
   extern __shared__ __align__(16) float s_sh[];
+  if (A.use && *A.use == 0u) return;
   constexpr int V = Pack<T>::N;
   constexpr int Q = V / 4;
   const int nchunk = A.ld / V;  // 16-byte chunks per row
@@ -189,6 +192,7 @@ __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_bulk_kernel(MvmArgs A) {
   const int r0 = (int)(((int64_t)blockIdx.x * A.nrow) / gridDim.x);
   const int r1 = (int)(((int64_t)(blockIdx.x + 1) * A.nrow) / gridDim.x);
   const int R = r1 - r0;
+  if (A.use && *A.use == 0u) return;
   // shared memory: barriers | slopes | rows | per-warp partial sums
   uint64_t *bars = reinterpret_cast<uint64_t *>(sm);
   float *s_sh = reinterpret_cast<float *>(sm + mvm_bars_bytes(A.rows_per_cta));
@@ -384,7 +388,7 @@ void aob_ls::ensure_packed(int p) {
   packed_valid[p] = true;
 }
 
-void aob_ls::comp_com(cudaStream_t s, uint32_t *bump) {
+void aob_ls::comp_com(cudaStream_t s, uint32_t *bump, const uint32_t *use) {
   if (open_loop) return;
   AOB_CUDA(cudaSetDevice(device));
   ensure_packed(prec);
@@ -399,6 +403,7 @@ void aob_ls::comp_com(cudaStream_t s, uint32_t *bump) {
   A.integrate = 1;
   A.bump = bump;
   A.status = status.p;
+  A.use = use;
   if (prec == AOB_PREC_F32) {
     A.mat = cm_f32.p;
     A.ld = (nslope + 3) / 4 * 4;

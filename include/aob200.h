@@ -250,6 +250,43 @@ int aob_ls_get_params(aob_ls *c, int *nslope, int *nactu, float *delay, float *g
                       int *open_loop, float *volt_min, float *volt_max, int *prec);
 
 
+/* ---- learned reconstructor (MLP) ---------------------------------------- *
+ * No counterpart in the reference.  A 3-layer MLP slopes -> DM commands
+ * (nin -> nh1 -> nh2 -> nout, GELU on the hidden layers), BF16 weights and
+ * activations with FP32 accumulation, trained on the GPU (tensor-core GEMMs,
+ * Adam).  The network works on x = slopes * in_scale and predicts
+ * commands / out_scale.  Weights are row-major [out][in] float32 on the host. */
+typedef struct aob_mlp aob_mlp;
+int aob_mlp_create(aob_mlp **out, int device, int nin, int nh1, int nh2, int nout);
+int aob_mlp_destroy(aob_mlp *m);
+/* layer 0, 1, 2: W [rows][cols] and b [rows]; resets the optimiser state. */
+int aob_mlp_set_params(aob_mlp *m, int layer, const float *w, const float *b);
+int aob_mlp_get_params(aob_mlp *m, int layer, float *w, float *b);
+int aob_mlp_set_scales(aob_mlp *m, float in_scale, float out_scale);
+/* Batched forward: dev_x [batch][nin] slopes -> dev_y [batch][nout] commands
+ * (dev_y may be NULL: the outputs stay in the network's buffer "y"). */
+int aob_mlp_forward(aob_mlp *m, const float *dev_x, int batch, float *dev_y, void *stream);
+/* Gradients of the mean-squared error against dev_target [batch][nout]
+ * (commands) after aob_mlp_forward on the same batch; dev_loss (may be NULL)
+ * receives the loss on the scaled outputs.  Buffers "dW1".."dW3", "db1".."db3". */
+int aob_mlp_backward(aob_mlp *m, const float *dev_target, int batch, float *dev_loss, void *stream);
+/* forward + backward + one Adam step with learning rate lr. */
+int aob_mlp_train_step(aob_mlp *m, const float *dev_x, const float *dev_target, int batch, float lr,
+                       float *dev_loss, void *stream);
+/* Batch-1 inference (GEMV kernels): dev_x [nin] -> dev_y [nout]. */
+int aob_mlp_infer(aob_mlp *m, const float *dev_x, float *dev_y, void *stream);
+/* Controller step with the learned reconstructor: commands c = MLP(centroids
+ * of ls); if ||c|| <= threshold, err = -c and the integrator of ls is applied,
+ * otherwise ls's own MVM runs (LS fallback, counted).  Then call
+ * aob_ls_comp_voltage as usual. */
+int aob_mlp_comp_com(aob_mlp *m, aob_ls *ls, float threshold, void *stream);
+/* Number of LS fallbacks so far (reset != 0: set it back to 0). */
+int aob_mlp_fallbacks(aob_mlp *m, uint32_t *count, int reset);
+/* which: "W1".."W3", "b1".."b3" (FP32 masters, padded), "dW1".."dW3", "db1".."db3", "y". */
+int aob_mlp_buffer(aob_mlp *m, const char *which, void **dev_ptr, int64_t *nelem);
+/* Padded sizes {nin, nh1, nh2, nout} (multiples of 8). */
+int aob_mlp_get_dims(aob_mlp *m, int *padded4);
+
 /* ---- batched 2-D FFT ---------------------------------------------------- *
  * In-place complex64 n x n transforms of `batch` contiguous images, n a power
  * of two in [8, 2048]; cuFFT sign convention (forward = exp(-i...)),
