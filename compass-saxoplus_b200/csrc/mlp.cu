@@ -105,6 +105,41 @@ __global__ void mlp_adam_kernel(float *w, float *m, float *v, const float *g, __
   }
 }
 
+// Partial dot product of one bf16 row (nchunk 16-byte chunks) with x (float,
+// shared memory) over the chunks lane, lane + 32, ...: GEMV_U loads in flight.
+constexpr int GEMV_U = 8;
+__device__ __forceinline__ float gemv_row(const uint4 *row, const float *x, int nchunk, int lane) {
+  float acc = 0.f;
+  for (int c0 = lane; c0 < nchunk; c0 += 32 * GEMV_U) {
+    uint4 q[GEMV_U];
+#pragma unroll
+    for (int u = 0; u < GEMV_U; ++u) {
+      const int c = c0 + 32 * u;
+      q[u] = c < nchunk ? __ldg(row + c) : make_uint4(0u, 0u, 0u, 0u);
+    }
+#pragma unroll
+    for (int u = 0; u < GEMV_U; ++u) {
+      const int c = c0 + 32 * u;
+      if (c < nchunk) {
+        const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q[u]);
+        const float4 x0 = *reinterpret_cast<const float4 *>(x + 8 * c);
+        const float4 x1 = *reinterpret_cast<const float4 *>(x + 8 * c + 4);
+        const float2 f0 = __bfloat1622float2(h[0]), f1 = __bfloat1622float2(h[1]);
+        const float2 f2 = __bfloat1622float2(h[2]), f3 = __bfloat1622float2(h[3]);
+        acc = fmaf(f0.x, x0.x, acc);
+        acc = fmaf(f0.y, x0.y, acc);
+        acc = fmaf(f1.x, x0.z, acc);
+        acc = fmaf(f1.y, x0.w, acc);
+        acc = fmaf(f2.x, x1.x, acc);
+        acc = fmaf(f2.y, x1.y, acc);
+        acc = fmaf(f3.x, x1.z, acc);
+        acc = fmaf(f3.y, x1.w, acc);
+      }
+    }
+  }
+  return acc;
+}
+
 // One layer for a single input vector: y[r] = act(W[r] . bf16(x * xscale) + b[r]) * yscale
 // for r < rows_real (0 in the padding).  One warp per row, 16-byte weight loads.
 // With Ws set, y[r] also gets + Ws[r] . bf16(xs_in * xs_scale) (the skip path).
@@ -121,40 +156,9 @@ __global__ void mlp_gemv_kernel(const __nv_bfloat16 *W, const float *bias, const
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int nchunk = ld / 8;
   for (int r = blockIdx.x * nw + warp; r < rows; r += gridDim.x * nw) {
-    const uint4 *row = reinterpret_cast<const uint4 *>(W + (int64_t)r * ld);
-    float acc = 0.f;
-    for (int c = lane; c < nchunk; c += 32) {
-      const uint4 q = __ldg(row + c);
-      const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
-      const float4 x0 = *reinterpret_cast<const float4 *>(xs + 8 * c);
-      const float4 x1 = *reinterpret_cast<const float4 *>(xs + 8 * c + 4);
-      const float2 f0 = __bfloat1622float2(h[0]), f1 = __bfloat1622float2(h[1]);
-      const float2 f2 = __bfloat1622float2(h[2]), f3 = __bfloat1622float2(h[3]);
-      acc = fmaf(f0.x, x0.x, acc);
-      acc = fmaf(f0.y, x0.y, acc);
-      acc = fmaf(f1.x, x0.z, acc);
-      acc = fmaf(f1.y, x0.w, acc);
-      acc = fmaf(f2.x, x1.x, acc);
-      acc = fmaf(f2.y, x1.y, acc);
-      acc = fmaf(f3.x, x1.z, acc);
-      acc = fmaf(f3.y, x1.w, acc);
-    }
-    acc = warp_sum(acc);
-    float sk = 0.f;
-    if (Ws) {
-      const uint4 *srow = reinterpret_cast<const uint4 *>(Ws + (int64_t)r * lds);
-      for (int c = lane; c < lds / 8; c += 32) {
-        const uint4 q = __ldg(srow + c);
-        const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const float2 f = __bfloat1622float2(h[e]);
-          sk = fmaf(f.x, xk[8 * c + 2 * e], sk);
-          sk = fmaf(f.y, xk[8 * c + 2 * e + 1], sk);
-        }
-      }
-      sk = warp_sum(sk);
-    }
+    const float acc = warp_sum(gemv_row(reinterpret_cast<const uint4 *>(W + (int64_t)r * ld), xs, nchunk, lane));
+    const float sk = Ws ? warp_sum(gemv_row(reinterpret_cast<const uint4 *>(Ws + (int64_t)r * lds), xk, lds / 8, lane))
+                        : 0.f;
     if (lane == 0) {
       float v = acc + bias[r] + sk;
       if (gelu) v = gelu_f(v);
