@@ -378,6 +378,7 @@ class LsController:
         self.h = ctypes.c_void_p()
         call("aob_ls_create", ctypes.addressof(self.h), int(device), int(nslope), int(nactu), float(delay))
         self.nslope, self.nactu = int(nslope), int(nactu)
+        self.precision = 0
 
     def __del__(self):
         h = getattr(self, "h", None)
@@ -429,7 +430,9 @@ class LsController:
         call("aob_ls_set_centroids", self.h, a.ctypes.data, int(a.size))
 
     def set_precision(self, prec):
-        call("aob_ls_set_precision", self.h, PRECISIONS[prec] if isinstance(prec, str) else int(prec))
+        p = PRECISIONS[prec] if isinstance(prec, str) else int(prec)
+        call("aob_ls_set_precision", self.h, p)
+        self.precision = p
 
     def comp_com(self, stream=None):
         call("aob_ls_comp_com", self.h, stream)
@@ -515,3 +518,88 @@ class Loop:
     def step(self, host_phase=None, host_voltage=None, noise=True, stream=None):
         """host_phase / host_voltage: numpy float32 arrays (pinned for speed) or None."""
         call("aob_loop_step", self.h, addr(host_phase), addr(host_voltage), 1 if noise else 0, stream)
+
+    def time(self, noise=True, warmup=3, iters=20) -> float:
+        """Device milliseconds of one step (device phase, no host copies)."""
+        ms = ctypes.c_float()
+        call("aob_loop_time", self.h, 1 if noise else 0, int(warmup), int(iters), ctypes.addressof(ms))
+        return float(ms.value)
+
+
+class Batch:
+    """Many SH loops advanced together by one persistent kernel launch per step.
+
+    The batched Monte Carlo mode (no counterpart in the reference, where each
+    simulation is a separate process): loops of uneven size -- sub-aperture
+    count, pixels, Nfft 16 or 32, any MVM precision -- are stepped by a single
+    launch, replayed from a CUDA graph, with results bit-identical to stepping
+    each ``Loop`` on its own.  Controllers must have delay 0 and no
+    perturbation.  The loops must outlive the batch.
+    """
+
+    INFO_KEYS = ("instances", "items", "ctas", "smem_bytes", "rows_per_item", "alg_bytes",
+                 "phase_floats", "volt_floats")
+
+    def __init__(self, loops, device=0, graph=True):
+        self.h = ctypes.c_void_p()
+        call("aob_batch_create", ctypes.addressof(self.h), int(device))
+        self.loops = list(loops)
+        for l in self.loops:
+            call("aob_batch_add", self.h, l.h)
+        self.use_graph(graph)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        try:
+            if h is not None and h.value and _lib._lib is not None:
+                _lib.lib().aob_batch_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown: module globals already cleared
+            pass
+        self.h = None
+
+    def use_graph(self, on=True):
+        call("aob_batch_use_graph", self.h, 1 if on else 0)
+
+    def set_tuning(self, subaps_per_item=0, mvm_kb=0, lag=2, ctas_per_sm=0, order=0):
+        """Tile shapes: sub-apertures per sensor item, command-matrix KB per MVM
+        item, lag (instances) between an instance's sensor and MVM items, CTAs
+        per SM, instance order (0 largest first, 1 as added).  Results do not
+        depend on them."""
+        call("aob_batch_set_tuning", self.h, int(subaps_per_item), int(mvm_kb), int(lag), int(ctas_per_sm),
+             int(order))
+
+    def refresh(self):
+        """Re-snapshot every loop's parameters at the next step."""
+        call("aob_batch_refresh", self.h)
+
+    def step(self, noise=True, stream=None):
+        call("aob_batch_step", self.h, 1 if noise else 0, stream)
+
+    def step_host(self, host_phases=None, host_volts=None, noise=True, stream=None):
+        """host_phases: all sensors' phases (each npup*npup, Fortran order as in
+        ``Loop.step``) concatenated in insertion order, or None for the device
+        phases; host_volts receives all voltages concatenated.  Waits for the stream."""
+        call("aob_batch_step_host", self.h, addr(host_phases), addr(host_volts), 1 if noise else 0, stream)
+
+    def info(self) -> dict:
+        v = (ctypes.c_int64 * 8)()
+        call("aob_batch_info", self.h, ctypes.addressof(v), 8)
+        return dict(zip(self.INFO_KEYS, (int(x) for x in v)))
+
+    def offsets(self):
+        n = len(self.loops)
+        p = (ctypes.c_int64 * n)()
+        q = (ctypes.c_int64 * n)()
+        call("aob_batch_offsets", self.h, ctypes.addressof(p), ctypes.addressof(q))
+        return np.array(p[:], dtype=np.int64), np.array(q[:], dtype=np.int64)
+
+    def status(self) -> int:
+        s = ctypes.c_uint32()
+        call("aob_batch_status", self.h, ctypes.addressof(s))
+        return int(s.value)
+
+    def time(self, noise=True, warmup=3, iters=10) -> float:
+        """Device milliseconds of one step (CUDA events on a private stream)."""
+        ms = ctypes.c_float()
+        call("aob_batch_time", self.h, 1 if noise else 0, int(warmup), int(iters), ctypes.addressof(ms))
+        return float(ms.value)

@@ -101,3 +101,68 @@ def build_sh_loop(setup: ShLoopSetup, precision="f32", device=0, graph=True, see
     ls.set_gain(0.4)
     loop = core.Loop(wfs, c, ls, graph=graph)
     return wfs, c, ls, loop
+
+
+# ---------------------------------------------------------------------------
+# Batched Monte Carlo: independent SH instances of uneven size
+@dataclass
+class McInstance:
+    index: int
+    nxsub: int
+    npix: int
+    r0: float
+    seed: int
+    setup: ShLoopSetup
+    phase: np.ndarray  # npup x npup von Karman screen at 0.5 um [um]
+
+
+def mc_instance_list(count=64, seed=0):
+    """(nxsub, npix, r0, seed) of each instance: nxsub uniform in [24, 40],
+    6x6 or 8x8 binned pixels, r0 uniform in [0.08, 0.20] m, seeds 0..count-1."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        nxsub = int(rng.integers(24, 41))
+        npix = int(rng.choice([6, 8]))
+        r0 = float(rng.uniform(0.08, 0.20))
+        out.append((nxsub, npix, r0, i))
+    return out
+
+
+def mc_make(nxsub, npix, r0, seed, pixsize=0.36, pd=6):
+    """One SAXO-like instance: ``pd`` phase pixels per sub-aperture (pupil
+    pd * nxsub), ``pixsize`` arcsec pixels at 0.7 um, guide star magnitude 8
+    with 0.5 e- readout noise and a weighted CoG; the DM has about
+    1377 * ((nxsub + 1) / 41)^2 actuators (the saxo40 count scaled by the
+    actuator grid); seeded command matrix and von Karman phase screen."""
+    p = G.ShParams(nxsub=nxsub, npix=npix, pixsize=pixsize, wavelength_um=0.7, fracsub=0.5, gsmag=8.0,
+                   noise=0.5)
+    g = G.sh_geometry(p, pd * nxsub, diam=8.0, cobs=0.14, ittime=0.001)
+    nact = int(round(1377 * ((nxsub + 1) / 41.0) ** 2))
+    rng = np.random.default_rng(1000 + seed)
+    cmat = (rng.standard_normal((nact, 2 * g.nvalid)) / np.sqrt(2 * g.nvalid)).astype(np.float32)
+    x = np.arange(g.npix) - (g.npix - 1) / 2.0
+    weights = np.exp(-(x[:, None] ** 2 + x[None, :] ** 2) / (2 * (g.npix / 2.35) ** 2)).astype(np.float32)
+    thr = 0.02 * g.nphotons / (g.npix * g.npix)
+    setup = ShLoopSetup(f"mc{seed}", g, cmat, float(thr), weights, 0.5, "wcog")
+    phase = von_karman_screens(g.tel.n, 8.0 / g.tel.pupdiam, r0, 25.0, 1, seed=2000 + seed)[0]
+    return McInstance(seed, nxsub, npix, r0, seed, setup, phase)
+
+
+def mc_setup(count=64, seed=0):
+    """The batched Monte Carlo workload: ``count`` instances from mc_instance_list."""
+    return [mc_make(nxsub, npix, r0, s) for nxsub, npix, r0, s in mc_instance_list(count, seed)]
+
+
+def build_mc_batch(instances, precision="bf16", device=0, graph=True):
+    """Loops of every instance (phases loaded) and the batch that steps them."""
+    from . import core
+
+    loops = []
+    for inst in instances:
+        wfs, c, ls, loop = build_sh_loop(inst.setup, precision=precision, device=device, graph=graph,
+                                         seed=1234 + inst.seed)
+        wfs.set_phase(inst.phase)
+        loops.append((wfs, c, ls, loop))
+    batch = core.Batch([l[3] for l in loops], device=device, graph=graph)
+    return loops, batch

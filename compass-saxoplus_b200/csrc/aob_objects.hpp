@@ -207,6 +207,44 @@ struct aob_loop {
 };
 
 // ---------------------------------------------------------------------------
+// many independent loops advanced by one persistent launch per step
+// (batched Monte Carlo; no counterpart in the reference)
+struct aob_batch {
+  int device = 0;
+  std::vector<aob_loop *> loops;
+  // tuning: sub-apertures per sensor item (0 = 8), command-matrix KB per MVM
+  // item (0 = 48), MVM items queued `lag` instances after their sensor items,
+  // CTAs per SM (0 = 2), instance order (0 = largest first, 1 = as added)
+  int subaps = 0, mvm_kb = 0, lag = 2, ctas_per_sm = 0, order = 0;
+  bool use_graph = true;
+  bool built = false;
+  uint64_t built_key = 0;
+  int grid = 0, nitems = 0, rows_max = 1;
+  size_t smem = 0;
+  int64_t alg_bytes = 0;  // algorithmic HBM bytes of one step
+  std::vector<int64_t> phase_off, volt_off;
+  std::vector<uint64_t> frame_seen;  // sensor frames the device counters hold
+  std::vector<uint32_t> h_frames;
+  aob::DevBuf<unsigned char> d_inst[2];
+  aob::DevBuf<int4> d_items;
+  aob::DevBuf<unsigned int> ctl, done;
+  aob::DevBuf<uint32_t> frames, status;
+  aob::DevBuf<float> phase_all, volt_all;  // staging for host phases / gathered voltages
+  cudaGraphExec_t graphs[2] = {nullptr, nullptr};
+
+  explicit aob_batch(int device);
+  ~aob_batch();
+  void add(aob_loop *l);
+  void set_tuning(int subaps, int mvm_kb, int lag, int ctas_per_sm, int order);
+  uint64_t key(bool noise) const;
+  void build(bool noise);
+  void launch(bool staged, cudaStream_t s);
+  void device_step(bool noise, bool staged, cudaStream_t s);
+  void step_host(const float *host_phase, float *host_volt, bool noise, cudaStream_t s);
+  void drop_graphs();
+};
+
+// ---------------------------------------------------------------------------
 // learned reconstructor: MLP slopes -> DM commands with a linear skip path
 // (no counterpart in the reference)
 struct aob_mlp {

@@ -59,6 +59,19 @@ int aob_device_count(void) {
   return n;
 }
 
+int aob_device_name(int device, char *buf, int len, int *num_sms) {
+  AOB_API_BEGIN
+  NEED(buf);
+  cudaDeviceProp prop;
+  AOB_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (len > 0) {
+    std::strncpy(buf, prop.name, (size_t)len - 1);
+    buf[len - 1] = 0;
+  }
+  if (num_sms) *num_sms = prop.multiProcessorCount;
+  AOB_API_END
+}
+
 int aob_memcpy_d2h(void *dst, const void *src, size_t bytes, void *stream) {
   AOB_API_BEGIN
   if (bytes == 0) return AOB_OK;

@@ -208,6 +208,38 @@ int aob_loop_step(aob_loop *l, const float *host_phase, float *host_voltage, int
   }
 }
 
+int aob_loop_time(aob_loop *l, int noise, int warmup, int iters, float *ms_per_step) {
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  try {
+    if (!l || !ms_per_step) throw Error("aob_loop_time: null pointer");
+    AOB_REQUIRE(warmup >= 0 && iters >= 1, "aob_loop_time: warmup >= 0 and iters >= 1 required");
+    AOB_CUDA(cudaSetDevice(l->wfs->device));
+    AOB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    AOB_CUDA(cudaEventCreate(&e0));
+    AOB_CUDA(cudaEventCreate(&e1));
+    for (int i = 0; i < warmup; ++i) l->step(nullptr, nullptr, noise != 0, s);
+    AOB_CUDA(cudaEventRecord(e0, s));
+    for (int i = 0; i < iters; ++i) l->step(nullptr, nullptr, noise != 0, s);
+    AOB_CUDA(cudaEventRecord(e1, s));
+    AOB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    AOB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    *ms_per_step = ms / (float)iters;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    return AOB_OK;
+  } catch (const std::exception &e) {
+    if (s) cudaStreamSynchronize(s);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (s) cudaStreamDestroy(s);
+    set_last_error(e.what());
+    return AOB_ERR;
+  }
+}
+
 int aob_loop_use_graph(aob_loop *l, int enable) {
   if (!l) {
     set_last_error("aob_loop_use_graph: null handle");

@@ -37,6 +37,8 @@ const char *aob_last_error(void);
 const char *aob_version(void);
 /* Number of CUDA devices visible (0 when none); never fails. */
 int aob_device_count(void);
+/* Device name (NUL-terminated, truncated to len) and SM count. */
+int aob_device_name(int device, char *buf, int len, int *num_sms);
 /* Copies between host and a device buffer owned by this library or the
  * caller (the carma array buffer protocol, python_module/carma/src/obj.hpp:32-76). */
 int aob_memcpy_d2h(void *dst_host, const void *src_dev, size_t bytes, void *stream);
@@ -392,6 +394,10 @@ int aob_loop_destroy(aob_loop *l);
  * floats, may be NULL) receives the voltages, and the call then waits for
  * the stream.  noise != 0 adds photon/readout noise. */
 int aob_loop_step(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream);
+/* Device time of one step (ms, CUDA events on a private stream; device
+ * phase, no host copies): warmup untimed steps, then the mean over iters
+ * steps.  Used by the autotuner; the loop state advances. */
+int aob_loop_time(aob_loop *l, int noise, int warmup, int iters, float *ms_per_step);
 /* Replay the device part of a step from a CUDA graph (enable != 0). */
 int aob_loop_use_graph(aob_loop *l, int enable);
 /* Kernels launched by the device part of the last step. */
@@ -401,6 +407,48 @@ int aob_loop_kernels_per_step(aob_loop *l, int *n);
  * if it does not fit); fused_batch = at most this many sub-apertures per CTA
  * and round in the fused kernel (0 = a CTA's whole share in one round). */
 int aob_loop_set_mode(aob_loop *l, int mode, int fused_batch);
+
+/* ---- batched Monte Carlo: many loops, one persistent launch per step --- *
+ * No counterpart in the reference, where each simulation is its own process
+ * stepping its own objects (CompassSupervisor.next, shesha/shesha/supervisor/
+ * compassSupervisor.py:175-289).  A batch holds any number of SH loops of
+ * uneven size (Nfft 16 or 32, any pixels, any MVM precision; controller delay
+ * 0, no perturbation) and advances all of them with ONE kernel launch, replayed
+ * from a CUDA graph: a queue of sensor items (runs of sub-apertures) and MVM
+ * items (blocks of command-matrix rows) taken by persistent CTAs, with the MVM
+ * items of an instance waiting (bounded) for its sensor items.  Results are
+ * bit-identical to stepping each loop with aob_loop_step.  Parameters are
+ * snapshot when the batch is (re)built: automatically on the first step and
+ * when a loop's graph-relevant parameters change; aob_batch_refresh forces it.
+ * Status bits of expired waits: 1 row copy, 4 sensor-item dependency. */
+typedef struct aob_batch aob_batch;
+int aob_batch_create(aob_batch **out, int device);
+int aob_batch_destroy(aob_batch *b);
+/* The loop must outlive the batch. */
+int aob_batch_add(aob_batch *b, aob_loop *loop);
+/* Tile shapes (the autotuner's choice): sub-apertures per sensor item (0 = 8,
+ * at most 64), command-matrix KB per MVM item (0 = 48, at most 200), lag in
+ * instances between an instance's sensor and MVM items, CTAs per SM (0 = 2,
+ * else 1 or 2), instance order (0 = largest first, 1 = as added). */
+int aob_batch_set_tuning(aob_batch *b, int subaps_per_item, int mvm_kb, int lag, int ctas_per_sm, int order);
+int aob_batch_use_graph(aob_batch *b, int enable);
+int aob_batch_refresh(aob_batch *b);
+/* One step of every loop with phases from each sensor's own device buffer. */
+int aob_batch_step(aob_batch *b, int noise, void *stream);
+/* One step with host I/O: host_phases (all sensors' npup*npup phases
+ * concatenated in insertion order; NULL = device phases) are copied in,
+ * host_volts (all nactu voltages concatenated; may be NULL) receive the
+ * voltages, and the call waits for the stream. */
+int aob_batch_step_host(aob_batch *b, const float *host_phases, float *host_volts, int noise, void *stream);
+/* info[0..n): instances, queue items, CTAs, shared bytes per CTA, rows per
+ * MVM item (max), algorithmic HBM bytes per step, phase floats, voltage floats. */
+int aob_batch_info(aob_batch *b, int64_t *info, int n);
+/* Offsets of each instance in the concatenated phase / voltage arrays. */
+int aob_batch_offsets(aob_batch *b, int64_t *phase_off, int64_t *volt_off);
+int aob_batch_status(aob_batch *b, uint32_t *status);
+/* Device time of one step (ms, CUDA events on a private stream): warmup
+ * untimed steps, then the mean over iters steps.  Used by the autotuner. */
+int aob_batch_time(aob_batch *b, int noise, int warmup, int iters, float *ms_per_step);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop
