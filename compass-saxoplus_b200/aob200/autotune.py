@@ -3,9 +3,9 @@
 Tuned objects and their knobs (none of them changes results -- every kernel
 reduces in a fixed order -- only the time):
 
-* ``Batch`` (batched Monte Carlo): sub-apertures per sensor item,
-  command-matrix KB per MVM item, lag between an instance's sensor and MVM
-  items, CTAs per SM, instance order;
+* ``Batch`` (batched Monte Carlo): sub-apertures per sensor item, threads
+  per sensor team, command-matrix KB per MVM item, lag between an
+  instance's sensor and MVM items, CTAs per SM, instance order;
 * ``Loop`` (one SH loop): sub-apertures per CTA and round in the fused
   single-kernel step.
 
@@ -28,7 +28,9 @@ import time
 
 from ._lib import call
 
-DEFAULT_BATCH_SPACE = dict(subaps=(4, 8, 16), mvm_kb=(24, 48, 96), lag=(1, 4), ctas_per_sm=(1, 2), order=(0,))
+DEFAULT_BATCH_SPACE = dict(subaps=(16, 32, 64), team=(64, 256), mvm_kb=(48, 96), lag=(16,), ctas_per_sm=(2, 3),
+                           order=(0,))
+_BATCH_KEYS = ("subaps", "team", "mvm_kb", "lag", "ctas_per_sm", "order")
 DEFAULT_LOOP_SPACE = dict(fused_batch=(0, 1, 2, 4, 8))
 
 
@@ -93,19 +95,20 @@ def tune_batch(batch, noise=True, space=None, warmup=3, iters=10, use_cache=True
     store = _load() if use_cache else {}
     if use_cache and key in store:
         t = store[key]["tuning"]
-        batch.set_tuning(t["subaps"], t["mvm_kb"], t["lag"], t["ctas_per_sm"], t["order"])
+        batch.set_tuning(*(t.get(k, 0) for k in _BATCH_KEYS))
         return dict(store[key], cached=True)
     trials = []
     for cand in _grid(space):
-        batch.set_tuning(cand["subaps"], cand["mvm_kb"], cand["lag"], cand["ctas_per_sm"], cand["order"])
+        cand = {k: cand.get(k, 0) for k in _BATCH_KEYS}
+        batch.set_tuning(*(cand[k] for k in _BATCH_KEYS))
         t0 = time.perf_counter()
         ms = batch.time(noise=noise, warmup=warmup, iters=iters)
         trials.append(dict(cand, ms=ms))
         if log:
             log(f"batch tuning {cand}: {ms * 1e3:.1f} us/step ({time.perf_counter() - t0:.2f} s)")
     best = min(trials, key=lambda r: r["ms"])
-    tuning = {k: best[k] for k in space}
-    batch.set_tuning(tuning["subaps"], tuning["mvm_kb"], tuning["lag"], tuning["ctas_per_sm"], tuning["order"])
+    tuning = {k: best[k] for k in _BATCH_KEYS}
+    batch.set_tuning(*(tuning[k] for k in _BATCH_KEYS))
     res = dict(tuning=tuning, ms=best["ms"], trials=trials)
     if use_cache:
         store = _load()

@@ -560,13 +560,13 @@ class Batch:
     def use_graph(self, on=True):
         call("aob_batch_use_graph", self.h, 1 if on else 0)
 
-    def set_tuning(self, subaps_per_item=0, mvm_kb=0, lag=2, ctas_per_sm=0, order=0):
-        """Tile shapes: sub-apertures per sensor item, command-matrix KB per MVM
-        item, lag (instances) between an instance's sensor and MVM items, CTAs
-        per SM, instance order (0 largest first, 1 as added).  Results do not
-        depend on them."""
-        call("aob_batch_set_tuning", self.h, int(subaps_per_item), int(mvm_kb), int(lag), int(ctas_per_sm),
-             int(order))
+    def set_tuning(self, subaps_per_item=0, team_threads=0, mvm_kb=0, lag=2, ctas_per_sm=0, order=0):
+        """Tile shapes: sub-apertures per sensor item, threads per sensor team,
+        command-matrix KB per MVM item, lag (instances) between an instance's
+        sensor and MVM items, CTAs per SM, instance order (0 largest first,
+        1 as added).  Results do not depend on them."""
+        call("aob_batch_set_tuning", self.h, int(subaps_per_item), int(team_threads), int(mvm_kb), int(lag),
+             int(ctas_per_sm), int(order))
 
     def refresh(self):
         """Re-snapshot every loop's parameters at the next step."""

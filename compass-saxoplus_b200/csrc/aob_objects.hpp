@@ -212,10 +212,12 @@ struct aob_loop {
 struct aob_batch {
   int device = 0;
   std::vector<aob_loop *> loops;
-  // tuning: sub-apertures per sensor item (0 = 8), command-matrix KB per MVM
-  // item (0 = 48), MVM items queued `lag` instances after their sensor items,
-  // CTAs per SM (0 = 2), instance order (0 = largest first, 1 = as added)
-  int subaps = 0, mvm_kb = 0, lag = 2, ctas_per_sm = 0, order = 0;
+  // tuning: sub-apertures per sensor item (0 = 32), threads per sensor team
+  // (0 = 32), command-matrix KB per MVM item (0 = 48), MVM items queued `lag`
+  // instances after their sensor items, CTAs per SM (0 = 2), instance order
+  // (0 = largest first, 1 = as added)
+  int subaps = 0, team = 0, mvm_kb = 0, lag = 2, ctas_per_sm = 0, order = 0;
+  int team_threads() const { return team > 0 ? team : 32; }
   bool use_graph = true;
   bool built = false;
   uint64_t built_key = 0;
@@ -235,7 +237,7 @@ struct aob_batch {
   explicit aob_batch(int device);
   ~aob_batch();
   void add(aob_loop *l);
-  void set_tuning(int subaps, int mvm_kb, int lag, int ctas_per_sm, int order);
+  void set_tuning(int subaps, int team, int mvm_kb, int lag, int ctas_per_sm, int order);
   uint64_t key(bool noise) const;
   void build(bool noise);
   void launch(bool staged, cudaStream_t s);

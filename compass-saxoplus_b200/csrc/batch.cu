@@ -32,9 +32,9 @@
 // run here by 8 warps that take two slots each.  Slopes, commands and
 // voltages are bit-identical to stepping each instance's own loop.
 //
-// Tile shapes (sub-apertures per sensor item, command-matrix bytes per MVM
-// item, the lag, CTAs per SM and the instance order) are parameters, chosen by
-// the autotuner in aob200/autotune.py.
+// Tile shapes (sub-apertures per sensor item, threads per sensor team,
+// command-matrix bytes per MVM item, the lag, CTAs per SM and the instance
+// order) are parameters, chosen by the autotuner in aob200/autotune.py.
 
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
@@ -70,7 +70,7 @@ struct BatchInst {
   int cls;    // sensor code path: 0 (Nfft 16, 6 px), 1 (32, 6), 2 (16, any), 3 (32, any)
   int nsensor;  // sensor items of this instance
   int noisy;  // frame advances after the step
-  int pad_;
+  int smax;   // sub-apertures per team and item, at most (sizes a team's work area)
 };
 
 struct BatchArgs {
@@ -82,6 +82,7 @@ struct BatchArgs {
   uint32_t *frames;    // noise frame per instance
   uint32_t *status;
   int rows_max;  // MVM rows per item, upper bound
+  int team;      // threads per sensor team (32, 64, 128 or 256)
 };
 
 __host__ __device__ inline size_t batch_bars_bytes(int rows) { return 128 * (((size_t)rows * 8 + 127) / 128); }
@@ -143,14 +144,28 @@ struct BPack<__nv_fp8_e4m3> {
   }
 };
 
+// Sub-apertures [first, first + count) by the CTA's teams of ``team``
+// threads: team t takes first + t + j * nteams, all in one batch.
 template <int NFFT, int PD>
-__device__ __forceinline__ void sensor_item(const ShKernelArgs &P, int first, int count, unsigned char *area,
-                                            bool reload) {
+__device__ __forceinline__ void sensor_item(const ShKernelArgs &P, int first, int count, int team, int smax,
+                                            unsigned char *area, bool reload) {
   const int pd = PD > 0 ? PD : P.pdiam;
-  const ShSmem L(NFFT, P.nu, P.nv, pd, P.nrebin2 * P.npix * P.npix, P.npix * P.npix, count);
-  if (reload) sh_load_tables<NFFT>(P, area, threadIdx.x, blockDim.x);
-  // (sh_batch synchronises before the tables are first read)
-  sh_batch<NFFT, PD>(P, first, 1, count, area, area + L.hdr, L);
+  const int nteams = blockDim.x / team, t = threadIdx.x / team;
+  const ShSmem L(NFFT, P.nu, P.nv, pd, P.nrebin2 * P.npix * P.npix, P.npix * P.npix, smax);
+  if (reload) {
+    sh_load_tables<NFFT>(P, area, threadIdx.x, blockDim.x);
+    __syncthreads();
+  }
+  const int S = (count - t + nteams - 1) / nteams;
+  if (S > 0) {
+    const Team T{(int)threadIdx.x - t * team, team, 1 + t};
+    unsigned char *work = area + L.hdr + (size_t)t * L.per_batch;
+    if (team == 32)
+      sh_batch<NFFT, PD, TEAM_WARP>(P, first + t, nteams, S, area, work, L, T);
+    else
+      sh_batch<NFFT, PD, TEAM_NAMED>(P, first + t, nteams, S, area, work, L, T);
+  }
+  __syncthreads();  // every slope of the item written
 }
 
 // Rows [r0, r0 + R) of instance ``ii``.  All barriers 0..rows_max-1 complete
@@ -275,7 +290,10 @@ __device__ __forceinline__ void mvm_item(const BatchInst &I, int ii, int r0, int
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(BATCH_THREADS, 2) batch_step_kernel(BatchArgs A) {
+// MINB: CTAs per SM the register budget is sized for (2: up to 128
+// registers per thread, 4: up to 64)
+template <int MINB>
+__global__ void __launch_bounds__(BATCH_THREADS, MINB) batch_step_kernel(BatchArgs A) {
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ __align__(16) BatchInst s_I;
   __shared__ int s_ticket;
@@ -307,10 +325,10 @@ __global__ void __launch_bounds__(BATCH_THREADS, 2) batch_step_kernel(BatchArgs 
     if (it.y == BI_SENSOR) {
       const bool reload = tables != it.x;
       switch (s_I.cls) {
-        case 0: sensor_item<16, 6>(s_I.sh, it.z, it.w, area, reload); break;
-        case 1: sensor_item<32, 6>(s_I.sh, it.z, it.w, area, reload); break;
-        case 2: sensor_item<16, 0>(s_I.sh, it.z, it.w, area, reload); break;
-        default: sensor_item<32, 0>(s_I.sh, it.z, it.w, area, reload); break;
+        case 0: sensor_item<16, 6>(s_I.sh, it.z, it.w, A.team, s_I.smax, area, reload); break;
+        case 1: sensor_item<32, 6>(s_I.sh, it.z, it.w, A.team, s_I.smax, area, reload); break;
+        case 2: sensor_item<16, 0>(s_I.sh, it.z, it.w, A.team, s_I.smax, area, reload); break;
+        default: sensor_item<32, 0>(s_I.sh, it.z, it.w, A.team, s_I.smax, area, reload); break;
       }
       tables = it.x;
       if (tid == 0) {
@@ -370,13 +388,16 @@ void aob_batch::add(aob_loop *l) {
   built = false;
 }
 
-void aob_batch::set_tuning(int subaps_, int mvm_kb_, int lag_, int ctas_per_sm_, int order_) {
-  AOB_REQUIRE(subaps_ >= 0 && subaps_ <= 64, "batch.set_tuning: subaps_per_item must be in [0, 64]");
+void aob_batch::set_tuning(int subaps_, int team_, int mvm_kb_, int lag_, int ctas_per_sm_, int order_) {
+  AOB_REQUIRE(subaps_ >= 0 && subaps_ <= 1024, "batch.set_tuning: subaps_per_item must be in [0, 1024]");
+  AOB_REQUIRE(team_ == 0 || team_ == 32 || team_ == 64 || team_ == 128 || team_ == 256,
+              "batch.set_tuning: team_threads must be 0, 32, 64, 128 or 256");
   AOB_REQUIRE(mvm_kb_ >= 0 && mvm_kb_ <= 200, "batch.set_tuning: mvm_kb must be in [0, 200]");
   AOB_REQUIRE(lag_ >= 0 && lag_ <= 1024, "batch.set_tuning: lag must be in [0, 1024]");
-  AOB_REQUIRE(ctas_per_sm_ >= 0 && ctas_per_sm_ <= 2, "batch.set_tuning: ctas_per_sm must be 0, 1 or 2");
+  AOB_REQUIRE(ctas_per_sm_ >= 0 && ctas_per_sm_ <= 4, "batch.set_tuning: ctas_per_sm must be in [0, 4]");
   AOB_REQUIRE(order_ == 0 || order_ == 1, "batch.set_tuning: order must be 0 or 1");
   subaps = subaps_;
+  team = team_;
   mvm_kb = mvm_kb_;
   lag = lag_;
   ctas_per_sm = ctas_per_sm_;
@@ -391,7 +412,7 @@ uint64_t aob_batch::key(bool noise) const {
     for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
   };
   mix(&noise, sizeof noise);
-  const int tune[5] = {subaps, mvm_kb, lag, ctas_per_sm, order};
+  const int tune[6] = {subaps, team, mvm_kb, lag, ctas_per_sm, order};
   mix(tune, sizeof tune);
   for (const aob_loop *l : loops) {
     const uint64_t k = l->key(noise);
@@ -435,7 +456,8 @@ void aob_batch::build(bool noise) {
   // dynamic shared memory per CTA (static shared memory and the per-block
   // reservation come on top), minus a fixed header for BATCH_MAX_ROWS rows of
   // barriers and epilogue inputs, is what one item may use
-  const size_t smem_cap = ctas_per_sm == 1 ? (size_t)226 * 1024 : (size_t)112 * 1024;
+  const int cps = ctas_per_sm > 0 ? ctas_per_sm : 2;
+  const size_t smem_cap = std::min<size_t>((size_t)226 * 1024, ((size_t)228 / cps - 2) * 1024);
   const size_t item_cap = smem_cap - batch_bars_bytes(BATCH_MAX_ROWS) - batch_pre_bytes(BATCH_MAX_ROWS);
   const size_t kb = mvm_kb > 0 ? (size_t)mvm_kb * 1024 : (size_t)48 * 1024;
   std::vector<int> S(n), RPI(n);
@@ -477,17 +499,19 @@ void aob_batch::build(bool noise) {
     I.noisy = (noise && w->noise > -1.f) ? 1 : 0;
     hf[i] = (uint32_t)w->frame;
     frame_seen[i] = w->frame;
-    // sensor items: `subaps` sub-apertures (auto: about 2 items per CTA slot over the batch)
+    // sensor items: `subaps` sub-apertures each, split over the CTA's teams
     const int npix2 = w->npix * w->npix;
-    int s = subaps > 0 ? subaps : 8;
-    s = std::max(1, std::min(s, w->nvalid));
+    const int tm = team_threads();
+    int s = std::max(1, std::min(subaps > 0 ? subaps : 32, w->nvalid));
     auto sh_bytes = [&](int b) {
-      const ShSmem L(w->nfft, w->nu, w->nv, w->nphase, w->nrebin * w->nrebin * npix2, npix2, b);
-      return L.bytes();
+      const int smax = (b + BATCH_THREADS / tm - 1) / (BATCH_THREADS / tm);
+      const ShSmem L(w->nfft, w->nu, w->nv, w->nphase, w->nrebin * w->nrebin * npix2, npix2, smax);
+      return L.team_bytes(BATCH_THREADS / tm);
     };
     while (s > 1 && sh_bytes(s) > item_cap) --s;
-    AOB_REQUIRE(sh_bytes(s) <= item_cap, "batch: instance " + std::to_string(i) + ": a sub-aperture does not fit");
+    AOB_REQUIRE(sh_bytes(s) <= item_cap, "batch: instance " + std::to_string(i) + ": a sensor item does not fit");
     S[i] = s;
+    I.smax = (s + BATCH_THREADS / tm - 1) / (BATCH_THREADS / tm);
     I.nsensor = (w->nvalid + s - 1) / s;
     // MVM items: about `kb` bytes of rows each
     const size_t row_bytes = (size_t)I.ld * esize;
@@ -515,12 +539,12 @@ void aob_batch::build(bool noise) {
     aob_loop *l = loops[i];
     aob_sh *w = l->wfs;
     const int npix2 = w->npix * w->npix;
-    const ShSmem L(w->nfft, w->nu, w->nv, w->nphase, w->nrebin * w->nrebin * npix2, npix2, S[i]);
+    const ShSmem L(w->nfft, w->nu, w->nv, w->nphase, w->nrebin * w->nrebin * npix2, npix2, hi[i].smax);
     const int esize = hi[i].prec == AOB_PREC_F32 ? 4 : (hi[i].prec == AOB_PREC_BF16 ? 2 : 1);
     const int V = 16 / esize;
     const size_t mv = (size_t)RPI[i] * hi[i].ld * esize + sizeof(float) * batch_slope_floats(hi[i].ld, V) +
                       sizeof(float) * BATCH_SLOTS * RPI[i];
-    area = std::max(area, std::max(L.bytes(), mv));
+    area = std::max(area, std::max(L.team_bytes(BATCH_THREADS / team_threads()), mv));
   }
   smem = batch_bars_bytes(rmax) + batch_pre_bytes(rmax) + area;
   AOB_REQUIRE(smem <= smem_cap, "batch: shared memory per CTA exceeds the budget");
@@ -555,12 +579,12 @@ void aob_batch::build(bool noise) {
     d_inst[v].alloc((int64_t)sizeof(BatchInst) * n);
     AOB_CUDA(cudaMemcpy(d_inst[v].p, t.data(), sizeof(BatchInst) * n, cudaMemcpyHostToDevice));
   }
-  AOB_CUDA(cudaFuncSetAttribute(batch_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  auto kern = cps <= 2 ? batch_step_kernel<2> : batch_step_kernel<4>;
+  AOB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  AOB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_step_kernel, BATCH_THREADS, smem));
+  AOB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BATCH_THREADS, smem));
   AOB_REQUIRE(per_sm >= 1, "batch: the kernel does not fit on an SM");
-  const int want = ctas_per_sm > 0 ? ctas_per_sm : 2;
-  grid = nsm * std::min(per_sm, want);
+  grid = nsm * std::min(per_sm, cps);
   // the resets above ran on the legacy stream; the steps may use any stream
   AOB_CUDA(cudaDeviceSynchronize());
   drop_graphs();
@@ -579,7 +603,11 @@ void aob_batch::launch(bool staged, cudaStream_t s) {
   A.frames = frames.p;
   A.status = status.p;
   A.rows_max = rows_max;
-  batch_step_kernel<<<grid, BATCH_THREADS, smem, s>>>(A);
+  A.team = team_threads();
+  if (ctas_per_sm == 0 || ctas_per_sm <= 2)
+    batch_step_kernel<2><<<grid, BATCH_THREADS, smem, s>>>(A);
+  else
+    batch_step_kernel<4><<<grid, BATCH_THREADS, smem, s>>>(A);
   AOB_LAUNCH_CHECK("batch_step_kernel");
 }
 
@@ -693,9 +721,10 @@ int aob_batch_add(aob_batch *b, aob_loop *loop) {
   b->add(loop);
   BATCH_END
 }
-int aob_batch_set_tuning(aob_batch *b, int subaps_per_item, int mvm_kb, int lag, int ctas_per_sm, int order) {
+int aob_batch_set_tuning(aob_batch *b, int subaps_per_item, int team_threads, int mvm_kb, int lag, int ctas_per_sm,
+                         int order) {
   BATCH_TRY BATCH_NEED(b);
-  b->set_tuning(subaps_per_item, mvm_kb, lag, ctas_per_sm, order);
+  b->set_tuning(subaps_per_item, team_threads, mvm_kb, lag, ctas_per_sm, order);
   BATCH_END
 }
 int aob_batch_use_graph(aob_batch *b, int enable) {

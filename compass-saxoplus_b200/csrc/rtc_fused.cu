@@ -151,7 +151,9 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
   unsigned char *shm = rows + (size_t)A.rows_per_cta * row_bytes;
   const int pd = PD > 0 ? PD : A.sh.pdiam;
   const ShSmem L(NFFT, A.sh.nu, A.sh.nv, pd, A.sh.nrebin2 * A.sh.npix * A.sh.npix, A.sh.npix * A.sh.npix, A.batch);
-  float *s_sh = reinterpret_cast<float *>(shm + L.bytes());
+  // sensor tables + work area, later the MVM's per-warp partial sums
+  const size_t work_bytes = max(L.bytes(), L.hdr + sizeof(float) * (FUSED_THREADS / 32) * A.rows_per_cta);
+  float *s_sh = reinterpret_cast<float *>(shm + work_bytes);
 
   if (threadIdx.x == 0) {
     for (int r = 0; r < R; ++r) mbar_init(&bars[r], 1);
@@ -180,11 +182,11 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
   }
   // ---- sensor images and slopes: this CTA's sub-apertures, A.batch per round ----
   sh_load_tables<NFFT>(A.sh, shm, threadIdx.x, blockDim.x);
-  // (sh_batch synchronises before the tables are first read)
+  __syncthreads();
   const int nvalid = A.sh.nvalid;
   for (int base = blockIdx.x; base < nvalid; base += A.batch * gridDim.x) {
     const int Sb = min(A.batch, (nvalid - base + (int)gridDim.x - 1) / (int)gridDim.x);
-    sh_batch<NFFT, PD>(A.sh, base, gridDim.x, Sb, shm, shm + L.hdr, L);
+    sh_batch<NFFT, PD>(A.sh, base, gridDim.x, Sb, shm, shm + L.hdr, L, Team{(int)threadIdx.x, (int)blockDim.x, 0});
   }
   // ---- all slopes published ----
   const bool ok = grid_barrier(A.gbar, gridDim.x, A.status);

@@ -1,7 +1,10 @@
 // Shack-Hartmann image formation for a batch of sub-apertures, shared by the
-// standalone sensor kernel (sh_wfs.cu) and the fused RTC kernel (rtc_fused.cu).
+// standalone sensor kernel (sh_wfs.cu), the fused RTC kernel (rtc_fused.cu)
+// and the batched Monte Carlo kernel (batch.cu).
 //
-// Every thread of the CTA works on the whole batch at once, stage by stage:
+// A team of threads -- the whole CTA, or a group of its warps synchronised by
+// a named barrier, or one warp -- works on the whole batch at once, stage by
+// stage:
 //   0. per-sub-aperture metadata (phase window, flux, image position, refs)
 //   1. complex field  pupil * exp(i (phase * 2 pi / lambda - offset))
 //   2. DFT along x at the nu frequencies binmap reads
@@ -10,9 +13,10 @@
 //      warp per sub-aperture, fixed summation order) and normalisation
 //   5. Philox photon / readout noise, cube + image writes, centroid weights
 //   6. CoG-family centroid per sub-aperture (one warp each, fixed order)
-// so a CTA pays each stage's latency once for the batch instead of once per
-// sub-aperture.  The reductions run in an order that does not depend on the
-// batch size or the CTA size: the standalone and the fused kernels give
+// so a team pays each stage's latency once for the batch instead of once per
+// sub-aperture; small teams (one warp) meet only at warp barriers and run
+// independently of the CTA's other teams.  The reductions run in an order
+// that does not depend on the batch size or the team size: every kernel gives
 // bit-identical images and slopes.
 #pragma once
 
@@ -69,15 +73,15 @@ __device__ __forceinline__ int udiv(int i, uint32_t magic) { return (int)__umulh
 // Shared-memory layout: CTA-wide tables, then the batch work area.
 struct ShSmem {
   size_t wxy, rk, hdr;                          // twiddle and 1/k table offsets, header size
-  size_t meta, E, Gt, I, bins, dw, ord, per_batch;  // offsets within the work area
+  size_t meta, E, Gt, I, bins, dw, ord, per_batch;  // offsets within a team's work area
   __host__ __device__ static size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
   __host__ __device__ ShSmem(int nfft, int nu, int nv, int pd, int ncb, int npix2, int S) {
     wxy = align16(sizeof(float2) * nfft + sizeof(int32_t) * (2 * nfft + ncb) + sizeof(float) * npix2);
     rk = align16(wxy + sizeof(float2) * (size_t)(nu + nv) * pd);
     hdr = align16(rk + sizeof(float) * (AOB_POISSON_INV_KMAX + 1));
     size_t o = 0;
-    meta = o;
-    o += align16(sizeof(int32_t) * 8 * (size_t)S);
+    meta = o;  // 8 values per sub-aperture, then the team's two pixel counters
+    o += align16(sizeof(int32_t) * (8 * (size_t)S + 2));
     E = o;
     o += align16(sizeof(float2) * (size_t)S * pd * pd);
     Gt = o;
@@ -93,7 +97,27 @@ struct ShSmem {
     per_batch = o;
   }
   __host__ __device__ size_t bytes() const { return hdr + per_batch; }
+  // tables plus one work area per team
+  __host__ __device__ size_t team_bytes(int nteams) const { return hdr + (size_t)nteams * per_batch; }
 };
+
+// A team of threads that runs sh_batch together: nt threads (a multiple of
+// 32) with team-relative index tid, synchronised according to its kind (a
+// compile-time parameter): the whole CTA (__syncthreads), one warp
+// (__syncwarp, nt = 32) or named barrier ``bar`` (1..15) over nt threads.
+enum : int { TEAM_CTA = 0, TEAM_WARP = 1, TEAM_NAMED = 2 };
+struct Team {
+  int tid, nt, bar;
+};
+template <int TK>
+__device__ __forceinline__ void team_sync(const Team &t) {
+  if constexpr (TK == TEAM_WARP)
+    __syncwarp();
+  else if constexpr (TK == TEAM_CTA)
+    __syncthreads();
+  else
+    asm volatile("bar.sync %0, %1;" ::"r"(t.bar), "r"(t.nt) : "memory");
+}
 
 // CTA-cooperative load of the tables (caller synchronises afterwards).
 template <int NFFT>
@@ -120,14 +144,16 @@ __device__ __forceinline__ void sh_load_tables(const ShKernelArgs &P, unsigned c
   }
 }
 
-// Sub-apertures k = base + s * stride for s < S, processed by the whole CTA.
-// Must be called by every thread of the CTA (it synchronises internally); the
-// caller guarantees base + (S - 1) * stride < nvalid.  On return the work area
-// may be reused.
-template <int NFFT, int PD>
+// Sub-apertures k = base + s * stride for s < S, processed by team T.  Must
+// be called by every thread of the team (it synchronises the team
+// internally); the caller guarantees base + (S - 1) * stride < nvalid.  On
+// return the team's work area may be reused.
+template <int NFFT, int PD, int TK = TEAM_CTA>
 __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int stride, int S,
-                                         const unsigned char *tables, unsigned char *work, const ShSmem &L) {
-  const int tid = threadIdx.x, nt = blockDim.x;
+                                         const unsigned char *tables, unsigned char *work, const ShSmem &L,
+                                         const Team &T) {
+  const int tid = TK == TEAM_CTA ? (int)threadIdx.x : T.tid;
+  const int nt = TK == TEAM_CTA ? (int)blockDim.x : (TK == TEAM_WARP ? 32 : T.nt);
   const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   const float2 *tw = reinterpret_cast<const float2 *>(tables);
   const int32_t *ul = reinterpret_cast<const int32_t *>(tw + NFFT);
@@ -139,14 +165,13 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
   const int pd = PD > 0 ? PD : P.pdiam;
   const int pd2 = pd * pd, nupd = nu * pd, nunv = nu * nv;
 
-  int32_t *m_px = reinterpret_cast<int32_t *>(work + L.meta);
-  int32_t *m_py = m_px + S;
-  int32_t *m_vx = m_py + S;
+  int32_t *m_vx = reinterpret_cast<int32_t *>(work + L.meta) + 2 * S;
   int32_t *m_vy = m_vx + S;
   float *m_fl = reinterpret_cast<float *>(m_vy + S);
   float *m_tot = m_fl + S;
   float *m_rx = m_tot + S;
   float *m_ry = m_rx + S;
+  int *n_listed = reinterpret_cast<int *>(m_ry + S);  // pixels listed for inversion / PTRS in stage 4
   float2 *E = reinterpret_cast<float2 *>(work + L.E);
   float2 *Gt = reinterpret_cast<float2 *>(work + L.Gt);
   float *I = reinterpret_cast<float *>(work + L.I);
@@ -158,8 +183,6 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
   // ---- 0. metadata of the batch (one global round trip for all of it) ----
   if (tid < S) {
     const int k = base + tid * stride;
-    m_px[tid] = P.puppixx[k];
-    m_py[tid] = P.puppixy[k];
     m_vx[tid] = P.validsubsx[k];
     m_vy[tid] = P.validsubsy[k];
     m_fl[tid] = P.flux[k];
@@ -169,9 +192,9 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
     }
   }
   const uint32_t frame = P.frame_ptr ? *P.frame_ptr : P.frame;
-  __shared__ int n_listed[2];  // pixels listed for inversion / PTRS in stage 4
   if (tid == 0) n_listed[0] = n_listed[1] = 0;
-  __syncthreads();
+  // (no barrier here: stage 1 reads the phase-window corners itself, the
+  // metadata and the counters are first used after stage 1's barrier)
 
   // ---- 1. complex field: loads of up to 4 elements issued before any use ----
   const int nE = S * pd2;
@@ -185,7 +208,8 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
         const int l = i - s * pd2;
         const int y = PD > 0 ? l / PD : udiv(l, P.mg_pd);
         const int x = l - y * pd;
-        const int id = (x + m_px[s]) + (y + m_py[s]) * P.npup;
+        const int k = base + s * stride;
+        const int id = (x + __ldg(P.puppixx + k)) + (y + __ldg(P.puppixy + k)) * P.npup;
         ph[j] = P.phase[id];
         am[j] = P.pupil[id];
         of[j] = P.offsets[l];
@@ -201,7 +225,7 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
       }
     }
   }
-  __syncthreads();
+  team_sync<TK>(T);
 
   if constexpr (PD > 0) {
     // Register-blocked DFTs: a thread keeps one input row (column) in registers
@@ -238,7 +262,7 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
         }
       }
     }
-    __syncthreads();
+    team_sync<TK>(T);
     // ---- 3. DFT along y and |.|^2: I[s][b][a] ----
     const int nbch = (nv + BCH - 1) / BCH;
     const uint32_t mgQ = udiv_magic((uint32_t)Q);
@@ -264,7 +288,7 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
         }
       }
     }
-    __syncthreads();
+    team_sync<TK>(T);
   } else {
     // ---- 2. DFT along x: Gt[s][y][a] = sum_x E[s][y][x] W^(u_a x) ----
     for (int i = tid; i < S * nupd; i += nt) {
@@ -281,7 +305,7 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
       }
       Gt[i] = make_float2(re, im);
     }
-    __syncthreads();
+    team_sync<TK>(T);
     // ---- 3. DFT along y and |.|^2: I[s][b][a] ----
     for (int i = tid; i < S * nunv; i += nt) {
       const int s = udiv(i, P.mg_nunv);
@@ -297,7 +321,7 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
       }
       I[i] = fmaf(re, re, im * im);
     }
-    __syncthreads();
+    team_sync<TK>(T);
   }
 
   const int nP = S * npix2;
@@ -353,7 +377,7 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
       }
     }
   }
-  __syncthreads();
+  team_sync<TK>(T);
 
   // ---- 5. noise, cube + image, centroid weights ----
   for (int t = tid; t < nP; t += nt) {
@@ -376,7 +400,7 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
     if (P.ckind == 1 || P.ckind == 2) d = (v > P.c_thresh) ? v - P.c_thresh : 1.e-6f;
     dw[i] = d * wgt;
   }
-  __syncthreads();
+  team_sync<TK>(T);
 
   // ---- 6. centroids ----
   if (P.ckind >= 0) {
@@ -402,7 +426,7 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
       }
     }
   }
-  __syncthreads();
+  team_sync<TK>(T);
 }
 
 }  // namespace aob

@@ -48,10 +48,10 @@ __global__ void __launch_bounds__(SH_THREADS) sh_image_kernel(ShKernelArgs P, in
   const int pd = PD > 0 ? PD : P.pdiam;
   const ShSmem L(NFFT, P.nu, P.nv, pd, P.nrebin2 * P.npix * P.npix, P.npix * P.npix, S);
   sh_load_tables<NFFT>(P, smem, threadIdx.x, blockDim.x);
-  // (sh_batch synchronises before the tables are first read)
+  __syncthreads();
   for (int base = blockIdx.x; base < P.nvalid; base += S * gridDim.x) {
     const int Sb = min(S, (P.nvalid - base + (int)gridDim.x - 1) / (int)gridDim.x);
-    sh_batch<NFFT, PD>(P, base, gridDim.x, Sb, smem, smem + L.hdr, L);
+    sh_batch<NFFT, PD>(P, base, gridDim.x, Sb, smem, smem + L.hdr, L, Team{(int)threadIdx.x, (int)blockDim.x, 0});
   }
 }
 

@@ -426,11 +426,14 @@ int aob_batch_create(aob_batch **out, int device);
 int aob_batch_destroy(aob_batch *b);
 /* The loop must outlive the batch. */
 int aob_batch_add(aob_batch *b, aob_loop *loop);
-/* Tile shapes (the autotuner's choice): sub-apertures per sensor item (0 = 8,
- * at most 64), command-matrix KB per MVM item (0 = 48, at most 200), lag in
+/* Tile shapes (the autotuner's choice): sub-apertures per sensor item (0 =
+ * 32, at most 1024), threads per sensor team (0 = 32; 32, 64, 128 or 256: an
+ * item's sub-apertures are shared by the CTA's teams, each runs its share as
+ * one batch), command-matrix KB per MVM item (0 = 48, at most 200), lag in
  * instances between an instance's sensor and MVM items, CTAs per SM (0 = 2,
- * else 1 or 2), instance order (0 = largest first, 1 = as added). */
-int aob_batch_set_tuning(aob_batch *b, int subaps_per_item, int mvm_kb, int lag, int ctas_per_sm, int order);
+ * at most 4), instance order (0 = largest first, 1 = as added). */
+int aob_batch_set_tuning(aob_batch *b, int subaps_per_item, int team_threads, int mvm_kb, int lag, int ctas_per_sm,
+                         int order);
 int aob_batch_use_graph(aob_batch *b, int enable);
 int aob_batch_refresh(aob_batch *b);
 /* One step of every loop with phases from each sensor's own device buffer. */

@@ -141,7 +141,8 @@ def test_batch_matches_each_loop(mods):
 
 @pytest.mark.parametrize(
     "tuning",
-    [(1, 4, 0, 1, 1), (3, 16, 1, 2, 0), (64, 200, 5, 1, 0), (8, 48, 2, 0, 1), (5, 1, 0, 2, 1)],
+    [(1, 256, 4, 0, 1, 1), (3, 64, 16, 1, 2, 0), (64, 128, 200, 5, 1, 0), (8, 32, 48, 2, 0, 1), (5, 0, 1, 0, 2, 1),
+     (1024, 32, 40, 3, 4, 0), (7, 64, 24, 1, 3, 1)],
 )
 def test_batch_tile_shapes_do_not_change_results(mods, tuning):
     core, W = mods
@@ -213,7 +214,7 @@ def test_batch_rejects_unsupported(mods):
     with pytest.raises(AobError, match="no instances"):
         empty.step()
     with pytest.raises(AobError, match="subaps_per_item"):
-        empty.set_tuning(65, 0, 0, 0, 0)
+        empty.set_tuning(1025, 0, 0, 0, 0, 0)
     with pytest.raises(AobError, match="added twice"):
         core.Batch([loop, loop])
 
