@@ -317,4 +317,32 @@ __device__ __forceinline__ float warp_sum(float v) {
   return v;
 }
 
+// Eight warp sums at once (9 shuffles instead of 40): the xor butterfly of
+// warp_sum with the eight values spread over the lanes as it goes -- at
+// distance 16 a lane keeps four of the values and sends the other four, at
+// 8 two, at 4 one.  Every total is formed by the same additions as
+// warp_sum(a[i]) (float addition commutes), so the results are bit-identical.
+// Returns the total of value ``row`` = 4 (lane>>4 & 1) + 2 (lane>>3 & 1) +
+// (lane>>2 & 1), which all four lanes of the group hold.
+__device__ __forceinline__ float warp_sum8(const float (&a)[8], int lane, int &row) {
+  const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+  float b[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float keep = h16 ? a[i + 4] : a[i], send = h16 ? a[i] : a[i + 4];
+    b[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+  float c[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const float keep = h8 ? b[i + 2] : b[i], send = h8 ? b[i] : b[i + 2];
+    c[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  float d = (h4 ? c[1] : c[0]) + __shfl_xor_sync(0xffffffffu, h4 ? c[0] : c[1], 4);
+  d += __shfl_xor_sync(0xffffffffu, d, 2);
+  d += __shfl_xor_sync(0xffffffffu, d, 1);
+  row = 4 * (int)h16 + 2 * (int)h8 + (int)h4;
+  return d;
+}
+
 }  // namespace aob

@@ -45,6 +45,7 @@ struct aob_sh {
   aob::DevBuf<float> bincube, binimg, intensities, slopes;
   aob::DevBuf<float> twiddle;       // exp(-2 pi i m / nfft) as (re, im) pairs
   aob::DevBuf<float> wxy;           // the same values gathered per (frequency, sample)
+  aob::DevBuf<int4> tblob;          // shared-memory table image (see ShSmem)
   // centroider whose slopes are fused into comp_image (may be null)
   aob_centro *fused = nullptr;
   uint64_t image_gen = 0;  // bumped whenever binimg changes

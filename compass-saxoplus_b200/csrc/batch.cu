@@ -96,9 +96,6 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
 }
 // order earlier generic-proxy accesses of shared memory before later bulk copies into it
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
 
 // Dot product of one 16-byte chunk with its slopes sv[0 .. N/4): the same
 // operation order as the standalone MVM kernels.
@@ -168,9 +165,9 @@ __device__ __forceinline__ void sensor_item(const ShKernelArgs &P, int first, in
   __syncthreads();  // every slope of the item written
 }
 
-// Rows [r0, r0 + R) of instance ``ii``.  All barriers 0..rows_max-1 complete
-// one phase per MVM item (rows beyond R by a plain arrival), so their parity
-// is the CTA's MVM-item count modulo 2.
+// Rows [r0, r0 + R) of instance ``ii``.  All row copies complete on one
+// barrier, which completes one phase per MVM item: its parity is the CTA's
+// MVM-item count modulo 2.
 template <typename T>
 __device__ __forceinline__ void mvm_item(const BatchInst &I, int ii, int r0, int R, const BatchArgs &A,
                                          uint64_t *bars, float *pre, unsigned char *area, uint32_t parity) {
@@ -187,17 +184,18 @@ __device__ __forceinline__ void mvm_item(const BatchInst &I, int ii, int r0, int
   if (tid == 0) {
     fence_proxy_async_smem();
     const unsigned char *src = static_cast<const unsigned char *>(I.mat) + (size_t)r0 * row_bytes;
-    for (int r = 0; r < R; ++r) {
-      mbar_expect_tx(&bars[r], row_bytes);
-      bulk_g2s(rows + (size_t)r * row_bytes, src + (size_t)r * row_bytes, row_bytes, &bars[r]);
-    }
-    for (int r = R; r < RM; ++r) mbar_arrive(&bars[r]);
+    mbar_expect_tx(&bars[0], (uint32_t)R * row_bytes);
+    for (int r = 0; r < R; ++r)
+      bulk_g2s(rows + (size_t)r * row_bytes, src + (size_t)r * row_bytes, row_bytes, &bars[0]);
   }
   for (int r = tid; r < R; r += nt) {
     const int gr = r0 + r;
-    pre[r] = I.rscale ? I.rscale[gr] : 1.f;
-    pre[RM + r] = I.mgain[gr];
-    pre[2 * RM + r] = I.com[gr];
+    const float sc = I.rscale ? __ldg(I.rscale + gr) : 1.f;
+    const float mg = __ldg(I.mgain + gr);
+    const float cm = __ldcg(I.com + gr);
+    pre[r] = sc;
+    pre[RM + r] = mg;
+    pre[2 * RM + r] = cm;
   }
   // the instance's slopes are complete once all its sensor items have finished
   __shared__ int s_dep;
@@ -237,7 +235,7 @@ __device__ __forceinline__ void mvm_item(const BatchInst &I, int ii, int r0, int
     }
   }
   bool rows_ok = true;
-  for (int r = 0; r < R; ++r) rows_ok &= mbar_wait(&bars[r], parity, BROW_MAX_POLLS);
+  rows_ok = mbar_wait(&bars[0], parity, BROW_MAX_POLLS);
   rows_ok = __syncthreads_and(rows_ok) != 0;  // also publishes the staged slopes
   if (!rows_ok && tid == 0) atomicOr(A.status, (uint32_t)ERR_MBAR_TIMEOUT);
   if (dep_ok && rows_ok) {
@@ -260,11 +258,9 @@ __device__ __forceinline__ void mvm_item(const BatchInst &I, int ii, int r0, int
               acc[u] += BPack<T>::dot(q4, sv);
             }
         }
-#pragma unroll
-        for (int u = 0; u < BATCH_RB; ++u) {
-          const float t = warp_sum(acc[u]);
-          if (lane == 0 && rb + u < R) part[slot * R + rb + u] = t;
-        }
+        int u;
+        const float t = warp_sum8(acc, lane, u);
+        if ((lane & 3) == 0 && rb + u < R) part[slot * R + rb + u] = t;
       }
     }
     __syncthreads();
@@ -285,7 +281,7 @@ __device__ __forceinline__ void mvm_item(const BatchInst &I, int ii, int r0, int
     }
   } else if (!rows_ok && tid == 0) {
     // no copy may still be landing when this area is reused
-    for (int r = 0; r < R; ++r) mbar_wait(&bars[r], parity, BROW_MAX_POLLS);
+    mbar_wait(&bars[0], parity, BROW_MAX_POLLS);
   }
   __syncthreads();
 }
@@ -302,7 +298,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, MINB) batch_step_kernel(BatchAr
   float *pre = reinterpret_cast<float *>(sm + batch_bars_bytes(A.rows_max));
   unsigned char *area = sm + batch_bars_bytes(A.rows_max) + batch_pre_bytes(A.rows_max);
   if (tid == 0) {
-    for (int r = 0; r < A.rows_max; ++r) mbar_init(&bars[r], 1);
+    mbar_init(&bars[0], 1);
     fence_mbar_init();
     s_ticket = (int)atomicAdd(&A.ctl[0], 1u);
   }
@@ -318,7 +314,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, MINB) batch_step_kernel(BatchAr
     if (it.x != cur) {
       const uint32_t *src = reinterpret_cast<const uint32_t *>(A.inst + it.x);
       uint32_t *dst = reinterpret_cast<uint32_t *>(&s_I);
-      for (int w = tid; w < (int)(sizeof(BatchInst) / 4); w += blockDim.x) dst[w] = src[w];
+      for (int w = tid; w < (int)(sizeof(BatchInst) / 4); w += blockDim.x) dst[w] = __ldg(src + w);
       cur = it.x;
       __syncthreads();
     }

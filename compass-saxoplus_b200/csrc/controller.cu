@@ -129,13 +129,13 @@ __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_kernel(MvmArgs A) {
     const int l = g & 31, jq = g >> 5;
     const int j = jq / Q, q = jq - j * Q;
     const int src = (l + 32 * j) * V + 4 * q + e;
-    s_sh[i] = (src < A.ncol) ? A.s[src] : 0.f;
+    s_sh[i] = (src < A.ncol) ? __ldcg(A.s + src) : 0.f;  // global-space load: may overtake the stores
   }
-  if (A.bump && blockIdx.x == 0 && threadIdx.x == 0) *A.bump += 1u;
+  if (A.bump && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.bump, 1u);
   __syncthreads();
   const float4 *sv = reinterpret_cast<const float4 *>(s_sh);
-  const int r0 = (int)(((int64_t)blockIdx.x * A.nrow) / gridDim.x);
-  const int r1 = (int)(((int64_t)(blockIdx.x + 1) * A.nrow) / gridDim.x);
+  const int r0 = (int)((blockIdx.x * (uint32_t)A.nrow) / gridDim.x);  // 32-bit: host-checked range
+  const int r1 = (int)(((blockIdx.x + 1) * (uint32_t)A.nrow) / gridDim.x);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nw = blockDim.x >> 5;
   const float4 *svl = sv + lane;
@@ -158,10 +158,14 @@ __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_kernel(MvmArgs A) {
     for (int u = 0; u < MVM_UNROLL; ++u) tot += acc[u];
     tot = warp_sum(tot);
     if (lane == 0) {
-      if (A.rscale) tot *= A.rscale[r];
+      // all loads before the first store (global-space loads, one round trip)
+      const float sc = A.rscale ? __ldg(A.rscale + r) : 1.f;
+      const float mg = A.integrate ? __ldg(A.mgain + r) : 0.f;
+      const float cm = A.integrate ? __ldcg(A.com + r) : 0.f;
+      if (A.rscale) tot *= sc;
       const float e = -tot;
       A.err[r] = e;
-      if (A.integrate) A.com[r] = A.gain * (e * A.mgain[r]) + A.com[r];
+      if (A.integrate) A.com[r] = A.gain * (e * mg) + cm;
     }
   }
 }
@@ -189,8 +193,8 @@ __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_bulk_kernel(MvmArgs A) {
   const int nchunk = A.ld / V;
   const int nsh = mvm_smem_floats(A.ld, V);
   const uint32_t row_bytes = (uint32_t)(A.ld * sizeof(T));
-  const int r0 = (int)(((int64_t)blockIdx.x * A.nrow) / gridDim.x);
-  const int r1 = (int)(((int64_t)(blockIdx.x + 1) * A.nrow) / gridDim.x);
+  const int r0 = (int)((blockIdx.x * (uint32_t)A.nrow) / gridDim.x);  // 32-bit: host-checked range
+  const int r1 = (int)(((blockIdx.x + 1) * (uint32_t)A.nrow) / gridDim.x);
   const int R = r1 - r0;
   if (A.use && *A.use == 0u) return;
   // shared memory: barriers | slopes | rows | per-warp partial sums
@@ -199,29 +203,38 @@ __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_bulk_kernel(MvmArgs A) {
   unsigned char *rows = reinterpret_cast<unsigned char *>(s_sh + nsh);
   float *part = reinterpret_cast<float *>(rows + (size_t)A.rows_per_cta * row_bytes);
   if (threadIdx.x == 0) {
-    for (int r = 0; r < R; ++r) mbar_init(&bars[r], 1);
+    mbar_init(&bars[0], 1);  // one barrier for all the rows
     fence_mbar_init();
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned char *src = static_cast<const unsigned char *>(A.mat) + (size_t)r0 * row_bytes;
-    for (int r = 0; r < R; ++r) {
-      mbar_expect_tx(&bars[r], row_bytes);
-      bulk_g2s(rows + (size_t)r * row_bytes, src + (size_t)r * row_bytes, row_bytes, &bars[r]);
+    mbar_expect_tx(&bars[0], (uint32_t)R * row_bytes);
+    for (int r = 0; r < R; ++r)
+      bulk_g2s(rows + (size_t)r * row_bytes, src + (size_t)r * row_bytes, row_bytes, &bars[0]);
+  }
+  if (A.bump && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.bump, 1u);
+  // epilogue inputs of this thread's row (R <= blockDim), fetched now
+  float e_sc = 1.f, e_mg = 0.f, e_cm = 0.f;
+  if ((int)threadIdx.x < R) {
+    const int gr = r0 + threadIdx.x;
+    if (A.rscale) e_sc = __ldg(A.rscale + gr);
+    if (A.integrate) {
+      e_mg = __ldg(A.mgain + gr);
+      e_cm = __ldcg(A.com + gr);
     }
   }
-  if (A.bump && blockIdx.x == 0 && threadIdx.x == 0) *A.bump += 1u;
   for (int g = threadIdx.x; g < nsh / 4; g += blockDim.x) {
     const int l = g & 31, jq = g >> 5;
     const int j = jq / Q, q = jq - j * Q;
     const int src = (l + 32 * j) * V + 4 * q;
     float4 v4;
     if (src + 3 < A.ncol) {
-      v4 = *reinterpret_cast<const float4 *>(A.s + src);
+      v4 = __ldcg(reinterpret_cast<const float4 *>(A.s + src));
     } else {
-      v4.x = src < A.ncol ? A.s[src] : 0.f;
-      v4.y = src + 1 < A.ncol ? A.s[src + 1] : 0.f;
-      v4.z = src + 2 < A.ncol ? A.s[src + 2] : 0.f;
+      v4.x = src < A.ncol ? __ldcg(A.s + src) : 0.f;
+      v4.y = src + 1 < A.ncol ? __ldcg(A.s + src + 1) : 0.f;
+      v4.z = src + 2 < A.ncol ? __ldcg(A.s + src + 2) : 0.f;
       v4.w = 0.f;
     }
     reinterpret_cast<float4 *>(s_sh)[g] = v4;
@@ -229,7 +242,7 @@ __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_bulk_kernel(MvmArgs A) {
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   bool rows_ok = true;
-  for (int r = 0; r < R; ++r) rows_ok &= mbar_wait(&bars[r], 0, MBAR_MAX_POLLS);
+  rows_ok = mbar_wait(&bars[0], 0, MBAR_MAX_POLLS);
   if (!rows_ok && threadIdx.x == 0 && A.status) atomicOr(A.status, (uint32_t)ERR_MBAR_TIMEOUT);
   const float4 *sv4 = reinterpret_cast<const float4 *>(s_sh);
   for (int rb = 0; rb < R; rb += RB) {
@@ -250,28 +263,25 @@ __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_bulk_kernel(MvmArgs A) {
           }
       }
     }
-#pragma unroll
-    for (int u = 0; u < RB; ++u) {
-      const float t = warp_sum(acc[u]);
-      if (lane == 0 && rb + u < R) part[warp * A.rows_per_cta + rb + u] = t;
-    }
+    int u;
+    const float t = warp_sum8(acc, lane, u);
+    if ((lane & 3) == 0 && rb + u < R) part[warp * A.rows_per_cta + rb + u] = t;
   }
   __syncthreads();
-  if (rows_ok) {
-    for (int r = threadIdx.x; r < R; r += blockDim.x) {
-      float tot = 0.f;
+  if (rows_ok && (int)threadIdx.x < R) {
+    const int r = threadIdx.x;
+    float tot = 0.f;
 #pragma unroll
-      for (int w = 0; w < NW; ++w) tot += part[w * A.rows_per_cta + r];
-      const int gr = r0 + r;
-      if (A.rscale) tot *= A.rscale[gr];
-      const float e = -tot;
-      A.err[gr] = e;
-      if (A.integrate) A.com[gr] = A.gain * (e * A.mgain[gr]) + A.com[gr];
-    }
+    for (int w = 0; w < NW; ++w) tot += part[w * A.rows_per_cta + r];
+    const int gr = r0 + r;
+    if (A.rscale) tot *= e_sc;
+    const float e = -tot;
+    A.err[gr] = e;
+    if (A.integrate) A.com[gr] = A.gain * (e * e_mg) + e_cm;
   }
   // no CTA may exit with a copy still landing in its shared memory
   if (!rows_ok && threadIdx.x == 0)
-    for (int r = 0; r < R; ++r) mbar_wait(&bars[r], 0, MBAR_MAX_POLLS);
+    mbar_wait(&bars[0], 0, MBAR_MAX_POLLS);
 }
 
 struct VoltArgs {
@@ -450,11 +460,12 @@ void aob_ls::launch_mvm(MvmArgs &A, cudaStream_t s) {
   int esize = prec == AOB_PREC_F32 ? 4 : (prec == AOB_PREC_BF16 ? 2 : 1);
   int V = 16 / esize;
   int grid = nblocks > 0 ? std::min(nblocks, nactu) : std::min(nactu, nsm);
+  AOB_REQUIRE((int64_t)nactu * grid < (int64_t)1 << 32, "ls: too many actuators for the MVM row split");
   const size_t slope_bytes = sizeof(float) * mvm_smem_floats(A.ld, V);
   const int rpc = (nactu + grid - 1) / grid;
   const size_t need = mvm_bars_bytes(rpc) + slope_bytes + (size_t)rpc * A.ld * esize +
                       sizeof(float) * (MVM_THREADS / 32) * rpc;
-  const bool bulk = (mvm_kind == 0 || mvm_kind == 1) && need <= MVM_SMEM_MAX && mvm_kind != 2;
+  const bool bulk = (mvm_kind == 0 || mvm_kind == 1) && need <= MVM_SMEM_MAX && mvm_kind != 2 && rpc <= MVM_THREADS;
   if (prec == AOB_PREC_F32)
     launch_mvm_t<float>(A, grid, bulk, s);
   else if (prec == AOB_PREC_BF16)

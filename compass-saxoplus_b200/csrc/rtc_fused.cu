@@ -140,8 +140,9 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
   constexpr int V = FPack<T>::N;
   constexpr int Q = V / 4;
   const uint32_t row_bytes = (uint32_t)(A.ld * sizeof(T));
-  const int r0 = (int)(((int64_t)blockIdx.x * A.nrow) / gridDim.x);
-  const int r1 = (int)(((int64_t)(blockIdx.x + 1) * A.nrow) / gridDim.x);
+  // (32-bit: nrow * gridDim < 2^32 is checked on the host)
+  const int r0 = (int)((blockIdx.x * (uint32_t)A.nrow) / gridDim.x);
+  const int r1 = (int)(((blockIdx.x + 1) * (uint32_t)A.nrow) / gridDim.x);
   const int R = r1 - r0;
   // shared memory: barriers | per-row epilogue inputs | matrix rows |
   //                sensor tables + batch work area | slopes
@@ -155,34 +156,47 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
   const size_t work_bytes = max(L.bytes(), L.hdr + sizeof(float) * (FUSED_THREADS / 32) * A.rows_per_cta);
   float *s_sh = reinterpret_cast<float *>(shm + work_bytes);
 
-  if (threadIdx.x == 0) {
-    for (int r = 0; r < R; ++r) mbar_init(&bars[r], 1);
+  // The last warp, which has the least sensor work in stage 1 (its threads
+  // take field samples only when a CTA has more than 13 sub-apertures of
+  // 6 x 6 samples), initialises the row barriers, issues the copies and fetches the
+  // epilogue inputs; the other threads first wait on the barriers after
+  // several __syncthreads.
+  const int helper = (int)blockDim.x - 32;
+  if ((int)threadIdx.x == helper) {
+    // one barrier for all the rows: a single wait later
+    mbar_init(&bars[0], 1);
     fence_mbar_init();
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
     const unsigned char *src = static_cast<const unsigned char *>(A.mat) + (size_t)r0 * row_bytes;
-    for (int r = 0; r < R; ++r) {
-      mbar_expect_tx(&bars[r], row_bytes);
-      bulk_g2s(rows + (size_t)r * row_bytes, src + (size_t)r * row_bytes, row_bytes, &bars[r]);
-    }
+    mbar_expect_tx(&bars[0], (uint32_t)R * row_bytes);
+    for (int r = 0; r < R; ++r)
+      bulk_g2s(rows + (size_t)r * row_bytes, src + (size_t)r * row_bytes, row_bytes, &bars[0]);
   }
   // epilogue inputs of this CTA's rows, fetched now so the epilogue makes no
   // global round trip: [scale | modal gain | com | ring[0] | ring[1]]
   const int RP = A.rows_per_cta;
-  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+  // (global-space loads, all issued before the shared stores)
+  for (int r = (int)threadIdx.x - helper; r >= 0 && r < R; r += 32) {
     const int gr = r0 + r;
-    pre[r] = A.rscale ? A.rscale[gr] : 1.f;
-    pre[RP + r] = A.mgain[gr];
-    pre[2 * RP + r] = A.com[gr];
+    const float sc = A.rscale ? __ldg(A.rscale + gr) : 1.f;
+    const float mg = __ldg(A.mgain + gr);
+    const float cm = __ldcg(A.com + gr);
+    float o0 = 0.f, o1 = 0.f;
     if (A.delayed) {
-      pre[3 * RP + r] = A.oldest[gr];
-      pre[4 * RP + r] = A.second[gr];
+      o0 = __ldcg(A.oldest + gr);
+      o1 = __ldcg(A.second + gr);
+    }
+    pre[r] = sc;
+    pre[RP + r] = mg;
+    pre[2 * RP + r] = cm;
+    if (A.delayed) {
+      pre[3 * RP + r] = o0;
+      pre[4 * RP + r] = o1;
     }
   }
   // ---- sensor images and slopes: this CTA's sub-apertures, A.batch per round ----
   sh_load_tables<NFFT>(A.sh, shm, threadIdx.x, blockDim.x);
-  __syncthreads();
+  // (the barrier closing sh_batch's stage 1 publishes the tables: stages 0-1
+  // read none of them, so their loads overlap the field's)
   const int nvalid = A.sh.nvalid;
   for (int base = blockIdx.x; base < nvalid; base += A.batch * gridDim.x) {
     const int Sb = min(A.batch, (nvalid - base + (int)gridDim.x - 1) / (int)gridDim.x);
@@ -191,7 +205,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
   // ---- all slopes published ----
   const bool ok = grid_barrier(A.gbar, gridDim.x, A.status);
   if (ok) {
-    if (A.bump && blockIdx.x == 0 && threadIdx.x == 0) *A.bump += 1u;
+    if (A.bump && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.bump, 1u);  // no round trip
     // slopes into shared memory, 16 bytes per load (L2 only: they were written by
     // other CTAs of this launch); group g of the layout holds slopes
     // [(chunk) * V + 4 q, +4) for chunk = (g & 31) + 32 j, g >> 5 = j * Q + q
@@ -220,7 +234,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
     const int nchunk = A.ld / V;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     bool rows_ok = true;
-    for (int r = 0; r < R; ++r) rows_ok &= mbar_wait(&bars[r], 0, ROW_MAX_POLLS);
+    rows_ok = mbar_wait(&bars[0], 0, ROW_MAX_POLLS);
     if (!rows_ok && lane == 0) atomicOr(A.status, (uint32_t)ERR_MBAR_TIMEOUT);
     float *part = reinterpret_cast<float *>(shm + L.hdr);  // [NW][rows_per_cta], sensor work area is free now
     const float4 *sv4 = reinterpret_cast<const float4 *>(s_sh);
@@ -242,11 +256,9 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
             }
         }
       }
-#pragma unroll
-      for (int u = 0; u < RB; ++u) {
-        const float t = warp_sum(acc[u]);
-        if (lane == 0 && rb + u < R) part[warp * A.rows_per_cta + rb + u] = t;
-      }
+      int u;
+      const float t = warp_sum8(acc, lane, u);
+      if ((lane & 3) == 0 && rb + u < R) part[warp * A.rows_per_cta + rb + u] = t;
     }
     __syncthreads();
     // integrator and voltage per row, one thread per row
@@ -273,8 +285,8 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
   }
   // no CTA may exit with a copy still landing in its shared memory
   __syncthreads();
-  if (threadIdx.x == 0)
-    for (int r = 0; r < R; ++r) mbar_wait(&bars[r], 0, ROW_MAX_POLLS);
+  if ((int)threadIdx.x == helper)
+    mbar_wait(&bars[0], 0, ROW_MAX_POLLS);
 }
 
 // ---------------------------------------------------------------------------
@@ -369,6 +381,7 @@ bool aob_loop::launch_fused(bool noise, cudaStream_t s, bool frame_on_device, bo
   A.gbar = gbar.p;
   const int nsm = num_sms(w->device);
   const int grid = std::min(nsm, c->nactu);
+  AOB_REQUIRE((int64_t)c->nactu * grid < (int64_t)1 << 32, "loop: too many actuators for the fused kernel");
   A.rows_per_cta = (c->nactu + grid - 1) / grid;
   // sub-apertures per CTA and round: the CTA's whole share if shared memory allows
   const size_t fixed = fused_bars_bytes(A.rows_per_cta) + fused_pre_bytes(A.rows_per_cta) +

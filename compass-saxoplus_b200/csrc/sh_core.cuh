@@ -34,6 +34,7 @@ struct ShKernelArgs {
   float scale;
   int pdiam, nvalid, npix, nrebin2;
   int nu, nv;
+  const int4 *tblob;      // twiddles, ulist, vlist, cbin and wxy in their shared-memory layout
   const float2 *twiddle;  // exp(-2 pi i m / nfft), m < nfft
   const int32_t *ulist;
   const int32_t *vlist;
@@ -71,14 +72,17 @@ __host__ __device__ inline uint32_t udiv_magic(uint32_t d) {
 __device__ __forceinline__ int udiv(int i, uint32_t magic) { return (int)__umulhi((uint32_t)i, magic); }
 
 // Shared-memory layout: CTA-wide tables, then the batch work area.
+// Tables: [tw | ulist | vlist | cbin | wxy | 1/k | wCoG weights]; everything
+// before the 1/k table is one contiguous image per sensor (ShKernelArgs::tblob).
 struct ShSmem {
-  size_t wxy, rk, hdr;                          // twiddle and 1/k table offsets, header size
+  size_t wxy, rk, wt, hdr;                      // table offsets, header size
   size_t meta, E, Gt, I, bins, dw, ord, per_batch;  // offsets within a team's work area
   __host__ __device__ static size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
   __host__ __device__ ShSmem(int nfft, int nu, int nv, int pd, int ncb, int npix2, int S) {
-    wxy = align16(sizeof(float2) * nfft + sizeof(int32_t) * (2 * nfft + ncb) + sizeof(float) * npix2);
+    wxy = align16(sizeof(float2) * nfft + sizeof(int32_t) * (2 * nfft + ncb));
     rk = align16(wxy + sizeof(float2) * (size_t)(nu + nv) * pd);
-    hdr = align16(rk + sizeof(float) * (AOB_POISSON_INV_KMAX + 1));
+    wt = align16(rk + sizeof(float) * (AOB_POISSON_INV_KMAX + 1));
+    hdr = align16(wt + sizeof(float) * npix2);
     size_t o = 0;
     meta = o;  // 8 values per sub-aperture, then the team's two pixel counters
     o += align16(sizeof(int32_t) * (8 * (size_t)S + 2));
@@ -119,25 +123,19 @@ __device__ __forceinline__ void team_sync(const Team &t) {
     asm volatile("bar.sync %0, %1;" ::"r"(t.bar), "r"(t.nt) : "memory");
 }
 
-// CTA-cooperative load of the tables (caller synchronises afterwards).
+// CTA-cooperative load of the tables (caller synchronises afterwards): the
+// sensor's table image with 16-byte loads (one page, one request per
+// thread), the wCoG weights and the 1/k table of the Poisson sampler.
 template <int NFFT>
 __device__ __forceinline__ void sh_load_tables(const ShKernelArgs &P, unsigned char *smem, int tid, int nthreads) {
-  float2 *tw = reinterpret_cast<float2 *>(smem);
-  int32_t *ul = reinterpret_cast<int32_t *>(tw + NFFT);
-  int32_t *vl = ul + NFFT;
-  int32_t *cb = vl + NFFT;
   const int npix2 = P.npix * P.npix;
-  const int ncb = P.nrebin2 * npix2;
-  float *wt = reinterpret_cast<float *>(cb + ncb);
-  for (int i = tid; i < NFFT; i += nthreads) tw[i] = P.twiddle[i];
-  for (int i = tid; i < P.nu; i += nthreads) ul[i] = P.ulist[i];
-  for (int i = tid; i < P.nv; i += nthreads) vl[i] = P.vlist[i];
-  for (int i = tid; i < ncb; i += nthreads) cb[i] = P.cbin[i];
-  if (P.ckind == 2 && !P.c_wper)
-    for (int i = tid; i < npix2; i += nthreads) wt[i] = P.c_weights[i];
-  const ShSmem L(NFFT, P.nu, P.nv, P.pdiam, ncb, npix2, 1);
-  float2 *wxy = reinterpret_cast<float2 *>(smem + L.wxy);
-  for (int i = tid; i < (P.nu + P.nv) * P.pdiam; i += nthreads) wxy[i] = P.wxy[i];
+  const ShSmem L(NFFT, P.nu, P.nv, P.pdiam, P.nrebin2 * npix2, npix2, 1);
+  int4 *dst = reinterpret_cast<int4 *>(smem);
+  for (int i = tid; i < (int)(L.rk / 16); i += nthreads) dst[i] = __ldg(P.tblob + i);
+  if (P.ckind == 2 && !P.c_wper) {
+    float *wt = reinterpret_cast<float *>(smem + L.wt);
+    for (int i = tid; i < npix2; i += nthreads) wt[i] = __ldg(P.c_weights + i);
+  }
   if (P.noise_mode >= 1) {
     float *rk = reinterpret_cast<float *>(smem + L.rk);
     for (int i = tid; i <= AOB_POISSON_INV_KMAX; i += nthreads) rk[i] = i ? __frcp_rn((float)i) : 0.f;
@@ -160,7 +158,7 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
   const int32_t *vl = ul + NFFT;
   const int32_t *cb = vl + NFFT;
   const int npix = P.npix, npix2 = npix * npix, nr2 = P.nrebin2;
-  const float *wt = reinterpret_cast<const float *>(cb + nr2 * npix2);
+  const float *wt = reinterpret_cast<const float *>(tables + L.wt);
   const int nu = P.nu, nv = P.nv;
   const int pd = PD > 0 ? PD : P.pdiam;
   const int pd2 = pd * pd, nupd = nu * pd, nunv = nu * nv;
@@ -180,18 +178,24 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
   int *order = reinterpret_cast<int *>(work + L.ord);  // stage 4-5 pixel list
   const float *rk = reinterpret_cast<const float *>(tables + L.rk);
 
-  // ---- 0. metadata of the batch (one global round trip for all of it) ----
+  // ---- 0. metadata of the batch (one global round trip for all of it:
+  //      global-space loads, free to overtake the shared stores) ----
+  const uint32_t frame = P.frame_ptr ? __ldcg(P.frame_ptr) : P.frame;
   if (tid < S) {
     const int k = base + tid * stride;
-    m_vx[tid] = P.validsubsx[k];
-    m_vy[tid] = P.validsubsy[k];
-    m_fl[tid] = P.flux[k];
+    const int vx = __ldg(P.validsubsx + k), vy = __ldg(P.validsubsy + k);
+    const float fl = __ldg(P.flux + k);
+    float rx = 0.f, ry = 0.f;
     if (P.ckind >= 0) {
-      m_rx[tid] = P.c_ref[P.c_order ? 2 * k : k];
-      m_ry[tid] = P.c_ref[P.c_order ? 2 * k + 1 : k + P.nvalid];
+      rx = __ldg(P.c_ref + (P.c_order ? 2 * k : k));
+      ry = __ldg(P.c_ref + (P.c_order ? 2 * k + 1 : k + P.nvalid));
     }
+    m_vx[tid] = vx;
+    m_vy[tid] = vy;
+    m_fl[tid] = fl;
+    m_rx[tid] = rx;
+    m_ry[tid] = ry;
   }
-  const uint32_t frame = P.frame_ptr ? *P.frame_ptr : P.frame;
   if (tid == 0) n_listed[0] = n_listed[1] = 0;
   // (no barrier here: stage 1 reads the phase-window corners itself, the
   // metadata and the counters are first used after stage 1's barrier)
@@ -210,9 +214,9 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
         const int x = l - y * pd;
         const int k = base + s * stride;
         const int id = (x + __ldg(P.puppixx + k)) + (y + __ldg(P.puppixy + k)) * P.npup;
-        ph[j] = P.phase[id];
-        am[j] = P.pupil[id];
-        of[j] = P.offsets[l];
+        ph[j] = __ldg(P.phase + id);
+        am[j] = __ldg(P.pupil + id);
+        of[j] = __ldg(P.offsets + l);
       }
     }
 #pragma unroll

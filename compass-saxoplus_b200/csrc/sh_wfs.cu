@@ -29,6 +29,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "aob_objects.hpp"
@@ -48,7 +49,8 @@ __global__ void __launch_bounds__(SH_THREADS) sh_image_kernel(ShKernelArgs P, in
   const int pd = PD > 0 ? PD : P.pdiam;
   const ShSmem L(NFFT, P.nu, P.nv, pd, P.nrebin2 * P.npix * P.npix, P.npix * P.npix, S);
   sh_load_tables<NFFT>(P, smem, threadIdx.x, blockDim.x);
-  __syncthreads();
+  // (the barrier closing sh_batch's stage 1 publishes the tables: stages 0-1
+  // read none of them, so their loads overlap the field's)
   for (int base = blockIdx.x; base < P.nvalid; base += S * gridDim.x) {
     const int Sb = min(S, (P.nvalid - base + (int)gridDim.x - 1) / (int)gridDim.x);
     sh_batch<NFFT, PD>(P, base, gridDim.x, Sb, smem, smem + L.hdr, L, Team{(int)threadIdx.x, (int)blockDim.x, 0});
@@ -154,6 +156,20 @@ void aob_sh::load_arrays(const int32_t *h_binmap, const float *h_offsets, const 
     for (int y = 0; y < nphase; ++y) tw(V[b] * y, &W[2 * ((size_t)(nu + b) * nphase + y)]);
   wxy.alloc((int64_t)W.size());
   wxy.upload(W.data(), (int64_t)W.size());
+  // the shared-memory table image [tw | ulist | vlist | cbin | wxy]
+  {
+    const ShSmem L(nfft, nu, nv, nphase, nr2 * np2, np2, 1);
+    std::vector<unsigned char> img(L.rk, 0);
+    std::vector<float> t(2 * nfft);
+    for (int m = 0; m < nfft; ++m) tw(m, &t[2 * m]);
+    std::memcpy(img.data(), t.data(), sizeof(float) * 2 * nfft);
+    std::memcpy(img.data() + sizeof(float) * 2 * nfft, U.data(), sizeof(int32_t) * nu);
+    std::memcpy(img.data() + sizeof(float) * 2 * nfft + sizeof(int32_t) * nfft, V.data(), sizeof(int32_t) * nv);
+    std::memcpy(img.data() + sizeof(float) * 2 * nfft + sizeof(int32_t) * 2 * nfft, C.data(), sizeof(int32_t) * C.size());
+    std::memcpy(img.data() + L.wxy, W.data(), sizeof(float) * W.size());
+    tblob.alloc((int64_t)(L.rk / 16));
+    AOB_CUDA(cudaMemcpy(tblob.p, img.data(), L.rk, cudaMemcpyHostToDevice));
+  }
   ulist.alloc(nu);
   vlist.alloc(nv);
   cbin.alloc((int64_t)nr2 * np2);
@@ -227,6 +243,7 @@ aob_centro *aob_sh::make_args(bool with_noise, float *slopes_dst, const uint32_t
   P.nu = nu;
   P.nv = nv;
   P.twiddle = reinterpret_cast<const float2 *>(twiddle.p);
+  P.tblob = tblob.p;
   P.wxy = reinterpret_cast<const float2 *>(wxy.p);
   P.ulist = ulist.p;
   P.vlist = vlist.p;
