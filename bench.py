@@ -18,6 +18,14 @@ Other keys of the JSON line:
             the measured HBM copy bandwidth in MEASURED_PEAKS.json;
   cpu_baseline  the float64 NumPy/SciPy restatement timed on the host cores.
 
+--workload selects what is measured: ``saxo40`` (default, the line above),
+or one of the other scope rows, each printing its own JSON line with its own
+metric, roofline and CPU baseline: ``mc64`` (64 uneven SH loops advanced by
+one persistent launch per step, BF16 MVM), ``pyr50`` (pyramid sensor, 24
+modulation points over 512 x 512 FFTs, slopes and a 1600-actuator LS MVM),
+``mlp`` (the learned reconstructor: batch-1 inference against the LS MVM and
+training throughput on the tensor cores).
+
 --impl reference runs the reference-algorithm CPU restatement (the reference
 has no CPU implementation of this path; its GPU code needs its own CMake build)
 as the baseline arm.  Multi-GPU (torchrun): the path does not shard -- every
@@ -120,6 +128,44 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def graph_time(torch, flush, fn, n=20, with_flush=True):
+    """Mean device seconds of fn(stream) per launch: n x [flush, fn] minus n x [flush],
+    each replayed as one CUDA graph (no host gaps), best of 5 replays."""
+    gs = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(gs):
+        for _ in range(2):
+            fn(gs.cuda_stream)
+    torch.cuda.synchronize()
+
+    def capture(body):
+        gr = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(gr, stream=gs):
+            for _ in range(n):
+                if with_flush:
+                    flush.zero_()
+                body()
+        return gr
+
+    g1 = capture(lambda: fn(gs.cuda_stream))
+    g0 = capture(lambda: None)
+    out = []
+    for gr in (g1, g0):
+        for _ in range(2):
+            gr.replay()
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(5):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            gr.replay()
+            b.record()
+            torch.cuda.synchronize()
+            best = min(best, a.elapsed_time(b) / 1000.0)
+        out.append(best)
+    return (out[0] - out[1]) / n
+
+
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -184,6 +230,218 @@ def run_reference(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# secondary workloads (--workload mc64 | pyr50 | mlp): one JSON line each
+def _line(args, workload, metric, value, unit, ms_per_step, dtype, config, **extra):
+    d = {"workload": workload, "metric": metric, "value": value, "unit": unit, "n_gpus": 1,
+         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+         "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic", "config": config}
+    d.update(extra)
+    print(json.dumps(d))
+
+
+def run_mc64(args, torch):
+    """64 uneven SH loops (nxsub 24..40, 6x6 / 8x8 px, seeds 0..63, r0 in 0.08..0.20 m,
+    photon + readout noise, wCoG, BF16 MVM) advanced by one persistent launch per step."""
+    from aob200 import autotune as AT
+    from aob200 import workloads as W
+
+    t0 = time.perf_counter()
+    insts = W.mc_setup(64)[:args.instances]
+    loops, batch = W.build_mc_batch(insts, precision="bf16")
+    setup_s = time.perf_counter() - t0
+    if args.no_tune:
+        batch.set_tuning(16, 256, 96, 16, 2, 0)
+        tune = {"tuning": {"subaps": 16, "team": 256, "mvm_kb": 96, "lag": 16, "ctas_per_sm": 2, "order": 0}}
+    else:
+        tune = AT.tune_batch(batch, noise=True)
+    info = batch.info()
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    for _ in range(args.warmup):
+        batch.step(True, sptr)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(0) as clk:
+        for a, b in ev:
+            a.record(stream)
+            batch.step(True, sptr)
+            b.record(stream)
+        torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    n = info["instances"]
+    peak, peak_kind = _peaks()
+    achieved = info["alg_bytes"] / (ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": _profile_traffic("batch_step_mc64"), "kernel": "batch_step_kernel",
+                "algorithmic_bytes_per_launch": info["alg_bytes"], "duration_us": ms * 1e3, "peak_source": peak_kind,
+                "note": "the sensor stages (54,048 sub-apertures) keep the SMs busy longer than the 240 MB stream"}
+    # e2e: all phases in from pinned host memory, all voltages out, every step
+    phases = torch.from_numpy(np.concatenate([np.ascontiguousarray(i.phase.ravel(order="F")) for i in insts]))
+    h_ph = phases.pin_memory()
+    h_v = torch.zeros(info["volt_floats"], dtype=torch.float32).pin_memory()
+    for _ in range(3):
+        batch.step_host(h_ph.data_ptr(), h_v.data_ptr(), True, sptr)
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for a, b in ev2:
+        a.record(stream)
+        batch.step_host(h_ph.data_ptr(), h_v.data_ptr(), True, sptr)
+        b.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = sum(a.elapsed_time(b) for a, b in ev2) / args.steps
+    e2e = {"value": n / (ms_e2e * 1e-3), "unit": "instance iters/s", "h2d_bytes_per_step": info["phase_floats"] * 4,
+           "d2h_bytes_per_step": info["volt_floats"] * 4, "call": "aob_batch_step_host"}
+    # the same 64 loops stepped one after another with their own fused kernels
+    seq_ms = 0.0
+    for (_, _, _, loop) in loops:
+        seq_ms += loop.time(noise=True, warmup=2, iters=10)
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle.loop_cpu import CpuShLoop
+
+        k, t_cpu = 0, 0.0
+        for inst in insts[:4]:
+            st = inst.setup
+            cl = CpuShLoop(st.geom, st.cmat, st.centroider, st.threshold, st.weights, st.noise)
+            cl.step(inst.phase)
+            t1 = time.perf_counter()
+            for _ in range(5):
+                cl.step(inst.phase)
+            t_cpu += time.perf_counter() - t1
+            k += 5
+        cpu = {"value": k / t_cpu, "unit": "instance iters/s", "cores": cl.workers, "kind": "port",
+               "sample": f"{k} loop iterations of the first 4 instances (float64 NumPy/SciPy, {cl.workers} threads)"}
+    _line(args, "mc64", "Monte Carlo instance iterations/s, %d uneven SH loops, one launch per step" % n, n / (ms * 1e-3),
+          "instance iters/s", ms, "f32 sensor, bf16 MVM",
+          {"workload": "mc64: %d SH loops, nxsub 24..40, 6x6/8x8 px, Nfft 16/32, photon + 0.5 e- noise, wCoG, " % n +
+                       "BF16 LS MVM; %d sub-apertures, %d actuators in total" % (
+                           sum(i.setup.geom.nvalid for i in insts), sum(i.setup.nactu for i in insts)),
+           "l2": "inputs (%.0f MB) larger than L2" % (info["alg_bytes"] / 1e6), "cuda_graph": True,
+           "tuning": tune["tuning"], "setup_s": setup_s},
+          roofline=roofline, e2e=e2e, cpu_baseline=cpu, clocks=clk.summary(), gpu_launches=args.steps,
+          sequential_loops_ms_per_step=seq_ms, speedup_vs_sequential_loops=seq_ms / ms)
+
+
+def run_pyr50(args, torch):
+    """Pyramid: 50 x 50 pupil samples, 24 modulation points at 3 lambda/D over 512 x 512
+    FFTs, photon + 0.3 e- noise, slopes and a 1600-actuator LS MVM."""
+    from aob200 import core as C
+    from aob200 import geometry as G
+
+    g = G.pyr_geometry(G.PyrParams(nxsub=50, wavelength_um=1.075, ampl=3.0, npts=24, pup_sep=32, fssize=3.2), 100,
+                       diam=8.0, cobs=0.14)
+    w = C.PyrWfs.from_geometry(g, noise=0.3, seed=3)
+    phase = (np.random.default_rng(0).standard_normal((g.tel.n, g.tel.n)) * 0.02).astype(np.float32)
+    w.set_phase(phase)
+    c = C.Centroider(g.nvalid, 0.0, 1.0, "pyr")
+    c.load_validpos(g.validsubsx, g.validsubsy)
+    c.attach(w)
+    ls = C.LsController(2 * g.nvalid, 1600)
+    ls.set_cmat((np.random.default_rng(1).standard_normal((1600, 2 * g.nvalid)) * 0.01).astype(np.float32))
+    d = ls.buffer("centroids")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def step(sp):
+        w.comp_image(True, sp)
+        c.get_cog(d.ptr, sp)
+        ls.comp_com(sp)
+
+    with ClockSampler(0) as clk:
+        t_step = graph_time(torch, flush, step, n=max(args.steps, 5))
+        t_img = graph_time(torch, flush, lambda sp: w.comp_image(True, sp), n=max(args.steps, 5))
+    nfft, npts = g.nfft, g.pyr_cx.size
+    flops = (2 * npts + 3) * 5 * nfft * nfft * np.log2(nfft * nfft)  # 2 FFTs per point + the convolution's 2 + 1
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import pyr as opyr
+
+        t1 = time.perf_counter()
+        k = 0
+        while k < 3:
+            opyr.comp_image(phase, g.tel.mpupil, g, g.wavelength_um, g.nphotons, noise=0.3, frame=k)
+            k += 1
+        dt = time.perf_counter() - t1
+        cpu = {"value": k / dt, "unit": "iters/s", "cores": 1, "kind": "port",
+               "sample": f"{k} pyramid images (float64 NumPy FFT, single thread)"}
+    _line(args, "pyr50", "pyramid loop iters/s (image + slopes + 1600-actuator LS MVM)", 1.0 / t_step, "iters/s",
+          t_step * 1e3, "f32",
+          {"workload": f"pyr50: {g.nxsub}x{g.nxsub} pupil samples per image, {npts} modulation points at 3 lambda/D, "
+                       f"{nfft}x{nfft} FFTs, {g.nvalid} valid, 1600-actuator LS MVM",
+           "l2": "flushed before every timed step (256 MB write)"},
+          roofline={"bound": "fp32 FFT", "achieved": flops / t_img / 1e12, "unit": "TFLOP/s", "peak": None,
+                    "frac": None, "traffic": None, "kernel": "pyramid image kernels",
+                    "flops_per_image": flops, "image_us": t_img * 1e6, "step_us": t_step * 1e6},
+          cpu_baseline=cpu, clocks=clk.summary(), gpu_launches=None)
+
+
+def run_mlp(args, torch):
+    """Learned reconstructor at the saxo40 geometry: 2496 slopes -> 1024 -> 1024 (GELU)
+    -> 1377 commands (+ linear skip), BF16 weights, FP32 accumulation."""
+    from aob200 import core as C
+    from aob200 import mlp as M
+    from aob200.workloads import sh_loop_setup
+
+    setup = sh_loop_setup("saxo40")
+    nin, nout = setup.nslope, setup.nactu
+    rng = np.random.default_rng(0)
+    ls = C.LsController(nin, nout)
+    ls.set_cmat(setup.cmat)
+    ls.set_gain(0.4)
+    ls.set_centroids(rng.standard_normal(nin).astype(np.float32))
+    net = M.MlpReconstructor(nin, nout, 1024, 1024, seed=1)
+    net.init_from_ls(setup.cmat, 10.0, 1.0)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    res = {}
+    with ClockSampler(0) as clk:
+        res["ls_f32_us"] = graph_time(torch, flush, lambda sp: ls.comp_com(sp)) * 1e6
+        ls.set_precision("bf16")
+        res["ls_bf16_us"] = graph_time(torch, flush, lambda sp: ls.comp_com(sp)) * 1e6
+        ls.set_precision("f32")
+        res["mlp_infer_us"] = graph_time(torch, flush, lambda sp: net.comp_com(ls, 3e38, sp)) * 1e6
+        params = nin * 1024 + 1024 * 1024 + 1024 * nout + nin * nout
+        B = 4096
+        X = torch.randn(B, nin, device="cuda")
+        T = torch.randn(B, nout, device="cuda")
+        t = graph_time(torch, flush, lambda sp: net.train_step(X.data_ptr(), T.data_ptr(), B, 1e-4, None, sp), n=5,
+                       with_flush=False)
+        res["train_step_B4096_us"] = t * 1e6
+        res["train_tflops"] = 6 * params * B / t / 1e12
+    peak_t = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak_t = float(json.load(f)["bf16_tflops"])
+    except Exception:
+        peak_t = 1590.0
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import mlp as om
+
+        P = net.get_params()
+        x = rng.standard_normal((1, nin)).astype(np.float32)
+        t1 = time.perf_counter()
+        k = 0
+        while k < 20:
+            om.forward(P, x, net.in_scale)
+            k += 1
+        cpu = {"value": k / (time.perf_counter() - t1), "unit": "inferences/s", "cores": 1, "kind": "port",
+               "sample": f"{k} batch-1 forward passes (NumPy, bfloat16-rounded weights)"}
+    _line(args, "mlp", "learned reconstructor batch-1 inferences/s (LS MVM alongside)", 1e6 / res["mlp_infer_us"],
+          "inferences/s", res["mlp_infer_us"] / 1e3, "bf16",
+          {"workload": f"mlp: {nin} -> 1024 -> 1024 -> {nout} + linear skip, BF16 weights, FP32 accumulation",
+           "l2": "flushed before every timed inference (256 MB write)"},
+          roofline={"bound": "tensor", "achieved": res["train_tflops"], "peak": peak_t, "unit": "TFLOP/s",
+                    "frac": res["train_tflops"] / peak_t, "traffic": None, "kernel": "mlp_gemm_kernel (training step)",
+                    **res},
+          cpu_baseline=cpu, clocks=clk.summary(), gpu_launches=None)
+
+
+def run_secondary(args):
+    import torch
+
+    torch.cuda.set_device(0)
+    return {"mc64": run_mc64, "pyr50": run_pyr50, "mlp": run_mlp}[args.workload](args, torch) or 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -193,10 +451,15 @@ def main():
     ap.add_argument("--precision", default="f32", choices=["f32", "bf16", "fp8"])
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="saxo40", choices=["saxo40", "mc64", "pyr50", "mlp"])
+    ap.add_argument("--instances", type=int, default=64, help="mc64: number of instances (the first N of the list)")
+    ap.add_argument("--no-tune", action="store_true", help="mc64: fixed tile shapes instead of the autotuner")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "saxo40":
+        return run_secondary(args)
 
     ws, rank, local = _dist()
     import torch
@@ -265,47 +528,11 @@ def main():
     launches = loop.kernels_per_step() * args.steps
 
     # ---- per-kernel device durations (graph replay, no host gaps) ----------
-    def graph_time(fn, n=20, with_flush=True):
-        """Mean device time of fn() per launch: n x [flush, fn] minus n x [flush], replayed as one graph."""
-        gs = torch.cuda.Stream()
-        torch.cuda.synchronize()
-        with torch.cuda.stream(gs):
-            for _ in range(2):
-                fn(gs.cuda_stream)
-        torch.cuda.synchronize()
-
-        def capture(body):
-            gr = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(gr, stream=gs):
-                for _ in range(n):
-                    if with_flush:
-                        flush.zero_()
-                    body()
-            return gr
-
-        g1 = capture(lambda: fn(gs.cuda_stream))
-        g0 = capture(lambda: None)
-        out = []
-        for gr in (g1, g0):
-            for _ in range(2):
-                gr.replay()
-            torch.cuda.synchronize()
-            best = float("inf")
-            for _ in range(5):
-                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                a.record()
-                gr.replay()
-                b.record()
-                torch.cuda.synchronize()
-                best = min(best, a.elapsed_time(b) / 1000.0)
-            out.append(best)
-        return (out[0] - out[1]) / n
-
     loop.use_graph(False)
-    t_step = graph_time(lambda sp: loop.step(None, None, True, sp))
+    t_step = graph_time(torch, flush, lambda sp: loop.step(None, None, True, sp))
     fused = loop.kernels_per_step() == 1
-    t_wfs = graph_time(lambda sp: wfs.comp_image(True, sp))
-    t_mvm = graph_time(lambda sp: ls.comp_com(sp))
+    t_wfs = graph_time(torch, flush, lambda sp: wfs.comp_image(True, sp))
+    t_mvm = graph_time(torch, flush, lambda sp: ls.comp_com(sp))
     loop.use_graph(not args.no_graph)
     esize = {"f32": 4, "bf16": 2, "fp8": 1}[args.precision]
     ld = {"f32": 4, "bf16": 8, "fp8": 16}[args.precision]
