@@ -10,8 +10,8 @@
  * is at x + y*n.
  *
  * Each entry point names the reference interface it replaces (paths within
- * the reference project).  The drop-in Python modules `sutra` / `carma` shipped
- * with this library bind exactly these symbols with ctypes.
+ * the reference project).  The Python package `aob200` (and the binding shown
+ * in INTEGRATION.md) binds exactly these symbols with ctypes.
  */
 #ifndef AOB200_H
 #define AOB200_H
