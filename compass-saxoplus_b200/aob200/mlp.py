@@ -89,6 +89,10 @@ class MlpReconstructor:
     def infer(self, dev_x, dev_y, stream=None):
         call("aob_mlp_infer", self.h, dev_x, dev_y, stream)
 
+    def set_mode(self, mode=0):
+        """0: one cooperative kernel per control step when it fits, 1: the multi-kernel path."""
+        call("aob_mlp_set_mode", self.h, int(mode))
+
     def comp_com(self, ls, threshold, stream=None):
         call("aob_mlp_comp_com", self.h, ls.h, float(threshold), stream)
 

@@ -268,6 +268,10 @@ struct aob_mlp {
   // batch-1 inference
   aob::DevBuf<float> ix, ih1, ih2, iy;
   aob::DevBuf<uint32_t> use_ls, fallbacks;
+  // single-launch control step (comp_com_fused)
+  int fused_mode = 0;  // 0: fused kernel when it fits, 1: multi-kernel path
+  aob::DevBuf<float> partial;
+  aob::DevBuf<unsigned long long> gbar;
 
   aob_mlp(int device, int nin, int nh1, int nh2, int nout);
   int rows(int l) const { return l == 0 ? ph1 : (l == 1 ? ph2 : pout); }
@@ -279,6 +283,7 @@ struct aob_mlp {
   void backward(const float *target, int batch, float *loss, cudaStream_t s);
   void adam(float lr, cudaStream_t s);
   void infer(const float *x, float *y_out, cudaStream_t s);
+  bool comp_com_fused(aob_ls *ls, float threshold, cudaStream_t s);
 };
 
 namespace aob {

@@ -45,6 +45,7 @@
 #include <vector>
 
 #include "aob_objects.hpp"
+#include "mvm_core.cuh"
 #include "sh_core.cuh"
 
 namespace aob {
@@ -87,7 +88,6 @@ struct BatchArgs {
 
 __host__ __device__ inline size_t batch_bars_bytes(int rows) { return 128 * (((size_t)rows * 8 + 127) / 128); }
 __host__ __device__ inline size_t batch_pre_bytes(int rows) { return 128 * (((size_t)rows * 12 + 127) / 128); }
-__host__ __device__ inline int batch_slope_floats(int ld, int v) { return ((ld / v + 31) / 32) * 32 * v; }
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
   unsigned v;
@@ -96,50 +96,6 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
 }
 // order earlier generic-proxy accesses of shared memory before later bulk copies into it
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-// Dot product of one 16-byte chunk with its slopes sv[0 .. N/4): the same
-// operation order as the standalone MVM kernels.
-template <typename T>
-struct BPack;
-template <>
-struct BPack<float> {
-  static constexpr int N = 4;
-  __device__ static float dot(const uint4 &q, const float4 *sv) {
-    const float *f = reinterpret_cast<const float *>(&q);
-    const float4 s = sv[0];
-    return fmaf(f[3], s.w, fmaf(f[2], s.z, fmaf(f[1], s.y, f[0] * s.x)));
-  }
-};
-template <>
-struct BPack<__nv_bfloat16> {
-  static constexpr int N = 8;
-  __device__ static float dot(const uint4 &q, const float4 *sv) {
-    const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
-    float a = 0.f;
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const float4 s = sv[i];
-      const float2 f0 = __bfloat1622float2(h[2 * i]), f1 = __bfloat1622float2(h[2 * i + 1]);
-      a = fmaf(f1.y, s.w, fmaf(f1.x, s.z, fmaf(f0.y, s.y, fmaf(f0.x, s.x, a))));
-    }
-    return a;
-  }
-};
-template <>
-struct BPack<__nv_fp8_e4m3> {
-  static constexpr int N = 16;
-  __device__ static float dot(const uint4 &q, const float4 *sv) {
-    const __nv_fp8x2_e4m3 *h = reinterpret_cast<const __nv_fp8x2_e4m3 *>(&q);
-    float a = 0.f;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const float4 s = sv[i];
-      const float2 f0 = static_cast<float2>(h[2 * i]), f1 = static_cast<float2>(h[2 * i + 1]);
-      a = fmaf(f1.y, s.w, fmaf(f1.x, s.z, fmaf(f0.y, s.y, fmaf(f0.x, s.x, a))));
-    }
-    return a;
-  }
-};
 
 // Sub-apertures [first, first + count) by the CTA's teams of ``team``
 // threads: team t takes first + t + j * nteams, all in one batch.
@@ -171,14 +127,14 @@ __device__ __forceinline__ void sensor_item(const ShKernelArgs &P, int first, in
 template <typename T>
 __device__ __forceinline__ void mvm_item(const BatchInst &I, int ii, int r0, int R, const BatchArgs &A,
                                          uint64_t *bars, float *pre, unsigned char *area, uint32_t parity) {
-  constexpr int V = BPack<T>::N;
+  constexpr int V = RowPack<T>::N;
   constexpr int Q = V / 4;
   const int tid = threadIdx.x, nt = blockDim.x;
   const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
   const uint32_t row_bytes = (uint32_t)(I.ld * sizeof(T));
   unsigned char *rows = area;
   float *s_sl = reinterpret_cast<float *>(area + (size_t)R * row_bytes);
-  const int nsl = batch_slope_floats(I.ld, V);
+  const int nsl = swizzled_slope_floats(I.ld, V);
   float *part = s_sl + nsl;
   const int RM = A.rows_max;
   if (tid == 0) {
@@ -255,7 +211,7 @@ __device__ __forceinline__ void mvm_item(const BatchInst &I, int ii, int r0, int
           for (int u = 0; u < BATCH_RB; ++u)
             if (rb + u < R) {
               const uint4 q4 = reinterpret_cast<const uint4 *>(rows + (size_t)(rb + u) * row_bytes)[c];
-              acc[u] += BPack<T>::dot(q4, sv);
+              acc[u] += RowPack<T>::dot(q4, sv);
             }
         }
         int u;
@@ -345,16 +301,22 @@ __global__ void __launch_bounds__(BATCH_THREADS, MINB) batch_step_kernel(BatchAr
     __syncthreads();
     t = s_ticket;
   }
-  // the last CTA out re-arms the queue for the next launch
+  // the last CTA out re-arms the queue for the next launch (all its threads:
+  // one pass over the instances instead of a serial chain of round trips)
+  __shared__ int s_last;
   if (tid == 0) {
     __threadfence();
-    const unsigned old = atomicAdd(&A.ctl[32], 1u);
-    if (old == gridDim.x - 1) {
-      __threadfence();
-      for (int i = 0; i < A.ninst; ++i) {
-        A.done[i] = 0u;
-        if (A.inst[i].noisy) A.frames[i] += 1u;
-      }
+    s_last = atomicAdd(&A.ctl[32], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    for (int i = tid; i < A.ninst; i += blockDim.x) {
+      A.done[i] = 0u;
+      if (__ldg(&A.inst[i].noisy)) A.frames[i] += 1u;
+    }
+    __syncthreads();
+    if (tid == 0) {
       A.ctl[0] = 0u;
       A.ctl[32] = 0u;
       __threadfence();
@@ -511,7 +473,7 @@ void aob_batch::build(bool noise) {
     I.nsensor = (w->nvalid + s - 1) / s;
     // MVM items: about `kb` bytes of rows each
     const size_t row_bytes = (size_t)I.ld * esize;
-    const size_t slope_b = sizeof(float) * batch_slope_floats(I.ld, V);
+    const size_t slope_b = sizeof(float) * swizzled_slope_floats(I.ld, V);
     int r = (int)std::max<size_t>(1, kb / row_bytes);
     r = std::min(r, c->nactu);
     auto mvm_bytes = [&](int rr) { return (size_t)rr * row_bytes + slope_b + sizeof(float) * BATCH_SLOTS * rr; };
@@ -538,7 +500,7 @@ void aob_batch::build(bool noise) {
     const ShSmem L(w->nfft, w->nu, w->nv, w->nphase, w->nrebin * w->nrebin * npix2, npix2, hi[i].smax);
     const int esize = hi[i].prec == AOB_PREC_F32 ? 4 : (hi[i].prec == AOB_PREC_BF16 ? 2 : 1);
     const int V = 16 / esize;
-    const size_t mv = (size_t)RPI[i] * hi[i].ld * esize + sizeof(float) * batch_slope_floats(hi[i].ld, V) +
+    const size_t mv = (size_t)RPI[i] * hi[i].ld * esize + sizeof(float) * swizzled_slope_floats(hi[i].ld, V) +
                       sizeof(float) * BATCH_SLOTS * RPI[i];
     area = std::max(area, std::max(L.team_bytes(BATCH_THREADS / team_threads()), mv));
   }

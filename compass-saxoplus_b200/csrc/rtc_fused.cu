@@ -21,58 +21,13 @@
 #include <algorithm>
 
 #include "aob_objects.hpp"
+#include "mvm_core.cuh"
 #include "sh_core.cuh"
 
 namespace aob {
 
-enum : uint32_t { ERR_GRID_TIMEOUT = 2u };
-constexpr uint32_t GRID_MAX_POLLS = 1u << 24;
 constexpr uint32_t ROW_MAX_POLLS = 1u << 22;
 constexpr int FUSED_THREADS = 512;
-
-// Dot product of one 16-byte chunk of a packed command-matrix row with its
-// slopes sv[0 .. N/4) (contiguous float4s).
-template <typename T>
-struct FPack;
-template <>
-struct FPack<float> {
-  static constexpr int N = 4;
-  __device__ static float dot(const uint4 &q, const float4 *sv) {
-    const float *f = reinterpret_cast<const float *>(&q);
-    const float4 s = sv[0];
-    return fmaf(f[3], s.w, fmaf(f[2], s.z, fmaf(f[1], s.y, f[0] * s.x)));
-  }
-};
-template <>
-struct FPack<__nv_bfloat16> {
-  static constexpr int N = 8;
-  __device__ static float dot(const uint4 &q, const float4 *sv) {
-    const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
-    float a = 0.f;
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const float4 s = sv[i];
-      const float2 f0 = __bfloat1622float2(h[2 * i]), f1 = __bfloat1622float2(h[2 * i + 1]);
-      a = fmaf(f1.y, s.w, fmaf(f1.x, s.z, fmaf(f0.y, s.y, fmaf(f0.x, s.x, a))));
-    }
-    return a;
-  }
-};
-template <>
-struct FPack<__nv_fp8_e4m3> {
-  static constexpr int N = 16;
-  __device__ static float dot(const uint4 &q, const float4 *sv) {
-    const __nv_fp8x2_e4m3 *h = reinterpret_cast<const __nv_fp8x2_e4m3 *>(&q);
-    float a = 0.f;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const float4 s = sv[i];
-      const float2 f0 = static_cast<float2>(h[2 * i]), f1 = static_cast<float2>(h[2 * i + 1]);
-      a = fmaf(f1.y, s.w, fmaf(f1.x, s.z, fmaf(f0.y, s.y, fmaf(f0.x, s.x, a))));
-    }
-    return a;
-  }
-};
 
 struct RtcFusedArgs {
   ShKernelArgs sh;     // sensor; sh.c_slopes is the controller's slope vector
@@ -96,48 +51,13 @@ struct RtcFusedArgs {
   int batch;  // sub-apertures per CTA and round
 };
 
-__host__ __device__ inline int fused_slope_floats(int ld, int v) { return ((ld / v + 31) / 32) * 32 * v; }
 __host__ __device__ inline size_t fused_bars_bytes(int rows) { return 128 * (((size_t)rows * 8 + 127) / 128); }
 __host__ __device__ inline size_t fused_pre_bytes(int rows) { return 128 * (((size_t)rows * 20 + 127) / 128); }
-
-// Grid-wide barrier for a cooperative launch.  ``ctr`` counts arrivals over the
-// whole life of the loop: launch n raises it from n * G to (n + 1) * G, so a
-// CTA's target is the next multiple of G above the value its own arrival saw
-// and nothing has to be reset between launches (every CTA arrives exactly
-// once per launch, also when a wait times out).  The wait is bounded; on
-// expiry ERR_GRID_TIMEOUT is set and false returned.
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ bool grid_barrier(unsigned long long *ctr, uint32_t nblocks, uint32_t *status) {
-  __shared__ int s_ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int ok = 1;
-    __threadfence();
-    const unsigned long long old = atomicAdd(ctr, 1ull);
-    const unsigned long long target = (old / nblocks + 1ull) * nblocks;
-    uint32_t i = 0;
-    while (ld_acquire_u64(ctr) < target) {
-      if (++i >= GRID_MAX_POLLS) {
-        ok = 0;
-        atomicOr(status, (uint32_t)ERR_GRID_TIMEOUT);
-        break;
-      }
-    }
-    __threadfence();
-    s_ok = ok;
-  }
-  __syncthreads();
-  return s_ok != 0;
-}
 
 template <typename T, int NFFT, int PD>
 __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArgs A) {
   extern __shared__ __align__(128) unsigned char sm[];
-  constexpr int V = FPack<T>::N;
+  constexpr int V = RowPack<T>::N;
   constexpr int Q = V / 4;
   const uint32_t row_bytes = (uint32_t)(A.ld * sizeof(T));
   // (32-bit: nrow * gridDim < 2^32 is checked on the host)
@@ -209,7 +129,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
     // slopes into shared memory, 16 bytes per load (L2 only: they were written by
     // other CTAs of this launch); group g of the layout holds slopes
     // [(chunk) * V + 4 q, +4) for chunk = (g & 31) + 32 j, g >> 5 = j * Q + q
-    const int ngrp = fused_slope_floats(A.ld, V) / 4;
+    const int ngrp = swizzled_slope_floats(A.ld, V) / 4;
     for (int g = threadIdx.x; g < ngrp; g += blockDim.x) {
       const int l = g & 31, jq = g >> 5;
       const int j = jq / Q, q = jq - j * Q;
@@ -252,7 +172,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
           for (int u = 0; u < RB; ++u)
             if (rb + u < R) {
               const uint4 q4 = reinterpret_cast<const uint4 *>(rows + (size_t)(rb + u) * row_bytes)[c];
-              acc[u] += FPack<T>::dot(q4, sv);
+              acc[u] += RowPack<T>::dot(q4, sv);
             }
         }
       }
@@ -385,7 +305,7 @@ bool aob_loop::launch_fused(bool noise, cudaStream_t s, bool frame_on_device, bo
   A.rows_per_cta = (c->nactu + grid - 1) / grid;
   // sub-apertures per CTA and round: the CTA's whole share if shared memory allows
   const size_t fixed = fused_bars_bytes(A.rows_per_cta) + fused_pre_bytes(A.rows_per_cta) +
-                       (size_t)A.rows_per_cta * A.ld * esize + sizeof(float) * fused_slope_floats(A.ld, V);
+                       (size_t)A.rows_per_cta * A.ld * esize + sizeof(float) * swizzled_slope_floats(A.ld, V);
   const int npix2 = w->npix * w->npix;
   const int share = (w->nvalid + grid - 1) / grid;
   int batch = fused_batch > 0 ? std::min(fused_batch, share) : share;

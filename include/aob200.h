@@ -282,6 +282,11 @@ int aob_mlp_infer(aob_mlp *m, const float *dev_x, float *dev_y, void *stream);
  * otherwise ls's own MVM runs (LS fallback, counted).  Then call
  * aob_ls_comp_voltage as usual. */
 int aob_mlp_comp_com(aob_mlp *m, aob_ls *ls, float threshold, void *stream);
+/* Control-step path: 0 = one cooperative kernel (all layers, the threshold
+ * test and the LS fallback in one launch; weights streamed into shared memory
+ * at entry) whenever it fits, 1 = the multi-kernel path (GEMV per layer,
+ * select, LS MVM).  The commands are the same bit for bit. */
+int aob_mlp_set_mode(aob_mlp *m, int mode);
 /* Number of LS fallbacks so far (reset != 0: set it back to 0). */
 int aob_mlp_fallbacks(aob_mlp *m, uint32_t *count, int reset);
 /* which: "W1".."W3", "b1".."b3" (FP32 masters, padded), "dW1".."dW3", "db1".."db3", "y". */

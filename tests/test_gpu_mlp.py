@@ -150,3 +150,47 @@ def test_learned_reconstructor_closes_the_loop(M):
     le_fb = run(fresh(), mlp=net, threshold=0.0)
     assert net.fallbacks() == 170
     assert abs(le_fb - le_ls) < 1e-6 * max(le_ls, 1e-6)
+
+
+@pytest.mark.parametrize("prec", ["f32", "bf16", "fp8"])
+@pytest.mark.parametrize("dims", [(2496, 1024, 1024, 1377), (131, 70, 45, 33)])
+def test_fused_control_step_equals_multi_kernel_path(M, prec, dims):
+    """The single-launch control step (all layers, the threshold test, the LS
+    fallback) gives the same commands, errors and fallback count as the
+    GEMV-per-layer path, bit for bit: network path (threshold inf) and LS
+    fallback (threshold 0), over several steps of the integrator."""
+    mlp, torch = M
+    from aob200 import core
+
+    nin, nh1, nh2, nout = dims
+    rng = np.random.default_rng(11)
+    cm = (rng.standard_normal((nout, nin)) / np.sqrt(nin)).astype(np.float32)
+
+    w3 = (rng.standard_normal((nout, nh2)) * 0.05).astype(np.float32)
+
+    def make(mode):
+        net = mlp.MlpReconstructor(nin, nout, nh1, nh2, seed=4)
+        net.init_from_ls(cm, 2.0, 0.5)
+        P = net.get_params()
+        P[2] = (w3, P[2][1] + 0.01)  # a non-zero last layer: the hidden path counts too
+        net.set_params(P)
+        net.set_mode(mode)
+        ls = core.LsController(nin, nout)
+        ls.set_precision(prec)
+        ls.set_cmat(cm)
+        ls.set_gain(0.4)
+        return net, ls
+
+    a_net, a_ls = make(0)
+    b_net, b_ls = make(1)
+    for it, thr in enumerate([np.inf, np.inf, 0.0, np.inf, 0.0]):
+        s = rng.standard_normal(nin).astype(np.float32)
+        a_ls.set_centroids(s)
+        b_ls.set_centroids(s)
+        a_net.comp_com(a_ls, thr)
+        b_net.comp_com(b_ls, thr)
+        for name in ("com", "err"):
+            np.testing.assert_array_equal(np.array(a_ls.buffer(name)), np.array(b_ls.buffer(name)),
+                                          err_msg=f"step {it}: {name}")
+    assert a_net.fallbacks() == b_net.fallbacks() == 2
+    assert a_ls.status() == 0
