@@ -89,6 +89,15 @@ class MlpReconstructor:
     def infer(self, dev_x, dev_y, stream=None):
         call("aob_mlp_infer", self.h, dev_x, dev_y, stream)
 
+    def set_gemm(self, kind=0):
+        """Training GEMMs: 0 the mma.sync kernel, 1 the tcgen05 / TMEM kernel."""
+        call("aob_mlp_set_gemm", self.h, int(kind))
+
+    def gemm_status(self, reset=False) -> int:
+        s = ctypes.c_uint32()
+        call("aob_mlp_gemm_status", self.h, ctypes.addressof(s), 1 if reset else 0)
+        return int(s.value)
+
     def set_mode(self, mode=0):
         """0: one cooperative kernel per control step when it fits, 1: the multi-kernel path."""
         call("aob_mlp_set_mode", self.h, int(mode))

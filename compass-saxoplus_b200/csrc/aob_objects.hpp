@@ -270,6 +270,8 @@ struct aob_mlp {
   aob::DevBuf<uint32_t> use_ls, fallbacks;
   // single-launch control step (comp_com_fused)
   int fused_mode = 0;  // 0: fused kernel when it fits, 1: multi-kernel path
+  int gemm_kind = 1;   // training GEMMs: 0 mma.sync kernel, 1 tcgen05 kernel
+  aob::DevBuf<uint32_t> tc_status;  // bounded waits of the tcgen05 GEMM that expired
   aob::DevBuf<float> partial;
   aob::DevBuf<unsigned long long> gbar;
 

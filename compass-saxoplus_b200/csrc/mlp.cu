@@ -3,7 +3,8 @@
 // in -> out, y = W3 h2 + b3 + Ws x.  With Ws set to the least-squares command
 // matrix and W3 = 0 the untrained network is the LS reconstructor; training
 // learns the non-linear correction on top of it.  Trained on the GPU with
-// the project's own BF16 tensor-core GEMM (mlp_gemm.cuh) and Adam, run in the
+// the project's own BF16 tensor-core GEMMs (tcgen05 / TMEM in mlp_tc.cuh, or
+// mma.sync in mlp_gemm.cuh) and Adam, run in the
 // loop by three batch-1 GEMV kernels, and backed by the least-squares MVM:
 // when the norm of the predicted commands exceeds a threshold the step uses
 // the LS commands instead.  There is no counterpart in the reference.
@@ -18,10 +19,12 @@
 
 #include <algorithm>
 #include <cmath>
+#include <string>
 #include <vector>
 
 #include "aob_objects.hpp"
 #include "mlp_gemm.cuh"
+#include "mlp_tc.cuh"
 #include "mvm_core.cuh"
 
 namespace aob {
@@ -195,11 +198,64 @@ __global__ void mlp_select_kernel(const float *y, int n, float threshold, float 
     }
 }
 
+// 2-D bf16 tensor map for the tcgen05 GEMM: inner (contiguous) extent, outer
+// extent, row stride in elements; box 64 (inner, 128 bytes) x box_outer, 128-byte
+// swizzle, zero fill outside the matrix.
+// (the driver entry point is looked up through the runtime, so the library
+// does not link the driver library itself and still loads on machines without it)
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    AOB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    AOB_REQUIRE(p != nullptr && q == cudaDriverEntryPointSuccess, "mlp gemm: cuTensorMapEncodeTiled not available");
+    fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+static void encode_map(CUtensorMap *m, const void *base, uint64_t inner, uint64_t outer, uint64_t ld, uint32_t box_outer) {
+  cuuint64_t dims[2] = {inner, outer};
+  cuuint64_t strides[1] = {ld * 2};
+  cuuint32_t box[2] = {64u, box_outer};
+  cuuint32_t es[2] = {1u, 1u};
+  const CUresult r = encode_tiled_fn()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides,
+                                       box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                       CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  AOB_REQUIRE(r == CUDA_SUCCESS, "mlp gemm: tensor map encoding failed (" + std::to_string((int)r) + ")");
+}
+
+// kind 0: mma.sync kernel, 1: tcgen05 kernel
 template <bool A_KM, bool B_KN>
-static void gemm(const GemmArgs &P, cudaStream_t s) {
+static void gemm(const GemmArgs &P, cudaStream_t s, int kind, uint32_t *status) {
   AOB_REQUIRE(P.M > 0 && P.N > 0 && P.K > 0, "mlp gemm: empty product");
   AOB_REQUIRE(P.lda % 8 == 0 && P.ldb % 8 == 0 && ((A_KM && B_KN) || P.K % 8 == 0),
               "mlp gemm: contiguous dimensions must be multiples of 8");
+  if (kind == 1) {
+    TcArgs T{P, A_KM ? 1 : 0, B_KN ? 1 : 0, status};
+    CUtensorMap ma, mb;
+    if (A_KM)
+      encode_map(&ma, P.A, (uint64_t)P.M, (uint64_t)P.K, (uint64_t)P.lda, 64u);
+    else
+      encode_map(&ma, P.A, (uint64_t)P.K, (uint64_t)P.M, (uint64_t)P.lda, (uint32_t)TC_BM);
+    if (B_KN)
+      encode_map(&mb, P.B, (uint64_t)P.N, (uint64_t)P.K, (uint64_t)P.ldb, 64u);
+    else
+      encode_map(&mb, P.B, (uint64_t)P.K, (uint64_t)P.N, (uint64_t)P.ldb, (uint32_t)TC_BN);
+    static bool configured = false;
+    if (!configured) {
+      AOB_CUDA(cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_BYTES));
+      configured = true;
+    }
+    dim3 grid((P.N + TC_BN - 1) / TC_BN, (P.M + TC_BM - 1) / TC_BM);
+    tc_gemm_kernel<<<grid, TC_THREADS, TC_SMEM_BYTES, s>>>(ma, mb, T);
+    AOB_LAUNCH_CHECK("tc_gemm_kernel");
+    return;
+  }
   dim3 grid((P.N + MG_BN - 1) / MG_BN, (P.M + MG_BM - 1) / MG_BM);
   mlp_gemm_kernel<A_KM, B_KN><<<grid, MG_THREADS, 0, s>>>(P);
   AOB_LAUNCH_CHECK("mlp_gemm_kernel");
@@ -243,6 +299,7 @@ aob_mlp::aob_mlp(int device_, int nin_, int nh1_, int nh2_, int nout_)
   iy.alloc(pout);
   use_ls.alloc(1);
   fallbacks.alloc(1);
+  tc_status.alloc(1);
 }
 
 static void real_dims(const aob_mlp &m, int l, int &rr, int &cr) {
@@ -318,18 +375,18 @@ void aob_mlp::forward(const float *x, int batch, float *y_out, cudaStream_t s) {
   // h1 = GELU(x W1^T + b1)
   P = GemmArgs{batch, ph1, pin, bf(xb), pin, bf(wb[0]), pin, b[0].p, MG_EPI_GELU, nullptr, z1.p, ph1,
                nullptr, bf(h1b), ph1, 0};
-  gemm<false, false>(P, s);
+  gemm<false, false>(P, s, gemm_kind, tc_status.p);
   // h2 = GELU(h1 W2^T + b2)
   P = GemmArgs{batch, ph2, ph1, bf(h1b), ph1, bf(wb[1]), ph1, b[1].p, MG_EPI_GELU, nullptr, z2.p, ph2,
                nullptr, bf(h2b), ph2, 0};
-  gemm<false, false>(P, s);
+  gemm<false, false>(P, s, gemm_kind, tc_status.p);
   // y = h2 W3^T + b3, then y += x Ws^T (skip path)
   P = GemmArgs{batch, pout, ph2, bf(h2b), ph2, bf(wb[2]), ph2, b[2].p, MG_EPI_NONE, nullptr, nullptr, 0,
                y.p, nullptr, pout, 0};
-  gemm<false, false>(P, s);
+  gemm<false, false>(P, s, gemm_kind, tc_status.p);
   P = GemmArgs{batch, pout, pin, bf(xb), pin, bf(wb[3]), pin, nullptr, MG_EPI_NONE, nullptr, nullptr, 0,
                y.p, nullptr, pout, 1};
-  gemm<false, false>(P, s);
+  gemm<false, false>(P, s, gemm_kind, tc_status.p);
   if (y_out) {
     mlp_output_kernel<<<grid_for((int64_t)batch * nout, device), 256, 0, s>>>(y.p, nout, pout, batch, out_scale,
                                                                               y_out);
@@ -353,27 +410,27 @@ void aob_mlp::backward(const float *target, int batch, float *loss, cudaStream_t
   mlp_colsum_kernel<<<(pout + 255) / 256, 256, 0, s>>>(bf(dy), batch, pout, gb[2].p);
   P = GemmArgs{pout, ph2, batch, bf(dy), pout, bf(h2b), ph2, nullptr, MG_EPI_NONE, nullptr, nullptr, 0,
                gw[2].p, nullptr, ph2, 0};
-  gemm<true, true>(P, s);
+  gemm<true, true>(P, s, gemm_kind, tc_status.p);
   P = GemmArgs{batch, ph2, pout, bf(dy), pout, bf(wb[2]), ph2, nullptr, MG_EPI_DGELU, z2.p, nullptr, ph2,
                nullptr, bf(dz2), ph2, 0};
-  gemm<false, true>(P, s);
+  gemm<false, true>(P, s, gemm_kind, tc_status.p);
   // layer 2
   mlp_colsum_kernel<<<(ph2 + 255) / 256, 256, 0, s>>>(bf(dz2), batch, ph2, gb[1].p);
   P = GemmArgs{ph2, ph1, batch, bf(dz2), ph2, bf(h1b), ph1, nullptr, MG_EPI_NONE, nullptr, nullptr, 0,
                gw[1].p, nullptr, ph1, 0};
-  gemm<true, true>(P, s);
+  gemm<true, true>(P, s, gemm_kind, tc_status.p);
   P = GemmArgs{batch, ph1, ph2, bf(dz2), ph2, bf(wb[1]), ph1, nullptr, MG_EPI_DGELU, z1.p, nullptr, ph1,
                nullptr, bf(dz1), ph1, 0};
-  gemm<false, true>(P, s);
+  gemm<false, true>(P, s, gemm_kind, tc_status.p);
   // layer 1
   mlp_colsum_kernel<<<(ph1 + 255) / 256, 256, 0, s>>>(bf(dz1), batch, ph1, gb[0].p);
   P = GemmArgs{ph1, pin, batch, bf(dz1), ph1, bf(xb), pin, nullptr, MG_EPI_NONE, nullptr, nullptr, 0,
                gw[0].p, nullptr, pin, 0};
-  gemm<true, true>(P, s);
+  gemm<true, true>(P, s, gemm_kind, tc_status.p);
   // skip path: dWs = dy^T x
   P = GemmArgs{pout, pin, batch, bf(dy), pout, bf(xb), pin, nullptr, MG_EPI_NONE, nullptr, nullptr, 0,
                gw[3].p, nullptr, pin, 0};
-  gemm<true, true>(P, s);
+  gemm<true, true>(P, s, gemm_kind, tc_status.p);
   AOB_LAUNCH_CHECK("mlp_colsum_kernel");
 }
 
@@ -861,6 +918,20 @@ int aob_mlp_comp_com(aob_mlp *m, aob_ls *ls, float threshold, void *stream) {
                                        m->use_ls.p, m->fallbacks.p);
   AOB_LAUNCH_CHECK("mlp_select_kernel");
   ls->comp_com(s, nullptr, m->use_ls.p);
+  MLP_END
+}
+int aob_mlp_set_gemm(aob_mlp *m, int kind) {
+  MLP_TRY MLP_NEED(m);
+  if (kind < 0 || kind > 1) throw aob::Error("mlp.set_gemm: kind must be 0 or 1");
+  m->gemm_kind = kind;
+  MLP_END
+}
+int aob_mlp_gemm_status(aob_mlp *m, uint32_t *status, int reset) {
+  MLP_TRY MLP_NEED(m);
+  MLP_NEED(status);
+  AOB_CUDA(cudaSetDevice(m->device));
+  AOB_CUDA(cudaMemcpy(status, m->tc_status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (reset) AOB_CUDA(cudaMemset(m->tc_status.p, 0, sizeof(uint32_t)));
   MLP_END
 }
 int aob_mlp_set_mode(aob_mlp *m, int mode) {

@@ -287,6 +287,11 @@ int aob_mlp_comp_com(aob_mlp *m, aob_ls *ls, float threshold, void *stream);
  * at entry) whenever it fits, 1 = the multi-kernel path (GEMV per layer,
  * select, LS MVM).  The commands are the same bit for bit. */
 int aob_mlp_set_mode(aob_mlp *m, int mode);
+/* Training GEMMs: 0 = mma.sync kernel (128 x 128 x 32 tiles), 1 = tcgen05
+ * kernel (TMA tensor loads, 128 x 128 FP32 accumulator in TMEM; the default). */
+int aob_mlp_set_gemm(aob_mlp *m, int kind);
+/* Error word of the tcgen05 GEMM's bounded waits (bit 3: a wait expired). */
+int aob_mlp_gemm_status(aob_mlp *m, uint32_t *status, int reset);
 /* Number of LS fallbacks so far (reset != 0: set it back to 0). */
 int aob_mlp_fallbacks(aob_mlp *m, uint32_t *count, int reset);
 /* which: "W1".."W3", "b1".."b3" (FP32 masters, padded), "dW1".."dW3", "db1".."db3", "y". */

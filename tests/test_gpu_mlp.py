@@ -32,11 +32,16 @@ def _dev(torch, a):
     return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
 
 
-@pytest.mark.parametrize("dims,batch", [((40, 32, 24, 20), 16), ((2496, 1024, 1024, 1377), 64), ((131, 70, 45, 33), 37)])
-def test_forward_and_gradients_match_oracle(M, dims, batch):
+@pytest.mark.parametrize("gemm", [0, 1])
+@pytest.mark.parametrize("dims,batch", [((40, 32, 24, 20), 16), ((2496, 1024, 1024, 1377), 64), ((131, 70, 45, 33), 37),
+                                        ((200, 256, 136, 72), 300)])
+def test_forward_and_gradients_match_oracle(M, dims, batch, gemm):
+    """Both GEMM kernels (0: mma.sync, 1: tcgen05 with TMA tensor loads and a
+    TMEM accumulator) against the oracle, every operand layout and epilogue."""
     mlp, torch = M
     nin, nh1, nh2, nout = dims
     net = mlp.MlpReconstructor(nin, nout, nh1, nh2, seed=3)
+    net.set_gemm(gemm)
     rng = np.random.default_rng(4)
     params = [(w, rng.standard_normal(w.shape[0]).astype(np.float32) * 0.1) for w, _ in net.get_params()[:3]]
     params.append((rng.standard_normal((nout, nin)).astype(np.float32) * 0.05, None))  # skip path
@@ -68,6 +73,7 @@ def test_forward_and_gradients_match_oracle(M, dims, batch):
         else:
             got = got[: real[name]]
         assert rel_rms(got, ref) < 3e-2, name
+    assert net.gemm_status() == 0
 
 
 def test_infer_equals_batched_forward(M):
@@ -88,9 +94,10 @@ def test_infer_equals_batched_forward(M):
         assert rel_rms(y1.cpu().numpy(), dyb[i].cpu().numpy()) < 3e-3
 
 
-def test_training_learns_a_linear_reconstructor(M):
+@pytest.mark.parametrize("gemm", [0, 1])
+def test_training_learns_a_linear_reconstructor(M, gemm):
     """On a noiseless linear map slopes -> commands the loss falls by 20x
-    (bfloat16 storage sets the floor)."""
+    (bfloat16 storage sets the floor), with either GEMM kernel."""
     mlp, torch = M
     rng = np.random.default_rng(7)
     nin, nout, n = 200, 60, 16384
@@ -98,6 +105,7 @@ def test_training_learns_a_linear_reconstructor(M):
     X = rng.standard_normal((n, nin)).astype(np.float32)
     T = X @ R.T
     net = mlp.MlpReconstructor(nin, nout, 256, 256, seed=8)
+    net.set_gemm(gemm)
     hist = net.fit(_dev(torch, X), _dev(torch, T), epochs=40, batch=512, lr=2e-3, lr_decay=0.93)
     assert hist[-1] < hist[0] / 20, hist
 
