@@ -430,7 +430,7 @@ def run_mlp(args, torch):
           {"workload": f"mlp: {nin} -> 1024 -> 1024 -> {nout} + linear skip, BF16 weights, FP32 accumulation",
            "l2": "flushed before every timed inference (256 MB write)"},
           roofline={"bound": "tensor", "achieved": res["train_tflops"], "peak": peak_t, "unit": "TFLOP/s",
-                    "frac": res["train_tflops"] / peak_t, "traffic": None, "kernel": "mlp_gemm_kernel (training step)",
+                    "frac": res["train_tflops"] / peak_t, "traffic": None, "kernel": "tc_gemm_kernel (training step)",
                     **res},
           cpu_baseline=cpu, clocks=clk.summary(), gpu_launches=None)
 

@@ -132,57 +132,65 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
   tc_fence_after();
   const uint32_t tmem = *tslot;
   bool ok = true;
-  if (warp == 0 && lane == 0) {
-    // ---- TMA producer ----
-    for (int kt = 0; kt < nk; ++kt) {
-      const int s = kt % TC_STAGES;
-      const uint32_t round = (uint32_t)(kt / TC_STAGES);
-      if (kt >= TC_STAGES && !mbar_wait(&empty[s], (round - 1u) & 1u, TC_MAX_POLLS)) {
-        ok = false;
-        break;
-      }
-      unsigned char *sa = sm + s * TC_STAGE_BYTES, *sb = sa + TC_TILE_BYTES;
-      mbar_expect_tx(&full[s], (uint32_t)TC_STAGE_BYTES);
-      const int k0 = kt * TC_BK;
-      if (T.a_mn) {
-        tma_load_2d(sa, &mapA, m0, k0, &full[s]);
-        tma_load_2d(sa + TC_TILE_BYTES / 2, &mapA, m0 + 64, k0, &full[s]);
-      } else {
-        tma_load_2d(sa, &mapA, k0, m0, &full[s]);
-      }
-      if (T.b_mn) {
-        tma_load_2d(sb, &mapB, n0, k0, &full[s]);
-        tma_load_2d(sb + TC_TILE_BYTES / 2, &mapB, n0 + 64, k0, &full[s]);
-      } else {
-        tma_load_2d(sb, &mapB, k0, n0, &full[s]);
-      }
+  // the other lanes of the two role warps wait at the warp barrier (not in a
+  // polling loop that would share the warp's issue slots with the role lane)
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---- TMA producer ----
+      for (int kt = 0; kt < nk; ++kt) {
+        const int s = kt % TC_STAGES;
+        const uint32_t round = (uint32_t)(kt / TC_STAGES);
+        if (kt >= TC_STAGES && !mbar_wait(&empty[s], (round - 1u) & 1u, TC_MAX_POLLS)) {
+          ok = false;
+          break;
+        }
+        unsigned char *sa = sm + s * TC_STAGE_BYTES, *sb = sa + TC_TILE_BYTES;
+        mbar_expect_tx(&full[s], (uint32_t)TC_STAGE_BYTES);
+        const int k0 = kt * TC_BK;
+        if (T.a_mn) {
+          tma_load_2d(sa, &mapA, m0, k0, &full[s]);
+          tma_load_2d(sa + TC_TILE_BYTES / 2, &mapA, m0 + 64, k0, &full[s]);
+        } else {
+          tma_load_2d(sa, &mapA, k0, m0, &full[s]);
+        }
+        if (T.b_mn) {
+          tma_load_2d(sb, &mapB, n0, k0, &full[s]);
+          tma_load_2d(sb + TC_TILE_BYTES / 2, &mapB, n0 + 64, k0, &full[s]);
+        } else {
+          tma_load_2d(sb, &mapB, k0, n0, &full[s]);
+        }
     }
-  } else if (warp == 1 && lane == 0) {
-    // ---- MMA issuer ----
-    const uint32_t idesc = umma_idesc_bf16(T.a_mn, T.b_mn);
-    int issued = 0;
-    for (int kt = 0; kt < nk; ++kt) {
-      const int s = kt % TC_STAGES;
-      if (!mbar_wait(&full[s], (uint32_t)(kt / TC_STAGES) & 1u, TC_MAX_POLLS)) {
-        ok = false;
-        break;
-      }
-      tc_fence_after();
-      const uint32_t sa = smem_addr(sm + s * TC_STAGE_BYTES), sb = sa + TC_TILE_BYTES;
-#pragma unroll
-      for (int k = 0; k < TC_BK / 16; ++k) {
-        // K-major: 16 elements = 32 bytes along the swizzled row; MN-major: 16 rows of 128 bytes
-        const uint64_t da = T.a_mn ? umma_desc_sw128(sa + k * 2048, TC_TILE_BYTES / 2, 1024)
-                                   : umma_desc_sw128(sa + k * 32, 16, 1024);
-        const uint64_t db = T.b_mn ? umma_desc_sw128(sb + k * 2048, TC_TILE_BYTES / 2, 1024)
-                                   : umma_desc_sw128(sb + k * 32, 16, 1024);
-        umma_bf16(tmem, da, db, idesc, (kt > 0 || k > 0) ? 1u : 0u);
-      }
-      umma_commit(&empty[s]);
-      ++issued;
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---- MMA issuer ----
+      const uint32_t idesc = umma_idesc_bf16(T.a_mn, T.b_mn);
+      int issued = 0;
+      for (int kt = 0; kt < nk; ++kt) {
+        const int s = kt % TC_STAGES;
+        if (!mbar_wait(&full[s], (uint32_t)(kt / TC_STAGES) & 1u, TC_MAX_POLLS)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_addr(sm + s * TC_STAGE_BYTES), sb = sa + TC_TILE_BYTES;
+  #pragma unroll
+        for (int k = 0; k < TC_BK / 16; ++k) {
+          // K-major: 16 elements = 32 bytes along the swizzled row; MN-major: 16 rows of 128 bytes
+          const uint64_t da = T.a_mn ? umma_desc_sw128(sa + k * 2048, TC_TILE_BYTES / 2, 1024)
+                                     : umma_desc_sw128(sa + k * 32, 16, 1024);
+          const uint64_t db = T.b_mn ? umma_desc_sw128(sb + k * 2048, TC_TILE_BYTES / 2, 1024)
+                                     : umma_desc_sw128(sb + k * 32, 16, 1024);
+          umma_bf16(tmem, da, db, idesc, (kt > 0 || k > 0) ? 1u : 0u);
+        }
+        umma_commit(&empty[s]);
+        ++issued;
     }
     umma_commit(accb);  // arrives once every MMA issued above has completed
     (void)issued;
+    }
+    __syncwarp();
   }
   // ---- epilogue: warp w owns TMEM lanes (tile rows) 32w .. 32w + 31.  Each
   //      32-column chunk goes TMEM -> registers (thread = row) -> shared memory
