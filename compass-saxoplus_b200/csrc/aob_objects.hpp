@@ -3,6 +3,7 @@
 // status codes.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -272,6 +273,8 @@ struct aob_mlp {
   int fused_mode = 0;  // 0: fused kernel when it fits, 1: multi-kernel path
   int gemm_kind = 1;   // training GEMMs: 0 mma.sync kernel, 1 tcgen05 kernel
   aob::DevBuf<uint32_t> tc_status;  // bounded waits of the tcgen05 GEMM that expired
+  aob::DevBuf<float> splitk;        // split-K partial products of the weight gradients
+  aob::DevBuf<float> colsum_part;   // row-chunk partial sums of the bias gradients
   aob::DevBuf<float> partial;
   aob::DevBuf<unsigned long long> gbar;
 
@@ -286,6 +289,7 @@ struct aob_mlp {
   void adam(float lr, cudaStream_t s);
   void infer(const float *x, float *y_out, cudaStream_t s);
   bool comp_com_fused(aob_ls *ls, float threshold, cudaStream_t s);
+  void colsum(const __nv_bfloat16 *d, int batch, int cols, float *out, cudaStream_t s);
 };
 
 namespace aob {

@@ -38,19 +38,14 @@ __global__ void f32_to_bf16_kernel(const float *src, __nv_bfloat16 *dst, int64_t
 
 // x [batch][nin] float -> xb [batch][pin] bf16 of x * scale, zero padding
 __global__ void mlp_input_kernel(const float *x, int nin, int pin, int batch, float scale, __nv_bfloat16 *xb) {
-  const int64_t n = (int64_t)batch * pin;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-    const int b = (int)(t / pin), i = (int)(t - (int64_t)b * pin);
-    xb[t] = __float2bfloat16_rn(i < nin ? x[(int64_t)b * nin + i] * scale : 0.f);
-  }
+  for (int b = blockIdx.x; b < batch; b += gridDim.x)
+    for (int i = threadIdx.x; i < pin; i += blockDim.x)
+      xb[(int64_t)b * pin + i] = __float2bfloat16_rn(i < nin ? x[(int64_t)b * nin + i] * scale : 0.f);
 }
 
 __global__ void mlp_output_kernel(const float *y, int nout, int pout, int batch, float scale, float *out) {
-  const int64_t n = (int64_t)batch * nout;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-    const int b = (int)(t / nout), o = (int)(t - (int64_t)b * nout);
-    out[t] = y[(int64_t)b * pout + o] * scale;
-  }
+  for (int b = blockIdx.x; b < batch; b += gridDim.x)
+    for (int o = threadIdx.x; o < nout; o += blockDim.x) out[(int64_t)b * nout + o] = y[(int64_t)b * pout + o] * scale;
 }
 
 // Mean-squared error on the scaled outputs: d = y - t / out_scale; the loss
@@ -60,14 +55,14 @@ __global__ void mlp_loss_kernel(const float *y, const float *t, int nout, int po
   __shared__ float red[256];
   const float g = 2.f / ((float)batch * (float)nout);
   float acc = 0.f;
-  const int64_t n = (int64_t)batch * pout;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int b = (int)(i / pout), o = (int)(i - (int64_t)b * pout);
-    float d = 0.f;
-    if (o < nout) d = y[i] - t[(int64_t)b * nout + o] * inv_out_scale;
-    dy[i] = __float2bfloat16_rn(g * d);
-    acc += d * d;
-  }
+  for (int b = blockIdx.x; b < batch; b += gridDim.x)
+    for (int o = threadIdx.x; o < pout; o += blockDim.x) {
+      const int64_t i = (int64_t)b * pout + o;
+      float d = 0.f;
+      if (o < nout) d = y[i] - t[(int64_t)b * nout + o] * inv_out_scale;
+      dy[i] = __float2bfloat16_rn(g * d);
+      acc += d * d;
+    }
   red[threadIdx.x] = acc;
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
@@ -86,10 +81,30 @@ __global__ void mlp_loss_final_kernel(const float *part, int nblocks, float deno
 }
 
 // bias gradient: column sums of a [batch][cols] bf16 matrix, batch order
-__global__ void mlp_colsum_kernel(const __nv_bfloat16 *d, int batch, int cols, float *out) {
+// Column sums of d [batch][cols] (bias gradients) in two deterministic passes:
+// partial sums over row chunks (block 32 columns x 8 row lanes, coalesced
+// rows), then the chunks added in order.
+constexpr int COLSUM_CHUNKS = 16;
+__global__ void mlp_colsum_part_kernel(const __nv_bfloat16 *d, int batch, int cols, float *part) {
+  __shared__ float red[8][33];
+  const int c = blockIdx.x * 32 + threadIdx.x;
+  const int rchunk = (batch + gridDim.y - 1) / gridDim.y;
+  const int r0 = blockIdx.y * rchunk, r1 = min(batch, r0 + rchunk);
+  float s = 0.f;
+  if (c < cols)
+    for (int b = r0 + threadIdx.y; b < r1; b += 8) s += __bfloat162float(d[(int64_t)b * cols + c]);
+  red[threadIdx.y][threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.y == 0 && c < cols) {
+    float t = 0.f;
+    for (int y = 0; y < 8; ++y) t += red[y][threadIdx.x];
+    part[(int64_t)blockIdx.y * cols + c] = t;
+  }
+}
+__global__ void mlp_colsum_final_kernel(const float *part, int nchunk, int cols, float *out) {
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
     float s = 0.f;
-    for (int b = 0; b < batch; ++b) s += __bfloat162float(d[(int64_t)b * cols + c]);
+    for (int y = 0; y < nchunk; ++y) s += part[(int64_t)y * cols + c];
     out[c] = s;
   }
 }
@@ -229,33 +244,72 @@ static void encode_map(CUtensorMap *m, const void *base, uint64_t inner, uint64_
   AOB_REQUIRE(r == CUDA_SUCCESS, "mlp gemm: tensor map encoding failed (" + std::to_string((int)r) + ")");
 }
 
-// kind 0: mma.sync kernel, 1: tcgen05 kernel
+// kind 0: mma.sync kernel, 1: tcgen05 kernel.  P2 (tcgen05 only, same M, N
+// and layouts): a second product added in the same accumulator.
 template <bool A_KM, bool B_KN>
-static void gemm(const GemmArgs &P, cudaStream_t s, int kind, uint32_t *status) {
+static void gemm(const GemmArgs &P, cudaStream_t s, int kind, uint32_t *status, const GemmArgs *P2 = nullptr,
+                 aob::DevBuf<float> *work = nullptr) {
   AOB_REQUIRE(P.M > 0 && P.N > 0 && P.K > 0, "mlp gemm: empty product");
   AOB_REQUIRE(P.lda % 8 == 0 && P.ldb % 8 == 0 && ((A_KM && B_KN) || P.K % 8 == 0),
               "mlp gemm: contiguous dimensions must be multiples of 8");
   if (kind == 1) {
-    TcArgs T{P, A_KM ? 1 : 0, B_KN ? 1 : 0, status};
-    CUtensorMap ma, mb;
-    if (A_KM)
-      encode_map(&ma, P.A, (uint64_t)P.M, (uint64_t)P.K, (uint64_t)P.lda, 64u);
-    else
-      encode_map(&ma, P.A, (uint64_t)P.K, (uint64_t)P.M, (uint64_t)P.lda, (uint32_t)TC_BM);
-    if (B_KN)
-      encode_map(&mb, P.B, (uint64_t)P.N, (uint64_t)P.K, (uint64_t)P.ldb, 64u);
-    else
-      encode_map(&mb, P.B, (uint64_t)P.K, (uint64_t)P.N, (uint64_t)P.ldb, (uint32_t)TC_BN);
+    TcArgs T{P, A_KM ? 1 : 0, B_KN ? 1 : 0, status, P2 ? P2->K : 0, 0, nullptr};
+    // split K when the output has too few tiles to fill the GPU (plain float
+    // products only: no bias, no activation, no accumulate, no bf16 copy)
+    const int tiles = ((P.N + TC_BN - 1) / TC_BN) * ((P.M + TC_BM - 1) / TC_BM);
+    int dev = 0;
+    AOB_CUDA(cudaGetDevice(&dev));
+    const int slots = 2 * num_sms(dev);
+    int nsplit = 1;
+    if (work && !P2 && P.epi == MG_EPI_NONE && !P.bias && !P.accumulate && !P.Cb && P.Cf && tiles < slots) {
+      const int nkt = (P.K + TC_BK - 1) / TC_BK;
+      nsplit = std::min((slots + tiles - 1) / tiles, std::max(1, nkt / 8));  // at least 8 stages per slice
+    }
+    if (nsplit > 1) {
+      const int per = (((P.K + TC_BK - 1) / TC_BK) + nsplit - 1) / nsplit;
+      nsplit = (((P.K + TC_BK - 1) / TC_BK) + per - 1) / per;
+      T.kchunk = per * TC_BK;
+      const int64_t need = (int64_t)nsplit * P.M * P.ldc;
+      if (work->n < need) work->alloc(need);
+      T.partial = work->p;
+    }
+    auto maps = [](const GemmArgs &Q, CUtensorMap &ma, CUtensorMap &mb) {
+      if (A_KM)
+        encode_map(&ma, Q.A, (uint64_t)Q.M, (uint64_t)Q.K, (uint64_t)Q.lda, 64u);
+      else
+        encode_map(&ma, Q.A, (uint64_t)Q.K, (uint64_t)Q.M, (uint64_t)Q.lda, (uint32_t)TC_BM);
+      if (B_KN)
+        encode_map(&mb, Q.B, (uint64_t)Q.N, (uint64_t)Q.K, (uint64_t)Q.ldb, 64u);
+      else
+        encode_map(&mb, Q.B, (uint64_t)Q.K, (uint64_t)Q.N, (uint64_t)Q.ldb, (uint32_t)TC_BN);
+    };
+    CUtensorMap ma, mb, ma2, mb2;
+    maps(P, ma, mb);
+    if (P2) {
+      AOB_REQUIRE(P2->M == P.M && P2->N == P.N && P2->K > 0 && P2->lda % 8 == 0 && P2->ldb % 8 == 0,
+                  "mlp gemm: the second product must have the first's shape");
+      maps(*P2, ma2, mb2);
+    } else {
+      ma2 = ma;
+      mb2 = mb;
+    }
     static bool configured = false;
     if (!configured) {
       AOB_CUDA(cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_BYTES));
       configured = true;
     }
-    dim3 grid((P.N + TC_BN - 1) / TC_BN, (P.M + TC_BM - 1) / TC_BM);
-    tc_gemm_kernel<<<grid, TC_THREADS, TC_SMEM_BYTES, s>>>(ma, mb, T);
+    dim3 grid((P.N + TC_BN - 1) / TC_BN, (P.M + TC_BM - 1) / TC_BM, nsplit);
+    tc_gemm_kernel<<<grid, TC_THREADS, TC_SMEM_BYTES, s>>>(ma, mb, ma2, mb2, T);
     AOB_LAUNCH_CHECK("tc_gemm_kernel");
+    if (nsplit > 1) {
+      const int64_t n = (int64_t)P.M * P.ldc;
+      tc_splitk_sum_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, s>>>(T.partial, nsplit, P.M, P.N,
+                                                                                        P.ldc, P.Cf);
+      AOB_LAUNCH_CHECK("tc_splitk_sum_kernel");
+    }
     return;
   }
+  AOB_REQUIRE(P2 == nullptr, "mlp gemm: a second product needs the tcgen05 kernel");
   dim3 grid((P.N + MG_BN - 1) / MG_BN, (P.M + MG_BM - 1) / MG_BM);
   mlp_gemm_kernel<A_KM, B_KN><<<grid, MG_THREADS, 0, s>>>(P);
   AOB_LAUNCH_CHECK("mlp_gemm_kernel");
@@ -369,7 +423,7 @@ static __nv_bfloat16 *bf(aob::DevBuf<uint16_t> &b) { return reinterpret_cast<__n
 void aob_mlp::forward(const float *x, int batch, float *y_out, cudaStream_t s) {
   AOB_CUDA(cudaSetDevice(device));
   ensure_batch(batch);
-  mlp_input_kernel<<<grid_for((int64_t)batch * pin, device), 256, 0, s>>>(x, nin, pin, batch, in_scale, bf(xb));
+  mlp_input_kernel<<<std::min(batch, 8 * num_sms(device)), 256, 0, s>>>(x, nin, pin, batch, in_scale, bf(xb));
   AOB_LAUNCH_CHECK("mlp_input_kernel");
   GemmArgs P{};
   // h1 = GELU(x W1^T + b1)
@@ -383,15 +437,27 @@ void aob_mlp::forward(const float *x, int batch, float *y_out, cudaStream_t s) {
   // y = h2 W3^T + b3, then y += x Ws^T (skip path)
   P = GemmArgs{batch, pout, ph2, bf(h2b), ph2, bf(wb[2]), ph2, b[2].p, MG_EPI_NONE, nullptr, nullptr, 0,
                y.p, nullptr, pout, 0};
-  gemm<false, false>(P, s, gemm_kind, tc_status.p);
-  P = GemmArgs{batch, pout, pin, bf(xb), pin, bf(wb[3]), pin, nullptr, MG_EPI_NONE, nullptr, nullptr, 0,
-               y.p, nullptr, pout, 1};
-  gemm<false, false>(P, s, gemm_kind, tc_status.p);
+  GemmArgs P2{batch, pout, pin, bf(xb), pin, bf(wb[3]), pin, nullptr, MG_EPI_NONE, nullptr, nullptr, 0,
+              y.p, nullptr, pout, 1};
+  if (gemm_kind == 1) {
+    gemm<false, false>(P, s, gemm_kind, tc_status.p, &P2);  // one K loop over [h2 | x]
+  } else {
+    gemm<false, false>(P, s, gemm_kind, tc_status.p);
+    gemm<false, false>(P2, s, gemm_kind, tc_status.p);
+  }
   if (y_out) {
-    mlp_output_kernel<<<grid_for((int64_t)batch * nout, device), 256, 0, s>>>(y.p, nout, pout, batch, out_scale,
+    mlp_output_kernel<<<std::min(batch, 8 * num_sms(device)), 256, 0, s>>>(y.p, nout, pout, batch, out_scale,
                                                                               y_out);
     AOB_LAUNCH_CHECK("mlp_output_kernel");
   }
+}
+
+// bias gradient: column sums of a [batch][cols] bf16 matrix
+void aob_mlp::colsum(const __nv_bfloat16 *d, int batch, int cols, float *out, cudaStream_t s) {
+  if (colsum_part.n < (int64_t)COLSUM_CHUNKS * cols) colsum_part.alloc((int64_t)COLSUM_CHUNKS * cols);
+  mlp_colsum_part_kernel<<<dim3((cols + 31) / 32, COLSUM_CHUNKS), dim3(32, 8), 0, s>>>(d, batch, cols, colsum_part.p);
+  mlp_colsum_final_kernel<<<(cols + 255) / 256, 256, 0, s>>>(colsum_part.p, COLSUM_CHUNKS, cols, out);
+  AOB_LAUNCH_CHECK("mlp_colsum_kernel");
 }
 
 // Gradients of the MSE after forward() on the same batch.
@@ -407,30 +473,30 @@ void aob_mlp::backward(const float *target, int batch, float *loss, cudaStream_t
   }
   GemmArgs P{};
   // layer 3: dW3 = dy^T h2, db3 = sum dy, dz2 = (dy W3) * GELU'(z2)
-  mlp_colsum_kernel<<<(pout + 255) / 256, 256, 0, s>>>(bf(dy), batch, pout, gb[2].p);
+  colsum(bf(dy), batch, pout, gb[2].p, s);
   P = GemmArgs{pout, ph2, batch, bf(dy), pout, bf(h2b), ph2, nullptr, MG_EPI_NONE, nullptr, nullptr, 0,
                gw[2].p, nullptr, ph2, 0};
-  gemm<true, true>(P, s, gemm_kind, tc_status.p);
+  gemm<true, true>(P, s, gemm_kind, tc_status.p, nullptr, &splitk);
   P = GemmArgs{batch, ph2, pout, bf(dy), pout, bf(wb[2]), ph2, nullptr, MG_EPI_DGELU, z2.p, nullptr, ph2,
                nullptr, bf(dz2), ph2, 0};
   gemm<false, true>(P, s, gemm_kind, tc_status.p);
   // layer 2
-  mlp_colsum_kernel<<<(ph2 + 255) / 256, 256, 0, s>>>(bf(dz2), batch, ph2, gb[1].p);
+  colsum(bf(dz2), batch, ph2, gb[1].p, s);
   P = GemmArgs{ph2, ph1, batch, bf(dz2), ph2, bf(h1b), ph1, nullptr, MG_EPI_NONE, nullptr, nullptr, 0,
                gw[1].p, nullptr, ph1, 0};
-  gemm<true, true>(P, s, gemm_kind, tc_status.p);
+  gemm<true, true>(P, s, gemm_kind, tc_status.p, nullptr, &splitk);
   P = GemmArgs{batch, ph1, ph2, bf(dz2), ph2, bf(wb[1]), ph1, nullptr, MG_EPI_DGELU, z1.p, nullptr, ph1,
                nullptr, bf(dz1), ph1, 0};
   gemm<false, true>(P, s, gemm_kind, tc_status.p);
   // layer 1
-  mlp_colsum_kernel<<<(ph1 + 255) / 256, 256, 0, s>>>(bf(dz1), batch, ph1, gb[0].p);
+  colsum(bf(dz1), batch, ph1, gb[0].p, s);
   P = GemmArgs{ph1, pin, batch, bf(dz1), ph1, bf(xb), pin, nullptr, MG_EPI_NONE, nullptr, nullptr, 0,
                gw[0].p, nullptr, pin, 0};
-  gemm<true, true>(P, s, gemm_kind, tc_status.p);
+  gemm<true, true>(P, s, gemm_kind, tc_status.p, nullptr, &splitk);
   // skip path: dWs = dy^T x
   P = GemmArgs{pout, pin, batch, bf(dy), pout, bf(xb), pin, nullptr, MG_EPI_NONE, nullptr, nullptr, 0,
                gw[3].p, nullptr, pin, 0};
-  gemm<true, true>(P, s, gemm_kind, tc_status.p);
+  gemm<true, true>(P, s, gemm_kind, tc_status.p, nullptr, &splitk);
   AOB_LAUNCH_CHECK("mlp_colsum_kernel");
 }
 

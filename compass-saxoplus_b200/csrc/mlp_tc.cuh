@@ -19,6 +19,13 @@
 //  * all 4 warps: the epilogue -- warp w reads TMEM lanes 32w..32w+31 (rows of
 //    the tile) with tcgen05.ld 32x32b, transposes each 32 x 32 chunk through
 //    shared memory and applies bias / GELU / GELU' with coalesced row accesses.
+// Split K (blockIdx.z slices, each writing its plain FP32 product to a
+// workspace that tc_splitk_sum_kernel adds in slice order: deterministic) keeps
+// the SMs busy for the weight-gradient products, whose outputs have few tiles
+// and whose K is the batch.
+// A second operand pair (A2, B2, same layouts, its own K) can follow the first
+// in the same K loop, so y = h2 W3^T + x Ws^T is one GEMM with no read-back of
+// the output.
 // Every mbarrier wait is bounded: on expiry a status bit is set, the kernel
 // still waits (bounded) for its MMAs, frees its TMEM and returns.  No cluster,
 // no multicast.
@@ -42,6 +49,9 @@ struct TcArgs {
   GemmArgs P;
   int a_mn, b_mn;    // 1: the operand's M (N) index is the contiguous one (KM / KN)
   uint32_t *status;  // error word (bounded waits that expired)
+  int K2;            // > 0: a second product A2 B2^T over K2, summed in the same accumulator
+  int kchunk;        // split K: blockIdx.z covers K [z kchunk, (z + 1) kchunk) (0: all of K)
+  float *partial;    // split K: slice z writes its plain product to partial + z * M * ldc
 };
 
 // shared memory bytes of the kernel (stages + barriers + 1024-byte alignment slack)
@@ -103,13 +113,20 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 
 // two CTAs per SM: one CTA's epilogue overlaps the other's main loop
 __global__ void __launch_bounds__(TC_THREADS, 2)
-    tc_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcArgs T) {
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                   const __grid_constant__ CUtensorMap mapA2, const __grid_constant__ CUtensorMap mapB2, TcArgs T) {
   extern __shared__ __align__(1024) unsigned char tc_raw[];
   unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(tc_raw) + 1023) & ~uintptr_t(1023));
   const GemmArgs &P = T.P;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * TC_BN;
-  const int nk = (P.K + TC_BK - 1) / TC_BK;
+  // K range of this CTA: the whole K (plus K2), or one split-K slice
+  int kt0 = 0, nk1 = (P.K + TC_BK - 1) / TC_BK;
+  if (T.kchunk > 0) {
+    kt0 = (int)blockIdx.z * (T.kchunk / TC_BK);
+    nk1 = min(nk1, kt0 + T.kchunk / TC_BK);
+  }
+  const int nk = nk1 - kt0 + (T.K2 > 0 ? (T.K2 + TC_BK - 1) / TC_BK : 0);
   uint64_t *full = reinterpret_cast<uint64_t *>(sm + TC_STAGES * TC_STAGE_BYTES);
   uint64_t *empty = full + TC_STAGES;
   uint64_t *accb = empty + TC_STAGES;
@@ -146,18 +163,20 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
         }
         unsigned char *sa = sm + s * TC_STAGE_BYTES, *sb = sa + TC_TILE_BYTES;
         mbar_expect_tx(&full[s], (uint32_t)TC_STAGE_BYTES);
-        const int k0 = kt * TC_BK;
+        const bool second = kt0 + kt >= nk1;
+        const CUtensorMap *ma = second ? &mapA2 : &mapA, *mb = second ? &mapB2 : &mapB;
+        const int k0 = (second ? kt0 + kt - nk1 : kt0 + kt) * TC_BK;
         if (T.a_mn) {
-          tma_load_2d(sa, &mapA, m0, k0, &full[s]);
-          tma_load_2d(sa + TC_TILE_BYTES / 2, &mapA, m0 + 64, k0, &full[s]);
+          tma_load_2d(sa, ma, m0, k0, &full[s]);
+          tma_load_2d(sa + TC_TILE_BYTES / 2, ma, m0 + 64, k0, &full[s]);
         } else {
-          tma_load_2d(sa, &mapA, k0, m0, &full[s]);
+          tma_load_2d(sa, ma, k0, m0, &full[s]);
         }
         if (T.b_mn) {
-          tma_load_2d(sb, &mapB, n0, k0, &full[s]);
-          tma_load_2d(sb + TC_TILE_BYTES / 2, &mapB, n0 + 64, k0, &full[s]);
+          tma_load_2d(sb, mb, n0, k0, &full[s]);
+          tma_load_2d(sb + TC_TILE_BYTES / 2, mb, n0 + 64, k0, &full[s]);
         } else {
-          tma_load_2d(sb, &mapB, k0, n0, &full[s]);
+          tma_load_2d(sb, mb, k0, n0, &full[s]);
         }
     }
     }
@@ -216,6 +235,10 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
       if (!ok || m >= P.M || n >= P.N) continue;
       float v = stage[i * 33 + n_lane];
       const size_t o = (size_t)m * P.ldc + n;
+      if (T.kchunk > 0) {  // split K: the plain product of this slice (summed later in slice order)
+        T.partial[(size_t)blockIdx.z * P.M * P.ldc + o] = v;
+        continue;
+      }
       if (P.accumulate) v += P.Cf[o];
       if (P.bias) v += bn;
       if (P.epi == MG_EPI_GELU) {
@@ -233,6 +256,18 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
   __syncthreads();
   if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)TC_BN));
   if (!ok && lane == 0 && T.status) atomicOr(T.status, (uint32_t)ERR_TC_TIMEOUT);
+}
+
+// out[m][n] = sum over slices z (in order) of part[z][m][n], n < N (rows of
+// stride ld): the split-K reduction
+__global__ void tc_splitk_sum_kernel(const float *part, int nslice, int M, int N, int ld, float *out) {
+  const int64_t total = (int64_t)M * ld;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    if ((int)(i % ld) >= N) continue;
+    float v = part[i];
+    for (int z = 1; z < nslice; ++z) v += part[(int64_t)z * total + i];
+    out[i] = v;
+  }
 }
 
 }  // namespace aob
