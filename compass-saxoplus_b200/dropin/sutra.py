@@ -1,0 +1,389 @@
+"""Drop-in `sutra` module for COMPASS's shesha: the hot-path classes of the
+reference's pybind11 `sutra` module (python_module/sutra/src/sutra.cpp:62-103)
+with their names, constructor arguments and method names, over libaob200.
+
+Covered (the calls shesha's supervisor makes on the RTC path):
+
+* ``Sensors`` (sensors.cpp:28-107, initgs :159-191) holding Shack-Hartmann
+  (``SHWFS``, wfs_sh.cpp:41-148) and pyramid (``PYRWFS``, wfs_pyrhr.cpp:131-163)
+  sensors: ``load_arrays``, ``comp_image``, ``set_noise``, ``set_pupil``,
+  ``fill_binimage``, ``d_binimg`` / ``d_bincube`` / ``d_intensities`` /
+  ``d_validsubsx`` / ``d_validsubsy`` / ``d_gs.d_phase.d_screen``;
+* ``Rtc_FFF`` (rtc.cpp:100-485): ``add_centroider`` (cog, tcog, wcog, pyr),
+  ``add_controller`` (ls), ``do_centroids``, ``do_control``, ``apply_control``,
+  ``comp_voltage``, ``do_clipping``, ``set_gain``, ``set_modal_gains``,
+  ``imat_svd``, ``build_cmat``, ``set_centroids_ref``, ``do_calibrate_img``,
+  ``d_centro`` / ``d_control``;
+* the centroiders (centroider.cpp:83-352) and the LS controller
+  (controller.cpp, controller_ls.cpp) with their ``d_*`` buffers and setters.
+
+Errors raise ``aob200._lib.AobError`` with the library's message, where the
+reference raises ``RuntimeError`` from its C++ layer.  Everything else of the
+reference (atmosphere, DMs, targets, other sensor / controller families) is not
+part of this path; ``aob200.optics`` / ``aob200.turbulence`` have the layers,
+DMs and targets the closed-loop tests use.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if _PKG not in sys.path:
+    sys.path.insert(0, _PKG)
+
+from aob200 import core as _core  # noqa: E402
+
+
+def _arr(a, n=None):
+    a = np.asarray(a)
+    return a.ravel() if n is None else a.ravel()[:n]
+
+
+# ---------------------------------------------------------------------------
+class _Phase:
+    """``wfs.d_gs.d_phase``: the guide-star phase screen (``d_screen``)."""
+
+    def __init__(self, wfs):
+        self._w = wfs
+
+    @property
+    def d_screen(self):
+        return self._w.d_phase
+
+
+class _GuideStar:
+    def __init__(self, wfs, lambda_um):
+        self.d_phase = _Phase(wfs)
+        self.Lambda = float(lambda_um)
+
+
+class _WfsBase:
+    """Properties shared by the sensor wrappers (wfs.cpp:54-225)."""
+
+    def __init__(self, impl, kind):
+        self._w = impl
+        self.type = kind
+        self.d_gs = None
+
+    nvalid = property(lambda self: self._w.nvalid)
+    npix = property(lambda self: self._w.npix)
+    nfft = property(lambda self: self._w.nfft)
+    ntot = property(lambda self: self._w.ntot)
+    nphase = property(lambda self: self._w.nphase)
+    nrebin = property(lambda self: self._w.nrebin)
+    nxsub = property(lambda self: self._w.nxsub)
+    nphot = property(lambda self: self._w.nphot)
+    noise = property(lambda self: self._w.noise)
+    d_binimg = property(lambda self: self._w.d_binimg)
+    d_validsubsx = property(lambda self: self._w.buffer("validsubsx", np.int32))
+    d_validsubsy = property(lambda self: self._w.buffer("validsubsy", np.int32))
+    d_fluxPerSub = property(lambda self: self._w.buffer("fluxPerSub"))
+
+    def comp_image(self, noise=True):
+        self._w.comp_image(noise=bool(noise))
+
+    def set_noise(self, noise, seed):
+        self._w.set_noise(float(noise), int(seed))
+
+    def set_pupil(self, pupil):
+        self._w.set_pupil(np.asarray(pupil, np.float32))
+
+
+class SHWFS(_WfsBase):
+    """SutraWfsSH (wfs_sh.cpp:41-148)."""
+
+    def __init__(self, nxsub, nvalid, npix, nphase, nrebin, nfft, ntot, npup, pdiam, nphot, nphot4imat, device):
+        super().__init__(_core.ShWfs(nxsub, nvalid, npix, nphase, nrebin, nfft, ntot, npup, pdiam, nphot,
+                                     nphot4imat, device=device), "sh")
+
+    def load_arrays(self, phasemap, hrmap, binmap, offsets, fluxPerSub, validsubsx, validsubsy, istart, jstart,
+                    ttprojmat=None, kernel=None):
+        self._w.load_arrays(phasemap, hrmap, binmap, offsets, fluxPerSub, validsubsx, validsubsy, istart, jstart)
+
+    d_bincube = property(lambda self: self._w.d_bincube)
+    d_intensities = property(lambda self: self._w.d_intensities)
+    d_slopes = property(lambda self: self._w.buffer("slopes"))
+
+    def fill_binimage(self, async_=False):
+        self._w.fill_binimage()
+
+
+class PYRWFS(_WfsBase):
+    """SutraWfs_PyrHR (wfs_pyrhr.cpp:131-163); npup here is the reference's number of
+    modulation points (its constructor's npup)."""
+
+    def __init__(self, nxsub, nvalid, npix, nphase, nrebin, nfft, ntot, npts, pdiam, nphot, nphot4imat, device):
+        super().__init__(_core.PyrWfs(nxsub, nvalid, npix, nphase, nrebin, nfft, ntot, npts, pdiam, nphot, nphot4imat,
+                                      device=device), "pyrhr")
+
+    def load_arrays(self, halfxy, cx, cy, weights, sincar, submask, validsubsx, validsubsy, phasemap=None,
+                    fluxPerSub=None, ttprojmat=None):
+        self._w.load_arrays(halfxy, cx, cy, weights, sincar, submask, validsubsx, validsubsy, phasemap, fluxPerSub)
+
+    def set_pyr_modulation_points(self, cx, cy, weights=None, npts=None):
+        self._w.set_modulation(cx, cy, weights)
+
+
+class Sensors:
+    """SutraSensors (sensors.cpp:28-107): one sensor per entry of ``type``."""
+
+    def __init__(self, context, d_tel, type, nwfs, nxsub, nvalid, npupils, npix, nphase, nrebin, nfft, ntot, npup,
+                 pdiam, nphot, nphot4imat, lgs, fakecam, max_flux_per_pix, max_pix_value, device, roket):
+        self.device = int(device)
+        self._wfs = []
+        for i in range(int(nwfs)):
+            args = (int(_arr(nxsub)[i]), int(_arr(nvalid)[i]), int(_arr(npix)[i]), int(_arr(nphase)[i]),
+                    int(_arr(nrebin)[i]), int(_arr(nfft)[i]), int(_arr(ntot)[i]), int(_arr(npup)[i]),
+                    float(_arr(pdiam)[i]), float(_arr(nphot)[i]), float(_arr(nphot4imat)[i]), self.device)
+            if type[i] == "sh":
+                self._wfs.append(SHWFS(*args))
+            elif type[i] == "pyrhr":
+                self._wfs.append(PYRWFS(*args))
+            else:
+                raise ValueError(f"Sensors: sensor type {type[i]!r} is not supported (sh, pyrhr)")
+
+    @property
+    def d_wfs(self):
+        return self._wfs
+
+    def initgs(self, xpos, ypos, lambda_um, mag, zerop, sizes, noise, seeds, G, thetaML, dx, dy):
+        """Guide stars (sensors.cpp:159-191): wavelength, noise level and noise seed per sensor."""
+        for i, w in enumerate(self._wfs):
+            w._w.set_lambda(float(_arr(lambda_um)[i]))
+            w._w.set_noise(float(_arr(noise)[i]), int(_arr(seeds)[i]))
+            w.d_gs = _GuideStar(w._w, float(_arr(lambda_um)[i]))
+        return 0
+
+
+# ---------------------------------------------------------------------------
+class Centroider:
+    """SutraCentroider{Cog,Tcog,Wcog,Pyr} (centroider.cpp:83-352)."""
+
+    def __init__(self, nvalid, offset, scale, typec, device, wfs=None):
+        self._c = _core.Centroider(int(nvalid), float(offset), float(scale), typec, device=int(device))
+        self.type = typec
+        self.device = int(device)
+        self.wfs = wfs
+        if wfs is not None:
+            self._c.attach(wfs._w)
+
+    nvalid = property(lambda self: self._c.nvalid)
+    nslopes = property(lambda self: 2 * self._c.nvalid)
+    d_centroids_ref = property(lambda self: self._c.buffer("centroids_ref"))
+    d_intensities = property(lambda self: self._c.buffer("intensities"))
+    d_img = property(lambda self: self._c.buffer("img"))
+    d_img_raw = property(lambda self: self._c.buffer("img_raw"))
+    d_validx = property(lambda self: self._c.buffer("validx", np.int32))
+    d_validy = property(lambda self: self._c.buffer("validy", np.int32))
+    d_weights = property(lambda self: self._c.buffer("weights"))
+
+    def load_validpos(self, validx, validy, N):
+        self._c.load_validpos(_arr(validx, int(N)), _arr(validy, int(N)))
+
+    def set_npix(self, npix):
+        self._c.set_npix(int(npix))
+
+    def set_scale(self, scale):
+        self._c.set_scale(float(scale))
+
+    def set_offset(self, offset):
+        self._c.set_offset(float(offset))
+
+    def set_threshold(self, threshold):
+        self._c.set_threshold(float(threshold))
+
+    def set_pyr_method(self, method):
+        """Pyramid slopes (centroider_pyr.cpp): 0 nosin_global, 1 sin_global, 2 nosin_local, 3 sin_local."""
+        self._c.set_pyr_method(int(method))
+
+    def set_pyr_thresh(self, thresh):
+        self._c.set_pyr_thresh(float(thresh))
+
+    def load_weights(self, weights, ndim):
+        self._c.load_weights(np.asarray(weights, np.float32), int(ndim))
+
+    def set_centroids_ref(self, refslopes):
+        self._c.set_centroids_ref(np.asarray(refslopes, np.float32))
+
+    def load_img(self, img, *args):
+        self._c.load_img(np.asarray(img, np.float32))
+
+    def calibrate_img(self):
+        self._c.calibrate_img()
+
+    def set_dark(self, dark, n):
+        self._c.set_dark(np.asarray(dark, np.float32), int(n))
+
+    def set_flat(self, flat, n):
+        self._c.set_flat(np.asarray(flat, np.float32), int(n))
+
+
+class ControllerLS:
+    """SutraControllerLs (controller.cpp, controller_ls.cpp)."""
+
+    def __init__(self, nslope, nactu, delay, device):
+        self._l = _core.LsController(int(nslope), int(nactu), delay=float(delay), device=int(device))
+        self.type = "ls"
+        self.nslope, self.nactu = int(nslope), int(nactu)
+        self.delay = float(delay)
+        self.gain = 0.0
+        self.centro_idx = []
+
+    d_centroids = property(lambda self: self._l.buffer("centroids"))
+    d_com = property(lambda self: self._l.buffer("com"))
+    d_com_clipped = property(lambda self: self._l.buffer("com_clipped"))
+    d_voltage = property(lambda self: self._l.buffer("voltage"))
+    d_err = property(lambda self: self._l.buffer("err"))
+    d_cmat = property(lambda self: self._l.buffer("cmat", shape=(self.nactu, self.nslope)))
+    d_imat = property(lambda self: self._l.buffer("imat", shape=(self.nslope, self.nactu)))
+    d_eigenvals = property(lambda self: self._l.buffer("eigenvals"))
+    d_gain = property(lambda self: self._l.buffer("gain"))
+
+    def set_cmat(self, cmat):
+        self._l.set_cmat(np.asarray(cmat, np.float32))
+
+    def set_imat(self, imat):
+        self._l.set_imat(np.asarray(imat, np.float32))
+
+    def set_gain(self, gain):
+        self.gain = float(gain)
+        self._l.set_gain(float(gain))
+
+    def set_modal_gains(self, mgain):
+        self._l.set_modal_gains(np.asarray(mgain, np.float32))
+
+    def set_delay(self, delay):
+        self.delay = float(delay)
+        self._l.set_delay(float(delay))
+
+    def set_com(self, com, nElem=None):
+        self._l.set_com(np.asarray(com, np.float32))
+
+    def set_comRange(self, comMin, comMax):
+        self._l.set_com_range(float(comMin), float(comMax))
+
+    def set_open_loop(self, open_loop, reset=True):
+        self._l.set_open_loop(bool(open_loop), bool(reset))
+
+    def comp_voltage(self):
+        self._l.comp_voltage()
+
+    def clip_commands(self):
+        self._l.clip()
+
+    def add_perturb_voltage(self, name, perturb, N):
+        self._l.add_perturb(name, np.asarray(perturb, np.float32), int(N))
+
+    def remove_perturb_voltage(self, name):
+        self._l.remove_perturb(name)
+
+    def enable_perturb_voltage(self, name):
+        self._l.enable_perturb(name, True)
+
+    def disable_perturb_voltage(self, name):
+        self._l.enable_perturb(name, False)
+
+    def reset_perturb_voltage(self):
+        self._l.reset_perturb()
+
+
+class Rtc_FFF:
+    """SutraRtc<float, float, float> (rtc.cpp:100-485).  A controller reads the
+    slopes of the centroiders listed in its ``centro_idx`` (all of them, in
+    order, by default), one block of 2 nvalid after the other."""
+
+    def __init__(self):
+        self.d_centro = []
+        self.d_control = []
+
+    def add_centroider(self, context, nvalid, offset, scale, filter_TT, device, typec, wfs=None):
+        if typec not in ("cog", "tcog", "wcog", "pyr"):
+            raise ValueError(f"add_centroider: centroider type {typec!r} is not supported (cog, tcog, wcog, pyr)")
+        self.d_centro.append(Centroider(nvalid, offset, scale, typec, device, wfs))
+        return 0
+
+    def add_controller(self, context, typec, device, delay, nslope, nactu, nslope_buffers=0, nstates=0,
+                       nstate_buffers=0, nmodes=0, niir_in=0, niir_out=0, polc=False, is_modal=False, dms=None,
+                       idx_dms=None, ndm=0, idx_centro=None, ncentro=0, Nphi=0, wfs_direction=False):
+        if typec != "ls":
+            raise ValueError(f"add_controller: controller type {typec!r} is not supported (ls)")
+        c = ControllerLS(nslope, nactu, delay, device)
+        c.centro_idx = ([int(i) for i in _arr(idx_centro)][: int(ncentro)] if idx_centro is not None and ncentro
+                        else list(range(len(self.d_centro))))
+        self.d_control.append(c)
+        return 0
+
+    def remove_controller(self, ncontrol):
+        del self.d_control[int(ncontrol)]
+
+    def remove_centroider(self, ncentro):
+        del self.d_centro[int(ncentro)]
+
+    def _slopes_of(self, ncontrol):
+        c = self.d_control[int(ncontrol)]
+        base = c.d_centroids
+        off = 0
+        for i in c.centro_idx:
+            yield self.d_centro[i], base.ptr + 4 * off
+            off += 2 * self.d_centro[i].nvalid
+
+    def do_calibrate_img(self, ncontrol):
+        for cen, _ in self._slopes_of(ncontrol):
+            if cen.wfs is None:
+                cen.calibrate_img()
+        return 0
+
+    def do_centroids(self, ncontrol):
+        for cen, ptr in self._slopes_of(ncontrol):
+            cen._c.get_cog(ptr)
+        return 0
+
+    def do_control(self, ncontrol):
+        self.d_control[int(ncontrol)]._l.comp_com()
+        return 0
+
+    def comp_voltage(self, ncontrol):
+        self.d_control[int(ncontrol)]._l.comp_voltage()
+        return 0
+
+    def apply_control(self, ncontrol, compVoltage=True):
+        """The voltages of controller ``ncontrol`` (comp_voltage when asked); the DM
+        shapes they drive are computed by the caller's DM objects."""
+        if compVoltage:
+            self.comp_voltage(ncontrol)
+        return 0
+
+    def do_clipping(self, ncontrol):
+        self.d_control[int(ncontrol)]._l.clip()
+        return 0
+
+    def set_gain(self, ncontrol, gain):
+        self.d_control[int(ncontrol)].set_gain(gain)
+        return 0
+
+    def set_modal_gains(self, ncontrol, mgain):
+        self.d_control[int(ncontrol)].set_modal_gains(mgain)
+        return 0
+
+    def imat_svd(self, ncontrol):
+        self.d_control[int(ncontrol)]._l.svdec_imat()
+        return 0
+
+    def build_cmat(self, ncontrol, nfilt, filt_tt=False):
+        if filt_tt:
+            raise ValueError("build_cmat: tip-tilt filtering is not supported")
+        self.d_control[int(ncontrol)]._l.build_cmat(int(nfilt))
+        return 0
+
+    def set_centroids_ref(self, centroidsRef):
+        ref = np.asarray(centroidsRef, np.float32).ravel()
+        off = 0
+        for cen in self.d_centro:
+            n = 2 * cen.nvalid
+            cen.set_centroids_ref(ref[off:off + n])
+            off += n
+        return 0

@@ -1,0 +1,67 @@
+"""The drop-in `carma` / `sutra` modules import without a GPU, carry the class and
+method names shesha calls on the hot path (the reference's pybind11 bindings:
+python_module/sutra/src/sutra.cpp:62-103, rtc.cpp:100-485, wfs_sh.cpp:41-148,
+wfs_pyrhr.cpp:131-163, centroider.cpp:83-352, controller.cpp), and reject
+unsupported sensor / centroider / controller types before any device work."""
+
+import os
+import sys
+
+import pytest
+
+DROPIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "compass-saxoplus_b200", "dropin")
+
+API = {
+    "Sensors": ["initgs", "d_wfs"],
+    "SHWFS": ["load_arrays", "comp_image", "set_noise", "set_pupil", "fill_binimage", "d_binimg", "d_bincube",
+              "d_intensities", "d_validsubsx", "d_validsubsy", "d_fluxPerSub"],
+    "PYRWFS": ["load_arrays", "comp_image", "set_noise", "set_pupil", "set_pyr_modulation_points", "d_binimg"],
+    "Centroider": ["load_validpos", "set_npix", "set_scale", "set_offset", "set_threshold", "load_weights",
+                   "set_centroids_ref", "load_img", "calibrate_img", "set_dark", "set_flat", "set_pyr_method",
+                   "set_pyr_thresh", "d_centroids_ref", "d_intensities", "d_img", "d_img_raw", "d_validx", "d_validy",
+                   "d_weights"],
+    "ControllerLS": ["set_cmat", "set_imat", "set_gain", "set_modal_gains", "set_delay", "set_com", "set_comRange",
+                     "set_open_loop", "comp_voltage", "clip_commands", "add_perturb_voltage",
+                     "remove_perturb_voltage", "enable_perturb_voltage", "disable_perturb_voltage",
+                     "reset_perturb_voltage", "d_centroids", "d_com", "d_com_clipped", "d_voltage", "d_err", "d_cmat",
+                     "d_imat", "d_eigenvals", "d_gain"],
+    "Rtc_FFF": ["add_centroider", "add_controller", "remove_controller", "remove_centroider", "do_calibrate_img",
+                "do_centroids", "do_control", "comp_voltage", "apply_control", "do_clipping", "set_gain",
+                "set_modal_gains", "imat_svd", "build_cmat", "set_centroids_ref"],
+}
+
+
+@pytest.fixture(scope="module")
+def mods():
+    sys.path.insert(0, DROPIN)
+    try:
+        import carma
+        import sutra
+    finally:
+        sys.path.remove(DROPIN)
+    return carma, sutra
+
+
+def test_names(mods):
+    carma, sutra = mods
+    for cls, names in API.items():
+        c = getattr(sutra, cls)
+        missing = [n for n in names if not hasattr(c, n)]
+        assert not missing, f"{cls} lacks {missing}"
+    for n in ("get_instance", "get_instance_1gpu", "get_instance_ngpu", "activate_device"):
+        assert hasattr(carma.context, n)
+
+
+def test_rejects_before_device_work(mods):
+    carma, sutra = mods
+    ctx = carma.context.get_instance()
+    assert ctx.ndevice >= 1
+    rtc = sutra.Rtc_FFF()
+    with pytest.raises(ValueError):
+        rtc.add_centroider(ctx, 10, 0.0, 1.0, False, 0, "bpcog")
+    with pytest.raises(ValueError):
+        rtc.add_controller(ctx, "generic", 0, 0.0, 20, 10)
+    with pytest.raises(ValueError):
+        sutra.Sensors(ctx, None, ["pyrlr"], 1, [8], [52], 1, [6], [8], [3], [16], [24], [64], [8.0], [100.0],
+                      [0.0], [False], False, 0, 0, 0, False)
+    assert rtc.d_centro == [] and rtc.d_control == []
