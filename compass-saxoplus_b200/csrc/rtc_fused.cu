@@ -78,19 +78,28 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
 
   // The last warp, which has the least sensor work in stage 1 (its threads
   // take field samples only when a CTA has more than 13 sub-apertures of
-  // 6 x 6 samples), initialises the row barriers, issues the copies and fetches the
-  // epilogue inputs; the other threads first wait on the barriers after
-  // several __syncthreads.
+  // 6 x 6 samples), initialises the row barrier, issues the copies and fetches the
+  // epilogue inputs; the other threads first wait on the barrier after
+  // several __syncthreads.  The copies go out once the first batch's field
+  // is formed: the sensor's own first loads (tables, pupil windows, phase)
+  // then do not queue behind the matrix stream, which still has the DFT,
+  // binning, noise and centroid stages to land.
   const int helper = (int)blockDim.x - 32;
   if ((int)threadIdx.x == helper) {
     // one barrier for all the rows: a single wait later
     mbar_init(&bars[0], 1);
     fence_mbar_init();
-    const unsigned char *src = static_cast<const unsigned char *>(A.mat) + (size_t)r0 * row_bytes;
-    mbar_expect_tx(&bars[0], (uint32_t)R * row_bytes);
-    for (int r = 0; r < R; ++r)
-      bulk_g2s(rows + (size_t)r * row_bytes, src + (size_t)r * row_bytes, row_bytes, &bars[0]);
   }
+  bool copies_out = false;
+  auto issue_rows = [&]() {
+    if (!copies_out && (int)threadIdx.x == helper) {
+      const unsigned char *src = static_cast<const unsigned char *>(A.mat) + (size_t)r0 * row_bytes;
+      mbar_expect_tx(&bars[0], (uint32_t)R * row_bytes);
+      for (int r = 0; r < R; ++r)
+        bulk_g2s(rows + (size_t)r * row_bytes, src + (size_t)r * row_bytes, row_bytes, &bars[0]);
+    }
+    copies_out = true;
+  };
   // epilogue inputs of this CTA's rows, fetched now so the epilogue makes no
   // global round trip: [scale | modal gain | com | ring[0] | ring[1]]
   const int RP = A.rows_per_cta;
@@ -120,8 +129,10 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
   const int nvalid = A.sh.nvalid;
   for (int base = blockIdx.x; base < nvalid; base += A.batch * gridDim.x) {
     const int Sb = min(A.batch, (nvalid - base + (int)gridDim.x - 1) / (int)gridDim.x);
-    sh_batch<NFFT, PD>(A.sh, base, gridDim.x, Sb, shm, shm + L.hdr, L, Team{(int)threadIdx.x, (int)blockDim.x, 0});
+    sh_batch<NFFT, PD>(A.sh, base, gridDim.x, Sb, shm, shm + L.hdr, L, Team{(int)threadIdx.x, (int)blockDim.x, 0},
+                       issue_rows);
   }
+  issue_rows();  // a CTA without sub-apertures
   // ---- all slopes published ----
   const bool ok = grid_barrier(A.gbar, gridDim.x, A.status);
   if (ok) {

@@ -142,14 +142,20 @@ __device__ __forceinline__ void sh_load_tables(const ShKernelArgs &P, unsigned c
   }
 }
 
+struct NoHook {
+  __device__ void operator()() const {}
+};
+
 // Sub-apertures k = base + s * stride for s < S, processed by team T.  Must
 // be called by every thread of the team (it synchronises the team
 // internally); the caller guarantees base + (S - 1) * stride < nvalid.  On
-// return the team's work area may be reused.
-template <int NFFT, int PD, int TK = TEAM_CTA>
+// return the team's work area may be reused.  ``after_field`` runs on every
+// thread of the team once the field stage is complete (its global loads have
+// returned), before the DFTs.
+template <int NFFT, int PD, int TK = TEAM_CTA, class Hook = NoHook>
 __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int stride, int S,
                                          const unsigned char *tables, unsigned char *work, const ShSmem &L,
-                                         const Team &T) {
+                                         const Team &T, const Hook &after_field = Hook{}) {
   const int tid = TK == TEAM_CTA ? (int)threadIdx.x : T.tid;
   const int nt = TK == TEAM_CTA ? (int)blockDim.x : (TK == TEAM_WARP ? 32 : T.nt);
   const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
@@ -230,6 +236,7 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
     }
   }
   team_sync<TK>(T);
+  after_field();
 
   if constexpr (PD > 0) {
     // Register-blocked DFTs: a thread keeps one input row (column) in registers
