@@ -65,34 +65,58 @@ constexpr uint32_t GRID_MAX_POLLS = 1u << 24;
 // whole life of its owner: launch n raises it from n * G to (n + 1) * G, so a
 // CTA's target is the next multiple of G above the value its own arrival saw
 // and nothing has to be reset between launches (every CTA arrives exactly
-// once per barrier, also when a wait times out).  The wait is bounded; on
-// expiry ERR_GRID_TIMEOUT is set and false returned.
+// once per barrier, also when a wait times out).  One thread per CTA arrives
+// with a release add (it publishes the CTA's writes, ordered before it by the
+// CTA barrier), spins on relaxed loads and closes with one acquire load.  The
+// wait is bounded; on expiry ERR_GRID_TIMEOUT is set and false returned.
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
   unsigned long long v;
   asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ bool grid_barrier(unsigned long long *ctr, uint32_t nblocks, uint32_t *status) {
-  __shared__ int s_ok;
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long atom_add_release_u64(unsigned long long *p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.add.release.gpu.global.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
+// Arrival half: every thread of the CTA calls it; thread 0 gets the target
+// count to wait for (the others 0).  Work placed between grid_arrive and
+// grid_wait overlaps the wait but is not published by the barrier.
+__device__ __forceinline__ unsigned long long grid_arrive(unsigned long long *ctr, uint32_t nblocks) {
   __syncthreads();
+  unsigned long long target = 0;
+  if (threadIdx.x == 0) {
+    const unsigned long long old = atom_add_release_u64(ctr, 1ull);
+    target = (old / nblocks + 1ull) * nblocks;
+  }
+  return target;
+}
+// Waiting half: every thread of the CTA calls it with grid_arrive's result.
+__device__ __forceinline__ bool grid_wait(const unsigned long long *ctr, unsigned long long target, uint32_t *status) {
+  __shared__ int s_ok;
   if (threadIdx.x == 0) {
     int ok = 1;
-    __threadfence();
-    const unsigned long long old = atomicAdd(ctr, 1ull);
-    const unsigned long long target = (old / nblocks + 1ull) * nblocks;
     uint32_t i = 0;
-    while (ld_acquire_u64(ctr) < target) {
+    while (ld_relaxed_u64(ctr) < target) {
       if (++i >= GRID_MAX_POLLS) {
         ok = 0;
         atomicOr(status, (uint32_t)ERR_GRID_TIMEOUT);
         break;
       }
     }
-    __threadfence();
+    (void)ld_acquire_u64(ctr);  // orders this CTA's later reads after the other CTAs' writes
     s_ok = ok;
   }
   __syncthreads();
   return s_ok != 0;
+}
+__device__ __forceinline__ bool grid_barrier(unsigned long long *ctr, uint32_t nblocks, uint32_t *status) {
+  return grid_wait(ctr, grid_arrive(ctr, nblocks), status);
 }
 
 }  // namespace aob

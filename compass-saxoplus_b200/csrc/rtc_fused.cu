@@ -126,42 +126,67 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
   sh_load_tables<NFFT>(A.sh, shm, threadIdx.x, blockDim.x);
   // (the barrier closing sh_batch's stage 1 publishes the tables: stages 0-1
   // read none of them, so their loads overlap the field's)
+  // With the CTA's whole share in one round (the usual case) the cube and
+  // image writes wait until the CTA has arrived at the grid barrier: the slopes
+  // go out first and the barrier's release does not wait on the image stores.
   const int nvalid = A.sh.nvalid;
-  for (int base = blockIdx.x; base < nvalid; base += A.batch * gridDim.x) {
-    const int Sb = min(A.batch, (nvalid - base + (int)gridDim.x - 1) / (int)gridDim.x);
-    sh_batch<NFFT, PD>(A.sh, base, gridDim.x, Sb, shm, shm + L.hdr, L, Team{(int)threadIdx.x, (int)blockDim.x, 0},
-                       issue_rows);
+  const Team team{(int)threadIdx.x, (int)blockDim.x, 0};
+  const bool one_round = A.batch * (int)gridDim.x >= nvalid;
+  const int S1 = (int)blockIdx.x < nvalid ? min(A.batch, (nvalid - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x) : 0;
+  if (one_round) {
+    if (S1 > 0)
+      sh_batch<NFFT, PD, TEAM_CTA, decltype(issue_rows), true>(A.sh, blockIdx.x, gridDim.x, S1, shm, shm + L.hdr, L,
+                                                               team, issue_rows);
+  } else {
+    for (int base = blockIdx.x; base < nvalid; base += A.batch * gridDim.x) {
+      const int Sb = min(A.batch, (nvalid - base + (int)gridDim.x - 1) / (int)gridDim.x);
+      sh_batch<NFFT, PD>(A.sh, base, gridDim.x, Sb, shm, shm + L.hdr, L, team, issue_rows);
+    }
   }
   issue_rows();  // a CTA without sub-apertures
   // ---- all slopes published ----
-  const bool ok = grid_barrier(A.gbar, gridDim.x, A.status);
+  const unsigned long long ticket = grid_arrive(A.gbar, gridDim.x);
+  if (one_round && S1 > 0) sh_store_images(A.sh, blockIdx.x, gridDim.x, S1, shm + L.hdr, L, team);
+  const bool ok = grid_wait(A.gbar, ticket, A.status);
   if (ok) {
     if (A.bump && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.bump, 1u);  // no round trip
     // slopes into shared memory, 16 bytes per load (L2 only: they were written by
     // other CTAs of this launch); group g of the layout holds slopes
     // [(chunk) * V + 4 q, +4) for chunk = (g & 31) + 32 j, g >> 5 = j * Q + q
     const int ngrp = swizzled_slope_floats(A.ld, V) / 4;
-    for (int g = threadIdx.x; g < ngrp; g += blockDim.x) {
-      const int l = g & 31, jq = g >> 5;
-      const int j = jq / Q, q = jq - j * Q;
-      const int src = (l + 32 * j) * V + 4 * q;
-      float4 v4;
-      if (src + 3 < A.ncol) {
-        v4 = __ldcg(reinterpret_cast<const float4 *>(A.sh.c_slopes + src));
-      } else {
-        v4.x = src < A.ncol ? __ldcg(A.sh.c_slopes + src) : 0.f;
-        v4.y = src + 1 < A.ncol ? __ldcg(A.sh.c_slopes + src + 1) : 0.f;
-        v4.z = src + 2 < A.ncol ? __ldcg(A.sh.c_slopes + src + 2) : 0.f;
-        v4.w = 0.f;
+    constexpr int SU = 2;  // groups per thread and pass: both loads go out before either store
+    for (int g0 = threadIdx.x; g0 < ngrp; g0 += SU * blockDim.x) {
+      float4 v4[SU];
+#pragma unroll
+      for (int u = 0; u < SU; ++u) {
+        const int g = g0 + u * (int)blockDim.x;
+        const int l = g & 31, jq = g >> 5;
+        const int j = jq / Q, q = jq - j * Q;
+        const int src = (l + 32 * j) * V + 4 * q;
+        if (g >= ngrp) {
+          v4[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+        } else if (src + 3 < A.ncol) {
+          v4[u] = __ldcg(reinterpret_cast<const float4 *>(A.sh.c_slopes + src));
+        } else {
+          v4[u].x = src < A.ncol ? __ldcg(A.sh.c_slopes + src) : 0.f;
+          v4[u].y = src + 1 < A.ncol ? __ldcg(A.sh.c_slopes + src + 1) : 0.f;
+          v4[u].z = src + 2 < A.ncol ? __ldcg(A.sh.c_slopes + src + 2) : 0.f;
+          v4[u].w = 0.f;
+        }
       }
-      reinterpret_cast<float4 *>(s_sh)[g] = v4;
+#pragma unroll
+      for (int u = 0; u < SU; ++u) {
+        const int g = g0 + u * (int)blockDim.x;
+        if (g < ngrp) reinterpret_cast<float4 *>(s_sh)[g] = v4[u];
+      }
     }
     __syncthreads();
     // Split-K over the CTA's rows: warp w, lane l take chunks c = l + 32 (w + NW i);
-    // each slope chunk is read once and applied to every row from registers,
-    // then the per-warp partial sums are added in warp order (deterministic).
+    // each slope chunk is read once and applied to every row from registers
+    // (up to RB rows in one pass), then the per-warp partial sums are added in
+    // warp order (deterministic).
     constexpr int NW = FUSED_THREADS / 32;
-    constexpr int RB = 8;  // rows per register block
+    constexpr int RB = 16;  // rows per register block: two transposed butterflies of 8
     const int nchunk = A.ld / V;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     bool rows_ok = true;
@@ -187,9 +212,16 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
             }
         }
       }
-      int u;
-      const float t = warp_sum8(acc, lane, u);
-      if ((lane & 3) == 0 && rb + u < R) part[warp * A.rows_per_cta + rb + u] = t;
+#pragma unroll
+      for (int h = 0; h < RB / 8; ++h) {
+        if (rb + 8 * h >= R) break;
+        float a8[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) a8[u] = acc[8 * h + u];
+        int u;
+        const float t = warp_sum8(a8, lane, u);
+        if ((lane & 3) == 0 && rb + 8 * h + u < R) part[warp * A.rows_per_cta + rb + 8 * h + u] = t;
+      }
     }
     __syncthreads();
     // integrator and voltage per row, one thread per row

@@ -11,8 +11,11 @@
 //   3. DFT along y at the nv frequencies binmap reads, |.|^2
 //   4. binning through the compact binmap, the flux per sub-aperture (one
 //      warp per sub-aperture, fixed summation order) and normalisation
-//   5. Philox photon / readout noise, cube + image writes, centroid weights
-//   6. CoG-family centroid per sub-aperture (one warp each, fixed order)
+//   5. Philox photon / readout noise, centroid weights
+//   6. CoG-family centroid per sub-aperture (one warp each, fixed order),
+//      then that sub-aperture's cube block and image window, coalesced
+//      (or, for a caller that wants the slopes out first, later through
+//      sh_store_images)
 // so a team pays each stage's latency once for the batch instead of once per
 // sub-aperture; small teams (one warp) meet only at warp barriers and run
 // independently of the CTA's other teams.  The reductions run in an order
@@ -146,13 +149,57 @@ struct NoHook {
   __device__ void operator()() const {}
 };
 
+// Where sh_batch keeps the batch's metadata in its work area.
+struct ShMeta {
+  int32_t *vx, *vy;
+  float *fl, *tot, *rx, *ry;
+  int *n_listed;  // pixels listed for inversion / PTRS in stage 4
+  __device__ ShMeta(unsigned char *work, const ShSmem &L, int S) {
+    vx = reinterpret_cast<int32_t *>(work + L.meta) + 2 * S;
+    vy = vx + S;
+    fl = reinterpret_cast<float *>(vy + S);
+    tot = fl + S;
+    rx = tot + S;
+    ry = rx + S;
+    n_listed = reinterpret_cast<int *>(ry + S);
+  }
+};
+
+// One warp writes sub-aperture k's pixels bs[0 .. npix^2): its block of the
+// cube (contiguous) and its npix x npix window of the binned image.
+__device__ __forceinline__ void sh_store_subap(const ShKernelArgs &P, int k, const float *bs, int vx, int vy,
+                                               int lane) {
+  const int npix = P.npix, npix2 = npix * npix;
+  for (int p = lane; p < npix2; p += 32) {
+    const float v = bs[p];
+    P.bincube[p + k * npix2] = v;
+    const int y = udiv(p, P.mg_np), x = p - y * npix;
+    P.binimg[(x + vx) + (y + vy) * P.img_size] = v;
+  }
+}
+
+// The image writes of a batch that sh_batch<..., DEFER_IMG = true> left in
+// its work area (same team, same arguments); the work area must be intact.
+template <int TK = TEAM_CTA>
+__device__ __forceinline__ void sh_store_images(const ShKernelArgs &P, int base, int stride, int S,
+                                                unsigned char *work, const ShSmem &L, const Team &T) {
+  const int tid = TK == TEAM_CTA ? (int)threadIdx.x : T.tid;
+  const int nt = TK == TEAM_CTA ? (int)blockDim.x : (TK == TEAM_WARP ? 32 : T.nt);
+  const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  const ShMeta M(work, L, S);
+  const float *bins = reinterpret_cast<const float *>(work + L.bins);
+  const int npix2 = P.npix * P.npix;
+  for (int s = warp; s < S; s += nw) sh_store_subap(P, base + s * stride, bins + s * npix2, M.vx[s], M.vy[s], lane);
+}
+
 // Sub-apertures k = base + s * stride for s < S, processed by team T.  Must
 // be called by every thread of the team (it synchronises the team
 // internally); the caller guarantees base + (S - 1) * stride < nvalid.  On
 // return the team's work area may be reused.  ``after_field`` runs on every
 // thread of the team once the field stage is complete (its global loads have
-// returned), before the DFTs.
-template <int NFFT, int PD, int TK = TEAM_CTA, class Hook = NoHook>
+// returned), before the DFTs.  With DEFER_IMG the cube and image writes are
+// left to sh_store_images (the noisy pixels stay in the work area).
+template <int NFFT, int PD, int TK = TEAM_CTA, class Hook = NoHook, bool DEFER_IMG = false>
 __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int stride, int S,
                                          const unsigned char *tables, unsigned char *work, const ShSmem &L,
                                          const Team &T, const Hook &after_field = Hook{}) {
@@ -169,13 +216,10 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
   const int pd = PD > 0 ? PD : P.pdiam;
   const int pd2 = pd * pd, nupd = nu * pd, nunv = nu * nv;
 
-  int32_t *m_vx = reinterpret_cast<int32_t *>(work + L.meta) + 2 * S;
-  int32_t *m_vy = m_vx + S;
-  float *m_fl = reinterpret_cast<float *>(m_vy + S);
-  float *m_tot = m_fl + S;
-  float *m_rx = m_tot + S;
-  float *m_ry = m_rx + S;
-  int *n_listed = reinterpret_cast<int *>(m_ry + S);  // pixels listed for inversion / PTRS in stage 4
+  const ShMeta M(work, L, S);
+  int32_t *m_vx = M.vx, *m_vy = M.vy;
+  float *m_fl = M.fl, *m_tot = M.tot, *m_rx = M.rx, *m_ry = M.ry;
+  int *n_listed = M.n_listed;
   float2 *E = reinterpret_cast<float2 *>(work + L.E);
   float2 *Gt = reinterpret_cast<float2 *>(work + L.Gt);
   float *I = reinterpret_cast<float *>(work + L.I);
@@ -390,7 +434,7 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
   }
   team_sync<TK>(T);
 
-  // ---- 5. noise, cube + image, centroid weights ----
+  // ---- 5. noise (the noisy pixel replaces its mean in bins), centroid weights ----
   for (int t = tid; t < nP; t += nt) {
     const int i = P.noise_mode >= 1 ? order[t] : t;
     const int s = udiv(i, P.mg_np2), p = i - s * npix2;
@@ -404,18 +448,16 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
       v = v < AOB_POISSON_INV_MAX_MEAN ? poisson_inversion(v, w0, rk) : poisson_ptrs(v, w0, pix, frame, P.k0, P.k1);
       if (P.noise_mode >= 2) v = v + P.noise * gauss_sample(w0);
     }
-    P.bincube[pix] = v;
-    const int y = udiv(p, P.mg_np), x = p - y * npix;
-    P.binimg[(x + m_vx[s]) + (y + m_vy[s]) * P.img_size] = v;
+    bins[i] = v;
     float d = v;
     if (P.ckind == 1 || P.ckind == 2) d = (v > P.c_thresh) ? v - P.c_thresh : 1.e-6f;
     dw[i] = d * wgt;
   }
   team_sync<TK>(T);
 
-  // ---- 6. centroids ----
-  if (P.ckind >= 0) {
-    for (int s = warp; s < S; s += nw) {
+  // ---- 6. centroids, then the sub-aperture's cube block and image window ----
+  for (int s = warp; s < S; s += nw) {
+    if (P.ckind >= 0) {
       float cs = 0.f, cx = 0.f, cy = 0.f;
       for (int p = lane; p < npix2; p += 32) {
         const float d = dw[s * npix2 + p];
@@ -436,6 +478,7 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
         P.c_intens[k] = cs;
       }
     }
+    if constexpr (!DEFER_IMG) sh_store_subap(P, base + s * stride, bins + s * npix2, m_vx[s], m_vy[s], lane);
   }
   team_sync<TK>(T);
 }
