@@ -580,7 +580,7 @@ def main():
         e2e_ms = float(t.item())
     e2e = {"value": ws * e2e_steps / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": nbytes_phase,
            "d2h_bytes_per_step": setup.nactu * 4, "wall_clock_value": e2e_steps / wall,
-           "call": "aob_loop_step(host phase -> host voltages)"}
+           "call": "aob_loop_step(host phase -> host voltages): phase by copy engine, voltages written into the pinned buffer by the fused kernel"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

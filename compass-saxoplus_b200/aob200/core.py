@@ -510,6 +510,11 @@ class Loop:
         kernel (0 = a CTA's whole share at once); results are unchanged."""
         call("aob_loop_set_mode", self.h, int(mode), int(fused_batch))
 
+    def set_host_io(self, mode=1):
+        """1: a pinned host voltage buffer of ``step`` is written by the fused
+        kernel itself; 0: copy-engine transfer.  Results are identical."""
+        call("aob_loop_set_host_io", self.h, int(mode))
+
     def kernels_per_step(self) -> int:
         n = ctypes.c_int()
         call("aob_loop_kernels_per_step", self.h, ctypes.addressof(n))

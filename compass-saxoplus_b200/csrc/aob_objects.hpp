@@ -193,12 +193,15 @@ struct aob_loop {
   std::vector<cudaGraphExec_t> graphs;   // one per command-ring rotation
   std::vector<uint64_t> graph_key;       // parameter snapshot each graph was built for
   std::vector<const void *> graph_front; // ring front buffer each graph was built for
+  std::vector<int> graph_kernels;        // kernels each graph launches
   uint64_t frame_mirror = ~0ull;         // value held by d_frame
   aob::DevBuf<unsigned long long> gbar;  // grid-barrier arrival counter of the fused kernel
   int mode = 0;                          // 0 auto (fused when it fits), 1 three kernels, 2 fused only
   int fused_batch = 0;                   // max sub-apertures per CTA and round in the fused kernel (0 = all)
   int last_kernels = 3;                  // kernels launched by the last device step
   uint32_t frame_host = 0;
+  int host_io = 1;                       // 1: the fused kernel writes pinned host voltages itself
+  float *io_volt = nullptr;              // device view of the caller's pinned voltages during a step
   aob_loop(aob_sh *w, aob_centro *c, aob_ls *l);
   ~aob_loop();
   void device_step(bool noise, cudaStream_t s, bool frame_on_device);

@@ -40,6 +40,7 @@ void aob_loop::drop_graphs() {
   graphs.clear();
   graph_key.clear();
   graph_front.clear();
+  graph_kernels.clear();
 }
 
 // Everything a captured graph bakes into its kernel parameters.
@@ -65,6 +66,7 @@ uint64_t aob_loop::key(bool noise) const {
   mix(&wfs->batch_override, sizeof wfs->batch_override);
   mix(&mode, sizeof mode);
   mix(&fused_batch, sizeof fused_batch);
+  mix(&io_volt, sizeof io_volt);
   const void *pm[4] = {ls->cm_f32.p, ls->cm_bf16.p, ls->cm_fp8.p, centro->weights.p};
   mix(pm, sizeof pm);
   return h;
@@ -89,8 +91,28 @@ void aob_loop::device_step(bool noise, cudaStream_t s, bool frame_on_device) {
   ls->comp_voltage(s);
 }
 
+// Device view of pinned, mapped host memory (nullptr for pageable memory).
+static const void *mapped_view(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
+
 void aob_loop::step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s) {
   AOB_CUDA(cudaSetDevice(wfs->device));
+  // Direct voltages: with the caller's voltage buffer pinned and mapped, the
+  // fused kernel's epilogue writes it as well (posted stores over the bus), so
+  // no copy-engine transfer follows the kernel.
+  io_volt = (host_io == 1 && host_voltage && mode != 1)
+                ? static_cast<float *>(const_cast<void *>(mapped_view(host_voltage)))
+                : nullptr;
+  struct Reset {
+    float *&p;
+    ~Reset() { p = nullptr; }
+  } reset_io{io_volt};
   if (host_phase)
     AOB_CUDA(cudaMemcpyAsync(wfs->phase.p, host_phase, wfs->phase.bytes(), cudaMemcpyHostToDevice, s));
   bool perturbed = false;
@@ -109,6 +131,7 @@ void aob_loop::step(const float *host_phase, float *host_voltage, bool noise, cu
       graphs.push_back(nullptr);
       graph_key.push_back(0);
       graph_front.push_back(front);
+      graph_kernels.push_back(0);
       slot = (int)graphs.size() - 1;
     }
     const uint64_t k = key(noise);
@@ -155,8 +178,10 @@ void aob_loop::step(const float *host_phase, float *host_voltage, bool noise, cu
       AOB_CUDA(e);
       graphs[slot] = ge;
       graph_key[slot] = k;
+      graph_kernels[slot] = last_kernels;  // set by the captured device step
     }
     AOB_CUDA(cudaGraphLaunch(graphs[slot], s));
+    last_kernels = graph_kernels[slot];
     // host-side state the graph's kernels correspond to
     if (noise && wfs->noise > -1.f) {
       ++wfs->frame;
@@ -170,7 +195,8 @@ void aob_loop::step(const float *host_phase, float *host_voltage, bool noise, cu
     ++wfs->image_gen;
   }
   if (host_voltage) {
-    AOB_CUDA(cudaMemcpyAsync(host_voltage, ls->com_clipped.p, ls->com_clipped.bytes(), cudaMemcpyDeviceToHost, s));
+    if (!(io_volt && last_kernels == 1))
+      AOB_CUDA(cudaMemcpyAsync(host_voltage, ls->com_clipped.p, ls->com_clipped.bytes(), cudaMemcpyDeviceToHost, s));
     AOB_CUDA(cudaStreamSynchronize(s));
   }
 }
@@ -195,6 +221,18 @@ int aob_loop_destroy(aob_loop *l) {
     delete l;
   }
   return AOB_OK;
+}
+
+int aob_loop_set_host_io(aob_loop *l, int mode) {
+  try {
+    if (!l) throw Error("aob_loop_set_host_io: null handle");
+    AOB_REQUIRE(mode == 0 || mode == 1, "aob_loop_set_host_io: mode must be 0 (copies) or 1 (direct when pinned)");
+    l->host_io = mode;
+    return AOB_OK;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return AOB_ERR;
+  }
 }
 
 int aob_loop_step(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream) {

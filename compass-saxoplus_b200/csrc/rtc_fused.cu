@@ -49,6 +49,7 @@ struct RtcFusedArgs {
   unsigned long long *gbar;  // grid-barrier arrival counter (never reset)
   int rows_per_cta;
   int batch;  // sub-apertures per CTA and round
+  float *volt_host;  // caller's pinned host voltages (mapped), also written, or null
 };
 
 __host__ __device__ inline size_t fused_bars_bytes(int rows) { return 128 * (((size_t)rows * 8 + 127) / 128); }
@@ -244,6 +245,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
       }
       if (A.do_clip) v = fminf(fmaxf(v, A.vmin), A.vmax);
       A.volt[gr] = v;
+      if (A.volt_host) A.volt_host[gr] = v;
     }
   }
   // no CTA may exit with a copy still landing in its shared memory
@@ -342,6 +344,7 @@ bool aob_loop::launch_fused(bool noise, cudaStream_t s, bool frame_on_device, bo
   A.bump = (frame_on_device && noisy) ? d_frame.p : nullptr;
   A.status = c->status.p;
   A.gbar = gbar.p;
+  A.volt_host = io_volt;
   const int nsm = num_sms(w->device);
   const int grid = std::min(nsm, c->nactu);
   AOB_REQUIRE((int64_t)c->nactu * grid < (int64_t)1 << 32, "loop: too many actuators for the fused kernel");

@@ -417,6 +417,13 @@ int aob_loop_kernels_per_step(aob_loop *l, int *n);
  * if it does not fit); fused_batch = at most this many sub-apertures per CTA
  * and round in the fused kernel (0 = a CTA's whole share in one round). */
 int aob_loop_set_mode(aob_loop *l, int mode, int fused_batch);
+/* Voltage output of aob_loop_step: mode 1 (default) = when host_voltage is
+ * pinned, mapped host memory and the fused kernel runs, its epilogue writes
+ * the voltages there directly (no copy-engine transfer after the kernel);
+ * mode 0 = always a device-to-host copy.  Results are identical.  No
+ * counterpart in the reference, whose controller keeps its voltages in device
+ * memory (d_voltage) for the DMs. */
+int aob_loop_set_host_io(aob_loop *l, int mode);
 
 /* ---- batched Monte Carlo: many loops, one persistent launch per step --- *
  * No counterpart in the reference, where each simulation is its own process

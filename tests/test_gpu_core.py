@@ -242,6 +242,59 @@ def test_loop_matches_separate_calls(core, graph, delay, mode, fused_batch):
     assert loop.kernels_per_step() == (1 if mode == 2 else 3)
 
 
+@pytest.mark.parametrize("graph", [False, True])
+@pytest.mark.parametrize("delay", [0.0, 1.4])
+def test_direct_host_io_equals_copies(core, graph, delay):
+    """With a pinned host voltage buffer the fused kernel's epilogue writes the
+    voltages to host memory itself (set_host_io(1)); the results, the sensor's
+    phase buffer and the loop state equal the copy-engine path bit for bit, also
+    when such steps alternate with device-only (graph) steps."""
+    import torch
+
+    g = sh_geometry("sh16")
+    nact = 97
+    rng = np.random.default_rng(8)
+    cm = (rng.standard_normal((nact, 2 * g.nvalid)) * 0.01).astype(np.float32)
+
+    def build(io):
+        w = core.ShWfs.from_geometry(g, noise=0.5, seed=5)
+        c = core.Centroider(g.nvalid, g.npix / 2 - 0.5, g.pixsize, "wcog")
+        c.set_npix(g.npix)
+        c.load_validpos(g.validsubsx, g.validsubsy)
+        c.set_threshold(1.0)
+        c.load_weights(np.ones((g.npix, g.npix), np.float32))
+        ls = core.LsController(2 * g.nvalid, nact, delay=delay)
+        ls.set_cmat(cm)
+        ls.set_gain(0.3)
+        ls.set_com_range(-0.5, 0.5)
+        loop = core.Loop(w, c, ls, graph=graph)
+        loop.set_host_io(io)
+        return w, ls, loop
+
+    wa, la, loopa = build(1)
+    wb, lb, loopb = build(0)
+    screens = [kolmogorov_screen(g.tel.n, 20.0, seed=40 + i).ravel(order="F") for i in range(6)]
+    ph = torch.from_numpy(np.ascontiguousarray(np.stack(screens))).pin_memory()
+    va = torch.zeros(nact, dtype=torch.float32).pin_memory()
+    vb = torch.zeros(nact, dtype=torch.float32).pin_memory()
+    for it in range(6):
+        if it == 3:  # a device-only step in between (phase already on the device)
+            loopa.step(None, None, noise=True)
+            loopb.step(None, None, noise=True)
+        else:
+            loopa.step(ph[it].data_ptr(), va.data_ptr(), noise=True)
+            loopb.step(ph[it].data_ptr(), vb.data_ptr(), noise=True)
+            np.testing.assert_array_equal(va.numpy(), vb.numpy())
+            np.testing.assert_array_equal(va.numpy(), np.array(la.buffer("voltage")))
+        np.testing.assert_array_equal(np.array(wa.d_phase), np.array(wb.d_phase))
+        np.testing.assert_array_equal(np.array(la.buffer("centroids")), np.array(lb.buffer("centroids")))
+        np.testing.assert_array_equal(np.array(la.buffer("com")), np.array(lb.buffer("com")))
+        np.testing.assert_array_equal(np.array(wa.d_binimg), np.array(wb.d_binimg))
+    assert wa.frame == wb.frame == 6
+    assert la.status() == 0 and loopa.kernels_per_step() == 1
+    assert np.abs(va.numpy()).max() > 0
+
+
 def test_sh_launch_shapes_agree(core):
     """Every autotuner launch shape of the sensor kernel gives the oracle's image,
     and all of them the same bits."""
