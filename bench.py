@@ -599,7 +599,9 @@ def main():
                                "wCoG+threshold, photon + 0.5 e- readout noise, LS 1377x2496 MVM + integrator + "
                                "voltage; one RTC iteration per step",
                    "l2": "flushed before every timed step (256 MB write)",
-                   "parallelism": f"replicas x{ws}", "cuda_graph": not args.no_graph,
+                   "parallelism": f"replicas x{ws}",
+                   "launch": ("one cooperative kernel per step, launched directly" if fused
+                              else ("three kernels per step, CUDA graph" if not args.no_graph else "three kernels per step")),
                    "mvm_precision": args.precision},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": launches,
     }

@@ -19,6 +19,8 @@
 #include <cuda_fp8.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 #include "aob_objects.hpp"
 #include "mvm_core.cuh"
@@ -258,14 +260,43 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
 template <typename T, int NFFT, int PD>
 static bool launch_fused_t(const RtcFusedArgs &A0, int grid, size_t sm, cudaStream_t s, bool dry) {
   auto kern = rtc_fused_kernel<T, NFFT, PD>;
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FUSED_THREADS, sm) != cudaSuccess || per_sm < 1) {
-    cudaGetLastError();
-    return false;
+  // The shared-memory opt-in (set once per device to the largest size, so no
+  // configuration lowers it under another) and the occupancy answer per size
+  // are kept, so a step that launches directly pays for them once.
+  struct Fit {
+    std::mutex mu;
+    std::map<int, size_t> opted;  // dynamic bytes allowed per device (0: the opt-in failed)
+    std::map<std::pair<int, size_t>, bool> ok;
+  };
+  static Fit fit;
+  int dev = 0;
+  AOB_CUDA(cudaGetDevice(&dev));
+  {
+    std::lock_guard<std::mutex> lock(fit.mu);
+    auto od = fit.opted.find(dev);
+    if (od == fit.opted.end()) {
+      int optin = 0;
+      cudaFuncAttributes fa{};
+      size_t allow = 0;
+      if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess &&
+          cudaFuncGetAttributes(&fa, kern) == cudaSuccess && (size_t)optin > fa.sharedSizeBytes) {
+        allow = (size_t)optin - fa.sharedSizeBytes;  // the kernel's static shared memory counts against the opt-in
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)allow) != cudaSuccess)
+          allow = 0;
+      }
+      if (!allow) cudaGetLastError();
+      od = fit.opted.emplace(dev, allow).first;
+    }
+    if (sm > od->second) return false;
+    auto it = fit.ok.find({dev, sm});
+    if (it == fit.ok.end()) {
+      int per_sm = 0;
+      const bool ok =
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FUSED_THREADS, sm) == cudaSuccess && per_sm >= 1;
+      if (!ok) cudaGetLastError();
+      it = fit.ok.emplace(std::make_pair(dev, sm), ok).first;
+    }
+    if (!it->second) return false;
   }
   if (dry) return true;
   RtcFusedArgs A = A0;

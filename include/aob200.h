@@ -408,7 +408,9 @@ int aob_loop_step(aob_loop *l, const float *host_phase, float *host_voltage, int
  * phase, no host copies): warmup untimed steps, then the mean over iters
  * steps.  Used by the autotuner; the loop state advances. */
 int aob_loop_time(aob_loop *l, int noise, int warmup, int iters, float *ms_per_step);
-/* Replay the device part of a step from a CUDA graph (enable != 0). */
+/* Replay the device part of a step from a CUDA graph (enable != 0).  Applies
+ * to the three-kernel step; the fused single-kernel step is always launched
+ * directly (a one-node graph only adds launch latency). */
 int aob_loop_use_graph(aob_loop *l, int enable);
 /* Kernels launched by the device part of the last step. */
 int aob_loop_kernels_per_step(aob_loop *l, int *n);
