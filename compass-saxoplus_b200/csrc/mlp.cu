@@ -254,16 +254,32 @@ static void gemm(const GemmArgs &P, cudaStream_t s, int kind, uint32_t *status, 
               "mlp gemm: contiguous dimensions must be multiples of 8");
   if (kind == 1) {
     TcArgs T{P, A_KM ? 1 : 0, B_KN ? 1 : 0, status, P2 ? P2->K : 0, 0, nullptr};
-    // split K when the output has too few tiles to fill the GPU (plain float
-    // products only: no bias, no activation, no accumulate, no bf16 copy)
+    // split K when it shortens the product (plain float products only: no
+    // bias, no activation, no accumulate, no bf16 copy).  Cost model, measured
+    // on B200: a CTA alone on an SM takes ~0.5 us per 64-deep stage and two
+    // co-resident CTAs share the SM, so a product takes ~ceil(CTAs / SMs) x
+    // stages per slice x 0.5 us; the slice sum streams (n + 1) M N floats at
+    // ~4 TB/s.  Slices keep at least 8 stages.
     const int tiles = ((P.N + TC_BN - 1) / TC_BN) * ((P.M + TC_BM - 1) / TC_BM);
     int dev = 0;
     AOB_CUDA(cudaGetDevice(&dev));
-    const int slots = 2 * num_sms(dev);
+    const int nsm = num_sms(dev);
     int nsplit = 1;
-    if (work && !P2 && P.epi == MG_EPI_NONE && !P.bias && !P.accumulate && !P.Cb && P.Cf && tiles < slots) {
+    if (work && !P2 && P.epi == MG_EPI_NONE && !P.bias && !P.accumulate && !P.Cb && P.Cf && P.ldc % 4 == 0 &&
+        reinterpret_cast<uintptr_t>(P.Cf) % 16 == 0) {
       const int nkt = (P.K + TC_BK - 1) / TC_BK;
-      nsplit = std::min((slots + tiles - 1) / tiles, std::max(1, nkt / 8));  // at least 8 stages per slice
+      auto cost_us = [&](int n) {
+        const int per = (nkt + n - 1) / n, ns = (nkt + per - 1) / per;
+        const double waves = (double)((tiles * ns + nsm - 1) / nsm);
+        const double sum = ns > 1 ? (double)(ns + 1) * P.M * P.N * 4.0 / 4.0e6 : 0.0;
+        return waves * per * 0.5 + sum;
+      };
+      double best = cost_us(1);
+      for (int n = 2; n <= 16 && nkt / n >= 8; ++n)
+        if (cost_us(n) < best) {
+          best = cost_us(n);
+          nsplit = n;
+        }
     }
     if (nsplit > 1) {
       const int per = (((P.K + TC_BK - 1) / TC_BK) + nsplit - 1) / nsplit;
@@ -302,9 +318,9 @@ static void gemm(const GemmArgs &P, cudaStream_t s, int kind, uint32_t *status, 
     tc_gemm_kernel<<<grid, TC_THREADS, TC_SMEM_BYTES, s>>>(ma, mb, ma2, mb2, T);
     AOB_LAUNCH_CHECK("tc_gemm_kernel");
     if (nsplit > 1) {
-      const int64_t n = (int64_t)P.M * P.ldc;
-      tc_splitk_sum_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, s>>>(T.partial, nsplit, P.M, P.N,
-                                                                                        P.ldc, P.Cf);
+      const int nq = (P.N + 3) / 4;
+      dim3 sgrid((nq + 255) / 256, (unsigned)std::min(P.M, 65535));
+      tc_splitk_sum_kernel<<<sgrid, 256, 0, s>>>(T.partial, nsplit, P.M, P.N, P.ldc, P.Cf);
       AOB_LAUNCH_CHECK("tc_splitk_sum_kernel");
     }
     return;

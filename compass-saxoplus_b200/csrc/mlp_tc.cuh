@@ -259,14 +259,32 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
 }
 
 // out[m][n] = sum over slices z (in order) of part[z][m][n], n < N (rows of
-// stride ld): the split-K reduction
+// stride ld): the split-K reduction.  Rows over blockIdx.y, 16-byte column
+// groups over x (ld a multiple of 4, 16-byte aligned buffers: checked on the
+// host); the slices are read streaming, the sum keeps the slice order.
 __global__ void tc_splitk_sum_kernel(const float *part, int nslice, int M, int N, int ld, float *out) {
   const int64_t total = (int64_t)M * ld;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-    if ((int)(i % ld) >= N) continue;
-    float v = part[i];
-    for (int z = 1; z < nslice; ++z) v += part[(int64_t)z * total + i];
-    out[i] = v;
+  const int nq = (N + 3) >> 2;
+  for (int m = blockIdx.y; m < M; m += gridDim.y) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+      const int64_t o = (int64_t)m * ld + 4 * q;
+      float4 v = __ldcs(reinterpret_cast<const float4 *>(part + o));
+      for (int z = 1; z < nslice; ++z) {
+        const float4 w = __ldcs(reinterpret_cast<const float4 *>(part + (int64_t)z * total + o));
+        v.x += w.x;
+        v.y += w.y;
+        v.z += w.z;
+        v.w += w.w;
+      }
+      const int n = 4 * q;
+      if (n + 3 < N) {
+        *reinterpret_cast<float4 *>(out + o) = v;
+      } else {
+        out[o] = v.x;
+        if (n + 1 < N) out[o + 1] = v.y;
+        if (n + 2 < N) out[o + 2] = v.z;
+      }
+    }
   }
 }
 
