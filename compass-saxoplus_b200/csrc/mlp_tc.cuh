@@ -229,26 +229,50 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
     __syncwarp();
     const int n = n0 + c * 32 + n_lane;
     const float bn = (P.bias && n < P.N) ? P.bias[n] : 0.f;
+    if (P.epi == MG_EPI_DGELU && T.kchunk == 0 && !P.accumulate && !P.bias) {
+      // GELU' epilogue (the data gradients): rows in blocks of 8 whose
+      // pre-activations are all requested before any is used, one memory
+      // latency per block instead of one per row
+#pragma unroll 1
+      for (int i0 = 0; i0 < 32; i0 += 8) {
+        float pin[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int m = m0 + warp * 32 + i0 + j;
+          pin[j] = (ok && m < P.M && n < P.N) ? __ldg(P.pre_in + (size_t)m * P.ldp + n) : 0.f;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int m = m0 + warp * 32 + i0 + j;
+          if (!ok || m >= P.M || n >= P.N) continue;
+          const float v = stage[(i0 + j) * 33 + n_lane] * gelu_grad_f(pin[j]);
+          const size_t o = (size_t)m * P.ldc + n;
+          if (P.Cf) P.Cf[o] = v;
+          if (P.Cb) P.Cb[o] = __float2bfloat16_rn(v);
+        }
+      }
+    } else {
 #pragma unroll 4
-    for (int i = 0; i < 32; ++i) {
-      const int m = m0 + warp * 32 + i;
-      if (!ok || m >= P.M || n >= P.N) continue;
-      float v = stage[i * 33 + n_lane];
-      const size_t o = (size_t)m * P.ldc + n;
-      if (T.kchunk > 0) {  // split K: the plain product of this slice (summed later in slice order)
-        T.partial[(size_t)blockIdx.z * P.M * P.ldc + o] = v;
-        continue;
+      for (int i = 0; i < 32; ++i) {
+        const int m = m0 + warp * 32 + i;
+        if (!ok || m >= P.M || n >= P.N) continue;
+        float v = stage[i * 33 + n_lane];
+        const size_t o = (size_t)m * P.ldc + n;
+        if (T.kchunk > 0) {  // split K: the plain product of this slice (summed later in slice order)
+          T.partial[(size_t)blockIdx.z * P.M * P.ldc + o] = v;
+          continue;
+        }
+        if (P.accumulate) v += P.Cf[o];
+        if (P.bias) v += bn;
+        if (P.epi == MG_EPI_GELU) {
+          if (P.pre_out) P.pre_out[(size_t)m * P.ldp + n] = v;
+          v = gelu_f(v);
+        } else if (P.epi == MG_EPI_DGELU) {
+          v *= gelu_grad_f(P.pre_in[(size_t)m * P.ldp + n]);
+        }
+        if (P.Cf) P.Cf[o] = v;
+        if (P.Cb) P.Cb[o] = __float2bfloat16_rn(v);
       }
-      if (P.accumulate) v += P.Cf[o];
-      if (P.bias) v += bn;
-      if (P.epi == MG_EPI_GELU) {
-        if (P.pre_out) P.pre_out[(size_t)m * P.ldp + n] = v;
-        v = gelu_f(v);
-      } else if (P.epi == MG_EPI_DGELU) {
-        v *= gelu_grad_f(P.pre_in[(size_t)m * P.ldp + n]);
-      }
-      if (P.Cf) P.Cf[o] = v;
-      if (P.Cb) P.Cb[o] = __float2bfloat16_rn(v);
     }
     __syncwarp();
   }
