@@ -5,7 +5,7 @@
 // without transposed copies: K-major operands use the K-major shared-memory
 // descriptor, M- or N-contiguous ones the MN-major descriptor.
 //
-// One CTA per 128 x 128 output tile, 4 warps, two CTAs per SM (97 KB of
+// One CTA per 128 x 128 output tile, 8 warps, two CTAs per SM (97 KB of
 // shared memory and 128 TMEM columns each):
 //  * warp 0, one lane: TMA producer -- 2-D tensor loads with 128-byte swizzle
 //    (K-major tile: one box of 64 (K) x 128 rows; MN-major: two boxes of
@@ -16,9 +16,11 @@
 //    per 64-wide stage) and tcgen05.commit on the stage's "empty" mbarrier,
 //    which hands the stage back to the producer once those MMAs completed;
 //    after the last stage, a commit on the accumulator barrier;
-//  * all 4 warps: the epilogue -- warp w reads TMEM lanes 32w..32w+31 (rows of
-//    the tile) with tcgen05.ld 32x32b, transposes each 32 x 32 chunk through
-//    shared memory and applies bias / GELU / GELU' with coalesced row accesses.
+//  * all 8 warps: the epilogue -- warps w and w + 4 read TMEM lanes
+//    32 (w & 3) .. + 31 (rows of the tile; a warp may only read its own lane
+//    quadrant), one half of the columns each, with tcgen05.ld 32x32b, transpose
+//    each 32 x 32 chunk through shared memory and apply bias / GELU / GELU'
+//    with coalesced row accesses.
 // Split K (blockIdx.z slices, each writing its plain FP32 product to a
 // workspace that tc_splitk_sum_kernel adds in slice order: deterministic) keeps
 // the SMs busy for the weight-gradient products, whose outputs have few tiles
@@ -39,7 +41,7 @@
 
 namespace aob {
 
-constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 64, TC_STAGES = 3, TC_THREADS = 128;
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 64, TC_STAGES = 3, TC_THREADS = 256;
 constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 2;  // one operand tile of a stage (16 KB)
 constexpr int TC_STAGE_BYTES = 2 * TC_TILE_BYTES;
 constexpr uint32_t TC_MAX_POLLS = 1u << 24;
@@ -218,12 +220,15 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
   ok &= mbar_wait(accb, 0, TC_MAX_POLLS);
   __syncwarp();
   tc_fence_after();
+  // warps w and w + 4 share TMEM lane quadrant w & 3 (a warp may only read
+  // its own quadrant) and take one half of the tile's columns each
+  const int quad = warp & 3, half = warp >> 2;
   float *stage = reinterpret_cast<float *>(sm) + warp * 32 * 33;
   const int n_lane = lane;
 #pragma unroll 1
-  for (int c = 0; c < TC_BN / 32; ++c) {
+  for (int c = half * (TC_BN / 64); c < (half + 1) * (TC_BN / 64); ++c) {
     uint32_t r[32];
-    tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 32), r);
+    tmem_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(c * 32), r);
 #pragma unroll
     for (int j = 0; j < 32; ++j) stage[lane * 33 + j] = __uint_as_float(r[j]);
     __syncwarp();
@@ -238,12 +243,12 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
         float pin[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-          const int m = m0 + warp * 32 + i0 + j;
+          const int m = m0 + quad * 32 + i0 + j;
           pin[j] = (ok && m < P.M && n < P.N) ? __ldg(P.pre_in + (size_t)m * P.ldp + n) : 0.f;
         }
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-          const int m = m0 + warp * 32 + i0 + j;
+          const int m = m0 + quad * 32 + i0 + j;
           if (!ok || m >= P.M || n >= P.N) continue;
           const float v = stage[(i0 + j) * 33 + n_lane] * gelu_grad_f(pin[j]);
           const size_t o = (size_t)m * P.ldc + n;
@@ -254,7 +259,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
     } else {
 #pragma unroll 4
       for (int i = 0; i < 32; ++i) {
-        const int m = m0 + warp * 32 + i;
+        const int m = m0 + quad * 32 + i;
         if (!ok || m >= P.M || n >= P.N) continue;
         float v = stage[i * 33 + n_lane];
         const size_t o = (size_t)m * P.ldc + n;
