@@ -5,7 +5,7 @@
 // without transposed copies: K-major operands use the K-major shared-memory
 // descriptor, M- or N-contiguous ones the MN-major descriptor.
 //
-// One CTA per 128 x 128 output tile, 8 warps, two CTAs per SM (97 KB of
+// One CTA per 128 x 128 output tile, 16 warps, two CTAs per SM (97 KB of
 // shared memory and 128 TMEM columns each):
 //  * warp 0, one lane: TMA producer -- 2-D tensor loads with 128-byte swizzle
 //    (K-major tile: one box of 64 (K) x 128 rows; MN-major: two boxes of
@@ -16,9 +16,9 @@
 //    per 64-wide stage) and tcgen05.commit on the stage's "empty" mbarrier,
 //    which hands the stage back to the producer once those MMAs completed;
 //    after the last stage, a commit on the accumulator barrier;
-//  * all 8 warps: the epilogue -- warps w and w + 4 read TMEM lanes
-//    32 (w & 3) .. + 31 (rows of the tile; a warp may only read its own lane
-//    quadrant), one half of the columns each, with tcgen05.ld 32x32b, transpose
+//  * all 16 warps: the epilogue -- warps w, w + 4, w + 8, w + 12 read TMEM
+//    lanes 32 (w & 3) .. + 31 (rows of the tile; a warp may only read its own
+//    lane quadrant), one 32-column chunk each, with tcgen05.ld 32x32b, transpose
 //    each 32 x 32 chunk through shared memory and apply bias / GELU / GELU'
 //    with coalesced row accesses.
 // Split K (blockIdx.z slices, each writing its plain FP32 product to a
@@ -41,7 +41,7 @@
 
 namespace aob {
 
-constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 64, TC_STAGES = 3, TC_THREADS = 256;
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 64, TC_STAGES = 3, TC_THREADS = 512;
 constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 2;  // one operand tile of a stage (16 KB)
 constexpr int TC_STAGE_BYTES = 2 * TC_TILE_BYTES;
 constexpr uint32_t TC_MAX_POLLS = 1u << 24;
@@ -220,13 +220,13 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
   ok &= mbar_wait(accb, 0, TC_MAX_POLLS);
   __syncwarp();
   tc_fence_after();
-  // warps w and w + 4 share TMEM lane quadrant w & 3 (a warp may only read
-  // its own quadrant) and take one half of the tile's columns each
-  const int quad = warp & 3, half = warp >> 2;
+  // warps w, w + 4, w + 8 and w + 12 share TMEM lane quadrant w & 3 (a warp
+  // may only read its own quadrant) and take one 32-column chunk each
+  const int quad = warp & 3, part = warp >> 2;
   float *stage = reinterpret_cast<float *>(sm) + warp * 32 * 33;
   const int n_lane = lane;
 #pragma unroll 1
-  for (int c = half * (TC_BN / 64); c < (half + 1) * (TC_BN / 64); ++c) {
+  for (int c = part * (TC_BN / 128); c < (part + 1) * (TC_BN / 128); ++c) {
     uint32_t r[32];
     tmem_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(c * 32), r);
 #pragma unroll
