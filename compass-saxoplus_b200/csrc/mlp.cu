@@ -37,10 +37,24 @@ __global__ void f32_to_bf16_kernel(const float *src, __nv_bfloat16 *dst, int64_t
 }
 
 // x [batch][nin] float -> xb [batch][pin] bf16 of x * scale, zero padding
+// (the row loops below take four elements per thread and pass, all loads
+// issued before any use, so that enough bytes are in flight per SM)
 __global__ void mlp_input_kernel(const float *x, int nin, int pin, int batch, float scale, __nv_bfloat16 *xb) {
+  const int nt = blockDim.x;
   for (int b = blockIdx.x; b < batch; b += gridDim.x)
-    for (int i = threadIdx.x; i < pin; i += blockDim.x)
-      xb[(int64_t)b * pin + i] = __float2bfloat16_rn(i < nin ? x[(int64_t)b * nin + i] * scale : 0.f);
+    for (int i0 = threadIdx.x; i0 < pin; i0 += 4 * nt) {
+      float v[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int i = i0 + k * nt;
+        v[k] = i < nin ? __ldcs(x + (int64_t)b * nin + i) : 0.f;
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int i = i0 + k * nt;
+        if (i < pin) xb[(int64_t)b * pin + i] = __float2bfloat16_rn(v[k] * scale);
+      }
+    }
 }
 
 __global__ void mlp_output_kernel(const float *y, int nout, int pout, int batch, float scale, float *out) {
@@ -55,13 +69,25 @@ __global__ void mlp_loss_kernel(const float *y, const float *t, int nout, int po
   __shared__ float red[256];
   const float g = 2.f / ((float)batch * (float)nout);
   float acc = 0.f;
+  const int nt = blockDim.x;
   for (int b = blockIdx.x; b < batch; b += gridDim.x)
-    for (int o = threadIdx.x; o < pout; o += blockDim.x) {
-      const int64_t i = (int64_t)b * pout + o;
-      float d = 0.f;
-      if (o < nout) d = y[i] - t[(int64_t)b * nout + o] * inv_out_scale;
-      dy[i] = __float2bfloat16_rn(g * d);
-      acc += d * d;
+    for (int o0 = threadIdx.x; o0 < pout; o0 += 4 * nt) {
+      float yv[4], tv[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int o = o0 + k * nt;
+        yv[k] = o < nout ? y[(int64_t)b * pout + o] : 0.f;
+        tv[k] = o < nout ? __ldcs(t + (int64_t)b * nout + o) : 0.f;
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int o = o0 + k * nt;
+        if (o >= pout) continue;
+        float d = 0.f;
+        if (o < nout) d = yv[k] - tv[k] * inv_out_scale;
+        dy[(int64_t)b * pout + o] = __float2bfloat16_rn(g * d);
+        acc += d * d;
+      }
     }
   red[threadIdx.x] = acc;
   __syncthreads();
@@ -85,20 +111,42 @@ __global__ void mlp_loss_final_kernel(const float *part, int nblocks, float deno
 // partial sums over row chunks (block 32 columns x 8 row lanes, coalesced
 // rows), then the chunks added in order.
 constexpr int COLSUM_CHUNKS = 16;
+// Partial column sums over a chunk of rows: a thread takes two adjacent
+// columns (cols even: one 4-byte load per row, 128 bytes per warp) and rows
+// r0 + ty + 8 j, four rows' loads issued before they are added (in row order).
 __global__ void mlp_colsum_part_kernel(const __nv_bfloat16 *d, int batch, int cols, float *part) {
-  __shared__ float red[8][33];
-  const int c = blockIdx.x * 32 + threadIdx.x;
+  __shared__ float red[8][2][33];
+  const int c = 2 * (blockIdx.x * 32 + threadIdx.x);
   const int rchunk = (batch + gridDim.y - 1) / gridDim.y;
   const int r0 = blockIdx.y * rchunk, r1 = min(batch, r0 + rchunk);
-  float s = 0.f;
+  float s0 = 0.f, s1 = 0.f;
   if (c < cols)
-    for (int b = r0 + threadIdx.y; b < r1; b += 8) s += __bfloat162float(d[(int64_t)b * cols + c]);
-  red[threadIdx.y][threadIdx.x] = s;
+    for (int b0 = r0 + threadIdx.y; b0 < r1; b0 += 32) {
+      __nv_bfloat162 v[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int b = b0 + 8 * k;
+        v[k] = b < r1 ? *reinterpret_cast<const __nv_bfloat162 *>(d + (int64_t)b * cols + c)
+                      : __floats2bfloat162_rn(0.f, 0.f);
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (b0 + 8 * k >= r1) break;
+        const float2 f = __bfloat1622float2(v[k]);
+        s0 += f.x;
+        s1 += f.y;
+      }
+    }
+  red[threadIdx.y][0][threadIdx.x] = s0;
+  red[threadIdx.y][1][threadIdx.x] = s1;
   __syncthreads();
-  if (threadIdx.y == 0 && c < cols) {
-    float t = 0.f;
-    for (int y = 0; y < 8; ++y) t += red[y][threadIdx.x];
-    part[(int64_t)blockIdx.y * cols + c] = t;
+  if (threadIdx.y < 2) {
+    const int cc = c + threadIdx.y;
+    if (cc < cols) {
+      float t = 0.f;
+      for (int y = 0; y < 8; ++y) t += red[y][threadIdx.y][threadIdx.x];
+      part[(int64_t)blockIdx.y * cols + cc] = t;
+    }
   }
 }
 __global__ void mlp_colsum_final_kernel(const float *part, int nchunk, int cols, float *out) {
@@ -471,7 +519,9 @@ void aob_mlp::forward(const float *x, int batch, float *y_out, cudaStream_t s) {
 // bias gradient: column sums of a [batch][cols] bf16 matrix
 void aob_mlp::colsum(const __nv_bfloat16 *d, int batch, int cols, float *out, cudaStream_t s) {
   if (colsum_part.n < (int64_t)COLSUM_CHUNKS * cols) colsum_part.alloc((int64_t)COLSUM_CHUNKS * cols);
-  mlp_colsum_part_kernel<<<dim3((cols + 31) / 32, COLSUM_CHUNKS), dim3(32, 8), 0, s>>>(d, batch, cols, colsum_part.p);
+  AOB_REQUIRE(cols % 2 == 0, "mlp.colsum: padded column count must be even");
+  mlp_colsum_part_kernel<<<dim3((cols / 2 + 31) / 32, COLSUM_CHUNKS), dim3(32, 8), 0, s>>>(d, batch, cols,
+                                                                                        colsum_part.p);
   mlp_colsum_final_kernel<<<(cols + 255) / 256, 256, 0, s>>>(colsum_part.p, COLSUM_CHUNKS, cols, out);
   AOB_LAUNCH_CHECK("mlp_colsum_kernel");
 }
