@@ -13,7 +13,8 @@ value is steps / (sum of step times).
 Other keys of the JSON line:
   e2e       the same step through the C ABI call a caller makes
             (aob_loop_step) with the phase screen copied in from pinned host
-            memory and the voltages copied back every step;
+            memory and the voltages written back into pinned host memory by
+            the fused kernel, every step;
   roofline  the dominant kernel's algorithmic bytes / measured duration against
             the measured HBM copy bandwidth in MEASURED_PEAKS.json;
   cpu_baseline  the float64 NumPy/SciPy restatement timed on the host cores.
@@ -126,6 +127,9 @@ class ClockSampler:
             pass
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # B200 FP32 (non-tensor), nominal
 
 
 def graph_time(torch, flush, fn, n=20, with_flush=True):
@@ -368,8 +372,10 @@ def run_pyr50(args, torch):
           {"workload": f"pyr50: {g.nxsub}x{g.nxsub} pupil samples per image, {npts} modulation points at 3 lambda/D, "
                        f"{nfft}x{nfft} FFTs, {g.nvalid} valid, 1600-actuator LS MVM",
            "l2": "flushed before every timed step (256 MB write)"},
-          roofline={"bound": "fp32 FFT", "achieved": flops / t_img / 1e12, "unit": "TFLOP/s", "peak": None,
-                    "frac": None, "traffic": None, "kernel": "pyramid image kernels",
+          # no measured FP32 (non-tensor) peak: nominal 148 SMs x 128 FP32 lanes x 2 FLOP x 1.965 GHz
+          roofline={"bound": "fp32 FFT", "achieved": flops / t_img / 1e12, "unit": "TFLOP/s", "peak": FP32_NOMINAL_TFLOPS,
+                    "frac": flops / t_img / 1e12 / FP32_NOMINAL_TFLOPS, "peak_source": "nominal (not measured)",
+                    "traffic": None, "kernel": "pyramid image kernels",
                     "flops_per_image": flops, "image_us": t_img * 1e6, "step_us": t_step * 1e6},
           cpu_baseline=cpu, clocks=clk.summary(), gpu_launches=None)
 
