@@ -88,12 +88,21 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
   // then do not queue behind the matrix stream, which still has the DFT,
   // binning, noise and centroid stages to land.
   const int helper = (int)blockDim.x - 32;
+  // The sensor tables arrive by bulk copy on bars[1], issued at entry: no
+  // thread holds a register waiting for them before the DFTs, so the field
+  // stage's loads (pupil windows, then phase) go out at once.
+  const ShSmem L1(NFFT, A.sh.nu, A.sh.nv, pd, A.sh.nrebin2 * A.sh.npix * A.sh.npix, A.sh.npix * A.sh.npix, 1);
+  const ShTableCopy tcopy(A.sh, L1);
   if ((int)threadIdx.x == helper) {
-    // one barrier for all the rows: a single wait later
+    // one barrier for all the rows: a single wait later; one for the tables
     mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
     fence_mbar_init();
+    mbar_expect_tx(&bars[1], tcopy.image_bytes + tcopy.wt_bytes);
+    bulk_g2s(shm, A.sh.tblob, tcopy.image_bytes, &bars[1]);
+    if (tcopy.wt_bytes) bulk_g2s(shm + L1.wt, A.sh.c_weights, tcopy.wt_bytes, &bars[1]);
   }
-  bool copies_out = false;
+  bool copies_out = false, tables_in = false;
   auto issue_rows = [&]() {
     if (!copies_out && (int)threadIdx.x == helper) {
       const unsigned char *src = static_cast<const unsigned char *>(A.mat) + (size_t)r0 * row_bytes;
@@ -102,6 +111,10 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
         bulk_g2s(rows + (size_t)r * row_bytes, src + (size_t)r * row_bytes, row_bytes, &bars[0]);
     }
     copies_out = true;
+    if (!tables_in) {  // every thread, before the first stage that reads the tables
+      if (!mbar_wait(&bars[1], 0, ROW_MAX_POLLS)) atomicOr(A.status, (uint32_t)ERR_MBAR_TIMEOUT);
+      tables_in = true;
+    }
   };
   // epilogue inputs of this CTA's rows, fetched now so the epilogue makes no
   // global round trip: [scale | modal gain | com | ring[0] | ring[1]]
@@ -126,9 +139,9 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
     }
   }
   // ---- sensor images and slopes: this CTA's sub-apertures, A.batch per round ----
-  sh_load_tables<NFFT>(A.sh, shm, threadIdx.x, blockDim.x);
-  // (the barrier closing sh_batch's stage 1 publishes the tables: stages 0-1
-  // read none of them, so their loads overlap the field's)
+  sh_load_tables<NFFT>(A.sh, shm, threadIdx.x, blockDim.x, true, tcopy.wt_bytes != 0);
+  // (stages 0-1 read no tables; the copied ones are waited for after stage 1,
+  // the rest is published by the barrier that closes stage 1)
   // With the CTA's whole share in one round (the usual case) the cube and
   // image writes wait until the CTA has arrived at the grid barrier: the slopes
   // go out first and the barrier's release does not wait on the image stores.
@@ -252,8 +265,10 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
   }
   // no CTA may exit with a copy still landing in its shared memory
   __syncthreads();
-  if ((int)threadIdx.x == helper)
+  if ((int)threadIdx.x == helper) {
     mbar_wait(&bars[0], 0, ROW_MAX_POLLS);
+    mbar_wait(&bars[1], 0, ROW_MAX_POLLS);
+  }
 }
 
 // ---------------------------------------------------------------------------

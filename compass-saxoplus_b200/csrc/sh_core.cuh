@@ -126,16 +126,33 @@ __device__ __forceinline__ void team_sync(const Team &t) {
     asm volatile("bar.sync %0, %1;" ::"r"(t.bar), "r"(t.nt) : "memory");
 }
 
+// The bulk-copyable part of the tables: the table image (ShSmem::rk bytes at
+// offset 0) and, when its size and address allow a bulk copy (16-byte
+// multiple and alignment), the shared wCoG weights (wt_bytes at ShSmem::wt).
+struct ShTableCopy {
+  uint32_t image_bytes, wt_bytes;
+  __device__ ShTableCopy(const ShKernelArgs &P, const ShSmem &L) {
+    const int npix2 = P.npix * P.npix;
+    image_bytes = (uint32_t)L.rk;
+    const bool wt = P.ckind == 2 && !P.c_wper && (npix2 * 4) % 16 == 0 &&
+                    (reinterpret_cast<uintptr_t>(P.c_weights) & 15) == 0;
+    wt_bytes = wt ? (uint32_t)(npix2 * 4) : 0u;
+  }
+};
+
 // CTA-cooperative load of the tables (caller synchronises afterwards): the
 // sensor's table image with 16-byte loads (one page, one request per
 // thread), the wCoG weights and the 1/k table of the Poisson sampler.
+// image_done / wt_done: those parts already arrive by bulk copy.
 template <int NFFT>
-__device__ __forceinline__ void sh_load_tables(const ShKernelArgs &P, unsigned char *smem, int tid, int nthreads) {
+__device__ __forceinline__ void sh_load_tables(const ShKernelArgs &P, unsigned char *smem, int tid, int nthreads,
+                                               bool image_done = false, bool wt_done = false) {
   const int npix2 = P.npix * P.npix;
   const ShSmem L(NFFT, P.nu, P.nv, P.pdiam, P.nrebin2 * npix2, npix2, 1);
   int4 *dst = reinterpret_cast<int4 *>(smem);
-  for (int i = tid; i < (int)(L.rk / 16); i += nthreads) dst[i] = __ldg(P.tblob + i);
-  if (P.ckind == 2 && !P.c_wper) {
+  if (!image_done)
+    for (int i = tid; i < (int)(L.rk / 16); i += nthreads) dst[i] = __ldg(P.tblob + i);
+  if (P.ckind == 2 && !P.c_wper && !wt_done) {
     float *wt = reinterpret_cast<float *>(smem + L.wt);
     for (int i = tid; i < npix2; i += nthreads) wt[i] = __ldg(P.c_weights + i);
   }
