@@ -248,8 +248,14 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
   // ---- 0. metadata of the batch (one global round trip for all of it:
   //      global-space loads, free to overtake the shared stores) ----
   const uint32_t frame = P.frame_ptr ? __ldcg(P.frame_ptr) : P.frame;
-  if (tid < S) {
-    const int k = base + tid * stride;
+  // (threads with no field element take the metadata when there are such:
+  // the shared stores wait for their loads, which would otherwise hold back a
+  // field thread's own loads by a round trip)
+  const int nE = S * pd2;
+  const int t0 = max(0, min(nE, nt - S));
+  for (int mt = tid - t0; mt < S; mt += nt) {
+    if (mt < 0) break;
+    const int k = base + mt * stride;
     const int vx = __ldg(P.validsubsx + k), vy = __ldg(P.validsubsy + k);
     const float fl = __ldg(P.flux + k);
     float rx = 0.f, ry = 0.f;
@@ -257,18 +263,17 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
       rx = __ldg(P.c_ref + (P.c_order ? 2 * k : k));
       ry = __ldg(P.c_ref + (P.c_order ? 2 * k + 1 : k + P.nvalid));
     }
-    m_vx[tid] = vx;
-    m_vy[tid] = vy;
-    m_fl[tid] = fl;
-    m_rx[tid] = rx;
-    m_ry[tid] = ry;
+    m_vx[mt] = vx;
+    m_vy[mt] = vy;
+    m_fl[mt] = fl;
+    m_rx[mt] = rx;
+    m_ry[mt] = ry;
   }
   if (tid == 0) n_listed[0] = n_listed[1] = 0;
   // (no barrier here: stage 1 reads the phase-window corners itself, the
   // metadata and the counters are first used after stage 1's barrier)
 
   // ---- 1. complex field: loads of up to 4 elements issued before any use ----
-  const int nE = S * pd2;
   for (int i0 = tid; i0 < nE; i0 += 4 * nt) {
     float ph[4], am[4], of[4];
 #pragma unroll
