@@ -291,6 +291,11 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       "l"(src), "r"(bytes), "r"(smem_addr(bar))
       : "memory");
 }
+// Prefetch [src, src + bytes) into L2 (bytes and src: multiples of 16); no
+// completion to wait for.
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
 // Bounded wait for phase ``parity`` of ``bar``: true when it completed, false
 // after ``max_polls`` unsuccessful polls (the caller records an error).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t max_polls) {

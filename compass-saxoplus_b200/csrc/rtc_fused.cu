@@ -94,6 +94,21 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
   const ShSmem L1(NFFT, A.sh.nu, A.sh.nv, pd, A.sh.nrebin2 * A.sh.npix * A.sh.npix, A.sh.npix * A.sh.npix, 1);
   const ShTableCopy tcopy(A.sh, L1);
   if ((int)threadIdx.x == helper) {
+    // this CTA's slice of the phase screen and of the pupil into L2: the field
+    // stage's loads depend on the pupil-window corners (a first round trip),
+    // and the values they then fetch are in L2 by that time
+    const uint32_t screen = (uint32_t)A.sh.npup * (uint32_t)A.sh.npup * 4u;
+    const uint32_t slice = ((screen + gridDim.x - 1) / gridDim.x + 15u) & ~15u;
+    const uint32_t off = blockIdx.x * slice;
+    if (off < screen) {
+      const uint32_t len = min(slice, (screen - off) & ~15u);
+      if (len) {
+        if ((reinterpret_cast<uintptr_t>(A.sh.phase) & 15) == 0)
+          bulk_prefetch_l2(reinterpret_cast<const unsigned char *>(A.sh.phase) + off, len);
+        if ((reinterpret_cast<uintptr_t>(A.sh.pupil) & 15) == 0)
+          bulk_prefetch_l2(reinterpret_cast<const unsigned char *>(A.sh.pupil) + off, len);
+      }
+    }
     // one barrier for all the rows: a single wait later; one for the tables
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
