@@ -5,8 +5,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 namespace aob {
 
@@ -28,6 +31,23 @@ inline void cuda_check(cudaError_t e, const char *what) {
   do {                                         \
     if (!(cond)) throw ::aob::Error(msg);      \
   } while (0)
+
+// Opt kernel ``fn`` into ``bytes`` of dynamic shared memory on the current
+// device.  Recorded per (kernel, device) and only ever raised, under a lock,
+// so that every device gets its own opt-in and no caller lowers the limit
+// another one relies on.
+inline void smem_opt_in(const void *fn, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, int> done;
+  int dev = 0;
+  AOB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  int &cur = done[{fn, dev}];
+  if (bytes > cur) {
+    AOB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    cur = bytes;
+  }
+}
 
 // RAII device buffer
 template <typename T>

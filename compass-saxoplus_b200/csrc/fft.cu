@@ -78,11 +78,7 @@ void fft2d(float2 *data, int n, int batch, bool inverse, int device, cudaStream_
   int logn = 0;
   while ((1 << logn) < n) ++logn;
   const float2 *tw = fft_twiddles(device, n);
-  static bool attr_set = false;
-  if (!attr_set) {
-    AOB_CUDA(cudaFuncSetAttribute(fft_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2048 * FFT_COLS * 8));
-    attr_set = true;
-  }
+  smem_opt_in(reinterpret_cast<const void *>(fft_cols_kernel), 2048 * FFT_COLS * 8);
   const int thr = std::min(512, std::max(32, n / 2));
   fft_rows_kernel<<<n * batch, thr, n * sizeof(float2), s>>>(data, n, logn, tw, inverse ? 1 : 0);
   AOB_LAUNCH_CHECK("fft_rows_kernel");

@@ -357,11 +357,7 @@ static void gemm(const GemmArgs &P, cudaStream_t s, int kind, uint32_t *status, 
       ma2 = ma;
       mb2 = mb;
     }
-    static bool configured = false;
-    if (!configured) {
-      AOB_CUDA(cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_BYTES));
-      configured = true;
-    }
+    smem_opt_in(reinterpret_cast<const void *>(tc_gemm_kernel), (int)TC_SMEM_BYTES);
     dim3 grid((P.N + TC_BN - 1) / TC_BN, (P.M + TC_BM - 1) / TC_BM, nsplit);
     tc_gemm_kernel<<<grid, TC_THREADS, TC_SMEM_BYTES, s>>>(ma, mb, ma2, mb2, T);
     AOB_LAUNCH_CHECK("tc_gemm_kernel");

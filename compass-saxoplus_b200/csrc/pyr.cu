@@ -293,16 +293,14 @@ template <int N>
 static void pyr_launch(const PyrArgs &A, int npts, int ntot, int nbin_ctas, cudaStream_t s) {
   const size_t sm = sizeof(float2) * (N * PYR_SEQ + N / 2);
   const size_t bin_sm = sm + sizeof(float) * N * PYR_SEQ;
-  static bool configured = false;
-  if (!configured) {
+  {
     const int lim = (int)std::max<size_t>(bin_sm, 48 * 1024);
-    AOB_CUDA(cudaFuncSetAttribute(pyr_rows_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    AOB_CUDA(cudaFuncSetAttribute(pyr_cols_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    AOB_CUDA(cudaFuncSetAttribute(pyr_accum_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    AOB_CUDA(cudaFuncSetAttribute(pyr_conv_rows_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    AOB_CUDA(cudaFuncSetAttribute(pyr_conv_cols_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    AOB_CUDA(cudaFuncSetAttribute(pyr_bin_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    configured = true;
+    smem_opt_in(reinterpret_cast<const void *>(pyr_rows_kernel<N>), lim);
+    smem_opt_in(reinterpret_cast<const void *>(pyr_cols_kernel<N>), lim);
+    smem_opt_in(reinterpret_cast<const void *>(pyr_accum_kernel<N>), lim);
+    smem_opt_in(reinterpret_cast<const void *>(pyr_conv_rows_kernel<N>), lim);
+    smem_opt_in(reinterpret_cast<const void *>(pyr_conv_cols_kernel<N>), lim);
+    smem_opt_in(reinterpret_cast<const void *>(pyr_bin_kernel<N>), lim);
   }
   pyr_rows_kernel<N><<<npts * ((ntot + PYR_SEQ - 1) / PYR_SEQ), PYR_THREADS, sm, s>>>(A);
   AOB_LAUNCH_CHECK("pyr_rows_kernel");
