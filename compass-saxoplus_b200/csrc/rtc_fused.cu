@@ -1,14 +1,18 @@
 // One RTC iteration in one cooperative kernel: Shack-Hartmann image + fused
 // centroids -> grid barrier -> command-matrix MVM + integrator + voltage.
 //
-// The MVM's HBM stream does not depend on the slopes, so it is started first:
-// at kernel entry one thread per CTA issues TMA bulk copies of that CTA's rows of
-// the packed command matrix into shared memory (one mbarrier per row).  While
+// At entry one thread per CTA bulk-copies the sensor tables into shared memory
+// and prefetches its slice of the phase screen and pupil into L2.  The MVM's
+// HBM stream does not depend on the slopes: once the first batch's complex
+// field is formed (so the sensor's own first loads did not queue behind it),
+// the same thread issues TMA bulk copies of the CTA's rows of the packed
+// command matrix into shared memory, all completing on one mbarrier.  While
 // those bytes are in flight the CTA forms the sensor images of its share of the
-// sub-apertures (k = blockIdx.x + j * gridDim.x) in batches (sh_core.cuh).
-// A bounded grid barrier then publishes the slopes; every CTA stages them in
-// shared memory and reduces its rows, which by then have landed, applying the
-// integrator (sutra_controller_ls.cpp:251-285, sutra_utils.cu:631-639) and the
+// sub-apertures (k = blockIdx.x + j * gridDim.x) (sh_core.cuh).  The CTA then
+// arrives at a bounded grid barrier, writes its cube and image while the other
+// CTAs arrive, and once all slopes are published stages them in shared memory
+// and reduces its rows, which by then have landed, applying the integrator
+// (sutra_controller_ls.cpp:251-285, sutra_utils.cu:631-639) and the
 // delay/latency/clip voltage stage (sutra_controller.cpp:205-263) per actuator.
 //
 // Co-residency of all CTAs is guaranteed by the cooperative launch attribute;
