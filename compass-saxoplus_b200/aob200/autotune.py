@@ -11,7 +11,10 @@ reduces in a fixed order -- only the time):
 
 Each candidate is timed with CUDA events on a private stream (``warmup``
 untimed steps, then the mean of ``iters`` steps); timing steps the objects,
-so their loop state (commands, noise frame) advances.  The winner is cached
+so their loop state (commands, noise frame) advances.  A candidate the
+library rejects (for instance one whose tiles do not fit in shared memory) is
+recorded with its error and skipped; only when no candidate runs does the
+search raise.  The winner is cached
 in a JSON file -- ``$AOB_AUTOTUNE_CACHE``, default
 ``~/.cache/aob200/autotune.json`` -- under a key made of the device name, its
 SM count and a signature of the workload's shapes, so a later run with the
@@ -26,7 +29,7 @@ import json
 import os
 import time
 
-from ._lib import call
+from ._lib import AobError, call
 
 DEFAULT_BATCH_SPACE = dict(subaps=(16, 32, 64), team=(64, 256), mvm_kb=(48, 96), lag=(16,), ctas_per_sm=(2, 3),
                            order=(0,))
@@ -86,6 +89,13 @@ def _grid(space: dict):
     return [dict(zip(keys, o)) for o in out]
 
 
+def _fastest(trials, what):
+    ran = [r for r in trials if r["ms"] is not None]
+    if not ran:
+        raise AobError(f"autotune: no {what} tuning candidate ran ({trials[0].get('error') if trials else 'empty space'})")
+    return min(ran, key=lambda r: r["ms"])
+
+
 def tune_batch(batch, noise=True, space=None, warmup=3, iters=10, use_cache=True, device=0, log=None):
     """Time every tuning in ``space`` (a dict of candidate lists, see
     DEFAULT_BATCH_SPACE) on ``batch``, apply the fastest and return
@@ -100,13 +110,19 @@ def tune_batch(batch, noise=True, space=None, warmup=3, iters=10, use_cache=True
     trials = []
     for cand in _grid(space):
         cand = {k: cand.get(k, 0) for k in _BATCH_KEYS}
-        batch.set_tuning(*(cand[k] for k in _BATCH_KEYS))
         t0 = time.perf_counter()
-        ms = batch.time(noise=noise, warmup=warmup, iters=iters)
+        try:
+            batch.set_tuning(*(cand[k] for k in _BATCH_KEYS))
+            ms = batch.time(noise=noise, warmup=warmup, iters=iters)
+        except AobError as e:
+            trials.append(dict(cand, ms=None, error=str(e)))
+            if log:
+                log(f"batch tuning {cand}: rejected ({e})")
+            continue
         trials.append(dict(cand, ms=ms))
         if log:
             log(f"batch tuning {cand}: {ms * 1e3:.1f} us/step ({time.perf_counter() - t0:.2f} s)")
-    best = min(trials, key=lambda r: r["ms"])
+    best = _fastest(trials, "batch")
     tuning = {k: best[k] for k in _BATCH_KEYS}
     batch.set_tuning(*(tuning[k] for k in _BATCH_KEYS))
     res = dict(tuning=tuning, ms=best["ms"], trials=trials)
@@ -132,12 +148,18 @@ def tune_loop(loop, noise=True, space=None, warmup=3, iters=20, use_cache=True, 
         return dict(store[key], cached=True)
     trials = []
     for cand in _grid(space):
-        loop.set_mode(2, cand["fused_batch"])
-        ms = loop.time(noise=noise, warmup=warmup, iters=iters)
+        try:
+            loop.set_mode(2, cand["fused_batch"])
+            ms = loop.time(noise=noise, warmup=warmup, iters=iters)
+        except AobError as e:
+            trials.append(dict(cand, ms=None, error=str(e)))
+            if log:
+                log(f"loop tuning {cand}: rejected ({e})")
+            continue
         trials.append(dict(cand, ms=ms))
         if log:
             log(f"loop tuning {cand}: {ms * 1e3:.1f} us/step")
-    best = min(trials, key=lambda r: r["ms"])
+    best = _fastest(trials, "loop")
     loop.set_mode(0, best["fused_batch"])
     res = dict(tuning={"fused_batch": best["fused_batch"]}, ms=best["ms"], trials=trials)
     if use_cache:
