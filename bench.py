@@ -133,8 +133,9 @@ FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # B200 FP32 (non-tensor), 
 
 
 def graph_time(torch, flush, fn, n=20, with_flush=True):
-    """Mean device seconds of fn(stream) per launch: n x [flush, fn] minus n x [flush],
-    each replayed as one CUDA graph (no host gaps), best of 5 replays."""
+    """Mean device seconds of fn(stream) per launch: n x [flush, fn] minus n x [flush]
+    (with_flush=False: n x [fn] alone), each replayed as one CUDA graph (no host
+    gaps), best of 5 replays."""
     gs = torch.cuda.Stream()
     torch.cuda.synchronize()
     with torch.cuda.stream(gs):
@@ -152,9 +153,10 @@ def graph_time(torch, flush, fn, n=20, with_flush=True):
         return gr
 
     g1 = capture(lambda: fn(gs.cuda_stream))
-    g0 = capture(lambda: None)
+    # the baseline graph holds the flushes alone; without flushes there is nothing to subtract
+    graphs = (g1, capture(lambda: None)) if with_flush else (g1,)
     out = []
-    for gr in (g1, g0):
+    for gr in graphs:
         for _ in range(2):
             gr.replay()
         torch.cuda.synchronize()
@@ -167,7 +169,7 @@ def graph_time(torch, flush, fn, n=20, with_flush=True):
             torch.cuda.synchronize()
             best = min(best, a.elapsed_time(b) / 1000.0)
         out.append(best)
-    return (out[0] - out[1]) / n
+    return (out[0] - (out[1] if with_flush else 0.0)) / n
 
 
 def _dist():

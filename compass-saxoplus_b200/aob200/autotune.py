@@ -14,7 +14,8 @@ untimed steps, then the mean of ``iters`` steps); timing steps the objects,
 so their loop state (commands, noise frame) advances.  A candidate the
 library rejects (for instance one whose tiles do not fit in shared memory) is
 recorded with its error and skipped; only when no candidate runs does the
-search raise.  The winner is cached
+search raise.  A failure that leaves the device broken (a sticky CUDA error,
+or an expired bounded wait in the object's status word) is raised at once.  The winner is cached
 in a JSON file -- ``$AOB_AUTOTUNE_CACHE``, default
 ``~/.cache/aob200/autotune.json`` -- under a key made of the device name, its
 SM count and a signature of the workload's shapes, so a later run with the
@@ -89,6 +90,16 @@ def _grid(space: dict):
     return [dict(zip(keys, o)) for o in out]
 
 
+def _reraise_if_broken(obj, err):
+    """A candidate the library refused on the host leaves the device usable and is
+    skipped.  A failure that left a sticky CUDA error or an expired bounded wait
+    (``obj.healthy()`` is False) would make every later timing meaningless: it is
+    raised at once."""
+    healthy = getattr(obj, "healthy", None)
+    if healthy is not None and not healthy():
+        raise AobError(f"autotune: the device failed while timing a candidate: {err}") from err
+
+
 def _fastest(trials, what):
     ran = [r for r in trials if r["ms"] is not None]
     if not ran:
@@ -115,6 +126,7 @@ def tune_batch(batch, noise=True, space=None, warmup=3, iters=10, use_cache=True
             batch.set_tuning(*(cand[k] for k in _BATCH_KEYS))
             ms = batch.time(noise=noise, warmup=warmup, iters=iters)
         except AobError as e:
+            _reraise_if_broken(batch, e)
             trials.append(dict(cand, ms=None, error=str(e)))
             if log:
                 log(f"batch tuning {cand}: rejected ({e})")
@@ -152,6 +164,7 @@ def tune_loop(loop, noise=True, space=None, warmup=3, iters=20, use_cache=True, 
             loop.set_mode(2, cand["fused_batch"])
             ms = loop.time(noise=noise, warmup=warmup, iters=iters)
         except AobError as e:
+            _reraise_if_broken(loop, e)
             trials.append(dict(cand, ms=None, error=str(e)))
             if log:
                 log(f"loop tuning {cand}: rejected ({e})")

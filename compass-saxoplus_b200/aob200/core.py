@@ -19,6 +19,16 @@ CENTRO_TYPES = {"cog": 0, "tcog": 1, "wcog": 2, "pyr": 3, "pyrhr": 3}
 PRECISIONS = {"f32": 0, "fp32": 0, "float32": 0, "bf16": 1, "bfloat16": 1, "fp8": 2, "e4m3": 2}
 
 
+def _device_ok() -> bool:
+    """True when a synchronisation of the legacy default stream succeeds (a
+    sticky CUDA error makes it fail)."""
+    try:
+        call("aob_stream_sync", None)
+        return True
+    except _lib.AobError:
+        return False
+
+
 class DeviceArray:
     """View of a device buffer owned by the library (the carma object role).
 
@@ -530,6 +540,11 @@ class Loop:
         call("aob_loop_time", self.h, 1 if noise else 0, int(warmup), int(iters), ctypes.addressof(ms))
         return float(ms.value)
 
+    def healthy(self) -> bool:
+        """False when the device context is broken (a sticky CUDA error makes the
+        synchronisation fail) or a bounded wait of the controller's kernels expired."""
+        return _device_ok() and self.ls.status() == 0
+
 
 class Batch:
     """Many SH loops advanced together by one persistent kernel launch per step.
@@ -608,3 +623,7 @@ class Batch:
         ms = ctypes.c_float()
         call("aob_batch_time", self.h, 1 if noise else 0, int(warmup), int(iters), ctypes.addressof(ms))
         return float(ms.value)
+
+    def healthy(self) -> bool:
+        """False when the device context is broken or a bounded wait expired."""
+        return _device_ok() and self.status() == 0

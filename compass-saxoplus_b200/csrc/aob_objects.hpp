@@ -202,6 +202,8 @@ struct aob_loop {
   uint32_t frame_host = 0;
   int host_io = 1;                       // 1: the fused kernel writes pinned host voltages itself
   float *io_volt = nullptr;              // device view of the caller's pinned voltages during a step
+  uint32_t test_grid_polls = 0;          // wait-expiry test: grid-barrier poll limit (0 = the default)
+  int test_absent_cta = -1;              // wait-expiry test: the CTA that never arrives (-1 = none)
   aob_loop(aob_sh *w, aob_centro *c, aob_ls *l);
   ~aob_loop();
   void device_step(bool noise, cudaStream_t s, bool frame_on_device);
@@ -238,6 +240,8 @@ struct aob_batch {
   aob::DevBuf<uint32_t> frames, status;
   aob::DevBuf<float> phase_all, volt_all;  // staging for host phases / gathered voltages
   cudaGraphExec_t graphs[2] = {nullptr, nullptr};
+  uint32_t test_dep_polls = 0;  // wait-expiry test: dependency-wait poll limit (0 = the default)
+  uint32_t test_dep_extra = 0;  // wait-expiry test: sensor items an MVM item waits for beyond its instance's
 
   explicit aob_batch(int device);
   ~aob_batch();

@@ -84,6 +84,8 @@ struct BatchArgs {
   uint32_t *status;
   int rows_max;  // MVM rows per item, upper bound
   int team;      // threads per sensor team (32, 64, 128 or 256)
+  uint32_t dep_polls;  // poll limit of an MVM item's dependency wait
+  uint32_t dep_extra;  // wait-expiry test: items waited for beyond the instance's sensor items (0)
 };
 
 __host__ __device__ inline size_t batch_bars_bytes(int rows) { return 128 * (((size_t)rows * 8 + 127) / 128); }
@@ -158,8 +160,9 @@ __device__ __forceinline__ void mvm_item(const BatchInst &I, int ii, int r0, int
   if (tid == 0) {
     int ok = 1;
     uint32_t i = 0;
-    while (ld_acquire_u32(&A.done[ii]) < (unsigned)I.nsensor) {
-      if (++i >= DEP_MAX_POLLS) {
+    const unsigned need = (unsigned)I.nsensor + A.dep_extra;
+    while (ld_acquire_u32(&A.done[ii]) < need) {
+      if (++i >= A.dep_polls) {
         ok = 0;
         atomicOr(A.status, (uint32_t)ERR_DEP_TIMEOUT);
         break;
@@ -562,6 +565,8 @@ void aob_batch::launch(bool staged, cudaStream_t s) {
   A.status = status.p;
   A.rows_max = rows_max;
   A.team = team_threads();
+  A.dep_polls = test_dep_polls ? test_dep_polls : DEP_MAX_POLLS;
+  A.dep_extra = test_dep_extra;
   if (ctas_per_sm == 0 || ctas_per_sm <= 2)
     batch_step_kernel<2><<<grid, BATCH_THREADS, smem, s>>>(A);
   else
@@ -688,6 +693,26 @@ int aob_batch_set_tuning(aob_batch *b, int subaps_per_item, int team_threads, in
 int aob_batch_use_graph(aob_batch *b, int enable) {
   BATCH_TRY BATCH_NEED(b);
   b->use_graph = enable != 0;
+  BATCH_END
+}
+int aob_batch_test_wait_expiry(aob_batch *b, uint32_t polls, int noise, void *stream) {
+  BATCH_TRY BATCH_NEED(b);
+  AOB_REQUIRE(polls >= 1, "aob_batch_test_wait_expiry: polls >= 1 required");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  struct Restore {
+    aob_batch *b;
+    bool g;
+    ~Restore() {
+      b->test_dep_polls = 0;
+      b->test_dep_extra = 0;
+      b->use_graph = g;
+    }
+  } restore{b, b->use_graph};
+  b->use_graph = false;  // the test values are kernel arguments: a direct launch
+  b->test_dep_polls = polls;
+  b->test_dep_extra = 1;
+  b->device_step(noise != 0, false, s);
+  AOB_CUDA(cudaStreamSynchronize(s));
   BATCH_END
 }
 int aob_batch_refresh(aob_batch *b) {

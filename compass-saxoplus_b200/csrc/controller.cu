@@ -438,11 +438,11 @@ void launch_mvm_t(const MvmArgs &A0, int grid, bool bulk, cudaStream_t s) {
     A.rows_per_cta = (A.nrow + grid - 1) / grid;
     const size_t sm = mvm_bars_bytes(A.rows_per_cta) + slope_bytes + (size_t)A.rows_per_cta * A.ld * sizeof(T) +
                       sizeof(float) * (MVM_THREADS / 32) * A.rows_per_cta;
-    AOB_CUDA(cudaFuncSetAttribute(ls_mvm_bulk_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    smem_opt_in(reinterpret_cast<const void *>(ls_mvm_bulk_kernel<T>), (int)sm);
     ls_mvm_bulk_kernel<T><<<grid, MVM_THREADS, sm, s>>>(A);
     AOB_LAUNCH_CHECK("ls_mvm_bulk_kernel");
   } else {
-    AOB_CUDA(cudaFuncSetAttribute(ls_mvm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slope_bytes));
+    smem_opt_in(reinterpret_cast<const void *>(ls_mvm_kernel<T>), (int)slope_bytes);
     ls_mvm_kernel<T><<<grid, MVM_THREADS, slope_bytes, s>>>(A);
     AOB_LAUNCH_CHECK("ls_mvm_kernel");
   }

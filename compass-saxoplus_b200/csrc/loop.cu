@@ -238,6 +238,34 @@ int aob_loop_set_host_io(aob_loop *l, int mode) {
   }
 }
 
+int aob_loop_test_wait_expiry(aob_loop *l, uint32_t polls, void *stream) {
+  try {
+    if (!l) throw Error("aob_loop_test_wait_expiry: null handle");
+    AOB_REQUIRE(polls >= 1, "aob_loop_test_wait_expiry: polls >= 1 required");
+    AOB_REQUIRE(l->ls->delay == 0.f, "aob_loop_test_wait_expiry: needs a controller without delay");
+    AOB_CUDA(cudaSetDevice(l->wfs->device));
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    AOB_REQUIRE(l->launch_fused(false, s, false, true), "aob_loop_test_wait_expiry: the fused kernel does not fit");
+    struct Restore {
+      aob_loop *l;
+      ~Restore() {
+        l->test_grid_polls = 0;
+        l->test_absent_cta = -1;
+      }
+    } restore{l};
+    l->test_grid_polls = polls;
+    l->test_absent_cta = 0;
+    AOB_REQUIRE(l->launch_fused(false, s, false, false), "aob_loop_test_wait_expiry: launch failed");
+    // CTA 0 never added its arrival: bring the counter back to a multiple of the grid
+    AOB_CUDA(cudaMemsetAsync(l->gbar.p, 0, sizeof(unsigned long long), s));
+    AOB_CUDA(cudaStreamSynchronize(s));
+    return AOB_OK;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return AOB_ERR;
+  }
+}
+
 int aob_loop_step(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream) {
   try {
     if (!l) throw Error("aob_loop_step: null handle");

@@ -96,14 +96,16 @@ __device__ __forceinline__ unsigned long long grid_arrive(unsigned long long *ct
   }
   return target;
 }
-// Waiting half: every thread of the CTA calls it with grid_arrive's result.
-__device__ __forceinline__ bool grid_wait(const unsigned long long *ctr, unsigned long long target, uint32_t *status) {
+// Waiting half: every thread of the CTA calls it with grid_arrive's result;
+// at most max_polls polls.
+__device__ __forceinline__ bool grid_wait(const unsigned long long *ctr, unsigned long long target, uint32_t *status,
+                                          uint32_t max_polls = GRID_MAX_POLLS) {
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
     int ok = 1;
     uint32_t i = 0;
     while (ld_relaxed_u64(ctr) < target) {
-      if (++i >= GRID_MAX_POLLS) {
+      if (++i >= max_polls) {
         ok = 0;
         atomicOr(status, (uint32_t)ERR_GRID_TIMEOUT);
         break;

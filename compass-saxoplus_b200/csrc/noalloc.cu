@@ -31,7 +31,10 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 static __device__ __align__(256) float g_extrude_scratch[NOALLOC_MAX_N + NOALLOC_MAX_N * NOALLOC_MAX_N];
 
 // Device address of g_extrude_scratch per device, filled on the first call made
-// for that device (host code may not use the symbol's name as a pointer).
+// for that device (host code may not use the symbol's name as a pointer).  The
+// address belongs to the device's primary context: after cudaDeviceReset (or
+// any teardown of that context) it is stale, and the process must not call
+// this entry point on that device again.
 float *g_scratch_ptr[NOALLOC_MAX_DEVICES] = {};
 std::mutex g_scratch_mutex;
 
@@ -69,6 +72,15 @@ extern "C" int aob_extrude_noalloc(float *dev_screen, int n, int nstencil, const
       throw aob::Error("aob_extrude_noalloc: direction must be +-1 (x) or +-2 (y)");
     if (layer_index < 0) throw aob::Error("aob_extrude_noalloc: negative layer index");
     if (device < 0 || device >= NOALLOC_MAX_DEVICES) throw aob::Error("aob_extrude_noalloc: device out of range");
+    // the caller's current device is put back on every return path
+    int prev = -1;
+    AOB_CUDA(cudaGetDevice(&prev));
+    struct Restore {
+      int dev;
+      ~Restore() {
+        if (dev >= 0) cudaSetDevice(dev);
+      }
+    } restore{prev};
     AOB_CUDA(cudaSetDevice(device));
     float *scratch = scratch_on(device);
     float *y = scratch;

@@ -56,6 +56,8 @@ struct RtcFusedArgs {
   int rows_per_cta;
   int batch;  // sub-apertures per CTA and round
   float *volt_host;  // caller's pinned host voltages (mapped), also written, or null
+  uint32_t grid_polls;  // poll limit of the grid-barrier wait
+  int absent_cta;       // test of the bounded wait: this CTA never arrives (-1: none)
 };
 
 __host__ __device__ inline size_t fused_bars_bytes(int rows) { return 128 * (((size_t)rows * 8 + 127) / 128); }
@@ -180,9 +182,11 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
   }
   issue_rows();  // a CTA without sub-apertures
   // ---- all slopes published ----
-  const unsigned long long ticket = grid_arrive(A.gbar, gridDim.x);
+  // (absent: the CTA a wait-expiry test keeps from arriving; it skips the MVM)
+  const bool absent = (int)blockIdx.x == A.absent_cta;
+  const unsigned long long ticket = absent ? 0ull : grid_arrive(A.gbar, gridDim.x);
   if (one_round && S1 > 0) sh_store_images(A.sh, blockIdx.x, gridDim.x, S1, shm + L.hdr, L, team);
-  const bool ok = grid_wait(A.gbar, ticket, A.status);
+  const bool ok = !absent && grid_wait(A.gbar, ticket, A.status, A.grid_polls);
   if (ok) {
     if (A.bump && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.bump, 1u);  // no round trip
     // slopes into shared memory, 16 bytes per load (L2 only: they were written by
@@ -410,6 +414,8 @@ bool aob_loop::launch_fused(bool noise, cudaStream_t s, bool frame_on_device, bo
   A.status = c->status.p;
   A.gbar = gbar.p;
   A.volt_host = io_volt;
+  A.grid_polls = test_grid_polls ? test_grid_polls : GRID_MAX_POLLS;
+  A.absent_cta = test_absent_cta;
   const int nsm = num_sms(w->device);
   const int grid = std::min(nsm, c->nactu);
   AOB_REQUIRE((int64_t)c->nactu * grid < (int64_t)1 << 32, "loop: too many actuators for the fused kernel");

@@ -204,13 +204,8 @@ int aob_sh::pick_batch() const {
 template <int NFFT, int PD>
 static void launch_sh(const ShKernelArgs &P, int nvalid, int S, size_t sm, cudaStream_t s) {
   const int grid = std::max(1, (nvalid + S - 1) / S);
-  // the attribute is set once per instantiation (a driver call per launch costs microseconds)
-  static size_t configured = 0;
-  if (sm > configured) {
-    AOB_CUDA(cudaFuncSetAttribute(sh_image_kernel<NFFT, PD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)std::max<size_t>(sm, 48 * 1024)));
-    configured = std::max<size_t>(sm, 48 * 1024);
-  }
+  // opt-in per (kernel, device), only ever raised (a driver call per launch costs microseconds)
+  smem_opt_in(reinterpret_cast<const void *>(sh_image_kernel<NFFT, PD>), (int)std::max<size_t>(sm, 48 * 1024));
   sh_image_kernel<NFFT, PD><<<grid, SH_THREADS, sm, s>>>(P, S);
 }
 

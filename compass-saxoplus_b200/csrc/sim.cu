@@ -183,7 +183,7 @@ void aob_atmos::Layer::extrude(int dir, int layer_index, cudaStream_t s) {
   const uint64_t sd = (uint64_t)seed;
   const int threads = 256;
   const int rows_per_cta = threads / 32;
-  const int grid = std::max(1, std::min((n + rows_per_cta - 1) / rows_per_cta, 2 * num_sms(0)));
+  const int grid = std::max(1, std::min((n + rows_per_cta - 1) / rows_per_cta, 2 * num_sms(device)));
   const size_t sm = sizeof(float) * (nst + n);
   extrude_gemv_kernel<<<grid, threads, sm, s>>>(src, n, nst, Arm.p, Brm.p, ist, x0ref, amplitude,
                                                  (uint32_t)(sd & 0xffffffffu), (uint32_t)(sd >> 32),
@@ -207,6 +207,7 @@ int aob_atmos::add_screen(int dim, int nst, float r0_pix, float alt, float dx, f
   AOB_CUDA(cudaSetDevice(device));
   layers.emplace_back(new Layer(dim, nst, r0_pix, alt, dx, dy, seed));
   Layer &L = *layers.back();
+  L.device = device;
   // A: dim x nst and B: dim x dim column-major (the reference's layout) -> row-major copies
   std::vector<float> ar((size_t)dim * nst), br((size_t)dim * dim);
   for (int i = 0; i < dim; ++i) {

@@ -37,6 +37,7 @@ struct aob_atmos {
     int64_t seed;
     uint64_t counter = 0;  // extrusions so far (noise stream counter)
     int cur = 0;           // which of the two screens is current
+    int device = 0;        // the atmosphere's device (grid sizing)
     aob::DevBuf<float> scr[2], Arm, Brm, ytmp;
     aob::DevBuf<uint32_t> istx, isty;
     Layer(int dim, int nst, float r0, float alt, float dx, float dy, int64_t seed);

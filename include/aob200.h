@@ -10,8 +10,8 @@
  * is at x + y*n.
  *
  * Each entry point names the reference interface it replaces (paths within
- * the reference project).  The Python package `aob200` (and the binding shown
- * in INTEGRATION.md) binds exactly these symbols with ctypes.
+ * the reference project).  The Python package `aob200` binds exactly these
+ * symbols with ctypes.
  */
 #ifndef AOB200_H
 #define AOB200_H
@@ -347,7 +347,12 @@ int aob_kolmo_factor_ab(int device, int n, int nst, const double *zz, const doub
  * loads the library until exit) shared by all calls: calls that overlap on the
  * GPU (other streams, other host threads) race on it -- order them.  The first
  * call on a device looks the array's address up (cudaGetSymbolAddress); make
- * that first call before any stream capture. */
+ * that first call before any stream capture.  The address is kept for the
+ * life of the process: after cudaDeviceReset (or another teardown of the
+ * device's primary context) do not call this entry point on that device
+ * again.  The stencil indexes are not checked on the device (a caller
+ * precondition, as stated above).  The caller's current device is left as it
+ * was. */
 #define AOB_NOALLOC_EXTRUDE_MAX_N 512
 int aob_extrude_noalloc(float *dev_screen, int n, int nstencil, const float *dev_A_rows,
                         const float *dev_B_rows, const uint32_t *dev_stencil, int direction, float amplitude,
@@ -427,6 +432,16 @@ int aob_loop_set_mode(aob_loop *l, int mode, int fused_batch);
  * memory (d_voltage) for the DMs. */
 int aob_loop_set_host_io(aob_loop *l, int mode);
 
+/* Test of the bounded grid-barrier wait (no counterpart in the reference):
+ * one noise-free fused step in which CTA 0 never arrives at the barrier, so
+ * the other CTAs' waits (at most `polls` polls each) expire.  Every CTA then
+ * skips the MVM and returns, the kernel sets bit 1 (2, grid wait expired) of
+ * the controller's status word (aob_ls_status), the arrival counter is
+ * re-armed on the stream and the call waits for the stream.  The commands and
+ * voltages are left as they were; later steps run normally.  Needs a
+ * configuration that runs the fused kernel and a controller with delay 0. */
+int aob_loop_test_wait_expiry(aob_loop *l, uint32_t polls, void *stream);
+
 /* ---- batched Monte Carlo: many loops, one persistent launch per step --- *
  * No counterpart in the reference, where each simulation is its own process
  * stepping its own objects (CompassSupervisor.next, shesha/shesha/supervisor/
@@ -454,6 +469,12 @@ int aob_batch_add(aob_batch *b, aob_loop *loop);
 int aob_batch_set_tuning(aob_batch *b, int subaps_per_item, int team_threads, int mvm_kb, int lag, int ctas_per_sm,
                          int order);
 int aob_batch_use_graph(aob_batch *b, int enable);
+/* Test of the bounded dependency wait: one step (direct launch) in which every
+ * MVM item waits for one sensor item more than its instance has, so each such
+ * wait expires after `polls` polls, the item skips its rows and the status
+ * word gets bit 2 (4).  The queue re-arms itself as after any step; the status
+ * word is cleared by the next rebuild (aob_batch_refresh).  Waits for the stream. */
+int aob_batch_test_wait_expiry(aob_batch *b, uint32_t polls, int noise, void *stream);
 int aob_batch_refresh(aob_batch *b);
 /* One step of every loop with phases from each sensor's own device buffer. */
 int aob_batch_step(aob_batch *b, int noise, void *stream);

@@ -1,7 +1,7 @@
 """Generate golden fixtures by running the reference's own Python init code.
 
 This script is run by hand in a container where the reference checkout is
-present (default path below, override with ``AO_REFERENCE``).  It imports the
+present; ``AO_REFERENCE`` names its directory (the one holding ``shesha/``).  It imports the
 reference's ``shesha`` package with small stub modules standing in for its
 compiled ``carma``/``sutra`` extensions and for optional third-party packages
 (``aenum``, ``h5py``, ``astropy``) that the init functions used here never
@@ -27,7 +27,9 @@ import types
 
 import numpy as np
 
-REF = os.environ.get("AO_REFERENCE", "/root/reference")
+REF = os.environ.get("AO_REFERENCE")
+if not REF:
+    raise SystemExit("make_golden.py: set AO_REFERENCE to the reference checkout (the directory holding shesha/)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

@@ -59,3 +59,20 @@ def test_skips_rejected_candidates_and_caches_the_fastest(cache):
 def test_raises_when_no_candidate_runs(cache):
     with pytest.raises(AobError, match="no batch tuning candidate ran"):
         autotune.tune_batch(FakeBatch(reject_all=True), use_cache=False)
+
+
+def test_a_failure_that_breaks_the_device_is_raised_at_once(cache):
+    class BrokenBatch(FakeBatch):
+        """The first timing fails and leaves the object unhealthy (as a sticky
+        CUDA error or an expired bounded wait would)."""
+
+        def time(self, noise=True, warmup=3, iters=10):
+            raise AobError("aob_batch_time: an illegal memory access was encountered")
+
+        def healthy(self):
+            return False
+
+    b = BrokenBatch()
+    with pytest.raises(AobError, match="device failed while timing"):
+        autotune.tune_batch(b, use_cache=False)
+    assert b.timed == []

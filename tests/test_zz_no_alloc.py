@@ -15,8 +15,6 @@ import ctypes
 import numpy as np
 import pytest
 
-from helpers import rel_rms
-
 pytestmark = pytest.mark.gpu
 
 
@@ -62,7 +60,8 @@ def test_noalloc_extrusion_matches_atmosphere_move():
         torch.cuda.synchronize()
         got = mine.cpu().numpy().reshape(n, n, order="F")
         ref = atm.screen_host(0)
-        assert rel_rms(got, ref) < 1e-6
+        # the same two kernels on the same operands: the screens are equal bit for bit
+        np.testing.assert_array_equal(got, ref)
 
 
 def test_noalloc_rejects_screens_beyond_the_fixed_scratch():
