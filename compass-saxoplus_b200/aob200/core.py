@@ -318,7 +318,8 @@ class Centroider:
             call("aob_centro_attach_wfs", self.h, wfs.h if wfs is not None else None)
 
     def set_pyr_method(self, method):
-        """0 nosin_global (default), 1 sin_global, 2 nosin_local, 3 sin_local."""
+        """The reference's encoding (Method_CoG, sutra_centroider_pyr.hpp:27-34): 0 sinus global,
+        1 nosinus global (the default), 2 sinus local, 3 nosinus local."""
         call("aob_centro_set_pyr_method", self.h, int(method))
 
     def set_pyr_thresh(self, thresh):

@@ -115,7 +115,7 @@ struct aob_centro {
   aob_sh *wfs = nullptr;
   aob_pyr *pyr = nullptr;       // pyramid centroider: the sensor whose image it reads
   float valid_thresh = 1.e-4f;  // pyramid: flux below which slopes are 0
-  int pyr_method = 0;           // pyramid: bit 0 sine of the ratio, bit 1 per-sub-aperture flux
+  int pyr_method = 1;           // pyramid: 0 sinus global, 1 nosinus global, 2 sinus local, 3 nosinus local
   aob::DevBuf<int32_t> validx, validy;
   aob::DevBuf<float> ref, weights, intensities;
   int weights_per_sub = 0;  // 0: one npix^2 map, 1: npix^2*nvalid

@@ -84,7 +84,7 @@ __global__ void tcog_writeback_kernel(float *img, int size, const int32_t *valid
 // Pyramid slopes (pyr2slopes_krnl, libsutra/src.cu/sutra_centroider_pyr.cu:27-69,
 // flux as intensities_krnl, sutra_wfs.cu:2041-2054).  Quadrant k of valid
 // sub-aperture i is the binned-image pixel (validx[i + k nvalid], validy[...]).
-// With the global method (the reference default, nosin_global) every
+// With a global method (the reference default is nosinus global, method 1) every
 // sub-aperture is normalised by the mean flux (fillvalues, carma_obj.cu:194-201);
 // the sum runs in a fixed order (per-thread partial sums, then a tree), so
 // the slopes are deterministic.  One CTA.
@@ -94,7 +94,9 @@ __global__ void __launch_bounds__(PYR_SLOPE_THREADS)
     pyr_slopes_kernel(const float *img, int ns, const int32_t *vx, const int32_t *vy, int nvalid, float scale,
                       float thresh, int method, const float *ref, int order, float *slopes, float *inten) {
   __shared__ float red[PYR_SLOPE_THREADS];
-  const bool sinus = method & 1, local = method & 2;
+  // the reference's Method_CoG(uint8_t) (sutra_centroider_pyr.hpp:27-34): 0 sinus global,
+  // 1 nosinus global, 2 sinus local, 3 nosinus local
+  const bool sinus = (method & 1) == 0, local = method > 1;
   auto quad = [&](int i, float *q) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) q[k] = img[vx[i + k * nvalid] + vy[i + k * nvalid] * ns];

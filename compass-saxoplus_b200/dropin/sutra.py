@@ -197,7 +197,8 @@ class Centroider:
         self._c.set_threshold(float(threshold))
 
     def set_pyr_method(self, method):
-        """Pyramid slopes (centroider_pyr.cpp): 0 nosin_global, 1 sin_global, 2 nosin_local, 3 sin_local."""
+        """Pyramid slopes as the reference's Method_CoG decodes them (sutra_centroider_pyr.hpp:27-34):
+        0 sinus global, 1 nosinus global (default), 2 sinus local, 3 nosinus local."""
         self._c.set_pyr_method(int(method))
 
     def set_pyr_thresh(self, thresh):

@@ -167,10 +167,11 @@ int aob_centro_set_slope_order(aob_centro *c, int order);
  * libsutra/src.cpp/sutra_centroider_pyr.cpp:101-130): reads the binned image
  * of the attached pyramid sensor; its valid positions are 4 * nvalid pixels
  * (quadrant k of sub-aperture i at entry i + k nvalid).  method (set_pyr_method,
- * python_module/sutra/src/centroider_pyr.cpp:35-64): bit 0 = sine of the
- * normalised difference, bit 1 = per-sub-aperture flux (default 0 = the
- * reference's nosin_global).  thresh: flux below which the slopes are 0
- * (reference default 1e-4). */
+ * python_module/sutra/src/centroider_pyr.cpp:35-64), decoded as the reference's
+ * Method_CoG(uint8_t) does (libsutra/include/sutra_centroider_pyr.hpp:27-34):
+ * 0 sinus global, 1 nosinus global (the default), 2 sinus local (per
+ * sub-aperture flux), 3 nosinus local.  thresh: flux below which the slopes
+ * are 0 (reference default 1e-4). */
 int aob_centro_attach_pyr(aob_centro *c, aob_pyr *p);
 int aob_centro_set_pyr_method(aob_centro *c, int method);
 int aob_centro_set_pyr_thresh(aob_centro *c, float thresh);

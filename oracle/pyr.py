@@ -64,15 +64,20 @@ def comp_image(phase, pupil, g, lam_um, nphot, weights=None, noise=-1.0, frame=0
     return b
 
 
-def slopes(img, validsubsx, validsubsy, nvalid, scale, ref=None, thresh=1e-4, method=0):
-    """Pyramid slopes (untied order) and the flux used for each sub-aperture."""
+def slopes(img, validsubsx, validsubsy, nvalid, scale, ref=None, thresh=1e-4, method=1):
+    """Pyramid slopes (untied order) and the flux used for each sub-aperture.
+
+    ``method`` as the reference decodes it (Method_CoG(uint8_t),
+    libsutra/include/sutra_centroider_pyr.hpp:27-34): 0 sinus global, 1 nosinus
+    global (the default, sutra_centroider_pyr.cpp:43), 2 sinus local, 3 nosinus
+    local."""
     b = np.asarray(img, np.float64)
     q = [b[validsubsx[k * nvalid:(k + 1) * nvalid], validsubsy[k * nvalid:(k + 1) * nvalid]] for k in range(4)]
     flux = q[0] + q[1] + q[2] + q[3]
-    f = flux if (method & 2) else np.full(nvalid, flux.sum() / nvalid)
+    f = flux if method > 1 else np.full(nvalid, flux.sum() / nvalid)
     tx = ((q[0] + q[3]) - (q[1] + q[2])) / f
     ty = ((q[0] + q[2]) - (q[1] + q[3])) / f
-    if method & 1:
+    if method % 2 == 0:
         tx, ty = np.sin(np.pi * tx / 2), np.sin(np.pi * ty / 2)
     s = np.concatenate([scale * tx, scale * ty])
     s[np.concatenate([f < thresh, f < thresh])] = 0.0
