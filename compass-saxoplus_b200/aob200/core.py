@@ -15,7 +15,8 @@ import numpy as np
 from . import _lib
 from ._lib import addr, call, d2h, h2d, host_array
 
-CENTRO_TYPES = {"cog": 0, "tcog": 1, "wcog": 2, "pyr": 3, "pyrhr": 3}
+CENTRO_TYPES = {"cog": 0, "tcog": 1, "wcog": 2, "pyr": 3, "pyrhr": 3, "maskedpix": 4, "bpcog": 5}
+COMMAND_LAWS = {"integrator": 1, "modal_integrator": 2, "2matrices": 3}
 PRECISIONS = {"f32": 0, "fp32": 0, "float32": 0, "bf16": 1, "bfloat16": 1, "fp8": 2, "e4m3": 2}
 
 
@@ -289,7 +290,10 @@ class PyrWfs:
 
 
 class Centroider:
-    """CoG / tCoG / wCoG / pyramid centroider (SutraCentroider*)."""
+    """CoG / tCoG / wCoG / bpCoG / pyramid / masked-pixel centroider (SutraCentroider*).
+
+    A masked-pixel centroider (``maskedpix``) takes ``nvalid`` = the number of
+    valid pixels (4 x the pyramid's sub-apertures) and writes one slope per pixel."""
 
     def __init__(self, nvalid, offset, scale, typec="cog", device=0, wfs: ShWfs | None = None):
         self.h = ctypes.c_void_p()
@@ -324,6 +328,14 @@ class Centroider:
 
     def set_pyr_thresh(self, thresh):
         call("aob_centro_set_pyr_thresh", self.h, float(thresh))
+
+    def set_nmax(self, nmax):
+        """bpCoG: the pixel of rank nmax (0 = the brightest) sets the threshold."""
+        call("aob_centro_set_nmax", self.h, int(nmax))
+
+    @property
+    def nslopes(self) -> int:
+        return self.nvalid if self.type == "maskedpix" else 2 * self.nvalid
 
     def set_npix(self, npix):
         call("aob_centro_set_npix", self.h, int(npix))
@@ -383,13 +395,47 @@ class Centroider:
 
 
 class LsController:
-    """Least-squares controller (SutraControllerLs + SutraController)."""
+    """Least-squares controller (SutraControllerLs + SutraController), or with
+    ``kind="generic"`` the generic controller (SutraControllerGeneric): the same
+    buffers and voltage stage, its command laws ("integrator" with a leaky
+    factor and optional pseudo-open-loop slopes, "modal_integrator",
+    "2matrices") instead of the LS integrator."""
 
-    def __init__(self, nslope, nactu, delay=0.0, device=0):
+    def __init__(self, nslope, nactu, delay=0.0, device=0, kind="ls"):
         self.h = ctypes.c_void_p()
-        call("aob_ls_create", ctypes.addressof(self.h), int(device), int(nslope), int(nactu), float(delay))
+        if kind not in ("ls", "generic"):
+            raise ValueError(f"controller kind must be 'ls' or 'generic', not {kind!r}")
+        fn = "aob_ls_create" if kind == "ls" else "aob_generic_create"
+        call(fn, ctypes.addressof(self.h), int(device), int(nslope), int(nactu), float(delay))
+        self.kind = kind
         self.nslope, self.nactu = int(nslope), int(nactu)
         self.precision = 0
+
+    def set_commandlaw(self, law):
+        call("aob_ls_set_commandlaw", self.h, COMMAND_LAWS[law] if isinstance(law, str) else int(law))
+
+    def set_leaky_factor(self, f):
+        call("aob_ls_set_leaky_factor", self.h, float(f))
+
+    def set_polc(self, on):
+        call("aob_ls_set_polc", self.h, 1 if on else 0)
+
+    def set_decay_factor(self, d):
+        self._vec("aob_ls_set_decay_factor", d)
+
+    def set_matE(self, m):
+        m = np.asarray(m)
+        if m.shape != (self.nactu, self.nactu):
+            raise ValueError(f"matE must be ({self.nactu}, {self.nactu})")
+        self._vec("aob_ls_set_matE", m)
+
+    def law(self) -> dict:
+        k, l, p = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        f = ctypes.c_float()
+        call("aob_ls_get_kind", self.h, *[ctypes.addressof(x) for x in (k, l, f, p)])
+        names = {v: n for n, v in COMMAND_LAWS.items()}
+        return dict(kind="generic" if k.value else "ls", law=names.get(l.value, "ls"), leaky=f.value,
+                    polc=bool(p.value))
 
     def __del__(self):
         h = getattr(self, "h", None)
@@ -474,6 +520,10 @@ class LsController:
 
     def reset_perturb(self):
         call("aob_ls_reset_perturb", self.h)
+
+    def apply_perturb(self, stream=None):
+        """com_clipped += the current row of every enabled perturbation buffer."""
+        call("aob_ls_apply_perturb", self.h, stream)
 
     def svdec_imat(self):
         call("aob_ls_svdec_imat", self.h)

@@ -116,6 +116,7 @@ struct aob_centro {
   aob_pyr *pyr = nullptr;       // pyramid centroider: the sensor whose image it reads
   float valid_thresh = 1.e-4f;  // pyramid: flux below which slopes are 0
   int pyr_method = 1;           // pyramid: 0 sinus global, 1 nosinus global, 2 sinus local, 3 nosinus local
+  int nmax = 0;                 // bpcog: rank of the threshold pixel (set_nmax)
   aob::DevBuf<int32_t> validx, validy;
   aob::DevBuf<float> ref, weights, intensities;
   int weights_per_sub = 0;  // 0: one npix^2 map, 1: npix^2*nvalid
@@ -129,6 +130,8 @@ struct aob_centro {
   uint64_t fused_params_gen = ~0ull;
 
   aob_centro(int device, int type, int nvalid, float offset, float scale);
+  // slopes this centroider writes: one per valid pixel (maskedpix), else 2 per sub-aperture
+  int nslopes() const { return type == AOB_CENTRO_MASKEDPIX ? nvalid : 2 * nvalid; }
   void touch() { ++params_gen; }
   bool fused_ready() const;
   void get_cog(float *dev_slopes, cudaStream_t s);
@@ -169,6 +172,13 @@ struct aob_ls {
   };
   std::map<std::string, Perturb> perturb;
 
+  // generic controller (SutraControllerGeneric): kind AOB_CTRL_GENERIC and its command law
+  int kind = AOB_CTRL_LS;
+  int law = 0;
+  float leaky = 1.f;
+  int polc = 0;
+  aob::DevBuf<float> decay, matE_rows, imat_rows, ol_meas, com1_tmp;
+
   aob_ls(int device, int nslope, int nactu, float delay);
   float *com() { return ring.back().p; }
   void set_delay(float d);
@@ -178,6 +188,11 @@ struct aob_ls {
   void launch_mvm(struct aob::MvmArgs &A, cudaStream_t s);
   void comp_voltage(cudaStream_t s);
   void clip(cudaStream_t s);
+  void apply_perturb(cudaStream_t s);
+  void make_generic();
+  void generic_comp_com(cudaStream_t s, uint32_t *bump);
+  void set_matE(const float *h_colmajor);
+  void set_imat_rows(const float *h_colmajor);
   void svdec_imat();
   void build_cmat(int nfilt);
 };

@@ -2,6 +2,7 @@
 // catches exceptions and returns AOB_OK / AOB_ERR; the message is kept per
 // thread for aob_last_error().
 
+#include <memory>
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -278,9 +279,22 @@ int aob_centro_attach_wfs(aob_centro *c, aob_sh *h) {
 int aob_centro_attach_pyr(aob_centro *c, aob_pyr *p) {
   AOB_API_BEGIN
   NEED(c);
-  if (c->type != AOB_CENTRO_PYR) throw Error("centro.attach_pyr: not a pyramid centroider");
-  if (p && p->nvalid != c->nvalid) throw Error("centro.attach_pyr: nvalid differs from the sensor's");
+  if (c->type != AOB_CENTRO_PYR && c->type != AOB_CENTRO_MASKEDPIX)
+    throw Error("centro.attach_pyr: not a pyramid or masked-pixel centroider");
+  if (p && c->type == AOB_CENTRO_PYR && p->nvalid != c->nvalid)
+    throw Error("centro.attach_pyr: nvalid differs from the sensor's");
+  if (p && c->type == AOB_CENTRO_MASKEDPIX && 4 * p->nvalid != c->nvalid)
+    throw Error("centro.attach_pyr: a masked-pixel centroider needs nvalid = 4 * the sensor's nvalid");
   c->pyr = p;
+  c->touch();
+  AOB_API_END
+}
+int aob_centro_set_nmax(aob_centro *c, int nmax) {
+  AOB_API_BEGIN
+  NEED(c);
+  if (c->type != AOB_CENTRO_BPCOG) throw Error("centro.set_nmax: not a bpcog centroider");
+  if (nmax < 0 || nmax >= 1024) throw Error("centro.set_nmax: nmax must be in [0, 1024)");
+  c->nmax = nmax;
   c->touch();
   AOB_API_END
 }
@@ -355,7 +369,7 @@ int aob_centro_set_centroids_ref(aob_centro *c, const float *ref) {
   AOB_API_BEGIN
   NEED(c); NEED(ref);
   AOB_CUDA(cudaSetDevice(c->device));
-  c->ref.upload(ref, 2 * (int64_t)c->nvalid);
+  c->ref.upload(ref, c->nslopes());
   c->touch();
   AOB_API_END
 }
@@ -448,6 +462,68 @@ int aob_ls_create(aob_ls **out, int device, int nslope, int nactu, float delay) 
   *out = new aob_ls(device, nslope, nactu, delay);
   AOB_API_END
 }
+int aob_generic_create(aob_ls **out, int device, int nslope, int nactu, float delay) {
+  AOB_API_BEGIN
+  NEED(out);
+  *out = nullptr;
+  std::unique_ptr<aob_ls> c(new aob_ls(device, nslope, nactu, delay));
+  c->make_generic();
+  *out = c.release();
+  AOB_API_END
+}
+int aob_ls_get_kind(aob_ls *c, int *kind, int *law, float *leaky, int *polc) {
+  AOB_API_BEGIN
+  NEED(c);
+  if (kind) *kind = c->kind;
+  if (law) *law = c->law;
+  if (leaky) *leaky = c->leaky;
+  if (polc) *polc = c->polc;
+  AOB_API_END
+}
+int aob_ls_set_commandlaw(aob_ls *c, int law) {
+  AOB_API_BEGIN
+  NEED(c);
+  if (c->kind != AOB_CTRL_GENERIC) throw Error("set_commandlaw: not a generic controller");
+  if (law != AOB_LAW_INTEGRATOR && law != AOB_LAW_MODAL_INTEGRATOR && law != AOB_LAW_2MATRICES)
+    throw Error("set_commandlaw: law must be integrator (1), modal_integrator (2) or 2matrices (3)");
+  c->law = law;
+  AOB_API_END
+}
+int aob_ls_set_leaky_factor(aob_ls *c, float leaky) {
+  AOB_API_BEGIN
+  NEED(c);
+  if (c->kind != AOB_CTRL_GENERIC) throw Error("set_leaky_factor: not a generic controller");
+  c->leaky = leaky;
+  AOB_API_END
+}
+int aob_ls_set_polc(aob_ls *c, int polc) {
+  AOB_API_BEGIN
+  NEED(c);
+  if (c->kind != AOB_CTRL_GENERIC) throw Error("set_polc: not a generic controller");
+  c->polc = polc ? 1 : 0;
+  AOB_API_END
+}
+int aob_ls_set_decay_factor(aob_ls *c, const float *decay) {
+  AOB_API_BEGIN
+  NEED(c); NEED(decay);
+  if (c->kind != AOB_CTRL_GENERIC) throw Error("set_decayFactor: not a generic controller");
+  AOB_CUDA(cudaSetDevice(c->device));
+  c->decay.upload(decay, c->nactu);
+  AOB_API_END
+}
+int aob_ls_apply_perturb(aob_ls *c, void *stream) {
+  AOB_API_BEGIN
+  NEED(c);
+  c->apply_perturb(S(stream));
+  AOB_API_END
+}
+int aob_ls_set_matE(aob_ls *c, const float *matE) {
+  AOB_API_BEGIN
+  NEED(c); NEED(matE);
+  if (c->kind != AOB_CTRL_GENERIC) throw Error("set_matE: not a generic controller");
+  c->set_matE(matE);
+  AOB_API_END
+}
 int aob_ls_destroy(aob_ls *c) {
   AOB_API_BEGIN
   if (c) {
@@ -472,6 +548,7 @@ int aob_ls_set_imat(aob_ls *c, const float *imat) {
   AOB_CUDA(cudaSetDevice(c->device));
   if (!c->imat.p) c->imat.alloc((int64_t)c->nslope * c->nactu);
   c->imat.upload(imat, c->imat.n);
+  if (c->kind == AOB_CTRL_GENERIC) c->set_imat_rows(imat);  // pseudo-open-loop slopes
   AOB_API_END
 }
 int aob_ls_set_modal_gains(aob_ls *c, const float *g) {

@@ -12,6 +12,7 @@
 // after that or a parameter was modified.
 
 #include <algorithm>
+#include <vector>
 
 #include "aob_objects.hpp"
 
@@ -160,6 +161,113 @@ __global__ void __launch_bounds__(PYR_SLOPE_THREADS)
   }
 }
 
+// Masked-pixel slopes (get_maskedPix_krnl, libsutra/src.cu/sutra_centroider_maskedPix.cu:26-38,
+// with fill_intensities_krnl :47-56 and the CUB sum of sutra_centroider_maskedPix.cpp:129-134):
+// every valid pixel of the image is a "slope", normalised by the mean flux of
+// the valid pixels: s[i] = img[i] / sum * n - ref[i] (-ref[i] when the sum is 0;
+// the reference initialises ref to 1).  intens[i] receives the pixel values and
+// intens[n] their sum.  One CTA; the sum runs in a fixed order.
+constexpr int MASKED_THREADS = 1024;
+__global__ void __launch_bounds__(MASKED_THREADS)
+    masked_pix_kernel(const float *img, int ns, const int32_t *vx, const int32_t *vy, int n, const float *ref,
+                      float *slopes, float *intens) {
+  __shared__ float red[MASKED_THREADS];
+  float part = 0.f;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float v = img[vx[i] + (int64_t)vy[i] * ns];
+    intens[i] = v;
+    part += v;
+  }
+  red[threadIdx.x] = part;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  const float sum = red[0];
+  if (threadIdx.x == 0) intens[n] = sum;
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    slopes[i] = sum != 0.f ? img[vx[i] + (int64_t)vy[i] * ns] / sum * (float)n - ref[i] : -ref[i];
+}
+
+// Brightest-pixel CoG (centroids<> of libsutra/src.cu/sutra_centroider_bpcog.cu:24-80):
+// the reference sorts a sub-aperture's npix^2 pixels -- padded with zeros up
+// to its CUB block size (16, 36, 64, 100, 144, 256, 512 or 1024) -- in
+// descending order, takes the value of rank nmax as the threshold, keeps
+// pix - threshold where pix > threshold (0 elsewhere), writes those values back
+// into the image and takes their centre of gravity.  Here one warp handles a
+// sub-aperture and finds the value of rank nmax by counting, for each pixel,
+// the larger ones (the padding zeros included).
+__global__ void bpcog_kernel(float *img, int size, const int32_t *validx, const int32_t *validy, int nvalid,
+                             int npix, int nmax, int npad, float scale, float offset, const float *ref, int order,
+                             float *slopes, float *intens) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int npix2 = npix * npix;  // <= 1024 (host-checked)
+  const int64_t lim = (int64_t)size * size;
+  for (int k = warp; k < nvalid; k += nwarps) {
+    const int vx = validx[k], vy = validy[k];
+    auto pix = [&](int p) -> float {
+      const int64_t idim = (int64_t)(p % npix + vx) + (int64_t)(p / npix + vy) * size;
+      return (idim >= 0 && idim < lim) ? img[idim] : 0.f;
+    };
+    // threshold: the value v with (#larger) <= nmax < (#larger) + (#equal), over
+    // the pixels and npad zeros; when no pixel holds rank nmax, a padding zero does
+    float thr = 0.f;
+    bool found = false;
+    for (int c0 = 0; c0 < npix2 && !found; c0 += 32) {
+      const int c = c0 + lane;
+      const float v = c < npix2 ? pix(c) : 0.f;
+      int gt = 0, eq = 0;
+      for (int p = 0; p < npix2; ++p) {
+        const float u = pix(p);
+        gt += u > v;
+        eq += u == v;
+      }
+      if (v < 0.f) gt += npad;
+      if (v == 0.f) eq += npad;
+      const bool hit = c < npix2 && gt <= nmax && nmax < gt + eq;
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
+      if (m) {
+        thr = __shfl_sync(0xffffffffu, v, __ffs(m) - 1);
+        found = true;
+      }
+    }
+    float cs = 0.f, cx = 0.f, cy = 0.f;
+    for (int p = lane; p < npix2; p += 32) {
+      const int x = p % npix, y = p / npix;
+      const int64_t idim = (int64_t)(x + vx) + (int64_t)(y + vy) * size;
+      if (idim < 0 || idim >= lim) continue;
+      const float v = img[idim];
+      const float d = v > thr ? v - thr : 0.f;
+      img[idim] = d;
+      cs += d;
+      cx = fmaf(d, (float)x, cx);
+      cy = fmaf(d, (float)y, cy);
+    }
+    cs = warp_sum(cs);
+    cx = warp_sum(cx);
+    cy = warp_sum(cy);
+    if (lane == 0) {
+      const int ix = order ? 2 * k : k;
+      const int iy = order ? 2 * k + 1 : k + nvalid;
+      slopes[ix] = (cx / (cs + 1.e-6f) - offset) * scale - ref[ix];
+      slopes[iy] = (cy / (cs + 1.e-6f) - offset) * scale - ref[iy];
+      intens[k] = cs;
+    }
+  }
+}
+
+// CUB block size the reference's bpcog launch picks for npix^2 pixels
+// (get_centroids, sutra_centroider_bpcog.cu:86-135)
+static int bpcog_block(int n) {
+  const int sizes[] = {16, 36, 64, 100, 144, 256, 512, 1024};
+  for (int b : sizes)
+    if (n <= b) return b;
+  return n;
+}
+
 __global__ void calib_kernel(const float *raw, float *cal, const float *dark, const float *flat, int64_t n) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
     cal[t] = (raw[t] - dark[t]) * flat[t];
@@ -172,11 +280,15 @@ using namespace aob;
 aob_centro::aob_centro(int device_, int type_, int nvalid_, float offset_, float scale_)
     : device(device_), type(type_), nvalid(nvalid_), offset(offset_), scale(scale_) {
   AOB_REQUIRE(nvalid > 0, "centroider: nvalid must be > 0");
-  AOB_REQUIRE(type >= 0 && type <= 3, "centroider: unknown type");
+  AOB_REQUIRE(type >= 0 && type <= 5, "centroider: unknown type");
   AOB_CUDA(cudaSetDevice(device));
-  ref.alloc(2 * (int64_t)nvalid);
-  intensities.alloc(nvalid);
-  fused_slopes.alloc(2 * (int64_t)nvalid);
+  ref.alloc(nslopes());
+  intensities.alloc(type == AOB_CENTRO_MASKEDPIX ? nvalid + 1 : nvalid);  // maskedpix: pixels, then their sum
+  fused_slopes.alloc(nslopes());
+  if (type == AOB_CENTRO_MASKEDPIX) {  // the reference starts its reference slopes at 1 (maskedPix.cpp:44-45)
+    std::vector<float> one(nvalid, 1.f);
+    ref.upload(one.data(), nvalid);
+  }
 }
 
 bool aob_centro::fused_ready() const {
@@ -200,6 +312,47 @@ void aob_centro::calibrate(cudaStream_t s) {
 }
 
 void aob_centro::get_cog(float *dev_slopes, cudaStream_t s) {
+  if (type == AOB_CENTRO_MASKEDPIX) {
+    AOB_REQUIRE(validx.p != nullptr && validx.n >= nvalid, "get_maskedPix: valid pixel positions not loaded");
+    const float *im;
+    int ns;
+    if (pyr) {
+      im = pyr->binimg.p;
+      ns = pyr->nbin();
+    } else {
+      AOB_REQUIRE(img.p != nullptr, "get_maskedPix: no image (attach a pyramid sensor or load_img + calibrate_img)");
+      im = img.p;
+      ns = img_m;
+    }
+    AOB_CUDA(cudaSetDevice(device));
+    masked_pix_kernel<<<1, MASKED_THREADS, 0, s>>>(im, ns, validx.p, validy.p, nvalid, ref.p, dev_slopes,
+                                                   intensities.p);
+    AOB_LAUNCH_CHECK("masked_pix_kernel");
+    return;
+  }
+  if (type == AOB_CENTRO_BPCOG) {
+    AOB_REQUIRE(npix > 0 && npix * npix <= 1024, "get_bpcog: npix not set (or npix^2 > 1024)");
+    AOB_REQUIRE(validx.p != nullptr && validx.n >= nvalid, "get_bpcog: valid positions not loaded");
+    AOB_REQUIRE(nmax < bpcog_block(npix * npix), "get_bpcog: nmax must be below the padded pixel count");
+    float *im;
+    int size;
+    if (wfs) {
+      im = wfs->binimg.p;
+      size = wfs->npix * wfs->nxsub;
+    } else {
+      AOB_REQUIRE(img.p != nullptr, "get_bpcog: no image (load_img + calibrate_img first)");
+      im = img.p;
+      size = img_m;
+    }
+    AOB_CUDA(cudaSetDevice(device));
+    const int npad = bpcog_block(npix * npix) - npix * npix;
+    const int grid = std::max(1, std::min((nvalid + 7) / 8, num_sms(device) * 8));
+    bpcog_kernel<<<grid, 256, 0, s>>>(im, size, validx.p, validy.p, nvalid, npix, nmax, npad, scale, offset, ref.p,
+                                      order, dev_slopes, intensities.p);
+    AOB_LAUNCH_CHECK("bpcog_kernel");
+    if (wfs) ++wfs->image_gen;  // the image now holds the thresholded pixels
+    return;
+  }
   if (type == 3) {
     AOB_REQUIRE(validx.p != nullptr && validx.n >= 4 * (int64_t)nvalid, "get_pyr: 4 * nvalid valid positions not loaded");
     const float *im;

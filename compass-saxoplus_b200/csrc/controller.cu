@@ -37,8 +37,9 @@ struct MvmArgs {
   const float *s;         // slopes (device)
   float *err;             // -cmat.s
   float *com;             // integrator state
-  const float *mgain;     // modal gains
+  const float *mgain;     // modal gains (null: 1 for every row)
   float gain;
+  float berta;            // integrator state factor: com = gain * e * mgain + berta * com
   int integrate;
   uint32_t *bump;         // incremented once per launch when set (noise frame counter)
   uint32_t *status;       // error word (bounded waits that expired)
@@ -160,12 +161,12 @@ __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_kernel(MvmArgs A) {
     if (lane == 0) {
       // all loads before the first store (global-space loads, one round trip)
       const float sc = A.rscale ? __ldg(A.rscale + r) : 1.f;
-      const float mg = A.integrate ? __ldg(A.mgain + r) : 0.f;
+      const float mg = (A.integrate && A.mgain) ? __ldg(A.mgain + r) : 1.f;
       const float cm = A.integrate ? __ldcg(A.com + r) : 0.f;
       if (A.rscale) tot *= sc;
       const float e = -tot;
       A.err[r] = e;
-      if (A.integrate) A.com[r] = A.gain * (e * mg) + cm;
+      if (A.integrate) A.com[r] = fmaf(A.gain, e * mg, A.berta * cm);
     }
   }
 }
@@ -215,12 +216,12 @@ __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_bulk_kernel(MvmArgs A) {
   }
   if (A.bump && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.bump, 1u);
   // epilogue inputs of this thread's row (R <= blockDim), fetched now
-  float e_sc = 1.f, e_mg = 0.f, e_cm = 0.f;
+  float e_sc = 1.f, e_mg = 1.f, e_cm = 0.f;
   if ((int)threadIdx.x < R) {
     const int gr = r0 + threadIdx.x;
     if (A.rscale) e_sc = __ldg(A.rscale + gr);
     if (A.integrate) {
-      e_mg = __ldg(A.mgain + gr);
+      if (A.mgain) e_mg = __ldg(A.mgain + gr);
       e_cm = __ldcg(A.com + gr);
     }
   }
@@ -277,11 +278,38 @@ __global__ void __launch_bounds__(MVM_THREADS) ls_mvm_bulk_kernel(MvmArgs A) {
     if (A.rscale) tot *= e_sc;
     const float e = -tot;
     A.err[gr] = e;
-    if (A.integrate) A.com[gr] = A.gain * (e * e_mg) + e_cm;
+    if (A.integrate) A.com[gr] = fmaf(A.gain, e * e_mg, A.berta * e_cm);
   }
   // no CTA may exit with a copy still landing in its shared memory
   if (!rows_ok && threadIdx.x == 0)
     mbar_wait(&bars[0], 0, MBAR_MAX_POLLS);
+}
+
+// y[i] = alpha * sum_j A[i][j] x[j] + beta * y[i] for a row-major A (lda
+// floats per row): the secondary products of the generic controller (the
+// pseudo-open-loop slopes, matE in the modal-integrator and two-matrix laws).
+// One warp per row; the row sum runs lane-strided, then a butterfly.
+__global__ void gemv_rows_kernel(const float *A, int lda, int nrow, int ncol, const float *x, float alpha, float beta,
+                                 float *y) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int r = warp; r < nrow; r += nw) {
+    const float *a = A + (size_t)r * lda;
+    float acc = 0.f;
+    for (int j = lane; j < ncol; j += 32) acc = fmaf(a[j], x[j], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) y[r] = beta == 0.f ? alpha * acc : fmaf(alpha, acc, beta * y[r]);
+  }
+}
+
+// x[i] = x[i] * scale[i] * gain (mult_krnl, libsutra/src.cu/sutra_utils.cu:603-610)
+__global__ void mult_vec_kernel(float *x, const float *scale, float gain, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = x[i] * scale[i] * gain;
+}
+// y[i] += x[i] (axpy with alpha 1)
+__global__ void add_vec_kernel(float *y, const float *x, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += x[i];
 }
 
 struct VoltArgs {
@@ -313,6 +341,11 @@ __global__ void voltage_kernel(VoltArgs A) {
     if (A.do_clip) v = fminf(fmaxf(v, A.vmin), A.vmax);
     A.out[i] = v;
   }
+}
+
+__global__ void add_perturb_kernel(float *y, const float *buf, int cpt, int nper, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] += buf[cpt + (int64_t)i * nper];
 }
 
 __global__ void clip_kernel(float *x, int n, float lo, float hi) {
@@ -401,6 +434,11 @@ void aob_ls::ensure_packed(int p) {
 void aob_ls::comp_com(cudaStream_t s, uint32_t *bump, const uint32_t *use) {
   if (open_loop) return;
   AOB_CUDA(cudaSetDevice(device));
+  if (kind == AOB_CTRL_GENERIC) {
+    AOB_REQUIRE(!use, "comp_com: the learned reconstructor drives LS controllers only");
+    generic_comp_com(s, bump);
+    return;
+  }
   ensure_packed(prec);
   MvmArgs A{};
   A.nrow = nactu;
@@ -410,6 +448,7 @@ void aob_ls::comp_com(cudaStream_t s, uint32_t *bump, const uint32_t *use) {
   A.com = com();
   A.mgain = gains.p;
   A.gain = gain;
+  A.berta = 1.f;
   A.integrate = 1;
   A.bump = bump;
   A.status = status.p;
@@ -474,6 +513,108 @@ void aob_ls::launch_mvm(MvmArgs &A, cudaStream_t s) {
     launch_mvm_t<__nv_fp8_e4m3>(A, grid, bulk, s);
 }
 
+// The command laws of SutraControllerGeneric::comp_com
+// (libsutra/src.cpp/sutra_controller_generic.cpp:219-328), single GPU:
+//   integrator        com = berta com - gain cmat s
+//   modal_integrator  buff = -(cmat s) * modal gains;  com = gain matE buff + berta com
+//   2matrices         buff = -(cmat s) * modal gains;  com = (matE com1) * decay + buff
+// with berta = leaky factor, and with pseudo-open-loop slopes (polc: s is
+// replaced by s - imat com_clipped, SutraController::comp_polc,
+// sutra_controller.cpp:349-375) berta = (1 - gain) leaky.  com1 is the previous
+// command: a copy of com without delay, the ring's second-newest buffer with
+// delay (SutraController::command_delay, sutra_controller.cpp:205-218).
+void aob_ls::generic_comp_com(cudaStream_t s, uint32_t *bump) {
+  ensure_packed(prec);
+  const int thr = 256, grid_v = std::max(1, std::min((nactu + thr - 1) / thr, 1024));
+  const float *sin = centroids.p;
+  float berta = leaky;
+  if (polc) {
+    AOB_REQUIRE(imat_rows.p != nullptr, "comp_com: polc needs the interaction matrix (set_imat)");
+    AOB_CUDA(cudaMemcpyAsync(ol_meas.p, centroids.p, sizeof(float) * nslope, cudaMemcpyDeviceToDevice, s));
+    gemv_rows_kernel<<<std::max(1, std::min((nslope + 7) / 8, 4096)), 256, 0, s>>>(
+        imat_rows.p, nactu, nslope, nactu, com_clipped.p, -1.f, 1.f, ol_meas.p);
+    AOB_LAUNCH_CHECK("gemv_rows_kernel (polc)");
+    sin = ol_meas.p;
+    berta = (1.f - gain) * leaky;
+  }
+  MvmArgs A{};
+  A.nrow = nactu;
+  A.ncol = nslope;
+  A.s = sin;
+  A.err = err.p;
+  A.com = com();
+  A.mgain = nullptr;
+  A.gain = gain;
+  A.berta = berta;
+  A.integrate = law == AOB_LAW_INTEGRATOR ? 1 : 0;
+  A.bump = bump;
+  A.status = status.p;
+  if (prec == AOB_PREC_F32) {
+    A.mat = cm_f32.p;
+    A.ld = (nslope + 3) / 4 * 4;
+  } else if (prec == AOB_PREC_BF16) {
+    A.mat = cm_bf16.p;
+    A.ld = (nslope + 7) / 8 * 8;
+  } else {
+    A.mat = cm_fp8.p;
+    A.rscale = row_scale.p;
+    A.ld = (nslope + 15) / 16 * 16;
+  }
+  launch_mvm(A, s);
+  if (law == AOB_LAW_INTEGRATOR) return;
+  // err = -(cmat s); buff = err * modal gains
+  AOB_REQUIRE(matE_rows.p != nullptr, "comp_com: this command law needs matE (set_matE)");
+  mult_vec_kernel<<<grid_v, thr, 0, s>>>(err.p, gains.p, 1.f, nactu);
+  AOB_LAUNCH_CHECK("mult_vec_kernel");
+  const int grid_r = std::max(1, std::min((nactu + 7) / 8, 4096));
+  if (law == AOB_LAW_MODAL_INTEGRATOR) {
+    gemv_rows_kernel<<<grid_r, 256, 0, s>>>(matE_rows.p, nactu, nactu, nactu, err.p, gain, berta, com());
+    AOB_LAUNCH_CHECK("gemv_rows_kernel (modal integrator)");
+    return;
+  }
+  // 2matrices
+  const float *com1;
+  if (delay > 0) {
+    com1 = ring[ring.size() - 2].p;
+  } else {
+    AOB_CUDA(cudaMemcpyAsync(com1_tmp.p, com(), sizeof(float) * nactu, cudaMemcpyDeviceToDevice, s));
+    com1 = com1_tmp.p;
+  }
+  gemv_rows_kernel<<<grid_r, 256, 0, s>>>(matE_rows.p, nactu, nactu, nactu, com1, 1.f, 0.f, com());
+  AOB_LAUNCH_CHECK("gemv_rows_kernel (2matrices)");
+  mult_vec_kernel<<<grid_v, thr, 0, s>>>(com(), decay.p, 1.f, nactu);
+  add_vec_kernel<<<grid_v, thr, 0, s>>>(com(), err.p, nactu);
+  AOB_LAUNCH_CHECK("2matrices update");
+}
+
+void aob_ls::make_generic() {
+  kind = AOB_CTRL_GENERIC;
+  law = AOB_LAW_INTEGRATOR;
+  AOB_CUDA(cudaSetDevice(device));
+  ol_meas.alloc(nslope);
+  com1_tmp.alloc(nactu);
+  decay.alloc(nactu);
+}
+
+void aob_ls::set_matE(const float *h) {
+  std::vector<float> rows((size_t)nactu * nactu);
+  for (int j = 0; j < nactu; ++j)
+    for (int i = 0; i < nactu; ++i) rows[(size_t)i * nactu + j] = h[i + (size_t)j * nactu];
+  AOB_CUDA(cudaSetDevice(device));
+  if (!matE_rows.p) matE_rows.alloc((int64_t)nactu * nactu);
+  matE_rows.upload(rows.data(), (int64_t)nactu * nactu);
+}
+
+void aob_ls::set_imat_rows(const float *h) {
+  // imat is [nslope, nactu] column-major: row i (slope) = h[i + j nslope]
+  std::vector<float> rows((size_t)nslope * nactu);
+  for (int j = 0; j < nactu; ++j)
+    for (int i = 0; i < nslope; ++i) rows[(size_t)i * nactu + j] = h[i + (size_t)j * nslope];
+  AOB_CUDA(cudaSetDevice(device));
+  if (!imat_rows.p) imat_rows.alloc((int64_t)nslope * nactu);
+  imat_rows.upload(rows.data(), (int64_t)nslope * nactu);
+}
+
 void aob_ls::comp_voltage(cudaStream_t s) {
   AOB_CUDA(cudaSetDevice(device));
   VoltArgs A{};
@@ -507,6 +648,20 @@ void aob_ls::comp_voltage(cudaStream_t s) {
     aob::DevBuf<float> t = std::move(ring.front());
     ring.pop_front();
     ring.push_back(std::move(t));
+  }
+}
+
+// SutraController::add_perturb (sutra_controller.cpp:266-285): every enabled
+// perturbation buffer adds its current row to com_clipped, then advances.
+void aob_ls::apply_perturb(cudaStream_t s) {
+  AOB_CUDA(cudaSetDevice(device));
+  const int grid = std::max(1, std::min((nactu + 255) / 256, 1024));
+  for (auto &kv : perturb) {
+    Perturb &p = kv.second;
+    if (!p.on) continue;
+    add_perturb_kernel<<<grid, 256, 0, s>>>(com_clipped.p, p.buf.p, p.cpt, p.n, nactu);
+    AOB_LAUNCH_CHECK("add_perturb_kernel");
+    p.cpt = (p.cpt < p.n - 1) ? p.cpt + 1 : 0;
   }
 }
 

@@ -1037,6 +1037,7 @@ int aob_mlp_comp_com(aob_mlp *m, aob_ls *ls, float threshold, void *stream) {
   MLP_TRY MLP_NEED(m);
   MLP_NEED(ls);
   if (ls->nslope != m->nin || ls->nactu != m->nout) throw aob::Error("mlp.comp_com: sizes differ from the controller's");
+  if (ls->kind != AOB_CTRL_LS) throw aob::Error("mlp.comp_com: the LS fallback needs an LS controller");
   if (ls->open_loop) return AOB_OK;
   AOB_CUDA(cudaSetDevice(m->device));
   cudaStream_t s = MS(stream);

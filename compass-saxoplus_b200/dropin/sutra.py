@@ -9,13 +9,14 @@ Covered (the calls shesha's supervisor makes on the RTC path):
   sensors: ``load_arrays``, ``comp_image``, ``set_noise``, ``set_pupil``,
   ``fill_binimage``, ``d_binimg`` / ``d_bincube`` / ``d_intensities`` /
   ``d_validsubsx`` / ``d_validsubsy`` / ``d_gs.d_phase.d_screen``;
-* ``Rtc_FFF`` (rtc.cpp:100-485): ``add_centroider`` (cog, tcog, wcog, pyr),
-  ``add_controller`` (ls), ``do_centroids``, ``do_control``, ``apply_control``,
+* ``Rtc_FFF`` (rtc.cpp:100-485): ``add_centroider`` (cog, tcog, wcog, bpcog,
+  pyr, maskedpix), ``add_controller`` (ls, generic), ``do_centroids``, ``do_control``, ``apply_control``,
   ``comp_voltage``, ``do_clipping``, ``set_gain``, ``set_modal_gains``,
   ``imat_svd``, ``build_cmat``, ``set_centroids_ref``, ``do_calibrate_img``,
   ``d_centro`` / ``d_control``;
-* the centroiders (centroider.cpp:83-352) and the LS controller
-  (controller.cpp, controller_ls.cpp) with their ``d_*`` buffers and setters.
+* the centroiders (centroider.cpp:83-352), the LS controller (controller.cpp,
+  controller_ls.cpp) and the generic controller (controller_generic.cpp) with
+  their ``d_*`` buffers and setters.
 
 Errors raise ``aob200._lib.AobError`` with the library's message, where the
 reference raises ``RuntimeError`` from its C++ layer.  Everything else of the
@@ -164,15 +165,23 @@ class Centroider:
     """SutraCentroider{Cog,Tcog,Wcog,Pyr} (centroider.cpp:83-352)."""
 
     def __init__(self, nvalid, offset, scale, typec, device, wfs=None):
+        if typec == "maskedpix" and wfs is not None:
+            nvalid = 4 * wfs._w.nvalid  # one slope per valid pixel (maskedPix.cpp:35-36)
         self._c = _core.Centroider(int(nvalid), float(offset), float(scale), typec, device=int(device))
         self.type = typec
         self.device = int(device)
+        self.offset, self.scale = float(offset), float(scale)
+        self.npix = 0
+        self.threshold = 0.0
+        self.nmax = 0
         self.wfs = wfs
         if wfs is not None:
             self._c.attach(wfs._w)
 
     nvalid = property(lambda self: self._c.nvalid)
-    nslopes = property(lambda self: 2 * self._c.nvalid)
+    nslopes = property(lambda self: self._c.nslopes)
+    d_dark = property(lambda self: self._c.buffer("dark"))
+    d_flat = property(lambda self: self._c.buffer("flat"))
     d_centroids_ref = property(lambda self: self._c.buffer("centroids_ref"))
     d_intensities = property(lambda self: self._c.buffer("intensities"))
     d_img = property(lambda self: self._c.buffer("img"))
@@ -185,16 +194,29 @@ class Centroider:
         self._c.load_validpos(_arr(validx, int(N)), _arr(validy, int(N)))
 
     def set_npix(self, npix):
+        self.npix = int(npix)
         self._c.set_npix(int(npix))
 
     def set_scale(self, scale):
+        self.scale = float(scale)
         self._c.set_scale(float(scale))
 
     def set_offset(self, offset):
+        self.offset = float(offset)
         self._c.set_offset(float(offset))
 
     def set_threshold(self, threshold):
+        self.threshold = float(threshold)
         self._c.set_threshold(float(threshold))
+
+    def set_nmax(self, nmax):
+        """bpCoG (centroider_bpcog.cpp): rank of the threshold pixel."""
+        self.nmax = int(nmax)
+        self._c.set_nmax(int(nmax))
+
+    def init_weights(self):
+        """wCoG (centroider_wcog.cpp:61-62): the weights are allocated by load_weights."""
+        return 0
 
     def set_pyr_method(self, method):
         """Pyramid slopes as the reference's Method_CoG decodes them (sutra_centroider_pyr.hpp:27-34):
@@ -212,6 +234,7 @@ class Centroider:
 
     def load_img(self, img, *args):
         self._c.load_img(np.asarray(img, np.float32))
+        return 0
 
     def calibrate_img(self):
         self._c.calibrate_img()
@@ -223,16 +246,21 @@ class Centroider:
         self._c.set_flat(np.asarray(flat, np.float32), int(n))
 
 
-class ControllerLS:
-    """SutraControllerLs (controller.cpp, controller_ls.cpp)."""
+class _Controller:
+    """SutraController (controller.cpp:65-330): the buffers, delay ring,
+    perturbation voltages, clip and comp_voltage common to every controller."""
+
+    _kind = "ls"
 
     def __init__(self, nslope, nactu, delay, device):
-        self._l = _core.LsController(int(nslope), int(nactu), delay=float(delay), device=int(device))
-        self.type = "ls"
+        self._l = _core.LsController(int(nslope), int(nactu), delay=float(delay), device=int(device), kind=self._kind)
+        self.type = self._kind
         self.nslope, self.nactu = int(nslope), int(nactu)
         self.delay = float(delay)
         self.gain = 0.0
+        self.comRange = (-1.0e6, 1.0e6)
         self.centro_idx = []
+        self._perturb = {}
 
     d_centroids = property(lambda self: self._l.buffer("centroids"))
     d_com = property(lambda self: self._l.buffer("com"))
@@ -241,8 +269,14 @@ class ControllerLS:
     d_err = property(lambda self: self._l.buffer("err"))
     d_cmat = property(lambda self: self._l.buffer("cmat", shape=(self.nactu, self.nslope)))
     d_imat = property(lambda self: self._l.buffer("imat", shape=(self.nslope, self.nactu)))
-    d_eigenvals = property(lambda self: self._l.buffer("eigenvals"))
     d_gain = property(lambda self: self._l.buffer("gain"))
+    d_circularComs0 = property(lambda self: self._l.buffer("com0"))
+    d_circularComs1 = property(lambda self: self._l.buffer("com1"))
+
+    @property
+    def d_perturb_map(self):
+        """name -> (perturbation voltages [N, nactu], counter, enabled), as the reference's map."""
+        return dict(self._perturb)
 
     def set_cmat(self, cmat):
         self._l.set_cmat(np.asarray(cmat, np.float32))
@@ -265,6 +299,7 @@ class ControllerLS:
         self._l.set_com(np.asarray(com, np.float32))
 
     def set_comRange(self, comMin, comMax):
+        self.comRange = (comMin, comMax)
         self._l.set_com_range(float(comMin), float(comMax))
 
     def set_open_loop(self, open_loop, reset=True):
@@ -272,24 +307,75 @@ class ControllerLS:
 
     def comp_voltage(self):
         self._l.comp_voltage()
+        for k, (a, cpt, on) in self._perturb.items():
+            if on:
+                self._perturb[k] = (a, (cpt + 1) % a.shape[0], on)
 
     def clip_commands(self):
         self._l.clip()
 
+    def add_perturb(self):
+        """com_clipped += the current row of every enabled perturbation (controller.cpp add_perturb)."""
+        self._l.apply_perturb()
+        for k, (a, cpt, on) in self._perturb.items():
+            if on:
+                self._perturb[k] = (a, (cpt + 1) % a.shape[0], on)
+
     def add_perturb_voltage(self, name, perturb, N):
-        self._l.add_perturb(name, np.asarray(perturb, np.float32), int(N))
+        a = np.array(perturb, np.float32)
+        self._l.add_perturb(name, a, int(N))
+        self._perturb[name] = (a, 0, True)
 
     def remove_perturb_voltage(self, name):
         self._l.remove_perturb(name)
+        self._perturb.pop(name, None)
 
     def enable_perturb_voltage(self, name):
         self._l.enable_perturb(name, True)
+        a, cpt, _ = self._perturb[name]
+        self._perturb[name] = (a, cpt, True)
 
     def disable_perturb_voltage(self, name):
         self._l.enable_perturb(name, False)
+        a, cpt, _ = self._perturb[name]
+        self._perturb[name] = (a, cpt, False)
 
     def reset_perturb_voltage(self):
         self._l.reset_perturb()
+        self._perturb = {}
+
+
+class ControllerLS(_Controller):
+    """SutraControllerLs (controller_ls.cpp)."""
+
+    _kind = "ls"
+    d_eigenvals = property(lambda self: self._l.buffer("eigenvals"))
+
+
+class ControllerGENERIC(_Controller):
+    """SutraControllerGeneric (controller_generic.cpp): command laws integrator
+    (leaky factor, pseudo-open-loop slopes), modal_integrator and 2matrices."""
+
+    _kind = "generic"
+
+    def set_commandlaw(self, law):
+        self._l.set_commandlaw(str(law))
+
+    @property
+    def command_law(self):
+        return self._l.law()["law"]
+
+    def set_leaky_factor(self, factor):
+        self._l.set_leaky_factor(float(factor))
+
+    def set_polc(self, polc):
+        self._l.set_polc(bool(polc))
+
+    def set_decayFactor(self, decay):
+        self._l.set_decay_factor(np.asarray(decay, np.float32))
+
+    def set_matE(self, matE):
+        self._l.set_matE(np.asarray(matE, np.float32))
 
 
 class Rtc_FFF:
@@ -302,17 +388,18 @@ class Rtc_FFF:
         self.d_control = []
 
     def add_centroider(self, context, nvalid, offset, scale, filter_TT, device, typec, wfs=None):
-        if typec not in ("cog", "tcog", "wcog", "pyr"):
-            raise ValueError(f"add_centroider: centroider type {typec!r} is not supported (cog, tcog, wcog, pyr)")
+        if typec not in ("cog", "tcog", "wcog", "bpcog", "pyr", "maskedpix"):
+            raise ValueError(f"add_centroider: centroider type {typec!r} is not supported "
+                             "(cog, tcog, wcog, bpcog, pyr, maskedpix)")
         self.d_centro.append(Centroider(nvalid, offset, scale, typec, device, wfs))
         return 0
 
     def add_controller(self, context, typec, device, delay, nslope, nactu, nslope_buffers=0, nstates=0,
                        nstate_buffers=0, nmodes=0, niir_in=0, niir_out=0, polc=False, is_modal=False, dms=None,
                        idx_dms=None, ndm=0, idx_centro=None, ncentro=0, Nphi=0, wfs_direction=False):
-        if typec != "ls":
-            raise ValueError(f"add_controller: controller type {typec!r} is not supported (ls)")
-        c = ControllerLS(nslope, nactu, delay, device)
+        if typec not in ("ls", "generic"):
+            raise ValueError(f"add_controller: controller type {typec!r} is not supported (ls, generic)")
+        c = (ControllerLS if typec == "ls" else ControllerGENERIC)(nslope, nactu, delay, device)
         c.centro_idx = ([int(i) for i in _arr(idx_centro)][: int(ncentro)] if idx_centro is not None and ncentro
                         else list(range(len(self.d_centro))))
         self.d_control.append(c)
@@ -330,7 +417,7 @@ class Rtc_FFF:
         off = 0
         for i in c.centro_idx:
             yield self.d_centro[i], base.ptr + 4 * off
-            off += 2 * self.d_centro[i].nvalid
+            off += self.d_centro[i].nslopes
 
     def do_calibrate_img(self, ncontrol):
         for cen, _ in self._slopes_of(ncontrol):
@@ -384,7 +471,7 @@ class Rtc_FFF:
         ref = np.asarray(centroidsRef, np.float32).ravel()
         off = 0
         for cen in self.d_centro:
-            n = 2 * cen.nvalid
+            n = cen.nslopes
             cen.set_centroids_ref(ref[off:off + n])
             off += n
         return 0

@@ -147,6 +147,15 @@ typedef struct aob_centro aob_centro;
 #define AOB_CENTRO_TCOG 1
 #define AOB_CENTRO_WCOG 2
 #define AOB_CENTRO_PYR 3
+/* SutraCentroiderMaskedPix (sutra_centroider_maskedPix.cpp, kernel
+ * sutra_centroider_maskedPix.cu:26-56): one slope per valid pixel,
+ * s[i] = pix[i] / sum(pix) * n - ref[i]; nvalid is the number of pixels (4 *
+ * the pyramid's nvalid) and the reference slopes start at 1. */
+#define AOB_CENTRO_MASKEDPIX 4
+/* SutraCentroiderBpcog (sutra_centroider_bpcog.cu:24-80): CoG over the pixels
+ * above the value of rank nmax (aob_centro_set_nmax), thresholded pixels
+ * written back into the image. */
+#define AOB_CENTRO_BPCOG 5
 #define AOB_SLOPES_UNTIED 0
 #define AOB_SLOPES_INTERLEAVED 1
 
@@ -165,7 +174,8 @@ int aob_centro_set_threshold(aob_centro *c, float threshold);
 int aob_centro_set_slope_order(aob_centro *c, int order);
 /* Pyramid centroider (type AOB_CENTRO_PYR, SutraCentroiderPyr::get_pyr,
  * libsutra/src.cpp/sutra_centroider_pyr.cpp:101-130): reads the binned image
- * of the attached pyramid sensor; its valid positions are 4 * nvalid pixels
+ * of the attached pyramid sensor (a masked-pixel centroider may be attached
+ * to one too); its valid positions are 4 * nvalid pixels
  * (quadrant k of sub-aperture i at entry i + k nvalid).  method (set_pyr_method,
  * python_module/sutra/src/centroider_pyr.cpp:35-64), decoded as the reference's
  * Method_CoG(uint8_t) does (libsutra/include/sutra_centroider_pyr.hpp:27-34):
@@ -173,6 +183,9 @@ int aob_centro_set_slope_order(aob_centro *c, int order);
  * sub-aperture flux), 3 nosinus local.  thresh: flux below which the slopes
  * are 0 (reference default 1e-4). */
 int aob_centro_attach_pyr(aob_centro *c, aob_pyr *p);
+/* set_nmax (python_module/sutra/src/centroider_bpcog.cpp): rank of the
+ * threshold pixel of a bpcog centroider, 0 <= nmax < 1024. */
+int aob_centro_set_nmax(aob_centro *c, int nmax);
 int aob_centro_set_pyr_method(aob_centro *c, int method);
 int aob_centro_set_pyr_thresh(aob_centro *c, float thresh);
 /* load_validpos (sutra_centroider.cpp:287-298); n = nvalid (4 * nvalid for a
@@ -241,6 +254,10 @@ int aob_ls_add_perturb(aob_ls *c, const char *name, const float *perturb, int n)
 int aob_ls_remove_perturb(aob_ls *c, const char *name);
 int aob_ls_enable_perturb(aob_ls *c, const char *name, int enable);
 int aob_ls_reset_perturb(aob_ls *c);
+/* add_perturb (sutra_controller.cpp:266-285): com_clipped += the current row
+ * of every enabled perturbation buffer, whose counter then advances (the step
+ * comp_voltage runs before its clip). */
+int aob_ls_apply_perturb(aob_ls *c, void *stream);
 /* One SVD-style eigen decomposition of imat^T imat in float64 on the GPU
  * (svdec_imat, sutra_controller_ls.cpp:116-150) and the filtered
  * pseudo-inverse (build_cmat, :174-217). */
@@ -251,6 +268,35 @@ int aob_ls_build_cmat(aob_ls *c, int nfilt);
 int aob_ls_buffer(aob_ls *c, const char *which, void **dev_ptr, int64_t *nelem);
 int aob_ls_get_params(aob_ls *c, int *nslope, int *nactu, float *delay, float *gain,
                       int *open_loop, float *volt_min, float *volt_max, int *prec);
+
+/* ---- generic controller ------------------------------------------------- *
+ * Replaces SutraControllerGeneric (libsutra/src.cpp/sutra_controller_generic.cpp,
+ * bound by python_module/sutra/src/controller_generic.cpp).  It is an aob_ls
+ * handle of kind AOB_CTRL_GENERIC: every aob_ls_* call applies (cmat, gain,
+ * modal gains, delay, perturbation, clip, comp_voltage, buffers), and comp_com
+ * runs its command law (comp_com, sutra_controller_generic.cpp:219-328):
+ *   AOB_LAW_INTEGRATOR        com = berta com - gain cmat s
+ *   AOB_LAW_MODAL_INTEGRATOR  b = -(cmat s) * modal gains; com = gain matE b + berta com
+ *   AOB_LAW_2MATRICES         b = -(cmat s) * modal gains; com = (matE com1) * decay + b
+ * with berta = the leaky factor, or with pseudo-open-loop control (polc: s
+ * replaced by s - imat com_clipped) (1 - gain) * leaky; com1 is the previous
+ * command.  The gain starts at 0, the leaky factor at 1.  No state vector
+ * (nstates = 0).  The fused RTC kernel and the batch take LS controllers only. */
+#define AOB_CTRL_LS 0
+#define AOB_CTRL_GENERIC 1
+#define AOB_LAW_INTEGRATOR 1
+#define AOB_LAW_MODAL_INTEGRATOR 2
+#define AOB_LAW_2MATRICES 3
+int aob_generic_create(aob_ls **out, int device, int nslope, int nactu, float delay);
+/* kind (AOB_CTRL_*), command law, leaky factor, polc flag. */
+int aob_ls_get_kind(aob_ls *c, int *kind, int *law, float *leaky, int *polc);
+/* set_commandlaw / set_leaky_factor / set_polc (controller_generic.cpp). */
+int aob_ls_set_commandlaw(aob_ls *c, int law);
+int aob_ls_set_leaky_factor(aob_ls *c, float leaky);
+int aob_ls_set_polc(aob_ls *c, int polc);
+/* set_decayFactor (nactu) and set_matE (nactu x nactu, column-major). */
+int aob_ls_set_decay_factor(aob_ls *c, const float *decay);
+int aob_ls_set_matE(aob_ls *c, const float *matE);
 
 
 /* ---- learned reconstructor (MLP) ---------------------------------------- *
