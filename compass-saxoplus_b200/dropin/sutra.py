@@ -175,17 +175,18 @@ class Centroider:
         self.threshold = 0.0
         self.nmax = 0
         self.wfs = wfs
+        self._img_shape = None  # (m, n) of the loaded image (the carma objects are 2-D)
         if wfs is not None:
             self._c.attach(wfs._w)
 
     nvalid = property(lambda self: self._c.nvalid)
     nslopes = property(lambda self: self._c.nslopes)
-    d_dark = property(lambda self: self._c.buffer("dark"))
-    d_flat = property(lambda self: self._c.buffer("flat"))
+    d_dark = property(lambda self: self._c.buffer("dark", shape=self._img_shape))
+    d_flat = property(lambda self: self._c.buffer("flat", shape=self._img_shape))
+    d_img = property(lambda self: self._c.buffer("img", shape=self._img_shape))
+    d_img_raw = property(lambda self: self._c.buffer("img_raw", shape=self._img_shape))
     d_centroids_ref = property(lambda self: self._c.buffer("centroids_ref"))
     d_intensities = property(lambda self: self._c.buffer("intensities"))
-    d_img = property(lambda self: self._c.buffer("img"))
-    d_img_raw = property(lambda self: self._c.buffer("img_raw"))
     d_validx = property(lambda self: self._c.buffer("validx", np.int32))
     d_validy = property(lambda self: self._c.buffer("validy", np.int32))
     d_weights = property(lambda self: self._c.buffer("weights"))
@@ -233,16 +234,20 @@ class Centroider:
         self._c.set_centroids_ref(np.asarray(refslopes, np.float32))
 
     def load_img(self, img, *args):
-        self._c.load_img(np.asarray(img, np.float32))
+        img = np.asarray(img, np.float32)
+        self._img_shape = img.shape if img.ndim == 2 else None
+        self._c.load_img(img)
         return 0
 
     def calibrate_img(self):
         self._c.calibrate_img()
 
     def set_dark(self, dark, n):
+        self._img_shape = self._img_shape or (int(n), int(n))
         self._c.set_dark(np.asarray(dark, np.float32), int(n))
 
     def set_flat(self, flat, n):
+        self._img_shape = self._img_shape or (int(n), int(n))
         self._c.set_flat(np.asarray(flat, np.float32), int(n))
 
 
@@ -260,7 +265,8 @@ class _Controller:
         self.gain = 0.0
         self.comRange = (-1.0e6, 1.0e6)
         self.centro_idx = []
-        self._perturb = {}
+        self._perturb = {}  # name -> (voltages, counter, enabled)
+        self._perturb_n = {}  # name -> number of rows
 
     d_centroids = property(lambda self: self._l.buffer("centroids"))
     d_com = property(lambda self: self._l.buffer("com"))
@@ -305,11 +311,14 @@ class _Controller:
     def set_open_loop(self, open_loop, reset=True):
         self._l.set_open_loop(bool(open_loop), bool(reset))
 
-    def comp_voltage(self):
-        self._l.comp_voltage()
+    def _advance_perturb(self):
         for k, (a, cpt, on) in self._perturb.items():
             if on:
-                self._perturb[k] = (a, (cpt + 1) % a.shape[0], on)
+                self._perturb[k] = (a, (cpt + 1) % self._perturb_n[k], on)
+
+    def comp_voltage(self):
+        self._l.comp_voltage()
+        self._advance_perturb()
 
     def clip_commands(self):
         self._l.clip()
@@ -317,18 +326,18 @@ class _Controller:
     def add_perturb(self):
         """com_clipped += the current row of every enabled perturbation (controller.cpp add_perturb)."""
         self._l.apply_perturb()
-        for k, (a, cpt, on) in self._perturb.items():
-            if on:
-                self._perturb[k] = (a, (cpt + 1) % a.shape[0], on)
+        self._advance_perturb()
 
     def add_perturb_voltage(self, name, perturb, N):
         a = np.array(perturb, np.float32)
         self._l.add_perturb(name, a, int(N))
         self._perturb[name] = (a, 0, True)
+        self._perturb_n[name] = int(N)
 
     def remove_perturb_voltage(self, name):
         self._l.remove_perturb(name)
         self._perturb.pop(name, None)
+        self._perturb_n.pop(name, None)
 
     def enable_perturb_voltage(self, name):
         self._l.enable_perturb(name, True)
@@ -342,7 +351,7 @@ class _Controller:
 
     def reset_perturb_voltage(self):
         self._l.reset_perturb()
-        self._perturb = {}
+        self._perturb, self._perturb_n = {}, {}
 
 
 class ControllerLS(_Controller):
