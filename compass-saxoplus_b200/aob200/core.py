@@ -117,7 +117,10 @@ class ShWfs:
         keep = [host_array(binmap, i32), host_array(offsets, f32), host_array(fluxPerSub, f32),
                 host_array(validsubsx, i32), host_array(validsubsy, i32), host_array(istart, i32),
                 host_array(jstart, i32)]
-        call("aob_sh_load_arrays", self.h, None, None, *[k.ctypes.data for k in keep], None, None)
+        # hrmap is read when the field of view is extended (ntot != nfft)
+        hr = host_array(hrmap, i32) if (hrmap is not None and self.ntot != self.nfft) else None
+        call("aob_sh_load_arrays", self.h, None, None if hr is None else hr.ctypes.data,
+             *[k.ctypes.data for k in keep], None, None)
 
     def set_pupil(self, pupil):
         a = host_array(pupil, np.float32)

@@ -274,8 +274,17 @@ def sh_geometry(p: ShParams, pupdiam: int, diam: float = 8.0, cobs: float = 0.14
         halfxy = ramp.astype(np.float32)
 
     if ntot != nfft:
-        raise NotImplementedError("extended field of view (Ntot != Nfft) is not supported")
-    hrmap = np.zeros((2, 2), dtype=np.int32)
+        # extended field of view (geom_init.py:847-867): the nfft x nfft spot sits
+        # in the middle of an ntot x ntot image, both centred on pixel 0 by the
+        # half-size rolls; hrmap lists the spot's pixel positions in that image
+        # (row-major order, which is the order the reference's indexfill reads)
+        lo = int((ntot - nfft) / 2.0)
+        block = np.zeros((ntot, ntot))
+        block[lo:lo + nfft, lo:lo + nfft] = 1
+        block = np.roll(np.roll(block, ntot // 2, axis=0), ntot // 2, axis=1)
+        hrmap = np.flatnonzero(block).astype(np.int32).reshape(-1, 1)
+    else:
+        hrmap = np.zeros((2, 2), dtype=np.int32)  # set even if unused, as the reference does
 
     span = nrebin * p.npix
     lo = int((ntot - span) / 2.0) + (1 if span % 2 != ntot % 2 else 0)

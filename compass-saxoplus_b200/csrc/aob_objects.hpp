@@ -38,6 +38,7 @@ struct aob_sh {
   aob::DevBuf<float> phase;        // npup x npup guide-star phase [um]
   aob::DevBuf<float> pupil;        // npup x npup amplitude
   aob::DevBuf<int32_t> istart, jstart, validsubsx, validsubsy, binmap;
+  aob::DevBuf<int32_t> hrmap;  // nfft^2 positions in the ntot x ntot image (ntot != nfft)
   aob::DevBuf<float> offsets, fluxPerSub;
   // pruned-DFT tables derived from binmap at load time
   int nu = 0, nv = 0;
@@ -55,7 +56,7 @@ struct aob_sh {
          int npup, float pdiam, float nphot, float nphot4imat);
   void load_arrays(const int32_t *binmap, const float *offsets, const float *fluxPerSub,
                    const int32_t *validsubsx, const int32_t *validsubsy, const int32_t *istart,
-                   const int32_t *jstart);
+                   const int32_t *jstart, const int32_t *hrmap = nullptr);
   void comp_image(bool noise, cudaStream_t s);
   // slopes_dst: write the fused centroider's slopes there instead of its staging
   // buffer; frame_ptr: read the noise frame number from device memory

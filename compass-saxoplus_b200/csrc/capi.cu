@@ -145,12 +145,12 @@ int aob_sh_destroy(aob_sh *h) {
   }
   AOB_API_END
 }
-int aob_sh_load_arrays(aob_sh *h, const int32_t *, const int32_t *, const int32_t *binmap, const float *offsets,
+int aob_sh_load_arrays(aob_sh *h, const int32_t *, const int32_t *hrmap, const int32_t *binmap, const float *offsets,
                        const float *flux, const int32_t *vx, const int32_t *vy, const int32_t *istart,
                        const int32_t *jstart, const float *, const float *) {
   AOB_API_BEGIN
   NEED(h);
-  h->load_arrays(binmap, offsets, flux, vx, vy, istart, jstart);
+  h->load_arrays(binmap, offsets, flux, vx, vy, istart, jstart, hrmap);
   AOB_API_END
 }
 int aob_sh_set_pupil(aob_sh *h, const float *pupil) {

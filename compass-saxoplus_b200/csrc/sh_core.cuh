@@ -411,13 +411,15 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
       const int32_t *c = cb + p * nr2;
       float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
       int r = 0;
+      // (an entry of -1 lies outside the spot's nfft x nfft support: zero)
+      auto at = [&](int ci) { return ci >= 0 ? Is[ci] : 0.f; };
       for (; r + 3 < nr2; r += 4) {
-        v0 += Is[c[r]];
-        v1 += Is[c[r + 1]];
-        v2 += Is[c[r + 2]];
-        v3 += Is[c[r + 3]];
+        v0 += at(c[r]);
+        v1 += at(c[r + 1]);
+        v2 += at(c[r + 2]);
+        v3 += at(c[r + 3]);
       }
-      for (; r < nr2; ++r) v0 += Is[c[r]];
+      for (; r < nr2; ++r) v0 += at(c[r]);
       const float v = (v0 + v1) + (v2 + v3);
       bins[s * npix2 + p] = v;
       part += v;

@@ -76,7 +76,8 @@ aob_sh::aob_sh(int device_, int nxsub_, int nvalid_, int npix_, int nphase_, int
       nfft(nfft_), ntot(ntot_), npup(npup_), pdiam(pdiam_), nphot(nphot_), nphot4imat(nphot4imat_) {
   AOB_REQUIRE(nvalid > 0 && npix > 0 && nphase > 0 && nrebin > 0 && npup > 0, "sh: sizes must be > 0");
   AOB_REQUIRE(nfft == 16 || nfft == 32 || nfft == 64, "sh: nfft must be 16, 32 or 64");
-  AOB_REQUIRE(ntot == nfft, "sh: extended field of view (ntot != nfft) is not supported");
+  AOB_REQUIRE(ntot >= nfft && ntot <= 4096, "sh: ntot must be in [nfft, 4096]");
+  AOB_REQUIRE((int64_t)nrebin * npix <= ntot, "sh: nrebin * npix exceeds the field of view ntot");
   AOB_REQUIRE(nphase <= nfft && nphase <= 32, "sh: nphase must be <= min(nfft, 32)");
   AOB_REQUIRE(npix >= 2 && nphase >= 2, "sh: npix and nphase must be >= 2");
   AOB_REQUIRE(nphase * nphase < 4096 && nfft * nfft <= 4096, "sh: sizes beyond the index arithmetic range");
@@ -107,9 +108,10 @@ aob_sh::aob_sh(int device_, int nxsub_, int nvalid_, int npix_, int nphase_, int
 
 void aob_sh::load_arrays(const int32_t *h_binmap, const float *h_offsets, const float *h_flux,
                          const int32_t *h_vx, const int32_t *h_vy, const int32_t *h_istart,
-                         const int32_t *h_jstart) {
+                         const int32_t *h_jstart, const int32_t *h_hrmap) {
   AOB_REQUIRE(h_binmap && h_offsets && h_flux && h_vx && h_vy && h_istart && h_jstart,
               "sh.load_arrays: a required array is NULL");
+  AOB_REQUIRE(ntot == nfft || h_hrmap, "sh.load_arrays: hrmap is required when ntot != nfft");
   AOB_CUDA(cudaSetDevice(device));
   const int nr2 = nrebin * nrebin, np2 = npix * npix;
   const int n2 = nfft * nfft;
@@ -121,11 +123,34 @@ void aob_sh::load_arrays(const int32_t *h_binmap, const float *h_offsets, const 
     AOB_REQUIRE(h_vx[i] >= 0 && h_vy[i] >= 0 && h_vx[i] + npix <= img && h_vy[i] + npix <= img,
                 "sh.load_arrays: sub-aperture outside the sensor image");
   }
-  // frequencies that binmap reads: kx = m % nfft, ky = m / nfft
+  // Binning map over the nfft x nfft spot.  With an extended field of view
+  // (ntot > nfft) the reference writes the spot into an ntot x ntot image at
+  // hrmap (indexfill_krnl, libsutra/src.cu/sutra_wfs.cu:462-473; zero elsewhere)
+  // and bins that image through binmap (sutra_wfs_sh.cpp:409-481): composed here
+  // into one map, where an entry of -1 reads a zero.
+  std::vector<int32_t> bm(nr2 * np2);
+  if (ntot != nfft) {
+    const int64_t nt2 = (int64_t)ntot * ntot;
+    std::vector<int32_t> inv(nt2, -1);
+    for (int i = 0; i < n2; ++i) {
+      AOB_REQUIRE(h_hrmap[i] >= 0 && h_hrmap[i] < nt2, "sh.load_arrays: hrmap entry out of range");
+      inv[h_hrmap[i]] = i;
+    }
+    for (int i = 0; i < nr2 * np2; ++i) {
+      AOB_REQUIRE(h_binmap[i] >= 0 && h_binmap[i] < nt2, "sh.load_arrays: binmap entry out of range");
+      bm[i] = inv[h_binmap[i]];
+    }
+  } else {
+    for (int i = 0; i < nr2 * np2; ++i) {
+      AOB_REQUIRE(h_binmap[i] >= 0 && h_binmap[i] < n2, "sh.load_arrays: binmap entry out of range");
+      bm[i] = h_binmap[i];
+    }
+  }
+  // frequencies that the map reads: kx = m % nfft, ky = m / nfft
   std::vector<int> usex(nfft, -1), usey(nfft, -1);
   for (int i = 0; i < nr2 * np2; ++i) {
-    const int m = h_binmap[i];
-    AOB_REQUIRE(m >= 0 && m < n2, "sh.load_arrays: binmap entry out of range");
+    const int m = bm[i];
+    if (m < 0) continue;
     usex[m % nfft] = 1;
     usey[m / nfft] = 1;
   }
@@ -139,8 +164,8 @@ void aob_sh::load_arrays(const int32_t *h_binmap, const float *h_offsets, const 
   AOB_REQUIRE(nu >= 2 && nv >= 2, "sh.load_arrays: binmap reads fewer than 2 frequencies along an axis");
   std::vector<int32_t> C(nr2 * np2);
   for (int i = 0; i < nr2 * np2; ++i) {
-    const int m = h_binmap[i];
-    C[i] = usex[m % nfft] + usey[m / nfft] * nu;
+    const int m = bm[i];
+    C[i] = m < 0 ? -1 : usex[m % nfft] + usey[m / nfft] * nu;
   }
   // per-geometry twiddles WX[a][x] = W^(U[a] x), WY[b][y] = W^(V[b] y): the same
   // float values as the nfft-point table, gathered so the DFT loops need no index math
@@ -177,6 +202,10 @@ void aob_sh::load_arrays(const int32_t *h_binmap, const float *h_offsets, const 
   vlist.upload(V.data(), nv);
   cbin.upload(C.data(), (int64_t)nr2 * np2);
   binmap.upload(h_binmap, (int64_t)nr2 * np2);
+  if (ntot != nfft) {
+    hrmap.alloc(n2);
+    hrmap.upload(h_hrmap, n2);
+  }
   offsets.upload(h_offsets, (int64_t)nphase * nphase);
   fluxPerSub.upload(h_flux, nvalid);
   validsubsx.upload(h_vx, nvalid);

@@ -57,15 +57,19 @@ int aob_fill_f32(float *dev, size_t n, float value, void *stream);
 typedef struct aob_sh aob_sh;
 
 /* Constructor arguments of SutraWfsSH (sutra_wfs_sh.cpp:27-75). npup is the
- * side of the guide-star phase screen the sensor reads (p_geom._n). */
+ * side of the guide-star phase screen the sensor reads (p_geom._n); ntot >= nfft
+ * (ntot > nfft: the field of view extended beyond the spot's FFT support). */
 int aob_sh_create(aob_sh **out, int device, int nxsub, int nvalid, int npix, int nphase,
                   int nrebin, int nfft, int ntot, int npup, float pdiam, float nphot,
                   float nphot4imat);
 int aob_sh_destroy(aob_sh *h);
-/* SutraWfsSH::load_arrays (sutra_wfs_sh.cpp:308-331); phasemap, hrmap,
- * ttprojmat and kernel are accepted for interface parity and may be NULL.
- * binmap is [nrebin^2, npix^2], offsets [nphase^2]; fluxPerSub, validsubsx,
- * validsubsy, istart and jstart have nvalid entries. */
+/* SutraWfsSH::load_arrays (sutra_wfs_sh.cpp:308-331); phasemap, ttprojmat and
+ * kernel are accepted for interface parity and may be NULL.  binmap is
+ * [nrebin^2, npix^2] indexes into the ntot x ntot image, offsets [nphase^2];
+ * fluxPerSub, validsubsx, validsubsy, istart and jstart have nvalid entries.
+ * hrmap (nfft^2 positions of the nfft x nfft spot in the ntot x ntot image) is
+ * required when ntot != nfft (extended field of view) and may be NULL
+ * otherwise. */
 int aob_sh_load_arrays(aob_sh *h, const int32_t *phasemap, const int32_t *hrmap,
                        const int32_t *binmap, const float *offsets, const float *fluxPerSub,
                        const int32_t *validsubsx, const int32_t *validsubsy,

@@ -10,8 +10,8 @@ Follows the reference's SutraWfsSH::comp_generic / fill_binimage
   subapnorm_krnl   sutra_utils.cu:170-193 flux normalisation (skipped when the sum is 0)
   prng('P'), prng('N', noise, 1)  sutra_wfs_sh.cpp:580-587 photon + readout noise
   bimg_krnl        sutra_wfs.cu:183-229   scatter to the 2-D image
-Only the Ntot == Nfft (no field-of-view extension), natural-guide-star path
-is restated.
+The natural-guide-star path is restated, with the field of view extended
+(Ntot > Nfft) or not; the kernel convolution and the field stop are not.
 
 Array convention: every 2-D numpy array ``a`` here is indexed ``a[x, y]`` with
 ``x`` the fastest-varying device index (the reference passes F-ordered arrays).
@@ -40,10 +40,19 @@ def hr_images(field):
     return np.abs(np.fft.fft2(field, axes=(0, 1))) ** 2
 
 
-def bin_cube(hr, binmap):
-    """bincube[p, k] = sum_r hr_flat[binmap[r, p], k] with hr_flat[x + y*nfft]."""
+def bin_cube(hr, binmap, hrmap=None, ntot=None):
+    """bincube[p, k] = sum_r hr_flat[binmap[r, p], k] with hr_flat[x + y*nfft].
+
+    With an extended field of view (ntot > nfft) the spot is first written into
+    an ntot x ntot image at ``hrmap`` (indexfill_krnl, libsutra/src.cu/
+    sutra_wfs.cu:462-473: element i of the spot goes to hrmap[i], the rest of
+    the image is zero; sutra_wfs_sh.cpp:409-481) and binmap indexes that image."""
     nfft = hr.shape[0]
     flat = hr.reshape(nfft * nfft, -1, order="F")
+    if ntot is not None and int(ntot) != nfft:
+        big = np.zeros((int(ntot) * int(ntot), flat.shape[1]), dtype=flat.dtype)
+        big[np.asarray(hrmap).ravel(), :] = flat
+        flat = big
     return flat[binmap, :].sum(axis=0)
 
 
@@ -88,7 +97,7 @@ def comp_image(phase, pupil, g, scale, nphot, noise=-1.0, seed=1234, frame=0):
     get = (lambda k: g[k]) if isinstance(g, dict) else (lambda k: getattr(g, k))
     field = spot_field(phase, pupil, get("validpuppixx"), get("validpuppixy"), get("halfxy"),
                        scale, int(get("pdiam")), int(get("nfft")))
-    cube = bin_cube(hr_images(field), get("binmap"))
+    cube = bin_cube(hr_images(field), get("binmap"), get("hrmap"), int(get("ntot")))
     cube, sums = normalise(cube, get("fluxPerSub").astype(np.float64), nphot)
     cube = add_noise(cube, noise, seed, frame)
     img = bin_image(cube, get("validsubsx"), get("validsubsy"), int(get("npix")), int(get("nxsub")))

@@ -66,6 +66,10 @@ SH_CASES = {
                  cobs=0.14, gsmag=8.0, r0=0.14, ittime=0.001),
     "sh8": dict(nxsub=8, pupdiam=48, npix=2, pixsize=0.3, lam=0.7, fracsub=0.5,
                 cobs=0.14, gsmag=8.0, r0=0.16, ittime=0.001),
+    # the reference's own test sensor (shesha/tests/pytest/par/test_sh.py): at
+    # 0.5 um its 8 pixels of 0.3" extend the field of view beyond the FFT support
+    "sh16x": dict(nxsub=16, pupdiam=128, npix=8, pixsize=0.3, lam=0.5, fracsub=0.8,
+                  cobs=0.12, gsmag=3.0, r0=0.16, ittime=0.002),
 }
 
 PYR_CASES = {
@@ -234,18 +238,22 @@ def main():
     import shesha.config as conf
     import shesha.init.geom_init as gi
 
+    only = os.environ.get("AO_GOLDEN_ONLY")
     for name, c in SH_CASES.items():
+        if only and only != name:
+            continue
         out = make_sh(conf, gi, c)
         np.savez_compressed(os.path.join(HERE, f"geom_{name}.npz"), **out)
         print(name, "nvalid", out["nvalid"], "nfft", out["nfft"], "nrebin", out["nrebin"])
     for name, c in PYR_CASES.items():
+        if only and only != name:
+            continue
         out = make_pyr(conf, gi, c)
         np.savez_compressed(os.path.join(HERE, f"geom_{name}.npz"), **out)
         print(name, "nvalid", out["nvalid"], "nfft", out["nfft"], "nrebin", out["nrebin"])
     import shesha.init.dm_init as dmi
     import shesha.util.iterkolmo as itk
 
-    only = os.environ.get("AO_GOLDEN_ONLY")
     for name, c in DM_CASES.items():
         if only and only != name:
             continue

@@ -3,7 +3,7 @@
 Run on a machine with a GPU after ``python oracle/build_ref.py`` built the
 reference's ``carma`` / ``sutra`` modules into ``oracle/_ref/``:
 
-    python tests/golden/make_ref_fixtures.py [OUT_DIR]
+    python tests/golden/make_ref_fixtures.py [OUT_DIR [CASE ...]]
 
 For each case the script builds the sensor, centroiders and least-squares
 controller through the reference's Python API in the order shesha's
@@ -153,18 +153,22 @@ def run_pyr(ctx, name, seed):
     return out
 
 
-def main(out_dir):
+def main(out_dir, only=None):
     os.makedirs(out_dir, exist_ok=True)
     ctx = carma.context.get_instance_1gpu(0)
     for i, name in enumerate(SH_CASES):
+        if only and name not in only:
+            continue
         d = run_sh(ctx, name, seed=100 + i)
         np.savez_compressed(os.path.join(out_dir, f"ref_{name}.npz"), **d)
         print(name, {k: getattr(v, "shape", v) for k, v in d.items()})
     for i, name in enumerate(PYR_CASES):
+        if only and name not in only:
+            continue
         d = run_pyr(ctx, name, seed=200 + i)
         np.savez_compressed(os.path.join(out_dir, f"ref_{name}.npz"), **d)
         print(name, {k: getattr(v, "shape", v) for k, v in d.items()})
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else HERE)
+    main(sys.argv[1] if len(sys.argv) > 1 else HERE, sys.argv[2:])

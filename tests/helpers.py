@@ -8,12 +8,15 @@ SH_CASES = {
     "sh8": (G.ShParams(nxsub=8, npix=2, pixsize=0.3, wavelength_um=0.7, fracsub=0.5, gsmag=8.0), 48),
     "sh16": (G.ShParams(nxsub=16, npix=8, pixsize=0.3, wavelength_um=0.7, fracsub=0.5, gsmag=8.0), 128),
     "sh40": (G.ShParams(nxsub=40, npix=6, pixsize=0.36, wavelength_um=0.7, fracsub=0.5, gsmag=8.0), 240),
+    # shesha/tests/pytest/par/test_sh.py's sensor: field of view extended (ntot 64 > nfft 32)
+    "sh16x": (G.ShParams(nxsub=16, npix=8, pixsize=0.3, wavelength_um=0.5, fracsub=0.8, gsmag=3.0), 128),
 }
+SH_TEL = {"sh16x": dict(cobs=0.12, ittime=0.002)}
 
 
 def sh_geometry(name):
     p, pup = SH_CASES[name]
-    return G.sh_geometry(p, pup, diam=8.0, cobs=0.14, ittime=0.001)
+    return G.sh_geometry(p, pup, diam=8.0, **SH_TEL.get(name, dict(cobs=0.14, ittime=0.001)))
 
 
 def kolmogorov_screen(n, r0_pixels, seed, lam_um=0.5):

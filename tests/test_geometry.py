@@ -10,14 +10,18 @@ SH = {
     "sh16": G.ShParams(nxsub=16, npix=8, pixsize=0.3, wavelength_um=0.7, fracsub=0.5, gsmag=8.0),
     "sh40": G.ShParams(nxsub=40, npix=6, pixsize=0.36, wavelength_um=0.7, fracsub=0.5, gsmag=8.0),
     "sh8": G.ShParams(nxsub=8, npix=2, pixsize=0.3, wavelength_um=0.7, fracsub=0.5, gsmag=8.0),
+    # shesha/tests/pytest/par/test_sh.py's sensor: extended field of view (ntot > nfft)
+    "sh16x": G.ShParams(nxsub=16, npix=8, pixsize=0.3, wavelength_um=0.5, fracsub=0.8, gsmag=3.0),
 }
-SH_PUP = {"sh16": 128, "sh40": 240, "sh8": 48}
+SH_PUP = {"sh16": 128, "sh40": 240, "sh8": 48, "sh16x": 128}
+SH_TEL = {"sh16x": dict(cobs=0.12, ittime=0.002)}
 
 
 @pytest.mark.parametrize("name", sorted(SH))
 def test_sh_geometry_matches_reference(name, golden):
     ref = golden("geom_" + name)
-    g = G.sh_geometry(SH[name], SH_PUP[name], diam=8.0, cobs=0.14, ittime=0.001)
+    tel = SH_TEL.get(name, dict(cobs=0.14, ittime=0.001))
+    g = G.sh_geometry(SH[name], SH_PUP[name], diam=8.0, **tel)
     for k in ("pdiam", "nfft", "ntot", "nrebin", "nvalid"):
         assert getattr(g, k) == int(ref[k]), k
     assert g.tel.n == int(ref["n"])

@@ -8,9 +8,9 @@ against NumPy, at the reference's precision (1e-2 on the maximum error
 relative to the largest value).  The same module-level set-up and the same
 checks run here through the drop-in modules (compass-saxoplus_b200/dropin),
 with the inputs a ``CompassSupervisor`` would give made by this project's own
-sensors: the SH image of test_sh.py's 16x16, 8-pixel sensor on a seeded
-screen (delay 3, gain 0.4; at 0.7 um, where the sensor's field of view needs
-no extension) and a pyramid image for the masked-pixel test.
+sensors: the SH image of test_sh.py's 16x16, 8-pixel sensor at 0.5 um on a
+seeded screen (delay 3, gain 0.4) and a pyramid image for the masked-pixel
+test.
 The reference's ``sup.rtc.get_command_matrix`` is a seeded random matrix here;
 the checks compare the drop-in against NumPy on that same matrix.
 """
@@ -51,9 +51,9 @@ def sh():
         import sutra
     finally:
         sys.path.remove(DROPIN)
-    # test_sh.py: 16x16 sub-apertures, 8 pixels of 0.3", fracsub 0.8, magnitude 3, no noise; at 0.7 um (the
-    # file's 0.5 um needs the extended field of view, Ntot != Nfft)
-    g = G.sh_geometry(G.ShParams(nxsub=16, npix=8, pixsize=0.3, wavelength_um=0.7, fracsub=0.8, gsmag=3.0), 128,
+    # test_sh.py: 16x16 sub-apertures, 8 pixels of 0.3" at 0.5 um (field of view extended: ntot 64 > nfft 32),
+    # fracsub 0.8, magnitude 3, no noise
+    g = G.sh_geometry(G.ShParams(nxsub=16, npix=8, pixsize=0.3, wavelength_um=0.5, fracsub=0.8, gsmag=3.0), 128,
                       diam=8.0, cobs=0.12, ittime=0.002)
     w = C.ShWfs.from_geometry(g)
     w.set_phase(kolmogorov_screen(g.tel.n, r0_pixels=0.16 / (8.0 / g.tel.pupdiam), seed=5, lam_um=0.5))
@@ -98,6 +98,7 @@ def test_init_and_setters(sh):
     assert control.nactu - NACTU < precision
     assert control.type == "generic"
     assert control.delay - DELAY < precision
+    assert g.ntot > g.nfft  # the file's sensor extends its field of view
     assert centro.npix - g.npix < precision
     assert relative_array_error(np.array(centro.d_validx), sh["xvalid"]) < precision
     assert relative_array_error(np.array(centro.d_validy), sh["yvalid"]) < precision
