@@ -100,6 +100,8 @@ class ShWfs:
                       g.validpuppixx, g.validpuppixy)
         w.set_pupil(g.tel.mpupil)
         w.set_noise(noise, seed)
+        if getattr(g, "submask", None) is not None:
+            w.set_field_stop(g.submask)
         return w
 
     def __del__(self):
@@ -127,6 +129,15 @@ class ShWfs:
         if a.size != self.npup * self.npup:
             raise ValueError("pupil must be npup x npup")
         call("aob_sh_set_pupil", self.h, a.ctypes.data)
+
+    def set_field_stop(self, mask):
+        """Focal-plane field stop of the full pupil (n x n, fftshifted; None removes it)."""
+        if mask is None:
+            call("aob_sh_set_field_stop", self.h, None, 0)
+            return
+        m = np.asarray(mask)
+        a = host_array(m, np.float32)
+        call("aob_sh_set_field_stop", self.h, a.ctypes.data, int(m.shape[0]))
 
     def set_noise(self, noise, seed=1234):
         self.noise = float(noise)

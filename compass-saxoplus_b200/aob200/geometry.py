@@ -146,6 +146,8 @@ class ShParams:
     zerop: float = 1e11
     optthroughput: float = 0.5
     noise: float = -1.0
+    fssize: float = 0.0   # field-stop size in arcsec (0: no field stop)
+    fstop: str = "round"  # field-stop shape: "round" or "square"
 
 
 @dataclass
@@ -177,6 +179,7 @@ class ShGeometry:
     ttprojmat: np.ndarray
     wavelength_um: float
     tel: Optional[TelescopeGeometry] = field(default=None, repr=False)
+    submask: Optional[np.ndarray] = None  # field-stop mask (fftshifted), None without field stop
 
 
 def _sh_sizes(p: ShParams, pdiam: int, diam: float):
@@ -199,6 +202,19 @@ def _sh_sizes(p: ShParams, pdiam: int, diam: float):
     if ntot % 2 != nfft % 2:
         ntot += 1
     return nfft, ntot, nrebin, float(pixsize), float(qpixsize)
+
+
+def _focal_mask(size: int, radius: int, shape: str) -> np.ndarray:
+    """Round or square field stop of ``radius`` pixels centred in a size x size
+    focal plane (geom_init.py:513-520 for the pyramid, :978-988 for the SH)."""
+    if shape == "round":
+        return radial_distance(size, xc=size / 2.0 - 0.5, yc=size / 2.0 - 0.5) < radius
+    if shape == "square":
+        ij = np.indices((size, size)) + 1
+        fx = ij[1] - (size + 1.0) / 2.0
+        fy = ij[0] - (size + 1.0) / 2.0
+        return (np.abs(fx) <= radius) * (np.abs(fy) <= radius)
+    raise ValueError("field stop must be 'round' or 'square'")
 
 
 def _tt_projection(mask_t: np.ndarray, i0: int, j0: int, nph: int):
@@ -302,6 +318,13 @@ def sh_geometry(p: ShParams, pupdiam: int, diam: float = 8.0, cobs: float = 0.14
 
     nphot = compute_nphotons("sh", ittime, p.optthroughput, diam, nxsub=nx,
                              zerop=p.zerop, gsmag=p.gsmag)
+    submask = None
+    if p.fssize != 0:
+        # field stop in the focal plane of the full pupil (geom_init.py:973-995)
+        fftsize = fft_goodsize(tel.mpupil.shape[0])
+        fspixsize = (tel.pupdiam * (p.wavelength_um * 1.0e-6) / diam * RAD2ARCSEC) / fftsize
+        rf = int(p.fssize / fspixsize / 2.0)
+        submask = np.fft.fftshift(_focal_mask(fftsize, rf, p.fstop) * 1.0)
     return ShGeometry(
         nxsub=nx, npix=p.npix, pdiam=pdiam, nfft=nfft, ntot=ntot, nrebin=nrebin,
         nvalid=nvalid, pixsize=pixsize, qpixsize=qpixsize, subapd=diam / nx,
@@ -311,7 +334,7 @@ def sh_geometry(p: ShParams, pupdiam: int, diam: float = 8.0, cobs: float = 0.14
         validpuppixx=(vx * pdiam + 2).astype(np.int32),
         validpuppixy=(vy * pdiam + 2).astype(np.int32),
         phasemap=phasemap, binmap=binmap, halfxy=halfxy, hrmap=hrmap, ttprojmat=ttproj,
-        wavelength_um=p.wavelength_um, tel=tel,
+        wavelength_um=p.wavelength_um, tel=tel, submask=submask,
     )
 
 
@@ -385,16 +408,7 @@ def pyr_geometry(p: PyrParams, pupdiam: int, diam: float = 8.0, cobs: float = 0.
     size = nfft
 
     rf = int(f32(p.fssize) / qpixsize / 2.0)
-    if p.fstop == "round":
-        focmask = radial_distance(size, xc=size / 2.0 - 0.5, yc=size / 2.0 - 0.5) < rf
-    elif p.fstop == "square":
-        ij = np.indices((size, size)) + 1
-        fx = ij[1] - (size + 1.0) / 2.0
-        fy = ij[0] - (size + 1.0) / 2.0
-        focmask = (np.abs(fx) <= rf) * (np.abs(fy) <= rf)
-    else:
-        raise ValueError("pyramid field stop must be 'round' or 'square'")
-    submask = np.fft.fftshift(focmask * 1.0)
+    submask = np.fft.fftshift(_focal_mask(size, rf, p.fstop) * 1.0)
 
     pup_sep = int(p.nxsub) if p.pup_sep == -1 else p.pup_sep
     gy = np.tile(np.arange(size) - size / 2, (size, 1))

@@ -39,6 +39,9 @@ struct aob_sh {
   aob::DevBuf<float> pupil;        // npup x npup amplitude
   aob::DevBuf<int32_t> istart, jstart, validsubsx, validsubsy, binmap;
   aob::DevBuf<int32_t> hrmap;  // nfft^2 positions in the ntot x ntot image (ntot != nfft)
+  int fs_n = 0;                // field stop: side of its focal plane (0: none)
+  aob::DevBuf<float> fs_mask;  // fs_n x fs_n focal-plane mask (fftshifted)
+  aob::DevBuf<float> fs_field; // fs_n x fs_n complex filtered field (float pairs)
   aob::DevBuf<float> offsets, fluxPerSub;
   // pruned-DFT tables derived from binmap at load time
   int nu = 0, nv = 0;
@@ -54,6 +57,8 @@ struct aob_sh {
 
   aob_sh(int device, int nxsub, int nvalid, int npix, int nphase, int nrebin, int nfft, int ntot,
          int npup, float pdiam, float nphot, float nphot4imat);
+  void set_field_stop(const float *mask, int n);
+  void field_stop_prepare(cudaStream_t s);
   void load_arrays(const int32_t *binmap, const float *offsets, const float *fluxPerSub,
                    const int32_t *validsubsx, const int32_t *validsubsy, const int32_t *istart,
                    const int32_t *jstart, const int32_t *hrmap = nullptr);

@@ -153,6 +153,12 @@ int aob_sh_load_arrays(aob_sh *h, const int32_t *, const int32_t *hrmap, const i
   h->load_arrays(binmap, offsets, flux, vx, vy, istart, jstart, hrmap);
   AOB_API_END
 }
+int aob_sh_set_field_stop(aob_sh *h, const float *mask, int n) {
+  AOB_API_BEGIN
+  NEED(h);
+  h->set_field_stop(mask, n);
+  AOB_API_END
+}
 int aob_sh_set_pupil(aob_sh *h, const float *pupil) {
   AOB_API_BEGIN
   NEED(h); NEED(pupil);

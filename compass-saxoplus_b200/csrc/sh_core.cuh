@@ -55,6 +55,11 @@ struct ShKernelArgs {
   float noise;
   uint32_t frame, k0, k1;
   const uint32_t *frame_ptr;  // when set, the frame number is read from device memory
+  // field stop: the filtered full-pupil field (fs_n x fs_n complex) read in place
+  // of the phase and pupil, scaled by fs_inv = 1 / fs_n^2 (sh_batch<..., FS = true>)
+  const float2 *fs_field;
+  int fs_n;
+  float fs_inv;
   // magic multipliers for the runtime divisions (see udiv)
   uint32_t mg_pd, mg_pd2, mg_nu, mg_nupd, mg_nunv, mg_np, mg_np2;
   // fused centroider (kind < 0: none)
@@ -216,7 +221,7 @@ __device__ __forceinline__ void sh_store_images(const ShKernelArgs &P, int base,
 // thread of the team once the field stage is complete (its global loads have
 // returned), before the DFTs.  With DEFER_IMG the cube and image writes are
 // left to sh_store_images (the noisy pixels stay in the work area).
-template <int NFFT, int PD, int TK = TEAM_CTA, class Hook = NoHook, bool DEFER_IMG = false>
+template <int NFFT, int PD, int TK = TEAM_CTA, class Hook = NoHook, bool DEFER_IMG = false, bool FS = false>
 __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int stride, int S,
                                          const unsigned char *tables, unsigned char *work, const ShSmem &L,
                                          const Team &T, const Hook &after_field = Hook{}) {
@@ -274,6 +279,36 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
   // metadata and the counters are first used after stage 1's barrier)
 
   // ---- 1. complex field: loads of up to 4 elements issued before any use ----
+  if constexpr (FS) {
+    // field stop: the sub-aperture's window of the filtered full-pupil field times
+    // exp(-i offset), normalised (camplipup_krnl, libsutra/src.cu/sutra_wfs.cu:87-117)
+    for (int i0 = tid; i0 < nE; i0 += 4 * nt) {
+      float2 fv[4];
+      float of[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int i = i0 + j * nt;
+        if (i < nE) {
+          const int s = PD > 0 ? i / (PD * PD) : udiv(i, P.mg_pd2);
+          const int l = i - s * pd2;
+          const int y = PD > 0 ? l / PD : udiv(l, P.mg_pd);
+          const int x = l - y * pd;
+          const int k = base + s * stride;
+          fv[j] = P.fs_field[(x + __ldg(P.puppixx + k)) + (y + __ldg(P.puppixy + k)) * P.fs_n];
+          of[j] = __ldg(P.offsets + l);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int i = i0 + j * nt;
+        if (i < nE) {
+          float so, co;
+          sincosf(of[j], &so, &co);
+          E[i] = make_float2((fv[j].x * co + fv[j].y * so) * P.fs_inv, (fv[j].y * co - fv[j].x * so) * P.fs_inv);
+        }
+      }
+    }
+  } else
   for (int i0 = tid; i0 < nE; i0 += 4 * nt) {
     float ph[4], am[4], of[4];
 #pragma unroll

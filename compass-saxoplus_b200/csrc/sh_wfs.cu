@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "aob_objects.hpp"
+#include "fft.cuh"
 #include "sh_core.cuh"
 
 namespace aob {
@@ -43,7 +44,7 @@ constexpr int SH_MAX_BATCH = 32;
 // PD > 0: phase-grid side known at compile time (the DFT loops unroll and all
 // their shared-memory loads issue back to back); PD == 0: runtime side.
 // Sub-apertures k = blockIdx.x + (r * S + s) * gridDim.x, s < S, rounds r.
-template <int NFFT, int PD>
+template <int NFFT, int PD, bool FS = false>
 __global__ void __launch_bounds__(SH_THREADS) sh_image_kernel(ShKernelArgs P, int S) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int pd = PD > 0 ? PD : P.pdiam;
@@ -53,7 +54,33 @@ __global__ void __launch_bounds__(SH_THREADS) sh_image_kernel(ShKernelArgs P, in
   // read none of them, so their loads overlap the field's)
   for (int base = blockIdx.x; base < P.nvalid; base += S * gridDim.x) {
     const int Sb = min(S, (P.nvalid - base + (int)gridDim.x - 1) / (int)gridDim.x);
-    sh_batch<NFFT, PD>(P, base, gridDim.x, Sb, smem, smem + L.hdr, L, Team{(int)threadIdx.x, (int)blockDim.x, 0});
+    sh_batch<NFFT, PD, TEAM_CTA, NoHook, false, FS>(P, base, gridDim.x, Sb, smem, smem + L.hdr, L,
+                                                    Team{(int)threadIdx.x, (int)blockDim.x, 0});
+  }
+}
+
+// Field stop (SutraWfsSH::comp_generic with a field stop, sutra_wfs_sh.cpp:366-391):
+// pupil * exp(i phase scale) in the top-left npup x npup corner of the n x n
+// array (fsamplipup_krnl, sutra_wfs.cu:148-166), zero elsewhere ...
+__global__ void fs_fill_kernel(float2 *out, int n, const float *phase, const float *pupil, int npup, float scale) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < (int64_t)n * n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(t % n), y = (int)(t / n);
+    float2 v = make_float2(0.f, 0.f);
+    if (x < npup && y < npup) {
+      const int id = x + y * npup;
+      float sn, cs;
+      sincosf(phase[id] * scale, &sn, &cs);
+      v = make_float2(cs * pupil[id], sn * pupil[id]);
+    }
+    out[t] = v;
+  }
+}
+// ... and, between the forward and inverse FFTs, the focal-plane mask (submask_krnl, :1868-1876)
+__global__ void fs_mask_kernel(float2 *d, const float *mask, int64_t n2) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n2; t += (int64_t)gridDim.x * blockDim.x) {
+    const float m = mask[t];
+    d[t] = make_float2(d[t].x * m, d[t].y * m);
   }
 }
 
@@ -230,12 +257,19 @@ int aob_sh::pick_batch() const {
   return b;
 }
 
-template <int NFFT, int PD>
-static void launch_sh(const ShKernelArgs &P, int nvalid, int S, size_t sm, cudaStream_t s) {
+template <int NFFT, int PD, bool FS>
+static void launch_sh_fs(const ShKernelArgs &P, int nvalid, int S, size_t sm, cudaStream_t s) {
   const int grid = std::max(1, (nvalid + S - 1) / S);
   // opt-in per (kernel, device), only ever raised (a driver call per launch costs microseconds)
-  smem_opt_in(reinterpret_cast<const void *>(sh_image_kernel<NFFT, PD>), (int)std::max<size_t>(sm, 48 * 1024));
-  sh_image_kernel<NFFT, PD><<<grid, SH_THREADS, sm, s>>>(P, S);
+  smem_opt_in(reinterpret_cast<const void *>(sh_image_kernel<NFFT, PD, FS>), (int)std::max<size_t>(sm, 48 * 1024));
+  sh_image_kernel<NFFT, PD, FS><<<grid, SH_THREADS, sm, s>>>(P, S);
+}
+template <int NFFT, int PD>
+static void launch_sh(const ShKernelArgs &P, int nvalid, int S, size_t sm, cudaStream_t s) {
+  if (P.fs_field)
+    launch_sh_fs<NFFT, PD, true>(P, nvalid, S, sm, s);
+  else
+    launch_sh_fs<NFFT, PD, false>(P, nvalid, S, sm, s);
 }
 
 template <int NFFT>
@@ -323,10 +357,45 @@ void aob_sh::after_image(const ShKernelArgs &P, aob_centro *c, bool staged) {
   }
 }
 
+void aob_sh::set_field_stop(const float *mask, int n) {
+  AOB_CUDA(cudaSetDevice(device));
+  if (!mask || n == 0) {
+    fs_n = 0;
+    fs_mask.release();
+    fs_field.release();
+    return;
+  }
+  AOB_REQUIRE(n >= 8 && n <= 2048 && (n & (n - 1)) == 0, "sh.set_field_stop: n must be a power of two in [8, 2048]");
+  AOB_REQUIRE(n >= npup, "sh.set_field_stop: the field-stop plane must hold the npup x npup screen");
+  fs_mask.alloc((int64_t)n * n);
+  fs_mask.upload(mask, (int64_t)n * n);
+  fs_field.alloc(2 * (int64_t)n * n);
+  fs_n = n;
+}
+
+// The filtered full-pupil field of the current phase (field stop).
+void aob_sh::field_stop_prepare(cudaStream_t s) {
+  const int64_t n2 = (int64_t)fs_n * fs_n;
+  const int grid = (int)std::min<int64_t>((n2 + 255) / 256, 8192);
+  float2 *f = reinterpret_cast<float2 *>(fs_field.p);
+  fs_fill_kernel<<<grid, 256, 0, s>>>(f, fs_n, phase.p, pupil.p, npup, (float)(2.0 * M_PI / (double)lambda_um));
+  AOB_LAUNCH_CHECK("fs_fill_kernel");
+  fft2d(f, fs_n, 1, false, device, s);
+  fs_mask_kernel<<<grid, 256, 0, s>>>(f, fs_mask.p, n2);
+  AOB_LAUNCH_CHECK("fs_mask_kernel");
+  fft2d(f, fs_n, 1, true, device, s);
+}
+
 void aob_sh::comp_image_to(bool with_noise, cudaStream_t s, float *slopes_dst, const uint32_t *frame_ptr) {
   AOB_CUDA(cudaSetDevice(device));
   ShKernelArgs P;
   aob_centro *c = make_args(with_noise, slopes_dst, frame_ptr, P);
+  if (fs_n) {
+    field_stop_prepare(s);
+    P.fs_field = reinterpret_cast<const float2 *>(fs_field.p);
+    P.fs_n = fs_n;
+    P.fs_inv = 1.f / ((float)fs_n * (float)fs_n);  // exact: fs_n is a power of two
+  }
   const int S = pick_batch();
   const size_t sm = smem_bytes(S);
   if (nfft == 16)

@@ -151,6 +151,13 @@ class Sensors:
     def d_wfs(self):
         return self._wfs
 
+    def set_field_stop(self, nwfs, field_stop, N):
+        """SutraSensors::set_field_stop (sensors.cpp:200-210): SH sensors only."""
+        w = self.d_wfs[int(nwfs)]
+        if isinstance(w, SHWFS):
+            w._w.set_field_stop(np.asarray(field_stop, np.float32).reshape(int(N), int(N)))
+        return 0
+
     def initgs(self, xpos, ypos, lambda_um, mag, zerop, sizes, noise, seeds, G, thetaML, dx, dy):
         """Guide stars (sensors.cpp:159-191): wavelength, noise level and noise seed per sensor."""
         for i, w in enumerate(self._wfs):

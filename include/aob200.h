@@ -75,6 +75,16 @@ int aob_sh_load_arrays(aob_sh *h, const int32_t *phasemap, const int32_t *hrmap,
                        const int32_t *validsubsx, const int32_t *validsubsy,
                        const int32_t *istart, const int32_t *jstart, const float *ttprojmat,
                        const float *kernel_c64);
+/* SutraSensors::set_field_stop / SutraWfsSH::set_field_stop (sutra_sensors.cpp:
+ * 223-229, sutra_wfs_sh.cpp:674-707): a focal-plane field stop of the full
+ * pupil, mask n x n (fftshifted, as the reference's geometry gives it), n a
+ * power of two in [8, 2048] and >= npup.  Each image then forms the field
+ * pupil * exp(i phase) in the top-left corner of the n x n plane, multiplies
+ * its FFT by the mask and reads the sub-aperture fields from the inverse FFT
+ * (sutra_wfs_sh.cpp:366-391).  mask NULL or n == 0 removes it.  Steps with a
+ * field stop run the separate-kernel path (not the fused RTC kernel or the
+ * batch). */
+int aob_sh_set_field_stop(aob_sh *h, const float *mask, int n);
 /* SutraWfs::set_pupil (sutra_wfs.cpp) -- npup x npup amplitude. */
 int aob_sh_set_pupil(aob_sh *h, const float *pupil_host);
 /* SutraWfs::set_noise (sutra_wfs.cpp:123-141); the generator is the

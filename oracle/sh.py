@@ -11,7 +11,8 @@ Follows the reference's SutraWfsSH::comp_generic / fill_binimage
   prng('P'), prng('N', noise, 1)  sutra_wfs_sh.cpp:580-587 photon + readout noise
   bimg_krnl        sutra_wfs.cu:183-229   scatter to the 2-D image
 The natural-guide-star path is restated, with the field of view extended
-(Ntot > Nfft) or not; the kernel convolution and the field stop are not.
+(Ntot > Nfft) or not, with or without the focal-plane field stop; the kernel
+convolution is not.
 
 Array convention: every 2-D numpy array ``a`` here is indexed ``a[x, y]`` with
 ``x`` the fastest-varying device index (the reference passes F-ordered arrays).
@@ -22,15 +23,36 @@ import numpy as np
 from . import philox
 
 
-def spot_field(phase, pupil, puppixx, puppixy, offsets, scale, pdiam, nfft):
-    """Complex field cube [nfft, nfft, nvalid], non-zero in the top-left pdiam x pdiam."""
+def field_stop_field(phase, pupil, scale, submask):
+    """Full-pupil field filtered by the focal-plane field stop, normalised.
+
+    fsamplipup_krnl (libsutra/src.cu/sutra_wfs.cu:148-166) puts pupil *
+    exp(i phase scale) in the top-left npup x npup corner of an n x n array;
+    a forward FFT, the fftshifted mask (submask_krnl, :1868-1876) and an
+    unnormalised inverse FFT follow (sutra_wfs_sh.cpp:366-391); the complex
+    camplipup_krnl (:87-117) divides by n^2."""
+    n = submask.shape[0]
+    npup = phase.shape[0]
+    f = np.zeros((n, n), dtype=np.complex128)
+    f[:npup, :npup] = pupil.astype(np.float64) * np.exp(1j * phase.astype(np.float64) * scale)
+    return np.fft.ifft2(np.fft.fft2(f) * submask)  # = unnormalised inverse / n^2
+
+
+def spot_field(phase, pupil, puppixx, puppixy, offsets, scale, pdiam, nfft, field=None):
+    """Complex field cube [nfft, nfft, nvalid], non-zero in the top-left pdiam x pdiam.
+
+    ``field``: the field-stop-filtered full-pupil field; the sub-aperture field is
+    then field * exp(-i offset) (camplipup_krnl, sutra_wfs.cu:87-117)."""
     nvalid = len(puppixx)
     x = np.arange(pdiam)
     ix = puppixx[None, None, :] + x[:, None, None]
     iy = puppixy[None, None, :] + x[None, :, None]
+    cube = np.zeros((nfft, nfft, nvalid), dtype=np.complex128)
+    if field is not None:
+        cube[:pdiam, :pdiam, :] = field[ix, iy] * np.exp(-1j * offsets.astype(np.float64)[:, :, None])
+        return cube
     ph = phase[ix, iy].astype(np.float64) * scale - offsets.astype(np.float64)[:, :, None]
     amp = pupil[ix, iy].astype(np.float64)
-    cube = np.zeros((nfft, nfft, nvalid), dtype=np.complex128)
     cube[:pdiam, :pdiam, :] = amp * np.exp(1j * ph)
     return cube
 
@@ -95,8 +117,13 @@ def comp_image(phase, pupil, g, scale, nphot, noise=-1.0, seed=1234, frame=0):
     halfxy, binmap, fluxPerSub, validsubsx/y, pdiam, nfft, npix, nxsub).
     """
     get = (lambda k: g[k]) if isinstance(g, dict) else (lambda k: getattr(g, k))
+    try:
+        submask = get("submask")
+    except (KeyError, AttributeError):
+        submask = None
+    fs = None if submask is None else field_stop_field(phase, pupil, scale, np.asarray(submask, np.float64))
     field = spot_field(phase, pupil, get("validpuppixx"), get("validpuppixy"), get("halfxy"),
-                       scale, int(get("pdiam")), int(get("nfft")))
+                       scale, int(get("pdiam")), int(get("nfft")), field=fs)
     cube = bin_cube(hr_images(field), get("binmap"), get("hrmap"), int(get("ntot")))
     cube, sums = normalise(cube, get("fluxPerSub").astype(np.float64), nphot)
     cube = add_noise(cube, noise, seed, frame)

@@ -70,6 +70,11 @@ SH_CASES = {
     # 0.5 um its 8 pixels of 0.3" extend the field of view beyond the FFT support
     "sh16x": dict(nxsub=16, pupdiam=128, npix=8, pixsize=0.3, lam=0.5, fracsub=0.8,
                   cobs=0.12, gsmag=3.0, r0=0.16, ittime=0.002),
+    # with a round field stop of 1.6 arcsec and a square one of 1.2 arcsec
+    "sh16fs": dict(nxsub=16, pupdiam=128, npix=8, pixsize=0.3, lam=0.7, fracsub=0.5,
+                   cobs=0.14, gsmag=8.0, r0=0.16, ittime=0.001, fssize=1.6, fstop="round"),
+    "sh16fsq": dict(nxsub=16, pupdiam=128, npix=8, pixsize=0.3, lam=0.7, fracsub=0.5,
+                    cobs=0.14, gsmag=8.0, r0=0.16, ittime=0.001, fssize=1.2, fstop="square"),
 }
 
 PYR_CASES = {
@@ -103,6 +108,11 @@ def make_sh(conf, gi, c):
     w.set_optthroughput(0.5)
     w.set_zerop(1e11)
     w.set_noise(0.5)
+    if c.get("fssize"):
+        import shesha.constants as scons
+
+        w.set_fssize(c["fssize"])
+        w.set_fstop(scons.FieldStopType.ROUND if c["fstop"] == "round" else scons.FieldStopType.SQUARE)
     with contextlib.redirect_stdout(io.StringIO()):
         gi.init_wfs_geom(w, c["r0"], p_tel, p_geom, c["ittime"], verbose=0)
     fluxPerSub = w._fluxPerSub.T[np.where(w._isvalid.T > 0)].copy()
@@ -118,6 +128,7 @@ def make_sh(conf, gi, c):
         validpuppixx=w._validpuppixx, validpuppixy=w._validpuppixy,
         phasemap=w._phasemap, binmap=w._binmap, halfxy=w._halfxy,
         hrmap=w._hrmap, ttprojmat=w._ttprojmat,
+        **({"submask": w._submask} if c.get("fssize") else {}),
     )
 
 

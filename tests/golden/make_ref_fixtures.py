@@ -84,6 +84,8 @@ def run_sh(ctx, name, seed):
     kernel = np.zeros((g.ntot, g.ntot), np.complex64)  # used only by the kernel convolution (off)
     wfs.load_arrays(g.phasemap, g.hrmap, g.binmap, g.halfxy, g.fluxPerSub, g.validsubsx, g.validsubsy,
                     g.validpuppixx, g.validpuppixy, g.ttprojmat, kernel)
+    if g.submask is not None:  # wfs_init.py:233-234
+        sensors.set_field_stop(0, g.submask.astype(np.float32), g.submask.shape[0])
     phase = phase_screen(g.tel.n, g.tel.pupdiam, seed)
     wfs.d_gs.set_phase(phase)
     nslope = 2 * g.nvalid

@@ -10,6 +10,8 @@ SH_CASES = {
     "sh40": (G.ShParams(nxsub=40, npix=6, pixsize=0.36, wavelength_um=0.7, fracsub=0.5, gsmag=8.0), 240),
     # shesha/tests/pytest/par/test_sh.py's sensor: field of view extended (ntot 64 > nfft 32)
     "sh16x": (G.ShParams(nxsub=16, npix=8, pixsize=0.3, wavelength_um=0.5, fracsub=0.8, gsmag=3.0), 128),
+    # a round focal-plane field stop of 1.6 arcsec over the full pupil
+    "sh16fs": (G.ShParams(nxsub=16, npix=8, pixsize=0.3, wavelength_um=0.7, fracsub=0.5, gsmag=8.0, fssize=1.6), 128),
 }
 SH_TEL = {"sh16x": dict(cobs=0.12, ittime=0.002)}
 

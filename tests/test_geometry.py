@@ -12,8 +12,13 @@ SH = {
     "sh8": G.ShParams(nxsub=8, npix=2, pixsize=0.3, wavelength_um=0.7, fracsub=0.5, gsmag=8.0),
     # shesha/tests/pytest/par/test_sh.py's sensor: extended field of view (ntot > nfft)
     "sh16x": G.ShParams(nxsub=16, npix=8, pixsize=0.3, wavelength_um=0.5, fracsub=0.8, gsmag=3.0),
+    # field stops in the focal plane of the full pupil
+    "sh16fs": G.ShParams(nxsub=16, npix=8, pixsize=0.3, wavelength_um=0.7, fracsub=0.5, gsmag=8.0, fssize=1.6,
+                         fstop="round"),
+    "sh16fsq": G.ShParams(nxsub=16, npix=8, pixsize=0.3, wavelength_um=0.7, fracsub=0.5, gsmag=8.0, fssize=1.2,
+                          fstop="square"),
 }
-SH_PUP = {"sh16": 128, "sh40": 240, "sh8": 48, "sh16x": 128}
+SH_PUP = {"sh16": 128, "sh40": 240, "sh8": 48, "sh16x": 128, "sh16fs": 128, "sh16fsq": 128}
 SH_TEL = {"sh16x": dict(cobs=0.12, ittime=0.002)}
 
 
@@ -34,6 +39,10 @@ def test_sh_geometry_matches_reference(name, golden):
         np.testing.assert_array_equal(a, ref[k], err_msg=k)
     for k in ("fluxPerSub", "fluxPerSub_grid", "halfxy"):
         np.testing.assert_array_equal(getattr(g, k), ref[k], err_msg=k)
+    if "submask" in ref:
+        np.testing.assert_array_equal(g.submask, ref["submask"])
+    else:
+        assert g.submask is None
     # tip/tilt projection (not on the image-formation path): float rounding only
     np.testing.assert_allclose(g.ttprojmat, ref["ttprojmat"], rtol=1e-6, atol=1e-7)
     # the reference keeps these two through float32 parameter setters

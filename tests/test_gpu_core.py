@@ -35,7 +35,7 @@ def _setup(core, name, noise=-1.0, seed=7):
     return g, w, phase
 
 
-@pytest.mark.parametrize("name", ["sh8", "sh16", "sh40", "sh16x"])
+@pytest.mark.parametrize("name", ["sh8", "sh16", "sh40", "sh16x", "sh16fs"])
 def test_sh_image_matches_oracle(core, name):
     g, w, phase = _setup(core, name)
     w.comp_image(noise=False)
@@ -50,7 +50,7 @@ def test_sh_image_matches_oracle(core, name):
 
 
 @pytest.mark.parametrize("kind", ["cog", "tcog", "wcog"])
-@pytest.mark.parametrize("name", ["sh16", "sh40", "sh16x"])
+@pytest.mark.parametrize("name", ["sh16", "sh40", "sh16x", "sh16fs"])
 def test_fused_and_standalone_centroids_match_oracle(core, name, kind):
     g, w, phase = _setup(core, name)
     offset, scale = g.npix / 2 - 0.5, g.pixsize
