@@ -130,6 +130,23 @@ class ShWfs:
             raise ValueError("pupil must be npup x npup")
         call("aob_sh_set_pupil", self.h, a.ctypes.data)
 
+    def set_fakecam(self, enable=True, max_flux_per_pix=0, max_pix_value=0):
+        """Digitise every image into the uint16 frame ``d_camimg`` (fakecam)."""
+        call("aob_sh_set_fakecam", self.h, 1 if enable else 0, int(max_flux_per_pix), int(max_pix_value))
+
+    def set_dark(self, dark, n=None):
+        a = host_array(dark, np.float32)
+        call("aob_sh_set_dark", self.h, a.ctypes.data, int(np.sqrt(a.size)))
+
+    def set_flat(self, flat, n=None):
+        a = host_array(flat, np.float32)
+        call("aob_sh_set_flat", self.h, a.ctypes.data, int(np.sqrt(a.size)))
+
+    @property
+    def d_camimg(self):
+        side = self.npix * self.nxsub
+        return self.buffer("camimg", dtype=np.uint16, shape=(side, side))
+
     def set_field_stop(self, mask):
         """Focal-plane field stop of the full pupil (n x n, fftshifted; None removes it)."""
         if mask is None:
@@ -379,9 +396,29 @@ class Centroider:
         call("aob_centro_load_weights", self.h, a.ctypes.data, int(a.size))
 
     def load_img(self, img, m=None, n=None):
+        """A float32 image, or a uint16 camera frame (host array, or a uint16
+        DeviceArray such as a sensor's ``d_camimg``, copied on the device)."""
+        if isinstance(img, DeviceArray):
+            if img.dtype != np.uint16:
+                raise TypeError("load_img from device memory takes a uint16 frame")
+            m_, n_ = img.shape
+            call("aob_centro_load_img_u16", self.h, img.ptr, int(m_), int(n_), 1, None)
+            return
+        img = np.asarray(img)
+        if img.dtype == np.uint16:
+            a = host_array(img, np.uint16)
+            call("aob_centro_load_img_u16", self.h, a.ctypes.data, int(img.shape[0]), int(img.shape[1]), 0, None)
+            return
         img = np.asarray(img, dtype=np.float32)
         a = host_array(img, np.float32)
         call("aob_centro_load_img", self.h, a.ctypes.data, int(img.shape[0]), int(img.shape[1]))
+
+    def set_lut_pix(self, lut):
+        a = host_array(lut, np.int32)
+        call("aob_centro_set_lut_pix", self.h, a.ctypes.data, int(a.size))
+
+    def calibrate_img_validpix(self, stream=None):
+        call("aob_centro_calibrate_img_validpix", self.h, stream)
 
     def set_dark(self, d, n=None):
         a = host_array(d, np.float32)

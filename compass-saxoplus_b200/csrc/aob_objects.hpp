@@ -39,6 +39,9 @@ struct aob_sh {
   aob::DevBuf<float> pupil;        // npup x npup amplitude
   aob::DevBuf<int32_t> istart, jstart, validsubsx, validsubsy, binmap;
   aob::DevBuf<int32_t> hrmap;  // nfft^2 positions in the ntot x ntot image (ntot != nfft)
+  int fakecam = 0, max_flux_per_pix = 0, max_pix_value = 0;  // uint16 camera frame of each image
+  aob::DevBuf<uint16_t> camimg;
+  aob::DevBuf<float> cam_dark, cam_flat;
   int fs_n = 0;                // field stop: side of its focal plane (0: none)
   aob::DevBuf<float> fs_mask;  // fs_n x fs_n focal-plane mask (fftshifted)
   aob::DevBuf<float> fs_field; // fs_n x fs_n complex filtered field (float pairs)
@@ -58,6 +61,8 @@ struct aob_sh {
   aob_sh(int device, int nxsub, int nvalid, int npix, int nphase, int nrebin, int nfft, int ntot,
          int npup, float pdiam, float nphot, float nphot4imat);
   void set_field_stop(const float *mask, int n);
+  void set_fakecam(int enable, int max_flux, int max_pix);
+  void digitalize(cudaStream_t s);
   void field_stop_prepare(cudaStream_t s);
   void load_arrays(const int32_t *binmap, const float *offsets, const float *fluxPerSub,
                    const int32_t *validsubsx, const int32_t *validsubsy, const int32_t *istart,
@@ -129,6 +134,9 @@ struct aob_centro {
   // image path when not attached to a sensor (load_img + calibrate_img)
   int img_m = 0, img_n = 0;
   aob::DevBuf<float> img_raw, img, dark, flat;
+  aob::DevBuf<uint16_t> img_raw_u16;  // camera frame (Rtc_UFF input)
+  bool raw_u16 = false;               // the last loaded frame is uint16
+  aob::DevBuf<int32_t> lut;           // pixel look-up table of the calibration
   // fused slopes staged by the sensor kernel
   aob::DevBuf<float> fused_slopes;
   uint64_t fused_gen = ~0ull;     // sensor image generation they belong to
@@ -141,7 +149,8 @@ struct aob_centro {
   void touch() { ++params_gen; }
   bool fused_ready() const;
   void get_cog(float *dev_slopes, cudaStream_t s);
-  void calibrate(cudaStream_t s);
+  void init_calib();
+  void calibrate(cudaStream_t s, bool valid_only = false);
 };
 
 // ---------------------------------------------------------------------------

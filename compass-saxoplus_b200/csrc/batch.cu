@@ -430,9 +430,10 @@ void aob_batch::build(bool noise) {
     aob_ls *c = l->ls;
     bool perturbed = false;
     for (auto &kv : c->perturb) perturbed |= kv.second.on;
-    AOB_REQUIRE(!perturbed && !c->open_loop && c->delay == 0.f && c->kind == AOB_CTRL_LS && !l->wfs->fs_n,
+    AOB_REQUIRE(!perturbed && !c->open_loop && c->delay == 0.f && c->kind == AOB_CTRL_LS && !l->wfs->fs_n &&
+                    !l->wfs->fakecam,
                 "batch: instance " + std::to_string(i) +
-                    ": needs an LS controller with delay 0, closed loop, no perturbation and no field stop");
+                    ": needs an LS controller with delay 0, closed loop, no perturbation, no field stop, no fakecam");
     AOB_REQUIRE(w->nfft == 16 || w->nfft == 32, "batch: instance " + std::to_string(i) + ": nfft must be 16 or 32");
     c->ensure_packed(c->prec);
     BatchInst &I = hi[i];

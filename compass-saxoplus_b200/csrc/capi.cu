@@ -153,6 +153,30 @@ int aob_sh_load_arrays(aob_sh *h, const int32_t *, const int32_t *hrmap, const i
   h->load_arrays(binmap, offsets, flux, vx, vy, istart, jstart, hrmap);
   AOB_API_END
 }
+int aob_sh_set_fakecam(aob_sh *h, int enable, int max_flux_per_pix, int max_pix_value) {
+  AOB_API_BEGIN
+  NEED(h);
+  h->set_fakecam(enable, max_flux_per_pix, max_pix_value);
+  AOB_API_END
+}
+int aob_sh_set_dark(aob_sh *h, const float *dark, int n) {
+  AOB_API_BEGIN
+  NEED(h); NEED(dark);
+  if (!h->fakecam) throw Error("sh.set_dark: enable fakecam first");
+  if ((int64_t)n * n != h->cam_dark.n) throw Error("sh.set_dark: the dark must match the image size");
+  AOB_CUDA(cudaSetDevice(h->device));
+  h->cam_dark.upload(dark, h->cam_dark.n);
+  AOB_API_END
+}
+int aob_sh_set_flat(aob_sh *h, const float *flat, int n) {
+  AOB_API_BEGIN
+  NEED(h); NEED(flat);
+  if (!h->fakecam) throw Error("sh.set_flat: enable fakecam first");
+  if ((int64_t)n * n != h->cam_flat.n) throw Error("sh.set_flat: the flat must match the image size");
+  AOB_CUDA(cudaSetDevice(h->device));
+  h->cam_flat.upload(flat, h->cam_flat.n);
+  AOB_API_END
+}
 int aob_sh_set_field_stop(aob_sh *h, const float *mask, int n) {
   AOB_API_BEGIN
   NEED(h);
@@ -211,7 +235,8 @@ int aob_sh_buffer(aob_sh *h, const char *which, void **p, int64_t *n) {
   }
   B("phase", phase) B("pupil", pupil) B("bincube", bincube) B("binimg", binimg) B("intensities", intensities)
   B("validsubsx", validsubsx) B("validsubsy", validsubsy) B("fluxPerSub", fluxPerSub) B("binmap", binmap)
-  B("offsets", offsets) B("istart", istart) B("jstart", jstart) B("slopes", slopes)
+  B("offsets", offsets) B("istart", istart) B("jstart", jstart) B("slopes", slopes) B("camimg", camimg)
+  B("dark", cam_dark) B("flat", cam_flat) B("hrmap", hrmap) B("submask", fs_mask)
 #undef B
   throw Error("sh.buffer: unknown buffer '" + w + "'");
   AOB_API_END
@@ -401,6 +426,39 @@ int aob_centro_load_img(aob_centro *c, const float *img, int m, int n) {
   c->img_m = m;
   c->img_n = n;
   c->img_raw.upload(img, (int64_t)m * n);
+  c->raw_u16 = false;
+  AOB_API_END
+}
+int aob_centro_load_img_u16(aob_centro *c, const uint16_t *img, int m, int n, int on_device, void *stream) {
+  AOB_API_BEGIN
+  NEED(c); NEED(img);
+  if (m <= 0 || n <= 0) throw Error("centro.load_img: bad size");
+  AOB_CUDA(cudaSetDevice(c->device));
+  const int64_t mn = (int64_t)m * n;
+  if (c->img_raw_u16.n != mn) c->img_raw_u16.alloc(mn);
+  c->img_m = m;
+  c->img_n = n;
+  AOB_CUDA(cudaMemcpyAsync(c->img_raw_u16.p, img, sizeof(uint16_t) * mn,
+                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, S(stream)));
+  if (!on_device) AOB_CUDA(cudaStreamSynchronize(S(stream)));
+  c->raw_u16 = true;
+  AOB_API_END
+}
+int aob_centro_set_lut_pix(aob_centro *c, const int32_t *lut, int n) {
+  AOB_API_BEGIN
+  NEED(c); NEED(lut);
+  if (n <= 0) throw Error("centro.set_lutPix: bad size");
+  for (int i = 0; i < n; ++i)
+    if (lut[i] < 0 || lut[i] >= n) throw Error("centro.set_lutPix: entry outside the image");
+  AOB_CUDA(cudaSetDevice(c->device));
+  if (c->lut.n != n) c->lut.alloc(n);
+  c->lut.upload(lut, n);
+  AOB_API_END
+}
+int aob_centro_calibrate_img_validpix(aob_centro *c, void *stream) {
+  AOB_API_BEGIN
+  NEED(c);
+  c->calibrate(S(stream), true);
   AOB_API_END
 }
 int aob_centro_set_dark(aob_centro *c, const float *d, int n) {
@@ -442,7 +500,12 @@ int aob_centro_buffer(aob_centro *c, const char *which, void **p, int64_t *n) {
     return AOB_OK;          \
   }
   B("validx", validx) B("validy", validy) B("centroids_ref", ref) B("weights", weights)
-  B("intensities", intensities) B("img_raw", img_raw) B("img", img) B("dark", dark) B("flat", flat)
+  B("intensities", intensities) B("img", img) B("dark", dark) B("flat", flat) B("lut", lut)
+  if (w == "img_raw") {  // the last loaded frame, float32 or uint16
+    *p = c->raw_u16 ? (void *)c->img_raw_u16.p : (void *)c->img_raw.p;
+    *n = c->raw_u16 ? c->img_raw_u16.n : c->img_raw.n;
+    return AOB_OK;
+  }
 #undef B
   throw Error("centro.buffer: unknown buffer '" + w + "'");
   AOB_API_END

@@ -268,9 +268,32 @@ static int bpcog_block(int n) {
   return n;
 }
 
-__global__ void calib_kernel(const float *raw, float *cal, const float *dark, const float *flat, int64_t n) {
+// Raw-image calibration through the pixel look-up table (calib_krnl,
+// libsutra/src.cu/sutra_centroider.cu:108-115): cal = (raw[lut] - dark) * flat,
+// raw in float32 or in the camera's uint16.
+template <typename Tin>
+__global__ void calib_kernel(const Tin *raw, float *cal, const float *dark, const float *flat, const int32_t *lut,
+                             int64_t n) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
-    cal[t] = (raw[t] - dark[t]) * flat[t];
+    cal[t] = ((float)raw[lut[t]] - dark[t]) * flat[t];
+}
+
+// The same calibration on the valid pixels only, the rest of the image at zero
+// (calibrate_img_validPix, sutra_centroider.cpp:194-223): the npix x npix window of
+// every valid sub-aperture (calibration_validPix_sh_krnl, sutra_centroider.cu:68-90)
+// or every listed pixel (calibration_validPix_pyr_krnl, :92-104).
+template <typename Tin>
+__global__ void calib_valid_kernel(const Tin *raw, float *cal, const float *dark, const float *flat,
+                                   const int32_t *lut, const int32_t *vx, const int32_t *vy, int nvalid, int npix,
+                                   int size) {
+  const int npix2 = npix * npix;
+  const int64_t lim = (int64_t)size * size;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < (int64_t)nvalid * npix2;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(t / npix2), p = (int)(t - (int64_t)k * npix2);
+    const int64_t i = (int64_t)(p % npix + vx[k]) + (int64_t)(p / npix + vy[k]) * size;
+    if (i < lim) cal[i] = ((float)raw[lut[i]] - dark[i]) * flat[i];
+  }
 }
 
 }  // namespace aob
@@ -296,9 +319,9 @@ bool aob_centro::fused_ready() const {
          fused_params_gen == params_gen;
 }
 
-void aob_centro::calibrate(cudaStream_t s) {
-  AOB_REQUIRE(img_raw.p != nullptr, "calibrate_img: image not loaded");
-  AOB_CUDA(cudaSetDevice(device));
+// dark 0, flat 1 and the identity pixel table for an m x n image when absent (init_calib,
+// sutra_centroider.cpp:104-127)
+void aob_centro::init_calib() {
   const int64_t n = (int64_t)img_m * img_n;
   if (!img.p || img.n != n) img.alloc(n);
   if (!dark.p || dark.n != n) dark.alloc(n);
@@ -307,8 +330,43 @@ void aob_centro::calibrate(cudaStream_t s) {
     std::vector<float> one(n, 1.f);
     flat.upload(one.data(), n);
   }
-  calib_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, s>>>(img_raw.p, img.p, dark.p, flat.p, n);
-  AOB_LAUNCH_CHECK("calib_kernel");
+  if (!lut.p || lut.n != n) {
+    lut.alloc(n);
+    std::vector<int32_t> id(n);
+    for (int64_t i = 0; i < n; ++i) id[i] = (int32_t)i;
+    lut.upload(id.data(), n);
+  }
+}
+
+void aob_centro::calibrate(cudaStream_t s, bool valid_only) {
+  AOB_REQUIRE(raw_u16 ? img_raw_u16.p != nullptr : img_raw.p != nullptr, "calibrate_img: image not loaded");
+  AOB_CUDA(cudaSetDevice(device));
+  init_calib();
+  const int64_t n = (int64_t)img_m * img_n;
+  if (!valid_only) {
+    const int grid = (int)std::min<int64_t>((n + 255) / 256, 4096);
+    if (raw_u16)
+      calib_kernel<uint16_t><<<grid, 256, 0, s>>>(img_raw_u16.p, img.p, dark.p, flat.p, lut.p, n);
+    else
+      calib_kernel<float><<<grid, 256, 0, s>>>(img_raw.p, img.p, dark.p, flat.p, lut.p, n);
+    AOB_LAUNCH_CHECK("calib_kernel");
+    return;
+  }
+  AOB_REQUIRE(validx.p != nullptr, "calibrate_img_validPix: valid positions not loaded");
+  // pyramid / masked-pixel centroiders list single pixels; SH ones npix x npix windows
+  const bool pixels = type == AOB_CENTRO_PYR || type == AOB_CENTRO_MASKEDPIX;
+  const int nv = (int)validx.n, np = pixels ? 1 : npix;
+  AOB_REQUIRE(np > 0, "calibrate_img_validPix: npix not set");
+  AOB_CUDA(cudaMemsetAsync(img.p, 0, sizeof(float) * n, s));
+  const int64_t work = (int64_t)nv * np * np;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, 4096));
+  if (raw_u16)
+    calib_valid_kernel<uint16_t><<<grid, 256, 0, s>>>(img_raw_u16.p, img.p, dark.p, flat.p, lut.p, validx.p,
+                                                      validy.p, nv, np, img_m);
+  else
+    calib_valid_kernel<float><<<grid, 256, 0, s>>>(img_raw.p, img.p, dark.p, flat.p, lut.p, validx.p, validy.p, nv,
+                                                   np, img_m);
+  AOB_LAUNCH_CHECK("calib_valid_kernel");
 }
 
 void aob_centro::get_cog(float *dev_slopes, cudaStream_t s) {

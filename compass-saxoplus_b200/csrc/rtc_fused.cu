@@ -381,7 +381,7 @@ bool aob_loop::launch_fused(bool noise, cudaStream_t s, bool frame_on_device, bo
   aob_ls *c = ls;
   bool perturbed = false;
   for (auto &kv : c->perturb) perturbed |= kv.second.on;
-  if (perturbed || c->open_loop || centro->type > 2 || c->kind != AOB_CTRL_LS || w->fs_n) return false;
+  if (perturbed || c->open_loop || centro->type > 2 || c->kind != AOB_CTRL_LS || w->fs_n || w->fakecam) return false;
   c->ensure_packed(c->prec);
   RtcFusedArgs A{};
   aob_centro *fc = w->make_args(noise, c->centroids.p, frame_on_device ? d_frame.p : nullptr, A.sh);

@@ -84,6 +84,19 @@ __global__ void fs_mask_kernel(float2 *d, const float *mask, int64_t n2) {
   }
 }
 
+// fakecam (SutraWfsSH::comp_image, sutra_wfs_sh.cpp:623-643, digitalize_krnl,
+// libsutra/src.cu/sutra_wfs.cu:2243-2255): the image as a uint16 camera frame,
+// min((img * flat + dark) / max_flux_per_pix, 1) * max_pix_value, truncated
+// (the float-to-integer conversion saturates at 0 and 65535).
+__global__ void digitalize_kernel(uint16_t *cam, const float *img, const float *dark, const float *flat,
+                                  int max_flux, int max_pix, int64_t n) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    float v = (img[t] * flat[t] + dark[t]) / (float)max_flux;
+    v = v < 1.f ? v : 1.f;
+    cam[t] = (uint16_t)(v * (float)max_pix);
+  }
+}
+
 __global__ void sh_fill_image_kernel(float *img, const float *cube, const int32_t *vx,
                                      const int32_t *vy, int npix, int nvalid, int size) {
   const int npix2 = npix * npix;
@@ -406,6 +419,33 @@ void aob_sh::comp_image_to(bool with_noise, cudaStream_t s, float *slopes_dst, c
     launch_sh_pd<64>(P, nvalid, S, sm, s);
   AOB_LAUNCH_CHECK("sh_image_kernel");
   after_image(P, c, slopes_dst == nullptr);
+  if (fakecam) digitalize(s);
+}
+
+void aob_sh::set_fakecam(int enable, int max_flux, int max_pix) {
+  AOB_REQUIRE(!enable || (max_flux > 0 && max_pix > 0 && max_pix <= 65535),
+              "sh.set_fakecam: max_flux_per_pix > 0 and 0 < max_pix_value <= 65535 required");
+  AOB_CUDA(cudaSetDevice(device));
+  fakecam = enable ? 1 : 0;
+  max_flux_per_pix = max_flux;
+  max_pix_value = max_pix;
+  const int64_t n = binimg.n;
+  if (fakecam && camimg.n != n) {
+    camimg.alloc(n);
+    if (cam_dark.n != n) cam_dark.alloc(n);  // dark 0 (reset), flat 1 (sutra_wfs_sh.cpp:100-104)
+    if (cam_flat.n != n) {
+      cam_flat.alloc(n);
+      std::vector<float> one(n, 1.f);
+      cam_flat.upload(one.data(), n);
+    }
+  }
+}
+
+void aob_sh::digitalize(cudaStream_t s) {
+  const int64_t n = binimg.n;
+  digitalize_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, s>>>(
+      camimg.p, binimg.p, cam_dark.p, cam_flat.p, max_flux_per_pix, max_pix_value, n);
+  AOB_LAUNCH_CHECK("digitalize_kernel");
 }
 
 void aob_sh::fill_binimage(cudaStream_t s) {

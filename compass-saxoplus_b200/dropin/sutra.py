@@ -14,6 +14,9 @@ Covered (the calls shesha's supervisor makes on the RTC path):
   ``comp_voltage``, ``do_clipping``, ``set_gain``, ``set_modal_gains``,
   ``imat_svd``, ``build_cmat``, ``set_centroids_ref``, ``do_calibrate_img``,
   ``d_centro`` / ``d_control``;
+* ``Rtc_UFF``, the camera path: centroiders that load uint16 frames (a
+  sensor's ``d_camimg`` under ``fakecam``) and calibrate them with dark, flat and
+  a pixel look-up table (``set_lutPix``, ``calibrate_img_validPix``);
 * the centroiders (centroider.cpp:83-352), the LS controller (controller.cpp,
   controller_ls.cpp) and the generic controller (controller_generic.cpp) with
   their ``d_*`` buffers and setters.
@@ -112,6 +115,15 @@ class SHWFS(_WfsBase):
     def fill_binimage(self, async_=False):
         self._w.fill_binimage()
 
+    # fakecam (Sensors(..., fakecam, max_flux_per_pix, max_pix_value)): the uint16 frame
+    d_camimg = property(lambda self: self._w.d_camimg)
+
+    def set_dark(self, dark, n):
+        self._w.set_dark(np.asarray(dark, np.float32), int(n))
+
+    def set_flat(self, flat, n):
+        self._w.set_flat(np.asarray(flat, np.float32), int(n))
+
 
 class PYRWFS(_WfsBase):
     """SutraWfs_PyrHR (wfs_pyrhr.cpp:131-163); npup here is the reference's number of
@@ -142,6 +154,8 @@ class Sensors:
                     float(_arr(pdiam)[i]), float(_arr(nphot)[i]), float(_arr(nphot4imat)[i]), self.device)
             if type[i] == "sh":
                 self._wfs.append(SHWFS(*args))
+                if bool(_arr(fakecam)[i]):
+                    self._wfs[-1]._w.set_fakecam(True, int(_arr(max_flux_per_pix)[i]), int(_arr(max_pix_value)[i]))
             elif type[i] == "pyrhr":
                 self._wfs.append(PYRWFS(*args))
             else:
@@ -171,7 +185,8 @@ class Sensors:
 class Centroider:
     """SutraCentroider{Cog,Tcog,Wcog,Pyr} (centroider.cpp:83-352)."""
 
-    def __init__(self, nvalid, offset, scale, typec, device, wfs=None):
+    def __init__(self, nvalid, offset, scale, typec, device, wfs=None, tin=np.float32):
+        self._tin = tin  # image type of load_img: float32 (Rtc_FFF) or uint16 (Rtc_UFF)
         if typec == "maskedpix" and wfs is not None:
             nvalid = 4 * wfs._w.nvalid  # one slope per valid pixel (maskedPix.cpp:35-36)
         self._c = _core.Centroider(int(nvalid), float(offset), float(scale), typec, device=int(device))
@@ -241,9 +256,24 @@ class Centroider:
         self._c.set_centroids_ref(np.asarray(refslopes, np.float32))
 
     def load_img(self, img, *args):
-        img = np.asarray(img, np.float32)
+        """A frame from the host (cast to the RTC's input type, as the reference's
+        pybind11 binding does) or, for a uint16 RTC, a uint16 device array such as
+        a sensor's ``d_camimg``."""
+        if isinstance(img, _core.DeviceArray):
+            self._img_shape = tuple(img.shape)
+            self._c.load_img(img)
+            return 0
+        img = np.asarray(img, self._tin)
         self._img_shape = img.shape if img.ndim == 2 else None
         self._c.load_img(img)
+        return 0
+
+    def calibrate_img_validPix(self):
+        self._c.calibrate_img_validpix()
+        return 0
+
+    def set_lutPix(self, lutPix, n=None):
+        self._c.set_lut_pix(np.asarray(lutPix, np.int32))
         return 0
 
     def calibrate_img(self):
@@ -399,6 +429,8 @@ class Rtc_FFF:
     slopes of the centroiders listed in its ``centro_idx`` (all of them, in
     order, by default), one block of 2 nvalid after the other."""
 
+    _tin = np.float32  # image type the centroiders load
+
     def __init__(self):
         self.d_centro = []
         self.d_control = []
@@ -407,7 +439,7 @@ class Rtc_FFF:
         if typec not in ("cog", "tcog", "wcog", "bpcog", "pyr", "maskedpix"):
             raise ValueError(f"add_centroider: centroider type {typec!r} is not supported "
                              "(cog, tcog, wcog, bpcog, pyr, maskedpix)")
-        self.d_centro.append(Centroider(nvalid, offset, scale, typec, device, wfs))
+        self.d_centro.append(Centroider(nvalid, offset, scale, typec, device, wfs, tin=self._tin))
         return 0
 
     def add_controller(self, context, typec, device, delay, nslope, nactu, nslope_buffers=0, nstates=0,
@@ -491,3 +523,12 @@ class Rtc_FFF:
             cen.set_centroids_ref(ref[off:off + n])
             off += n
         return 0
+
+
+class Rtc_UFF(Rtc_FFF):
+    """SutraRtc<uint16_t, float, float> (rtc.cpp; sutra.cpp:62-103): the camera
+    path -- the centroiders load uint16 frames (load_img from the host or a
+    sensor's d_camimg), calibrate them to float with dark, flat and the pixel
+    look-up table, then compute as Rtc_FFF does."""
+
+    _tin = np.uint16

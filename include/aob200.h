@@ -85,6 +85,17 @@ int aob_sh_load_arrays(aob_sh *h, const int32_t *phasemap, const int32_t *hrmap,
  * field stop run the separate-kernel path (not the fused RTC kernel or the
  * batch). */
 int aob_sh_set_field_stop(aob_sh *h, const float *mask, int n);
+/* fakecam (Sensors(..., fakecam, max_flux_per_pix, max_pix_value),
+ * sutra_wfs_sh.cpp:95-105,623-643): every image is also digitised into the
+ * uint16 frame "camimg", min((binimg * flat + dark) / max_flux_per_pix, 1) *
+ * max_pix_value truncated (digitalize_krnl, libsutra/src.cu/sutra_wfs.cu:
+ * 2243-2255); dark starts at 0 and flat at 1.  Steps with fakecam run the
+ * separate-kernel path. */
+int aob_sh_set_fakecam(aob_sh *h, int enable, int max_flux_per_pix, int max_pix_value);
+/* Wfs.set_dark / set_flat (python_module/sutra/src/wfs.cpp) of the fakecam
+ * digitisation: n x n with n the image side. */
+int aob_sh_set_dark(aob_sh *h, const float *dark, int n);
+int aob_sh_set_flat(aob_sh *h, const float *flat, int n);
 /* SutraWfs::set_pupil (sutra_wfs.cpp) -- npup x npup amplitude. */
 int aob_sh_set_pupil(aob_sh *h, const float *pupil_host);
 /* SutraWfs::set_noise (sutra_wfs.cpp:123-141); the generator is the
@@ -99,7 +110,8 @@ int aob_sh_get_frame(aob_sh *h, uint64_t *frame);
 /* Device pointers of the sensor's buffers (the Wfs d_* properties,
  * python_module/sutra/src/wfs.cpp:54-225). which: "phase", "pupil",
  * "bincube", "binimg", "intensities", "validsubsx", "validsubsy",
- * "fluxPerSub", "binmap", "offsets", "istart", "jstart", "slopes". */
+ * "fluxPerSub", "binmap", "offsets", "istart", "jstart", "slopes", "hrmap",
+ * "submask" (field stop), "camimg" (uint16), "dark", "flat" (fakecam). */
 int aob_sh_buffer(aob_sh *h, const char *which, void **dev_ptr, int64_t *nelem);
 /* SutraWfsSH::comp_image(noise) (sutra_wfs_sh.cpp:623-643): fused field fill,
  * pruned 2-D DFT, |E|^2, binning, flux normalisation, photon/readout noise
@@ -216,6 +228,20 @@ int aob_centro_load_img(aob_centro *c, const float *img, int m, int n);
 int aob_centro_set_dark(aob_centro *c, const float *dark, int n);
 int aob_centro_set_flat(aob_centro *c, const float *flat, int n);
 int aob_centro_calibrate_img(aob_centro *c, void *stream);
+/* The camera path (Rtc_UFF: uint16 input, SutraCentroider<uint16_t, float>,
+ * sutra_centroider.cpp:246-285): load_img of an m x n uint16 frame from host
+ * (on_device 0; the call waits for the copy) or device memory.  calibrate_img
+ * then gives float (raw[lut] - dark) * flat (calib_krnl,
+ * libsutra/src.cu/sutra_centroider.cu:108-115); "img_raw" returns the last
+ * loaded frame in its type. */
+int aob_centro_load_img_u16(aob_centro *c, const uint16_t *img, int m, int n, int on_device, void *stream);
+/* set_lutPix (sutra_centroider.cpp:163-172): raw pixel read for each image
+ * pixel (identity until set), n = m * n entries, each < n. */
+int aob_centro_set_lut_pix(aob_centro *c, const int32_t *lut, int n);
+/* calibrate_img_validPix (sutra_centroider.cpp:194-223): the calibration on the
+ * valid pixels only (SH: the npix x npix window of each valid sub-aperture;
+ * pyramid and masked-pixel: each listed pixel), the rest of the image zero. */
+int aob_centro_calibrate_img_validpix(aob_centro *c, void *stream);
 /* get_cog (sutra_centroider_cog.cpp:51-98): slopes into dev_slopes (2*nvalid
  * floats, device) and intensities into the centroider's buffer. */
 int aob_centro_get_cog(aob_centro *c, float *dev_slopes, void *stream);

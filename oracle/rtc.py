@@ -117,3 +117,36 @@ class LsController:
                 self.perturb[name][1] = cpt + 1 if cpt < buf.shape[0] - 1 else 0
         self.clip()
         return self.com_clipped
+
+
+def digitalize(img, dark, flat, max_flux_per_pix, max_pix_value):
+    """uint16 camera frame of a sensor image (digitalize_krnl,
+    libsutra/src.cu/sutra_wfs.cu:2243-2255): min((img * flat + dark) /
+    max_flux_per_pix, 1) * max_pix_value, truncated, saturating at 0 and 65535."""
+    v = (np.asarray(img, np.float64) * flat + dark) / float(max_flux_per_pix)
+    v = np.minimum(v, 1.0) * float(max_pix_value)
+    return np.clip(np.trunc(v), 0, 65535).astype(np.uint16)
+
+
+def calibrate(raw, dark, flat, lut=None, valid=None, npix=None):
+    """Calibrated image (raw[lut] - dark) * flat (calib_krnl,
+    libsutra/src.cu/sutra_centroider.cu:108-115), arrays in [x, y] order with the
+    lut over the flattened Fortran-order image.  valid = (validx, validy): only
+    those windows (npix x npix, or single pixels when npix is None) are
+    calibrated, the rest is zero (calibrate_img_validPix,
+    sutra_centroider.cpp:194-223)."""
+    raw = np.asarray(raw)
+    m, n = raw.shape
+    flat_raw = raw.ravel(order="F").astype(np.float64)
+    idx = np.arange(m * n) if lut is None else np.asarray(lut).ravel()
+    cal = (flat_raw[idx] - np.asarray(dark, np.float64).ravel(order="F")) * np.asarray(flat, np.float64).ravel(order="F")
+    if valid is None:
+        return cal.reshape(m, n, order="F")
+    keep = np.zeros(m * n, bool)
+    vx, vy = valid
+    w = 1 if npix is None else npix
+    for x0, y0 in zip(vx, vy):
+        xs = (np.arange(w)[:, None] + x0 + (np.arange(w)[None, :] + y0) * m).ravel()
+        keep[xs[xs < m * n]] = True
+    out = np.where(keep, cal, 0.0)
+    return out.reshape(m, n, order="F")
