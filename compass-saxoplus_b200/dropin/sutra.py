@@ -198,6 +198,7 @@ class Centroider:
         self.nmax = 0
         self.wfs = wfs
         self._img_shape = None  # (m, n) of the loaded image (the carma objects are 2-D)
+        self._raw_dtype = np.float32  # type of the loaded frame
         if wfs is not None:
             self._c.attach(wfs._w)
 
@@ -206,7 +207,7 @@ class Centroider:
     d_dark = property(lambda self: self._c.buffer("dark", shape=self._img_shape))
     d_flat = property(lambda self: self._c.buffer("flat", shape=self._img_shape))
     d_img = property(lambda self: self._c.buffer("img", shape=self._img_shape))
-    d_img_raw = property(lambda self: self._c.buffer("img_raw", shape=self._img_shape))
+    d_img_raw = property(lambda self: self._c.buffer("img_raw", dtype=self._raw_dtype, shape=self._img_shape))
     d_centroids_ref = property(lambda self: self._c.buffer("centroids_ref"))
     d_intensities = property(lambda self: self._c.buffer("intensities"))
     d_validx = property(lambda self: self._c.buffer("validx", np.int32))
@@ -261,10 +262,12 @@ class Centroider:
         a sensor's ``d_camimg``."""
         if isinstance(img, _core.DeviceArray):
             self._img_shape = tuple(img.shape)
+            self._raw_dtype = img.dtype
             self._c.load_img(img)
             return 0
         img = np.asarray(img, self._tin)
         self._img_shape = img.shape if img.ndim == 2 else None
+        self._raw_dtype = img.dtype
         self._c.load_img(img)
         return 0
 
