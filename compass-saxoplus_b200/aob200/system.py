@@ -17,6 +17,7 @@ import numpy as np
 
 from . import core, dm_geometry, optics, turbulence
 from . import geometry as G
+from ._lib import call
 
 
 @dataclass
@@ -133,14 +134,33 @@ class ShAoSystem:
         self.centro.get_cog(dst.ptr, stream)
         return np.array(dst)
 
-    def calibrate(self, push=None, maxcond=None):
+    def interaction_matrix(self, push=None, chunk=0):
+        """Push-pull interaction matrix of the DM seen by the sensor, every actuator
+        poked in one batch (aob_imat_build: four launches per chunk of actuators)."""
+        push = self.cfg.push4imat if push is None else push
+        self.centro.attach(self.wfs)
+        imat = np.zeros((self.ls.nslope, self.nactu), dtype=np.float32)
+        self.ls.set_imat(imat)  # allocates the controller's imat buffer
+        out = self.ls.buffer("imat")
+        call("aob_imat_build", self.wfs.h, self.centro.h, self.dm.h, float(self.dm_off), float(self.dm_off),
+             float(push), int(chunk), out.ptr, None)
+        return np.array(self.ls.buffer("imat", shape=(self.ls.nslope, self.nactu)))
+
+    def calibrate(self, push=None, maxcond=None, batched=True):
         """Push-pull interaction matrix through DM -> sensor, then the filtered LS inverse.
 
-        Modes whose singular value is below the largest over ``maxcond`` are
-        filtered (the eigenvalues of imat^T imat are squared singular values).
+        ``batched``: all actuators in one batch (interaction_matrix), else one poke
+        after the other through the separate calls.  Modes whose singular value is
+        below the largest over ``maxcond`` are filtered (the eigenvalues of
+        imat^T imat are squared singular values).
         """
         push = self.cfg.push4imat if push is None else push
         maxcond = self.cfg.maxcond if maxcond is None else maxcond
+        if batched:
+            imat = self.interaction_matrix(push)
+            self.dm.set_com(np.zeros(self.nactu, dtype=np.float32))
+            self.dm.comp_shape()
+            return self._finish_calibration(imat, maxcond)
         imat = np.zeros((self.ls.nslope, self.nactu), dtype=np.float32)
         com = np.zeros(self.nactu, dtype=np.float32)
         for a in range(self.nactu):
@@ -158,6 +178,9 @@ class ShAoSystem:
             imat[:, a] = (sp - sm) / (2 * push)
         self.dm.set_com(com)
         self.dm.comp_shape()
+        return self._finish_calibration(imat, maxcond)
+
+    def _finish_calibration(self, imat, maxcond):
         self.imat = imat
         self.ls.set_imat(imat)
         self.ls.svdec_imat()

@@ -191,6 +191,7 @@ struct ShMeta {
 // cube (contiguous) and its npix x npix window of the binned image.
 __device__ __forceinline__ void sh_store_subap(const ShKernelArgs &P, int k, const float *bs, int vx, int vy,
                                                int lane) {
+  if (!P.bincube) return;  // (slopes only: the batched interaction-matrix images keep no cube or image)
   const int npix = P.npix, npix2 = npix * npix;
   for (int p = lane; p < npix2; p += 32) {
     const float v = bs[p];

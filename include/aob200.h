@@ -459,6 +459,20 @@ int aob_dm_comp_shape(aob_dm *d, const float *dev_com, void *stream);
 /* which: "shape", "com". */
 int aob_dm_buffer(aob_dm *d, const char *which, void **dev_ptr, int64_t *nelem);
 
+/* ---- interaction matrix ------------------------------------------------------ *
+ * SutraRtc::do_imat (libsutra/src.cpp/sutra_rtc.cpp:150-292), every actuator of
+ * the DM poked in one batch: the push (+push) and pull (-push) DM shapes of a
+ * chunk of actuators (chunk 0 = all), their bilinear raytrace onto the sensor's
+ * npup x npup phase grid at offset (xoff, yoff) in the DM screen, the sensor
+ * images with the attached CoG-family centroider over all pokes in one launch
+ * (noise-free, the sensor's current photon count), and the columns
+ * (s_push - s_pull) / (2 push) into dev_imat, nslope x nact column-major on the
+ * device.  Equal bit for bit to poking one actuator after the other with
+ * aob_dm_comp_shape, aob_raytrace, aob_sh_comp_image and aob_centro_get_cog.
+ * Needs about 2 chunk (dim^2 + npup^2) floats of scratch; waits for the stream. */
+int aob_imat_build(aob_sh *w, aob_centro *c, aob_dm *dm, float xoff, float yoff, float push, int chunk,
+                   float *dev_imat, void *stream);
+
 /* ---- raytracing ------------------------------------------------------------ *
  * SutraSource::raytrace (libsutra/src.cpp/sutra_source.cpp:222-320) with the
  * bilinear generic_raytrace (sutra_target.cu:25-70): out (nx x ny) = (reset ? 0 :

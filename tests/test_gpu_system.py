@@ -31,6 +31,21 @@ def test_interaction_matrix_is_sane(plain16):
     assert np.median(d) > 0.9
 
 
+def test_batched_interaction_matrix_equals_poke_by_poke():
+    """aob_imat_build (all actuators in one batch, one sensor launch) gives the
+    matrix of poking one actuator after the other through the separate calls,
+    bit for bit, also in chunks."""
+    from aob200 import system
+
+    s = system.ShAoSystem(system.plain16())
+    seq = s.calibrate(batched=False).copy()
+    s2 = system.ShAoSystem(system.plain16())
+    bat = s2.interaction_matrix()
+    np.testing.assert_array_equal(bat, seq)
+    np.testing.assert_array_equal(s2.interaction_matrix(chunk=37), seq)
+    assert np.abs(seq).max() > 0
+
+
 def test_closed_loop_raises_strehl(plain16):
     s = plain16
     s.target.reset_le()
