@@ -27,9 +27,10 @@ modulation points over 512 x 512 FFTs, slopes and a 1600-actuator LS MVM),
 ``mlp`` (the learned reconstructor: batch-1 inference against the LS MVM and
 training throughput on the tensor cores).
 
---impl reference runs the reference-algorithm CPU restatement (the reference
-has no CPU implementation of this path; its GPU code needs its own CMake build)
-as the baseline arm.  Multi-GPU (torchrun): the path does not shard -- every
+--impl reference runs the reference's own implementation of the path, its
+sutra CUDA code built from its sources into oracle/_ref (oracle/build_ref.py),
+on the same GPU through its Python API, as the baseline arm; without that
+build or a GPU it falls back to the float64 CPU restatement of its algorithm.  Multi-GPU (torchrun): the path does not shard -- every
 rank runs an independent replica; value = total steps / max-over-ranks time.
 """
 
@@ -198,6 +199,38 @@ def cpu_baseline(setup, budget_s=12.0, max_iters=400):
             "sample": f"{n} iterations of the saxo40 RTC step (float64 NumPy/SciPy, {loop.workers} threads)"}
 
 
+def run_reference_gpu(args, setup):
+    """The reference's own implementation of the path -- its sutra CUDA code,
+    built from its sources into oracle/_ref -- on this GPU, through its Python
+    API in the supervisor's order: each step copies the phase from the host,
+    forms the SH image with photon and readout noise, computes the wCoG slopes
+    with threshold, the LS commands and the voltages, and reads the voltages
+    back to the host.  The L2 cache is flushed between steps (outside the
+    timed span); the step is timed by the host clock around the calls (they
+    end with the voltages on the host)."""
+    import torch
+
+    from aob200.workloads import von_karman_screens
+    from oracle.ref_sutra import RefShLoop
+
+    g = setup.geom
+    loop = RefShLoop(g, setup.cmat, setup.centroider, setup.threshold, setup.weights, noise=setup.noise, seed=1234)
+    screens = von_karman_screens(g.tel.n, 8.0 / g.tel.pupdiam, 0.14, 25.0, 8, seed=0)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    for i in range(args.warmup):
+        loop.step(screens[i % 8])
+    total = 0.0
+    with ClockSampler(0) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            loop.step(screens[i % 8])
+            total += time.perf_counter() - t0
+    v = args.steps / total
+    return v, clk.summary()
+
+
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -205,6 +238,37 @@ def run_reference(args):
     from aob200.workloads import sh_loop_setup
 
     setup = sh_loop_setup("saxo40")
+    workload = ("saxo40: 40x40 SH, 1248 valid, 6x6 px, Nfft 32, wCoG+thr, photon+0.5e- noise, "
+                "1377x2496 LS MVM")
+    from oracle import ref_sutra
+
+    gpu = False
+    try:
+        import torch
+
+        gpu = torch.cuda.is_available() and ref_sutra.available()
+    except Exception:
+        gpu = False
+    if gpu:
+        v, clocks = run_reference_gpu(args, setup)
+        g = setup.geom
+        sample = (f"{args.steps} RTC iterations of the reference's sutra CUDA build (oracle/_ref) on the GPU, "
+                  "driven from one host thread through its Python API")
+        line = {
+            "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload, "device": "gpu: the reference's own sutra CUDA code, built from its sources",
+                       "l2": "flushed before every timed step (256 MB write)",
+                       "timing": "host clock per step: phase from host, comp_image, do_centroids, do_control, "
+                                 "comp_voltage, voltages to host"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": g.tel.n * g.tel.n * 4,
+                    "d2h_bytes_per_step": setup.nactu * 4},
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+        return 0
     from oracle.loop_cpu import CpuShLoop
     from aob200.workloads import von_karman_screens
 
@@ -226,8 +290,8 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "saxo40: 40x40 SH, 1248 valid, 6x6 px, Nfft 32, wCoG+thr, photon+0.5e- noise, "
-                               "1377x2496 LS MVM", "device": "cpu"},
+        "config": {"workload": workload, "device": "cpu (the reference's CUDA build is not available here: "
+                                                   "its float64 NumPy restatement)"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": res[0]["cores"], "kind": "port",
                          "sample": res[0]["sample"]},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -34,8 +34,9 @@ for p in (os.path.join(ROOT, "oracle", "_ref"), os.path.join(ROOT, "compass-saxo
     if p not in sys.path:
         sys.path.insert(0, p)
 
-import carma  # noqa: E402  (the reference's module, built by oracle/build_ref.py)
-import sutra  # noqa: E402
+from oracle import ref_sutra  # noqa: E402
+
+carma, sutra = ref_sutra.modules()  # the reference's modules, built by oracle/build_ref.py
 
 from aob200.workloads import von_karman_screens  # noqa: E402
 
@@ -49,43 +50,21 @@ def phase_screen(n, pupdiam, seed):
 
 
 def _telescope(ctx, tel):
-    sp = tel.spupil.astype(np.float32)
-    return sutra.Telescope(ctx, sp.shape[0], int(np.where(sp > 0)[0].size), sp, tel.mpupil.shape[0],
-                           tel.mpupil.astype(np.float32))
+    return ref_sutra.telescope(sutra, ctx, tel)
 
 
 def _initgs(sensors, n, lam, mag):
-    one = lambda v, t=np.float32: np.array([v], dtype=t)  # noqa: E731
-    sensors.initgs(one(0.0), one(0.0), one(lam), one(mag), 1e11, one(n, np.int64), one(-1.0),
-                   one(1234, np.int64), one(1.0), one(0.0), one(0.0), one(0.0))
+    ref_sutra.initgs(sensors, n, lam, mag)
 
 
 def _ls(ctx, rtc, nslope, cmat):
-    rtc.add_controller(ctx, "ls", ctx.active_device, 0.0, nslope, NACTU, idx_centro=np.zeros(1, np.int32),
-                       ncentro=1)
-    c = rtc.d_control[0]
-    c.set_cmat(cmat)
-    c.set_gain(GAIN)
-    c.set_modal_gains(np.ones(NACTU, np.float32))
-    return c
+    return ref_sutra.add_ls(ctx, rtc, nslope, cmat, GAIN)
 
 
 def run_sh(ctx, name, seed):
     g = sh_geometry(name)
     tel = _telescope(ctx, g.tel)
-    i64 = lambda v: np.array([v], dtype=np.int64)  # noqa: E731
-    f32 = lambda v: np.array([v], dtype=np.float32)  # noqa: E731
-    sensors = sutra.Sensors(ctx, tel, ["sh"], 1, i64(g.nxsub), i64(g.nvalid), i64(1), i64(g.npix), i64(g.pdiam),
-                            i64(g.nrebin), i64(g.nfft), i64(g.ntot), i64(g.tel.n), f32(g.subapd), f32(g.nphotons),
-                            f32(g.nphotons), np.zeros(1, np.int32), np.zeros(1, bool), np.zeros(1, np.int32),
-                            np.zeros(1, np.int32), ctx.active_device, False)
-    _initgs(sensors, g.tel.n, g.wavelength_um, 8.0)
-    wfs = sensors.d_wfs[0]
-    kernel = np.zeros((g.ntot, g.ntot), np.complex64)  # used only by the kernel convolution (off)
-    wfs.load_arrays(g.phasemap, g.hrmap, g.binmap, g.halfxy, g.fluxPerSub, g.validsubsx, g.validsubsy,
-                    g.validpuppixx, g.validpuppixy, g.ttprojmat, kernel)
-    if g.submask is not None:  # wfs_init.py:233-234
-        sensors.set_field_stop(0, g.submask.astype(np.float32), g.submask.shape[0])
+    sensors, wfs = ref_sutra.sh_sensors(sutra, ctx, tel, g)
     phase = phase_screen(g.tel.n, g.tel.pupdiam, seed)
     wfs.d_gs.set_phase(phase)
     nslope = 2 * g.nvalid
@@ -99,16 +78,7 @@ def run_sh(ctx, name, seed):
             out["binimg"] = np.array(wfs.d_binimg)
             out["intensities"] = np.array(wfs.d_intensities)
         rtc = sutra.Rtc_FFF()
-        rtc.add_centroider(ctx, g.nvalid, g.npix // 2.0 - 0.5, g.pixsize, False, ctx.active_device, kind, wfs)
-        ce = rtc.d_centro[0]
-        ce.load_validpos(g.validsubsx, g.validsubsy, g.nvalid)
-        ce.set_npix(g.npix)
-        if kind in ("tcog", "wcog"):
-            ce.set_threshold(thr)
-        if kind == "wcog":
-            ce.init_weights()
-            w = wcog_weights(g.npix)
-            ce.load_weights(w, w.ndim)
+        ref_sutra.add_centroider(ctx, rtc, wfs, g, kind, thr, wcog_weights(g.npix))
         c = _ls(ctx, rtc, nslope, cmat)
         rtc.do_centroids(0)
         rtc.do_control(0)
