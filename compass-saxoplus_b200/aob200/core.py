@@ -632,9 +632,12 @@ class Loop:
         call("aob_loop_kernels_per_step", self.h, ctypes.addressof(n))
         return n.value
 
-    def step(self, host_phase=None, host_voltage=None, noise=True, stream=None):
-        """host_phase / host_voltage: numpy float32 arrays (pinned for speed) or None."""
-        call("aob_loop_step", self.h, addr(host_phase), addr(host_voltage), 1 if noise else 0, stream)
+    def step(self, host_phase=None, host_voltage=None, noise=True, stream=None, wait=True):
+        """host_phase / host_voltage: numpy float32 arrays (pinned for speed) or None.
+        wait=False: enqueue the step and return (aob_loop_step_async); the voltages
+        are valid once the stream has reached the step."""
+        fn = "aob_loop_step" if wait else "aob_loop_step_async"
+        call(fn, self.h, addr(host_phase), addr(host_voltage), 1 if noise else 0, stream)
 
     def time(self, noise=True, warmup=3, iters=20) -> float:
         """Device milliseconds of one step (device phase, no host copies)."""

@@ -238,7 +238,7 @@ struct aob_loop {
   ~aob_loop();
   void device_step(bool noise, cudaStream_t s, bool frame_on_device);
   bool launch_fused(bool noise, cudaStream_t s, bool frame_on_device, bool dry);
-  void step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s);
+  void step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s, bool wait = true);
   uint64_t key(bool noise) const;
   void drop_graphs();
 };

@@ -101,7 +101,7 @@ static const void *mapped_view(const void *p) {
   return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
 }
 
-void aob_loop::step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s) {
+void aob_loop::step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s, bool wait) {
   AOB_CUDA(cudaSetDevice(wfs->device));
   // Direct voltages: with the caller's voltage buffer pinned and mapped, the
   // fused kernel's epilogue writes it as well (posted stores over the bus), so
@@ -200,7 +200,7 @@ void aob_loop::step(const float *host_phase, float *host_voltage, bool noise, cu
   if (host_voltage) {
     if (!(io_volt && last_kernels == 1))
       AOB_CUDA(cudaMemcpyAsync(host_voltage, ls->com_clipped.p, ls->com_clipped.bytes(), cudaMemcpyDeviceToHost, s));
-    AOB_CUDA(cudaStreamSynchronize(s));
+    if (wait) AOB_CUDA(cudaStreamSynchronize(s));
   }
 }
 
@@ -270,6 +270,17 @@ int aob_loop_step(aob_loop *l, const float *host_phase, float *host_voltage, int
   try {
     if (!l) throw Error("aob_loop_step: null handle");
     l->step(host_phase, host_voltage, noise != 0, reinterpret_cast<cudaStream_t>(stream));
+    return AOB_OK;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return AOB_ERR;
+  }
+}
+
+int aob_loop_step_async(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream) {
+  try {
+    if (!l) throw Error("aob_loop_step_async: null handle");
+    l->step(host_phase, host_voltage, noise != 0, reinterpret_cast<cudaStream_t>(stream), false);
     return AOB_OK;
   } catch (const std::exception &e) {
     set_last_error(e.what());

@@ -510,6 +510,14 @@ int aob_loop_destroy(aob_loop *l);
  * floats, may be NULL) receives the voltages, and the call then waits for
  * the stream.  noise != 0 adds photon/readout noise. */
 int aob_loop_step(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream);
+/* The same step without the final wait: the phase copy, the kernels and the
+ * voltages' way back to host_voltage are enqueued on the stream and the call
+ * returns.  The voltages are valid once the stream has reached this point (an
+ * event or a synchronisation); host_phase must stay unchanged until then.  With
+ * pinned host buffers nothing in the call blocks the host (pageable buffers make
+ * the copies synchronous).  For callers that step many iterations and read the
+ * results later, as the reference's supervisor loop does between frames. */
+int aob_loop_step_async(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream);
 /* Device time of one step (ms, CUDA events on a private stream; device
  * phase, no host copies): warmup untimed steps, then the mean over iters
  * steps.  Used by the autotuner; the loop state advances. */

@@ -293,6 +293,12 @@ def test_direct_host_io_equals_copies(core, graph, delay):
     assert wa.frame == wb.frame == 6
     assert la.status() == 0 and loopa.kernels_per_step() == 1
     assert np.abs(va.numpy()).max() > 0
+    # the asynchronous step (aob_loop_step_async) gives the same voltages once the stream has reached it
+    loopa.step(ph[0].data_ptr(), va.data_ptr(), noise=True, wait=False)
+    loopb.step(ph[0].data_ptr(), vb.data_ptr(), noise=True)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(va.numpy(), vb.numpy())
+    np.testing.assert_array_equal(np.array(la.buffer("com")), np.array(lb.buffer("com")))
 
 
 def test_sh_launch_shapes_agree(core):
