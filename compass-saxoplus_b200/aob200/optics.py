@@ -100,9 +100,12 @@ class Target:
     def comp_image(self, dev_phase=None, comp_le=True, stream=None):
         call("aob_target_comp_image", self.h, dev_phase, 1 if comp_le else 0, stream)
 
-    def strehl(self, stream=None):
+    def strehl(self, stream=None, fit=False):
+        """(short, long exposure) Strehl: the image peaks, or with ``fit`` the
+        reference's sinc fit of the peak (comp_strehl(do_fit))."""
         se, le = ctypes.c_float(), ctypes.c_float()
-        call("aob_target_strehl", self.h, ctypes.addressof(se), ctypes.addressof(le), stream)
+        call("aob_target_strehl_fit" if fit else "aob_target_strehl", self.h, ctypes.addressof(se),
+             ctypes.addressof(le), stream)
         return se.value, le.value
 
     def reset_le(self, stream=None):

@@ -156,6 +156,37 @@ __global__ void target_abs2_kernel(float *se, float *le, const float2 *amp, int6
   }
 }
 
+// Index of the largest value (the first one on ties, as cuBLAS Isamax used by
+// CarmaObj::aimax): one 64-bit max over (value bits, ~index) -- the images are
+// non-negative, so their float bits order like their values.
+__global__ void argmax_kernel(const float *img, int64_t n, unsigned long long *best) {
+  unsigned long long m = 0ull;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned long long key =
+        ((unsigned long long)__float_as_uint(img[t]) << 32) | (unsigned long long)(0xffffffffu - (uint32_t)t);
+    m = key > m ? key : m;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long v = __shfl_xor_sync(0xffffffffu, m, o);
+    m = v > m ? v : m;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(best, m);
+}
+
+// The (2 h + 1)^2 window of an n x n image centred on pixel c, read as if the
+// image were periodic (extract_krnl with roll, libcarma/src.cu/carma_obj.cu:454-488).
+__global__ void extract_roll_kernel(float *out, const float *img, int n, const unsigned long long *best, int h) {
+  const int w = 2 * h + 1;
+  const int t = threadIdx.x;
+  if (t >= w * w) return;
+  const uint32_t c = 0xffffffffu - (uint32_t)(*best & 0xffffffffull);
+  const int cy = (int)(c / n), cx = (int)(c % n);
+  int y = cy + t / w - h, x = cx + t % w - h;
+  y = (y + n) % n;
+  x = (x + n) % n;
+  out[t] = img[x + (int64_t)y * n];
+}
+
 }  // namespace aob
 
 using namespace aob;
@@ -418,6 +449,58 @@ void aob_target::strehl(float *sr_se, float *sr_le, cudaStream_t s) {
   float fse, fle;
   std::memcpy(&fse, &m[0], 4);
   std::memcpy(&fle, &m[1], 4);
+  if (sr_se) *sr_se = fse;
+  if (sr_le) *sr_le = le_count > 0 ? fle / (float)le_count : fse;
+}
+
+// SutraSource::fitmax2x1dSinc (libsutra/src.cpp/sutra_source.cpp:451-488): a
+// parabola through the 3-pixel cross around the maximum gives its sub-pixel
+// position (x0, y0); the peak there is the Shannon (sinc) interpolation of the
+// 7 x 7 window, which the well-sampled image allows.  The window is read on the
+// device, the fit on the host, as in the reference.
+static float sinc_of(double x) {
+  if (x == 0) return 1;
+  x *= M_PI;
+  return (float)(std::sin(x) / x);
+}
+
+float aob_target::fit_peak(const float *img, cudaStream_t s) {
+  constexpr int H = 3, W = 2 * H + 1;
+  const int64_t n2 = (int64_t)nfft * nfft;
+  AOB_CUDA(cudaMemsetAsync(fit_best.p, 0, sizeof(unsigned long long), s));
+  argmax_kernel<<<(int)std::min<int64_t>((n2 + 255) / 256, 2 * 148), 256, 0, s>>>(img, n2, fit_best.p);
+  AOB_LAUNCH_CHECK("argmax_kernel");
+  extract_roll_kernel<<<1, 64, 0, s>>>(fit_win.p, img, nfft, fit_best.p, H);
+  AOB_LAUNCH_CHECK("extract_roll_kernel");
+  float w[W * W];
+  AOB_CUDA(cudaMemcpyAsync(w, fit_win.p, sizeof(w), cudaMemcpyDeviceToHost, s));
+  AOB_CUDA(cudaStreamSynchronize(s));
+  const int center = (W * W - 1) / 2;
+  const float A = 0.5 * (w[center - W] + w[center + W]) - w[center];
+  const float B = 0.5 * (w[center - 1] + w[center + 1]) - w[center];
+  if (A * B == 0) return 0.f;  // (the reference reports it cannot estimate the Strehl)
+  const float x0 = -0.5 * (w[center + W] - w[center - W]) / 2. / A;
+  const float y0 = -0.5 * (w[center + 1] - w[center - 1]) / 2. / B;
+  float val = 0.f;
+  int ind = 0;
+  for (int i = -H; i < H + 1; ++i) {
+    const float ti = sinc_of(x0 - i);
+    for (int j = -H; j < H + 1; ++j) {
+      const float tj = sinc_of(y0 - j);
+      val += ti * tj * w[ind++];
+    }
+  }
+  return val;
+}
+
+void aob_target::strehl_fit(float *sr_se, float *sr_le, cudaStream_t s) {
+  AOB_CUDA(cudaSetDevice(device));
+  if (!fit_best.p) {
+    fit_best.alloc(1);
+    fit_win.alloc(64);
+  }
+  const float fse = fit_peak(se.p, s);
+  const float fle = fit_peak(le.p, s);
   if (sr_se) *sr_se = fse;
   if (sr_le) *sr_le = le_count > 0 ? fle / (float)le_count : fse;
 }

@@ -69,8 +69,12 @@ struct aob_target {
   aob::DevBuf<float> mask, phase, se, le;
   aob::DevBuf<float2> amp;
   aob::DevBuf<unsigned int> maxes;
+  aob::DevBuf<unsigned long long> fit_best;  // argmax key of the sinc fit
+  aob::DevBuf<float> fit_win;                // its 7 x 7 window
   aob_target(int device, int npup, int nfft, const float *pupil, float lambda_um);
   void comp_image(const float *dev_phase, bool comp_le, cudaStream_t s);
   void strehl(float *sr_se, float *sr_le, cudaStream_t s);
   void reset_le(cudaStream_t s);
+  float fit_peak(const float *img, cudaStream_t s);
+  void strehl_fit(float *sr_se, float *sr_le, cudaStream_t s);
 };

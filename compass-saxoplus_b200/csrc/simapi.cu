@@ -152,6 +152,11 @@ int aob_target_strehl(aob_target *t, float *se, float *le, void *stream) {
   t->strehl(se, le, S(stream));
   API_END
 }
+int aob_target_strehl_fit(aob_target *t, float *se, float *le, void *stream) {
+  API_TRY NEED(t);
+  t->strehl_fit(se, le, S(stream));
+  API_END
+}
 int aob_target_reset_le(aob_target *t, void *stream) {
   API_TRY NEED(t);
   t->reset_le(S(stream));

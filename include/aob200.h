@@ -482,15 +482,22 @@ int aob_raytrace(float *dev_out, int nx, int ny, int nsrc, const float *const *d
                  const float *xoff, const float *yoff, int reset, void *stream);
 
 /* ---- science target -------------------------------------------------------- *
- * SutraSource::comp_image / comp_strehl (sutra_source.cpp:397-515) without the
- * sinc fit: short- and long-exposure PSF normalised so that the peak is the
- * Strehl ratio. */
+ * SutraSource::comp_image / comp_strehl (sutra_source.cpp:397-515): short- and
+ * long-exposure PSF normalised so that the peak is the Strehl ratio; the peak
+ * read directly (aob_target_strehl) or by the reference's sinc fit
+ * (aob_target_strehl_fit). */
 typedef struct aob_target aob_target;
 int aob_target_create(aob_target **out, int device, int npup, int nfft, const float *pupil, float lambda_um);
 int aob_target_destroy(aob_target *t);
 /* dev_phase: npup x npup phase in micron (NULL = the target's own buffer). */
 int aob_target_comp_image(aob_target *t, const float *dev_phase, int comp_le, void *stream);
 int aob_target_strehl(aob_target *t, float *se, float *le, void *stream);
+/* comp_strehl(do_fit = true) (sutra_source.cpp:491-515, fitmax2x1dSinc
+ * :451-488): the peak of each image estimated by a sinc (Shannon) interpolation
+ * at the sub-pixel maximum that parabolas through the 3-pixel cross around the
+ * brightest pixel give, over its 7 x 7 periodic window; the long exposure is
+ * divided by the number of images summed.  Waits for the stream. */
+int aob_target_strehl_fit(aob_target *t, float *se, float *le, void *stream);
 int aob_target_reset_le(aob_target *t, void *stream);
 /* which: "phase", "image_se", "image_le", "amplipup". */
 int aob_target_buffer(aob_target *t, const char *which, void **dev_ptr, int64_t *nelem);

@@ -87,3 +87,35 @@ def psf(phase, pupil, lam_um, nfft):
     amp[:npup, :npup][m] = np.exp(1j * 2 * np.pi / lam_um * phase[m])
     img = np.abs(np.fft.fft2(amp)) ** 2
     return img / float(m.sum()) ** 2
+
+
+def strehl_sinc_fit(img, half=3):
+    """Peak of a well-sampled PSF by sinc interpolation at its sub-pixel maximum
+    (SutraSource::fitmax2x1dSinc, libsutra/src.cpp/sutra_source.cpp:451-488):
+    parabolas through the 3-pixel cross around the brightest pixel (first one on
+    ties) give the offset (x0, y0); the (2 half + 1)^2 window, read
+    periodically (extract_krnl with roll, libcarma/src.cu/carma_obj.cu:454-488),
+    is summed with weights sinc(x0 - i) sinc(y0 - j).  ``img`` is [x, y]."""
+    n = img.shape[0]
+    flat = np.asarray(img, np.float64).ravel(order="F")
+    c = int(np.argmax(flat))
+    cx, cy = c % n, c // n
+    w = 2 * half + 1
+    win = np.empty(w * w)
+    for t in range(w * w):
+        y = (cy + t // w - half) % n
+        x = (cx + t % w - half) % n
+        win[t] = flat[x + y * n]
+    ctr = (w * w - 1) // 2
+    A = 0.5 * (win[ctr - w] + win[ctr + w]) - win[ctr]
+    B = 0.5 * (win[ctr - 1] + win[ctr + 1]) - win[ctr]
+    if A * B == 0:
+        return 0.0
+    x0 = -0.5 * (win[ctr + w] - win[ctr - w]) / 2.0 / A
+    y0 = -0.5 * (win[ctr + 1] - win[ctr - 1]) / 2.0 / B
+    val, ind = 0.0, 0
+    for i in range(-half, half + 1):
+        for j in range(-half, half + 1):
+            val += np.sinc(x0 - i) * np.sinc(y0 - j) * win[ind]
+            ind += 1
+    return float(val)

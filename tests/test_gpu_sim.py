@@ -146,3 +146,32 @@ def test_target_psf_and_strehl(lib):
     t.comp_image()
     se, le = t.strehl()
     assert abs(se - 1.0) < 1e-5 and abs(le - 1.0) < 1e-5
+    sf, lf = t.strehl(fit=True)
+    assert abs(sf - 1.0) < 1e-4 and abs(lf - 1.0) < 1e-4
+
+
+def test_target_strehl_sinc_fit_matches_oracle(lib):
+    """comp_strehl(do_fit): the sinc fit of a tilted (off-pixel) PSF peak, short and
+    long exposure, against the oracle's restatement."""
+    from aob200 import geometry as G
+    from aob200 import optics
+
+    tel = G.telescope_geometry(120, 8.0, 0.14)
+    pup = tel.spupil
+    t = optics.Target(pup, 1.65, 256)
+    rng = np.random.default_rng(6)
+    x = np.arange(pup.shape[0])
+    imgs = []
+    for k in range(3):
+        tilt = 1.65 * (0.37 + 0.1 * k) / pup.shape[0] * 2.13  # a fraction of a pixel in the focal plane
+        ph = (tilt * x[:, None] + 0.03 * rng.standard_normal(pup.shape)).astype(np.float32)
+        t.d_phase.set(ph)
+        t.comp_image()
+        imgs.append(np.array(t.d_image_se).astype(np.float64))
+    sf, lf = t.strehl(fit=True)
+    ref_se = OT.strehl_sinc_fit(imgs[-1])
+    ref_le = OT.strehl_sinc_fit(sum(imgs)) / len(imgs)
+    assert abs(sf - ref_se) < 1e-5 * max(ref_se, 1e-3) + 1e-6
+    assert abs(lf - ref_le) < 1e-4 * ref_le
+    se, le = t.strehl()
+    assert sf >= se - 1e-6  # the fitted peak is at least the brightest pixel
