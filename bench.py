@@ -25,7 +25,9 @@ metric, roofline and CPU baseline: ``mc64`` (64 uneven SH loops advanced by
 one persistent launch per step, BF16 MVM), ``pyr50`` (pyramid sensor, 24
 modulation points over 512 x 512 FFTs, slopes and a 1600-actuator LS MVM),
 ``mlp`` (the learned reconstructor: batch-1 inference against the LS MVM and
-training throughput on the tensor cores).
+training throughput on the tensor cores), ``precision`` (the saxo40 closed
+loop with its own LS command matrix: command error and residual-wavefront rms
+of the F32 / BF16 / FP8 MVM against a float64 reconstruction).
 
 --impl reference runs the reference's own implementation of the path, its
 sutra CUDA code built from its sources into oracle/_ref (oracle/build_ref.py),
@@ -301,7 +303,7 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
-# secondary workloads (--workload mc64 | pyr50 | mlp): one JSON line each
+# secondary workloads (--workload mc64 | pyr50 | mlp | precision): one JSON line each
 def _line(args, workload, metric, value, unit, ms_per_step, dtype, config, **extra):
     d = {"workload": workload, "metric": metric, "value": value, "unit": unit, "n_gpus": 1,
          "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -397,11 +399,14 @@ def run_pyr50(args, torch):
     FFTs, photon + 0.3 e- noise, slopes and a 1600-actuator LS MVM."""
     from aob200 import core as C
     from aob200 import geometry as G
+    from aob200 import workloads as W
 
     g = G.pyr_geometry(G.PyrParams(nxsub=50, wavelength_um=1.075, ampl=3.0, npts=24, pup_sep=32, fssize=3.2), 100,
                        diam=8.0, cobs=0.14)
     w = C.PyrWfs.from_geometry(g, noise=0.3, seed=3)
-    phase = (np.random.default_rng(0).standard_normal((g.tel.n, g.tel.n)) * 0.02).astype(np.float32)
+    # the second stage sees the residual of the seeded saxo40 closed loop
+    res, pd_in = W.saxo40_residual(niter=200)
+    phase = W.resample_pupil(res, pd_in, g.tel.n, g.tel.pupdiam)
     w.set_phase(phase)
     c = C.Centroider(g.nvalid, 0.0, 1.0, "pyr")
     c.load_validpos(g.validsubsx, g.validsubsy)
@@ -425,19 +430,21 @@ def run_pyr50(args, torch):
     if not args.no_cpu_baseline:
         from oracle import pyr as opyr
 
+        ncores = len(os.sched_getaffinity(0))
         t1 = time.perf_counter()
         k = 0
         while k < 3:
-            opyr.comp_image(phase, g.tel.mpupil, g, g.wavelength_um, g.nphotons, noise=0.3, frame=k)
+            opyr.comp_image(phase, g.tel.mpupil, g, g.wavelength_um, g.nphotons, noise=0.3, frame=k, workers=ncores)
             k += 1
         dt = time.perf_counter() - t1
-        cpu = {"value": k / dt, "unit": "iters/s", "cores": 1, "kind": "port",
-               "sample": f"{k} pyramid images (float64 NumPy FFT, single thread)"}
+        cpu = {"value": k / dt, "unit": "iters/s", "cores": ncores, "kind": "port",
+               "sample": f"{k} pyramid images (float64 scipy.fft, modulation points batched over {ncores} threads)"}
     _line(args, "pyr50", "pyramid loop iters/s (image + slopes + 1600-actuator LS MVM)", 1.0 / t_step, "iters/s",
           t_step * 1e3, "f32",
           {"workload": f"pyr50: {g.nxsub}x{g.nxsub} pupil samples per image, {npts} modulation points at 3 lambda/D, "
                        f"{nfft}x{nfft} FFTs, {g.nvalid} valid, 1600-actuator LS MVM",
-           "l2": "flushed before every timed step (256 MB write)"},
+           "l2": "flushed before every timed step (256 MB write)",
+           "input": "residual phase of the seeded saxo40 closed loop after 200 iterations, resampled to the pupil"},
           # no measured FP32 (non-tensor) peak: nominal 148 SMs x 128 FP32 lanes x 2 FLOP x 1.965 GHz
           roofline={"bound": "fp32 FFT", "achieved": flops / t_img / 1e12, "unit": "TFLOP/s", "peak": FP32_NOMINAL_TFLOPS,
                     "frac": flops / t_img / 1e12 / FP32_NOMINAL_TFLOPS, "peak_source": "nominal (not measured)",
@@ -488,15 +495,21 @@ def run_mlp(args, torch):
     if not args.no_cpu_baseline:
         from oracle import mlp as om
 
+        from threadpoolctl import threadpool_info, threadpool_limits
+
+        ncores = len(os.sched_getaffinity(0))
         P = net.get_params()
         x = rng.standard_normal((1, nin)).astype(np.float32)
-        t1 = time.perf_counter()
-        k = 0
-        while k < 20:
-            om.forward(P, x, net.in_scale)
-            k += 1
-        cpu = {"value": k / (time.perf_counter() - t1), "unit": "inferences/s", "cores": 1, "kind": "port",
-               "sample": f"{k} batch-1 forward passes (NumPy, bfloat16-rounded weights)"}
+        with threadpool_limits(limits=ncores, user_api="blas"):
+            blas = max([d.get("num_threads", 1) for d in threadpool_info() if d.get("user_api") == "blas"] or [1])
+            t1 = time.perf_counter()
+            k = 0
+            while k < 20:
+                om.forward(P, x, net.in_scale)
+                k += 1
+            dt = time.perf_counter() - t1
+        cpu = {"value": k / dt, "unit": "inferences/s", "cores": blas, "kind": "port",
+               "sample": f"{k} batch-1 forward passes (NumPy, bfloat16-rounded weights, BLAS on {blas} threads)"}
     _line(args, "mlp", "learned reconstructor batch-1 inferences/s (LS MVM alongside)", 1e6 / res["mlp_infer_us"],
           "inferences/s", res["mlp_infer_us"] / 1e3, "bf16",
           {"workload": f"mlp: {nin} -> 1024 -> 1024 -> {nout} + linear skip, BF16 weights, FP32 accumulation",
@@ -507,11 +520,31 @@ def run_mlp(args, torch):
           cpu_baseline=cpu, clocks=clk.summary(), gpu_launches=None)
 
 
+def run_precision(args, torch):
+    """saxo40 with its own LS command matrix (push-pull imat, float64 inverse):
+    the command error of one MVM and the closed-loop residual-wavefront rms and
+    LE Strehl of each MVM precision against a float64 host reconstruction of
+    the same seeded loop (aob200.precision.study)."""
+    from aob200 import precision as P
+
+    t0 = time.perf_counter()
+    res = P.study(niter=args.loop_iters, nskip=args.loop_iters // 10, sample_every=max(args.loop_iters // 100, 1))
+    print(json.dumps({"workload": "precision", "metric": "relative residual-wavefront rms change vs float64 "
+                      "reconstruction (closed loop), and relative command error of one MVM",
+                      "unit": "relative", "dtype": "f32/bf16/fp8 MVM, f32 sensor", "data": "synthetic",
+                      "config": {"workload": "saxo40 closed loop: 3-layer von Karman (r0 0.14 m), photon + 0.5 e- "
+                                 "noise at magnitude 8, wCoG + threshold, gain 0.4, LE Strehl at 1.65 um",
+                                 "iterations": args.loop_iters}, "seconds": round(time.perf_counter() - t0, 1),
+                      **res}))
+    return 0
+
+
 def run_secondary(args):
     import torch
 
     torch.cuda.set_device(0)
-    return {"mc64": run_mc64, "pyr50": run_pyr50, "mlp": run_mlp}[args.workload](args, torch) or 0
+    fn = {"mc64": run_mc64, "pyr50": run_pyr50, "mlp": run_mlp, "precision": run_precision}[args.workload]
+    return fn(args, torch) or 0
 
 
 def main():
@@ -523,7 +556,8 @@ def main():
     ap.add_argument("--precision", default="f32", choices=["f32", "bf16", "fp8"])
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="saxo40", choices=["saxo40", "mc64", "pyr50", "mlp"])
+    ap.add_argument("--workload", default="saxo40", choices=["saxo40", "mc64", "pyr50", "mlp", "precision"])
+    ap.add_argument("--loop-iters", type=int, default=5000, help="precision: closed-loop iterations per run")
     ap.add_argument("--instances", type=int, default=64, help="mc64: number of instances (the first N of the list)")
     ap.add_argument("--no-tune", action="store_true", help="mc64: fixed tile shapes instead of the autotuner")
     args = ap.parse_args()

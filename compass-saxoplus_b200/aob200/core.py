@@ -62,6 +62,25 @@ class DeviceArray:
     def get_dims(self):
         return self.shape
 
+
+class OwnedDeviceArray(DeviceArray):
+    """A device buffer allocated here (aob_malloc) and freed with the object."""
+
+    def __init__(self, n: int, dtype=np.float32, shape=None, device=0):
+        p = ctypes.c_void_p()
+        nbytes = max(int(n), 1) * np.dtype(dtype).itemsize
+        call("aob_malloc", ctypes.addressof(p), nbytes, int(device))
+        super().__init__(p.value, n, dtype, shape)
+        call("aob_memcpy_h2d", self.ptr, np.zeros(nbytes, np.uint8).ctypes.data, nbytes, None)
+
+    def __del__(self):
+        try:
+            if self.ptr and _lib._lib is not None:
+                _lib.lib().aob_free(ctypes.c_void_p(self.ptr))
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
+        self.ptr = 0
+
     def __len__(self):
         return self.shape[0]
 
@@ -97,7 +116,7 @@ class ShWfs:
         w = cls(g.nxsub, g.nvalid, g.npix, g.pdiam, g.nrebin, g.nfft, g.ntot, g.tel.n, g.subapd,
                 g.nphotons, device=device, lambda_um=g.wavelength_um)
         w.load_arrays(g.phasemap, g.hrmap, g.binmap, g.halfxy, g.fluxPerSub, g.validsubsx, g.validsubsy,
-                      g.validpuppixx, g.validpuppixy)
+                      g.validpuppixx, g.validpuppixy, g.ttprojmat)
         w.set_pupil(g.tel.mpupil)
         w.set_noise(noise, seed)
         if getattr(g, "submask", None) is not None:
@@ -121,8 +140,18 @@ class ShWfs:
                 host_array(jstart, i32)]
         # hrmap is read when the field of view is extended (ntot != nfft)
         hr = host_array(hrmap, i32) if (hrmap is not None and self.ntot != self.nfft) else None
-        call("aob_sh_load_arrays", self.h, None, None if hr is None else hr.ctypes.data,
-             *[k.ctypes.data for k in keep], None, None)
+        # phasemap and ttprojmat are kept for the geometric slopes (slopes_geom)
+        pm = host_array(phasemap, i32) if phasemap is not None else None
+        tt = host_array(ttprojmat, f32) if ttprojmat is not None else None
+        call("aob_sh_load_arrays", self.h, None if pm is None else pm.ctypes.data,
+             None if hr is None else hr.ctypes.data, *[k.ctypes.data for k in keep],
+             None if tt is None else tt.ctypes.data, None)
+
+    def slopes_geom(self, type=0, dev_slopes=None, stream=None):
+        """Geometric slopes of the phase (SutraWfs::slopes_geom): 0 edge
+        differences, 1 pupil-weighted finite differences, 2 tip/tilt projection
+        (needs ttprojmat).  Into ``dev_slopes`` or the sensor's "slopes" buffer."""
+        call("aob_sh_slopes_geom", self.h, int(type), dev_slopes, stream)
 
     def set_pupil(self, pupil):
         a = host_array(pupil, np.float32)
@@ -167,6 +196,15 @@ class ShWfs:
     def set_nphot(self, nphot):
         self.nphot = float(nphot)
         call("aob_sh_set_nphot", self.h, float(nphot))
+
+    def set_bincube(self, cube):
+        """Overwrite the sub-aperture images (npix x npix x nvalid, Fortran order)."""
+        a = host_array(cube, np.float32)
+        call("aob_sh_set_bincube", self.h, a.ctypes.data, int(a.size))
+
+    def set_binimg(self, img):
+        a = host_array(img, np.float32)
+        call("aob_sh_set_binimg", self.h, a.ctypes.data, int(a.size))
 
     @property
     def frame(self) -> int:
@@ -231,7 +269,8 @@ class PyrWfs:
 
     @classmethod
     def from_geometry(cls, g, device=0, noise=-1.0, seed=1234, weights=None):
-        w = cls(g.nxsub, g.nvalid, g.npix, g.pdiam, g.nrebin, g.nfft, g.ntot, g.pyr_cx.size, g.pdiam,
+        subapd = g.tel.diam / g.nxsub if g.tel is not None else float(g.pdiam)
+        w = cls(g.nxsub, g.nvalid, g.npix, g.pdiam, g.nrebin, g.nfft, g.ntot, g.pyr_cx.size, subapd,
                 g.nphotons, device=device, lambda_um=g.wavelength_um)
         w.load_arrays(g.halfxy, g.pyr_cx, g.pyr_cy, weights, g.sincar, g.submask, g.validsubsx, g.validsubsy,
                       g.phasemap, g.fluxPerSub)
@@ -259,8 +298,31 @@ class PyrWfs:
         keep = [hx, host_array(cx, f32), host_array(cy, f32), host_array(w, f32), host_array(sincar, f32),
                 host_array(submask, f32), host_array(validsubsx, np.int32), host_array(validsubsy, np.int32)]
         flux = host_array(fluxPerSub, f32) if fluxPerSub is not None else None
-        call("aob_pyr_load_arrays", self.h, *[k.ctypes.data for k in keep], None,
-             flux.ctypes.data if flux is not None else None, None)
+        pm = host_array(phasemap, np.int32) if phasemap is not None else None
+        tt = host_array(ttprojmat, f32) if ttprojmat is not None else None
+        call("aob_pyr_load_arrays", self.h, *[k.ctypes.data for k in keep], None if pm is None else pm.ctypes.data,
+             flux.ctypes.data if flux is not None else None, None if tt is None else tt.ctypes.data)
+
+    def set_submask(self, submask):
+        a = host_array(submask, np.float32)
+        call("aob_pyr_set_submask", self.h, a.ctypes.data, int(a.size))
+
+    def set_phalfxy(self, phalfxy):
+        """The pyramid mask exp(i phase) as nfft x nfft complex64 (already in the
+        sensor's layout, as the reference's set_phalfxy takes it)."""
+        a = np.ascontiguousarray(np.asarray(phalfxy, np.complex64).ravel(order="F"))
+        call("aob_pyr_set_phalfxy", self.h, a.view(np.float32).ctypes.data, int(a.size))
+
+    def set_binimg(self, img):
+        a = host_array(img, np.float32)
+        call("aob_pyr_set_binimg", self.h, a.ctypes.data, int(a.size))
+
+    def set_compute_focalplane(self, on=True):
+        call("aob_pyr_set_compute_focalplane", self.h, 1 if on else 0)
+
+    def slopes_geom(self, type=0, dev_slopes=None, stream=None):
+        """Geometric slopes of the phase (SutraWfs::slopes_geom), see ShWfs.slopes_geom."""
+        call("aob_pyr_slopes_geom", self.h, int(type), dev_slopes, stream)
 
     def set_modulation(self, cx, cy, weights=None):
         f32 = np.float32

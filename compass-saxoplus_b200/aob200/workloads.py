@@ -104,6 +104,43 @@ def build_sh_loop(setup: ShLoopSetup, precision="f32", device=0, graph=True, see
 
 
 # ---------------------------------------------------------------------------
+# Second-stage input: the residual of the saxo40 closed loop
+def saxo40_residual(niter=200, device=0):
+    """Residual phase (micron) on the target's pupil grid after ``niter``
+    seeded iterations of the saxo40 closed loop (3-layer von Karman turbulence,
+    photon + readout noise, its own push-pull LS command matrix)."""
+    from . import system as S
+
+    sy = S.ShAoSystem(S.saxo40(), device)
+    sy.calibrate()
+    sy.close(graph=False)
+    for _ in range(niter):
+        sy.next(compute_psf=False, noise=True)
+    sy.trace_target()
+    ph = np.array(sy.target.d_phase, dtype=np.float64)
+    pup = sy.geom.tel.spupil > 0
+    ph = np.where(pup, ph - ph[pup].mean(), 0.0)
+    return ph.astype(np.float32), float(sy.geom.tel.pupdiam)
+
+
+def resample_pupil(phase, pupdiam_in, n_out, pupdiam_out):
+    """Bilinear resampling of a phase given on a pupil grid of ``pupdiam_in``
+    pixels across (the pupil filling the array, centred) onto an ``n_out`` x
+    ``n_out`` grid whose centred pupil is ``pupdiam_out`` pixels across."""
+    n_in = phase.shape[0]
+    off_in = (n_in - pupdiam_in) / 2.0
+    off_out = (n_out - pupdiam_out) / 2.0
+    r = pupdiam_in / pupdiam_out
+    u = np.clip((np.arange(n_out) - off_out + 0.5) * r - 0.5 + off_in, 0.0, n_in - 1.0)
+    i0 = np.minimum(np.floor(u).astype(np.int64), n_in - 2)
+    t = u - i0
+    p = phase.astype(np.float64)
+    rows = p[i0] * (1 - t)[:, None] + p[i0 + 1] * t[:, None]
+    out = rows[:, i0] * (1 - t)[None, :] + rows[:, i0 + 1] * t[None, :]
+    return out.astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
 # Batched Monte Carlo: independent SH instances of uneven size
 @dataclass
 class McInstance:

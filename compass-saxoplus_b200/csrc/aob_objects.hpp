@@ -46,6 +46,10 @@ struct aob_sh {
   aob::DevBuf<float> fs_mask;  // fs_n x fs_n focal-plane mask (fftshifted)
   aob::DevBuf<float> fs_field; // fs_n x fs_n complex filtered field (float pairs)
   aob::DevBuf<float> offsets, fluxPerSub;
+  // geometric slopes (slopes_geom): phase-sample indexes per sub-aperture and
+  // the tip/tilt projection matrix, both in the reference's column-major layout
+  aob::DevBuf<int32_t> phasemap;  // nphase^2 x nvalid
+  aob::DevBuf<float> ttprojmat;   // nphase^2 x 2 nvalid
   // pruned-DFT tables derived from binmap at load time
   int nu = 0, nv = 0;
   aob::DevBuf<int32_t> ulist, vlist, cbin;
@@ -103,6 +107,12 @@ struct aob_pyr {
   aob::DevBuf<float> binimg, partial;              // (nfft/nrebin)^2 image, per-row sums
   aob::DevBuf<int32_t> validsubsx, validsubsy;     // 4 * nvalid pupil-image pixels
   aob::DevBuf<float> fluxPerSub;
+  aob::DevBuf<int32_t> phasemap;                   // slopes_geom: nphase^2 x nvalid
+  aob::DevBuf<float> ttprojmat;                    // slopes_geom: nphase^2 x 2 nvalid
+  aob::DevBuf<float> slopes;                       // 2 nvalid geometric slopes
+  bool compute_focalplane = false;                 // accumulate the focal plane image
+  aob::DevBuf<float> focalplane;                   // nfft x nfft sum_p w_p |field stop x focal field|^2
+  aob::DevBuf<float> focal_work;                   // npts x nfft x nfft, summed in point order
 
   aob_pyr(int device, int nxsub, int nvalid, int npix, int nphase, int nrebin, int nfft, int ntot, int npts,
           float pdiam, float nphot, float nphot4imat);

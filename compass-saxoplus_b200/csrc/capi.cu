@@ -145,12 +145,31 @@ int aob_sh_destroy(aob_sh *h) {
   }
   AOB_API_END
 }
-int aob_sh_load_arrays(aob_sh *h, const int32_t *, const int32_t *hrmap, const int32_t *binmap, const float *offsets,
-                       const float *flux, const int32_t *vx, const int32_t *vy, const int32_t *istart,
-                       const int32_t *jstart, const float *, const float *) {
+// phasemap / ttprojmat (optional): kept for slopes_geom; every phasemap entry
+// must index the phase screen
+static void load_geom_arrays(int device, aob::DevBuf<int32_t> &pm, aob::DevBuf<float> &tt, const int32_t *phasemap,
+                             const float *ttprojmat, int nphase, int nvalid, int64_t nscreen) {
+  const int64_t m = (int64_t)nphase * nphase * nvalid;
+  AOB_CUDA(cudaSetDevice(device));
+  if (phasemap) {
+    for (int64_t i = 0; i < m; ++i)
+      if (phasemap[i] < 0 || phasemap[i] >= nscreen) throw Error("load_arrays: phasemap entry outside the phase screen");
+    if (pm.n != m) pm.alloc(m);
+    pm.upload(phasemap, m);
+  }
+  if (ttprojmat) {
+    if (tt.n != 2 * m) tt.alloc(2 * m);
+    tt.upload(ttprojmat, 2 * m);
+  }
+}
+
+int aob_sh_load_arrays(aob_sh *h, const int32_t *phasemap, const int32_t *hrmap, const int32_t *binmap,
+                       const float *offsets, const float *flux, const int32_t *vx, const int32_t *vy,
+                       const int32_t *istart, const int32_t *jstart, const float *ttprojmat, const float *) {
   AOB_API_BEGIN
   NEED(h);
   h->load_arrays(binmap, offsets, flux, vx, vy, istart, jstart, hrmap);
+  load_geom_arrays(h->device, h->phasemap, h->ttprojmat, phasemap, ttprojmat, h->nphase, h->nvalid, h->phase.n);
   AOB_API_END
 }
 int aob_sh_set_fakecam(aob_sh *h, int enable, int max_flux_per_pix, int max_pix_value) {
@@ -236,7 +255,8 @@ int aob_sh_buffer(aob_sh *h, const char *which, void **p, int64_t *n) {
   B("phase", phase) B("pupil", pupil) B("bincube", bincube) B("binimg", binimg) B("intensities", intensities)
   B("validsubsx", validsubsx) B("validsubsy", validsubsy) B("fluxPerSub", fluxPerSub) B("binmap", binmap)
   B("offsets", offsets) B("istart", istart) B("jstart", jstart) B("slopes", slopes) B("camimg", camimg)
-  B("dark", cam_dark) B("flat", cam_flat) B("hrmap", hrmap) B("submask", fs_mask)
+  B("dark", cam_dark) B("flat", cam_flat) B("hrmap", hrmap) B("submask", fs_mask) B("phasemap", phasemap)
+  B("ttprojmat", ttprojmat)
 #undef B
   throw Error("sh.buffer: unknown buffer '" + w + "'");
   AOB_API_END
@@ -828,11 +848,41 @@ int aob_pyr_load_arrays(aob_pyr *h, const float *halfxy_c64, const float *cx, co
                         const float *ttprojmat) {
   AOB_API_BEGIN
   NEED(h);
-  (void)phasemap;
-  (void)ttprojmat;
   AOB_CUDA(cudaSetDevice(h->device));
   h->load_arrays(reinterpret_cast<const float2 *>(halfxy_c64), cx, cy, weights, sincar, submask, validsubsx,
                  validsubsy, fluxPerSub);
+  load_geom_arrays(h->device, h->phasemap, h->ttprojmat, phasemap, ttprojmat, h->nphase, h->nvalid, h->phase.n);
+  AOB_API_END
+}
+int aob_pyr_set_submask(aob_pyr *h, const float *submask, int64_t n) {
+  AOB_API_BEGIN
+  NEED(h); NEED(submask);
+  if (n != h->submask.n) throw Error("pyr.set_submask: wrong dimensions (nfft x nfft)");
+  AOB_CUDA(cudaSetDevice(h->device));
+  h->submask.upload(submask, n);
+  AOB_API_END
+}
+int aob_pyr_set_phalfxy(aob_pyr *h, const float *phalfxy_c64, int64_t n) {
+  AOB_API_BEGIN
+  NEED(h); NEED(phalfxy_c64);
+  if (n != h->phalfxy.n) throw Error("pyr.set_phalfxy: wrong dimensions (nfft x nfft complex)");
+  AOB_CUDA(cudaSetDevice(h->device));
+  h->phalfxy.upload(reinterpret_cast<const float2 *>(phalfxy_c64), n);
+  AOB_API_END
+}
+int aob_pyr_set_binimg(aob_pyr *h, const float *img, int64_t n) {
+  AOB_API_BEGIN
+  NEED(h); NEED(img);
+  if (n != h->binimg.n) throw Error("pyr.set_binimg: wrong dimensions");
+  AOB_CUDA(cudaSetDevice(h->device));
+  h->binimg.upload(img, n);
+  ++h->image_gen;
+  AOB_API_END
+}
+int aob_pyr_set_compute_focalplane(aob_pyr *h, int enable) {
+  AOB_API_BEGIN
+  NEED(h);
+  h->compute_focalplane = enable != 0;
   AOB_API_END
 }
 int aob_pyr_set_modulation(aob_pyr *h, const float *cx, const float *cy, const float *weights, int npts) {
@@ -894,6 +944,26 @@ int aob_pyr_buffer(aob_pyr *h, const char *which, void **dev_ptr, int64_t *nelem
   else if (w == "validsubsx") { p = h->validsubsx.p; n = h->validsubsx.n; }
   else if (w == "validsubsy") { p = h->validsubsy.p; n = h->validsubsy.n; }
   else if (w == "fluxPerSub") { p = h->fluxPerSub.p; n = h->fluxPerSub.n; }
+  else if (w == "submask") { p = h->submask.p; n = h->submask.n; }
+  else if (w == "phalfxy") { p = h->phalfxy.p; n = 2 * h->phalfxy.n; }
+  else if (w == "sincar") { p = h->sincar.p; n = h->sincar.n; }
+  else if (w == "phasemap") { p = h->phasemap.p; n = h->phasemap.n; }
+  else if (w == "ttprojmat") { p = h->ttprojmat.p; n = h->ttprojmat.n; }
+  else if (w == "slopes") {
+    if (h->slopes.n != 2LL * h->nvalid) {
+      AOB_CUDA(cudaSetDevice(h->device));
+      h->slopes.alloc(2LL * h->nvalid);
+    }
+    p = h->slopes.p; n = h->slopes.n;
+  }
+  else if (w == "pyrfocalplane") {
+    if (h->focalplane.n != (int64_t)h->nfft * h->nfft) {
+      AOB_CUDA(cudaSetDevice(h->device));
+      h->focalplane.alloc((int64_t)h->nfft * h->nfft);
+      AOB_CUDA(cudaMemset(h->focalplane.p, 0, sizeof(float) * h->focalplane.n));
+    }
+    p = h->focalplane.p; n = h->focalplane.n;
+  }
   else throw Error("pyr.buffer: unknown buffer '" + w + "'");
   *dev_ptr = p;
   if (nelem) *nelem = n;

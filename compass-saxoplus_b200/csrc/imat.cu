@@ -127,6 +127,9 @@ extern "C" int aob_imat_build(aob_sh *w, aob_centro *c, aob_dm *dm, float xoff, 
     ShKernelArgs P;
     aob_centro *fc = w->make_args(false, nullptr, nullptr, P);
     AOB_REQUIRE(fc == c, "aob_imat_build: attach the CoG-family centroider to the sensor first");
+    // the reference forms the calibration images with nphot4imat photons
+    // (SutraRtc::comp_images_imat, sutra_rtc.cpp:380-395); 0 keeps nphot
+    if (w->nphot4imat > 0.f) P.nphot = w->nphot4imat;
     const int nact = dm->nact, nslope = 2 * w->nvalid;
     const int per = chunk > 0 ? std::min(chunk, nact) : nact;
     AOB_REQUIRE(2 * (int64_t)per <= 65535, "aob_imat_build: at most 32767 actuators per chunk");

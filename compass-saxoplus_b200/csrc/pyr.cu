@@ -57,6 +57,7 @@ struct PyrArgs {
   float *hrimg;      // N x N
   float *binimg;     // nb x nb
   float *partial;    // nb row sums
+  float *focal_work; // npts x N x N, w_p |field stop x focal field|^2 (null: not computed)
   int nrebin, nb, rows_per_bin_cta;
 };
 
@@ -130,7 +131,10 @@ __global__ void __launch_bounds__(PYR_THREADS) pyr_cols_kernel(PyrArgs A) {
     const size_t g = (size_t)(c0 + c) + (size_t)m * N;
     const float2 a = sm[t];
     const float msk = A.submask[g];
-    sm[t] = cmul(make_float2(a.x * msk, a.y * msk), A.phalfxy[g]);
+    const float2 f = make_float2(a.x * msk, a.y * msk);
+    // the focal plane image (compute_pyrfocalplane): abs2_krnl with the point's weight
+    if (A.focal_work) A.focal_work[(size_t)p * N * N + g] = A.w[p] * (f.x * f.x + f.y * f.y);
+    sm[t] = cmul(f, A.phalfxy[g]);
   }
   __syncthreads();
   fft_ct<N, PYR_SEQ, PYR_THREADS>(sm, tws, false);
@@ -289,6 +293,16 @@ __global__ void pyr_norm_noise_kernel(float *binimg, const float *partial, int n
   }
 }
 
+// focal plane: the per-point images summed in point order from zero, as the
+// reference accumulates d_pyrfocalplane (sutra_wfs_pyr_pyrhr.cpp:398-401,501-506)
+__global__ void pyr_focal_sum_kernel(float *focal, const float *work, int npts, int64_t n2) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n2; i += (int64_t)gridDim.x * blockDim.x) {
+    float acc = 0.f;
+    for (int p = 0; p < npts; ++p) acc += work[(size_t)p * n2 + i];
+    focal[i] = acc;
+  }
+}
+
 template <int N>
 static void pyr_launch(const PyrArgs &A, int npts, int ntot, int nbin_ctas, cudaStream_t s) {
   const size_t sm = sizeof(float2) * (N * PYR_SEQ + N / 2);
@@ -406,6 +420,13 @@ void aob_pyr::comp_image(bool with_noise, cudaStream_t s) {
   A.nrebin = nrebin;
   A.nb = nbin();
   A.rows_per_bin_cta = (PYR_SEQ / nrebin) * nrebin;
+  const int64_t n2 = (int64_t)nfft * nfft;
+  A.focal_work = nullptr;
+  if (compute_focalplane) {
+    if (focal_work.n != npts * n2) focal_work.alloc(npts * n2);
+    if (focalplane.n != n2) focalplane.alloc(n2);
+    A.focal_work = focal_work.p;
+  }
   const int nbin_ctas = nfft / A.rows_per_bin_cta;
   switch (nfft) {
     case 64: pyr_launch<64>(A, npts, ntot, nbin_ctas, s); break;
@@ -414,6 +435,11 @@ void aob_pyr::comp_image(bool with_noise, cudaStream_t s) {
     case 512: pyr_launch<512>(A, npts, ntot, nbin_ctas, s); break;
     case 1024: pyr_launch<1024>(A, npts, ntot, nbin_ctas, s); break;
     default: pyr_launch<2048>(A, npts, ntot, nbin_ctas, s); break;
+  }
+  if (compute_focalplane) {
+    pyr_focal_sum_kernel<<<(int)std::min<int64_t>((n2 + 255) / 256, 8 * num_sms(device)), 256, 0, s>>>(
+        focalplane.p, focal_work.p, npts, n2);
+    AOB_LAUNCH_CHECK("pyr_focal_sum_kernel");
   }
   const float nz = with_noise ? noise : -1.f;
   const int noise_mode = nz > 0 ? 2 : (nz > -1 ? 1 : 0);

@@ -4,13 +4,22 @@ with their names, constructor arguments and method names, over libaob200.
 
 Covered (the calls shesha's supervisor makes on the RTC path):
 
-* ``Sensors`` (sensors.cpp:28-107, initgs :159-191) holding Shack-Hartmann
-  (``SHWFS``, wfs_sh.cpp:41-148) and pyramid (``PYRWFS``, wfs_pyrhr.cpp:131-163)
-  sensors: ``load_arrays``, ``comp_image``, ``set_noise``, ``set_pupil``,
-  ``fill_binimage``, ``d_binimg`` / ``d_bincube`` / ``d_intensities`` /
-  ``d_validsubsx`` / ``d_validsubsy`` / ``d_gs.d_phase.d_screen``;
+* ``Sensors`` (sensors.cpp:28-107, initgs :159-191, set_field_stop :200-210)
+  holding Shack-Hartmann (``SHWFS``, wfs_sh.cpp:41-148) and pyramid
+  (``PYRWFS``, wfs_pyrhr.cpp:131-163) sensors: ``load_arrays``,
+  ``comp_image``, ``slopes_geom`` (wfs.cpp:242-262), ``set_noise``,
+  ``set_pupil``, ``set_binimg``, ``fill_binimage``, ``comp_nphot``,
+  ``set_bincube``, ``set_dark`` / ``set_flat`` (SH camera), ``set_phalfxy`` /
+  ``set_submask`` / ``set_pyrimg`` / ``compute_pyrfocalplane`` (pyramid),
+  ``d_binimg`` / ``d_bincube`` / ``d_binmap`` / ``d_intensities`` /
+  ``d_slopes`` / ``d_validsubsx`` / ``d_validsubsy`` /
+  ``d_pyrfocalplane`` / ``d_gs.d_phase.d_screen``, ``d_gs.add_layer``;
+* ``Dms`` / ``Dm`` (dms.cpp:120-600) for piezo-stack DMs: ``add_dm``,
+  ``pzt_loadarrays``, ``set_com``, ``comp_shape``, ``comp_oneactu``,
+  ``reset_shape``, ``d_shape`` / ``d_com``;
 * ``Rtc_FFF`` (rtc.cpp:100-485): ``add_centroider`` (cog, tcog, wcog, bpcog,
-  pyr, maskedpix), ``add_controller`` (ls, generic), ``do_centroids``, ``do_control``, ``apply_control``,
+  pyr, maskedpix), ``add_controller`` (ls, generic), ``do_imat`` (one batched
+  push-pull evaluation per DM), ``do_centroids``, ``do_control``, ``apply_control``,
   ``comp_voltage``, ``do_clipping``, ``set_gain``, ``set_modal_gains``,
   ``imat_svd``, ``build_cmat``, ``set_centroids_ref``, ``do_calibrate_img``,
   ``d_centro`` / ``d_control``;
@@ -23,9 +32,9 @@ Covered (the calls shesha's supervisor makes on the RTC path):
 
 Errors raise ``aob200._lib.AobError`` with the library's message, where the
 reference raises ``RuntimeError`` from its C++ layer.  Everything else of the
-reference (atmosphere, DMs, targets, other sensor / controller families) is not
-part of this path; ``aob200.optics`` / ``aob200.turbulence`` have the layers,
-DMs and targets the closed-loop tests use.
+reference (atmosphere, targets, other DM, sensor and controller families) is
+not part of this path; ``aob200.optics`` / ``aob200.turbulence`` have the
+layers and targets the closed-loop tests use.
 """
 
 from __future__ import annotations
@@ -60,9 +69,18 @@ class _Phase:
 
 
 class _GuideStar:
+    """``wfs.d_gs``: the guide star's phase and the DM layers it sees
+    (SutraSource::add_layer, source.cpp; the offsets shesha's wfs_init gives)."""
+
     def __init__(self, wfs, lambda_um):
         self.d_phase = _Phase(wfs)
         self.Lambda = float(lambda_um)
+        self.dm_layers = {}  # DM index -> (xoff, yoff) on the sensor's phase grid
+
+    def add_layer(self, type, idx, xoff, yoff):
+        if str(type) in ("pzt", "tt", "kl"):
+            self.dm_layers[int(idx)] = (float(xoff), float(yoff))
+        return 0
 
 
 class _WfsBase:
@@ -87,8 +105,30 @@ class _WfsBase:
     d_validsubsy = property(lambda self: self._w.buffer("validsubsy", np.int32))
     d_fluxPerSub = property(lambda self: self._w.buffer("fluxPerSub"))
 
+    d_slopes = property(lambda self: self._w.buffer("slopes"))
+
     def comp_image(self, noise=True):
         self._w.comp_image(noise=bool(noise))
+
+    def slopes_geom(self, *args, **kw):
+        """slopes_geom(type=0) into d_slopes, or slopes_geom(slopes, type=0) into the
+        given float32 host array (wfs.cpp:242-262): 0 edge differences, 1 derivative
+        weighted by the pupil, 2 tip/tilt projection."""
+        slopes = kw.pop("slopes", None)
+        if args and isinstance(args[0], np.ndarray):
+            slopes, args = args[0], args[1:]
+        t = int(args[0]) if args else int(kw.pop("type", 0))
+        self._w.slopes_geom(t)
+        if slopes is not None:
+            slopes[...] = np.array(self.d_slopes).reshape(slopes.shape, order="F")
+        return 0
+
+    def set_binimg(self, binimg, nElem):
+        a = np.asarray(binimg, np.float32)
+        if a.size != int(nElem):
+            raise ValueError("set_binimg: nElem does not match the array")
+        self._w.set_binimg(a)
+        return 0
 
     def set_noise(self, noise, seed):
         self._w.set_noise(float(noise), int(seed))
@@ -106,14 +146,34 @@ class SHWFS(_WfsBase):
 
     def load_arrays(self, phasemap, hrmap, binmap, offsets, fluxPerSub, validsubsx, validsubsy, istart, jstart,
                     ttprojmat=None, kernel=None):
-        self._w.load_arrays(phasemap, hrmap, binmap, offsets, fluxPerSub, validsubsx, validsubsy, istart, jstart)
+        self._w.load_arrays(phasemap, hrmap, binmap, offsets, fluxPerSub, validsubsx, validsubsy, istart, jstart,
+                            ttprojmat)
 
     d_bincube = property(lambda self: self._w.d_bincube)
     d_intensities = property(lambda self: self._w.d_intensities)
-    d_slopes = property(lambda self: self._w.buffer("slopes"))
+    d_binmap = property(lambda self: self._w.buffer("binmap", np.int32))
+    d_validpuppixx = property(lambda self: self._w.buffer("istart", np.int32))
+    d_validpuppixy = property(lambda self: self._w.buffer("jstart", np.int32))
 
     def fill_binimage(self, async_=False):
         self._w.fill_binimage()
+
+    def comp_nphot(self, ittime, optthroughput, diam, nxsub, zerop=0, gsmag=0, lgsreturnperwatt=0, laserpower=0):
+        """Photons per sub-aperture and frame (sutra_wfs_sh.cpp:645-663)."""
+        if laserpower == 0:
+            zp = 1e11 if zerop == 0 else float(zerop)
+            nphot = zp * 10.0 ** (-0.4 * float(gsmag)) * ittime * optthroughput * (diam / nxsub) ** 2
+        else:
+            nphot = lgsreturnperwatt * laserpower * optthroughput * (diam / nxsub) ** 2 * 1e4 * ittime
+        self._w.set_nphot(np.float32(nphot))
+        return 0
+
+    def set_bincube(self, bincube, nElem):
+        a = np.asarray(bincube, np.float32)
+        if a.size != int(nElem):
+            raise ValueError("set_bincube: nElem does not match the array")
+        self._w.set_bincube(a)
+        return 0
 
     # fakecam (Sensors(..., fakecam, max_flux_per_pix, max_pix_value)): the uint16 frame
     d_camimg = property(lambda self: self._w.d_camimg)
@@ -135,10 +195,51 @@ class PYRWFS(_WfsBase):
 
     def load_arrays(self, halfxy, cx, cy, weights, sincar, submask, validsubsx, validsubsy, phasemap=None,
                     fluxPerSub=None, ttprojmat=None):
-        self._w.load_arrays(halfxy, cx, cy, weights, sincar, submask, validsubsx, validsubsy, phasemap, fluxPerSub)
+        self._w.load_arrays(halfxy, cx, cy, weights, sincar, submask, validsubsx, validsubsy, phasemap, fluxPerSub,
+                            ttprojmat)
+        self._compute_focal = False
 
     def set_pyr_modulation_points(self, cx, cy, weights=None, npts=None):
         self._w.set_modulation(cx, cy, weights)
+
+    d_submask = property(lambda self: self._w.buffer("submask", shape=(self._w.nfft, self._w.nfft)))
+    d_hrimg = property(lambda self: self._w.buffer("hrimg", shape=(self._w.nfft, self._w.nfft)))
+    d_pyrfocalplane = property(lambda self: self._w.buffer("pyrfocalplane", shape=(self._w.nfft, self._w.nfft)))
+
+    @property
+    def d_phalfxy(self):
+        a = self._w.buffer("phalfxy")
+        n = self._w.nfft
+        return _core.DeviceArray(a.ptr, n * n, np.complex64, (n, n), owner=a)
+
+    @property
+    def compute_pyrfocalplane(self):
+        return getattr(self, "_compute_focal", False)
+
+    @compute_pyrfocalplane.setter
+    def compute_pyrfocalplane(self, on):
+        """When set, every comp_image also forms d_pyrfocalplane (wfs_pyrhr.cpp:83-90)."""
+        self._compute_focal = bool(on)
+        self._w.set_compute_focalplane(bool(on))
+
+    def set_phalfxy(self, phalfxy):
+        """The pyramid mask exp(i phase), nfft x nfft complex64 (wfs_pyrhr.cpp:235-242)."""
+        self._w.set_phalfxy(phalfxy)
+        return 0
+
+    def set_submask(self, submask):
+        self._w.set_submask(np.asarray(submask, np.float32))
+        return 0
+
+    def set_pyrimg(self, img):
+        self._w.set_binimg(np.asarray(img, np.float32))
+        return 0
+
+    def comp_nphot(self, ittime, optthroughput, diam, cobs, zerop=0, gsmag=0):
+        """Photons per frame over the pupil (sutra_wfs_pyr_pyrhr.cpp:722-729)."""
+        nphot = zerop * 10.0 ** (-0.4 * gsmag) * ittime * optthroughput * np.pi / 4.0 * (1 - cobs * cobs) * diam * diam
+        self._w.set_nphot(np.float32(nphot))
+        return 0
 
 
 class Sensors:
@@ -182,6 +283,122 @@ class Sensors:
 
 
 # ---------------------------------------------------------------------------
+class Dm:
+    """SutraDm of the piezo-stack type (python_module/sutra/src/dms.cpp:270-600):
+    the command vector, the shape on its dim x dim support and the single-actuator
+    poke that do_imat uses."""
+
+    def __init__(self, type, alt, dim, nactus, influsize, push4imat, device):
+        if type != "pzt":
+            raise ValueError(f"add_dm: DM type {type!r} is not supported (pzt)")
+        self.type, self.altitude = type, float(alt)
+        self.dim, self.nactus, self.influsize = int(dim), int(nactus), int(influsize)
+        self.push4imat = float(push4imat)
+        self.device = int(device)
+        self._d = None
+        self._one = None
+
+    def _need(self):
+        if self._d is None:
+            raise ValueError("Dm: pzt_loadarrays has not been called")
+        return self._d
+
+    def pzt_loadarrays(self, influ, influpos, npoints, istart, xoff, yoff):
+        """The influence functions [influsize, influsize, nactus] and each
+        actuator's corner (xoff, yoff) on the support, as dm_init.py:186-193 passes
+        them; influpos / npoints / istart (the reference's pixel lists) are
+        rebuilt from these by the library."""
+        from aob200 import optics
+
+        influ = np.asarray(influ, np.float32)
+        i1, j1 = np.asarray(xoff, np.int64), np.asarray(yoff, np.int64)
+        # comp_dmgeom (dm_init.py:902-955) places actuator a's sample (x, y) at
+        # screen pixel (offs + i1[a] + x) + dim (offs + j1[a] + y), offs > 0 when
+        # the DM support is smaller than the screen: read offs off the first
+        # listed sample
+        off = 0
+        npts, ist, pos = np.asarray(npoints), np.asarray(istart), np.asarray(influpos)
+        nz = np.flatnonzero(npts[: self.dim * self.dim]) if npts.size else np.empty(0, np.int64)
+        if nz.size:
+            p = int(nz[0])
+            q = int(pos[int(ist[p])])
+            s = influ.shape[0]
+            a, y, x = q // (s * s), (q // s) % s, q % s
+            off = p % self.dim - x - int(i1[a])
+            if p // self.dim - y - int(j1[a]) != off:
+                raise ValueError("pzt_loadarrays: influpos does not match xoff / yoff")
+        self._d = optics.Dm(self.dim, influ, i1 + off, j1 + off, device=self.device)
+        return 0
+
+    @property
+    def d_shape(self):
+        return self._need().d_shape
+
+    @property
+    def d_com(self):
+        return self._need().buffer("com")
+
+    def set_com(self, com, shape_dm=True):
+        self._need().set_com(np.asarray(com, np.float32))
+        if shape_dm:
+            self.comp_shape()
+        return 0
+
+    def comp_shape(self, com=None):
+        d = self._need()
+        if com is not None:
+            d.set_com(np.asarray(com, np.float32))
+        d.comp_shape()
+        return 0
+
+    def reset_shape(self):
+        self._need()
+        self.d_shape.set(np.zeros((self.dim, self.dim), np.float32))
+        return 0
+
+    def comp_oneactu(self, nactu, ampli):
+        """The shape of actuator ``nactu`` alone at ``ampli`` volts; d_com is left as it is."""
+        d = self._need()
+        if self._one is None:
+            self._one = _core.OwnedDeviceArray(self.nactus, np.float32, device=self.device)
+        v = np.zeros(self.nactus, np.float32)
+        v[int(nactu)] = ampli
+        self._one.set(v)
+        d.comp_shape(self._one.ptr)
+        return 0
+
+
+class Dms:
+    """SutraDms (dms.cpp:120-260): the list of DMs."""
+
+    def __init__(self):
+        self._dms = []
+
+    @property
+    def d_dms(self):
+        return self._dms
+
+    def add_dm(self, context, type, alt, dim, nactus, influsize, ninflupos, n_npoints, push4imat, nord, *rest):
+        """Both reference overloads: (..., nord, device) and (..., nord, dx, dy,
+        thetaML, G, device); only a registration of dx = dy = thetaML = 0, G = 1 is
+        supported."""
+        if len(rest) == 5:
+            dx, dy, theta, G, device = rest
+            if (dx, dy, theta, G) != (0, 0, 0, 1):
+                raise ValueError("add_dm: DM mis-registration is not supported")
+        elif len(rest) == 1:
+            (device,) = rest
+        else:
+            raise TypeError("add_dm: expected (..., nord, device) or (..., nord, dx, dy, thetaML, G, device)")
+        self._dms.append(Dm(type, alt, dim, nactus, influsize, push4imat, device))
+        return 0
+
+    def remove_dm(self, idx):
+        del self._dms[int(idx)]
+        return 0
+
+
+# ---------------------------------------------------------------------------
 class Centroider:
     """SutraCentroider{Cog,Tcog,Wcog,Pyr} (centroider.cpp:83-352)."""
 
@@ -213,6 +430,13 @@ class Centroider:
     d_validx = property(lambda self: self._c.buffer("validx", np.int32))
     d_validy = property(lambda self: self._c.buffer("validy", np.int32))
     d_weights = property(lambda self: self._c.buffer("weights"))
+
+    def get_cog(self):
+        """Centroids of the sensor's current image into its d_slopes (centroider.cpp:186-188)."""
+        if self.wfs is None:
+            raise ValueError("get_cog: the centroider has no sensor (use Rtc.do_centroids)")
+        self._c.get_cog(self.wfs._w.buffer("slopes").ptr)
+        return 0
 
     def load_validpos(self, validx, validy, N):
         self._c.load_validpos(_arr(validx, int(N)), _arr(validy, int(N)))
@@ -453,7 +677,51 @@ class Rtc_FFF:
         c = (ControllerLS if typec == "ls" else ControllerGENERIC)(nslope, nactu, delay, device)
         c.centro_idx = ([int(i) for i in _arr(idx_centro)][: int(ncentro)] if idx_centro is not None and ncentro
                         else list(range(len(self.d_centro))))
+        # the DMs the controller drives (d_dmseen): indexes into ``dms``
+        c.dm_idx = ([int(i) for i in _arr(idx_dms)][: int(ndm)] if idx_dms is not None and ndm else None)
         self.d_control.append(c)
+        return 0
+
+    def do_imat(self, ncontrol, dms, kernconv=False):
+        """Push-pull interaction matrix (sutra_rtc.cpp:150-292): every actuator of
+        every DM the controller drives, pushed and pulled by its push4imat, seen
+        by the controller's SH sensors (noise-free, nphot4imat photons), the
+        slopes (s_push - s_pull) / (2 push) as the columns of the controller's
+        d_imat.  All actuators of a DM go through one batched evaluation
+        (aob_imat_build) per sensor."""
+        from aob200._lib import call
+
+        if kernconv:
+            raise ValueError("do_imat: the spot convolution kernel is not supported")
+        c = self.d_control[int(ncontrol)]
+        if c._kind != "ls":
+            raise ValueError("do_imat: the controller must be ls")
+        seen = [dms.d_dms[i] for i in c.dm_idx] if c.dm_idx is not None else list(dms.d_dms)
+        idx_of = {id(d): i for i, d in enumerate(dms.d_dms)}
+        if sum(d.nactus for d in seen) != c.nactu:
+            raise ValueError("do_imat: the DMs' actuators do not add up to the controller's nactu")
+        imat = np.zeros((c.nslope, c.nactu), np.float32)
+        a0 = 0
+        for dm in seen:
+            d = dm._need()
+            off = 0
+            for i in c.centro_idx:
+                cen = self.d_centro[i]
+                ns = cen.nslopes
+                w = cen.wfs
+                if not isinstance(w, SHWFS):
+                    raise ValueError("do_imat: only Shack-Hartmann sensors are supported")
+                n = w._w.npup
+                layer = w.d_gs.dm_layers.get(idx_of[id(dm)]) if w.d_gs is not None else None
+                xoff, yoff = layer if layer is not None else ((dm.dim - n) / 2.0,) * 2
+                cen._c.attach(w._w)
+                tmp = _core.OwnedDeviceArray(ns * dm.nactus, np.float32, (ns, dm.nactus), device=dm.device)
+                call("aob_imat_build", w._w.h, cen._c.h, d.h, float(xoff), float(yoff), float(dm.push4imat), 0,
+                     tmp.ptr, None)
+                imat[off:off + ns, a0:a0 + dm.nactus] = np.array(tmp)
+                off += ns
+            a0 += dm.nactus
+        c.set_imat(imat)
         return 0
 
     def remove_controller(self, ncontrol):

@@ -63,8 +63,10 @@ int aob_sh_create(aob_sh **out, int device, int nxsub, int nvalid, int npix, int
                   int nrebin, int nfft, int ntot, int npup, float pdiam, float nphot,
                   float nphot4imat);
 int aob_sh_destroy(aob_sh *h);
-/* SutraWfsSH::load_arrays (sutra_wfs_sh.cpp:308-331); phasemap, ttprojmat and
- * kernel are accepted for interface parity and may be NULL.  binmap is
+/* SutraWfsSH::load_arrays (sutra_wfs_sh.cpp:308-331).  phasemap [nphase^2,
+ * nvalid] (indexes into the npup x npup phase screen) and ttprojmat
+ * [nphase^2, 2 nvalid], both column-major, are kept for aob_sh_slopes_geom
+ * and may be NULL; kernel is accepted for interface parity.  binmap is
  * [nrebin^2, npix^2] indexes into the ntot x ntot image, offsets [nphase^2];
  * fluxPerSub, validsubsx, validsubsy, istart and jstart have nvalid entries.
  * hrmap (nfft^2 positions of the nfft x nfft spot in the ntot x ntot image) is
@@ -127,6 +129,13 @@ int aob_sh_set_tuning(aob_sh *h, int subaps_per_cta);
 /* set_bincube / set_binimg: overwrite from host. */
 int aob_sh_set_bincube(aob_sh *h, const float *host, int64_t n);
 int aob_sh_set_binimg(aob_sh *h, const float *host, int64_t n);
+/* SutraWfs::slopes_geom(slopes, type) (sutra_wfs.cpp:199-251): geometric
+ * slopes of the sensor's phase into dev_slopes (2 nvalid floats; NULL: the
+ * sensor's own slopes buffer).  type 0: edge differences (phase_reduce), 1:
+ * pupil-weighted finite differences over fluxPerSub (phase_derive), 2: the
+ * tip/tilt projection matrix (phase_project).  Needs the phasemap (and for
+ * type 2 ttprojmat) from load_arrays. */
+int aob_sh_slopes_geom(aob_sh *h, int type, float *dev_slopes, void *stream);
 
 /* ---- pyramid sensor ------------------------------------------------- *
  * Replaces SutraWfs_PyrHR (libsutra/src.cpp/sutra_wfs_pyr_pyrhr.cpp) as bound
@@ -144,7 +153,8 @@ int aob_pyr_destroy(aob_pyr *h);
  * halfxy = exp(i pyramid phase) as nfft^2 complex64 (float pairs), the
  * reference's layout; cx, cy, weights: npts modulation tilts / weights
  * (weights may be NULL = 1); sincar, submask: nfft^2; validsubsx / validsubsy:
- * 4 * nvalid; phasemap and ttprojmat are accepted for interface parity. */
+ * 4 * nvalid; phasemap [nphase^2, nvalid] and ttprojmat [nphase^2, 2 nvalid]
+ * (column-major, may be NULL) are kept for aob_pyr_slopes_geom. */
 int aob_pyr_load_arrays(aob_pyr *h, const float *halfxy_c64, const float *cx, const float *cy,
                         const float *weights, const float *sincar, const float *submask,
                         const int32_t *validsubsx, const int32_t *validsubsy, const int32_t *phasemap,
@@ -159,10 +169,27 @@ int aob_pyr_set_lambda(aob_pyr *h, float lambda_um);
 int aob_pyr_set_nphot(aob_pyr *h, float nphot);
 int aob_pyr_set_frame(aob_pyr *h, uint64_t frame);
 int aob_pyr_get_frame(aob_pyr *h, uint64_t *frame);
-/* which: "phase", "pupil", "binimg", "hrimg", "validsubsx", "validsubsy", "fluxPerSub". */
+/* which: "phase", "pupil", "binimg", "hrimg", "validsubsx", "validsubsy",
+ * "fluxPerSub", "submask", "phalfxy" (2 nfft^2 floats), "sincar", "phasemap",
+ * "ttprojmat", "slopes" (geometric slopes), "pyrfocalplane" (nfft^2). */
 int aob_pyr_buffer(aob_pyr *h, const char *which, void **dev_ptr, int64_t *nelem);
 /* SutraWfs_PyrHR::comp_image(noise) (sutra_wfs_pyr_pyrhr.cpp:379-627). */
 int aob_pyr_comp_image(aob_pyr *h, int noise, void *stream);
+/* PYRWFS.set_submask (python_module/sutra/src/wfs_pyrhr.cpp:255-270,
+ * sutra_wfs_pyr_pyrhr.cpp:361-377): the focal-plane field stop, nfft^2. */
+int aob_pyr_set_submask(aob_pyr *h, const float *submask, int64_t n);
+/* SutraWfs_PyrHR::set_phalfxy (sutra_wfs_pyr_pyrhr.cpp:731-744): the pyramid
+ * mask exp(i phase), nfft^2 complex64 as float pairs (n = nfft^2). */
+int aob_pyr_set_phalfxy(aob_pyr *h, const float *phalfxy_c64, int64_t n);
+/* PYRWFS.set_pyrimg / set_binimg (wfs_pyrhr.cpp:190-205): the binned image. */
+int aob_pyr_set_binimg(aob_pyr *h, const float *img, int64_t n);
+/* PYRWFS.compute_pyrfocalplane (wfs_pyrhr.cpp:83-90): while enabled every
+ * comp_image also forms the focal-plane image sum_p w_p |submask x focal
+ * field_p|^2 (sutra_wfs_pyr_pyrhr.cpp:398-401) into "pyrfocalplane". */
+int aob_pyr_set_compute_focalplane(aob_pyr *h, int enable);
+/* SutraWfs::slopes_geom for the pyramid sensor (see aob_sh_slopes_geom);
+ * dev_slopes NULL: the sensor's "slopes" buffer. */
+int aob_pyr_slopes_geom(aob_pyr *h, int type, float *dev_slopes, void *stream);
 
 /* ---- centroiders ------------------------------------------------------ *
  * Replaces SutraCentroiderCog / Tcog / Wcog (libsutra/src.cpp/
@@ -465,10 +492,12 @@ int aob_dm_buffer(aob_dm *d, const char *which, void **dev_ptr, int64_t *nelem);
  * chunk of actuators (chunk 0 = all), their bilinear raytrace onto the sensor's
  * npup x npup phase grid at offset (xoff, yoff) in the DM screen, the sensor
  * images with the attached CoG-family centroider over all pokes in one launch
- * (noise-free, the sensor's current photon count), and the columns
+ * (noise-free, with the sensor's nphot4imat photons when it is > 0 as
+ * SutraRtc::comp_images_imat does, else its current photon count), and the columns
  * (s_push - s_pull) / (2 push) into dev_imat, nslope x nact column-major on the
  * device.  Equal bit for bit to poking one actuator after the other with
- * aob_dm_comp_shape, aob_raytrace, aob_sh_comp_image and aob_centro_get_cog.
+ * aob_dm_comp_shape, aob_raytrace, aob_sh_comp_image and aob_centro_get_cog
+ * (at the same photon count).
  * Needs about 2 chunk (dim^2 + npup^2) floats of scratch; waits for the stream. */
 int aob_imat_build(aob_sh *w, aob_centro *c, aob_dm *dm, float xoff, float yoff, float push, int chunk,
                    float *dev_imat, void *stream);

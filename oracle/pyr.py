@@ -22,8 +22,12 @@ import numpy as np
 from . import philox
 
 
-def hr_image(phase, pupil, g, lam_um, weights=None):
-    """High-resolution modulated image (before the pixel transfer function)."""
+def hr_image(phase, pupil, g, lam_um, weights=None, workers=None):
+    """High-resolution modulated image (before the pixel transfer function).
+
+    ``workers``: None runs one modulation point after the other through
+    numpy.fft; an integer batches the points through scipy.fft on that many
+    threads (the same sums, for the multi-core CPU baseline)."""
     n_fft = g.nfft
     n = phase.shape[0]
     off = int((n_fft - n) / 2.0)
@@ -34,22 +38,61 @@ def hr_image(phase, pupil, g, lam_um, weights=None):
     hr = np.zeros((n_fft, n_fft))
     base = phase.astype(np.float64) * mic2rad
     amp = pupil.astype(np.float64)
+    npts = g.pyr_cx.size
+    chunk = 1 if workers is None else max(1, min(npts, 8))
+    for p0 in range(0, npts, chunk):
+        pts = range(p0, min(p0 + chunk, npts))
+        f = np.zeros((len(pts), n_fft, n_fft), dtype=np.complex128)
+        for k, p in enumerate(pts):
+            phi = float(g.pyr_cx[p]) * xx[:, None] + float(g.pyr_cy[p]) * xx[None, :]
+            f[k, off:off + n, off:off + n] = amp * np.exp(1j * (base + phi))
+        if workers is None:
+            F = np.fft.ifft2(f) * (n_fft * n_fft)
+            G = np.fft.fft2(F * mask)
+        else:
+            import scipy.fft as sf
+
+            F = sf.ifft2(f, workers=workers) * (n_fft * n_fft)
+            G = sf.fft2(F * mask, workers=workers)
+        for k, p in enumerate(pts):
+            hr += w[p] * (G[k].real ** 2 + G[k].imag ** 2)
+    return hr
+
+
+def focal_plane(phase, pupil, g, lam_um, weights=None):
+    """The focal plane image of compute_pyrfocalplane: sum over the modulation
+    points of w_p |submask x F_p|^2, F_p the inverse FFT of the tilted pupil field
+    (abs2 of d_camplifoc after apply_submask, sutra_wfs_pyr_pyrhr.cpp:384-401)."""
+    n_fft = g.nfft
+    n = phase.shape[0]
+    off = int((n_fft - n) / 2.0)
+    xx = np.arange(n) - n / 2.0
+    sm = g.submask.astype(np.float64)
+    w = np.ones(g.pyr_cx.size) if weights is None else np.asarray(weights, np.float64)
+    base = phase.astype(np.float64) * (2 * np.pi / lam_um)
+    amp = pupil.astype(np.float64)
+    out = np.zeros((n_fft, n_fft))
     for p in range(g.pyr_cx.size):
         phi = float(g.pyr_cx[p]) * xx[:, None] + float(g.pyr_cy[p]) * xx[None, :]
         f = np.zeros((n_fft, n_fft), dtype=np.complex128)
         f[off:off + n, off:off + n] = amp * np.exp(1j * (base + phi))
-        F = np.fft.ifft2(f) * (n_fft * n_fft)
-        G = np.fft.fft2(F * mask)
-        hr += w[p] * (G.real ** 2 + G.imag ** 2)
-    return hr
+        F = np.fft.ifft2(f) * (n_fft * n_fft) * sm
+        out += w[p] * (F.real ** 2 + F.imag ** 2)
+    return out
 
 
-def comp_image(phase, pupil, g, lam_um, nphot, weights=None, noise=-1.0, frame=0, seed=1234):
+def comp_image(phase, pupil, g, lam_um, nphot, weights=None, noise=-1.0, frame=0, seed=1234, workers=None):
     """Binned, normalised (and optionally noisy) pyramid image [nb, nb]."""
     n_fft = g.nfft
-    hr = hr_image(phase, pupil, g, lam_um, weights)
-    T = np.fft.ifft2(hr) * (n_fft * n_fft)
-    hr2 = np.fft.fft2(T * g.sincar.astype(np.float64)).real
+    hr = hr_image(phase, pupil, g, lam_um, weights, workers)
+    if workers is None:
+        T = np.fft.ifft2(hr) * (n_fft * n_fft)
+        hr2 = np.fft.fft2(T * g.sincar.astype(np.float64)).real
+    else:
+        import scipy.fft as sf
+
+        T = sf.ifft2(hr, workers=workers) * (n_fft * n_fft)
+        hr2 = sf.fft2(T * g.sincar.astype(np.float64), workers=workers).real
     r = g.nrebin
     nb = n_fft // r
     b = hr2.reshape(nb, r, nb, r).sum(axis=(1, 3)) / (r * r)

@@ -129,3 +129,46 @@ def comp_image(phase, pupil, g, scale, nphot, noise=-1.0, seed=1234, frame=0):
     cube = add_noise(cube, noise, seed, frame)
     img = bin_image(cube, get("validsubsx"), get("validsubsy"), int(get("npix")), int(get("nxsub")))
     return cube, img, sums
+
+
+def slopes_geom(phase, pupil, phasemap, flux_per_sub, subapd, nphase, kind=0, ttprojmat=None):
+    """Geometric slopes of the phase (SutraWfs::slopes_geom, libsutra/src.cpp/
+    sutra_wfs.cpp:199-251) in float64; the reference's float alpha is kept.
+
+    ``phase`` / ``pupil``: the sensor's n x n screen and pupil ([x, y]);
+    ``phasemap``: [nphase^2, nvalid] indexes into the Fortran-flattened screen;
+    ``ttprojmat``: [nphase^2, 2 nvalid].
+      kind 0  reduce_phasex / reduce_phasey (sutra_wfs.cu:866-910)
+      kind 1  derive_phasex / derive_phasey (sutra_wfs.cu:912-970)
+      kind 2  project_gather + two strided-batched GEMMs (sutra_wfs.cu:1049-1082)
+    """
+    n = int(nphase)
+    ph = np.asarray(phase, np.float64).ravel(order="F")
+    pup = np.asarray(pupil, np.float64).ravel(order="F")
+    pm = np.asarray(phasemap)
+    nvalid = pm.shape[1]
+    alpha = float(np.float32(0.206265 / float(np.float32(subapd)) * n / (n - 1)))
+    v = ph[pm]  # [n^2, nvalid]
+    if kind == 0:
+        rows = v.reshape(n, n, nvalid, order="F")  # rows[a, b, k]: sample a + b n
+        sx = (rows[n - 1, :, :] - rows[0, :, :]).sum(axis=0) / n * alpha
+        sy = (rows[:, n - 1, :] - rows[:, 0, :]).sum(axis=0) / n * alpha
+    elif kind == 1:
+        m = pup[pm]
+        a = np.arange(n * n) % n
+        i = np.arange(n * n)
+        ip1, im1 = np.minimum(i + 1, n * n - 1), np.maximum(i - 1, 0)
+        dx = np.where((a == 0)[:, None], v[ip1] - v, np.where((a == n - 1)[:, None], v - v[im1], v[ip1] - v[im1]))
+        ipn, imn = np.minimum(i + n, n * n - 1), np.maximum(i - n, 0)
+        dy = np.where((i < n)[:, None], v[ipn] - v,
+                      np.where((i >= n * (n - 1))[:, None], v - v[imn], v[ipn] - v[imn]))
+        f = np.asarray(flux_per_sub, np.float64)
+        sx = (dx * m).sum(axis=0) / n * alpha / f / 2
+        sy = (dy * m).sum(axis=0) / n / 2 * alpha / f
+    elif kind == 2:
+        M = np.asarray(ttprojmat, np.float64)
+        sx = (M[:, :nvalid] * v).sum(axis=0)
+        sy = (M[:, nvalid:] * v).sum(axis=0)
+    else:
+        raise ValueError("slopes_geom: kind must be 0, 1 or 2")
+    return np.concatenate([sx, sy])

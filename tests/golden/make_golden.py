@@ -229,6 +229,10 @@ def make_dm(conf, gi, dmi, c):
         xpos=p_dm._xpos, ypos=p_dm._ypos, i1=a["i1"], j1=a["j1"], influ=a["influ"],
         ntotact=p_dm._ntotact, influsize=p_dm._influsize, pitch=np.float64(p_dm._pitch),
         n1=p_dm._n1, n2=p_dm._n2, dim=args[3], n_mpupil=p_geom._n, cent=np.float64(p_geom.cent),
+        # the reference's per-pixel lists of influence samples (comp_dmgeom), for
+        # driving its own SutraDm in the reference-run fixtures
+        influpos=np.asarray(a["influpos"], np.int32), ninflu=np.asarray(a["ninflu"], np.int32),
+        influstart=np.asarray(a["influstart"], np.int32),
     )
 
 

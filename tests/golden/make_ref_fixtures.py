@@ -4,6 +4,7 @@ Run on a machine with a GPU after ``python oracle/build_ref.py`` built the
 reference's ``carma`` / ``sutra`` modules into ``oracle/_ref/``:
 
     python tests/golden/make_ref_fixtures.py [OUT_DIR [CASE ...]]
+    python tests/golden/make_ref_fixtures.py extras [OUT_DIR]
 
 For each case the script builds the sensor, centroiders and least-squares
 controller through the reference's Python API in the order shesha's
@@ -17,7 +18,9 @@ phase screen and a seeded command matrix.  It stores the inputs and what the
 reference computes -- ``d_bincube``, ``d_binimg``, ``d_intensities``, the
 CoG / tCoG / wCoG slopes and the LS commands (SH), the pyramid image and its
 slopes -- as ``ref_<case>.npz``.  The sensors are noise-free (noise -1), the
-path where the reference's output is deterministic.
+path where the reference's output is deterministic.  ``extras`` stores the
+geometric slopes, the 17x17-DM interaction matrix (do_imat) and the pyramid
+focal plane as ``ref_extras_sh16.npz`` / ``ref_extras_pyr16.npz``.
 
 The tests (tests/test_gpu_refparity.py) compare this project's kernels, and
 the CPU oracle, with these files; nothing reads the reference at test time.
@@ -125,6 +128,82 @@ def run_pyr(ctx, name, seed):
     return out
 
 
+def run_sh_extras(ctx, name, seed):
+    """Geometric slopes (SutraWfs::slopes_geom, all three methods) and the
+    push-pull interaction matrix of the 17x17 DM (SutraRtc::do_imat with a CoG
+    centroider and an LS controller), on the reference's own objects."""
+    g = sh_geometry(name)
+    tel = _telescope(ctx, g.tel)
+    sensors, wfs = ref_sutra.sh_sensors(sutra, ctx, tel, g)
+    phase = phase_screen(g.tel.n, g.tel.pupdiam, seed)
+    wfs.d_gs.set_phase(phase)
+    out = dict(phase=phase)
+    for t in (0, 1, 2):
+        wfs.slopes_geom(t)
+        out[f"geom{t}"] = np.array(wfs.d_slopes)
+    dm = dict(np.load(os.path.join(HERE, "dm17.npz")))
+    dms = sutra.Dms()
+    dim = int(dm["dim"])
+    push = 0.05
+    dms.add_dm(ctx, "pzt", 0.0, dim, int(dm["ntotact"]), int(dm["influsize"]), int(dm["influpos"].size),
+               int(dm["ninflu"].size), push, 0, ctx.active_device)
+    dms.d_dms[0].pzt_loadarrays(dm["influ"], dm["influpos"], dm["ninflu"], dm["influstart"], dm["i1"], dm["j1"])
+    off = (dim - g.tel.n) / 2.0
+    wfs.d_gs.add_layer("pzt", 0, off, off)
+    rtc = sutra.Rtc_FFF()
+    ref_sutra.add_centroider(ctx, rtc, wfs, g, "cog")
+    nactu = int(dm["ntotact"])
+    rtc.add_controller(ctx, "ls", ctx.active_device, 0.0, 2 * g.nvalid, nactu, dms=dms,
+                       idx_dms=np.zeros(1, np.int32), ndm=1, idx_centro=np.zeros(1, np.int32), ncentro=1)
+    rtc.do_imat(0, dms, False)
+    out["imat"] = np.array(rtc.d_control[0].d_imat)
+    out["push4imat"] = push
+    out["dm_offset"] = off
+    return out
+
+
+def run_pyr_extras(ctx, name, seed):
+    """The pyramid focal plane (compute_pyrfocalplane) and geometric slopes
+    (methods 0 and 1) on the reference's own sensor."""
+    g = pyr_geometry(name)
+    tel = _telescope(ctx, g.tel)
+    i64 = lambda v: np.array([v], dtype=np.int64)  # noqa: E731
+    f32 = lambda v: np.array([v], dtype=np.float32)  # noqa: E731
+    npts = int(g.pyr_cx.size)
+    subapd = float(g.tel.diam) / g.nxsub
+    sensors = sutra.Sensors(ctx, tel, ["pyrhr"], 1, i64(g.nxsub), i64(g.nvalid), i64(4),
+                            i64(int(g.validsubsx.size)), i64(g.pdiam), i64(g.nrebin), i64(g.nfft), i64(g.ntot),
+                            i64(npts), f32(subapd), f32(g.nphotons), f32(g.nphotons), np.zeros(1, np.int32),
+                            np.zeros(1, bool), np.zeros(1, np.int32), np.zeros(1, np.int32), ctx.active_device,
+                            False)
+    _initgs(sensors, g.tel.n, g.wavelength_um, 6.0)
+    wfs = sensors.d_wfs[0]
+    halfxy = np.exp(1j * g.halfxy).astype(np.complex64).T.copy()
+    ttproj = np.zeros((g.pdiam * g.pdiam, 2 * g.nvalid), np.float32)
+    wfs.load_arrays(halfxy, g.pyr_cx, g.pyr_cy, np.ones(npts, np.float32), g.sincar, g.submask, g.validsubsx,
+                    g.validsubsy, g.phasemap, g.fluxPerSub, ttproj)
+    phase = (np.random.default_rng(seed).standard_normal((g.tel.n, g.tel.n)) * 0.02).astype(np.float32)
+    wfs.d_gs.set_phase(phase)
+    wfs.compute_pyrfocalplane = True
+    wfs.comp_image(False)
+    out = dict(phase=phase, focal=np.array(wfs.d_pyrfocalplane), binimg=np.array(wfs.d_binimg), subapd=subapd)
+    for t in (0, 1):
+        wfs.slopes_geom(t)
+        out[f"geom{t}"] = np.array(wfs.d_slopes)
+    return out
+
+
+def main_extras(out_dir):
+    os.makedirs(out_dir, exist_ok=True)
+    ctx = carma.context.get_instance_1gpu(0)
+    d = run_sh_extras(ctx, "sh16", seed=300)
+    np.savez_compressed(os.path.join(out_dir, "ref_extras_sh16.npz"), **d)
+    print("sh16 extras", {k: getattr(v, "shape", v) for k, v in d.items()})
+    d = run_pyr_extras(ctx, "pyr16", seed=301)
+    np.savez_compressed(os.path.join(out_dir, "ref_extras_pyr16.npz"), **d)
+    print("pyr16 extras", {k: getattr(v, "shape", v) for k, v in d.items()})
+
+
 def main(out_dir, only=None):
     os.makedirs(out_dir, exist_ok=True)
     ctx = carma.context.get_instance_1gpu(0)
@@ -143,4 +222,8 @@ def main(out_dir, only=None):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else HERE, sys.argv[2:])
+    args = sys.argv[1:]
+    if args and args[0] == "extras":
+        main_extras(args[1] if len(args) > 1 else HERE)
+    else:
+        main(args[0] if args else HERE, args[1:])

@@ -13,11 +13,17 @@ import pytest
 DROPIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "compass-saxoplus_b200", "dropin")
 
 API = {
-    "Sensors": ["initgs", "d_wfs"],
+    "Sensors": ["initgs", "d_wfs", "set_field_stop"],
     "SHWFS": ["load_arrays", "comp_image", "set_noise", "set_pupil", "fill_binimage", "d_binimg", "d_bincube",
-              "d_intensities", "d_validsubsx", "d_validsubsy", "d_fluxPerSub"],
-    "PYRWFS": ["load_arrays", "comp_image", "set_noise", "set_pupil", "set_pyr_modulation_points", "d_binimg"],
-    "Centroider": ["load_validpos", "set_npix", "set_scale", "set_offset", "set_threshold", "load_weights",
+              "d_intensities", "d_validsubsx", "d_validsubsy", "d_fluxPerSub", "slopes_geom", "set_binimg",
+              "set_dark", "set_flat", "comp_nphot", "set_bincube", "d_binmap", "d_slopes", "d_camimg",
+              "d_validpuppixx", "d_validpuppixy"],
+    "PYRWFS": ["load_arrays", "comp_image", "set_noise", "set_pupil", "set_pyr_modulation_points", "d_binimg",
+               "slopes_geom", "set_binimg", "set_phalfxy", "set_submask", "compute_pyrfocalplane",
+               "d_pyrfocalplane", "set_pyrimg", "comp_nphot", "d_submask", "d_phalfxy", "d_hrimg", "d_slopes"],
+    "Dms": ["add_dm", "remove_dm", "d_dms"],
+    "Dm": ["pzt_loadarrays", "set_com", "comp_shape", "comp_oneactu", "reset_shape", "d_shape", "d_com"],
+    "Centroider": ["get_cog", "load_validpos", "set_npix", "set_scale", "set_offset", "set_threshold", "load_weights",
                    "set_centroids_ref", "load_img", "calibrate_img", "set_dark", "set_flat", "set_pyr_method",
                    "set_pyr_thresh", "d_centroids_ref", "d_intensities", "d_img", "d_img_raw", "d_validx", "d_validy",
                    "d_weights", "set_nmax", "init_weights", "d_dark", "d_flat", "nslopes"],
@@ -32,7 +38,7 @@ API = {
                           "d_com_clipped", "d_voltage", "d_cmat", "d_centroids"],
     "Rtc_FFF": ["add_centroider", "add_controller", "remove_controller", "remove_centroider", "do_calibrate_img",
                 "do_centroids", "do_control", "comp_voltage", "apply_control", "do_clipping", "set_gain",
-                "set_modal_gains", "imat_svd", "build_cmat", "set_centroids_ref"],
+                "set_modal_gains", "imat_svd", "build_cmat", "set_centroids_ref", "do_imat"],
 }
 
 

@@ -244,3 +244,16 @@ def test_pyramid_tilt_response_is_linear_and_signed(pyr16):
     (sx1, sy1), (sx2, sy2) = out
     assert abs(sx1) > 1e-3 and abs(sx2 / sx1 - 2) < 0.1
     assert abs(sy1) < 0.05 * abs(sx1) and abs(sy2) < 0.05 * abs(sx2)
+
+
+def test_pyramid_threaded_image_equals_sequential(pyr16):
+    """The multi-threaded baseline path (scipy.fft, modulation points batched) forms
+    the same image as the point-by-point numpy.fft path."""
+    from oracle import pyr as opyr
+
+    g = pyr16
+    n = g.tel.n
+    ph = np.random.default_rng(5).standard_normal((n, n)) * 0.05
+    a = opyr.comp_image(ph, g.tel.mpupil, g, g.wavelength_um, g.nphotons)
+    b = opyr.comp_image(ph, g.tel.mpupil, g, g.wavelength_um, g.nphotons, workers=4)
+    np.testing.assert_allclose(b, a, rtol=1e-10, atol=1e-9 * a.max())
