@@ -13,12 +13,21 @@ Two measurements:
 
 * ``command_errors`` -- the relative error ||c_p - c_64|| / ||c_64|| of the
   command of one MVM, for slope vectors taken from the closed loop;
-* ``closed_loop`` -- the same seeded closed loop (turbulence, photon and
-  readout noise, the sensor in float32) run once per reconstruction: the
-  float64 host reconstruction, then the device MVM in each precision.  It
-  reports the time-averaged residual-wavefront rms on the target and the
-  long-exposure Strehl (sinc fit), so the relative residual-rms change of each
-  precision is stated against the float64 loop.
+* ``closed_loop`` -- the same seeded closed loop (turbulence, the sensor in
+  float32) run once per reconstruction: the float64 host reconstruction, then
+  the device MVM in each precision.  It reports the time-averaged
+  residual-wavefront rms on the target and the long-exposure Strehl (sinc
+  fit), so the relative residual-rms change of each precision is stated
+  against the float64 loop.
+
+The comparison is made noise-free, where two loops that differ only by the
+rounding of their commands stay on neighbouring trajectories.  With photon
+noise they do not: a Poisson draw is a step function of the pixel's mean, so
+a change in the last bit of one command (even rounding the float64 command
+matrix to float32) selects other counts in some pixel within a few frames,
+and from there the two loops see different noise.  With noise the study
+therefore compares statistics of whole runs (mean residual, long-exposure
+Strehl), not trajectories.
 """
 
 from __future__ import annotations
@@ -85,14 +94,15 @@ class LoopRun:
         return float(np.mean(self.residual[nskip:]))
 
 
-def closed_loop(cfg, cmat32, recon, niter, nskip, cmat64=None, sample_every=0, device=0):
+def closed_loop(cfg, cmat32, recon, niter, nskip, cmat64=None, sample_every=0, device=0, noise=True):
     """One seeded closed loop of ``niter`` iterations with the given command matrix.
 
     ``recon``: "fp64" (slopes read back, the integrator evaluated on the host
     in float64 with ``cmat64``, the command written back; every
     ``sample_every``-th slope vector is kept) or a device precision "f32" /
     "bf16" / "fp8" (the loop's own MVM).  The long-exposure image is
-    accumulated from iteration ``nskip`` on.
+    accumulated from iteration ``nskip`` on; ``noise``: the sensor's photon and
+    readout noise on or off.
     """
     sy = S.ShAoSystem(cfg, device)
     sy.ls.set_cmat(cmat32)
@@ -117,7 +127,7 @@ def closed_loop(cfg, cmat32, recon, niter, nskip, cmat64=None, sample_every=0, d
             sy.atmos.move()
             sy.trace_target()
             sy.trace_wfs()
-            sy.wfs.comp_image(True)
+            sy.wfs.comp_image(noise)
             sy.centro.get_cog(cen.ptr)
             s = np.array(cen, dtype=np.float64)
             com -= gain * (cmat64 @ s)
@@ -129,7 +139,7 @@ def closed_loop(cfg, cmat32, recon, niter, nskip, cmat64=None, sample_every=0, d
             if sample_every and it % sample_every == 0:
                 run.slopes.append(s.astype(np.float32))
         else:
-            sy.next(compute_psf=True, noise=True)
+            sy.next(compute_psf=True, noise=noise)
         res[it] = sy.residual_rms()
     run.seconds = time.perf_counter() - t0
     run.strehl_le = sy.target.strehl(fit=True)[1]
@@ -137,10 +147,11 @@ def closed_loop(cfg, cmat32, recon, niter, nskip, cmat64=None, sample_every=0, d
     return run
 
 
-def study(cfg=None, niter=1000, nskip=200, precisions=("f32", "bf16", "fp8"), sample_every=50, device=0):
+def study(cfg=None, niter=1000, nskip=200, precisions=("f32", "bf16", "fp8"), sample_every=50, device=0,
+          noise_modes=(False, True)):
     """Calibrate ``cfg`` (push-pull imat in one batch, float64 inverse on the
-    device), then the command errors and the closed loops.  Returns a dict of
-    plain numbers."""
+    device), then the command errors and, for each entry of ``noise_modes``,
+    the closed loops.  Returns a dict of plain numbers."""
     cfg = cfg or S.saxo40()
     t0 = time.perf_counter()
     sy = S.ShAoSystem(cfg, device)
@@ -151,22 +162,30 @@ def study(cfg=None, niter=1000, nskip=200, precisions=("f32", "bf16", "fp8"), sa
     cmat_err = float(np.linalg.norm(cmat32 - cmat64) / np.linalg.norm(cmat64))
     nfilt, nslope, nactu = sy.nfilt, sy.ls.nslope, sy.nactu
     del sy
-    runs = {"fp64": closed_loop(cfg, cmat32, "fp64", niter, nskip, cmat64=cmat64, sample_every=sample_every,
-                                device=device)}
-    for p in precisions:
-        runs[p] = closed_loop(cfg, cmat32, p, niter, nskip, device=device)
-    cerr = command_errors(cmat32, cmat64, runs["fp64"].slopes, precisions, device=device)
-    r64 = runs["fp64"].mean_residual(nskip)
     out = dict(nslope=nslope, nactu=nactu, nfilt=nfilt, niter=niter, nskip=nskip, calib_s=round(t_cal, 3),
-               cmat_f32_vs_fp64=cmat_err, nsamples=len(runs["fp64"].slopes),
-               fp64=dict(residual_rms_um=r64, strehl_le=runs["fp64"].strehl_le,
-                         strehl_le_peak=runs["fp64"].strehl_le_peak))
-    for p in precisions:
-        r = runs[p]
-        rp = r.mean_residual(nskip)
-        d = r.residual[nskip:] - runs["fp64"].residual[nskip:]
-        out[p] = dict(command_rel_err_median=float(np.median(cerr[p])), command_rel_err_max=float(np.max(cerr[p])),
-                      residual_rms_um=rp, residual_rel_change=(rp - r64) / r64,
-                      residual_per_iter_rel_rms=float(np.sqrt(np.mean(d**2)) / r64),
-                      strehl_le=r.strehl_le, strehl_le_peak=r.strehl_le_peak, loop_s=round(r.seconds, 3))
+               cmat_f32_vs_fp64=cmat_err)
+    slopes = None
+    for noise in noise_modes:
+        key = "noisy" if noise else "noiseless"
+        runs = {"fp64": closed_loop(cfg, cmat32, "fp64", niter, nskip, cmat64=cmat64, sample_every=sample_every,
+                                    device=device, noise=noise)}
+        for p in precisions:
+            runs[p] = closed_loop(cfg, cmat32, p, niter, nskip, device=device, noise=noise)
+        if noise or slopes is None:
+            slopes = runs["fp64"].slopes  # command errors on the slopes of the noisy loop when it runs
+        r64 = runs["fp64"].mean_residual(nskip)
+        res = dict(fp64=dict(residual_rms_um=r64, strehl_le=runs["fp64"].strehl_le,
+                             strehl_le_peak=runs["fp64"].strehl_le_peak, loop_s=round(runs["fp64"].seconds, 3)))
+        for p in precisions:
+            r = runs[p]
+            rp = r.mean_residual(nskip)
+            d = r.residual[nskip:] - runs["fp64"].residual[nskip:]
+            res[p] = dict(residual_rms_um=rp, residual_rel_change=(rp - r64) / r64,
+                          residual_per_iter_rel_rms=float(np.sqrt(np.mean(d**2)) / r64),
+                          strehl_le=r.strehl_le, strehl_le_peak=r.strehl_le_peak, loop_s=round(r.seconds, 3))
+        out[key] = res
+    cerr = command_errors(cmat32, cmat64, slopes, precisions, device=device)
+    out["nsamples"] = len(slopes)
+    out["command"] = {p: dict(rel_err_median=float(np.median(cerr[p])), rel_err_max=float(np.max(cerr[p])))
+                      for p in precisions}
     return out

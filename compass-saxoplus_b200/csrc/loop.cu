@@ -26,7 +26,7 @@ aob_loop::aob_loop(aob_sh *w, aob_centro *c, aob_ls *l) : wfs(w), centro(c), ls(
   AOB_REQUIRE(c->nvalid == w->nvalid, "loop: centroider nvalid differs from the sensor's");
   AOB_CUDA(cudaSetDevice(w->device));
   d_frame.alloc(1);
-  gbar.alloc(1);
+  gbar.alloc(GRID_WORDS);
   if (c->wfs && c->wfs->fused == c && c->wfs != w) c->wfs->fused = nullptr;
   c->wfs = w;
   w->fused = c;
@@ -257,7 +257,7 @@ int aob_loop_test_wait_expiry(aob_loop *l, uint32_t polls, void *stream) {
     l->test_absent_cta = 0;
     AOB_REQUIRE(l->launch_fused(false, s, false, false), "aob_loop_test_wait_expiry: launch failed");
     // CTA 0 never added its arrival: bring the counter back to a multiple of the grid
-    AOB_CUDA(cudaMemsetAsync(l->gbar.p, 0, sizeof(unsigned long long), s));
+    AOB_CUDA(cudaMemsetAsync(l->gbar.p, 0, sizeof(unsigned long long) * GRID_WORDS, s));
     AOB_CUDA(cudaStreamSynchronize(s));
     return AOB_OK;
   } catch (const std::exception &e) {

@@ -908,7 +908,7 @@ bool aob_mlp::comp_com_fused(aob_ls *ls, float threshold, cudaStream_t s) {
   A.h2 = ih2.p;
   A.y = iy.p;
   if (partial.n < G) partial.alloc(G);
-  if (gbar.n < 1) gbar.alloc(1);
+  if (gbar.n < GRID_WORDS) gbar.alloc(GRID_WORDS);
   A.partial = partial.p;
   A.n1 = per(ph1);
   A.n2 = per(ph2);

@@ -9,10 +9,15 @@ Bounds (stated):
 * cmat (float32 copy) against the host float64 inverse: relative 1e-5;
 * one-MVM command error, relative l2, every sampled closed-loop slope vector:
   f32 1e-5, BF16 1e-2, FP8 (E4M3, row scales) 8e-2;
-* closed loop (same turbulence, same photon/readout noise streams): the
-  time-averaged residual-wavefront rms changes by at most 1e-3 relative for
-  f32, the accuracy contract for floating point; BF16 and FP8 are held to
-  1e-2 and 5e-2 and their measured values are printed.
+* noise-free closed loop (same turbulence): the time-averaged
+  residual-wavefront rms changes by at most 1e-3 relative for f32, the
+  accuracy contract for floating point, and so does its per-iteration
+  difference; BF16 and FP8 are held to 1e-2 and 5e-2 and their measured values
+  are printed;
+* with photon and readout noise, the loops of different precisions see
+  different noise after a few frames (a Poisson draw is a step function of
+  the pixel's mean), so only run statistics are compared: the long-exposure
+  Strehl at 1.65 um within 1 % of the float64 loop's.
 """
 
 import numpy as np
@@ -40,18 +45,28 @@ def test_cmat_matches_host_fp64(result):
 
 @pytest.mark.parametrize("prec,tol", [("f32", 1e-5), ("bf16", 1e-2), ("fp8", 8e-2)])
 def test_command_error_vs_fp64(result, prec, tol):
-    r = result[prec]
-    print(f"{prec}: command rel err median {r['command_rel_err_median']:.3e} max {r['command_rel_err_max']:.3e}")
+    r = result["command"][prec]
+    print(f"{prec}: command rel err median {r['rel_err_median']:.3e} max {r['rel_err_max']:.3e}")
     assert result["nsamples"] >= 10
-    assert r["command_rel_err_max"] < tol
+    assert r["rel_err_max"] < tol
 
 
 @pytest.mark.parametrize("prec,tol", [("f32", 1e-3), ("bf16", 1e-2), ("fp8", 5e-2)])
-def test_closed_loop_residual_vs_fp64(result, prec, tol):
-    r, r64 = result[prec], result["fp64"]
-    print(f"{prec}: residual {r['residual_rms_um']:.5f} um vs fp64 {r64['residual_rms_um']:.5f} "
-          f"(rel {r['residual_rel_change']:+.2e}), LE SR {r['strehl_le']:.4f} vs {r64['strehl_le']:.4f}")
+def test_noiseless_closed_loop_residual_vs_fp64(result, prec, tol):
+    r, r64 = result["noiseless"][prec], result["noiseless"]["fp64"]
+    print(f"noiseless {prec}: residual {r['residual_rms_um']:.6f} um vs fp64 {r64['residual_rms_um']:.6f} "
+          f"(rel {r['residual_rel_change']:+.2e}, per iteration {r['residual_per_iter_rel_rms']:.2e}), "
+          f"LE SR {r['strehl_le']:.4f} vs {r64['strehl_le']:.4f}")
     # the loop is closed: the residual is a fraction of the open-loop turbulence
     assert 0.0 < r64["residual_rms_um"] < 0.3
     assert r64["strehl_le"] > 0.3
     assert abs(r["residual_rel_change"]) < tol
+    assert r["residual_per_iter_rel_rms"] < tol
+
+
+@pytest.mark.parametrize("prec", ["f32", "bf16", "fp8"])
+def test_noisy_closed_loop_strehl_vs_fp64(result, prec):
+    r, r64 = result["noisy"][prec], result["noisy"]["fp64"]
+    print(f"noisy {prec}: residual {r['residual_rms_um']:.5f} um vs fp64 {r64['residual_rms_um']:.5f}, "
+          f"LE SR {r['strehl_le']:.4f} vs {r64['strehl_le']:.4f}")
+    assert abs(r["strehl_le"] - r64["strehl_le"]) < 0.01 * r64["strehl_le"]
