@@ -27,7 +27,9 @@ modulation points over 512 x 512 FFTs, slopes and a 1600-actuator LS MVM),
 ``mlp`` (the learned reconstructor: batch-1 inference against the LS MVM and
 training throughput on the tensor cores), ``precision`` (the saxo40 closed
 loop with its own LS command matrix: command error and residual-wavefront rms
-of the F32 / BF16 / FP8 MVM against a float64 reconstruction).
+of the F32 / BF16 / FP8 MVM against a float64 reconstruction), ``c4`` (the learned
+reconstructor trained at the saxo40 geometry on closed-loop pairs over r0 0.08-0.20 m
+and magnitudes 6-10, then its closed-loop long-exposure Strehl against LS).
 
 --impl reference runs the reference's own implementation of the path, its
 sutra CUDA code built from its sources into oracle/_ref (oracle/build_ref.py),
@@ -541,11 +543,90 @@ def run_precision(args, torch):
     return 0
 
 
+def run_c4(args, torch):
+    """The learned reconstructor at its configured scale: the saxo40 geometry, pairs of
+    (noisy slopes, DM-projected residual phase) from closed LS loops at r0 0.08-0.20 m and
+    guide-star magnitudes 6-10, trained on the GPU by the project's kernels, then the
+    closed loop of each reconstructor on the same held-out seeded turbulence (r0 0.14 m,
+    magnitude 8): long-exposure Strehl at 1.65 um (sinc fit) and residual rms."""
+    import dataclasses
+
+    from aob200 import mlp as M
+    from aob200 import system as S
+
+    t0 = time.perf_counter()
+    base = S.saxo40()
+    cal = S.ShAoSystem(base)
+    cal.calibrate()
+    cmat, imat = cal.cmat, cal.imat
+    P, mask = M.dm_projector(cal)
+    del cal
+    systems = []
+    for j, r0 in enumerate((0.08, 0.11, 0.14, 0.17, 0.20)):
+        sy = S.ShAoSystem(dataclasses.replace(base, r0=r0, seeds=(500 + 3 * j, 501 + 3 * j, 502 + 3 * j)))
+        sy.imat = imat
+        sy.ls.set_cmat(cmat)
+        sy.close(graph=False)
+        systems.append(sy)
+    t_setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    X, T = M.collect_closed_loop(systems, args.pairs, P, mask, seed=3)
+    t_pairs = time.perf_counter() - t0
+    del systems
+    n = X.shape[0]
+    ntr = int(0.95 * n)
+    net = M.MlpReconstructor(X.shape[1], T.shape[1], 1024, 1024, seed=1)
+    net.set_gemm(1)
+    net.init_from_ls(cmat, 1.0 / float(X[:ntr].std()), float(T[:ntr].std()))
+    t0 = time.perf_counter()
+    hist = net.fit(X[:ntr], T[:ntr], epochs=args.epochs, batch=1024, lr=2e-4, lr_decay=0.8, scales_from_data=False)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    Y = torch.zeros((n - ntr, T.shape[1]), device="cuda")
+    net.forward(X[ntr:].data_ptr(), n - ntr, Y.data_ptr())
+    torch.cuda.synchronize()
+    Tv = T[ntr:].double()
+    ct = torch.as_tensor(np.asarray(cmat, np.float32), device="cuda")
+    err_mlp = float(torch.linalg.norm(Y.double() - Tv) / torch.linalg.norm(Tv))
+    err_ls = float(torch.linalg.norm((X[ntr:] @ ct.T).double() - Tv) / torch.linalg.norm(Tv))
+
+    def closed(mlp=None):
+        sy = S.ShAoSystem(base)
+        sy.ls.set_cmat(cmat)
+        sy.close(graph=False)
+        for _ in range(args.settle):
+            sy.next(compute_psf=False, mlp=mlp, threshold=np.inf)
+        sy.target.reset_le()
+        res = []
+        for _ in range(args.loop_iters):
+            sy.next(mlp=mlp, threshold=np.inf)
+            res.append(sy.residual_rms())
+        return sy.target.strehl(fit=True)[1], float(np.mean(res))
+
+    sr_ls, res_ls = closed()
+    sr_mlp, res_mlp = closed(net)
+    print(json.dumps({"workload": "c4", "metric": "long-exposure Strehl at 1.65 um, learned vs LS reconstructor "
+                      "(closed loop, same seeded turbulence)", "value": sr_mlp, "unit": "Strehl",
+                      "ls_value": sr_ls, "rel_diff": (sr_mlp - sr_ls) / sr_ls,
+                      "residual_rms_um": {"mlp": res_mlp, "ls": res_ls},
+                      "heldout_rel_err": {"mlp": err_mlp, "ls": err_ls},
+                      "dtype": "bf16 weights, f32 accumulation", "data": "synthetic",
+                      "config": {"workload": "c4: saxo40 geometry, MLP 2496 -> 1024 -> 1024 (GELU) -> 1352 + linear "
+                                 "skip initialised to the LS matrix; pairs from closed LS loops at r0 0.08-0.20 m and "
+                                 "magnitudes 6-10; evaluation at r0 0.14 m, magnitude 8, held-out seeds",
+                                 "pairs": n, "train_pairs": ntr, "epochs": args.epochs,
+                                 "loop_iterations": args.loop_iters},
+                      "seconds": {"setup": round(t_setup, 1), "pairs": round(t_pairs, 1), "train": round(t_train, 1)},
+                      "loss_per_epoch": hist}))
+    return 0
+
+
 def run_secondary(args):
     import torch
 
     torch.cuda.set_device(0)
-    fn = {"mc64": run_mc64, "pyr50": run_pyr50, "mlp": run_mlp, "precision": run_precision}[args.workload]
+    fn = {"mc64": run_mc64, "pyr50": run_pyr50, "mlp": run_mlp, "precision": run_precision,
+          "c4": run_c4}[args.workload]
     return fn(args, torch) or 0
 
 
@@ -558,8 +639,11 @@ def main():
     ap.add_argument("--precision", default="f32", choices=["f32", "bf16", "fp8"])
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="saxo40", choices=["saxo40", "mc64", "pyr50", "mlp", "precision"])
-    ap.add_argument("--loop-iters", type=int, default=5000, help="precision: closed-loop iterations per run")
+    ap.add_argument("--workload", default="saxo40", choices=["saxo40", "mc64", "pyr50", "mlp", "precision", "c4"])
+    ap.add_argument("--loop-iters", type=int, default=5000, help="precision, c4: closed-loop iterations per run")
+    ap.add_argument("--pairs", type=int, default=200000, help="c4: training pairs")
+    ap.add_argument("--epochs", type=int, default=8, help="c4: training epochs")
+    ap.add_argument("--settle", type=int, default=100, help="c4: closed-loop iterations before the long exposure")
     ap.add_argument("--instances", type=int, default=64, help="mc64: number of instances (the first N of the list)")
     ap.add_argument("--no-tune", action="store_true", help="mc64: fixed tile shapes instead of the autotuner")
     args = ap.parse_args()

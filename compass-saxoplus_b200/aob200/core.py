@@ -62,6 +62,17 @@ class DeviceArray:
     def get_dims(self):
         return self.shape
 
+    @property
+    def __cuda_array_interface__(self):
+        """The buffer as a CUDA array (Fortran order, no copy), e.g. for
+        ``torch.as_tensor(buf, device="cuda")``."""
+        st, acc = [], self.dtype.itemsize
+        for d in self.shape:
+            st.append(acc)
+            acc *= int(d)
+        return {"shape": tuple(int(d) for d in self.shape), "typestr": self.dtype.str, "data": (self.ptr, False),
+                "strides": tuple(st), "version": 3}
+
 
 class OwnedDeviceArray(DeviceArray):
     """A device buffer allocated here (aob_malloc) and freed with the object."""

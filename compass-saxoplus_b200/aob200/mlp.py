@@ -172,7 +172,11 @@ def dm_projector(sys, maxcond=None, rcond=1e-2):
     maxcond = sys.cfg.maxcond if maxcond is None else maxcond
     _, S, Vt = np.linalg.svd(np.asarray(sys.imat, np.float64), full_matrices=False)
     Vk = Vt[S >= S.max() / maxcond].T
-    Fp = np.linalg.pinv(F, rcond=rcond)
+    # F^+ through the normal equations (F has many more pupil pixels than
+    # actuators): F^T F = V diag(s^2) V^T, singular values below rcond * max dropped
+    ev, V = np.linalg.eigh(F.T @ F)
+    keep = ev >= (rcond**2) * ev.max()
+    Fp = (V[:, keep] / ev[keep]) @ (V[:, keep].T @ F.T)
     return Vk @ (Vk.T @ Fp), mask
 
 
@@ -212,4 +216,53 @@ def collect_open_loop(sys, nsamples, projector, mask, strengths=(0.5, 1.0, 1.5, 
         X[i] = np.array(d)
         v = ph.ravel(order="F")[mask].astype(np.float64)
         T[i] = (projector @ (v - v.mean())).astype(np.float32)
+    return X, T
+
+
+def collect_closed_loop(systems, nsamples, projector, mask, mags=(6.0, 10.0), segment=100, settle=20, seed=0,
+                        batch=256):
+    """(slopes, DM-projected residual phase) pairs from closed LS loops, on the
+    device (torch tensors X [n][nslope], T [n][nactu]).
+
+    ``systems``: closed ShAoSystem loops of one geometry at several turbulence
+    strengths; the pairs cycle through them in segments of ``segment`` steps,
+    each segment at a guide-star magnitude drawn uniformly in ``mags`` (the
+    photon count scaled from the geometry's, the wCoG threshold kept).  At
+    every step the sensor's phase is the residual its slopes measure; the
+    target is the command vector whose DM shape best fits it (``projector``,
+    applied on the device in batches)."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    s0 = systems[0]
+    nslope, nactu = s0.ls.nslope, s0.nactu
+    X = torch.empty((nsamples, nslope), device="cuda", dtype=torch.float32)
+    T = torch.empty((nsamples, nactu), device="cuda", dtype=torch.float32)
+    Pt = torch.as_tensor(np.asarray(projector, np.float32), device="cuda")
+    idx = torch.as_tensor(np.flatnonzero(mask), device="cuda", dtype=torch.int64)
+    PH = torch.empty((batch, idx.numel()), device="cuda", dtype=torch.float32)
+    for sy in systems:
+        for _ in range(settle):
+            sy.next(compute_psf=False)
+    views = [(torch.as_tensor(sy.ls.buffer("centroids"), device="cuda"),
+              torch.as_tensor(sy.wfs.buffer("phase"), device="cuda")) for sy in systems]
+    nph0 = [sy.geom.nphotons for sy in systems]
+    i, j0, seg = 0, 0, 0
+    while i < nsamples:
+        k = seg % len(systems)
+        sy = systems[k]
+        sy.wfs.set_nphot(nph0[k] * 10.0 ** (-0.4 * (rng.uniform(*mags) - 8.0)))
+        cen, ph = views[k]
+        for _ in range(min(segment, nsamples - i)):
+            sy.next(compute_psf=False)
+            X[i].copy_(cen)
+            v = ph.index_select(0, idx)
+            PH[i - j0].copy_(v - v.mean())
+            i += 1
+            if i - j0 == batch or i == nsamples:
+                T[j0:i] = PH[: i - j0] @ Pt.T
+                j0 = i
+        sy.wfs.set_nphot(nph0[k])
+        seg += 1
+    torch.cuda.synchronize()
     return X, T

@@ -543,7 +543,7 @@ void aob_batch::build(bool noise) {
     AOB_CUDA(cudaMemcpy(d_inst[v].p, t.data(), sizeof(BatchInst) * n, cudaMemcpyHostToDevice));
   }
   auto kern = cps <= 2 ? batch_step_kernel<2> : batch_step_kernel<4>;
-  AOB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  smem_opt_in(reinterpret_cast<const void *>(kern), (int)smem);  // only ever raised, per device
   int per_sm = 0;
   AOB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BATCH_THREADS, smem));
   AOB_REQUIRE(per_sm >= 1, "batch: the kernel does not fit on an SM");

@@ -930,7 +930,9 @@ bool aob_mlp::comp_com_fused(aob_ls *ls, float threshold, cudaStream_t s) {
   const MlpFusedSmem L(pin, ph1, ph2, A.n1, A.n2, A.n3, A.nls, swizzled_slope_floats(ld_ls, V));
   if (L.bytes > 227 * 1024 || A.nls > MLP_FUSED_THREADS) return false;
   auto launch = [&](auto kern) {
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes) != cudaSuccess) {
+    try {
+      smem_opt_in(reinterpret_cast<const void *>(kern), (int)L.bytes);  // only ever raised, per device
+    } catch (const std::exception &) {
       cudaGetLastError();
       return false;
     }

@@ -182,76 +182,86 @@ __global__ void __launch_bounds__(PYR_THREADS) pyr_accum_kernel(PyrArgs A) {
   }
 }
 
-// 4. pixel transfer function: PYR_SEQ rows of hrimg (real), inverse transform along x.
-template <int N>
-__global__ void __launch_bounds__(PYR_THREADS) pyr_conv_rows_kernel(PyrArgs A) {
+// The single-image tails below (pixel-transfer convolution and binning) take
+// TSEQ sequences per CTA on TSEQ * 64 threads, so one image spreads over
+// N / TSEQ CTAs (256 at N = 512, TSEQ = 2) instead of N / PYR_SEQ; each
+// sequence's transform is the same whatever the CTA shape.
+// 4. pixel transfer function: TSEQ rows of hrimg (real), inverse transform along x.
+template <int N, int TSEQ>
+__global__ void __launch_bounds__(TSEQ * 64) pyr_conv_rows_kernel(PyrArgs A) {
+  constexpr int NT = TSEQ * 64;
   extern __shared__ float2 sm[];
-  float2 *tws = pyr_load_twiddles<N>(sm, A.tw);
-  const int y0 = blockIdx.x * PYR_SEQ;
-  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+  float2 *tws = sm + N * TSEQ;
+  for (int i = threadIdx.x; i < N / 2; i += NT) tws[i] = A.tw[i];
+  const int y0 = blockIdx.x * TSEQ;
+  for (int t = threadIdx.x; t < N * TSEQ; t += NT) {
     const int c = t / N, i = t - c * N;
-    sm[i * PYR_SEQ + c] = make_float2(A.hrimg[(size_t)(y0 + c) * N + i], 0.f);
+    sm[i * TSEQ + c] = make_float2(A.hrimg[(size_t)(y0 + c) * N + i], 0.f);
   }
   __syncthreads();
-  fft_ct<N, PYR_SEQ, PYR_THREADS>(sm, tws, true);
-  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+  fft_ct<N, TSEQ, NT>(sm, tws, true);
+  for (int t = threadIdx.x; t < N * TSEQ; t += NT) {
     const int c = t / N, i = t - c * N;
-    A.conv[(size_t)(y0 + c) * N + i] = sm[i * PYR_SEQ + c];
+    A.conv[(size_t)(y0 + c) * N + i] = sm[i * TSEQ + c];
   }
 }
 
 // 5. columns: inverse transform along y, x sinc, forward transform along y.
-template <int N>
-__global__ void __launch_bounds__(PYR_THREADS) pyr_conv_cols_kernel(PyrArgs A) {
+template <int N, int TSEQ>
+__global__ void __launch_bounds__(TSEQ * 64) pyr_conv_cols_kernel(PyrArgs A) {
+  constexpr int NT = TSEQ * 64;
   extern __shared__ float2 sm[];
-  float2 *tws = pyr_load_twiddles<N>(sm, A.tw);
-  const int c0 = blockIdx.x * PYR_SEQ;
+  float2 *tws = sm + N * TSEQ;
+  for (int i = threadIdx.x; i < N / 2; i += NT) tws[i] = A.tw[i];
+  const int c0 = blockIdx.x * TSEQ;
   float2 *base = A.conv + c0;
-  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
-    const int m = t / PYR_SEQ, c = t - m * PYR_SEQ;
+  for (int t = threadIdx.x; t < N * TSEQ; t += NT) {
+    const int m = t / TSEQ, c = t - m * TSEQ;
     sm[t] = base[(size_t)m * N + c];
   }
   __syncthreads();
-  fft_ct<N, PYR_SEQ, PYR_THREADS>(sm, tws, true);
-  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
-    const int m = t / PYR_SEQ, c = t - m * PYR_SEQ;
+  fft_ct<N, TSEQ, NT>(sm, tws, true);
+  for (int t = threadIdx.x; t < N * TSEQ; t += NT) {
+    const int m = t / TSEQ, c = t - m * TSEQ;
     const float msk = A.sincar[(size_t)(c0 + c) + (size_t)m * N];
     const float2 a = sm[t];
     sm[t] = make_float2(a.x * msk, a.y * msk);
   }
   __syncthreads();
-  fft_ct<N, PYR_SEQ, PYR_THREADS>(sm, tws, false);
-  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
-    const int m = t / PYR_SEQ, c = t - m * PYR_SEQ;
+  fft_ct<N, TSEQ, NT>(sm, tws, false);
+  for (int t = threadIdx.x; t < N * TSEQ; t += NT) {
+    const int m = t / TSEQ, c = t - m * TSEQ;
     base[(size_t)m * N + c] = sm[t];
   }
 }
 
-// 6. rows_per_bin_cta (a multiple of nrebin, <= PYR_SEQ) rows per CTA: forward
+// 6. rows_per_bin_cta (a multiple of nrebin, <= TSEQ) rows per CTA: forward
 //    transform along x, real part, binning (pyr_bimg_krnl order: x offset
 //    outer, y offset inner, then / nrebin^2) and the row sums of the binned
 //    image for the normalisation.
-template <int N>
-__global__ void __launch_bounds__(PYR_THREADS) pyr_bin_kernel(PyrArgs A) {
+template <int N, int TSEQ>
+__global__ void __launch_bounds__(TSEQ * 64) pyr_bin_kernel(PyrArgs A) {
+  constexpr int NT = TSEQ * 64;
   extern __shared__ float2 sm[];
-  float2 *tws = pyr_load_twiddles<N>(sm, A.tw);
-  float *real = reinterpret_cast<float *>(tws + N / 2);  // PYR_SEQ x N
+  float2 *tws = sm + N * TSEQ;
+  for (int i = threadIdx.x; i < N / 2; i += NT) tws[i] = A.tw[i];
+  float *real = reinterpret_cast<float *>(tws + N / 2);  // TSEQ x N
   const int rows = A.rows_per_bin_cta;
   const int y0 = blockIdx.x * rows;
-  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+  for (int t = threadIdx.x; t < N * TSEQ; t += NT) {
     const int c = t / N, i = t - c * N;
-    sm[i * PYR_SEQ + c] = c < rows ? A.conv[(size_t)(y0 + c) * N + i] : make_float2(0.f, 0.f);
+    sm[i * TSEQ + c] = c < rows ? A.conv[(size_t)(y0 + c) * N + i] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  fft_ct<N, PYR_SEQ, PYR_THREADS>(sm, tws, false);
-  for (int t = threadIdx.x; t < N * PYR_SEQ; t += PYR_THREADS) {
+  fft_ct<N, TSEQ, NT>(sm, tws, false);
+  for (int t = threadIdx.x; t < N * TSEQ; t += NT) {
     const int c = t / N, i = t - c * N;
-    real[c * N + i] = sm[i * PYR_SEQ + c].x;
+    real[c * N + i] = sm[i * TSEQ + c].x;
   }
   __syncthreads();
   const int nbr = rows / A.nrebin;
   const float div = (float)(A.nrebin * A.nrebin);
-  for (int t = threadIdx.x; t < nbr * A.nb; t += PYR_THREADS) {
+  for (int t = threadIdx.x; t < nbr * A.nb; t += NT) {
     const int br = t / A.nb, bx = t - br * A.nb;
     float o = 0.f;
     for (int ii = 0; ii < A.nrebin; ++ii)
@@ -274,10 +284,12 @@ __global__ void pyr_norm_noise_kernel(float *binimg, const float *partial, int n
   __shared__ float rk[AOB_POISSON_INV_KMAX + 1];
   if (noise_mode >= 1)
     for (int i = threadIdx.x; i <= AOB_POISSON_INV_KMAX; i += blockDim.x) rk[i] = i ? __frcp_rn((float)i) : 0.f;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
+    // the row sums in a fixed order: lane-strided partial sums, then a butterfly
     float s = 0.f;
-    for (int r = 0; r < nb; ++r) s += partial[r];
-    s_fact = nphot / s;
+    for (int r = threadIdx.x; r < nb; r += 32) s += partial[r];
+    s = warp_sum(s);
+    if (threadIdx.x == 0) s_fact = nphot / s;
   }
   __syncthreads();
   const float fact = s_fact;
@@ -303,18 +315,30 @@ __global__ void pyr_focal_sum_kernel(float *focal, const float *work, int npts, 
   }
 }
 
+template <int N, int TSEQ>
+static void pyr_launch_tails(const PyrArgs &A, int nbin_ctas, cudaStream_t s) {
+  const size_t sm = sizeof(float2) * (N * TSEQ + N / 2);
+  const size_t bin_sm = sm + sizeof(float) * N * TSEQ;
+  const int lim = (int)std::max<size_t>(bin_sm, 48 * 1024);
+  smem_opt_in(reinterpret_cast<const void *>(pyr_conv_rows_kernel<N, TSEQ>), lim);
+  smem_opt_in(reinterpret_cast<const void *>(pyr_conv_cols_kernel<N, TSEQ>), lim);
+  smem_opt_in(reinterpret_cast<const void *>(pyr_bin_kernel<N, TSEQ>), lim);
+  pyr_conv_rows_kernel<N, TSEQ><<<N / TSEQ, TSEQ * 64, sm, s>>>(A);
+  AOB_LAUNCH_CHECK("pyr_conv_rows_kernel");
+  pyr_conv_cols_kernel<N, TSEQ><<<N / TSEQ, TSEQ * 64, sm, s>>>(A);
+  AOB_LAUNCH_CHECK("pyr_conv_cols_kernel");
+  pyr_bin_kernel<N, TSEQ><<<nbin_ctas, TSEQ * 64, bin_sm, s>>>(A);
+  AOB_LAUNCH_CHECK("pyr_bin_kernel");
+}
+
 template <int N>
-static void pyr_launch(const PyrArgs &A, int npts, int ntot, int nbin_ctas, cudaStream_t s) {
+static void pyr_launch(const PyrArgs &A, int npts, int ntot, int nrebin, cudaStream_t s) {
   const size_t sm = sizeof(float2) * (N * PYR_SEQ + N / 2);
-  const size_t bin_sm = sm + sizeof(float) * N * PYR_SEQ;
   {
-    const int lim = (int)std::max<size_t>(bin_sm, 48 * 1024);
+    const int lim = (int)std::max<size_t>(sm, 48 * 1024);
     smem_opt_in(reinterpret_cast<const void *>(pyr_rows_kernel<N>), lim);
     smem_opt_in(reinterpret_cast<const void *>(pyr_cols_kernel<N>), lim);
     smem_opt_in(reinterpret_cast<const void *>(pyr_accum_kernel<N>), lim);
-    smem_opt_in(reinterpret_cast<const void *>(pyr_conv_rows_kernel<N>), lim);
-    smem_opt_in(reinterpret_cast<const void *>(pyr_conv_cols_kernel<N>), lim);
-    smem_opt_in(reinterpret_cast<const void *>(pyr_bin_kernel<N>), lim);
   }
   pyr_rows_kernel<N><<<npts * ((ntot + PYR_SEQ - 1) / PYR_SEQ), PYR_THREADS, sm, s>>>(A);
   AOB_LAUNCH_CHECK("pyr_rows_kernel");
@@ -322,12 +346,14 @@ static void pyr_launch(const PyrArgs &A, int npts, int ntot, int nbin_ctas, cuda
   AOB_LAUNCH_CHECK("pyr_cols_kernel");
   pyr_accum_kernel<N><<<N, PYR_THREADS, sm, s>>>(A);
   AOB_LAUNCH_CHECK("pyr_accum_kernel");
-  pyr_conv_rows_kernel<N><<<N / PYR_SEQ, PYR_THREADS, sm, s>>>(A);
-  AOB_LAUNCH_CHECK("pyr_conv_rows_kernel");
-  pyr_conv_cols_kernel<N><<<N / PYR_SEQ, PYR_THREADS, sm, s>>>(A);
-  AOB_LAUNCH_CHECK("pyr_conv_cols_kernel");
-  pyr_bin_kernel<N><<<nbin_ctas, PYR_THREADS, bin_sm, s>>>(A);
-  AOB_LAUNCH_CHECK("pyr_bin_kernel");
+  // tails: as few rows per CTA as the binning allows (rows_per_bin_cta == TSEQ)
+  const int nbin_ctas = N / A.rows_per_bin_cta;
+  if (A.rows_per_bin_cta <= 2)
+    pyr_launch_tails<N, 2>(A, nbin_ctas, s);
+  else if (A.rows_per_bin_cta <= 4)
+    pyr_launch_tails<N, 4>(A, nbin_ctas, s);
+  else
+    pyr_launch_tails<N, 8>(A, nbin_ctas, s);
 }
 
 }  // namespace aob
@@ -341,8 +367,8 @@ aob_pyr::aob_pyr(int device_, int nxsub_, int nvalid_, int npix_, int nphase_, i
   AOB_REQUIRE(nvalid > 0 && nrebin > 0 && ntot > 0 && npts > 0, "pyr: sizes must be > 0");
   AOB_REQUIRE(nfft >= 64 && nfft <= 2048 && (nfft & (nfft - 1)) == 0,
               "pyr: nfft must be a power of two in [64, 2048]");
-  AOB_REQUIRE(nrebin <= PYR_SEQ && nfft % ((PYR_SEQ / nrebin) * nrebin) == 0,
-              "pyr: nrebin must be <= 8 and the binning rows must tile nfft");
+  AOB_REQUIRE(nrebin <= PYR_SEQ && (nrebin & (nrebin - 1)) == 0,
+              "pyr: nrebin must be a power of two <= 8 (the binning rows tile nfft)");
   AOB_REQUIRE(ntot <= nfft, "pyr: the phase grid (ntot) must fit in nfft");
   AOB_REQUIRE(nfft % nrebin == 0, "pyr: nfft must be a multiple of nrebin");
   while ((1 << logn) < nfft) ++logn;
@@ -419,7 +445,8 @@ void aob_pyr::comp_image(bool with_noise, cudaStream_t s) {
   A.partial = partial.p;
   A.nrebin = nrebin;
   A.nb = nbin();
-  A.rows_per_bin_cta = (PYR_SEQ / nrebin) * nrebin;
+  // binning rows per CTA: nrebin, at least 2 (a power of two dividing nfft)
+  A.rows_per_bin_cta = std::max(nrebin, 2);
   const int64_t n2 = (int64_t)nfft * nfft;
   A.focal_work = nullptr;
   if (compute_focalplane) {
@@ -427,14 +454,13 @@ void aob_pyr::comp_image(bool with_noise, cudaStream_t s) {
     if (focalplane.n != n2) focalplane.alloc(n2);
     A.focal_work = focal_work.p;
   }
-  const int nbin_ctas = nfft / A.rows_per_bin_cta;
   switch (nfft) {
-    case 64: pyr_launch<64>(A, npts, ntot, nbin_ctas, s); break;
-    case 128: pyr_launch<128>(A, npts, ntot, nbin_ctas, s); break;
-    case 256: pyr_launch<256>(A, npts, ntot, nbin_ctas, s); break;
-    case 512: pyr_launch<512>(A, npts, ntot, nbin_ctas, s); break;
-    case 1024: pyr_launch<1024>(A, npts, ntot, nbin_ctas, s); break;
-    default: pyr_launch<2048>(A, npts, ntot, nbin_ctas, s); break;
+    case 64: pyr_launch<64>(A, npts, ntot, nrebin, s); break;
+    case 128: pyr_launch<128>(A, npts, ntot, nrebin, s); break;
+    case 256: pyr_launch<256>(A, npts, ntot, nrebin, s); break;
+    case 512: pyr_launch<512>(A, npts, ntot, nrebin, s); break;
+    case 1024: pyr_launch<1024>(A, npts, ntot, nrebin, s); break;
+    default: pyr_launch<2048>(A, npts, ntot, nrebin, s); break;
   }
   if (compute_focalplane) {
     pyr_focal_sum_kernel<<<(int)std::min<int64_t>((n2 + 255) / 256, 8 * num_sms(device)), 256, 0, s>>>(
