@@ -335,10 +335,9 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
 // error word written by kernels whose bounded waits expired
 enum : uint32_t { ERR_MBAR_TIMEOUT = 1u };
 
-// grid-barrier words (mvm_core.cuh): the arrival counter, and at GRID_FLAG
-// (128 bytes further) the flag the last arrival sets; owners allocate GRID_WORDS
-constexpr int GRID_FLAG = 16;
-constexpr int GRID_WORDS = 32;
+// grid-barrier words (mvm_core.cuh) an owner allocates: the arrival counter on
+// a 128-byte line of its own
+constexpr int GRID_WORDS = 16;
 
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float warp_sum(float v) {

@@ -66,15 +66,9 @@ constexpr uint32_t GRID_MAX_POLLS = 1u << 24;
 // CTA's target is the next multiple of G above the value its own arrival saw
 // and nothing has to be reset between launches (every CTA arrives exactly
 // once per barrier, also when a wait times out).  One thread per CTA arrives
-// with an acquire-release add (it publishes the CTA's writes, ordered before
-// it by the CTA barrier).  The CTA whose add completes the count opens the
-// barrier with a release store of the target into a separate flag word,
-// ctr[GRID_FLAG], on its own 128-byte line: the waiters spin on relaxed loads
-// of that line, which is written once per barrier, so their polls do not
-// contend with the arrivals' atomics, and close with one acquire load.  The
-// owner allocates GRID_WORDS words.  The wait is bounded; on expiry
-// ERR_GRID_TIMEOUT is set and false returned.  (GRID_FLAG / GRID_WORDS:
-// aob_common.cuh.)
+// with a release add (it publishes the CTA's writes, ordered before it by the
+// CTA barrier), spins on relaxed loads and closes with one acquire load.  The
+// wait is bounded; on expiry ERR_GRID_TIMEOUT is set and false returned.
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
   unsigned long long v;
   asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
@@ -85,13 +79,10 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
   asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ unsigned long long atom_add_acqrel_u64(unsigned long long *p, unsigned long long v) {
+__device__ __forceinline__ unsigned long long atom_add_release_u64(unsigned long long *p, unsigned long long v) {
   unsigned long long old;
-  asm volatile("atom.add.acq_rel.gpu.global.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  asm volatile("atom.add.release.gpu.global.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
   return old;
-}
-__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 // Arrival half: every thread of the CTA calls it; thread 0 gets the target
 // count to wait for (the others 0).  Work placed between grid_arrive and
@@ -100,10 +91,8 @@ __device__ __forceinline__ unsigned long long grid_arrive(unsigned long long *ct
   __syncthreads();
   unsigned long long target = 0;
   if (threadIdx.x == 0) {
-    const unsigned long long old = atom_add_acqrel_u64(ctr, 1ull);
+    const unsigned long long old = atom_add_release_u64(ctr, 1ull);
     target = (old / nblocks + 1ull) * nblocks;
-    // the last arrival has acquired every other CTA's release: open the barrier
-    if (old + 1ull == target) st_release_u64(ctr + GRID_FLAG, target);
   }
   return target;
 }
@@ -115,15 +104,14 @@ __device__ __forceinline__ bool grid_wait(const unsigned long long *ctr, unsigne
   if (threadIdx.x == 0) {
     int ok = 1;
     uint32_t i = 0;
-    const unsigned long long *flag = ctr + GRID_FLAG;
-    while (ld_relaxed_u64(flag) < target) {
+    while (ld_relaxed_u64(ctr) < target) {
       if (++i >= max_polls) {
         ok = 0;
         atomicOr(status, (uint32_t)ERR_GRID_TIMEOUT);
         break;
       }
     }
-    (void)ld_acquire_u64(flag);  // orders this CTA's later reads after the other CTAs' writes
+    (void)ld_acquire_u64(ctr);  // orders this CTA's later reads after the other CTAs' writes
     s_ok = ok;
   }
   __syncthreads();
