@@ -148,15 +148,22 @@ class MlpReconstructor:
         return hist
 
 
-def dm_projector(sys, maxcond=None, rcond=1e-2):
+def dm_projector(sys, maxcond=None, rcond=1e-2, sensed_only=False):
     """Projector from the sensor's phase grid to DM commands (float64): the
     least-squares DM fit of a pupil phase, F^+ (influence functions F seen by
     the sensor inside the pupil, singular values below rcond * max dropped),
     restricted to the command modes the interaction matrix senses -- the
     right singular vectors of imat kept by the same condition limit as the LS
     inverse -- so that the target holds no component the slopes cannot see
-    (waffle and other unsensed DM patterns)."""
-    mask = (sys.geom.tel.mpupil > 0).ravel(order="F")
+    (waffle and other unsensed DM patterns).  ``sensed_only``: fit only the
+    phase samples inside valid sub-apertures (the sensor's phasemap), not the
+    pupil's edge pixels that no slope sees."""
+    if sensed_only:
+        mask = np.zeros(sys.n * sys.n, bool)
+        mask[np.unique(np.asarray(sys.geom.phasemap).ravel())] = True
+        mask &= (sys.geom.tel.mpupil > 0).ravel(order="F")
+    else:
+        mask = (sys.geom.tel.mpupil > 0).ravel(order="F")
     F = np.zeros((int(mask.sum()), sys.nactu))
     com = np.zeros(sys.nactu, np.float32)
     for a in range(sys.nactu):
