@@ -140,6 +140,7 @@ struct aob_centro {
   int nmax = 0;                 // bpcog: rank of the threshold pixel (set_nmax)
   aob::DevBuf<int32_t> validx, validy;
   aob::DevBuf<float> ref, weights, intensities;
+  aob::DevBuf<float> pyr_partial;  // pyramid slopes: per-CTA flux sums
   int weights_per_sub = 0;  // 0: one npix^2 map, 1: npix^2*nvalid
   // image path when not attached to a sensor (load_img + calibrate_img)
   int img_m = 0, img_n = 0;

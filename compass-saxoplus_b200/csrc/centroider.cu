@@ -89,76 +89,70 @@ __global__ void tcog_writeback_kernel(float *img, int size, const int32_t *valid
 // sub-aperture is normalised by the mean flux (fillvalues, carma_obj.cu:194-201);
 // the sum runs in a fixed order (per-thread partial sums, then a tree), so
 // the slopes are deterministic.  One CTA.
-constexpr int PYR_SLOPE_THREADS = 1024;
-constexpr int PYR_SLOPE_REG = 4;  // sub-apertures per thread kept in registers
+// Pyramid slopes over the whole GPU in two launches: per-CTA sums of the
+// sub-aperture fluxes (the intensities written as they are formed), then every
+// CTA adds the CTA sums in a fixed order for the global mean and emits the
+// slopes of its sub-apertures (the reference's Method_CoG(uint8_t),
+// sutra_centroider_pyr.hpp:27-34: 0 sinus global, 1 nosinus global, 2 sinus
+// local, 3 nosinus local; pyr2slopes_krnl, sutra_centroider_pyr.cu:27-69).
+constexpr int PYR_SLOPE_THREADS = 256;
+__device__ __forceinline__ void pyr_quad(const float *img, int ns, const int32_t *vx, const int32_t *vy, int nvalid,
+                                         int i, float *q) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) q[k] = img[vx[i + k * nvalid] + vy[i + k * nvalid] * ns];
+}
+__global__ void __launch_bounds__(PYR_SLOPE_THREADS)
+    pyr_flux_kernel(const float *img, int ns, const int32_t *vx, const int32_t *vy, int nvalid, float *inten,
+                    float *partial) {
+  __shared__ float red[PYR_SLOPE_THREADS / 32];
+  const int i = blockIdx.x * PYR_SLOPE_THREADS + threadIdx.x;
+  float f = 0.f;
+  if (i < nvalid) {
+    float q[4];
+    pyr_quad(img, ns, vx, vy, nvalid, i, q);
+    f = q[0] + q[1] + q[2] + q[3];
+    inten[i] = f;
+  }
+  f = warp_sum(f);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = f;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.f;
+    for (int w = 0; w < PYR_SLOPE_THREADS / 32; ++w) t += red[w];
+    partial[blockIdx.x] = t;
+  }
+}
 __global__ void __launch_bounds__(PYR_SLOPE_THREADS)
     pyr_slopes_kernel(const float *img, int ns, const int32_t *vx, const int32_t *vy, int nvalid, float scale,
-                      float thresh, int method, const float *ref, int order, float *slopes, float *inten) {
-  __shared__ float red[PYR_SLOPE_THREADS];
-  // the reference's Method_CoG(uint8_t) (sutra_centroider_pyr.hpp:27-34): 0 sinus global,
-  // 1 nosinus global, 2 sinus local, 3 nosinus local
+                      float thresh, int method, const float *ref, int order, const float *partial, int nparts,
+                      float *slopes, float *inten) {
+  __shared__ float s_mean;
   const bool sinus = (method & 1) == 0, local = method > 1;
-  auto quad = [&](int i, float *q) {
-#pragma unroll
-    for (int k = 0; k < 4; ++k) q[k] = img[vx[i + k * nvalid] + vy[i + k * nvalid] * ns];
-  };
-  // quadrant pixels of this thread's sub-apertures: gathered once (all loads
-  // issued before use) and kept in registers for the slope pass
-  float qr[PYR_SLOPE_REG][4];
-#pragma unroll
-  for (int it = 0; it < PYR_SLOPE_REG; ++it) {
-    const int i = threadIdx.x + it * blockDim.x;
-    if (i < nvalid) quad(i, qr[it]);
+  if (threadIdx.x < 32) {
+    float t = 0.f;
+    for (int b = threadIdx.x; b < nparts; b += 32) t += partial[b];
+    t = warp_sum(t);
+    if (threadIdx.x == 0) s_mean = t / (float)nvalid;
   }
-  float part = 0.f;
-#pragma unroll
-  for (int it = 0; it < PYR_SLOPE_REG; ++it) {
-    const int i = threadIdx.x + it * blockDim.x;
-    if (i < nvalid) {
-      const float f = qr[it][0] + qr[it][1] + qr[it][2] + qr[it][3];
-      inten[i] = f;
-      part += f;
-    }
-  }
-  for (int i = threadIdx.x + PYR_SLOPE_REG * blockDim.x; i < nvalid; i += blockDim.x) {
-    float q[4];
-    quad(i, q);
-    const float f = q[0] + q[1] + q[2] + q[3];
-    inten[i] = f;
-    part += f;
-  }
-  red[threadIdx.x] = part;
+  const int i = blockIdx.x * PYR_SLOPE_THREADS + threadIdx.x;
+  float q[4];
+  if (i < nvalid) pyr_quad(img, ns, vx, vy, nvalid, i, q);
   __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-    __syncthreads();
+  if (i >= nvalid) return;
+  const float mean = s_mean;
+  const float f = local ? inten[i] : mean;
+  const int ix = order ? 2 * i : i;
+  const int iy = order ? 2 * i + 1 : i + nvalid;
+  float sx = 0.f, sy = 0.f;
+  if (!(f < thresh)) {
+    const float tx = ((q[0] + q[3]) - (q[1] + q[2])) / f;
+    const float ty = ((q[0] + q[2]) - (q[1] + q[3])) / f;
+    sx = sinus ? scale * sinpif(tx / 2.f) : scale * tx;
+    sy = sinus ? scale * sinpif(ty / 2.f) : scale * ty;
   }
-  const float mean = red[0] / (float)nvalid;
-  auto emit = [&](int i, const float *q) {
-    const float f = local ? inten[i] : mean;
-    const int ix = order ? 2 * i : i;
-    const int iy = order ? 2 * i + 1 : i + nvalid;
-    float sx = 0.f, sy = 0.f;
-    if (!(f < thresh)) {
-      const float tx = ((q[0] + q[3]) - (q[1] + q[2])) / f;
-      const float ty = ((q[0] + q[2]) - (q[1] + q[3])) / f;
-      sx = sinus ? scale * sinpif(tx / 2.f) : scale * tx;
-      sy = sinus ? scale * sinpif(ty / 2.f) : scale * ty;
-    }
-    slopes[ix] = sx - ref[ix];
-    slopes[iy] = sy - ref[iy];
-    if (!local) inten[i] = mean;
-  };
-#pragma unroll
-  for (int it = 0; it < PYR_SLOPE_REG; ++it) {
-    const int i = threadIdx.x + it * blockDim.x;
-    if (i < nvalid) emit(i, qr[it]);
-  }
-  for (int i = threadIdx.x + PYR_SLOPE_REG * blockDim.x; i < nvalid; i += blockDim.x) {
-    float q[4];
-    quad(i, q);
-    emit(i, q);
-  }
+  slopes[ix] = sx - ref[ix];
+  slopes[iy] = sy - ref[iy];
+  if (!local) inten[i] = mean;
 }
 
 // Masked-pixel slopes (get_maskedPix_krnl, libsutra/src.cu/sutra_centroider_maskedPix.cu:26-38,
@@ -424,8 +418,14 @@ void aob_centro::get_cog(float *dev_slopes, cudaStream_t s) {
       ns = img_m;
     }
     AOB_CUDA(cudaSetDevice(device));
-    pyr_slopes_kernel<<<1, PYR_SLOPE_THREADS, 0, s>>>(im, ns, validx.p, validy.p, nvalid, scale, valid_thresh, pyr_method,
-                                                      ref.p, order, dev_slopes, intensities.p);
+    const int nparts = (nvalid + PYR_SLOPE_THREADS - 1) / PYR_SLOPE_THREADS;
+    if (pyr_partial.n < nparts) pyr_partial.alloc(nparts);
+    pyr_flux_kernel<<<nparts, PYR_SLOPE_THREADS, 0, s>>>(im, ns, validx.p, validy.p, nvalid, intensities.p,
+                                                        pyr_partial.p);
+    AOB_LAUNCH_CHECK("pyr_flux_kernel");
+    pyr_slopes_kernel<<<nparts, PYR_SLOPE_THREADS, 0, s>>>(im, ns, validx.p, validy.p, nvalid, scale, valid_thresh,
+                                                          pyr_method, ref.p, order, pyr_partial.p, nparts, dev_slopes,
+                                                          intensities.p);
     AOB_LAUNCH_CHECK("pyr_slopes_kernel");
     return;
   }
