@@ -544,106 +544,24 @@ def run_precision(args, torch):
 
 
 def run_c4(args, torch):
-    """The learned reconstructor at its configured scale: the saxo40 geometry, pairs of
-    (noisy slopes, DM-projected residual phase) from closed LS loops at r0 0.08-0.20 m and
-    guide-star magnitudes 6-10, trained on the GPU by the project's kernels, then the
-    closed loop of each reconstructor on the same held-out seeded turbulence (r0 0.14 m,
-    magnitude 8): long-exposure Strehl at 1.65 um (sinc fit) and residual rms."""
-    import dataclasses
+    """The learned reconstructor at its configured scale (aob200.learned.c4_experiment):
+    the saxo40 geometry, closed-loop training pairs over r0 0.08-0.20 m and magnitudes
+    6-10, training on the GPU, the output gain chosen on a validation loop, then the
+    long-exposure Strehl of both reconstructors on the held-out loop."""
+    from aob200 import learned
 
-    from aob200 import mlp as M
-    from aob200 import system as S
-
-    t0 = time.perf_counter()
-    base = S.saxo40()
-    cal = S.ShAoSystem(base)
-    cal.calibrate()
-    cmat, imat = cal.cmat, cal.imat
-    P, mask = M.dm_projector(cal)
-    # slopes of known random DM shapes (noise-free): the reconstructors' response gain
-    cal.close(graph=False)
-    rng_c = np.random.default_rng(11)
-    Cs, Ss = [], []
-    for _ in range(32):
-        c = (rng_c.standard_normal(cal.nactu) * 0.02).astype(np.float32)
-        cal.dm.set_com(c)
-        cal.dm.comp_shape()
-        cal.trace_wfs(with_atmos=False)
-        Cs.append(c)
-        Ss.append(cal.measure_slopes().astype(np.float32))
-    Cs = np.array(Cs, np.float64)
-    Ss = torch.as_tensor(np.array(Ss), device="cuda")
-    del cal
-    systems = []
-    for j, r0 in enumerate((0.08, 0.11, 0.14, 0.17, 0.20)):
-        sy = S.ShAoSystem(dataclasses.replace(base, r0=r0, seeds=(500 + 3 * j, 501 + 3 * j, 502 + 3 * j)))
-        sy.imat = imat
-        sy.ls.set_cmat(cmat)
-        sy.close(graph=False)
-        systems.append(sy)
-    t_setup = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    X, T = M.collect_closed_loop(systems, args.pairs, P, mask, seed=3)
-    t_pairs = time.perf_counter() - t0
-    del systems
-    n = X.shape[0]
-    ntr = int(0.95 * n)
-    net = M.MlpReconstructor(X.shape[1], T.shape[1], 1024, 1024, seed=1)
-    net.set_gemm(1)
-    net.init_from_ls(cmat, 1.0 / float(X[:ntr].std()), float(T[:ntr].std()))
-    t0 = time.perf_counter()
-    hist = net.fit(X[:ntr], T[:ntr], epochs=args.epochs, batch=1024, lr=2e-4, lr_decay=0.8, scales_from_data=False)
-    torch.cuda.synchronize()
-    t_train = time.perf_counter() - t0
-    Y = torch.zeros((n - ntr, T.shape[1]), device="cuda")
-    net.forward(X[ntr:].data_ptr(), n - ntr, Y.data_ptr())
-    torch.cuda.synchronize()
-    Tv = T[ntr:].double()
-    ct = torch.as_tensor(np.asarray(cmat, np.float32), device="cuda")
-    err_mlp = float(torch.linalg.norm(Y.double() - Tv) / torch.linalg.norm(Tv))
-    err_ls = float(torch.linalg.norm((X[ntr:] @ ct.T).double() - Tv) / torch.linalg.norm(Tv))
-
-    def closed(mlp=None):
-        sy = S.ShAoSystem(base)
-        sy.ls.set_cmat(cmat)
-        sy.close(graph=False)
-        for _ in range(args.settle):
-            sy.next(compute_psf=False, mlp=mlp, threshold=np.inf)
-        sy.target.reset_le()
-        res = []
-        for _ in range(args.loop_iters):
-            sy.next(mlp=mlp, threshold=np.inf)
-            res.append(sy.residual_rms())
-        return sy.target.strehl(fit=True)[1], float(np.mean(res))
-
-    def response_gain():
-        # mean response to the slopes of known DM shapes, relative to the shapes' commands
-        Yg = torch.zeros((Ss.shape[0], T.shape[1]), device="cuda")
-        net.forward(Ss.data_ptr(), Ss.shape[0], Yg.data_ptr())
-        torch.cuda.synchronize()
-        Yn = Yg.double().cpu().numpy()
-        return float((Yn * Cs).sum() / (Cs * Cs).sum())
-
-    sr_ls, res_ls = closed()
-    sr_mlp, res_mlp = closed(net)
-    gain = response_gain()
-    net.set_scales(net.in_scale, net.out_scale / gain)  # the LS response to a DM shape is 1
-    sr_eq, res_eq = closed(net)
+    res = learned.c4_experiment(pairs=args.pairs, epochs=args.epochs, loop_iters=args.loop_iters,
+                                settle=args.settle)
     print(json.dumps({"workload": "c4", "metric": "long-exposure Strehl at 1.65 um, learned vs LS reconstructor "
-                      "(closed loop, same seeded turbulence)", "value": max(sr_mlp, sr_eq), "unit": "Strehl",
-                      "ls_value": sr_ls, "rel_diff": (max(sr_mlp, sr_eq) - sr_ls) / sr_ls,
-                      "mlp_raw": {"strehl_le": sr_mlp, "residual_rms_um": res_mlp},
-                      "mlp_gain_equalised": {"strehl_le": sr_eq, "residual_rms_um": res_eq, "response_gain": gain},
-                      "residual_rms_um": {"ls": res_ls},
-                      "heldout_rel_err": {"mlp": err_mlp, "ls": err_ls},
+                      "(closed loop, same seeded turbulence)", "value": res["mlp"]["strehl_le"], "unit": "Strehl",
+                      "ls_value": res["ls"]["strehl_le"], "rel_diff": res["rel_diff"],
                       "dtype": "bf16 weights, f32 accumulation", "data": "synthetic",
                       "config": {"workload": "c4: saxo40 geometry, MLP 2496 -> 1024 -> 1024 (GELU) -> 1352 + linear "
                                  "skip initialised to the LS matrix; pairs from closed LS loops at r0 0.08-0.20 m and "
-                                 "magnitudes 6-10; evaluation at r0 0.14 m, magnitude 8, held-out seeds",
-                                 "pairs": n, "train_pairs": ntr, "epochs": args.epochs,
+                                 "magnitudes 6-10; output gain chosen on a validation loop; evaluation at r0 0.14 m, "
+                                 "magnitude 8, held-out seeds", "pairs": args.pairs, "epochs": args.epochs,
                                  "loop_iterations": args.loop_iters},
-                      "seconds": {"setup": round(t_setup, 1), "pairs": round(t_pairs, 1), "train": round(t_train, 1)},
-                      "loss_per_epoch": hist}))
+                      **{k: v for k, v in res.items() if k not in ("rel_diff", "net")}}))
     return 0
 
 
@@ -668,7 +586,7 @@ def main():
     ap.add_argument("--workload", default="saxo40", choices=["saxo40", "mc64", "pyr50", "mlp", "precision", "c4"])
     ap.add_argument("--loop-iters", type=int, default=5000, help="precision, c4: closed-loop iterations per run")
     ap.add_argument("--pairs", type=int, default=200000, help="c4: training pairs")
-    ap.add_argument("--epochs", type=int, default=8, help="c4: training epochs")
+    ap.add_argument("--epochs", type=int, default=16, help="c4: training epochs")
     ap.add_argument("--settle", type=int, default=100, help="c4: closed-loop iterations before the long exposure")
     ap.add_argument("--instances", type=int, default=64, help="mc64: number of instances (the first N of the list)")
     ap.add_argument("--no-tune", action="store_true", help="mc64: fixed tile shapes instead of the autotuner")

@@ -226,6 +226,38 @@ def collect_open_loop(sys, nsamples, projector, mask, strengths=(0.5, 1.0, 1.5, 
     return X, T
 
 
+def dm_probe(sys, count=32, amplitude=0.02, seed=11):
+    """Noise-free slopes of ``count`` random DM commands (the atmosphere off):
+    (commands [count][nactu] float64, slopes [count][nslope] float32).  The LS
+    reconstructor returns the commands with unit gain on these."""
+    rng = np.random.default_rng(seed)
+    C, Sl = [], []
+    for _ in range(count):
+        c = (rng.standard_normal(sys.nactu) * amplitude).astype(np.float32)
+        sys.dm.set_com(c)
+        sys.dm.comp_shape()
+        sys.trace_wfs(with_atmos=False)
+        C.append(c)
+        Sl.append(sys.measure_slopes().astype(np.float32))
+    sys.dm.set_com(np.zeros(sys.nactu, np.float32))
+    sys.dm.comp_shape()
+    return np.array(C, np.float64), np.array(Sl, np.float32)
+
+
+def response_gain(net, probe):
+    """Mean response of the network to the probe's slopes, relative to the
+    probe's commands (1 for the LS reconstructor)."""
+    import torch
+
+    C, Sl = probe
+    x = torch.as_tensor(Sl, device="cuda")
+    y = torch.zeros((x.shape[0], net.nout), device="cuda")
+    net.forward(x.data_ptr(), x.shape[0], y.data_ptr())
+    torch.cuda.synchronize()
+    Y = y.double().cpu().numpy()
+    return float((Y * C).sum() / (C * C).sum())
+
+
 def collect_closed_loop(systems, nsamples, projector, mask, mags=(6.0, 10.0), segment=100, settle=20, seed=0,
                         batch=256):
     """(slopes, DM-projected residual phase) pairs from closed LS loops, on the
