@@ -28,7 +28,7 @@ from . import mlp as M
 from . import system as S
 
 R0S = (0.08, 0.11, 0.14, 0.17, 0.20)
-FACTORS = (1.0, 1.1, 1.2, 1.35, 1.5)
+FACTORS = (1.0, 1.2, 1.35, 1.5, 1.75, 2.0)
 
 
 def c4_experiment(pairs=200000, epochs=16, loop_iters=3000, settle=100, device=0):
