@@ -712,6 +712,19 @@ class Loop:
         fn = "aob_loop_step" if wait else "aob_loop_step_async"
         call(fn, self.h, addr(host_phase), addr(host_voltage), 1 if noise else 0, stream)
 
+    def persist_start(self, noise=True, host_voltage=None, door_polls=0):
+        """Keep the fused kernel resident (matrix rows, tables and the integrator
+        state in shared memory); each ``persist_step`` then rings it once.
+        host_voltage: a pinned host array the kernel writes at every step."""
+        call("aob_loop_persist_start", self.h, 1 if noise else 0, addr(host_voltage), int(door_polls))
+
+    def persist_step(self, host_phase=None, host_voltage=None, noise=True, stream=None, wait=True):
+        call("aob_loop_persist_step", self.h, addr(host_phase), addr(host_voltage), 1 if noise else 0, stream,
+             1 if wait else 0)
+
+    def persist_stop(self):
+        call("aob_loop_persist_stop", self.h)
+
     def time(self, noise=True, warmup=3, iters=20) -> float:
         """Device milliseconds of one step (device phase, no host copies)."""
         ms = ctypes.c_float()

@@ -333,7 +333,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
 }
 
 // error word written by kernels whose bounded waits expired
-enum : uint32_t { ERR_MBAR_TIMEOUT = 1u };
+enum : uint32_t { ERR_MBAR_TIMEOUT = 1u, ERR_DOOR_TIMEOUT = 16u };
 
 // grid-barrier words (mvm_core.cuh) an owner allocates: the arrival counter on
 // a 128-byte line of its own

@@ -245,6 +245,19 @@ struct aob_loop {
   float *io_volt = nullptr;              // device view of the caller's pinned voltages during a step
   uint32_t test_grid_polls = 0;          // wait-expiry test: grid-barrier poll limit (0 = the default)
   int test_absent_cta = -1;              // wait-expiry test: the CTA that never arrives (-1 = none)
+  // persistent mode: the fused kernel resident, one step per doorbell
+  aob::DevBuf<uint32_t> persist_ctl;     // doorbell, stop, done, completions (one line each)
+  bool persist_on = false;
+  bool persist_launch = false;           // launch_fused starts the resident kernel
+  bool persist_noise = true;
+  uint32_t persist_id = 0;               // id of the last step rung
+  uint32_t persist_door_polls = 0;
+  cudaStream_t persist_stream = nullptr; // the resident kernel's stream
+  cudaStream_t persist_last = nullptr;   // stream of the last step rung
+  float *persist_volt = nullptr;         // device view of the pinned voltages the kernel writes
+  void persist_start(bool noise, float *host_voltage, uint32_t door_polls);
+  void persist_step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s, bool wait);
+  void persist_stop();
   aob_loop(aob_sh *w, aob_centro *c, aob_ls *l);
   ~aob_loop();
   void device_step(bool noise, cudaStream_t s, bool frame_on_device);

@@ -12,11 +12,27 @@
 // command-history ring rotates every iteration, one graph is captured per
 // rotation phase; a graph is rebuilt when a parameter it baked in changes.
 
+#include <cuda.h>
+
 #include <cstring>
 
 #include "aob_objects.hpp"
 
 using namespace aob;
+
+// control-word layout and exit value shared with the kernel (rtc_fused.cu)
+namespace aob {
+constexpr int PERSIST_DOOR = 0, PERSIST_STOP = 32, PERSIST_DONE = 64, PERSIST_WORDS = 128;
+constexpr uint32_t PERSIST_DEFAULT_POLLS = 1u << 21;  // ~2 s of polls (an L2 round trip and a 256 ns sleep each)
+}
+
+static void cu_check(CUresult r, const char *what) {
+  if (r != CUDA_SUCCESS) {
+    const char *msg = nullptr;
+    cuGetErrorString(r, &msg);
+    throw Error(std::string(what) + ": " + (msg ? msg : "driver error"));
+  }
+}
 
 aob_loop::aob_loop(aob_sh *w, aob_centro *c, aob_ls *l) : wfs(w), centro(c), ls(l) {
   AOB_REQUIRE(w && c && l, "loop: sensor, centroider and controller are required");
@@ -32,7 +48,13 @@ aob_loop::aob_loop(aob_sh *w, aob_centro *c, aob_ls *l) : wfs(w), centro(c), ls(
   w->fused = c;
 }
 
-aob_loop::~aob_loop() { drop_graphs(); }
+aob_loop::~aob_loop() {
+  try {
+    persist_stop();
+  } catch (...) {
+  }
+  drop_graphs();
+}
 
 void aob_loop::drop_graphs() {
   for (auto &g : graphs)
@@ -101,7 +123,114 @@ static const void *mapped_view(const void *p) {
   return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
 }
 
+// ---------------------------------------------------------------------------
+// Persistent mode: the fused kernel stays resident (its command-matrix rows,
+// sensor tables and the integrator state stay in shared memory) and runs one
+// step per doorbell.  A step on the caller's stream: the phase copy, a stream
+// write of the step id into the doorbell, a stream wait until the kernel
+// reports the id done, and the voltages (written into pinned host memory by
+// the kernel itself, or copied).  The kernel's waits are bounded; when it
+// leaves it sets "done" far ahead, so no stream waits for a step that will
+// not run.
+void aob_loop::persist_start(bool noise, float *host_voltage, uint32_t door_polls) {
+  AOB_REQUIRE(!persist_on, "loop.persist_start: the persistent kernel is already running");
+  AOB_CUDA(cudaSetDevice(wfs->device));
+  AOB_REQUIRE(ls->delay <= 0.f, "loop.persist_start: the persistent mode needs a controller without delay");
+  AOB_REQUIRE(mode != 1, "loop.persist_start: the persistent mode runs the fused kernel (mode 0 or 2)");
+  AOB_REQUIRE(launch_fused(noise, nullptr, true, true),
+              "loop.persist_start: the fused kernel does not fit this configuration");
+  float *volt = nullptr;
+  if (host_voltage) {
+    volt = static_cast<float *>(const_cast<void *>(mapped_view(host_voltage)));
+    AOB_REQUIRE(volt != nullptr, "loop.persist_start: host_voltage must be pinned, mapped host memory");
+  }
+  if (persist_ctl.n < PERSIST_WORDS) persist_ctl.alloc(PERSIST_WORDS);
+  AOB_CUDA(cudaMemset(persist_ctl.p, 0, sizeof(uint32_t) * PERSIST_WORDS));
+  // the device frame counter starts at the host's
+  frame_host = (uint32_t)wfs->frame;
+  AOB_CUDA(cudaMemcpy(d_frame.p, &frame_host, sizeof frame_host, cudaMemcpyHostToDevice));
+  frame_mirror = wfs->frame;
+  AOB_CUDA(cudaStreamCreateWithFlags(&persist_stream, cudaStreamNonBlocking));
+  persist_door_polls = door_polls ? door_polls : PERSIST_DEFAULT_POLLS;
+  persist_launch = true;
+  io_volt = volt;
+  bool ok = false;
+  try {
+    ok = launch_fused(noise, persist_stream, true, false);
+  } catch (...) {
+    persist_launch = false;
+    io_volt = nullptr;
+    cudaStreamDestroy(persist_stream);
+    persist_stream = nullptr;
+    throw;
+  }
+  persist_launch = false;
+  io_volt = nullptr;
+  if (!ok) {
+    cudaStreamDestroy(persist_stream);
+    persist_stream = nullptr;
+    throw Error("loop.persist_start: launch failed");
+  }
+  persist_on = true;
+  persist_noise = noise;
+  persist_volt = volt;
+  persist_id = 0;
+  persist_last = nullptr;
+}
+
+void aob_loop::persist_step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s, bool wait) {
+  AOB_REQUIRE(persist_on, "loop.persist_step: the persistent kernel is not running (persist_start)");
+  AOB_REQUIRE(noise == persist_noise, "loop.persist_step: the noise setting differs from persist_start's");
+  AOB_CUDA(cudaSetDevice(wfs->device));
+  if (host_phase)
+    AOB_CUDA(cudaMemcpyAsync(wfs->phase.p, host_phase, wfs->phase.bytes(), cudaMemcpyHostToDevice, s));
+  const uint32_t id = persist_id + 1;
+  CUstream cs = reinterpret_cast<CUstream>(s);
+  cu_check(cuStreamWriteValue32(cs, reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_DOOR), id, 0),
+           "loop.persist_step: doorbell");
+  cu_check(cuStreamWaitValue32(cs, reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_DONE), id,
+                               CU_STREAM_WAIT_VALUE_GEQ),
+           "loop.persist_step: wait");
+  persist_id = id;
+  persist_last = s;
+  if (host_voltage && mapped_view(host_voltage) != persist_volt)
+    AOB_CUDA(cudaMemcpyAsync(host_voltage, ls->com_clipped.p, ls->com_clipped.bytes(), cudaMemcpyDeviceToHost, s));
+  // host-side state the step corresponds to
+  if (noise && wfs->noise > -1.f) {
+    ++wfs->frame;
+    ++frame_mirror;
+  }
+  ++wfs->image_gen;
+  if (wait) AOB_CUDA(cudaStreamSynchronize(s));
+}
+
+void aob_loop::persist_stop() {
+  if (!persist_on) return;
+  AOB_CUDA(cudaSetDevice(wfs->device));
+  persist_on = false;
+  // the steps already rung first (the kernel finishes them, or its bounded
+  // waits expire and it releases their waits)
+  if (persist_last) cudaStreamSynchronize(persist_last);
+  // the stop flag through a stream of its own (no implicit ordering with any other)
+  cudaStream_t ss = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&ss, cudaStreamNonBlocking);
+  if (e == cudaSuccess) {
+    const CUresult r = cuStreamWriteValue32(reinterpret_cast<CUstream>(ss),
+                                            reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_STOP), 1u, 0);
+    e = r == CUDA_SUCCESS ? cudaStreamSynchronize(ss) : cudaErrorUnknown;
+    cudaStreamDestroy(ss);
+  }
+  const cudaError_t e2 = cudaStreamSynchronize(persist_stream);
+  cudaStreamDestroy(persist_stream);
+  persist_stream = nullptr;
+  persist_last = nullptr;
+  persist_volt = nullptr;
+  AOB_CUDA(e);
+  AOB_CUDA(e2);
+}
+
 void aob_loop::step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s, bool wait) {
+  AOB_REQUIRE(!persist_on, "loop.step: the persistent kernel is running (persist_step / persist_stop)");
   AOB_CUDA(cudaSetDevice(wfs->device));
   // Direct voltages: with the caller's voltage buffer pinned and mapped, the
   // fused kernel's epilogue writes it as well (posted stores over the bus), so
@@ -259,6 +388,40 @@ int aob_loop_test_wait_expiry(aob_loop *l, uint32_t polls, void *stream) {
     // CTA 0 never added its arrival: bring the counter back to a multiple of the grid
     AOB_CUDA(cudaMemsetAsync(l->gbar.p, 0, sizeof(unsigned long long) * GRID_WORDS, s));
     AOB_CUDA(cudaStreamSynchronize(s));
+    return AOB_OK;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return AOB_ERR;
+  }
+}
+
+int aob_loop_persist_start(aob_loop *l, int noise, float *host_voltage, uint32_t door_polls) {
+  try {
+    if (!l) throw Error("aob_loop_persist_start: null handle");
+    l->persist_start(noise != 0, host_voltage, door_polls);
+    return AOB_OK;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return AOB_ERR;
+  }
+}
+
+int aob_loop_persist_step(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream,
+                          int wait) {
+  try {
+    if (!l) throw Error("aob_loop_persist_step: null handle");
+    l->persist_step(host_phase, host_voltage, noise != 0, reinterpret_cast<cudaStream_t>(stream), wait != 0);
+    return AOB_OK;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return AOB_ERR;
+  }
+}
+
+int aob_loop_persist_stop(aob_loop *l) {
+  try {
+    if (!l) throw Error("aob_loop_persist_stop: null handle");
+    l->persist_stop();
     return AOB_OK;
   } catch (const std::exception &e) {
     set_last_error(e.what());

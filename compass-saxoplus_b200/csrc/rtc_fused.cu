@@ -58,7 +58,26 @@ struct RtcFusedArgs {
   float *volt_host;  // caller's pinned host voltages (mapped), also written, or null
   uint32_t grid_polls;  // poll limit of the grid-barrier wait
   int absent_cta;       // test of the bounded wait: this CTA never arrives (-1: none)
+  // persistent mode (ctl non-null): the kernel stays resident and runs one step
+  // per doorbell.  ctl[PERSIST_DOOR]: the id of the step to run (written by the
+  // host's stream), ctl[PERSIST_STOP]: non-zero to leave, ctl[PERSIST_DONE]: the
+  // id of the last step every CTA finished (read by the host's stream),
+  // ctl[PERSIST_FIN]: CTA completions.  Step ids count from 1.
+  uint32_t *ctl;
+  uint32_t door_polls;  // poll limit of one doorbell wait (each poll sleeps ~256 ns)
 };
+
+// control words of the persistent mode, one 128-byte line each
+constexpr int PERSIST_DOOR = 0, PERSIST_STOP = 32, PERSIST_DONE = 64, PERSIST_FIN = 96, PERSIST_WORDS = 128;
+// done value a persistent kernel leaves behind when it exits: far ahead of every
+// step id a host stream may be waiting for (the waits compare cyclically)
+constexpr uint32_t PERSIST_EXIT_AHEAD = 0x40000000u;
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 
 __host__ __device__ inline size_t fused_bars_bytes(int rows) { return 128 * (((size_t)rows * 8 + 127) / 128); }
 __host__ __device__ inline size_t fused_pre_bytes(int rows) { return 128 * (((size_t)rows * 20 + 127) / 128); }
@@ -159,8 +178,43 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
       pre[4 * RP + r] = o1;
     }
   }
-  // ---- sensor images and slopes: this CTA's sub-apertures, A.batch per round ----
   sh_load_tables<NFFT>(A.sh, shm, threadIdx.x, blockDim.x, true, tcopy.wt_bytes != 0);
+  const bool persist = A.ctl != nullptr;
+  __shared__ uint32_t s_go;
+  uint32_t step = 0;
+  for (;;) {
+  if (persist) {
+    // the next step: its doorbell rung, and every CTA done with the previous step
+    // (so no CTA overwrites slopes another one still reads)
+    if (threadIdx.x == 0) {
+      uint32_t go = 0;
+      for (uint32_t i = 0; i < A.door_polls; ++i) {
+        if (ld_acquire_u32(A.ctl + PERSIST_STOP)) break;
+        if ((int32_t)(ld_acquire_u32(A.ctl + PERSIST_DOOR) - (step + 1)) >= 0 &&
+            (int32_t)(ld_acquire_u32(A.ctl + PERSIST_DONE) - step) >= 0) {
+          go = 1;
+          break;
+        }
+        __nanosleep(256);
+      }
+      if (!go && !ld_acquire_u32(A.ctl + PERSIST_STOP)) atomicOr(A.status, (uint32_t)ERR_DOOR_TIMEOUT);
+      s_go = go;
+    }
+    __syncthreads();
+    if (!s_go) break;
+    ++step;
+    if ((int)threadIdx.x == helper && step > 1) {
+      // this step's phase slice into L2 (the first step's went out at entry)
+      const uint32_t screen = (uint32_t)A.sh.npup * (uint32_t)A.sh.npup * 4u;
+      const uint32_t slice = ((screen + gridDim.x - 1) / gridDim.x + 15u) & ~15u;
+      const uint32_t off = blockIdx.x * slice;
+      if (off < screen && (reinterpret_cast<uintptr_t>(A.sh.phase) & 15) == 0) {
+        const uint32_t len = min(slice, (screen - off) & ~15u);
+        if (len) bulk_prefetch_l2(reinterpret_cast<const unsigned char *>(A.sh.phase) + off, len);
+      }
+    }
+  }
+  // ---- sensor images and slopes: this CTA's sub-apertures, A.batch per round ----
   // (stages 0-1 read no tables; the copied ones are waited for after stage 1,
   // the rest is published by the barrier that closes stage 1)
   // With the CTA's whole share in one round (the usual case) the cube and
@@ -274,6 +328,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
       A.err[gr] = e;
       const float c = A.gain * (e * pre[RP + r]) + pre[2 * RP + r];
       A.com[gr] = c;
+      pre[2 * RP + r] = c;  // the integrator's state for a next (persistent) step
       float v;
       if (A.delayed) {
         v = A.a * pre[3 * RP + r] + A.b * pre[4 * RP + r];
@@ -285,6 +340,25 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
       A.volt[gr] = v;
       if (A.volt_host) A.volt_host[gr] = v;
     }
+  }
+  if (!persist) break;
+  // end of a persistent step: the last CTA to finish publishes its id (the
+  // voltages written to host memory are made visible to the host first)
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence_system();
+    const uint32_t old = atomicAdd(A.ctl + PERSIST_FIN, 1u);
+    if (old + 1u == step * gridDim.x) {
+      __threadfence_system();
+      atomicExch(A.ctl + PERSIST_DONE, step);
+    }
+  }
+  if (!ok) break;  // a bounded wait expired: leave (the status word says which)
+  }  // step loop
+  if (persist && threadIdx.x == 0) {
+    // release any host stream still waiting for a step that will not run
+    __threadfence_system();
+    atomicMax(A.ctl + PERSIST_DONE, step + PERSIST_EXIT_AHEAD);
   }
   // no CTA may exit with a copy still landing in its shared memory
   __syncthreads();
@@ -416,6 +490,8 @@ bool aob_loop::launch_fused(bool noise, cudaStream_t s, bool frame_on_device, bo
   A.volt_host = io_volt;
   A.grid_polls = test_grid_polls ? test_grid_polls : GRID_MAX_POLLS;
   A.absent_cta = test_absent_cta;
+  A.ctl = persist_launch ? persist_ctl.p : nullptr;
+  A.door_polls = persist_door_polls;
   const int nsm = num_sms(w->device);
   const int grid = std::min(nsm, c->nactu);
   AOB_REQUIRE((int64_t)c->nactu * grid < (int64_t)1 << 32, "loop: too many actuators for the fused kernel");
@@ -444,6 +520,7 @@ bool aob_loop::launch_fused(bool noise, cudaStream_t s, bool frame_on_device, bo
     ok = launch_fused_n<__nv_fp8_e4m3>(w->nfft, w->nphase, A, grid, sm, s, dry);
   if (!ok || dry) return ok;
   AOB_LAUNCH_CHECK("rtc_fused_kernel");
+  if (persist_launch) return true;  // the steps run, and are accounted for, one doorbell at a time
   w->after_image(A.sh, fc, false);
   if (A.delayed) {
     aob::DevBuf<float> t = std::move(c->ring.front());

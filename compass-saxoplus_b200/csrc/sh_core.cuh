@@ -322,7 +322,7 @@ __device__ __forceinline__ void sh_batch(const ShKernelArgs &P, int base, int st
         const int x = l - y * pd;
         const int k = base + s * stride;
         const int id = (x + __ldg(P.puppixx + k)) + (y + __ldg(P.puppixy + k)) * P.npup;
-        ph[j] = __ldg(P.phase + id);
+        ph[j] = __ldcg(P.phase + id);  // (L2: a resident kernel reads a new phase every step)
         am[j] = __ldg(P.pupil + id);
         of[j] = __ldg(P.offsets + l);
       }

@@ -554,6 +554,26 @@ int aob_loop_step(aob_loop *l, const float *host_phase, float *host_voltage, int
  * the copies synchronous).  For callers that step many iterations and read the
  * results later, as the reference's supervisor loop does between frames. */
 int aob_loop_step_async(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream);
+/* Persistent mode (no counterpart in the reference): the fused kernel stays
+ * resident -- its command-matrix rows, sensor tables and the integrator state
+ * in shared memory -- and runs one RTC step per doorbell.  persist_start
+ * launches it (noise: the setting every step uses; host_voltage: pinned,
+ * mapped host memory the kernel writes the voltages into at every step, or
+ * NULL; door_polls: limit of one wait for a doorbell, 0 = about two seconds,
+ * after which the kernel leaves and sets bit 4 (16) of aob_ls_status).
+ * persist_step enqueues one step on stream: the host phase copy (if given), a
+ * stream write of the step's doorbell, a stream wait until the kernel reports
+ * it done, and the voltages into host_voltage (copied unless it is the
+ * buffer given to persist_start); wait = 1 also synchronises.  Results equal
+ * aob_loop_step's bit for bit.  persist_stop lets the kernel leave after the
+ * steps already rung.  While the kernel runs, the sensor, centroider and
+ * controller must not be changed or stepped otherwise; the controller must
+ * have no delay.  Needs the driver's stream memory operations. */
+int aob_loop_persist_start(aob_loop *l, int noise, float *host_voltage, uint32_t door_polls);
+int aob_loop_persist_step(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream,
+                          int wait);
+int aob_loop_persist_stop(aob_loop *l);
+
 /* Device time of one step (ms, CUDA events on a private stream; device
  * phase, no host copies): warmup untimed steps, then the mean over iters
  * steps.  Used by the autotuner; the loop state advances. */
