@@ -27,11 +27,27 @@ constexpr uint32_t PERSIST_DEFAULT_POLLS = 1u << 21;  // ~2 s of polls (an L2 ro
 }
 
 static void cu_check(CUresult r, const char *what) {
-  if (r != CUDA_SUCCESS) {
-    const char *msg = nullptr;
-    cuGetErrorString(r, &msg);
-    throw Error(std::string(what) + ": " + (msg ? msg : "driver error"));
-  }
+  if (r != CUDA_SUCCESS) throw Error(std::string(what) + ": driver error " + std::to_string((int)r));
+}
+
+// The driver's stream memory operations, looked up through the runtime (the
+// library does not link the driver library itself and still loads on
+// machines without it).
+using StreamValue32Fn = CUresult (*)(CUstream, CUdeviceptr, cuuint32_t, unsigned int);
+static StreamValue32Fn driver_fn(const char *name) {
+  void *p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  AOB_CUDA(cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q));
+  AOB_REQUIRE(p != nullptr && q == cudaDriverEntryPointSuccess, std::string("loop: ") + name + " not available");
+  return reinterpret_cast<StreamValue32Fn>(p);
+}
+static StreamValue32Fn write_value32() {
+  static StreamValue32Fn fn = driver_fn("cuStreamWriteValue32");
+  return fn;
+}
+static StreamValue32Fn wait_value32() {
+  static StreamValue32Fn fn = driver_fn("cuStreamWaitValue32");
+  return fn;
 }
 
 aob_loop::aob_loop(aob_sh *w, aob_centro *c, aob_ls *l) : wfs(w), centro(c), ls(l) {
@@ -186,10 +202,10 @@ void aob_loop::persist_step(const float *host_phase, float *host_voltage, bool n
     AOB_CUDA(cudaMemcpyAsync(wfs->phase.p, host_phase, wfs->phase.bytes(), cudaMemcpyHostToDevice, s));
   const uint32_t id = persist_id + 1;
   CUstream cs = reinterpret_cast<CUstream>(s);
-  cu_check(cuStreamWriteValue32(cs, reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_DOOR), id, 0),
+  cu_check(write_value32()(cs, reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_DOOR), id, 0),
            "loop.persist_step: doorbell");
-  cu_check(cuStreamWaitValue32(cs, reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_DONE), id,
-                               CU_STREAM_WAIT_VALUE_GEQ),
+  cu_check(wait_value32()(cs, reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_DONE), id,
+                          CU_STREAM_WAIT_VALUE_GEQ),
            "loop.persist_step: wait");
   persist_id = id;
   persist_last = s;
@@ -215,8 +231,12 @@ void aob_loop::persist_stop() {
   cudaStream_t ss = nullptr;
   cudaError_t e = cudaStreamCreateWithFlags(&ss, cudaStreamNonBlocking);
   if (e == cudaSuccess) {
-    const CUresult r = cuStreamWriteValue32(reinterpret_cast<CUstream>(ss),
-                                            reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_STOP), 1u, 0);
+    CUresult r = CUDA_ERROR_NOT_SUPPORTED;
+    try {
+      r = write_value32()(reinterpret_cast<CUstream>(ss), reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_STOP),
+                          1u, 0);
+    } catch (...) {
+    }
     e = r == CUDA_SUCCESS ? cudaStreamSynchronize(ss) : cudaErrorUnknown;
     cudaStreamDestroy(ss);
   }
