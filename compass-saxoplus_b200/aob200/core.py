@@ -725,6 +725,11 @@ class Loop:
     def persist_stop(self):
         call("aob_loop_persist_stop", self.h)
 
+    def persist_flush(self, dev_buf, nbytes, stream=None):
+        """The resident kernel writes nbytes of zeros at dev_buf (an L2 flush
+        between timed steps; no other kernel runs beside it)."""
+        call("aob_loop_persist_flush", self.h, int(dev_buf), int(nbytes), stream)
+
     def time(self, noise=True, warmup=3, iters=20) -> float:
         """Device milliseconds of one step (device phase, no host copies)."""
         ms = ctypes.c_float()

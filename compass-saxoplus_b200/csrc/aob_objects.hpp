@@ -258,6 +258,8 @@ struct aob_loop {
   void persist_start(bool noise, float *host_voltage, uint32_t door_polls);
   void persist_step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s, bool wait);
   void persist_stop();
+  void persist_flush(void *dev_buf, size_t bytes, cudaStream_t s);
+  uint32_t persist_cmd = 0;              // last command rung (1: a flush; the next step resets it)
   aob_loop(aob_sh *w, aob_centro *c, aob_ls *l);
   ~aob_loop();
   void device_step(bool noise, cudaStream_t s, bool frame_on_device);

@@ -23,6 +23,7 @@ using namespace aob;
 // control-word layout and exit value shared with the kernel (rtc_fused.cu)
 namespace aob {
 constexpr int PERSIST_DOOR = 0, PERSIST_STOP = 32, PERSIST_DONE = 64, PERSIST_WORDS = 128;
+constexpr int PERSIST_CMD = 4, PERSIST_ARG = 8;
 constexpr uint32_t PERSIST_DEFAULT_POLLS = 1u << 21;  // ~2 s of polls (an L2 round trip and a 256 ns sleep each)
 }
 
@@ -192,6 +193,7 @@ void aob_loop::persist_start(bool noise, float *host_voltage, uint32_t door_poll
   persist_volt = volt;
   persist_id = 0;
   persist_last = nullptr;
+  persist_cmd = 0;
 }
 
 void aob_loop::persist_step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s, bool wait) {
@@ -202,6 +204,11 @@ void aob_loop::persist_step(const float *host_phase, float *host_voltage, bool n
     AOB_CUDA(cudaMemcpyAsync(wfs->phase.p, host_phase, wfs->phase.bytes(), cudaMemcpyHostToDevice, s));
   const uint32_t id = persist_id + 1;
   CUstream cs = reinterpret_cast<CUstream>(s);
+  if (persist_cmd) {  // the previous command was a flush
+    cu_check(write_value32()(cs, reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_CMD), 0u, 0),
+             "loop.persist_step: command");
+    persist_cmd = 0;
+  }
   cu_check(write_value32()(cs, reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_DOOR), id, 0),
            "loop.persist_step: doorbell");
   cu_check(wait_value32()(cs, reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_DONE), id,
@@ -209,7 +216,7 @@ void aob_loop::persist_step(const float *host_phase, float *host_voltage, bool n
            "loop.persist_step: wait");
   persist_id = id;
   persist_last = s;
-  if (host_voltage && mapped_view(host_voltage) != persist_volt)
+  if (host_voltage && (persist_volt == nullptr || mapped_view(host_voltage) != persist_volt))
     AOB_CUDA(cudaMemcpyAsync(host_voltage, ls->com_clipped.p, ls->com_clipped.bytes(), cudaMemcpyDeviceToHost, s));
   // host-side state the step corresponds to
   if (noise && wfs->noise > -1.f) {
@@ -218,6 +225,30 @@ void aob_loop::persist_step(const float *host_phase, float *host_voltage, bool n
   }
   ++wfs->image_gen;
   if (wait) AOB_CUDA(cudaStreamSynchronize(s));
+}
+
+void aob_loop::persist_flush(void *dev_buf, size_t bytes, cudaStream_t s) {
+  AOB_REQUIRE(persist_on, "loop.persist_flush: the persistent kernel is not running (persist_start)");
+  AOB_REQUIRE(dev_buf != nullptr && (reinterpret_cast<uintptr_t>(dev_buf) & 15) == 0 && bytes % 16 == 0,
+              "loop.persist_flush: a 16-byte aligned device buffer and a multiple of 16 bytes are required");
+  AOB_CUDA(cudaSetDevice(wfs->device));
+  const uint32_t id = persist_id + 1;
+  CUstream cs = reinterpret_cast<CUstream>(s);
+  const uint64_t ptr = reinterpret_cast<uint64_t>(dev_buf), n = bytes;
+  const uint32_t w[5] = {1u, (uint32_t)ptr, (uint32_t)(ptr >> 32), (uint32_t)n, (uint32_t)(n >> 32)};
+  cu_check(write_value32()(cs, reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_CMD), w[0], 0),
+           "loop.persist_flush: command");
+  for (int k = 0; k < 4; ++k)
+    cu_check(write_value32()(cs, reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_ARG + k), w[1 + k], 0),
+             "loop.persist_flush: arguments");
+  cu_check(write_value32()(cs, reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_DOOR), id, 0),
+           "loop.persist_flush: doorbell");
+  cu_check(wait_value32()(cs, reinterpret_cast<CUdeviceptr>(persist_ctl.p + PERSIST_DONE), id,
+                          CU_STREAM_WAIT_VALUE_GEQ),
+           "loop.persist_flush: wait");
+  persist_id = id;
+  persist_last = s;
+  persist_cmd = 1;
 }
 
 void aob_loop::persist_stop() {
@@ -431,6 +462,17 @@ int aob_loop_persist_step(aob_loop *l, const float *host_phase, float *host_volt
   try {
     if (!l) throw Error("aob_loop_persist_step: null handle");
     l->persist_step(host_phase, host_voltage, noise != 0, reinterpret_cast<cudaStream_t>(stream), wait != 0);
+    return AOB_OK;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return AOB_ERR;
+  }
+}
+
+int aob_loop_persist_flush(aob_loop *l, void *dev_buf, size_t bytes, void *stream) {
+  try {
+    if (!l) throw Error("aob_loop_persist_flush: null handle");
+    l->persist_flush(dev_buf, bytes, reinterpret_cast<cudaStream_t>(stream));
     return AOB_OK;
   } catch (const std::exception &e) {
     set_last_error(e.what());

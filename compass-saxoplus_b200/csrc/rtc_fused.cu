@@ -69,6 +69,10 @@ struct RtcFusedArgs {
 
 // control words of the persistent mode, one 128-byte line each
 constexpr int PERSIST_DOOR = 0, PERSIST_STOP = 32, PERSIST_DONE = 64, PERSIST_FIN = 96, PERSIST_WORDS = 128;
+// on the doorbell's line, written before it: the command (0 an RTC step, 1 write
+// ARG bytes of zeros at ARG pointer -- the L2 flush of a benchmark, which has to
+// come from the resident kernel since it holds every SM's registers)
+constexpr int PERSIST_CMD = 4, PERSIST_ARG = 8;
 // done value a persistent kernel leaves behind when it exits: far ahead of every
 // step id a host stream may be waiting for (the waits compare cyclically)
 constexpr uint32_t PERSIST_EXIT_AHEAD = 0x40000000u;
@@ -180,7 +184,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
   }
   sh_load_tables<NFFT>(A.sh, shm, threadIdx.x, blockDim.x, true, tcopy.wt_bytes != 0);
   const bool persist = A.ctl != nullptr;
-  __shared__ uint32_t s_go;
+  __shared__ uint32_t s_go, s_cmd[5];
   uint32_t step = 0;
   for (;;) {
   if (persist) {
@@ -199,10 +203,22 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
       }
       if (!go && !ld_acquire_u32(A.ctl + PERSIST_STOP)) atomicOr(A.status, (uint32_t)ERR_DOOR_TIMEOUT);
       s_go = go;
+      s_cmd[0] = go ? ld_acquire_u32(A.ctl + PERSIST_CMD) : 0u;
+      for (int k = 0; k < 4; ++k) s_cmd[1 + k] = go ? ld_acquire_u32(A.ctl + PERSIST_ARG + k) : 0u;
     }
     __syncthreads();
     if (!s_go) break;
     ++step;
+    if (s_cmd[0] == 1u) {
+      // zeros over the buffer, this CTA's slice, 16 bytes per store
+      float4 *buf = reinterpret_cast<float4 *>((uint64_t)s_cmd[1] | ((uint64_t)s_cmd[2] << 32));
+      const uint64_t n16 = ((uint64_t)s_cmd[3] | ((uint64_t)s_cmd[4] << 32)) / 16;
+      for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n16; i += (uint64_t)gridDim.x * blockDim.x)
+        buf[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+  bool ok = true;
+  if (!persist || s_cmd[0] == 0u) {
     if ((int)threadIdx.x == helper && step > 1) {
       // this step's phase slice into L2 (the first step's went out at entry)
       const uint32_t screen = (uint32_t)A.sh.npup * (uint32_t)A.sh.npup * 4u;
@@ -213,7 +229,6 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
         if (len) bulk_prefetch_l2(reinterpret_cast<const unsigned char *>(A.sh.phase) + off, len);
       }
     }
-  }
   // ---- sensor images and slopes: this CTA's sub-apertures, A.batch per round ----
   // (stages 0-1 read no tables; the copied ones are waited for after stage 1,
   // the rest is published by the barrier that closes stage 1)
@@ -240,7 +255,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
   const bool absent = (int)blockIdx.x == A.absent_cta;
   const unsigned long long ticket = absent ? 0ull : grid_arrive(A.gbar, gridDim.x);
   if (one_round && S1 > 0) sh_store_images(A.sh, blockIdx.x, gridDim.x, S1, shm + L.hdr, L, team);
-  const bool ok = !absent && grid_wait(A.gbar, ticket, A.status, A.grid_polls);
+  ok = !absent && grid_wait(A.gbar, ticket, A.status, A.grid_polls);
   if (ok) {
     if (A.bump && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.bump, 1u);  // no round trip
     // slopes into shared memory, 16 bytes per load (L2 only: they were written by
@@ -341,6 +356,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
       if (A.volt_host) A.volt_host[gr] = v;
     }
   }
+  }  // RTC step
   if (!persist) break;
   // end of a persistent step: the last CTA to finish publishes its id (the
   // voltages written to host memory are made visible to the host first)

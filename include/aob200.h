@@ -573,6 +573,12 @@ int aob_loop_persist_start(aob_loop *l, int noise, float *host_voltage, uint32_t
 int aob_loop_persist_step(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream,
                           int wait);
 int aob_loop_persist_stop(aob_loop *l);
+/* While the kernel is resident it holds every SM's registers, so no other
+ * kernel runs beside it: persist_flush has the resident kernel itself write
+ * bytes of zeros over dev_buf (16-byte aligned, a multiple of 16 bytes), e.g.
+ * to flush L2 between timed steps of a benchmark.  Enqueued on stream like a
+ * step; it does not count as an RTC step (no noise frame). */
+int aob_loop_persist_flush(aob_loop *l, void *dev_buf, size_t bytes, void *stream);
 
 /* Device time of one step (ms, CUDA events on a private stream; device
  * phase, no host copies): warmup untimed steps, then the mean over iters

@@ -3,8 +3,10 @@
 The saxo40 loop (rtc_fused_kernel<float, 32, 6>, photon + readout noise,
 wCoG with threshold, LS integrator) is stepped from host phases twice: once
 with one kernel launch per step (aob_loop_step), once with the kernel resident
-and rung once per step.  Voltages must be equal bit for bit at every step, with
-the kernel writing them into pinned host memory or with a copy.  A doorbell
+and rung once per step, with the resident kernel's buffer-clearing command
+(the benchmark's L2 flush) between some steps.  Voltages must be equal bit for
+bit at every step, with the kernel writing them into pinned host memory or
+with a copy.  A doorbell
 that never rings makes the resident kernel's bounded wait run out: it leaves,
 sets bit 16 of the controller's status and the context stays usable.
 """
@@ -55,10 +57,13 @@ def test_persistent_steps_equal_launched_steps(env, direct):
     ref = _launched(setup, phases, torch)
     wfs, c, ls, loop = build_sh_loop(setup, graph=False)
     hv = torch.zeros(setup.nactu, dtype=torch.float32).pin_memory()
+    scratch = torch.empty(8 * 1024 * 1024, dtype=torch.float32, device="cuda")
     loop.persist_start(noise=True, host_voltage=hv.data_ptr() if direct else None)
     try:
         v = np.zeros(setup.nactu, np.float32)
         for i in range(NSTEPS):
+            if i % 2:  # the resident kernel's own flush between steps changes nothing
+                loop.persist_flush(scratch.data_ptr(), scratch.numel() * 4)
             if direct:
                 loop.persist_step(phases[i % 4].data_ptr(), hv.data_ptr(), noise=True, wait=True)
                 got = hv.numpy().copy()
