@@ -746,7 +746,8 @@ def main():
                                           noise=True, stream=sptr, wait=False)
                         b.record(stream)
                         evs.append((a, b))
-                    torch.cuda.synchronize()
+                    # (the stream only: a device-wide synchronise would wait for the resident kernel)
+                    stream.synchronize()
                     return sum(a.elapsed_time(b) for a, b in evs)
 
                 pms = [timed(False), timed(True)]

@@ -568,7 +568,9 @@ int aob_loop_step_async(aob_loop *l, const float *host_phase, float *host_voltag
  * aob_loop_step's bit for bit.  persist_stop lets the kernel leave after the
  * steps already rung.  While the kernel runs, the sensor, centroider and
  * controller must not be changed or stepped otherwise; the controller must
- * have no delay.  Needs the driver's stream memory operations. */
+ * have no delay, and nothing may synchronise the whole device (it would wait
+ * for the resident kernel until its doorbell wait runs out): synchronise
+ * streams.  Needs the driver's stream memory operations. */
 int aob_loop_persist_start(aob_loop *l, int noise, float *host_voltage, uint32_t door_polls);
 int aob_loop_persist_step(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream,
                           int wait);
