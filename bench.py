@@ -727,7 +727,7 @@ def main():
     # and integrator state in shared memory), one doorbell per step; the L2 flush
     # between steps is written by the resident kernel itself (it holds every
     # SM's registers, no other kernel runs beside it) ------------------------
-    persistent, pms = None, [float("nan"), float("nan")]
+    persistent, pms, busy_us = None, [float("nan"), float("nan")], float("nan")
     if fused:
         try:
             loop.persist_start(noise=True, host_voltage=h_volt.data_ptr())
@@ -750,7 +750,11 @@ def main():
                     stream.synchronize()
                     return sum(a.elapsed_time(b) for a, b in evs)
 
-                pms = [timed(False), timed(True)]
+                n0, t0 = loop.persist_stats()
+                pms = [timed(False)]
+                n1, t1 = loop.persist_stats()
+                pms.append(timed(True))
+                busy_us = (t1 - t0) / max(n1 - n0, 1) / 1000.0
             finally:
                 loop.persist_stop()
             if ls.status():
@@ -765,6 +769,7 @@ def main():
     if fused and persistent is None and np.isfinite(pms).all():
         persistent = {
             "value": ws * e2e_steps / (pms[0] / 1000.0), "unit": UNIT, "ms_per_step": pms[0] / e2e_steps,
+            "kernel_busy_us_per_step": busy_us,
             "e2e": {"value": ws * e2e_steps / (pms[1] / 1000.0), "unit": UNIT, "h2d_bytes_per_step": nbytes_phase,
                     "d2h_bytes_per_step": setup.nactu * 4},
             "call": "aob_loop_persist_step: stream write of the doorbell, stream wait for the kernel's done "

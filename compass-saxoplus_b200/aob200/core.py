@@ -725,6 +725,12 @@ class Loop:
     def persist_stop(self):
         call("aob_loop_persist_stop", self.h)
 
+    def persist_stats(self):
+        """(RTC steps rung, summed busy nanoseconds measured by the resident kernel)."""
+        n, t = ctypes.c_uint64(), ctypes.c_uint64()
+        call("aob_loop_persist_stats", self.h, ctypes.addressof(n), ctypes.addressof(t))
+        return n.value, t.value
+
     def persist_flush(self, dev_buf, nbytes, stream=None):
         """The resident kernel writes nbytes of zeros at dev_buf (an L2 flush
         between timed steps; no other kernel runs beside it)."""

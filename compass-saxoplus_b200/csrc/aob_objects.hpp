@@ -260,6 +260,7 @@ struct aob_loop {
   void persist_stop();
   void persist_flush(void *dev_buf, size_t bytes, cudaStream_t s);
   uint32_t persist_cmd = 0;              // last command rung (1: a flush; the next step resets it)
+  uint64_t persist_rtc_steps = 0;        // RTC steps rung since persist_start
   aob_loop(aob_sh *w, aob_centro *c, aob_ls *l);
   ~aob_loop();
   void device_step(bool noise, cudaStream_t s, bool frame_on_device);

@@ -194,6 +194,7 @@ void aob_loop::persist_start(bool noise, float *host_voltage, uint32_t door_poll
   persist_id = 0;
   persist_last = nullptr;
   persist_cmd = 0;
+  persist_rtc_steps = 0;
 }
 
 void aob_loop::persist_step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s, bool wait) {
@@ -216,6 +217,7 @@ void aob_loop::persist_step(const float *host_phase, float *host_voltage, bool n
            "loop.persist_step: wait");
   persist_id = id;
   persist_last = s;
+  ++persist_rtc_steps;
   if (host_voltage && (persist_volt == nullptr || mapped_view(host_voltage) != persist_volt))
     AOB_CUDA(cudaMemcpyAsync(host_voltage, ls->com_clipped.p, ls->com_clipped.bytes(), cudaMemcpyDeviceToHost, s));
   // host-side state the step corresponds to
@@ -473,6 +475,28 @@ int aob_loop_persist_flush(aob_loop *l, void *dev_buf, size_t bytes, void *strea
   try {
     if (!l) throw Error("aob_loop_persist_flush: null handle");
     l->persist_flush(dev_buf, bytes, reinterpret_cast<cudaStream_t>(stream));
+    return AOB_OK;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return AOB_ERR;
+  }
+}
+
+int aob_loop_persist_stats(aob_loop *l, uint64_t *steps, uint64_t *busy_ns) {
+  try {
+    if (!l || !steps || !busy_ns) throw Error("aob_loop_persist_stats: null pointer");
+    AOB_REQUIRE(l->persist_ctl.p != nullptr, "aob_loop_persist_stats: the persistent kernel never ran");
+    AOB_CUDA(cudaSetDevice(l->wfs->device));
+    unsigned long long t = 0;
+    // (the control words are read with a copy on a stream of its own: no device-wide wait)
+    cudaStream_t ss = nullptr;
+    AOB_CUDA(cudaStreamCreateWithFlags(&ss, cudaStreamNonBlocking));
+    cudaError_t e = cudaMemcpyAsync(&t, l->persist_ctl.p + 74, sizeof t, cudaMemcpyDeviceToHost, ss);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ss);
+    cudaStreamDestroy(ss);
+    AOB_CUDA(e);
+    *steps = l->persist_rtc_steps;
+    *busy_ns = t;
     return AOB_OK;
   } catch (const std::exception &e) {
     set_last_error(e.what());

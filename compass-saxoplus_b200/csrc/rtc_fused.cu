@@ -73,6 +73,15 @@ constexpr int PERSIST_DOOR = 0, PERSIST_STOP = 32, PERSIST_DONE = 64, PERSIST_FI
 // ARG bytes of zeros at ARG pointer -- the L2 flush of a benchmark, which has to
 // come from the resident kernel since it holds every SM's registers)
 constexpr int PERSIST_CMD = 4, PERSIST_ARG = 8;
+// on the done line: the global-timer time CTA 0 saw the doorbell (64 bits) and
+// the sum over steps of (done - that time) in nanoseconds (64 bits)
+constexpr int PERSIST_T0 = 72, PERSIST_TSUM = 74;
+
+__device__ __forceinline__ unsigned long long global_timer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 // done value a persistent kernel leaves behind when it exits: far ahead of every
 // step id a host stream may be waiting for (the waits compare cyclically)
 constexpr uint32_t PERSIST_EXIT_AHEAD = 0x40000000u;
@@ -209,6 +218,8 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
     __syncthreads();
     if (!s_go) break;
     ++step;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+      *reinterpret_cast<unsigned long long *>(A.ctl + PERSIST_T0) = global_timer_ns();
     if (s_cmd[0] == 1u) {
       // zeros over the buffer, this CTA's slice, 16 bytes per store
       float4 *buf = reinterpret_cast<float4 *>((uint64_t)s_cmd[1] | ((uint64_t)s_cmd[2] << 32));
@@ -365,6 +376,10 @@ __global__ void __launch_bounds__(FUSED_THREADS, 1) rtc_fused_kernel(RtcFusedArg
     __threadfence_system();
     const uint32_t old = atomicAdd(A.ctl + PERSIST_FIN, 1u);
     if (old + 1u == step * gridDim.x) {
+      if (s_cmd[0] == 0u) {  // busy time of an RTC step, doorbell seen by CTA 0 to done
+        const unsigned long long t0 = *reinterpret_cast<volatile unsigned long long *>(A.ctl + PERSIST_T0);
+        atomicAdd(reinterpret_cast<unsigned long long *>(A.ctl + PERSIST_TSUM), global_timer_ns() - t0);
+      }
       __threadfence_system();
       atomicExch(A.ctl + PERSIST_DONE, step);
     }

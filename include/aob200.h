@@ -581,6 +581,10 @@ int aob_loop_persist_stop(aob_loop *l);
  * to flush L2 between timed steps of a benchmark.  Enqueued on stream like a
  * step; it does not count as an RTC step (no noise frame). */
 int aob_loop_persist_flush(aob_loop *l, void *dev_buf, size_t bytes, void *stream);
+/* The resident kernel's own account of its RTC steps since persist_start:
+ * the number of steps rung and the sum of their busy times in nanoseconds
+ * (GPU global timer, from the doorbell seen by CTA 0 to the step's done). */
+int aob_loop_persist_stats(aob_loop *l, uint64_t *steps, uint64_t *busy_ns);
 
 /* Device time of one step (ms, CUDA events on a private stream; device
  * phase, no host copies): warmup untimed steps, then the mean over iters
