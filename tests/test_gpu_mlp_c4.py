@@ -5,7 +5,7 @@ magnitudes 6-10, 16 epochs on the project's tcgen05 GEMM, the output gain
 chosen on a validation loop, then both reconstructors on the same held-out
 closed loop (r0 0.14 m, magnitude 8, 2000 iterations after 100 settling ones).
 
-Bounds: the learned loop's long-exposure Strehl at
+Bounds (the accuracy target of the learned reconstructor): the learned loop's long-exposure Strehl at
 1.65 um within 1 % of the LS loop's (or above it); on held-out pairs the
 network predicts the DM-projected residual with a smaller error than LS.
 """
