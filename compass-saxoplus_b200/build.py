@@ -78,7 +78,35 @@ def build(force=False, jobs=None, verbose=False, extra=()):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed: " + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+    build_native_dropin(force=force)
     return LIB
+
+
+NATIVE = os.path.join(HERE, "dropin_native")
+
+
+def build_native_dropin(force=False):
+    """The compiled drop-in modules `carma` and `sutra` (pybind11, g++), linked
+    against libaob200.so next to them (rpath $ORIGIN/../aob200)."""
+    import sysconfig
+
+    import pybind11
+
+    suffix = sysconfig.get_config_var("EXT_SUFFIX")
+    hdrs = glob.glob(os.path.join(NATIVE, "*.hpp")) + [os.path.join(ROOT, "include", "aob200.h"), __file__]
+    cflags = ["-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden", "-I" + pybind11.get_include(),
+              "-I" + sysconfig.get_paths()["include"], "-I" + os.path.join(ROOT, "include")]
+    out = []
+    for name in ("carma", "sutra"):
+        src = os.path.join(NATIVE, name + ".cpp")
+        so = os.path.join(NATIVE, name + suffix)
+        if force or _stale(so, [src] + hdrs + [LIB]):
+            cmd = ["g++"] + cflags + [src, "-o", so, "-L" + OUT_DIR, "-laob200", "-Wl,-rpath,$ORIGIN/../aob200"]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError("native drop-in build failed: " + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+        out.append(so)
+    return out
 
 
 if __name__ == "__main__":

@@ -1,4 +1,6 @@
-"""Shared test inputs: seeded phase screens and geometry builders."""
+"""Shared test inputs: seeded phase screens, geometry builders and the drop-in modules."""
+
+import os
 
 import numpy as np
 
@@ -39,3 +41,29 @@ def rel_rms(a, b):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     return float(np.sqrt(np.mean((a - b) ** 2)) / max(np.sqrt(np.mean(b**2)), 1e-300))
+
+
+_PKG = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "compass-saxoplus_b200")
+DROPIN_DIRS = {"python": os.path.join(_PKG, "dropin"), "native": os.path.join(_PKG, "dropin_native")}
+
+
+def import_dropin(kind):
+    """(carma, sutra) of the Python drop-in (``kind="python"``) or of the compiled
+    pybind11 pair (``"native"``).  Both are named carma / sutra, so whatever
+    those names held in sys.modules before is put back afterwards."""
+    import sys
+
+    path = DROPIN_DIRS[kind]
+    saved = {k: sys.modules.pop(k) for k in ("carma", "sutra") if k in sys.modules}
+    sys.path.insert(0, path)
+    try:
+        import carma
+        import sutra
+    finally:
+        sys.path.remove(path)
+        for k in ("carma", "sutra"):
+            sys.modules.pop(k, None)
+        sys.modules.update(saved)
+    if kind == "native":
+        assert sutra.__file__.endswith(".so") and carma.__file__.endswith(".so"), "the compiled drop-in is not built"
+    return carma, sutra

@@ -3,14 +3,15 @@ method names shesha calls on the hot path (the reference's pybind11 bindings:
 python_module/sutra/src/sutra.cpp:62-103, rtc.cpp:100-485, wfs_sh.cpp:41-148,
 wfs_pyrhr.cpp:131-163, centroider.cpp:83-352, controller.cpp), and reject
 unsupported sensor / centroider / controller types (correlation centroider,
-minimum-variance controller, low-resolution pyramid) before any device work."""
+minimum-variance controller, low-resolution pyramid) before any device work.
 
-import os
-import sys
+Both implementations are checked: the Python drop-in (dropin/) and the compiled
+pybind11 pair (dropin_native/), which carries the real-time classes only (no DMs,
+do_imat or uint16 camera RTC)."""
 
 import pytest
 
-DROPIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "compass-saxoplus_b200", "dropin")
+from helpers import import_dropin
 
 API = {
     "Sensors": ["initgs", "d_wfs", "set_field_stop"],
@@ -42,29 +43,29 @@ API = {
 }
 
 
-@pytest.fixture(scope="module")
-def mods():
-    sys.path.insert(0, DROPIN)
-    try:
-        import carma
-        import sutra
-    finally:
-        sys.path.remove(DROPIN)
-    return carma, sutra
+# what the compiled pair leaves to the Python drop-in
+NATIVE_ABSENT = {"Dms", "Dm", "do_imat", "d_img_raw", "d_perturb_map"}
+
+
+@pytest.fixture(scope="module", params=["python", "native"])
+def mods(request):
+    return (request.param,) + import_dropin(request.param)
 
 
 def test_names(mods):
-    carma, sutra = mods
+    kind, carma, sutra = mods
     for cls, names in API.items():
+        if kind == "native" and cls in NATIVE_ABSENT:
+            continue
         c = getattr(sutra, cls)
-        missing = [n for n in names if not hasattr(c, n)]
+        missing = [n for n in names if not hasattr(c, n) and not (kind == "native" and n in NATIVE_ABSENT)]
         assert not missing, f"{cls} lacks {missing}"
     for n in ("get_instance", "get_instance_1gpu", "get_instance_ngpu", "activate_device"):
         assert hasattr(carma.context, n)
 
 
 def test_rejects_before_device_work(mods):
-    carma, sutra = mods
+    kind, carma, sutra = mods
     ctx = carma.context.get_instance()
     assert ctx.ndevice >= 1
     rtc = sutra.Rtc_FFF()

@@ -4,35 +4,26 @@ A supervisor-style loop (shesha's sequence: set the guide-star phase, comp_image
 do_centroids, do_control, apply_control) over one Shack-Hartmann and one
 pyramid sensor feeding one LS controller must equal, bit for bit, the same
 loop written with ``aob200.core`` calls; the controller reads the two
-centroiders' slopes one block after the other.
+centroiders' slopes one block after the other.  It runs through both drop-ins:
+the Python modules (dropin/) and the compiled pybind11 pair (dropin_native/).
 """
-
-import os
-import sys
 
 import numpy as np
 import pytest
 
-from helpers import kolmogorov_screen, sh_geometry
+from helpers import import_dropin, kolmogorov_screen, sh_geometry
 
 pytestmark = pytest.mark.gpu
 
-DROPIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "compass-saxoplus_b200", "dropin")
 
-
-@pytest.fixture(scope="module")
-def mods():
+@pytest.fixture(scope="module", params=["python", "native"])
+def mods(request):
     from aob200 import _lib
     from aob200 import core as C
 
     if _lib.device_count() < 1:
         pytest.fail("no CUDA device visible to libaob200")
-    sys.path.insert(0, DROPIN)
-    try:
-        import carma
-        import sutra
-    finally:
-        sys.path.remove(DROPIN)
+    carma, sutra = import_dropin(request.param)
     return C, carma, sutra
 
 
@@ -140,3 +131,75 @@ def test_supervisor_loop_equals_core_calls(mods, delay):
         np.testing.assert_array_equal(np.array(ctl.d_voltage), np.array(l1.buffer("voltage")))
     assert np.abs(np.array(ctl.d_voltage)).max() > 0
 
+
+
+def test_native_pair_methods_equal_core_calls():
+    """The compiled pair beyond the loop above: get_cog into the sensor's own
+    slopes, geometric slopes, the generic controller's leaky integrator, and a
+    shape error raised as RuntimeError (the reference's std::runtime_error)."""
+    from aob200 import _lib
+    from aob200 import core as C
+
+    if _lib.device_count() < 1:
+        pytest.fail("no CUDA device visible to libaob200")
+    carma, sutra = import_dropin("native")
+    g = sh_geometry("sh16")
+    ctx = carma.context.get_instance_1gpu(0)
+    sens = sutra.Sensors(ctx, None, ["sh"], 1, g.nxsub, g.nvalid, 1, g.npix, g.pdiam, g.nrebin, g.nfft, g.ntot,
+                         g.tel.n, np.float32(g.subapd), np.float32(g.nphotons), 0.0, False, False, 0, 0, 0, False)
+    w = sens.d_wfs[0]
+    assert isinstance(w, sutra.SHWFS)
+    w.load_arrays(g.phasemap, g.hrmap, g.binmap, g.halfxy, g.fluxPerSub, g.validsubsx, g.validsubsy,
+                  g.validpuppixx, g.validpuppixy, g.ttprojmat)
+    w.set_pupil(g.tel.mpupil)
+    sens.initgs(0, 0, g.wavelength_um, 0, 0, 0, -1.0, 3, 0, 0, 0, 0)
+    ph = kolmogorov_screen(g.tel.n, 20.0, seed=31)
+    w.d_gs.d_phase.d_screen.set(ph)
+    w.comp_image(False)
+    rtc = sutra.Rtc_FFF()
+    rtc.add_centroider(ctx, g.nvalid, g.npix / 2 - 0.5, g.pixsize, False, 0, "cog", w)
+    cen = rtc.d_centro[0]
+    cen.set_npix(g.npix)
+    cen.load_validpos(g.validsubsx, g.validsubsy, g.nvalid)
+    nact = 40
+    rtc.add_controller(ctx, "generic", 0, 0.0, 2 * g.nvalid, nact)
+    ctl = rtc.d_control[0]
+    assert isinstance(ctl, sutra.ControllerGENERIC)
+    cm = (np.random.default_rng(6).standard_normal((nact, 2 * g.nvalid)) * 0.01).astype(np.float32)
+    ctl.set_cmat(cm)
+    ctl.set_commandlaw("integrator")
+    ctl.set_leaky_factor(0.95)
+    rtc.set_gain(0, 0.4)
+    with pytest.raises(RuntimeError):
+        ctl.set_cmat(cm.T)
+
+    w1 = C.ShWfs.from_geometry(g)
+    w1.set_phase(ph)
+    w1.comp_image(noise=False)
+    c1 = C.Centroider(g.nvalid, g.npix / 2 - 0.5, g.pixsize, "cog")
+    c1.set_npix(g.npix)
+    c1.load_validpos(g.validsubsx, g.validsubsy)
+    c1.attach(w1)
+    l1 = C.LsController(2 * g.nvalid, nact, kind="generic")
+    l1.set_cmat(cm)
+    l1.set_commandlaw("integrator")
+    l1.set_leaky_factor(0.95)
+    l1.set_gain(0.4)
+    for _ in range(3):
+        rtc.do_centroids(0)
+        rtc.do_control(0)
+        rtc.apply_control(0)
+        c1.get_cog(l1.buffer("centroids").ptr)
+        l1.comp_com()
+        l1.comp_voltage()
+    np.testing.assert_array_equal(np.array(ctl.d_centroids), np.array(l1.buffer("centroids")))
+    np.testing.assert_array_equal(np.array(ctl.d_com), np.array(l1.buffer("com")))
+    np.testing.assert_array_equal(np.array(ctl.d_voltage), np.array(l1.buffer("voltage")))
+    assert ctl.command_law == "integrator"
+
+    cen.get_cog()  # into the sensor's d_slopes
+    np.testing.assert_array_equal(np.array(w.d_slopes), np.array(ctl.d_centroids))
+    for kind in (0, 1, 2):
+        w.slopes_geom(kind)
+        w1.slopes_geom(kind)
+        np.testing.assert_array_equal(np.array(w.d_slopes), np.array(w1.buffer("slopes")))
