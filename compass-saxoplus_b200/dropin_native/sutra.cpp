@@ -5,11 +5,11 @@
 // Failures raise RuntimeError with the library's message, as the reference's
 // C++ layer does (std::runtime_error).
 //
-// Covered: Sensors (SHWFS, PYRWFS, guide star), Rtc_FFF with the cog, tcog,
-// wcog, bpcog, pyr and maskedpix centroiders and the ls and generic controllers
-// (do_centroids, do_control, apply_control, comp_voltage, do_clipping, gains,
-// imat_svd, build_cmat, reference slopes, perturbation voltages).  DMs, do_imat
-// and the uint16 camera RTC (Rtc_UFF) are in the Python drop-in (dropin/sutra.py).
+// Covered: Sensors (SHWFS, PYRWFS, guide star), Dms / Dm (piezo stacks), Rtc_FFF
+// and Rtc_UFF (uint16 frames) with the cog, tcog, wcog, bpcog, pyr and maskedpix
+// centroiders and the ls and generic controllers (do_centroids, do_control,
+// apply_control, comp_voltage, do_clipping, gains, do_imat, imat_svd, build_cmat,
+// reference slopes, perturbation voltages).
 
 #include "sutra_rtc.hpp"
 
@@ -86,27 +86,53 @@ void bind_controllers(py::module_ &m) {
             check(aob_ls_set_open_loop(c.l->h, ol ? 1 : 0, reset ? 1 : 0), "set_open_loop");
           },
           py::arg("open_loop"), py::arg("reset") = true)
-      .def("comp_voltage", [](Controller &c) { check(aob_ls_comp_voltage(c.l->h, nullptr), "comp_voltage"); })
+      .def("comp_voltage",
+           [](Controller &c) {
+             check(aob_ls_comp_voltage(c.l->h, nullptr), "comp_voltage");
+             c.advance_perturb();
+           })
       .def("clip_commands", [](Controller &c) { check(aob_ls_clip(c.l->h, nullptr), "clip_commands"); })
-      .def("add_perturb", [](Controller &c) { check(aob_ls_apply_perturb(c.l->h, nullptr), "add_perturb"); })
+      .def("add_perturb",
+           [](Controller &c) {
+             // com_clipped += the current row of every enabled perturbation (controller.cpp add_perturb)
+             check(aob_ls_apply_perturb(c.l->h, nullptr), "add_perturb");
+             c.advance_perturb();
+           })
       .def("add_perturb_voltage",
            [](Controller &c, const std::string &name, const farray<float> &p, int N) {
              check(aob_ls_add_perturb(c.l->h, name.c_str(), p.data(), N), "add_perturb_voltage");
+             c.perturb[name] = std::make_tuple(py::object(py::array(p).attr("copy")()), 0, true);
+             c.perturb_n[name] = N;
            })
       .def("remove_perturb_voltage",
            [](Controller &c, const std::string &name) {
              check(aob_ls_remove_perturb(c.l->h, name.c_str()), "remove_perturb_voltage");
+             c.perturb.erase(name);
+             c.perturb_n.erase(name);
            })
       .def("enable_perturb_voltage",
            [](Controller &c, const std::string &name) {
              check(aob_ls_enable_perturb(c.l->h, name.c_str(), 1), "enable_perturb_voltage");
+             std::get<2>(c.perturb.at(name)) = true;
            })
       .def("disable_perturb_voltage",
            [](Controller &c, const std::string &name) {
              check(aob_ls_enable_perturb(c.l->h, name.c_str(), 0), "disable_perturb_voltage");
+             std::get<2>(c.perturb.at(name)) = false;
            })
       .def("reset_perturb_voltage",
-           [](Controller &c) { check(aob_ls_reset_perturb(c.l->h), "reset_perturb_voltage"); });
+           [](Controller &c) {
+             check(aob_ls_reset_perturb(c.l->h), "reset_perturb_voltage");
+             c.perturb.clear();
+             c.perturb_n.clear();
+           })
+      .def_property_readonly("d_perturb_map", [](const Controller &c) {
+        // name -> (perturbation voltages [N, nactu], counter, enabled), as the reference's map
+        py::dict d;
+        for (auto &kv : c.perturb)
+          d[py::str(kv.first)] = py::make_tuple(std::get<0>(kv.second), std::get<1>(kv.second), std::get<2>(kv.second));
+        return d;
+      });
 
   py::class_<ControllerLS, Controller, std::shared_ptr<ControllerLS>>(m, "ControllerLS")
       .def_property_readonly("d_eigenvals", [](const ControllerLS &c) { return c.buffer("eigenvals"); });
@@ -170,6 +196,7 @@ void bind_rtc_fff(py::module_ &m) {
             c->nvalid = (typec == "maskedpix" && wfs) ? 4 * wfs->nvalid : nvalid;
             c->offset = offset;
             c->scale = scale;
+            c->tin_u16 = r.u16;
             c->c = std::make_shared<CentroOwner>();
             check(aob_centro_create(&c->c->h, device, centro_type(typec), c->nvalid, offset, scale), "add_centroider");
             if (wfs) {
@@ -203,6 +230,10 @@ void bind_rtc_fff(py::module_ &m) {
               check(aob_ls_create(&c->l->h, device, nslope, nactu, delay), "add_controller");
             else
               check(aob_generic_create(&c->l->h, device, nslope, nactu, delay), "add_controller");
+            if (!idx_dms.is_none() && ndm > 0) {
+              for (int i = 0; i < ndm; ++i) c->dm_idx.push_back(elem<int>(idx_dms, i));
+              c->dm_idx_set = true;
+            }
             if (!idx_centro.is_none() && ncentro > 0) {
               for (int i = 0; i < ncentro; ++i) c->centro_idx.push_back(elem<int>(idx_centro, i));
             } else {
@@ -217,6 +248,63 @@ void bind_rtc_fff(py::module_ &m) {
           py::arg("is_modal") = false, py::arg("dms") = py::none(), py::arg("idx_dms") = py::none(),
           py::arg("ndm") = 0, py::arg("idx_centro") = py::none(), py::arg("ncentro") = 0, py::arg("Nphi") = 0,
           py::arg("wfs_direction") = false)
+      .def(
+          "do_imat",
+          [](Rtc &r, int ncontrol, std::shared_ptr<Dms> dms, bool kernconv) {
+            // push-pull interaction matrix (sutra_rtc.cpp:150-292): every actuator of every
+            // DM the controller drives, pushed and pulled by its push4imat, seen by the
+            // controller's SH sensors (noise-free, nphot4imat photons); the slopes
+            // (s_push - s_pull) / (2 push) are the columns of d_imat.  All actuators of a
+            // DM go through one batched evaluation (aob_imat_build) per sensor.
+            if (kernconv) throw std::runtime_error("do_imat: the spot convolution kernel is not supported");
+            Controller &c = r.ctl(ncontrol);
+            if (c.type != "ls") throw std::runtime_error("do_imat: the controller must be ls");
+            std::vector<std::pair<int, std::shared_ptr<Dm>>> seen;
+            if (c.dm_idx_set)
+              for (int i : c.dm_idx) seen.emplace_back(i, dms->dms.at(i));
+            else
+              for (size_t i = 0; i < dms->dms.size(); ++i) seen.emplace_back((int)i, dms->dms[i]);
+            int total = 0;
+            for (auto &p : seen) total += p.second->nactus;
+            if (total != c.nactu)
+              throw std::runtime_error("do_imat: the DMs' actuators do not add up to the controller's nactu");
+            std::vector<float> imat((size_t)c.nslope * c.nactu, 0.f);  // Fortran order, nslope x nactu
+            int a0 = 0;
+            for (auto &p : seen) {
+              Dm &dm = *p.second;
+              aob_dm *dh = dm.need();
+              int off = 0;
+              for (int i : c.centro_idx) {
+                Centroider &cen = *r.centro.at(i);
+                const int ns = cen.nslopes();
+                if (!cen.wfs || !cen.wfs->sh)
+                  throw std::runtime_error("do_imat: only Shack-Hartmann sensors are supported");
+                if (off + ns > c.nslope) throw std::runtime_error("do_imat: the slopes exceed the controller's nslope");
+                Wfs &w = *cen.wfs;
+                // the DM's place on the sensor's phase grid (wfs.d_gs.add_layer), else centred
+                float xoff = (float)((dm.dim - w.npup) / 2.0), yoff = xoff;
+                if (w.gs) {
+                  auto it = w.gs->dm_layers.find(p.first);
+                  if (it != w.gs->dm_layers.end()) xoff = it->second.first, yoff = it->second.second;
+                }
+                check(aob_centro_attach_wfs(cen.c->h, w.sh->h), "do_imat");
+                DevAlloc tmp(sizeof(float) * (size_t)ns * dm.nactus, dm.device);
+                check(aob_imat_build(w.sh->h, cen.c->h, dh, xoff, yoff, dm.push4imat, 0, static_cast<float *>(tmp.p),
+                                     nullptr),
+                      "do_imat");
+                std::vector<float> h((size_t)ns * dm.nactus);
+                check(aob_memcpy_d2h(h.data(), tmp.p, sizeof(float) * h.size(), nullptr), "do_imat");
+                for (int a = 0; a < dm.nactus; ++a)
+                  for (int k = 0; k < ns; ++k)
+                    imat[(size_t)(off + k) + (size_t)(a0 + a) * c.nslope] = h[(size_t)k + (size_t)a * ns];
+                off += ns;
+              }
+              a0 += dm.nactus;
+            }
+            check(aob_ls_set_imat(c.l->h, imat.data()), "do_imat");
+            return 0;
+          },
+          py::arg("ncontrol"), py::arg("dms"), py::arg("kernconv") = false)
       .def("remove_controller", [](Rtc &r, int n) { r.control.erase(r.control.begin() + n); })
       .def("remove_centroider", [](Rtc &r, int n) { r.centro.erase(r.centro.begin() + n); })
       .def("do_centroids",
@@ -290,6 +378,12 @@ void bind_rtc_fff(py::module_ &m) {
       });
 }
 
+// SutraRtc<uint16_t, float, float>: the centroiders load uint16 frames (from the host
+// or a sensor's d_camimg) and calibrate them with dark, flat and a pixel look-up table
+struct RtcU : Rtc {
+  RtcU() { u16 = true; }
+};
+
 }  // namespace
 
 PYBIND11_MODULE(sutra, m) {
@@ -299,5 +393,7 @@ PYBIND11_MODULE(sutra, m) {
   bind_sensors(m);
   bind_rtc(m);
   bind_controllers(m);
+  bind_dms(m);
   bind_rtc_fff(m);
+  py::class_<RtcU, Rtc, std::shared_ptr<RtcU>>(m, "Rtc_UFF").def(py::init([]() { return std::make_shared<RtcU>(); }));
 }

@@ -6,7 +6,9 @@
 #pragma once
 
 #include <algorithm>
+#include <tuple>
 
+#include "sutra_dms.hpp"
 #include "sutra_sensors.hpp"
 
 namespace aobpy {
@@ -41,6 +43,8 @@ struct Centroider {
   std::shared_ptr<CentroOwner> c;
   std::shared_ptr<Wfs> wfs;
   std::vector<py::ssize_t> img_shape;
+  bool tin_u16 = false;                            // Rtc_UFF: frames are uint16
+  py::dtype raw_dtype = py::dtype::of<float>();  // type of the loaded frame
 
   int nslopes() const { return type == "maskedpix" ? nvalid : 2 * nvalid; }
   DevArr buffer(const char *which, py::dtype dt, std::vector<py::ssize_t> shape = {}) const {
@@ -60,8 +64,17 @@ struct Controller {
   float delay = 0.f, gain = 0.f;
   std::pair<float, float> comRange{-1.0e6f, 1.0e6f};
   std::vector<int> centro_idx;
+  std::vector<int> dm_idx;  // the DMs it drives (indexes into the Dms given to do_imat)
+  bool dm_idx_set = false;
   std::shared_ptr<LsOwner> l;
+  // perturbation voltages: name -> (voltages [N, nactu], row counter, enabled), N
+  std::map<std::string, std::tuple<py::object, int, bool>> perturb;
+  std::map<std::string, int> perturb_n;
   virtual ~Controller() = default;
+  void advance_perturb() {
+    for (auto &kv : perturb)
+      if (std::get<2>(kv.second)) std::get<1>(kv.second) = (std::get<1>(kv.second) + 1) % perturb_n[kv.first];
+  }
   DevArr buffer(const char *which, std::vector<py::ssize_t> shape = {}) const {
     void *p = nullptr;
     int64_t n = 0;
@@ -73,6 +86,8 @@ struct ControllerLS : Controller {};
 struct ControllerGENERIC : Controller {};
 
 struct Rtc {
+  bool u16 = false;  // Rtc_UFF
+  virtual ~Rtc() = default;
   std::vector<std::shared_ptr<Centroider>> centro;
   std::vector<std::shared_ptr<Controller>> control;
   Controller &ctl(int n) { return *control.at(n); }
@@ -164,12 +179,56 @@ inline void bind_rtc(py::module_ &m) {
              check(aob_centro_set_centroids_ref(x.c->h, r.data()), "set_centroids_ref");
            })
       .def("load_img",
-           [](Centroider &x, py::array img, py::args) {
-             // a float32 frame from the host (Rtc_FFF's input type)
+           [](Centroider &x, py::object img, py::args) {
+             // a frame from the host, cast to the RTC's input type as the reference's
+             // binding does, or for a uint16 RTC a uint16 device array (a sensor's d_camimg)
+             if (py::isinstance<DevArr>(img) || py::hasattr(img, "__cuda_array_interface__")) {
+               // a device frame: 2-D uint16 in column-major order (the layout of this
+               // library's buffers), copied on the device
+               py::dict cai = img.attr("__cuda_array_interface__");
+               const auto shape = cai["shape"].cast<std::vector<py::ssize_t>>();
+               const std::string ts = cai["typestr"].cast<std::string>();
+               const bool fortran = cai.contains("strides") && !cai["strides"].is_none() && shape.size() == 2 &&
+                                    cai["strides"].cast<std::vector<py::ssize_t>>() ==
+                                        std::vector<py::ssize_t>{2, 2 * shape[0]};
+               if (ts != "<u2" || shape.size() != 2 || !fortran)
+                 throw std::runtime_error("load_img from device memory takes a 2-D column-major uint16 frame");
+               const auto ptr = cai["data"].cast<py::tuple>()[0].cast<uintptr_t>();
+               x.img_shape = shape;
+               x.raw_dtype = py::dtype::of<uint16_t>();
+               check(aob_centro_load_img_u16(x.c->h, reinterpret_cast<const uint16_t *>(ptr), (int)shape[0],
+                                             (int)shape[1], 1, nullptr),
+                     "load_img");
+               return 0;
+             }
+             if (x.tin_u16) {
+               farray<uint16_t> a = img.cast<farray<uint16_t>>();
+               if (a.ndim() != 2) throw std::runtime_error("load_img: a 2-D image is required");
+               x.img_shape = {a.shape(0), a.shape(1)};
+               x.raw_dtype = py::dtype::of<uint16_t>();
+               check(aob_centro_load_img_u16(x.c->h, a.data(), (int)a.shape(0), (int)a.shape(1), 0, nullptr),
+                     "load_img");
+               return 0;
+             }
              farray<float> a = img.cast<farray<float>>();
              if (a.ndim() != 2) throw std::runtime_error("load_img: a 2-D image is required");
              x.img_shape = {a.shape(0), a.shape(1)};
+             x.raw_dtype = py::dtype::of<float>();
              check(aob_centro_load_img(x.c->h, a.data(), (int)a.shape(0), (int)a.shape(1)), "load_img");
+             return 0;
+           })
+      .def_property_readonly("d_img_raw",
+                             [](const Centroider &x) { return x.buffer("img_raw", x.raw_dtype, x.img_shape); })
+      .def(
+          "set_lutPix",
+          [](Centroider &x, const farray<int32_t> &lut, py::object) {
+            check(aob_centro_set_lut_pix(x.c->h, lut.data(), (int)lut.size()), "set_lutPix");
+            return 0;
+          },
+          py::arg("lutPix"), py::arg("n") = py::none())
+      .def("calibrate_img_validPix",
+           [](Centroider &x) {
+             check(aob_centro_calibrate_img_validpix(x.c->h, nullptr), "calibrate_img_validPix");
              return 0;
            })
       .def("calibrate_img", [](Centroider &x) { check(aob_centro_calibrate_img(x.c->h, nullptr), "calibrate_img"); })

@@ -7,6 +7,7 @@
 
 #include <cmath>
 #include <map>
+#include <type_traits>
 
 #include "native_common.hpp"
 
@@ -26,13 +27,20 @@ struct PyrOwner {
 };
 
 // numpy's view of an argument: element i of np.asarray(a).ravel() (the reference
-// passes per-sensor arrays; a scalar stands for every sensor)
+// passes per-sensor arrays; a scalar stands for every sensor), converted as
+// Python's int() / float() / bool() would (a float index array counts)
 template <typename T>
 T elem(const py::object &a, int i) {
   py::module_ np = py::module_::import("numpy");
   py::object r = np.attr("asarray")(a).attr("ravel")();
   const int n = r.attr("size").cast<int>();
-  return r[py::int_(n == 1 ? 0 : i)].cast<T>();
+  py::object v = r[py::int_(n == 1 ? 0 : i)];
+  if constexpr (std::is_same_v<T, bool>)
+    return py::bool_(v).cast<bool>();
+  else if constexpr (std::is_integral_v<T>)
+    return py::int_(v).cast<T>();
+  else
+    return py::float_(v).cast<T>();
 }
 
 // The guide star's phase screen of one sensor: d_gs.d_phase.d_screen

@@ -6,8 +6,7 @@ unsupported sensor / centroider / controller types (correlation centroider,
 minimum-variance controller, low-resolution pyramid) before any device work.
 
 Both implementations are checked: the Python drop-in (dropin/) and the compiled
-pybind11 pair (dropin_native/), which carries the real-time classes only (no DMs,
-do_imat or uint16 camera RTC)."""
+pybind11 pair (dropin_native/)."""
 
 import pytest
 
@@ -27,7 +26,8 @@ API = {
     "Centroider": ["get_cog", "load_validpos", "set_npix", "set_scale", "set_offset", "set_threshold", "load_weights",
                    "set_centroids_ref", "load_img", "calibrate_img", "set_dark", "set_flat", "set_pyr_method",
                    "set_pyr_thresh", "d_centroids_ref", "d_intensities", "d_img", "d_img_raw", "d_validx", "d_validy",
-                   "d_weights", "set_nmax", "init_weights", "d_dark", "d_flat", "nslopes"],
+                   "d_weights", "set_nmax", "init_weights", "d_dark", "d_flat", "nslopes", "set_lutPix",
+                   "calibrate_img_validPix"],
     "ControllerLS": ["set_cmat", "set_imat", "set_gain", "set_modal_gains", "set_delay", "set_com", "set_comRange",
                      "set_open_loop", "comp_voltage", "clip_commands", "add_perturb_voltage",
                      "remove_perturb_voltage", "enable_perturb_voltage", "disable_perturb_voltage",
@@ -37,14 +37,11 @@ API = {
     "ControllerGENERIC": ["set_cmat", "set_gain", "set_modal_gains", "set_commandlaw", "set_leaky_factor", "set_polc",
                           "set_decayFactor", "set_matE", "set_imat", "comp_voltage", "add_perturb", "d_com",
                           "d_com_clipped", "d_voltage", "d_cmat", "d_centroids"],
+    "Rtc_UFF": ["add_centroider", "add_controller", "do_centroids", "do_control", "do_calibrate_img"],
     "Rtc_FFF": ["add_centroider", "add_controller", "remove_controller", "remove_centroider", "do_calibrate_img",
                 "do_centroids", "do_control", "comp_voltage", "apply_control", "do_clipping", "set_gain",
                 "set_modal_gains", "imat_svd", "build_cmat", "set_centroids_ref", "do_imat"],
 }
-
-
-# what the compiled pair leaves to the Python drop-in
-NATIVE_ABSENT = {"Dms", "Dm", "do_imat", "d_img_raw", "d_perturb_map"}
 
 
 @pytest.fixture(scope="module", params=["python", "native"])
@@ -55,10 +52,8 @@ def mods(request):
 def test_names(mods):
     kind, carma, sutra = mods
     for cls, names in API.items():
-        if kind == "native" and cls in NATIVE_ABSENT:
-            continue
         c = getattr(sutra, cls)
-        missing = [n for n in names if not hasattr(c, n) and not (kind == "native" and n in NATIVE_ABSENT)]
+        missing = [n for n in names if not hasattr(c, n)]
         assert not missing, f"{cls} lacks {missing}"
     for n in ("get_instance", "get_instance_1gpu", "get_instance_ngpu", "activate_device"):
         assert hasattr(carma.context, n)

@@ -11,18 +11,14 @@ rounding before the truncation); calibrated images relative rms <= 1e-6;
 slopes <= 1e-4 against the oracle's CoG of the oracle's calibrated image.
 """
 
-import os
-import sys
-
 import numpy as np
 import pytest
 
-from helpers import kolmogorov_screen, rel_rms, sh_geometry
+from helpers import import_dropin, kolmogorov_screen, rel_rms, sh_geometry
 from oracle import rtc as ortc
 
 pytestmark = pytest.mark.gpu
 
-DROPIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "compass-saxoplus_b200", "dropin")
 MAX_FLUX, MAX_PIX = 2000, 60000
 
 
@@ -58,17 +54,14 @@ def test_fakecam_frame_matches_oracle(cam):
     assert frame.max() == MAX_PIX  # the brightest pixels saturate at max_pix_value
 
 
+@pytest.mark.parametrize("impl", ["python", "native"])
 @pytest.mark.parametrize("kind", ["cog", "wcog"])
-def test_uint16_rtc_calibrates_and_centroids(cam, kind):
+def test_uint16_rtc_calibrates_and_centroids(cam, kind, impl):
     """Rtc_UFF: load the sensor's d_camimg (device copy), calibrate with a dark, a
-    flat and a pixel permutation, then CoG / wCoG -- against the oracle."""
+    flat and a pixel permutation, then CoG / wCoG -- against the oracle; through
+    the Python drop-in and the compiled pair."""
     C, g, w, _, _ = cam
-    sys.path.insert(0, DROPIN)
-    try:
-        import carma
-        import sutra
-    finally:
-        sys.path.remove(DROPIN)
+    carma, sutra = import_dropin(impl)
     ctx = carma.context.get_instance()
     rtc = sutra.Rtc_UFF()
     rtc.add_centroider(ctx, g.nvalid, g.npix / 2 - 0.5, g.pixsize, False, 0, kind)

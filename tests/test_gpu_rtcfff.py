@@ -22,11 +22,10 @@ import numpy as np
 import pytest
 from scipy.ndimage import center_of_mass
 
-from helpers import kolmogorov_screen
+from helpers import import_dropin, kolmogorov_screen
 
 pytestmark = pytest.mark.gpu
 
-DROPIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "compass-saxoplus_b200", "dropin")
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 precision = 1e-2
 DELAY, GAIN, NACTU = 3.0, 0.4, 243
@@ -36,21 +35,17 @@ def relative_array_error(array1, array2):
     return np.abs((array1 - array2) / array2.max()).max()
 
 
-@pytest.fixture(scope="module")
-def sh():
-    """Module-level set-up of test_rtcFFF.py:33-79."""
+@pytest.fixture(scope="module", params=["python", "native"])
+def sh(request):
+    """Module-level set-up of test_rtcFFF.py:33-79, through the Python drop-in and
+    the compiled pair."""
     from aob200 import _lib
     from aob200 import core as C
     from aob200 import geometry as G
 
     if _lib.device_count() < 1:
         pytest.fail("no CUDA device visible to libaob200")
-    sys.path.insert(0, DROPIN)
-    try:
-        import carma
-        import sutra
-    finally:
-        sys.path.remove(DROPIN)
+    carma, sutra = import_dropin(request.param)
     # test_sh.py: 16x16 sub-apertures, 8 pixels of 0.3" at 0.5 um (field of view extended: ntot 64 > nfft 32),
     # fracsub 0.8, magnitude 3, no noise
     g = G.sh_geometry(G.ShParams(nxsub=16, npix=8, pixsize=0.3, wavelength_um=0.5, fracsub=0.8, gsmag=3.0), 128,
@@ -286,7 +281,7 @@ def test_generic_command_laws(sh):
     c.set_modal_gains(mg)
     c.set_matE(matE)
     c.set_decayFactor(decay)
-    c._l.set_centroids(s)
+    c.d_centroids.set(s)
     c0 = rng.standard_normal(na).astype(np.float32)
     f64 = lambda a: np.asarray(a, np.float64)  # noqa: E731
 
@@ -316,21 +311,19 @@ def test_generic_command_laws(sh):
     assert c.command_law == "2matrices"
 
 
-def test_doCentroids_maskedPix():
+@pytest.mark.parametrize("impl", ["python", "native"])
+def test_doCentroids_maskedPix(impl):
     """test_rtcFFF_pyramid.py:26-87: masked-pixel centroider and generic controller on a pyramid image."""
     from aob200 import _lib
     from aob200 import core as C
 
     if _lib.device_count() < 1:
         pytest.fail("no CUDA device visible to libaob200")
-    sys.path.insert(0, DROPIN)
+    carma, sutra = import_dropin(impl)
     sys.path.insert(0, GOLD)
     try:
-        import carma
-        import sutra
         import ref_cases as RC
     finally:
-        sys.path.remove(DROPIN)
         sys.path.remove(GOLD)
     g = RC.pyr_geometry("pyr16")
     w = C.PyrWfs.from_geometry(g)

@@ -25,7 +25,7 @@ import sys
 import numpy as np
 import pytest
 
-from helpers import rel_rms
+from helpers import import_dropin, rel_rms
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 sys.path.insert(0, GOLD)
@@ -33,7 +33,6 @@ import ref_cases as RC  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-DROPIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "compass-saxoplus_b200", "dropin")
 
 
 @pytest.fixture(scope="module")
@@ -142,15 +141,9 @@ def test_pyr_setters_equal_load_arrays(core):
     assert rel_rms(np.array(w.d_binimg), a) > 1e-3
 
 
-@pytest.fixture(scope="module")
-def mods(core):
-    sys.path.insert(0, DROPIN)
-    try:
-        import carma
-        import sutra
-    finally:
-        sys.path.remove(DROPIN)
-    return carma, sutra
+@pytest.fixture(scope="module", params=["python", "native"])
+def mods(core, request):
+    return import_dropin(request.param)
 
 
 def _dropin_sh(carma, sutra, g):
@@ -223,4 +216,4 @@ def test_dropin_sh_comp_nphot(mods):
     ctx, sens, w = _dropin_sh(carma, sutra, g)
     w.comp_nphot(0.001, 0.5, 8.0, 16, zerop=1e11, gsmag=8.0)
     expect = np.float32(1e11 * 10 ** (-0.4 * 8.0) * 0.001 * 0.5 * (8.0 / 16) ** 2)
-    assert w._w.nphot == pytest.approx(float(expect), rel=1e-7)
+    assert w.nphot == pytest.approx(float(expect), rel=1e-7)
