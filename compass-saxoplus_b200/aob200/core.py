@@ -675,6 +675,9 @@ class Loop:
         self.wfs, self.centro, self.ls = wfs, centro, ls
         centro.wfs = wfs
         self.use_graph(graph)
+        # the per-iteration entry points, bound once (a step is on a real-time path)
+        lib = _lib.lib()
+        self._step_fns = ((lib.aob_loop_step_async, "aob_loop_step_async"), (lib.aob_loop_step, "aob_loop_step"))
 
     def __del__(self):
         h = getattr(self, "h", None)
@@ -709,8 +712,11 @@ class Loop:
         """host_phase / host_voltage: numpy float32 arrays (pinned for speed) or None.
         wait=False: enqueue the step and return (aob_loop_step_async); the voltages
         are valid once the stream has reached the step."""
-        fn = "aob_loop_step" if wait else "aob_loop_step_async"
-        call(fn, self.h, addr(host_phase), addr(host_voltage), 1 if noise else 0, stream)
+        hp = host_phase if host_phase is None or type(host_phase) is int else addr(host_phase)
+        hv = host_voltage if host_voltage is None or type(host_voltage) is int else addr(host_voltage)
+        fn, name = self._step_fns[1 if wait else 0]
+        if fn(self.h, hp, hv, 1 if noise else 0, stream) != 0:
+            raise _lib.AobError(f"{name}: {_lib.lib().aob_last_error().decode()}")
 
     def persist_start(self, noise=True, host_voltage=None, door_polls=0):
         """Keep the fused kernel resident (matrix rows, tables and the integrator

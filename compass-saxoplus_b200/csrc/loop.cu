@@ -285,6 +285,9 @@ void aob_loop::persist_stop() {
 void aob_loop::step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s, bool wait) {
   AOB_REQUIRE(!persist_on, "loop.step: the persistent kernel is running (persist_step / persist_stop)");
   AOB_CUDA(cudaSetDevice(wfs->device));
+  // the phase copy goes out first: nothing else of the step can start before it lands
+  if (host_phase)
+    AOB_CUDA(cudaMemcpyAsync(wfs->phase.p, host_phase, wfs->phase.bytes(), cudaMemcpyHostToDevice, s));
   // Direct voltages: with the caller's voltage buffer pinned and mapped, the
   // fused kernel's epilogue writes it as well (posted stores over the bus), so
   // no copy-engine transfer follows the kernel.
@@ -295,8 +298,6 @@ void aob_loop::step(const float *host_phase, float *host_voltage, bool noise, cu
     float *&p;
     ~Reset() { p = nullptr; }
   } reset_io{io_volt};
-  if (host_phase)
-    AOB_CUDA(cudaMemcpyAsync(wfs->phase.p, host_phase, wfs->phase.bytes(), cudaMemcpyHostToDevice, s));
   bool perturbed = false;
   for (auto &kv : ls->perturb) perturbed |= kv.second.on;
   // A graph only pays for the three-kernel step: the fused step is one
