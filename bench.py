@@ -487,6 +487,30 @@ def run_mlp(args, torch):
                        with_flush=False)
         res["train_step_B4096_us"] = t * 1e6
         res["train_tflops"] = 6 * params * B / t / 1e12
+        # one whole RTC iteration with each reconstructor on the same sensor stages:
+        # image with the fused wCoG, slopes to the controller, commands, voltages
+        from aob200.workloads import build_sh_loop
+
+        wfs, cen, ls2, loop = build_sh_loop(setup, graph=False)
+        cptr = ls2.buffer("centroids").ptr
+
+        def it_learned(sp):
+            wfs.comp_image(True, sp)
+            cen.get_cog(cptr, sp)
+            net.comp_com(ls2, 3e38, sp)
+            ls2.comp_voltage(sp)
+
+        def it_ls(sp):
+            wfs.comp_image(True, sp)
+            cen.get_cog(cptr, sp)
+            ls2.comp_com(sp)
+            ls2.comp_voltage(sp)
+
+        loop_us = {"learned": graph_time(torch, flush, it_learned) * 1e6,
+                   "ls_same_kernels": graph_time(torch, flush, it_ls) * 1e6,
+                   "ls_fused_kernel": graph_time(torch, flush, lambda sp: loop.step(None, None, True, sp)) * 1e6,
+                   "what": "one saxo40 RTC iteration (sensor image + wCoG, reconstruction, voltages), graph replay "
+                           "with a flushed L2; the learned reconstructor's Strehl parity is the c4 workload's"}
     peak_t = None
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -519,7 +543,7 @@ def run_mlp(args, torch):
           roofline={"bound": "tensor", "achieved": res["train_tflops"], "peak": peak_t, "unit": "TFLOP/s",
                     "frac": res["train_tflops"] / peak_t, "traffic": None, "kernel": "tc_gemm_kernel (training step)",
                     **res},
-          cpu_baseline=cpu, clocks=clk.summary(), gpu_launches=None)
+          cpu_baseline=cpu, clocks=clk.summary(), gpu_launches=None, loop_us=loop_us)
 
 
 def run_precision(args, torch):
