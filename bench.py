@@ -506,7 +506,10 @@ def run_mlp(args, torch):
             ls2.comp_com(sp)
             ls2.comp_voltage(sp)
 
-        loop_us = {"learned": graph_time(torch, flush, it_learned) * 1e6,
+        loop_us = {"learned_fused_kernel": graph_time(torch, flush,
+                                                      lambda sp: loop.step_mlp(net, 3e38, None, None, True, sp,
+                                                                               wait=False)) * 1e6,
+                   "learned": graph_time(torch, flush, it_learned) * 1e6,
                    "ls_same_kernels": graph_time(torch, flush, it_ls) * 1e6,
                    "ls_fused_kernel": graph_time(torch, flush, lambda sp: loop.step(None, None, True, sp)) * 1e6,
                    "what": "one saxo40 RTC iteration (sensor image + wCoG, reconstruction, voltages), graph replay "

@@ -718,6 +718,15 @@ class Loop:
         if fn(self.h, hp, hv, 1 if noise else 0, stream) != 0:
             raise _lib.AobError(f"{name}: {_lib.lib().aob_last_error().decode()}")
 
+    def step_mlp(self, net, threshold, host_phase=None, host_voltage=None, noise=True, stream=None, wait=True):
+        """One iteration with the learned reconstructor ``net`` (an
+        ``aob200.mlp.MlpReconstructor``) in place of the LS matrix: sensor image
+        with fused centroids, the network's control step (threshold test, LS
+        fallback on this loop's controller), voltages -- one fused kernel when it
+        fits (aob_loop_step_mlp)."""
+        fn = "aob_loop_step_mlp" if wait else "aob_loop_step_mlp_async"
+        call(fn, self.h, net.h, float(threshold), addr(host_phase), addr(host_voltage), 1 if noise else 0, stream)
+
     def persist_start(self, noise=True, host_voltage=None, door_polls=0):
         """Keep the fused kernel resident (matrix rows, tables and the integrator
         state in shared memory); each ``persist_step`` then rings it once.

@@ -22,6 +22,10 @@ struct MvmArgs;
 struct ShKernelArgs;
 }
 
+struct aob_mlp;
+// Device view of pinned, mapped host memory (nullptr for pageable memory).
+const void *mapped_view(const void *p);
+
 // ---------------------------------------------------------------------------
 // Shack-Hartmann sensor (replaces SutraWfsSH, libsutra/src.cpp/sutra_wfs_sh.cpp)
 struct aob_sh {
@@ -265,6 +269,10 @@ struct aob_loop {
   ~aob_loop();
   void device_step(bool noise, cudaStream_t s, bool frame_on_device);
   bool launch_fused(bool noise, cudaStream_t s, bool frame_on_device, bool dry);
+  // one iteration with the learned reconstructor m (rtc_mlp.cu)
+  bool launch_mlp(aob_mlp *m, float threshold, bool noise, cudaStream_t s, bool dry);
+  void step_mlp(aob_mlp *m, float threshold, const float *host_phase, float *host_voltage, bool noise,
+                cudaStream_t s, bool wait);
   void step(const float *host_phase, float *host_voltage, bool noise, cudaStream_t s, bool wait = true);
   uint64_t key(bool noise) const;
   void drop_graphs();
@@ -315,6 +323,10 @@ struct aob_batch {
 // ---------------------------------------------------------------------------
 // learned reconstructor: MLP slopes -> DM commands with a linear skip path
 // (no counterpart in the reference)
+namespace aob {
+struct MlpFusedArgs;
+}
+
 struct aob_mlp {
   int device = 0;
   int nin, nh1, nh2, nout;  // as given
@@ -353,6 +365,7 @@ struct aob_mlp {
   void adam(float lr, cudaStream_t s);
   void infer(const float *x, float *y_out, cudaStream_t s);
   bool comp_com_fused(aob_ls *ls, float threshold, cudaStream_t s);
+  bool fused_args(aob_ls *ls, float threshold, aob::MlpFusedArgs &A, size_t &smem_bytes);
   void colsum(const __nv_bfloat16 *d, int batch, int cols, float *out, cudaStream_t s);
 };
 

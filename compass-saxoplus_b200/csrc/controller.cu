@@ -384,15 +384,23 @@ aob_ls::aob_ls(int device_, int nslope_, int nactu_, float delay_)
   gains.upload(one.data(), nactu);
   cmat.alloc((int64_t)nactu * nslope);
   h_cmat.assign((size_t)nactu * nslope, 0.f);
-  const int nring = delay > 0 ? (int)delay + 2 : 1;
-  for (int i = 0; i < nring; ++i) ring.emplace_back(nactu);
 }
 
+// The delay and its interpolation weights; the command ring grows to the
+// buffers the delay needs (floor(delay) + 2), so a delay set after construction
+// reads only allocated buffers.  New buffers go in front as the oldest commands
+// (zeros); the current command (the ring's back) is kept.
 void aob_ls::set_delay(float d) {
+  AOB_REQUIRE(d >= 0.f, "ls.set_delay: the delay must be >= 0");
   delay = d;
   const int fl = (int)d;
   a = d - (float)fl;
   b = 1.f - a;
+  const int nring = delay > 0 ? fl + 2 : 1;
+  if ((int)ring.size() < nring) {
+    AOB_CUDA(cudaSetDevice(device));
+    while ((int)ring.size() < nring) ring.emplace_front(nactu);
+  }
 }
 
 void aob_ls::ensure_packed(int p) {

@@ -131,7 +131,7 @@ void aob_loop::device_step(bool noise, cudaStream_t s, bool frame_on_device) {
 }
 
 // Device view of pinned, mapped host memory (nullptr for pageable memory).
-static const void *mapped_view(const void *p) {
+const void *mapped_view(const void *p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();

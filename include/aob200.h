@@ -554,6 +554,20 @@ int aob_loop_step(aob_loop *l, const float *host_phase, float *host_voltage, int
  * the copies synchronous).  For callers that step many iterations and read the
  * results later, as the reference's supervisor loop does between frames. */
 int aob_loop_step_async(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream);
+/* One iteration with the learned reconstructor m in place of the LS matrix (no
+ * counterpart in the reference, whose reconstructors are linear): the sensor
+ * image with fused centroids into the controller, aob_mlp_comp_com's control
+ * step (the network, the threshold test, then the integrator or the LS
+ * fallback on the controller's own matrix), the voltages.  Host buffers as in
+ * aob_loop_step.  With an FP32 LS matrix and a configuration that fits, one
+ * cooperative kernel does all of it (rtc_mlp_kernel), else separate launches;
+ * the results are the same bit for bit.  The network's sizes must be the
+ * controller's (nin = nslope, nout = nactu). */
+int aob_loop_step_mlp(aob_loop *l, aob_mlp *m, float threshold, const float *host_phase, float *host_voltage,
+                      int noise, void *stream);
+/* The same without the final wait (as aob_loop_step_async). */
+int aob_loop_step_mlp_async(aob_loop *l, aob_mlp *m, float threshold, const float *host_phase,
+                            float *host_voltage, int noise, void *stream);
 /* Persistent mode (no counterpart in the reference): the fused kernel stays
  * resident -- its command-matrix rows, sensor tables and the integrator state
  * in shared memory -- and runs one RTC step per doorbell.  persist_start
