@@ -17,7 +17,10 @@ Other keys of the JSON line:
             the fused kernel, every step;
   roofline  the dominant kernel's algorithmic bytes / measured duration against
             the measured HBM copy bandwidth in MEASURED_PEAKS.json;
-  cpu_baseline  the float64 NumPy/SciPy restatement timed on the host cores.
+  cpu_baseline  the float64 NumPy/SciPy restatement timed on the host cores;
+  learned   the same iteration with the learned reconstructor in place of the LS
+            matrix (aob_loop_step_mlp, one kernel per step), timed like value;
+            its Strehl parity with LS is the c4 workload's.
 
 --workload selects what is measured: ``saxo40`` (default, the line above),
 or one of the other scope rows, each printing its own JSON line with its own
@@ -750,6 +753,43 @@ def main():
                    "engine, voltages written into the pinned host buffer by the fused kernel; device-timed from before "
                    "the phase copy to after the voltages, wall_clock_value includes the host's wait"}
 
+    # ---- the same iteration with the learned reconstructor in place of the LS
+    # matrix (2496 -> 1024 -> 1024 -> 1377 + the linear skip; its Strehl parity with
+    # LS is the c4 workload's), timed like value: device-resident phase, L2 flushed
+    # before every step, one rtc_mlp_kernel launch per step --------------------
+    learned = None
+    try:
+        from aob200 import mlp as M
+
+        net = M.MlpReconstructor(setup.nslope, setup.nactu, 1024, 1024, device=device, seed=1)
+        net.init_from_ls(setup.cmat, 10.0, 1.0)
+        wfs_l, _c_l, _ls_l, loop_l = build_sh_loop(setup, precision="f32", device=device, graph=False,
+                                                   seed=1234 + rank)
+        ph_l = wfs_l.d_phase.ptr
+        for i in range(args.warmup):
+            _lib.call("aob_memcpy_d2d", ph_l, d_screens[i % nscreen].data_ptr(), nbytes_phase, sptr)
+            flush.zero_()
+            loop_l.step_mlp(net, 3e38, None, None, True, sptr, wait=False)
+        torch.cuda.synchronize()
+        st = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        en = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        for i in range(args.steps):
+            _lib.call("aob_memcpy_d2d", ph_l, d_screens[i % nscreen].data_ptr(), nbytes_phase, sptr)
+            flush.zero_()
+            st[i].record(stream)
+            loop_l.step_mlp(net, 3e38, None, None, True, sptr, wait=False)
+            en[i].record(stream)
+        torch.cuda.synchronize()
+        lms = sum(a.elapsed_time(b) for a, b in zip(st, en)) / args.steps
+        learned = {"value": 1000.0 / lms, "unit": UNIT, "ms_per_step": lms,
+                   "kernels_per_step": loop_l.kernels_per_step(),
+                   "call": "aob_loop_step_mlp: one rtc_mlp_kernel per step (sensor stages, the network's control "
+                           "step with its LS fallback test, voltages)",
+                   "strehl": "long-exposure Strehl within 1 % of LS at this geometry: bench.py --workload c4"}
+        del loop_l, wfs_l, net
+    except Exception as e:  # reported, the headline stands
+        learned = {"error": str(e)[:300]}
+
     # ---- persistent mode: the fused kernel resident (matrix rows, sensor tables
     # and integrator state in shared memory), one doorbell per step; the L2 flush
     # between steps is written by the resident kernel itself (it holds every
@@ -830,6 +870,7 @@ def main():
                    "mvm_precision": args.precision},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": launches,
         "persistent": persistent,
+        "learned": learned,
     }
     print(json.dumps(line))
     return 0
