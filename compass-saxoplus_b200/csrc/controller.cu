@@ -386,10 +386,11 @@ aob_ls::aob_ls(int device_, int nslope_, int nactu_, float delay_)
   h_cmat.assign((size_t)nactu * nslope, 0.f);
 }
 
-// The delay and its interpolation weights; the command ring grows to the
-// buffers the delay needs (floor(delay) + 2), so a delay set after construction
-// reads only allocated buffers.  New buffers go in front as the oldest commands
-// (zeros); the current command (the ring's back) is kept.
+// The delay and its interpolation weights.  The command ring holds the last
+// floor(delay) + 2 commands (1 without delay): ring[0] is read as the command of
+// floor(delay) + 1 steps back, so its length follows the delay.  A longer ring
+// gets zero buffers in front (the oldest commands); a shorter one drops its
+// oldest; the current command (the ring's back) is kept either way.
 void aob_ls::set_delay(float d) {
   AOB_REQUIRE(d >= 0.f, "ls.set_delay: the delay must be >= 0");
   delay = d;
@@ -401,6 +402,7 @@ void aob_ls::set_delay(float d) {
     AOB_CUDA(cudaSetDevice(device));
     while ((int)ring.size() < nring) ring.emplace_front(nactu);
   }
+  while ((int)ring.size() > nring) ring.pop_front();
 }
 
 void aob_ls::ensure_packed(int p) {

@@ -97,6 +97,9 @@ uint64_t aob_loop::key(bool noise) const {
   mix(&centro->params_gen, sizeof centro->params_gen);
   mix(&ls->gain, sizeof ls->gain);
   mix(&ls->a, sizeof ls->a);
+  mix(&ls->delay, sizeof ls->delay);  // the delay ring's length and buffers
+  const size_t nring = ls->ring.size();
+  mix(&nring, sizeof nring);
   mix(&ls->volt_min, sizeof ls->volt_min);
   mix(&ls->volt_max, sizeof ls->volt_max);
   mix(&ls->prec, sizeof ls->prec);

@@ -172,6 +172,30 @@ def test_ls_voltage_delay_perturb_clip_matches_oracle(core):
             assert rel_rms(np.array(c.buffer("com")), o.com) < 1e-5, (delay, it)
 
 
+@pytest.mark.parametrize("built,later", [(0.0, 1.5), (0.0, 2.0), (3.0, 1.0), (2.7, 0.0)])
+def test_delay_set_after_construction_equals_constructor_delay(core, built, later):
+    """set_delay resizes the command ring (floor(delay) + 2 buffers): a controller
+    built with one delay and given another before its first step runs exactly like
+    one built with the second."""
+    rng = np.random.default_rng(11)
+    nslope, nactu = 120, 40
+    cm = rng.standard_normal((nactu, nslope)).astype(np.float32) * 0.05
+    a = core.LsController(nslope, nactu, delay=built)
+    a.set_delay(later)
+    b = core.LsController(nslope, nactu, delay=later)
+    for c in (a, b):
+        c.set_cmat(cm)
+        c.set_gain(0.3)
+    for it in range(6):
+        s = rng.standard_normal(nslope).astype(np.float32)
+        for c in (a, b):
+            c.set_centroids(s)
+            c.comp_com()
+            c.comp_voltage()
+        np.testing.assert_array_equal(np.array(a.buffer("voltage")), np.array(b.buffer("voltage")), err_msg=str(it))
+    assert a.status() == 0 and b.status() == 0
+
+
 def test_svd_cmat_matches_numpy(core):
     rng = np.random.default_rng(4)
     nslope, nactu = 300, 120
