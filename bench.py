@@ -180,6 +180,22 @@ def graph_time(torch, flush, fn, n=20, with_flush=True):
     return (out[0] - (out[1] if with_flush else 0.0)) / n
 
 
+def max_over_ranks(dist, torch, values, device):
+    """Element-wise maximum over the ranks of a list of times (the slowest rank's),
+    unchanged without a process group.  Every rank calls it at the same point."""
+    if not dist:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def job_rate(ws, steps, total_ms):
+    """Whole-job iterations/s: each of the ws ranks ran ``steps`` iterations and the
+    job took the slowest rank's total_ms."""
+    return ws * steps / (total_ms / 1000.0)
+
+
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -683,14 +699,10 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    if dist:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(dist, torch, [sum(s.elapsed_time(e) for s, e in zip(starts, ends))], "cuda")[0]
     clocks = clk.summary()
     ms_per_step = total_ms / args.steps
-    value = ws * args.steps / (total_ms / 1000.0)
+    value = job_rate(ws, args.steps, total_ms)
     launches = loop.kernels_per_step() * args.steps
 
     # ---- per-kernel device durations (graph replay, no host gaps) ----------
@@ -742,12 +754,8 @@ def main():
         b.synchronize()
         wall += time.perf_counter() - w0
     torch.cuda.synchronize()
-    e2e_ms = sum(a.elapsed_time(b) for a, b in ev)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": ws * e2e_steps / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": nbytes_phase,
+    e2e_ms = max_over_ranks(dist, torch, [sum(a.elapsed_time(b) for a, b in ev)], "cuda")[0]
+    e2e = {"value": job_rate(ws, e2e_steps, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": nbytes_phase,
            "d2h_bytes_per_step": setup.nactu * 4, "wall_clock_value": e2e_steps / wall,
            "call": "aob_loop_step_async(host phase -> host voltages), then an event the host waits on: phase by copy "
                    "engine, voltages written into the pinned host buffer by the fused kernel; device-timed from before "
@@ -757,7 +765,7 @@ def main():
     # matrix (2496 -> 1024 -> 1024 -> 1377 + the linear skip; its Strehl parity with
     # LS is the c4 workload's), timed like value: device-resident phase, L2 flushed
     # before every step, one rtc_mlp_kernel launch per step --------------------
-    learned = None
+    learned, learned_ms, learned_kernels = None, float("nan"), 0
     try:
         from aob200 import mlp as M
 
@@ -780,15 +788,18 @@ def main():
             loop_l.step_mlp(net, 3e38, None, None, True, sptr, wait=False)
             en[i].record(stream)
         torch.cuda.synchronize()
-        lms = sum(a.elapsed_time(b) for a, b in zip(st, en)) / args.steps
-        learned = {"value": 1000.0 / lms, "unit": UNIT, "ms_per_step": lms,
-                   "kernels_per_step": loop_l.kernels_per_step(),
-                   "call": "aob_loop_step_mlp: one rtc_mlp_kernel per step (sensor stages, the network's control "
-                           "step with its LS fallback test, voltages)",
-                   "strehl": "long-exposure Strehl within 1 % of LS at this geometry: bench.py --workload c4"}
+        learned_ms = sum(a.elapsed_time(b) for a, b in zip(st, en))
+        learned_kernels = loop_l.kernels_per_step()
         del loop_l, wfs_l, net
     except Exception as e:  # reported, the headline stands
         learned = {"error": str(e)[:300]}
+    learned_ms = max_over_ranks(dist, torch, [learned_ms], "cuda")[0]  # every rank, also after an error
+    if learned is None and np.isfinite(learned_ms):
+        learned = {"value": job_rate(ws, args.steps, learned_ms), "unit": UNIT, "ms_per_step": learned_ms / args.steps,
+                   "kernels_per_step": learned_kernels,
+                   "call": "aob_loop_step_mlp: one rtc_mlp_kernel per step (sensor stages, the network's control "
+                           "step with its LS fallback test, voltages)",
+                   "strehl": "long-exposure Strehl within 1 % of LS at this geometry: bench.py --workload c4"}
 
     # ---- persistent mode: the fused kernel resident (matrix rows, sensor tables
     # and integrator state in shared memory), one doorbell per step; the L2 flush
@@ -829,15 +840,12 @@ def main():
         except Exception as e:  # reported in the line, the launched numbers stand
             persistent = {"error": str(e)[:300]}
             pms = [float("nan"), float("nan")]
-    if dist:
-        t = torch.tensor(pms, device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        pms = [float(x) for x in t.tolist()]
+    pms = max_over_ranks(dist, torch, pms, "cuda")
     if fused and persistent is None and np.isfinite(pms).all():
         persistent = {
-            "value": ws * e2e_steps / (pms[0] / 1000.0), "unit": UNIT, "ms_per_step": pms[0] / e2e_steps,
+            "value": job_rate(ws, e2e_steps, pms[0]), "unit": UNIT, "ms_per_step": pms[0] / e2e_steps,
             "kernel_busy_us_per_step": busy_us,
-            "e2e": {"value": ws * e2e_steps / (pms[1] / 1000.0), "unit": UNIT, "h2d_bytes_per_step": nbytes_phase,
+            "e2e": {"value": job_rate(ws, e2e_steps, pms[1]), "unit": UNIT, "h2d_bytes_per_step": nbytes_phase,
                     "d2h_bytes_per_step": setup.nactu * 4},
             "call": "aob_loop_persist_step: stream write of the doorbell, stream wait for the kernel's done "
                     "word (e2e: after the phase copy from pinned memory; voltages written into the pinned host "
