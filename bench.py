@@ -20,7 +20,9 @@ Other keys of the JSON line:
   cpu_baseline  the float64 NumPy/SciPy restatement timed on the host cores;
   learned   the same iteration with the learned reconstructor in place of the LS
             matrix (aob_loop_step_mlp, one kernel per step), timed like value;
-            its Strehl parity with LS is the c4 workload's.
+            its Strehl parity with LS is the c4 workload's;
+  closed_loop_extras  the stages around it (screen extrusion, raytrace, DM shape)
+            and the whole closed-loop iteration, each in graph replay.
 
 --workload selects what is measured: ``saxo40`` (default, the line above),
 or one of the other scope rows, each printing its own JSON line with its own
@@ -801,6 +803,33 @@ def main():
                            "step with its LS fallback test, voltages)",
                    "strehl": "long-exposure Strehl within 1 % of LS at this geometry: bench.py --workload c4"}
 
+    # ---- the closed-loop stages around the RTC iteration, each timed alone (graph
+    # replay, L2 flushed): the three-layer screen extrusion, the raytrace of the
+    # layers and the DM into the sensor's phase, the DM shape from the voltages;
+    # then the whole closed-loop iteration (ShAoSystem.next without the PSF) -----
+    extras, ex_us, dm_bytes, dm_nact = None, [float("nan")] * 4, 0, 0
+    try:
+        from aob200 import system as S
+
+        sy = S.ShAoSystem(S.saxo40(), device)
+        sy.close(graph=False)
+        dm = sy.dm
+        dm_bytes, dm_nact = 4 * (dm.influsize * dm.influsize * dm.nact + dm.nact + dm.dim * dm.dim), dm.nact
+        ex_us = [graph_time(torch, flush, lambda sp: sy.atmos.move(sp)) * 1e6,
+                 graph_time(torch, flush, lambda sp: sy.trace_wfs(sp)) * 1e6,
+                 graph_time(torch, flush, lambda sp: dm.comp_shape(None, sp)) * 1e6,
+                 graph_time(torch, flush, lambda sp: sy.next(sp, compute_psf=False, noise=True)) * 1e6]
+        del sy
+    except Exception as e:  # reported, the headline stands
+        extras = {"error": str(e)[:300]}
+    ex_us = max_over_ranks(dist, torch, ex_us, "cuda")  # every rank, also after an error
+    if extras is None and all(np.isfinite(ex_us)):
+        extras = {"extrusion_us": ex_us[0], "raytrace_wfs_us": ex_us[1], "dm_shape_us": ex_us[2],
+                  "dm_shape_bytes": dm_bytes, "dm_shape_gbs": dm_bytes / ex_us[2] / 1e3, "iteration_us": ex_us[3],
+                  "what": f"saxo40 closed loop (3 von Karman layers, {dm_nact}-actuator DM): extrusion of every layer, "
+                          "raytrace into the sensor's phase, DM shape, and the whole iteration (extrusion, "
+                          "raytrace, fused RTC step, DM shape)"}
+
     # ---- persistent mode: the fused kernel resident (matrix rows, sensor tables
     # and integrator state in shared memory), one doorbell per step; the L2 flush
     # between steps is written by the resident kernel itself (it holds every
@@ -879,6 +908,7 @@ def main():
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": launches,
         "persistent": persistent,
         "learned": learned,
+        "closed_loop_extras": extras,
     }
     print(json.dumps(line))
     return 0
