@@ -9,9 +9,11 @@
 // scratch (the new column and a copy of the screen, for n <= 512) in one
 // file-scope device array that every GPU loading the library holds until exit.
 //
-// The math is the same two kernels the atmosphere object launches
-// (extrude_gemv_kernel, extrude_shift_kernel in sim.cu), so the result equals
-// aob_atmos_move's for the same operators, noise counter and layer index.
+// It launches the two-kernel form of the extrusion (extrude_gemv_kernel, then
+// extrude_shift_kernel, in sim.cu); the atmosphere object runs the same
+// arithmetic fused into extrude_fused_kernel, so the result equals
+// aob_atmos_move's for the same operators, noise counter and layer index, and
+// the two forms check each other.
 
 #include <algorithm>
 #include <mutex>

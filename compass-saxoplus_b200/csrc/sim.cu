@@ -79,6 +79,123 @@ __global__ void extrude_shift_kernel(float *dst, const float *src, const float *
   }
 }
 
+// One extrusion of every job's layer in one launch (blockIdx.y = job): the rows
+// of extrude_gemv_kernel write the new column / row straight to its place in
+// the next screen, and the grid shifts the rest of the screen by one sample as
+// extrude_shift_kernel does.  The arithmetic of both is unchanged (each row's
+// dot products keep their order), so the screens equal the two-kernel
+// sequence's bit for bit, with one launch per round of extrusions instead of
+// two per layer.  The launch is short and its data cold, so it is bound by
+// chains of memory latency, not bytes: a warp loads its first row of A and B
+// into registers before anything else (a lane's share fits for nst, n <= 512),
+// and the shift issues four loads per thread before their stores.
+constexpr int EXTRUDE_PRE = 16;  // values of a row a lane holds, per operand
+constexpr int EXTRUDE_ILP = 4;   // shift loads in flight per thread
+
+__global__ void __launch_bounds__(256) extrude_fused_kernel(const __grid_constant__ ExtrudeBatch B) {
+  if ((int)blockIdx.y >= B.njobs) return;
+  const ExtrudeJob &J = B.job[blockIdx.y];
+  const int n = J.n, nst = J.nst, dir = J.dir;
+  const float *__restrict__ src = J.src;
+  float *__restrict__ dst = J.dst;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int r0 = blockIdx.x * nw + warp;
+  const bool pre = r0 < n && nst <= 32 * EXTRUDE_PRE && n <= 32 * EXTRUDE_PRE;
+  float pa[EXTRUDE_PRE], pb[EXTRUDE_PRE];
+  if (pre) {
+    const float *a = J.Arm + (size_t)r0 * nst;
+    const float *b = J.Brm + (size_t)r0 * n;
+#pragma unroll
+    for (int q = 0; q < EXTRUDE_PRE; ++q) {
+      const int t = lane + 32 * q;
+      pa[q] = t < nst ? __ldg(a + t) : 0.f;
+      pb[q] = t < n ? __ldg(b + t) : 0.f;
+    }
+  }
+  // the shift; the new column / row is left to the rows below.  n*n < 2^31
+  // (the stencil and column fit 48 KB of shared memory, so n < 12288).
+  const int nn = n * n;
+  const int off = dir == 1 ? 1 : dir == -1 ? -1 : dir == 2 ? n : -n;
+  const int stride = gridDim.x * blockDim.x;
+  for (int t0 = blockIdx.x * blockDim.x + threadIdx.x; t0 < nn; t0 += EXTRUDE_ILP * stride) {
+    float v[EXTRUDE_ILP];
+    bool keep[EXTRUDE_ILP];
+#pragma unroll
+    for (int u = 0; u < EXTRUDE_ILP; ++u) {
+      const int t = t0 + u * stride;
+      const int i = t % n, j = t / n;
+      keep[u] = t < nn && (dir == 1 ? i < n - 1 : dir == -1 ? i > 0 : dir == 2 ? j < n - 1 : j > 0);
+      v[u] = keep[u] ? src[t + off] : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < EXTRUDE_ILP; ++u)
+      if (keep[u]) dst[t0 + u * stride] = v[u];
+  }
+  if ((int)blockIdx.x * nw >= n) return;  // no rows for this block (block-uniform)
+  extern __shared__ float sh[];
+  float *z = sh;
+  float *xi = sh + nst;
+  const float ref = src[J.x0ref];
+  for (int t = threadIdx.x; t < nst; t += blockDim.x) z[t] = src[J.ist[t]] - ref;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    const U4 w = philox4x32_10(U4{(uint32_t)t, J.counter, 2u, J.layer}, J.k0, J.k1);
+    const float u1 = ((float)(w.x >> 8) + 0.5f) * 5.9604644775390625e-08f;
+    const float u2 = ((float)(w.z >> 8) + 0.5f) * 5.9604644775390625e-08f;
+    xi[t] = sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+  }
+  __syncthreads();
+  for (int r = r0; r < n; r += gridDim.x * nw) {
+    float sa = 0.f, sb = 0.f;
+    if (pre && r == r0) {
+#pragma unroll
+      for (int q = 0; q < EXTRUDE_PRE; ++q)
+        if (lane + 32 * q < nst) sa = fmaf(pa[q], z[lane + 32 * q], sa);
+#pragma unroll
+      for (int q = 0; q < EXTRUDE_PRE; ++q)
+        if (lane + 32 * q < n) sb = fmaf(pb[q], xi[lane + 32 * q], sb);
+    } else {
+      const float *a = J.Arm + (size_t)r * nst;
+      const float *b = J.Brm + (size_t)r * n;
+      for (int t = lane; t < nst; t += 32) sa = fmaf(a[t], z[t], sa);
+      for (int t = lane; t < n; t += 32) sb = fmaf(b[t], xi[t], sb);
+    }
+    sa = warp_sum(sa);
+    sb = warp_sum(sb);
+    if (lane == 0) {
+      // where extrude_shift_kernel puts y[r]
+      int at;
+      if (dir == 1)
+        at = (n - 1) + r * n;
+      else if (dir == -1)
+        at = (n - 1 - r) * n;
+      else if (dir == 2)
+        at = r + (n - 1) * n;
+      else
+        at = n - 1 - r;
+      dst[at] = (sa + J.amp * sb) + ref;
+    }
+  }
+}
+
+void launch_extrude(const ExtrudeBatch &B, int device, cudaStream_t s) {
+  AOB_REQUIRE(B.njobs >= 1 && B.njobs <= EXTRUDE_MAX_JOBS, "extrude: bad job count");
+  int nmax = 0;
+  size_t sm = 0;
+  for (int q = 0; q < B.njobs; ++q) {
+    nmax = std::max(nmax, B.job[q].n);
+    sm = std::max(sm, sizeof(float) * ((size_t)B.job[q].nst + B.job[q].n));
+  }
+  const int threads = 256;
+  const int rows_per_cta = threads / 32;
+  // enough blocks for every row of the widest layer and for four shift loads per thread
+  const int64_t nn = (int64_t)nmax * nmax;
+  const int64_t want = std::max<int64_t>((nmax + rows_per_cta - 1) / rows_per_cta,
+                                         (nn + threads * EXTRUDE_ILP - 1) / (threads * EXTRUDE_ILP));
+  const int gx = (int)std::max<int64_t>(1, std::min<int64_t>(want, 4 * num_sms(device)));
+  extrude_fused_kernel<<<dim3(gx, B.njobs), threads, sm, s>>>(B);
+  AOB_LAUNCH_CHECK("extrude_fused_kernel");
+}
+
 // ------------------------------------------------------------------ raytrace
 __global__ void raytrace_kernel(float *out, int nx, int ny, RaySources S, int reset) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -104,11 +221,33 @@ __global__ void raytrace_kernel(float *out, int nx, int ny, RaySources S, int re
 }
 
 // ------------------------------------------------------------------ DM shape
+// Each pixel sums its actuators' weighted commands in CSR order.  A group of up
+// to 16 entries -- every entry of most pixels -- has its index and weight loads
+// issued before its command gathers and those before the sum, which keeps the
+// entry order.  On saxo40's DM (77,284 pixels, 1.06 M entries, at most 25 per
+// pixel) this takes the kernel from 7.07 to 6.13 us after an L2 flush; larger
+// groups and an entry-major (coalesced) copy of the lists were slower.
+constexpr int DM_GROUP = 16;
+
 __global__ void dm_shape_kernel(float *shape, int npix, const int32_t *rowptr, const int32_t *act, const float *w,
                                 const float *com) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+    const int k0 = __ldg(rowptr + p), k1 = __ldg(rowptr + p + 1);
     float v = 0.f;
-    for (int k = rowptr[p]; k < rowptr[p + 1]; ++k) v += com[act[k]] * w[k];
+    for (int k = k0; k < k1; k += DM_GROUP) {
+      int a[DM_GROUP];
+      float ww[DM_GROUP], c[DM_GROUP];
+#pragma unroll
+      for (int u = 0; u < DM_GROUP; ++u) {
+        a[u] = k + u < k1 ? __ldg(act + k + u) : 0;
+        ww[u] = k + u < k1 ? __ldg(w + k + u) : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < DM_GROUP; ++u) c[u] = k + u < k1 ? com[a[u]] : 0.f;
+#pragma unroll
+      for (int u = 0; u < DM_GROUP; ++u)
+        if (k + u < k1) v = fmaf(c[u], ww[u], v);
+    }
     shape[p] = v;
   }
 }
@@ -197,34 +336,36 @@ aob_atmos::Layer::Layer(int dim_, int nst_, float r0, float alt, float dx, float
   amplitude = powf(r0, -5.0f / 6.0f) * 0.5f / (2.0f * (float)M_PI);
   scr[0].alloc((int64_t)dim * dim);
   scr[1].alloc((int64_t)dim * dim);
-  ytmp.alloc(dim);
+}
+
+aob::ExtrudeJob aob_atmos::Layer::next_job(int dir, int layer_index) {
+  const int n = dim;
+  aob::ExtrudeJob J;
+  J.src = scr[cur].p;
+  J.dst = scr[1 - cur].p;
+  J.Arm = Arm.p;
+  J.Brm = Brm.p;
+  J.ist = (dir == 1 || dir == -1) ? istx.p : isty.p;
+  J.n = n;
+  J.nst = nst;
+  J.dir = dir;
+  J.x0ref = (dir == 1 || dir == -2) ? n - 1 : n * (n - 1);
+  J.amp = amplitude;
+  const uint64_t sd = (uint64_t)seed;
+  J.k0 = (uint32_t)(sd & 0xffffffffu);
+  J.k1 = (uint32_t)(sd >> 32);
+  J.counter = (uint32_t)counter;
+  J.layer = (uint32_t)layer_index;
+  cur = 1 - cur;
+  ++counter;
+  return J;
 }
 
 void aob_atmos::Layer::extrude(int dir, int layer_index, cudaStream_t s) {
-  const int n = dim;
-  const float *src = scr[cur].p;
-  float *dst = scr[1 - cur].p;
-  const bool alongx = (dir == 1 || dir == -1);
-  const uint32_t *ist = alongx ? istx.p : isty.p;
-  int x0ref;
-  if (dir == 1 || dir == -2)
-    x0ref = n - 1;
-  else
-    x0ref = n * (n - 1);
-  const uint64_t sd = (uint64_t)seed;
-  const int threads = 256;
-  const int rows_per_cta = threads / 32;
-  const int grid = std::max(1, std::min((n + rows_per_cta - 1) / rows_per_cta, 2 * num_sms(device)));
-  const size_t sm = sizeof(float) * (nst + n);
-  extrude_gemv_kernel<<<grid, threads, sm, s>>>(src, n, nst, Arm.p, Brm.p, ist, x0ref, amplitude,
-                                                 (uint32_t)(sd & 0xffffffffu), (uint32_t)(sd >> 32),
-                                                 (uint32_t)counter, (uint32_t)layer_index, ytmp.p);
-  AOB_LAUNCH_CHECK("extrude_gemv_kernel");
-  const int64_t nn = (int64_t)n * n;
-  extrude_shift_kernel<<<(int)std::min<int64_t>((nn + 255) / 256, 8192), 256, 0, s>>>(dst, src, ytmp.p, n, dir);
-  AOB_LAUNCH_CHECK("extrude_shift_kernel");
-  cur = 1 - cur;
-  ++counter;
+  aob::ExtrudeBatch B{};
+  B.njobs = 1;
+  B.job[0] = next_job(dir, layer_index);
+  aob::launch_extrude(B, device, s);
 }
 
 int aob_atmos::add_screen(int dim, int nst, float r0_pix, float alt, float dx, float dy, const float *A,
@@ -265,18 +406,37 @@ void aob_atmos::refresh(int idx, cudaStream_t s) {
   for (int i = 0; i < 2 * L.dim; ++i) L.extrude(L.deltax > 0 ? 1 : -1, idx, s);
 }
 
+// Each layer's extrusions of this move run in order (x first, then y, as
+// SutraAtmos::move_atmos does); the layers are independent, so round r of the
+// move extrudes every layer that has an r-th extrusion in one launch.
 void aob_atmos::move(cudaStream_t s) {
   AOB_CUDA(cudaSetDevice(device));
+  std::vector<std::vector<int>> dirs(layers.size());
+  size_t rounds = 0;
   for (size_t l = 0; l < layers.size(); ++l) {
     Layer &L = *layers[l];
     L.accumx += L.deltax;
     L.accumy += L.deltay;
     const int dx = (int)L.accumx, dy = (int)L.accumy;
     const int cx = dx > 0 ? 1 : -1, cy = dy > 0 ? 1 : -1;
-    for (int c = 0; c < cx * dx; ++c) L.extrude(1 * cx, (int)l, s);
+    for (int c = 0; c < cx * dx; ++c) dirs[l].push_back(1 * cx);
     L.accumx -= dx;
-    for (int c = 0; c < cy * dy; ++c) L.extrude(2 * cy, (int)l, s);
+    for (int c = 0; c < cy * dy; ++c) dirs[l].push_back(2 * cy);
     L.accumy -= dy;
+    rounds = std::max(rounds, dirs[l].size());
+  }
+  for (size_t r = 0; r < rounds; ++r) {
+    aob::ExtrudeBatch B{};
+    B.njobs = 0;
+    for (size_t l = 0; l < layers.size(); ++l) {
+      if (r >= dirs[l].size()) continue;
+      B.job[B.njobs++] = layers[l]->next_job(dirs[l][r], (int)l);
+      if (B.njobs == aob::EXTRUDE_MAX_JOBS) {
+        aob::launch_extrude(B, device, s);
+        B.njobs = 0;
+      }
+    }
+    if (B.njobs) aob::launch_extrude(B, device, s);
   }
 }
 

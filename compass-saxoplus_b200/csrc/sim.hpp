@@ -24,6 +24,24 @@ __global__ void extrude_gemv_kernel(const float *screen, int n, int nst, const f
                                     const uint32_t *ist, int x0ref, float amp, uint32_t k0, uint32_t k1,
                                     uint32_t counter, uint32_t layer, float *y);
 __global__ void extrude_shift_kernel(float *dst, const float *src, const float *y, int n, int dir);
+
+// The same extrusion for several independent layers in one launch (sim.cu):
+// one job per layer, each writing the next screen `dst` from the current `src`.
+constexpr int EXTRUDE_MAX_JOBS = 16;
+struct ExtrudeJob {
+  const float *src;
+  float *dst;
+  const float *Arm, *Brm;
+  const uint32_t *ist;
+  int n, nst, dir, x0ref;
+  float amp;
+  uint32_t k0, k1, counter, layer;
+};
+struct ExtrudeBatch {
+  int njobs;
+  ExtrudeJob job[EXTRUDE_MAX_JOBS];
+};
+void launch_extrude(const ExtrudeBatch &B, int device, cudaStream_t s);
 void kolmo_factor_ab(int device, int n, int nst, const double *zz, const double *xz, const double *xx, float *A,
                      float *B);
 
@@ -38,9 +56,12 @@ struct aob_atmos {
     uint64_t counter = 0;  // extrusions so far (noise stream counter)
     int cur = 0;           // which of the two screens is current
     int device = 0;        // the atmosphere's device (grid sizing)
-    aob::DevBuf<float> scr[2], Arm, Brm, ytmp;
+    aob::DevBuf<float> scr[2], Arm, Brm;
     aob::DevBuf<uint32_t> istx, isty;
     Layer(int dim, int nst, float r0, float alt, float dx, float dy, int64_t seed);
+    // the next extrusion as a job (current screen -> the other one); flips the
+    // current screen and advances the noise counter, the launch is the caller's
+    aob::ExtrudeJob next_job(int dir, int layer_index);
     void extrude(int dir, int layer_index, cudaStream_t s);
   };
   int device = 0;
