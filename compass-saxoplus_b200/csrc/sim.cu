@@ -88,9 +88,12 @@ __global__ void extrude_shift_kernel(float *dst, const float *src, const float *
 // two per layer.  The launch is short and its data cold, so it is bound by
 // chains of memory latency, not bytes: a warp loads its first row of A and B
 // into registers before anything else (a lane's share fits for nst, n <= 512),
-// and the shift issues four loads per thread before their stores.
-constexpr int EXTRUDE_PRE = 16;  // values of a row a lane holds, per operand
-constexpr int EXTRUDE_ILP = 4;   // shift loads in flight per thread
+// the stencil's indexes are loaded at entry too and its screen values before
+// the noise is generated, and the shift issues four loads per thread before
+// their stores.
+constexpr int EXTRUDE_PRE = 16;   // values of a row a lane holds, per operand
+constexpr int EXTRUDE_PRE_Z = 2;  // stencil points a thread gathers ahead (nst <= 512)
+constexpr int EXTRUDE_ILP = 4;    // shift loads in flight per thread
 
 __global__ void __launch_bounds__(256) extrude_fused_kernel(const __grid_constant__ ExtrudeBatch B) {
   if ((int)blockIdx.y >= B.njobs) return;
@@ -100,7 +103,19 @@ __global__ void __launch_bounds__(256) extrude_fused_kernel(const __grid_constan
   float *__restrict__ dst = J.dst;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int r0 = blockIdx.x * nw + warp;
+  const bool rows = (int)blockIdx.x * nw < n;  // this block computes rows (block-uniform)
+  const bool prez = rows && nst <= EXTRUDE_PRE_Z * (int)blockDim.x;
   const bool pre = r0 < n && nst <= 32 * EXTRUDE_PRE && n <= 32 * EXTRUDE_PRE;
+  float ref = 0.f;
+  uint32_t iz[EXTRUDE_PRE_Z];
+  if (rows) ref = src[J.x0ref];
+  if (prez) {
+#pragma unroll
+    for (int q = 0; q < EXTRUDE_PRE_Z; ++q) {
+      const int t = threadIdx.x + q * blockDim.x;
+      iz[q] = t < nst ? __ldg(J.ist + t) : 0u;
+    }
+  }
   float pa[EXTRUDE_PRE], pb[EXTRUDE_PRE];
   if (pre) {
     const float *a = J.Arm + (size_t)r0 * nst;
@@ -131,17 +146,29 @@ __global__ void __launch_bounds__(256) extrude_fused_kernel(const __grid_constan
     for (int u = 0; u < EXTRUDE_ILP; ++u)
       if (keep[u]) dst[t0 + u * stride] = v[u];
   }
-  if ((int)blockIdx.x * nw >= n) return;  // no rows for this block (block-uniform)
+  if (!rows) return;
   extern __shared__ float sh[];
   float *z = sh;
   float *xi = sh + nst;
-  const float ref = src[J.x0ref];
-  for (int t = threadIdx.x; t < nst; t += blockDim.x) z[t] = src[J.ist[t]] - ref;
+  float zv[EXTRUDE_PRE_Z];
+  if (prez) {
+#pragma unroll
+    for (int q = 0; q < EXTRUDE_PRE_Z; ++q) zv[q] = (int)(threadIdx.x + q * blockDim.x) < nst ? src[iz[q]] : 0.f;
+  } else {
+    for (int t = threadIdx.x; t < nst; t += blockDim.x) z[t] = src[J.ist[t]] - ref;
+  }
   for (int t = threadIdx.x; t < n; t += blockDim.x) {
     const U4 w = philox4x32_10(U4{(uint32_t)t, J.counter, 2u, J.layer}, J.k0, J.k1);
     const float u1 = ((float)(w.x >> 8) + 0.5f) * 5.9604644775390625e-08f;
     const float u2 = ((float)(w.z >> 8) + 0.5f) * 5.9604644775390625e-08f;
     xi[t] = sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+  }
+  if (prez) {
+#pragma unroll
+    for (int q = 0; q < EXTRUDE_PRE_Z; ++q) {
+      const int t = threadIdx.x + q * blockDim.x;
+      if (t < nst) z[t] = zv[q] - ref;
+    }
   }
   __syncthreads();
   for (int r = r0; r < n; r += gridDim.x * nw) {
