@@ -11,10 +11,13 @@ iteration.  Each step is bracketed by CUDA events on the launching stream; the
 value is steps / (sum of step times).
 
 Other keys of the JSON line:
-  e2e       the same step through the C ABI call a caller makes
-            (aob_loop_step) with the phase screen copied in from pinned host
-            memory and the voltages written back into pinned host memory by
-            the fused kernel, every step;
+  e2e       the same step through the C ABI calls a caller makes, with every
+            step's phase screen copied in from pinned host memory and its
+            voltages written back into pinned host memory by the fused kernel;
+            streamed (step k+1's phase crosses the bus while step k computes,
+            the pipeline of aob_loop_run), L2 flushed before every step outside
+            its span; per_step_sync is the same one step at a time, run_api is
+            aob_loop_run itself over all steps in one call;
   roofline  the dominant kernel's algorithmic bytes / measured duration against
             the measured HBM copy bandwidth in MEASURED_PEAKS.json;
   cpu_baseline  the float64 NumPy/SciPy restatement timed on the host cores;
@@ -736,32 +739,94 @@ def main():
                 "duration_us": dt * 1e6, "peak_source": peak_kind, "timing": "graph replay, L2 flushed per launch",
                 "kernels_us": {"rtc_step": t_step * 1e6, "sh_image": t_wfs * 1e6, "ls_mvm": t_mvm * 1e6}}
 
-    # ---- e2e: through aob_loop_step with pinned host buffers ---------------
+    # ---- e2e: host phases in, host voltages out, through the C ABI ----------
+    # Streamed, as a real-time controller runs: the phase of step k + 1 crosses
+    # the bus (aob_memcpy_h2d on a copy stream, into one of two staging buffers)
+    # while step k computes (aob_memcpy_d2d into the sensor's phase, then
+    # aob_loop_step_async, whose fused kernel writes the voltages into pinned host
+    # memory) -- the pipeline aob_loop_run runs.  L2 is flushed before every step
+    # outside its span; span k runs from after the flush until both step k's
+    # voltages and step k + 1's phase have landed, so every step's copy is inside
+    # a span (step 0's in series with its own compute).
     h_phase = torch.from_numpy(np.ascontiguousarray(np.stack([s.ravel(order="F") for s in screens]))).pin_memory()
-    h_volt = torch.zeros(setup.nactu, dtype=torch.float32).pin_memory()
     e2e_steps = max(10, args.steps)
+    h_volts = torch.zeros((e2e_steps, setup.nactu), dtype=torch.float32).pin_memory()
+    h_volt = h_volts[0]  # one step's voltages (pinned)
+    cstream = torch.cuda.Stream(device)
+    cptr = cstream.cuda_stream
+    stage = [torch.empty(n * n, dtype=torch.float32, device="cuda") for _ in range(2)]
+
+    def h2d(k):
+        _lib.call("aob_memcpy_h2d_async", stage[k % 2].data_ptr(), h_phase[k % nscreen].data_ptr(), nbytes_phase,
+                  cptr)
+
     for i in range(3):
         loop.step(h_phase[i % nscreen].data_ptr(), h_volt.data_ptr(), noise=True, stream=sptr)
+    torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(e2e_steps)]
+    copied = [torch.cuda.Event() for _ in range(e2e_steps)]
+    for k, (a, b) in enumerate(ev):
+        flush.zero_()
+        a.record(stream)
+        cstream.wait_event(a)  # the copy stream follows the flush (and the last read of its staging buffer)
+        if k == 0:
+            h2d(0)
+            copied[0].record(cstream)
+        if k + 1 < e2e_steps:
+            h2d(k + 1)
+            copied[k + 1].record(cstream)
+        stream.wait_event(copied[k])
+        _lib.call("aob_memcpy_d2d", phase_ptr, stage[k % 2].data_ptr(), nbytes_phase, sptr)
+        loop.step(None, h_volts[k].data_ptr(), noise=True, stream=sptr, wait=False)
+        if k + 1 < e2e_steps:
+            stream.wait_event(copied[k + 1])
+        b.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in ev)
+
+    # the same steps one at a time: each step's phase copy, kernel and voltages,
+    # then the host waits (no overlap), L2 flushed before each
+    ev1 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(e2e_steps)]
     wall = 0.0
-    for i, (a, b) in enumerate(ev):
+    for i, (a, b) in enumerate(ev1):
         flush.zero_()
         torch.cuda.synchronize()
         w0 = time.perf_counter()
         a.record(stream)
-        # enqueue: phase in by the copy engine, the fused kernel, voltages written
-        # into the pinned host buffer by its epilogue; b completes when they are there
         loop.step(h_phase[i % nscreen].data_ptr(), h_volt.data_ptr(), noise=True, stream=sptr, wait=False)
         b.record(stream)
         b.synchronize()
         wall += time.perf_counter() - w0
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(dist, torch, [sum(a.elapsed_time(b) for a, b in ev)], "cuda")[0]
+    sync_ms = sum(a.elapsed_time(b) for a, b in ev1)
+
+    # aob_loop_run itself: e2e_steps streamed steps in one call, no flush between
+    # them (the command matrix stays in L2), device span and the call's wall clock
+    run_wall = float("nan")
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    flush.zero_()
+    torch.cuda.synchronize()
+    a.record(stream)
+    w0 = time.perf_counter()
+    loop.run(h_phase.data_ptr(), e2e_steps, h_volts.data_ptr(), noise=True, stream=sptr, nphases=nscreen)
+    run_wall = time.perf_counter() - w0
+    b.record(stream)
+    torch.cuda.synchronize()
+    run_ms = a.elapsed_time(b)
+    e2e_ms, sync_ms, run_ms, wall, run_wall = max_over_ranks(dist, torch, [e2e_ms, sync_ms, run_ms, wall, run_wall],
+                                                             "cuda")
     e2e = {"value": job_rate(ws, e2e_steps, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": nbytes_phase,
-           "d2h_bytes_per_step": setup.nactu * 4, "wall_clock_value": e2e_steps / wall,
-           "call": "aob_loop_step_async(host phase -> host voltages), then an event the host waits on: phase by copy "
-                   "engine, voltages written into the pinned host buffer by the fused kernel; device-timed from before "
-                   "the phase copy to after the voltages, wall_clock_value includes the host's wait"}
+           "d2h_bytes_per_step": setup.nactu * 4, "ms_per_step": e2e_ms / e2e_steps,
+           "call": "streamed: aob_memcpy_h2d_async of step k+1's pinned host phase on a copy stream while step k runs "
+                   "(aob_memcpy_d2d into the sensor's phase, aob_loop_step_async: the fused kernel writes the voltages "
+                   "into pinned host memory); L2 flushed before each step outside its span; span k = until step k's "
+                   "voltages and step k+1's phase are both there",
+           "per_step_sync": {"value": job_rate(ws, e2e_steps, sync_ms), "wall_clock_value": ws * e2e_steps / wall,
+                             "call": "aob_loop_step_async then an event the host waits on, one step at a time "
+                                     "(phase copy, kernel, voltages in series), L2 flushed before each"},
+           "run_api": {"value": job_rate(ws, e2e_steps, run_ms), "wall_clock_value": ws * e2e_steps / run_wall,
+                       "call": f"aob_loop_run: {e2e_steps} streamed steps in one call (pinned phases cycled, pinned "
+                               "voltages), no L2 flush between steps"}}
 
     # ---- the same iteration with the learned reconstructor in place of the LS
     # matrix (2496 -> 1024 -> 1024 -> 1377 + the linear skip; its Strehl parity with

@@ -718,6 +718,30 @@ class Loop:
         if fn(self.h, hp, hv, 1 if noise else 0, stream) != 0:
             raise _lib.AobError(f"{name}: {_lib.lib().aob_last_error().decode()}")
 
+    def run(self, host_phases, nsteps, host_voltages=None, noise=True, stream=None, wait=True, nphases=None):
+        """``nsteps`` iterations streamed from the host (aob_loop_run): step k
+        takes row ``k % nphases`` of ``host_phases`` (a C-contiguous float32
+        array, one Fortran-order phase per row, or an int host address with
+        ``nphases`` given) and writes row k of ``host_voltages`` (nsteps x nactu
+        float32, or None).  The voltages equal ``nsteps`` calls of ``step``; the
+        next phase crosses the bus while the current step computes, so pinned
+        buffers give the overlap."""
+        if type(host_phases) is int:
+            if nphases is None:
+                raise ValueError("Loop.run: nphases is required with a host address")
+            hp = host_phases
+        else:
+            a = host_phases
+            if not isinstance(a, np.ndarray) or a.dtype != np.float32 or not a.flags.c_contiguous or a.ndim < 2:
+                raise ValueError("Loop.run: host_phases must be a C-contiguous float32 array, one phase per row")
+            nphases, hp = a.shape[0], a.ctypes.data
+        hv = host_voltages
+        if isinstance(hv, np.ndarray):
+            if hv.dtype != np.float32 or not hv.flags.c_contiguous or hv.shape[0] < nsteps:
+                raise ValueError("Loop.run: host_voltages must be a C-contiguous float32 array with nsteps rows")
+            hv = hv.ctypes.data
+        call("aob_loop_run", self.h, hp, int(nphases), int(nsteps), hv, 1 if noise else 0, stream, 1 if wait else 0)
+
     def step_mlp(self, net, threshold, host_phase=None, host_voltage=None, noise=True, stream=None, wait=True):
         """One iteration with the learned reconstructor ``net`` (an
         ``aob200.mlp.MlpReconstructor``) in place of the LS matrix: sensor image

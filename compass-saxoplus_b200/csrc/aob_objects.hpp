@@ -265,6 +265,14 @@ struct aob_loop {
   void persist_flush(void *dev_buf, size_t bytes, cudaStream_t s);
   uint32_t persist_cmd = 0;              // last command rung (1: a flush; the next step resets it)
   uint64_t persist_rtc_steps = 0;        // RTC steps rung since persist_start
+  // streamed steps (run): the next step's host phase is copied on a stream of
+  // its own into one of two staging buffers while the current step computes
+  cudaStream_t run_copy = nullptr;
+  cudaEvent_t run_entry = nullptr, run_copied[2] = {nullptr, nullptr}, run_used[2] = {nullptr, nullptr};
+  aob::DevBuf<float> run_stage[2];
+  void run(const float *host_phases, int nphases, int nsteps, float *host_volts, bool noise, cudaStream_t s,
+           bool wait);
+  void run_release();
   aob_loop(aob_sh *w, aob_centro *c, aob_ls *l);
   ~aob_loop();
   void device_step(bool noise, cudaStream_t s, bool frame_on_device);

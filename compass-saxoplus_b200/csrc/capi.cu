@@ -89,6 +89,13 @@ int aob_memcpy_h2d(void *dst, const void *src, size_t bytes, void *stream) {
   AOB_CUDA(cudaStreamSynchronize(S(stream)));
   AOB_API_END
 }
+int aob_memcpy_h2d_async(void *dst, const void *src, size_t bytes, void *stream) {
+  AOB_API_BEGIN
+  if (bytes == 0) return AOB_OK;
+  NEED(dst); NEED(src);
+  AOB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, S(stream)));
+  AOB_API_END
+}
 int aob_memcpy_d2d(void *dst, const void *src, size_t bytes, void *stream) {
   AOB_API_BEGIN
   if (bytes == 0) return AOB_OK;

@@ -70,7 +70,21 @@ aob_loop::~aob_loop() {
     persist_stop();
   } catch (...) {
   }
+  run_release();
   drop_graphs();
+}
+
+void aob_loop::run_release() {
+  if (run_copy) {
+    cudaStreamSynchronize(run_copy);
+    cudaStreamDestroy(run_copy);
+    run_copy = nullptr;
+  }
+  for (cudaEvent_t *e : {&run_entry, &run_copied[0], &run_copied[1], &run_used[0], &run_used[1]})
+    if (*e) {
+      cudaEventDestroy(*e);
+      *e = nullptr;
+    }
 }
 
 void aob_loop::drop_graphs() {
@@ -390,6 +404,53 @@ void aob_loop::step(const float *host_phase, float *host_voltage, bool noise, cu
   }
 }
 
+// nsteps iterations with host phases and host voltages, as nsteps calls of
+// step() would run them (the same kernels in the same order on s, so the same
+// voltages bit for bit), except that the phase of step k + 1 crosses the bus
+// while step k computes: it is copied on run_copy into the staging buffer step
+// k - 1 used, and step k + 1 starts with a device copy of it into the sensor's
+// phase.  Step k reads host_phases[k % nphases] and writes host_volts[k].
+void aob_loop::run(const float *host_phases, int nphases, int nsteps, float *host_volts, bool noise, cudaStream_t s,
+                   bool wait) {
+  AOB_REQUIRE(!persist_on, "loop.run: the persistent kernel is running (persist_step / persist_stop)");
+  AOB_REQUIRE(host_phases && nphases >= 1 && nsteps >= 1,
+              "loop.run: host_phases, nphases >= 1 and nsteps >= 1 are required");
+  AOB_CUDA(cudaSetDevice(wfs->device));
+  const int64_t np = wfs->phase.n;
+  const size_t pb = wfs->phase.bytes();
+  if (!run_copy) {
+    AOB_CUDA(cudaStreamCreateWithFlags(&run_copy, cudaStreamNonBlocking));
+    AOB_CUDA(cudaEventCreateWithFlags(&run_entry, cudaEventDisableTiming));
+    for (int b = 0; b < 2; ++b) {
+      AOB_CUDA(cudaEventCreateWithFlags(&run_copied[b], cudaEventDisableTiming));
+      AOB_CUDA(cudaEventCreateWithFlags(&run_used[b], cudaEventDisableTiming));
+    }
+  }
+  for (int b = 0; b < 2; ++b)
+    if (run_stage[b].n != np) run_stage[b].alloc(np);
+  auto phase_of = [&](int k) { return host_phases + (size_t)(k % nphases) * (size_t)np; };
+  // the copies start after all the work already queued on s (an earlier run's
+  // last steps may still read the staging buffers)
+  AOB_CUDA(cudaEventRecord(run_entry, s));
+  AOB_CUDA(cudaStreamWaitEvent(run_copy, run_entry, 0));
+  AOB_CUDA(cudaMemcpyAsync(run_stage[0].p, phase_of(0), pb, cudaMemcpyHostToDevice, run_copy));
+  AOB_CUDA(cudaEventRecord(run_copied[0], run_copy));
+  for (int k = 0; k < nsteps; ++k) {
+    const int b = k & 1;
+    if (k + 1 < nsteps) {
+      // buffer 1 - b was last read by step k - 1's device copy
+      if (k >= 1) AOB_CUDA(cudaStreamWaitEvent(run_copy, run_used[1 - b], 0));
+      AOB_CUDA(cudaMemcpyAsync(run_stage[1 - b].p, phase_of(k + 1), pb, cudaMemcpyHostToDevice, run_copy));
+      AOB_CUDA(cudaEventRecord(run_copied[1 - b], run_copy));
+    }
+    AOB_CUDA(cudaStreamWaitEvent(s, run_copied[b], 0));
+    AOB_CUDA(cudaMemcpyAsync(wfs->phase.p, run_stage[b].p, pb, cudaMemcpyDeviceToDevice, s));
+    AOB_CUDA(cudaEventRecord(run_used[b], s));
+    step(nullptr, host_volts ? host_volts + (size_t)k * (size_t)ls->nactu : nullptr, noise, s, false);
+  }
+  if (wait) AOB_CUDA(cudaStreamSynchronize(s));
+}
+
 extern "C" {
 
 int aob_loop_create(aob_loop **out, aob_sh *wfs, aob_centro *centro, aob_ls *ls) {
@@ -534,6 +595,19 @@ int aob_loop_step_async(aob_loop *l, const float *host_phase, float *host_voltag
   try {
     if (!l) throw Error("aob_loop_step_async: null handle");
     l->step(host_phase, host_voltage, noise != 0, reinterpret_cast<cudaStream_t>(stream), false);
+    return AOB_OK;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return AOB_ERR;
+  }
+}
+
+int aob_loop_run(aob_loop *l, const float *host_phases, int nphases, int nsteps, float *host_voltages, int noise,
+                 void *stream, int wait) {
+  try {
+    if (!l) throw Error("aob_loop_run: null handle");
+    l->run(host_phases, nphases, nsteps, host_voltages, noise != 0, reinterpret_cast<cudaStream_t>(stream),
+           wait != 0);
     return AOB_OK;
   } catch (const std::exception &e) {
     set_last_error(e.what());

@@ -43,6 +43,11 @@ int aob_device_name(int device, char *buf, int len, int *num_sms);
  * caller (the carma array buffer protocol, python_module/carma/src/obj.hpp:32-76). */
 int aob_memcpy_d2h(void *dst_host, const void *src_dev, size_t bytes, void *stream);
 int aob_memcpy_h2d(void *dst_dev, const void *src_host, size_t bytes, void *stream);
+/* aob_memcpy_h2d without the final wait: the copy is enqueued on the stream
+ * and the call returns (host memory must stay unchanged until the stream has
+ * reached the copy; pinned memory keeps it asynchronous).  No counterpart in
+ * the reference, whose array copies complete before they return. */
+int aob_memcpy_h2d_async(void *dst_dev, const void *src_host, size_t bytes, void *stream);
 int aob_memcpy_d2d(void *dst_dev, const void *src_dev, size_t bytes, void *stream);
 int aob_malloc(void **dev_ptr, size_t bytes, int device);
 int aob_free(void *dev_ptr);
@@ -554,6 +559,21 @@ int aob_loop_step(aob_loop *l, const float *host_phase, float *host_voltage, int
  * the copies synchronous).  For callers that step many iterations and read the
  * results later, as the reference's supervisor loop does between frames. */
 int aob_loop_step_async(aob_loop *l, const float *host_phase, float *host_voltage, int noise, void *stream);
+/* nsteps iterations streamed from the host: no single counterpart in the
+ * reference, whose supervisor calls set_phase, comp_image, do_centroids,
+ * do_control and comp_voltage once per frame (CompassSupervisor.next,
+ * shesha/shesha/supervisor/compassSupervisor.py:175); this is
+ * nsteps of those frames in one call.  Step k takes host_phases[k % nphases]
+ * (nphases phases of npup*npup floats back to back) and writes its voltages to
+ * host_voltages + k*nactu (may be NULL).  The kernels and their order are those
+ * of nsteps aob_loop_step calls, so the voltages are the same bit for bit; the
+ * phase of step k+1 is copied to the device on a stream of the loop's own while
+ * step k computes.  Host buffers should be pinned: pageable ones make the copies
+ * synchronous and remove the overlap.  wait != 0 waits for the stream at the end;
+ * otherwise host_phases must stay unchanged and host_voltages unread until the
+ * stream reaches that point. */
+int aob_loop_run(aob_loop *l, const float *host_phases, int nphases, int nsteps, float *host_voltages, int noise,
+                 void *stream, int wait);
 /* One iteration with the learned reconstructor m in place of the LS matrix (no
  * counterpart in the reference, whose reconstructors are linear): the sensor
  * image with fused centroids into the controller, aob_mlp_comp_com's control

@@ -365,3 +365,65 @@ def test_mvm_kernels_agree_and_status_clean(core, prec):
     base = out[(2, 0)]
     for k, v in out.items():
         assert rel_rms(v, base) < 1e-6, k
+
+
+@pytest.mark.parametrize("graph", [False, True])
+@pytest.mark.parametrize("delay", [0.0, 1.4])
+@pytest.mark.parametrize("io", [1, 0])
+def test_streamed_run_equals_steps(core, graph, delay, io):
+    """aob_loop_run streams nsteps host phases (the next one copied while the
+    current step computes) and equals nsteps aob_loop_step calls bit for bit:
+    every step's voltages, the sensor images, the controller state and the noise
+    frame counter, across two runs in a row (the second one asynchronous) and
+    with pageable numpy buffers as well as pinned ones."""
+    import torch
+
+    g = sh_geometry("sh16")
+    nact = 97
+    rng = np.random.default_rng(9)
+    cm = (rng.standard_normal((nact, 2 * g.nvalid)) * 0.01).astype(np.float32)
+
+    def build():
+        w = core.ShWfs.from_geometry(g, noise=0.5, seed=6)
+        c = core.Centroider(g.nvalid, g.npix / 2 - 0.5, g.pixsize, "wcog")
+        c.set_npix(g.npix)
+        c.load_validpos(g.validsubsx, g.validsubsy)
+        c.set_threshold(1.0)
+        c.load_weights(np.ones((g.npix, g.npix), np.float32))
+        ls = core.LsController(2 * g.nvalid, nact, delay=delay)
+        ls.set_cmat(cm)
+        ls.set_gain(0.3)
+        ls.set_com_range(-0.5, 0.5)
+        loop = core.Loop(w, c, ls, graph=graph)
+        loop.set_host_io(io)
+        return w, ls, loop
+
+    wa, la, loopa = build()
+    wb, lb, loopb = build()
+    nph = 3
+    screens = [kolmogorov_screen(g.tel.n, 20.0, seed=60 + i).ravel(order="F") for i in range(nph)]
+    ph = torch.from_numpy(np.ascontiguousarray(np.stack(screens))).pin_memory()
+    n1, n2 = 7, 4
+    va = torch.zeros((n1, nact), dtype=torch.float32).pin_memory()
+    vb = torch.zeros(nact, dtype=torch.float32).pin_memory()
+    loopa.run(ph.data_ptr(), n1, va.data_ptr(), noise=True, nphases=nph)
+    for k in range(n1):
+        loopb.step(ph[k % nph].data_ptr(), vb.data_ptr(), noise=True)
+        np.testing.assert_array_equal(va[k].numpy(), vb.numpy())
+    # a second, asynchronous run from pageable numpy buffers continues the same state
+    ph_np = np.ascontiguousarray(ph.numpy()[::-1])
+    va2 = np.zeros((n2, nact), np.float32)
+    loopa.run(ph_np, n2, va2, noise=True, wait=False)
+    torch.cuda.synchronize()
+    for k in range(n2):
+        loopb.step(ph_np[k % nph], vb.data_ptr(), noise=True)
+        np.testing.assert_array_equal(va2[k], vb.numpy())
+    np.testing.assert_array_equal(np.array(wa.d_phase), np.array(wb.d_phase))
+    np.testing.assert_array_equal(np.array(wa.d_binimg), np.array(wb.d_binimg))
+    np.testing.assert_array_equal(np.array(la.buffer("com")), np.array(lb.buffer("com")))
+    np.testing.assert_array_equal(np.array(la.buffer("centroids")), np.array(lb.buffer("centroids")))
+    assert wa.frame == wb.frame == n1 + n2
+    assert la.status() == 0
+    assert np.abs(va2).max() > 0
+    with pytest.raises(Exception):
+        loopa.run(ph_np, 0, None)
