@@ -84,7 +84,7 @@ __global__ void extrude_shift_kernel(float *dst, const float *src, const float *
 // the next screen, and the grid shifts the rest of the screen by one sample as
 // extrude_shift_kernel does.  The arithmetic of both is unchanged (each row's
 // dot products keep their order), so the screens equal the two-kernel
-// sequence's bit for bit, with one launch per round of extrusions instead of
+// sequence's bit for bit, with one launch per pass of extrusions instead of
 // two per layer.  The launch is short and its data cold, so it is bound by
 // chains of memory latency, not bytes: a warp loads its first row of A and B
 // into registers before anything else (a lane's share fits for nst, n <= 512),
@@ -434,12 +434,12 @@ void aob_atmos::refresh(int idx, cudaStream_t s) {
 }
 
 // Each layer's extrusions of this move run in order (x first, then y, as
-// SutraAtmos::move_atmos does); the layers are independent, so round r of the
+// SutraAtmos::move_atmos does); the layers are independent, so pass r of the
 // move extrudes every layer that has an r-th extrusion in one launch.
 void aob_atmos::move(cudaStream_t s) {
   AOB_CUDA(cudaSetDevice(device));
   std::vector<std::vector<int>> dirs(layers.size());
-  size_t rounds = 0;
+  size_t passes = 0;
   for (size_t l = 0; l < layers.size(); ++l) {
     Layer &L = *layers[l];
     L.accumx += L.deltax;
@@ -450,9 +450,9 @@ void aob_atmos::move(cudaStream_t s) {
     L.accumx -= dx;
     for (int c = 0; c < cy * dy; ++c) dirs[l].push_back(2 * cy);
     L.accumy -= dy;
-    rounds = std::max(rounds, dirs[l].size());
+    passes = std::max(passes, dirs[l].size());
   }
-  for (size_t r = 0; r < rounds; ++r) {
+  for (size_t r = 0; r < passes; ++r) {
     aob::ExtrudeBatch B{};
     B.njobs = 0;
     for (size_t l = 0; l < layers.size(); ++l) {
